@@ -1,0 +1,410 @@
+/*
+ * psycles_cuda.h -- C ABI of the B200 path-trace integrator.
+ *
+ * This is the drop-in boundary for Psycles' render contract.  Each entry
+ * point replaces one call of the reference interface; the mapping is given
+ * beside every declaration (paths are relative to the Psycles source tree):
+ *
+ *   contract::RendererBackend::compile_scene   include/psycles/contract/render.h:176
+ *   contract::RendererBackend::create_session  include/psycles/contract/render.h:179
+ *   contract::RenderSession::reset             include/psycles/contract/render.h:167
+ *   contract::RenderSession::render_samples    include/psycles/contract/render.h:168
+ *   contract::RenderSession::cancel            include/psycles/contract/render.h:169
+ *   contract::OutputSink::write (pass data)    include/psycles/contract/render.h:141
+ *   contract::CompiledScene::source_revision   include/psycles/contract/render.h:153
+ *
+ * Conventions: plain pointers and sizes, no exceptions, every call returns a
+ * psy_status; psy_last_error() returns a thread-local message for the last
+ * failing call.  Matrices are column-major 4x4 (elements 0..3 are column 0,
+ * the translation is elements 12..14), the layout of psycles::Mat4f
+ * (include/psycles/core/math.h:31).
+ */
+#ifndef PSYCLES_CUDA_H
+#define PSYCLES_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSY_ABI_VERSION 1u
+
+typedef enum psy_status {
+    PSY_OK = 0,
+    PSY_ERROR_INVALID_ARGUMENT = 1,
+    PSY_ERROR_OUT_OF_MEMORY = 2,
+    PSY_ERROR_CUDA = 3,
+    PSY_ERROR_CANCELLED = 4,
+    PSY_ERROR_RANGE = 5,
+    PSY_ERROR_UNSUPPORTED = 6,
+    PSY_ERROR_STATE = 7,
+    PSY_ERROR_TIMEOUT = 8
+} psy_status;
+
+typedef struct psy_context psy_context;
+typedef struct psy_scene psy_scene;
+typedef struct psy_session psy_session;
+
+/* ---------------------------------------------------------------- scene -- */
+
+/* Triangle mesh.  Mirrors contract::MeshDesc positions/normals/indices
+ * (include/psycles/contract/scene.h).  `materials` optionally assigns a
+ * material per triangle (Cycles' per-face shader); NULL uses the instance
+ * material. */
+typedef struct psy_mesh_desc {
+    const float *positions;      /* vertex_count * 3 */
+    const float *normals;        /* vertex_count * 3; may be NULL if !smooth */
+    const uint32_t *indices;     /* triangle_count * 3 */
+    const uint32_t *materials;   /* triangle_count, or NULL */
+    uint32_t vertex_count;
+    uint32_t triangle_count;
+    uint32_t smooth;             /* 1: interpolate vertex normals */
+    uint32_t reserved;
+} psy_mesh_desc;
+
+/* Contract RayVisibility bits (include/psycles/contract/scene.h:282). */
+#define PSY_VISIBILITY_CAMERA 1u
+#define PSY_VISIBILITY_DIFFUSE 2u
+#define PSY_VISIBILITY_GLOSSY 4u
+#define PSY_VISIBILITY_TRANSMISSION 8u
+#define PSY_VISIBILITY_SHADOW 16u
+#define PSY_VISIBILITY_VOLUME_SCATTER 32u
+#define PSY_VISIBILITY_ALL 63u
+
+/* Mirrors contract::InstanceDesc (include/psycles/contract/scene.h:304). */
+typedef struct psy_instance_desc {
+    float object_to_world[16];   /* column-major */
+    uint32_t mesh;
+    uint32_t material;
+    uint32_t visibility;         /* PSY_VISIBILITY_* */
+    uint32_t reserved;
+} psy_instance_desc;
+
+/* Closure operations of the in-scope SurfaceProgram subset
+ * (compiler::ClosureOperation, include/psycles/compiler/surface_program.h:415). */
+typedef enum psy_closure_op {
+    PSY_CLOSURE_NULL = 0,
+    PSY_CLOSURE_DIFFUSE = 1,
+    PSY_CLOSURE_EMISSION = 2,
+    PSY_CLOSURE_TRANSPARENT = 3,
+    PSY_CLOSURE_ADD = 4,
+    PSY_CLOSURE_MIX = 5
+} psy_closure_op;
+
+/* One closure instruction.  `color` names a vector slot and `scalar` a
+ * scalar slot of the material's parameter block (emission strength, mix
+ * factor); `a`/`b` are child instruction indices for add and mix. */
+typedef struct psy_closure_instruction {
+    uint32_t op;
+    uint32_t a;
+    uint32_t b;
+    uint32_t color;
+    uint32_t scalar;
+} psy_closure_instruction;
+
+/* contract::EmissionSampling (include/psycles/contract/scene.h:69). */
+#define PSY_EMISSION_SAMPLING_NONE 0u
+#define PSY_EMISSION_SAMPLING_AUTOMATIC 1u
+#define PSY_EMISSION_SAMPLING_FRONT 2u
+#define PSY_EMISSION_SAMPLING_BACK 3u
+#define PSY_EMISSION_SAMPLING_FRONT_BACK 4u
+
+/* A compiled SurfaceProgram (closure tree) with its SurfaceParameterBlock
+ * (compiler::SurfaceProgram surface_program.h:512, SurfaceParameterBlock
+ * surface_program.h:570). */
+typedef struct psy_material_desc {
+    const psy_closure_instruction *closures;
+    uint32_t closure_count;
+    uint32_t root;
+    const float *scalars;        /* scalar_count floats */
+    uint32_t scalar_count;
+    uint32_t vector_count;
+    const float *vectors;        /* vector_count * 3 floats */
+    uint32_t emission_sampling;  /* PSY_EMISSION_SAMPLING_* */
+    uint32_t reserved;
+} psy_material_desc;
+
+/* contract::LightType order (include/psycles/contract/scene.h:369). */
+typedef enum psy_light_type {
+    PSY_LIGHT_POINT = 0,
+    PSY_LIGHT_SPOT = 1,
+    PSY_LIGHT_AREA = 2,
+    PSY_LIGHT_DISTANT = 3
+} psy_light_type;
+
+#define PSY_LIGHT_FLAG_SPHERE 1u      /* point/spot radius is a sphere */
+#define PSY_LIGHT_FLAG_NORMALIZE 2u   /* divide power by emitter area */
+
+/* Analytic light (LightGpu, src/luisa/path_tracer_types.h:142). */
+typedef struct psy_light_desc {
+    uint32_t type;
+    uint32_t flags;
+    uint32_t max_bounces;
+    uint32_t reserved;
+    float position[3];
+    float axis_x[3];
+    float axis_y[3];
+    float axis_z[3];             /* spot/area: emission axis; sun: D at centre */
+    float axis_scale[3];
+    float color[3];
+    float power;
+    float radius;
+    float size_u;
+    float size_v;
+    float spot_angle;
+    float spot_smooth;
+    float angle;                 /* sun angular diameter */
+} psy_light_desc;
+
+/* contract::CameraDesc (include/psycles/contract/scene.h:347),
+ * perspective projection. */
+typedef struct psy_camera_desc {
+    float camera_to_world[16];   /* column-major */
+    float field_of_view;         /* vertical angle, radians */
+    float horizontal_field_of_view;
+    uint32_t sensor_fit;         /* 0 automatic, 1 horizontal, 2 vertical */
+    float lens_shift_x;
+    float lens_shift_y;
+    float near_clip;
+    float far_clip;
+    uint32_t reserved;
+} psy_camera_desc;
+
+/* A flattened SceneSnapshot (include/psycles/contract/scene.h:458). */
+typedef struct psy_scene_desc {
+    const psy_mesh_desc *meshes;
+    const psy_instance_desc *instances;
+    const psy_material_desc *materials;
+    const psy_light_desc *lights;
+    uint32_t mesh_count;
+    uint32_t instance_count;
+    uint32_t material_count;
+    uint32_t light_count;
+    psy_camera_desc camera;
+    float background[3];         /* constant world colour */
+    uint32_t world_visibility;   /* PSY_VISIBILITY_* */
+    uint64_t revision;           /* SceneSnapshot revision */
+} psy_scene_desc;
+
+/* ------------------------------------------------------------- settings -- */
+
+/* contract::PassKind values used by psy_session_read_pass
+ * (include/psycles/contract/render.h:14). */
+#define PSY_PASS_COMBINED 0u
+#define PSY_PASS_NORMAL 2u
+#define PSY_PASS_ALBEDO 4u
+#define PSY_PASS_DENOISING_NORMAL 18u
+#define PSY_PASS_DENOISING_ALBEDO 19u
+#define PSY_PASS_SAMPLE_COUNT 20u
+
+/* contract::PixelFilter (render.h:69). */
+#define PSY_FILTER_BOX 0u
+#define PSY_FILTER_GAUSSIAN 1u
+#define PSY_FILTER_BLACKMAN_HARRIS 2u
+
+/* contract::DirectLightSampling (render.h:75). */
+#define PSY_DIRECT_LIGHT_MIS 0u
+#define PSY_DIRECT_LIGHT_FORWARD 1u
+#define PSY_DIRECT_LIGHT_NEE 2u
+
+/* contract::RenderSettings + PathIntegratorSettings (render.h:81-115) and
+ * the next_event_estimation option of the Luisa backend
+ * (include/psycles/luisa/path_tracer.h:46). */
+typedef struct psy_render_settings {
+    uint32_t full_width;
+    uint32_t full_height;
+    uint32_t window_x;
+    uint32_t window_y;
+    uint32_t window_width;       /* 0 -> full extent */
+    uint32_t window_height;
+    uint32_t seed;
+    uint32_t transparent_background;
+    uint32_t pixel_filter;
+    float filter_width;
+    float pass_alpha_threshold;
+    uint32_t max_bounces;
+    uint32_t min_bounces;
+    uint32_t diffuse_bounces;
+    uint32_t glossy_bounces;
+    uint32_t transmission_bounces;
+    uint32_t transparent_min_bounces;
+    uint32_t transparent_max_bounces;
+    float sample_clamp_direct;
+    float sample_clamp_indirect;
+    float film_exposure;
+    float light_sampling_threshold;
+    uint32_t use_light_tree;
+    uint32_t direct_light_sampling;
+    uint32_t next_event_estimation;
+    uint32_t reserved;
+} psy_render_settings;
+
+/* Fills the defaults of contract::RenderSettings / PathIntegratorSettings. */
+void psy_render_settings_default(psy_render_settings *settings);
+
+/* --------------------------------------------------------- entry points -- */
+
+const char *psy_last_error(void);
+uint32_t psy_abi_version(void);
+
+/* One context per CUDA device; owns the stream all sessions launch on. */
+psy_status psy_context_create(int device, psy_context **out);
+void psy_context_destroy(psy_context *context);
+
+/* RendererBackend::compile_scene (render.h:176, implemented by
+ * LuisaPathTracerBackend at src/luisa/path_tracer_scene.cpp:50): uploads
+ * geometry, builds the two-level BVH, parameter blocks, emitter tables and
+ * the flat light distribution.  The descriptor is copied; the caller may
+ * free it on return. */
+psy_status psy_scene_compile(psy_context *context, const psy_scene_desc *desc,
+                             psy_scene **out);
+void psy_scene_destroy(psy_scene *scene);
+/* CompiledScene::source_revision (render.h:153). */
+uint64_t psy_scene_source_revision(const psy_scene *scene);
+
+/* Parameter-only material edit: the MaterialLibrary `parameters_rebound`
+ * outcome (src/compiler/material_library.cpp:51-97) applied on the device.
+ * Rewrites the material's parameter block in place; no BVH or program
+ * rebuild.  Counts must equal the compiled block's counts. */
+psy_status psy_scene_rebind_parameters(psy_scene *scene, uint32_t material,
+                                       const float *scalars,
+                                       uint32_t scalar_count,
+                                       const float *vectors,
+                                       uint32_t vector_count);
+
+/* RendererBackend::create_session (render.h:179,
+ * src/luisa/path_tracer.cpp:23).  Returns PSY_ERROR_INVALID_ARGUMENT where
+ * the reference returns nullptr. */
+psy_status psy_session_create(psy_scene *scene,
+                              const psy_render_settings *settings,
+                              psy_session **out);
+void psy_session_destroy(psy_session *session);
+/* RenderSession::reset (render.h:167): clears the film. */
+psy_status psy_session_reset(psy_session *session,
+                             const psy_render_settings *settings);
+
+/* RenderSession::render_samples (render.h:168,
+ * src/luisa/path_tracer_session.cpp:272).  Renders AA samples
+ * [first + offset, first + offset + count) of a render whose total sample
+ * count is `total` (SampleRange, render.h:119).  Blocks until the film is
+ * updated.  Fails with PSY_ERROR_RANGE for count == 0 or a range beyond
+ * total, PSY_ERROR_STATE if total changed within the session, and
+ * PSY_ERROR_CANCELLED after cancel(). */
+psy_status psy_session_render_samples(psy_session *session, uint32_t first,
+                                      uint32_t count, uint32_t offset,
+                                      uint32_t total);
+
+/* RenderSession::cancel (render.h:169); callable from any thread. */
+void psy_session_cancel(psy_session *session);
+
+/* Pass readback, the data write_passes() hands to OutputSink::write
+ * (src/luisa/path_tracer_session.cpp:71-270): the window's pixels,
+ * row-major, `channels` floats each (4, or 1 for sample count), already
+ * divided by the per-pixel sample count.  `capacity` counts floats. */
+psy_status psy_session_read_pass(psy_session *session, uint32_t pass_kind,
+                                 float *out, uint64_t capacity,
+                                 uint32_t *channels);
+
+/* Rendered samples per pixel so far. */
+uint32_t psy_session_rendered_samples(const psy_session *session);
+
+/* Per-path trace of one (full-film pixel, absolute sample) for the next
+ * render_samples call (LuisaPathTraceRequest,
+ * include/psycles/luisa/path_tracer.h:34).  x counts from the left and y
+ * from the top of the output image. */
+#define PSY_TRACE_MAX_EVENTS 16u
+typedef struct psy_path_event {
+    uint32_t rng_offset;
+    uint32_t bounce;
+    uint32_t transparent_bounce;
+    uint32_t flag;               /* path flags after the transition */
+    uint32_t visibility;         /* Cycles path visibility after it */
+    uint32_t hit_object;         /* 0xffffffff on a miss */
+    uint32_t hit_primitive;
+    uint32_t closure_index;      /* selected closure, 0xffffffff if none */
+    uint32_t label;              /* Cycles ClosureLabel of the sample */
+    uint32_t light_kind;         /* LightDistributionEmitterKind */
+    uint32_t light_index;
+    uint32_t terminated;         /* 1 when the path ended at this event */
+    float hit_t;
+    float hit_u;
+    float hit_v;
+    float random_terminate;
+    float random_light[3];
+    float random_light_terminate;
+    float random_bsdf[3];
+    float continuation_probability;
+    float bsdf_pdf;
+    float wi[3];
+    float throughput[3];         /* after the scatter */
+    float emission[3];           /* contribution added at this event */
+    float nee[3];                /* NEE contribution (after the shadow ray) */
+} psy_path_event;
+
+typedef struct psy_path_trace {
+    uint32_t pixel_x;
+    uint32_t pixel_y;
+    uint32_t sample;
+    uint32_t rng_hash;
+    uint32_t event_count;
+    uint32_t valid;
+    float filter[2];
+    float ray_origin[3];
+    float ray_direction[3];
+    float radiance[3];
+    psy_path_event events[PSY_TRACE_MAX_EVENTS];
+} psy_path_trace;
+
+psy_status psy_session_request_trace(psy_session *session, uint32_t x,
+                                     uint32_t y, uint32_t sample);
+psy_status psy_session_read_trace(psy_session *session, psy_path_trace *out);
+
+/* Counters of the last render_samples call: traced rays and device time
+ * per kernel class, measured with CUDA events on the session stream. */
+typedef struct psy_render_stats {
+    uint64_t camera_rays;
+    uint64_t closest_rays;       /* camera + continuation rays traced */
+    uint64_t shadow_rays;
+    uint64_t path_segments;
+    float ms_total;
+    float ms_intersect;
+    float ms_shade;
+    float ms_shadow;
+    float ms_film;
+    uint32_t kernel_launches;
+    uint32_t batches;
+} psy_render_stats;
+
+psy_status psy_session_stats(const psy_session *session,
+                             psy_render_stats *out);
+
+/* ------------------------------------------- host precompute (no GPU) -- */
+
+/* tabulated_sobol::sequence_size_for_samples
+ * (src/sampling/tabulated_sobol.cpp:156). */
+uint32_t psy_sobol_sequence_size_for_samples(uint32_t samples);
+/* tabulated_sobol::generate_table (src/sampling/tabulated_sobol.cpp:175):
+ * writes 256 * sequence_size float4 rows (4 floats each) to `out`. */
+psy_status psy_sobol_generate_table(uint32_t sequence_size, float *out);
+/* sampling::make_pixel_filter_table (src/sampling/pixel_filter.cpp:30):
+ * writes 1024 floats. */
+psy_status psy_pixel_filter_table(uint32_t filter, float width, float *out);
+
+/* ------------------------------------------------ device probes (GPU) -- */
+
+/* Evaluates cycles_sampler::sample_4d (include/psycles/luisa/cycles_sampler.h:260)
+ * on the device for `count` queries of (x, y_cycles, seed, sample, dimension)
+ * against the table of `sequence_size`, writing 4 floats per query and the
+ * shuffled table index per query. */
+psy_status psy_debug_sobol_samples(psy_context *context,
+                                   uint32_t sequence_size,
+                                   const uint32_t *queries, uint32_t count,
+                                   float *out_samples, uint32_t *out_indices);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSYCLES_CUDA_H */

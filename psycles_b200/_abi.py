@@ -1,0 +1,208 @@
+"""ctypes mirror of include/psycles_cuda.h and the loader of the in-tree
+libpsycles_cuda.so.  The library is the product path: there is no Python or
+CPU fallback, and loading fails loudly when the extension is missing."""
+
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libpsycles_cuda.so"
+
+c_float_p = ctypes.POINTER(ctypes.c_float)
+c_uint32_p = ctypes.POINTER(ctypes.c_uint32)
+
+PSY_OK = 0
+STATUS_NAMES = {
+    0: "ok", 1: "invalid argument", 2: "out of memory", 3: "cuda error", 4: "cancelled",
+    5: "range", 6: "unsupported", 7: "state", 8: "timeout",
+}
+
+CLOSURE_NULL, CLOSURE_DIFFUSE, CLOSURE_EMISSION, CLOSURE_TRANSPARENT, CLOSURE_ADD, CLOSURE_MIX = range(6)
+LIGHT_POINT, LIGHT_SPOT, LIGHT_AREA, LIGHT_DISTANT = range(4)
+LIGHT_FLAG_SPHERE, LIGHT_FLAG_NORMALIZE = 1, 2
+VIS_CAMERA, VIS_DIFFUSE, VIS_GLOSSY, VIS_TRANSMISSION, VIS_SHADOW, VIS_VOLUME = 1, 2, 4, 8, 16, 32
+VIS_ALL = 63
+EMISSION_NONE, EMISSION_AUTOMATIC, EMISSION_FRONT, EMISSION_BACK, EMISSION_FRONT_BACK = range(5)
+PASS_COMBINED, PASS_NORMAL, PASS_ALBEDO = 0, 2, 4
+PASS_DENOISING_NORMAL, PASS_DENOISING_ALBEDO, PASS_SAMPLE_COUNT = 18, 19, 20
+FILTER_BOX, FILTER_GAUSSIAN, FILTER_BLACKMAN_HARRIS = 0, 1, 2
+DIRECT_MIS, DIRECT_FORWARD, DIRECT_NEE = 0, 1, 2
+TRACE_MAX_EVENTS = 16
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("positions", c_float_p), ("normals", c_float_p), ("indices", c_uint32_p),
+                ("materials", c_uint32_p), ("vertex_count", ctypes.c_uint32),
+                ("triangle_count", ctypes.c_uint32), ("smooth", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class InstanceDesc(ctypes.Structure):
+    _fields_ = [("object_to_world", ctypes.c_float * 16), ("mesh", ctypes.c_uint32),
+                ("material", ctypes.c_uint32), ("visibility", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class ClosureInstruction(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_uint32), ("a", ctypes.c_uint32), ("b", ctypes.c_uint32),
+                ("color", ctypes.c_uint32), ("scalar", ctypes.c_uint32)]
+
+
+class MaterialDesc(ctypes.Structure):
+    _fields_ = [("closures", ctypes.POINTER(ClosureInstruction)), ("closure_count", ctypes.c_uint32),
+                ("root", ctypes.c_uint32), ("scalars", c_float_p), ("scalar_count", ctypes.c_uint32),
+                ("vector_count", ctypes.c_uint32), ("vectors", c_float_p),
+                ("emission_sampling", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class LightDesc(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("max_bounces", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("position", ctypes.c_float * 3), ("axis_x", ctypes.c_float * 3),
+                ("axis_y", ctypes.c_float * 3), ("axis_z", ctypes.c_float * 3), ("axis_scale", ctypes.c_float * 3),
+                ("color", ctypes.c_float * 3), ("power", ctypes.c_float), ("radius", ctypes.c_float),
+                ("size_u", ctypes.c_float), ("size_v", ctypes.c_float), ("spot_angle", ctypes.c_float),
+                ("spot_smooth", ctypes.c_float), ("angle", ctypes.c_float)]
+
+
+class CameraDesc(ctypes.Structure):
+    _fields_ = [("camera_to_world", ctypes.c_float * 16), ("field_of_view", ctypes.c_float),
+                ("horizontal_field_of_view", ctypes.c_float), ("sensor_fit", ctypes.c_uint32),
+                ("lens_shift_x", ctypes.c_float), ("lens_shift_y", ctypes.c_float),
+                ("near_clip", ctypes.c_float), ("far_clip", ctypes.c_float), ("reserved", ctypes.c_uint32)]
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [("meshes", ctypes.POINTER(MeshDesc)), ("instances", ctypes.POINTER(InstanceDesc)),
+                ("materials", ctypes.POINTER(MaterialDesc)), ("lights", ctypes.POINTER(LightDesc)),
+                ("mesh_count", ctypes.c_uint32), ("instance_count", ctypes.c_uint32),
+                ("material_count", ctypes.c_uint32), ("light_count", ctypes.c_uint32),
+                ("camera", CameraDesc), ("background", ctypes.c_float * 3),
+                ("world_visibility", ctypes.c_uint32), ("revision", ctypes.c_uint64)]
+
+
+class RenderSettings(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in (
+        "full_width", "full_height", "window_x", "window_y", "window_width", "window_height", "seed",
+        "transparent_background", "pixel_filter")] + [
+        ("filter_width", ctypes.c_float), ("pass_alpha_threshold", ctypes.c_float)] + [
+        (n, ctypes.c_uint32) for n in (
+            "max_bounces", "min_bounces", "diffuse_bounces", "glossy_bounces", "transmission_bounces",
+            "transparent_min_bounces", "transparent_max_bounces")] + [
+        (n, ctypes.c_float) for n in (
+            "sample_clamp_direct", "sample_clamp_indirect", "film_exposure", "light_sampling_threshold")] + [
+        (n, ctypes.c_uint32) for n in (
+            "use_light_tree", "direct_light_sampling", "next_event_estimation", "reserved")]
+
+
+class PathEvent(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in (
+        "rng_offset", "bounce", "transparent_bounce", "flag", "visibility", "hit_object", "hit_primitive",
+        "closure_index", "label", "light_kind", "light_index", "terminated")] + [
+        ("hit_t", ctypes.c_float), ("hit_u", ctypes.c_float), ("hit_v", ctypes.c_float),
+        ("random_terminate", ctypes.c_float), ("random_light", ctypes.c_float * 3),
+        ("random_light_terminate", ctypes.c_float), ("random_bsdf", ctypes.c_float * 3),
+        ("continuation_probability", ctypes.c_float), ("bsdf_pdf", ctypes.c_float),
+        ("wi", ctypes.c_float * 3), ("throughput", ctypes.c_float * 3), ("emission", ctypes.c_float * 3),
+        ("nee", ctypes.c_float * 3)]
+
+
+class PathTrace(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in (
+        "pixel_x", "pixel_y", "sample", "rng_hash", "event_count", "valid")] + [
+        ("filter", ctypes.c_float * 2), ("ray_origin", ctypes.c_float * 3),
+        ("ray_direction", ctypes.c_float * 3), ("radiance", ctypes.c_float * 3),
+        ("events", PathEvent * TRACE_MAX_EVENTS)]
+
+
+class RenderStats(ctypes.Structure):
+    _fields_ = [("camera_rays", ctypes.c_uint64), ("closest_rays", ctypes.c_uint64),
+                ("shadow_rays", ctypes.c_uint64), ("path_segments", ctypes.c_uint64),
+                ("ms_total", ctypes.c_float), ("ms_intersect", ctypes.c_float), ("ms_shade", ctypes.c_float),
+                ("ms_shadow", ctypes.c_float), ("ms_film", ctypes.c_float),
+                ("kernel_launches", ctypes.c_uint32), ("batches", ctypes.c_uint32)]
+
+
+# Entry points declared by include/psycles_cuda.h: (name, restype, argtypes).
+SIGNATURES = [
+    ("psy_last_error", ctypes.c_char_p, []),
+    ("psy_abi_version", ctypes.c_uint32, []),
+    ("psy_render_settings_default", None, [ctypes.POINTER(RenderSettings)]),
+    ("psy_context_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("psy_context_destroy", None, [ctypes.c_void_p]),
+    ("psy_scene_compile", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SceneDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    ("psy_scene_destroy", None, [ctypes.c_void_p]),
+    ("psy_scene_source_revision", ctypes.c_uint64, [ctypes.c_void_p]),
+    ("psy_scene_rebind_parameters", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_uint32, c_float_p, ctypes.c_uint32, c_float_p, ctypes.c_uint32]),
+    ("psy_session_create", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.POINTER(RenderSettings), ctypes.POINTER(ctypes.c_void_p)]),
+    ("psy_session_destroy", None, [ctypes.c_void_p]),
+    ("psy_session_reset", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RenderSettings)]),
+    ("psy_session_render_samples", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("psy_session_cancel", None, [ctypes.c_void_p]),
+    ("psy_session_read_pass", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_uint32, c_float_p, ctypes.c_uint64, c_uint32_p]),
+    ("psy_session_rendered_samples", ctypes.c_uint32, [ctypes.c_void_p]),
+    ("psy_session_request_trace", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("psy_session_read_trace", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PathTrace)]),
+    ("psy_session_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RenderStats)]),
+    ("psy_sobol_sequence_size_for_samples", ctypes.c_uint32, [ctypes.c_uint32]),
+    ("psy_sobol_generate_table", ctypes.c_int, [ctypes.c_uint32, c_float_p]),
+    ("psy_pixel_filter_table", ctypes.c_int, [ctypes.c_uint32, ctypes.c_float, c_float_p]),
+    ("psy_debug_sobol_samples", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_uint32, c_uint32_p, ctypes.c_uint32, c_float_p, c_uint32_p]),
+]
+
+def default_settings() -> RenderSettings:
+    """contract::RenderSettings / PathIntegratorSettings defaults
+    (include/psycles/contract/render.h:81-115); equals psy_render_settings_default."""
+    s = RenderSettings()
+    s.filter_width = 1.0
+    s.pass_alpha_threshold = 0.5
+    s.max_bounces, s.diffuse_bounces, s.glossy_bounces = 12, 4, 4
+    s.transmission_bounces, s.transparent_max_bounces = 12, 8
+    s.film_exposure = 1.0
+    s.light_sampling_threshold = 0.01
+    s.direct_light_sampling = DIRECT_MIS
+    s.next_event_estimation = 1
+    return s
+
+
+_lib = None
+
+
+class PsyError(RuntimeError):
+    """A psy_status other than PSY_OK, with psy_last_error()'s message."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def load() -> ctypes.CDLL:
+    """Loads the in-tree libpsycles_cuda.so (built by psycles_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m psycles_b200.build` first")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, restype, argtypes in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    if status != PSY_OK:
+        raise PsyError(status, load().psy_last_error().decode())
+
+
+def ptr(array, ctype=ctypes.c_float):
+    """Pointer to a contiguous numpy array (or None for None)."""
+    if array is None:
+        return ctypes.cast(None, ctypes.POINTER(ctype))
+    return array.ctypes.data_as(ctypes.POINTER(ctype))

@@ -1,0 +1,253 @@
+"""Host mirror of the reference render contract over the C ABI.
+
+Names and argument meaning follow include/psycles/contract/render.h:
+RendererBackend.compile_scene -> SceneCompilation(scene, diagnostics);
+create_session -> RenderSession or None; RenderSession.render_samples(
+SampleRange, OutputSink) -> bool (False for a cancelled session, an empty or
+out-of-range SampleRange, a changed total, or a failed dispatch), reset,
+cancel; OutputSink.begin / write(PassTile) / end.  Every call goes through
+libpsycles_cuda.so.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import threading
+
+import numpy as np
+
+from . import _abi
+from .scenes import Scene
+
+PassKind = {
+    "combined": _abi.PASS_COMBINED, "normal": _abi.PASS_NORMAL, "albedo": _abi.PASS_ALBEDO,
+    "denoising_normal": _abi.PASS_DENOISING_NORMAL, "denoising_albedo": _abi.PASS_DENOISING_ALBEDO,
+    "sample_count": _abi.PASS_SAMPLE_COUNT,
+}
+
+
+@dataclasses.dataclass
+class PassRequest:
+    kind: int = _abi.PASS_COMBINED
+    name: str = ""
+    channels: int = 4
+
+
+@dataclasses.dataclass
+class SampleRange:
+    first: int = 0
+    count: int = 0
+    offset: int = 0
+    total: int = 0
+
+
+@dataclasses.dataclass
+class PassTile:
+    pass_: PassRequest
+    window: tuple[int, int, int, int]
+    full_extent: tuple[int, int]
+    pixels: np.ndarray  # float32 [height, width, channels]
+
+
+class OutputSink:
+    def begin(self, settings) -> None:  # pragma: no cover - interface
+        pass
+
+    def write(self, tile: PassTile) -> None:  # pragma: no cover - interface
+        raise NotImplementedError
+
+    def end(self, cancelled: bool) -> None:  # pragma: no cover - interface
+        pass
+
+
+class MemoryOutputSink(OutputSink):
+    """io::MemoryOutputSink (include/psycles/io/image.h:21): keeps the last tile per pass."""
+
+    def __init__(self) -> None:
+        self.tiles: dict[int, PassTile] = {}
+        self.began = 0
+        self.ended: bool | None = None
+
+    def begin(self, settings) -> None:
+        self.began += 1
+        self.tiles = {}
+
+    def write(self, tile: PassTile) -> None:
+        self.tiles[tile.pass_.kind] = tile
+
+    def end(self, cancelled: bool) -> None:
+        self.ended = cancelled
+
+    def pass_pixels(self, kind: int) -> np.ndarray:
+        return self.tiles[kind].pixels
+
+
+@dataclasses.dataclass
+class RenderDiagnostic:
+    message: str
+
+
+class Context:
+    """One CUDA device and its stream (psy_context)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _abi.load()
+        h = ctypes.c_void_p()
+        _abi.check(self.lib.psy_context_create(device, ctypes.byref(h)))
+        self.handle = h
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.psy_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CompiledScene:
+    def __init__(self, context: Context, handle: ctypes.c_void_p, scene: Scene):
+        self.context = context
+        self.handle = handle
+        self.scene = scene
+        self.lib = context.lib
+
+    def source_revision(self) -> int:
+        return int(self.lib.psy_scene_source_revision(self.handle))
+
+    def rebind_parameters(self, material: int, scalars: np.ndarray, vectors: np.ndarray) -> None:
+        """Parameter-only edit: rewrites one material's parameter block on the device."""
+        sc = np.ascontiguousarray(scalars, dtype=np.float32).reshape(-1)
+        vc = np.ascontiguousarray(vectors, dtype=np.float32).reshape(-1)
+        _abi.check(self.lib.psy_scene_rebind_parameters(self.handle, material, _abi.ptr(sc), sc.size,
+                                                        _abi.ptr(vc), vc.size // 3))
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.psy_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclasses.dataclass
+class SceneCompilation:
+    scene: CompiledScene | None
+    diagnostics: list[RenderDiagnostic]
+
+    def ok(self) -> bool:
+        return self.scene is not None
+
+
+class RenderSession:
+    def __init__(self, compiled: CompiledScene, handle: ctypes.c_void_p, settings: _abi.RenderSettings,
+                 passes: list[PassRequest]):
+        self.compiled = compiled
+        self.handle = handle
+        self.settings = settings
+        self.passes = passes
+        self.lib = compiled.lib
+        self.diagnostics: list[RenderDiagnostic] = []
+        self._lock = threading.Lock()
+
+    @property
+    def window(self) -> tuple[int, int, int, int]:
+        s = self.settings
+        return (s.window_x, s.window_y, s.window_width or s.full_width, s.window_height or s.full_height)
+
+    def reset(self, settings: _abi.RenderSettings) -> None:
+        _abi.check(self.lib.psy_session_reset(self.handle, ctypes.byref(settings)))
+        self.settings = settings
+
+    def cancel(self) -> None:
+        self.lib.psy_session_cancel(self.handle)
+
+    def render_samples(self, samples: SampleRange, output: OutputSink | None = None) -> bool:
+        with self._lock:
+            status = self.lib.psy_session_render_samples(self.handle, samples.first, samples.count,
+                                                         samples.offset, samples.total)
+            if status != _abi.PSY_OK:
+                self.diagnostics.append(RenderDiagnostic(self.lib.psy_last_error().decode()))
+                return False
+            if output is not None:
+                output.begin(self.settings)
+                for p in self.passes:
+                    output.write(PassTile(p, self.window, (self.settings.full_width, self.settings.full_height),
+                                          self.read_pass(p.kind)))
+                output.end(False)
+            return True
+
+    def read_pass(self, kind: int) -> np.ndarray:
+        x, y, w, h = self.window
+        ch = 1 if kind == _abi.PASS_SAMPLE_COUNT else 4
+        out = np.zeros((h, w, ch), dtype=np.float32)
+        channels = ctypes.c_uint32()
+        _abi.check(self.lib.psy_session_read_pass(self.handle, kind, _abi.ptr(out), out.size, ctypes.byref(channels)))
+        return out
+
+    def rendered_samples(self) -> int:
+        return int(self.lib.psy_session_rendered_samples(self.handle))
+
+    def request_trace(self, x: int, y: int, sample: int) -> None:
+        _abi.check(self.lib.psy_session_request_trace(self.handle, x, y, sample))
+
+    def read_trace(self) -> _abi.PathTrace:
+        t = _abi.PathTrace()
+        _abi.check(self.lib.psy_session_read_trace(self.handle, ctypes.byref(t)))
+        return t
+
+    def stats(self) -> _abi.RenderStats:
+        s = _abi.RenderStats()
+        _abi.check(self.lib.psy_session_stats(self.handle, ctypes.byref(s)))
+        return s
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.psy_session_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+DEFAULT_PASSES = [PassRequest(_abi.PASS_COMBINED, "Combined"), PassRequest(_abi.PASS_NORMAL, "Normal"),
+                  PassRequest(_abi.PASS_ALBEDO, "Albedo"),
+                  PassRequest(_abi.PASS_DENOISING_NORMAL, "Denoising Normal"),
+                  PassRequest(_abi.PASS_DENOISING_ALBEDO, "Denoising Albedo"),
+                  PassRequest(_abi.PASS_SAMPLE_COUNT, "Sample Count", 1)]
+
+
+class CudaPathTracerBackend:
+    """contract::RendererBackend over libpsycles_cuda.so (one CUDA device)."""
+
+    def __init__(self, device: int = 0, next_event_estimation: bool = True):
+        self.context = Context(device)
+        self.next_event_estimation = next_event_estimation
+
+    def compile_scene(self, scene: Scene) -> SceneCompilation:
+        desc = scene.to_desc()
+        h = ctypes.c_void_p()
+        status = self.context.lib.psy_scene_compile(self.context.handle, desc.pointer, ctypes.byref(h))
+        if status != _abi.PSY_OK:
+            return SceneCompilation(None, [RenderDiagnostic(self.context.lib.psy_last_error().decode())])
+        return SceneCompilation(CompiledScene(self.context, h, scene), [])
+
+    def create_session(self, compiled: CompiledScene, settings: _abi.RenderSettings,
+                       passes: list[PassRequest] | None = None) -> RenderSession | None:
+        settings.next_event_estimation = 1 if self.next_event_estimation else 0
+        h = ctypes.c_void_p()
+        status = self.context.lib.psy_session_create(compiled.handle, ctypes.byref(settings), ctypes.byref(h))
+        if status != _abi.PSY_OK:
+            return None
+        return RenderSession(compiled, h, settings, list(passes or DEFAULT_PASSES))

@@ -1,0 +1,71 @@
+"""Build libpsycles_cuda.so in-tree for sm_100a.
+
+    python -m psycles_b200.build          # or psycles_b200.build.build()
+
+The CUDA sources are compiled by nvcc with -gencode arch=compute_100a,
+code=sm_100a, no fast math and no FMA contraction (-fmad=false: the
+kernels spell out every fused operation the reference prescribes); the
+host translation unit by g++ with -ffp-contract=off, so host tables are
+bit-identical to the reference's construction.
+"""
+
+from __future__ import annotations
+
+import os
+import pathlib
+import shutil
+import subprocess
+import sys
+
+HERE = pathlib.Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+OUT = HERE / "libpsycles_cuda.so"
+BUILD = HERE / "_build"
+
+CUDA_HOME = pathlib.Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+NVCC = str(CUDA_HOME / "bin" / "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
+              "-ftz=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+              "--expt-relaxed-constexpr"]
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-Wextra"]
+
+SOURCES_CU = ["psy_kernels.cu"]
+SOURCES_CPP = ["psy_host.cpp"]
+
+
+def _run(cmd: list[str]) -> None:
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def _stale(target: pathlib.Path, deps: list[pathlib.Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose_ptxas: bool = False) -> pathlib.Path:
+    BUILD.mkdir(exist_ok=True)
+    headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "psycles_cuda.h"]
+    objects = []
+    for src in SOURCES_CU:
+        obj = BUILD / (src + ".o")
+        objects.append(obj)
+        if force or _stale(obj, [CSRC / src] + headers):
+            extra = ["-Xptxas", "-v"] if verbose_ptxas else []
+            _run([NVCC, *ARCH, *NVCC_FLAGS, *extra, "-c", str(CSRC / src), "-o", str(obj)])
+    cxx = shutil.which("g++") or "g++"
+    for src in SOURCES_CPP:
+        obj = BUILD / (src + ".o")
+        objects.append(obj)
+        if force or _stale(obj, [CSRC / src] + headers):
+            _run([cxx, *CXX_FLAGS, f"-I{CUDA_HOME / 'include'}", "-c", str(CSRC / src), "-o", str(obj)])
+    if force or _stale(OUT, objects):
+        _run([NVCC, *ARCH, "-shared", "-o", str(OUT), *map(str, objects), "-lcudart"])
+    return OUT
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose_ptxas="--ptxas" in sys.argv)

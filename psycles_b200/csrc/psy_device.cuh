@@ -1,0 +1,925 @@
+// Device building blocks of the path-trace kernels: tabulated-Sobol lookup,
+// closure programs, light sampling, two-level BVH traversal with the Cycles
+// closest-hit predicate, and hit reconstruction.  Each function names the
+// Psycles function it implements.
+#pragma once
+
+#include "psy_math.cuh"
+#include "psy_scene.h"
+
+namespace psy {
+
+// ------------------------------------------------------------- sampler
+// include/psycles/luisa/cycles_sampler.h:36-339.
+
+__device__ __forceinline__ uint32_t reverse_bits(uint32_t v) { return __brev(v); }
+
+__device__ __forceinline__ uint32_t reversed_bit_owen(uint32_t v, uint32_t seed) {
+    v ^= v * 0x3d20adeau;
+    v += seed;
+    v *= (seed >> 16u) | 1u;
+    v ^= v * 0x05526c56u;
+    v ^= v * 0x53a22864u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t hash_wang_seeded_uint(uint32_t v, uint32_t seed) {
+    v = (v ^ 61u) ^ seed;
+    v += v << 3u;
+    v ^= v >> 4u;
+    v *= 0x27d4eb2du;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t shuffled_pattern_index(uint32_t dimension, uint32_t seed) {
+    uint32_t v = dimension & 0xffu;
+    const uint32_t mask = 0xffu;
+    v ^= seed;
+    v *= 0xe170893du;
+    v ^= seed >> 16u;
+    v ^= (v & mask) >> 4u;
+    v ^= seed >> 8u;
+    v *= 0x0929eb3fu;
+    v ^= seed >> 23u;
+    v ^= (v & mask) >> 1u;
+    v *= 1u | (seed >> 27u);
+    v *= 0x6935fa69u;
+    v ^= (v & mask) >> 11u;
+    v *= 0x74dcb303u;
+    v ^= (v & mask) >> 2u;
+    v *= 0x9e501cc3u;
+    v ^= (v & mask) >> 2u;
+    v *= 0xc860a3dfu;
+    v &= mask;
+    v ^= v >> 5u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t pixel_hash(uint32_t x, uint32_t y, uint32_t seed) {
+    const uint32_t qx = 1103515245u * ((x >> 1u) ^ y);
+    const uint32_t qy = 1103515245u * ((y >> 1u) ^ x);
+    const uint32_t h = 1103515245u * (qx ^ (qy >> 3u));
+    return h ^ seed;
+}
+
+__device__ __forceinline__ uint32_t shuffled_sample_index(uint32_t sample, uint32_t dimension, uint32_t seed,
+                                                          uint32_t size) {
+    const uint32_t pattern = shuffled_pattern_index(dimension, seed);
+    const uint32_t mask = size - 1u;
+    const uint32_t shuffled =
+        reverse_bits(reversed_bit_owen(reverse_bits(sample), hash_wang_seeded_uint(dimension, seed)));
+    sample = (sample & ~mask) | (shuffled & mask);
+    return ((pattern * size) + sample) % (size * 256u);
+}
+
+__device__ __forceinline__ float4 sample_4d(const RenderParams &p, uint32_t sample, uint32_t rng_hash, uint32_t dim) {
+    return __ldg(&p.sobol[shuffled_sample_index(sample, dim, rng_hash, p.sobol_size)]);
+}
+
+// pixel_filter::sample (include/psycles/luisa/pixel_filter.h:17-29).
+__device__ __forceinline__ float pixel_filter_sample(const float *table, float random) {
+    const uint32_t last = 1023u;
+    const float coordinate = clampf_(random, 0.0f, 1.0f) * static_cast<float>(last);
+    const uint32_t index = min(static_cast<uint32_t>(coordinate), last);
+    const uint32_t next = min(index + 1u, last);
+    const float t = coordinate - static_cast<float>(index);
+    return lerpf_(__ldg(&table[index]), __ldg(&table[next]), t);
+}
+
+// ---------------------------------------------------------- sample maps
+// include/psycles/luisa/cycles_sample_mapping.h:49-339.
+
+__device__ __forceinline__ f2 sample_uniform_disk(f2 r) {
+    const float a = 2.0f * r.x - 1.0f;
+    const float b = 2.0f * r.y - 1.0f;
+    const bool x_major = a * a > b * b;
+    const float safe_a = a != 0.0f ? a : 1.0f;
+    const float safe_b = b != 0.0f ? b : 1.0f;
+    const float radius = x_major ? a : b;
+    const float angle = x_major ? 0.25f * kPi * (b / safe_a) : 0.5f * kPi - 0.25f * kPi * (a / safe_b);
+    if (a == 0.0f && b == 0.0f) return {0.0f, 0.0f};
+    return {cos_(angle) * radius, sin_(angle) * radius};
+}
+
+struct Basis {
+    f3 tangent, bitangent;
+};
+
+__device__ __forceinline__ Basis make_orthonormals(f3 n) {
+    const f3 general = mk3(n.z - n.y, n.x - n.z, n.y - n.x);
+    const f3 equal = mk3(n.z - n.y, n.x + n.z, -n.y - n.x);
+    const bool use_general = (n.x != n.y) || (n.x != n.z);
+    const f3 t = normalize(use_general ? general : equal);
+    return {t, cross(n, t)};
+}
+
+__device__ __forceinline__ f3 sample_cosine_hemisphere(f3 n, f2 r, float *pdf) {
+    const f2 d = sample_uniform_disk(r);
+    const float c = sqrtf(maxf_(1.0f - dot(d, d), 0.0f));
+    const Basis b = make_orthonormals(n);
+    if (pdf) *pdf = c * kInvPi;
+    return b.tangent * d.x + b.bitangent * d.y + n * c;
+}
+
+struct ConeSample {
+    f3 direction;
+    float cosine, pdf;
+};
+
+__device__ __forceinline__ ConeSample sample_uniform_cone(f3 axis, float one_minus_cosine, f2 r) {
+    const f2 disk = sample_uniform_disk(r);
+    const float r2 = dot(disk, disk);
+    const float cosine = 1.0f - r2 * one_minus_cosine;
+    const float scale = sqrtf(maxf_(one_minus_cosine * (2.0f - one_minus_cosine * r2), 0.0f));
+    const f2 mapped = disk * scale;
+    const Basis b = make_orthonormals(axis);
+    const f3 finite_dir = b.tangent * mapped.x + b.bitangent * mapped.y + axis * cosine;
+    if (one_minus_cosine > 0.0f) return {finite_dir, cosine, kInvTwoPi / one_minus_cosine};
+    return {axis, 1.0f, 1.0f};
+}
+
+// ------------------------------------------------------ closure programs
+// GraphSurfaceImplementation::for_each_closure (src/luisa/graph_surface_closures.cpp:5-356)
+// with allocation (src/luisa/graph_surface_state.cpp:19-48).
+
+constexpr uint32_t kMaxClosures = 16u;
+constexpr uint32_t kMaxClosureStack = 32u;
+
+struct PhysicalClosure {
+    f3 weight;
+    f3 normal;
+    float sample_weight;
+    uint32_t op;
+};
+
+struct SurfaceClosures {
+    PhysicalClosure c[kMaxClosures];
+    uint32_t count;
+    f3 emission;
+};
+
+__device__ __forceinline__ float closure_sample_weight(f3 w) { return fabsf((w.x + w.y + w.z) / 3.0f); }
+
+__device__ __forceinline__ f3 bsdf_allocated_weight(f3 v) {
+    v = max3(v, mk3(0.0f));
+    const float average = (v.x + v.y + v.z) / 3.0f;
+    return average >= 1.0e-5f ? v : mk3(0.0f);
+}
+
+__device__ __forceinline__ f3 ld_vector(const SceneView &s, const MaterialGpu &m, uint32_t slot) {
+    return ld3(s.vectors + 3u * (m.vector_offset + slot));
+}
+__device__ __forceinline__ float ld_scalar(const SceneView &s, const MaterialGpu &m, uint32_t slot) {
+    return s.scalars[m.scalar_offset + slot];
+}
+
+// Visits closure leaves depth-first, `a` before `b`, with the add / mix
+// weight rule; `visit(op, weight)` receives diffuse / transparent /
+// emission leaves.
+template <typename Visit>
+__device__ __forceinline__ void walk_closures(const SceneView &s, const MaterialGpu &m, Visit visit) {
+    uint32_t stack_id[kMaxClosureStack];
+    float stack_w[kMaxClosureStack];
+    int sp = 0;
+    stack_id[sp] = m.root;
+    stack_w[sp] = 1.0f;
+    ++sp;
+    while (sp > 0) {
+        --sp;
+        const uint32_t id = stack_id[sp];
+        const float w = stack_w[sp];
+        if (id >= m.code_count) continue;
+        const psy_closure_instruction c = s.code[m.code_offset + id];
+        if (c.op == PSY_CLOSURE_ADD) {
+            if (sp + 2 > int(kMaxClosureStack)) continue;
+            stack_id[sp] = c.b; stack_w[sp] = w; ++sp;
+            stack_id[sp] = c.a; stack_w[sp] = w; ++sp;
+        } else if (c.op == PSY_CLOSURE_MIX) {
+            if (sp + 2 > int(kMaxClosureStack)) continue;
+            const float f = clampf_(ld_scalar(s, m, c.scalar), 0.0f, 1.0f);
+            stack_id[sp] = c.b; stack_w[sp] = w * f; ++sp;
+            stack_id[sp] = c.a; stack_w[sp] = w * (1.0f - f); ++sp;
+        } else if (c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_TRANSPARENT) {
+            visit(c.op, ld_vector(s, m, c.color) * w);
+        } else if (c.op == PSY_CLOSURE_EMISSION) {
+            visit(c.op, ld_vector(s, m, c.color) * ld_scalar(s, m, c.scalar) * w);
+        }
+    }
+}
+
+__device__ __forceinline__ void collect_surface(const SceneView &s, const MaterialGpu &m, f3 shading_normal,
+                                                SurfaceClosures &out) {
+    out.count = 0u;
+    out.emission = mk3(0.0f);
+    const f3 closure_normal = safe_normalize(shading_normal, shading_normal);
+    walk_closures(s, m, [&](uint32_t op, f3 w) {
+        if (op == PSY_CLOSURE_EMISSION) {
+            out.emission = out.emission + w;
+            return;
+        }
+        if (out.count >= kMaxClosures) return;
+        PhysicalClosure p;
+        p.op = op;
+        if (op == PSY_CLOSURE_DIFFUSE) {
+            p.weight = bsdf_allocated_weight(w);
+            p.sample_weight = closure_sample_weight(p.weight);
+            p.normal = closure_normal;
+            if (!any_nonzero(p.weight)) return;
+        } else {
+            const float sw = closure_sample_weight(w);
+            if (!(sw >= 1.0e-5f)) return;
+            p.weight = w;
+            p.sample_weight = sw;
+            p.normal = shading_normal;
+        }
+        out.c[out.count++] = p;
+    });
+}
+
+__device__ __forceinline__ f3 material_emission(const SceneView &s, const MaterialGpu &m) {
+    f3 r = mk3(0.0f);
+    walk_closures(s, m, [&](uint32_t op, f3 w) {
+        if (op == PSY_CLOSURE_EMISSION) r = r + w;
+    });
+    return r;
+}
+
+// transparent_extinction (src/luisa/graph_surface_implementation.cpp:354-372).
+__device__ __forceinline__ f3 transparent_extinction(const SceneView &s, const MaterialGpu &m) {
+    f3 r = mk3(0.0f);
+    walk_closures(s, m, [&](uint32_t op, f3 w) {
+        if (op == PSY_CLOSURE_TRANSPARENT && closure_sample_weight(w) >= 1.0e-5f) r = r + w;
+    });
+    return r;
+}
+
+constexpr uint32_t kEventReflection = 1u, kEventTransmission = 2u, kEventDiffuse = 4u, kEventGlossy = 8u,
+                   kEventSingular = 16u, kEventTransparent = 32u;
+constexpr uint32_t kLabelTransmit = 1u, kLabelReflect = 2u, kLabelDiffuse = 4u, kLabelGlossy = 8u,
+                   kLabelSingular = 16u, kLabelTransparent = 32u;
+constexpr uint32_t kRuntimeBackfacing = 1u, kRuntimeBsdf = 8u, kRuntimeBsdfHasEval = 16u,
+                   kRuntimeTransparent = 1024u, kRuntimeBsdfHasTransmission = 2048u;
+
+__device__ __forceinline__ uint32_t label_from_events(uint32_t e) {
+    uint32_t l = 0u;
+    if (e & kEventTransmission) l |= kLabelTransmit;
+    if (e & kEventReflection) l |= kLabelReflect;
+    if (e & kEventDiffuse) l |= kLabelDiffuse;
+    if (e & kEventGlossy) l |= kLabelGlossy;
+    if (e & kEventSingular) l |= kLabelSingular;
+    if (e & kEventTransparent) l |= kLabelTransparent;
+    return l;
+}
+
+__device__ __forceinline__ uint32_t runtime_flags(const SurfaceClosures &s, bool back_facing) {
+    uint32_t f = back_facing ? kRuntimeBackfacing : 0u;
+    for (uint32_t i = 0; i < s.count; ++i)
+        f |= s.c[i].op == PSY_CLOSURE_DIFFUSE ? (kRuntimeBsdf | kRuntimeBsdfHasEval) : (kRuntimeBsdf | kRuntimeTransparent);
+    return f;
+}
+
+// bump_shadowing_term (src/luisa/graph_surface_scattering.cpp:219-281).
+__device__ __forceinline__ float bump_shadowing(f3 smooth, f3 cn, f3 dir) {
+    if (cn.x == smooth.x && cn.y == smooth.y && cn.z == smooth.z) return 1.0f;
+    return (dot(smooth, dir) * dot(smooth, cn) * dot(cn, dir) < 0.0f) ? 0.0f : 1.0f;
+}
+
+struct Evaluation {
+    f3 f;
+    float pdf;
+    uint32_t events;
+};
+
+// surface_closure_evaluation_contribution + accumulator
+// (src/luisa/surface_closure_evaluation.cpp:71-438).
+__device__ __forceinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, f3 shading_normal, f3 outgoing_raw,
+                                                       uint32_t lobe_mask, int selected) {
+    const f3 outgoing = safe_normalize(outgoing_raw, shading_normal);
+    Evaluation e{mk3(0.0f), 0.0f, 0u};
+    float total = 0.0f, weighted_pdf = 0.0f;
+    const bool diffuse_enabled = (lobe_mask & kEventDiffuse) != 0u;
+    const bool transparent_enabled = (lobe_mask & kEventTransparent) != 0u;
+    for (uint32_t i = 0; i < s.count; ++i) {
+        const PhysicalClosure &c = s.c[i];
+        if (c.op == PSY_CLOSURE_TRANSPARENT) {
+            if (transparent_enabled) total += c.sample_weight;
+            continue;
+        }
+        const float bump = bump_shadowing(shading_normal, c.normal, outgoing);
+        const bool pdf_valid = bump != 0.0f || int(i) == selected;
+        float pdf = maxf_(dot(c.normal, outgoing), 0.0f) * kInvPi;
+        if (!pdf_valid) pdf = 0.0f;
+        if (!diffuse_enabled) continue;
+        const float nl = maxf_(dot(c.normal, outgoing), 0.0f);
+        const f3 value = c.weight * (nl * kInvPi) * bump;
+        e.f = e.f + value;
+        total += c.sample_weight;
+        weighted_pdf += c.sample_weight * pdf;
+        if (closure_sample_weight(value) > 0.0f) e.events |= kEventDiffuse | kEventReflection;
+    }
+    e.pdf = total > 0.0f ? weighted_pdf / maxf_(total, 1.0e-20f) : 0.0f;
+    if (!(weighted_pdf > 0.0f)) e.events = 0u;
+    return e;
+}
+
+struct SurfaceSample {
+    bool valid;
+    f3 wi;
+    Evaluation eval;
+    uint32_t closure_index;
+};
+
+// SurfaceClosureSamplingVisitor::visit (src/luisa/surface_closure_sampling_core.cpp:744-812).
+__device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s, f3 shading_normal, f3 geometric_normal,
+                                                        f3 incoming, float u_lobe, f2 u_dir, uint32_t lobe_mask) {
+    SurfaceSample out;
+    out.valid = false;
+    out.wi = mk3(0.0f);
+    out.eval = {mk3(0.0f), 0.0f, 0u};
+    out.closure_index = kInvalid;
+    const bool diffuse_enabled = (lobe_mask & kEventDiffuse) != 0u;
+    const bool transparent_enabled = (lobe_mask & kEventTransparent) != 0u;
+    float total = 0.0f;
+    for (uint32_t i = 0; i < s.count; ++i) {
+        const bool eligible = s.c[i].op == PSY_CLOSURE_DIFFUSE ? diffuse_enabled : transparent_enabled;
+        total += eligible ? s.c[i].sample_weight : 0.0f;
+    }
+    const float random_lobe = clampf_(u_lobe, 0.0f, 0.99999994f);
+    const float target = random_lobe * total;
+    float accumulated = 0.0f;
+    int chosen = -1;
+    float chosen_weight = 0.0f;
+    for (uint32_t i = 0; i < s.count; ++i) {
+        const bool eligible = s.c[i].op == PSY_CLOSURE_DIFFUSE ? diffuse_enabled : transparent_enabled;
+        const float w = eligible ? s.c[i].sample_weight : 0.0f;
+        const float next = accumulated + w;
+        if (chosen < 0 && w > 0.0f && target < next) {
+            chosen = int(i);
+            chosen_weight = w;
+        }
+        accumulated = next;
+    }
+    if (chosen < 0) return out;
+    const PhysicalClosure c = s.c[chosen];
+    const bool transparent = c.op == PSY_CLOSURE_TRANSPARENT;
+    const f3 direction = transparent ? -incoming : sample_cosine_hemisphere(c.normal, u_dir, nullptr);
+    out.closure_index = uint32_t(chosen);
+    out.wi = direction;
+    if (!(transparent || dot(geometric_normal, direction) > 0.0f)) return out;
+    const Evaluation mixture = evaluate_mixture(s, shading_normal, direction, lobe_mask, chosen);
+    Evaluation r;
+    r.f = mixture.f;
+    float delta = 0.0f;
+    if (transparent) {
+        r.f = r.f + c.weight * 1.0e6f;
+        delta = 1.0e6f * chosen_weight;
+    }
+    r.pdf = mixture.pdf + delta / maxf_(total, 1.0e-20f);
+    r.events = transparent ? (kEventTransmission | kEventTransparent) : (kEventDiffuse | kEventReflection);
+    out.eval = r;
+    out.valid = true;
+    return out;
+}
+
+// AOV visitor (src/luisa/surface_closure_operations.cpp:402-462).
+__device__ __forceinline__ void surface_aov(const SurfaceClosures &s, f3 shading_normal, f3 &albedo, f3 &normal,
+                                            f3 &transparency) {
+    albedo = mk3(0.0f);
+    transparency = mk3(0.0f);
+    f3 n = mk3(0.0f);
+    float total = 0.0f;
+    for (uint32_t i = 0; i < s.count; ++i) {
+        const PhysicalClosure &c = s.c[i];
+        if (c.op == PSY_CLOSURE_DIFFUSE) {
+            albedo = albedo + c.weight;
+            const float w = closure_sample_weight(c.weight);
+            n = n + c.normal * w;
+            total += w;
+        } else {
+            transparency = transparency + c.weight;
+        }
+    }
+    normal = safe_normalize(total > 0.0f ? n : shading_normal, shading_normal);
+}
+
+// ---------------------------------------------------------- intersection
+
+struct Ray {
+    f3 o, d;
+    float tmin, tmax;
+};
+
+struct Hit {
+    float t, u, v;
+    uint32_t instance, prim, object, cycles_prim;
+};
+
+// clamp_bvh_direction (cycles_triangle_intersection_component.cpp:31-37).
+__device__ __forceinline__ float clamp_bvh_direction(float v) {
+    const float m = 8.271806e-25f;
+    return fabsf(v) > m ? v : copysignf(m, v);
+}
+
+__device__ __forceinline__ f3 pl_cross(f3 a, f3 b) {
+    return {fmaf(a.y, b.z, -(a.z * b.y)), fmaf(a.z, b.x, -(a.x * b.z)), fmaf(a.x, b.y, -(a.y * b.x))};
+}
+__device__ __forceinline__ float pl_dot(f3 a, f3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+
+// PlueckerTriangleIntersectionComponent::intersect
+// (cycles_triangle_intersection_component.cpp:39-105).
+__device__ __forceinline__ bool intersect_triangle(f3 o, f3 d, float tmin, float tmax, f3 p0, f3 p1, f3 p2,
+                                                   float &t_out, float &u_out, float &v_out) {
+    const f3 v0 = p0 - o, v1 = p1 - o, v2 = p2 - o;
+    const f3 e0 = v2 - v0, e1 = v0 - v1, e2 = v1 - v2;
+    const float u = pl_dot(pl_cross(e0, v2 + v0), d);
+    const float v = pl_dot(pl_cross(e1, v0 + v1), d);
+    const float w = pl_dot(pl_cross(e2, v1 + v2), d);
+    const float sum = u + v + w;
+    const float tol = 1.1920928955078125e-07f * fabsf(sum);
+    const float mn = minf_(u, minf_(v, w));
+    const float mx = maxf_(u, maxf_(v, w));
+    if (!((mn >= -tol) || (mx <= tol))) return false;
+    const f3 n2 = pl_cross(e1, e0) * 2.0f;
+    const float den = pl_dot(n2, d);
+    if (den == 0.0f) return false;
+    const float t = pl_dot(v0, n2) / den;
+    if (!((t >= tmin) && (t <= tmax))) return false;
+    const float rs = fabsf(sum) >= 1.0e-18f ? 1.0f / sum : 0.0f;
+    t_out = t;
+    u_out = minf_(u * rs, 1.0f);
+    v_out = minf_(v * rs, 1.0f);
+    return true;
+}
+
+__device__ __forceinline__ Xform load_xform(const float *m) {
+    return {ld3(m), ld3(m + 3), ld3(m + 6), ld3(m + 9)};
+}
+
+// Slab test of both children of a binary node.  Boxes are padded at build
+// time and the far bound widened by a relative 2^-20, so a triangle that the
+// Pluecker predicate accepts inside [tmin, tmax] is never culled.
+__device__ __forceinline__ void node_slabs(const BvhNodeGpu &n, f3 org_inv, f3 inv, float tmin, float tmax,
+                                           float &lnear, float &rnear, bool &lhit, bool &rhit) {
+    const float lx0 = fmaf(n.x.x, inv.x, -org_inv.x), lx1 = fmaf(n.x.y, inv.x, -org_inv.x);
+    const float ly0 = fmaf(n.y.x, inv.y, -org_inv.y), ly1 = fmaf(n.y.y, inv.y, -org_inv.y);
+    const float lz0 = fmaf(n.z.x, inv.z, -org_inv.z), lz1 = fmaf(n.z.y, inv.z, -org_inv.z);
+    const float rx0 = fmaf(n.x.z, inv.x, -org_inv.x), rx1 = fmaf(n.x.w, inv.x, -org_inv.x);
+    const float ry0 = fmaf(n.y.z, inv.y, -org_inv.y), ry1 = fmaf(n.y.w, inv.y, -org_inv.y);
+    const float rz0 = fmaf(n.z.z, inv.z, -org_inv.z), rz1 = fmaf(n.z.w, inv.z, -org_inv.z);
+    const float ln = fmaxf(fmaxf(fminf(lx0, lx1), fminf(ly0, ly1)), fmaxf(fminf(lz0, lz1), tmin));
+    const float lf = fminf(fminf(fmaxf(lx0, lx1), fmaxf(ly0, ly1)), fminf(fmaxf(lz0, lz1), tmax));
+    const float rn = fmaxf(fmaxf(fminf(rx0, rx1), fminf(ry0, ry1)), fmaxf(fminf(rz0, rz1), tmin));
+    const float rf = fminf(fminf(fmaxf(rx0, rx1), fmaxf(ry0, ry1)), fminf(fmaxf(rz0, rz1), tmax));
+    lhit = ln <= lf * 1.00000095367431640625f + 1.0e-30f || ln <= lf;
+    rhit = rn <= rf * 1.00000095367431640625f + 1.0e-30f || rn <= rf;
+    lnear = ln;
+    rnear = rn;
+}
+
+__device__ __forceinline__ BvhNodeGpu load_node(const BvhNodeGpu *nodes, int idx) {
+    const float4 *p = reinterpret_cast<const float4 *>(nodes + idx);
+    BvhNodeGpu n;
+    n.x = __ldg(p + 0);
+    n.y = __ldg(p + 1);
+    n.z = __ldg(p + 2);
+    const float4 c = __ldg(p + 3);
+    n.child = make_int4(__float_as_int(c.x), __float_as_int(c.y), __float_as_int(c.z), __float_as_int(c.w));
+    return n;
+}
+
+constexpr int kStackSize = 64;
+
+// Closest hit of the whole scene under the Cycles predicate
+// (UnifiedSceneTraversalComponent::trace, src/luisa/path_kernel_scene_traversal.cpp:301-490):
+// closed [tmin, tmax], exclusion of the source and light identities, and
+// equal distances resolved to the greatest (object, primitive).  `any_hit`
+// returns at the first accepted candidate (opaque shadow rays).
+__device__ __forceinline__ bool trace_closest(const SceneView &s, const Ray &ray, uint32_t visibility,
+                                              uint32_t src_obj, uint32_t src_prim, uint32_t light_obj,
+                                              uint32_t light_prim, bool any_hit, Hit &best) {
+    bool has = false;
+    best.t = ray.tmax;
+    best.u = best.v = 0.0f;
+    best.instance = best.prim = best.object = best.cycles_prim = kInvalid;
+    // world-space ray for the TLAS
+    const f3 wd = mk3(clamp_bvh_direction(ray.d.x), clamp_bvh_direction(ray.d.y), clamp_bvh_direction(ray.d.z));
+    const f3 winv = mk3(1.0f / wd.x, 1.0f / wd.y, 1.0f / wd.z);
+    const f3 worg_inv = mk3(ray.o.x * winv.x, ray.o.y * winv.y, ray.o.z * winv.z);
+    int tstack[kStackSize];
+    int tsp = 0;
+    int node = 0;
+    if (s.instance_count == 0u) return false;
+    for (;;) {
+        // TLAS: nodes whose children are instances (leaf count 1, index ~i)
+        const BvhNodeGpu n = load_node(s.tlas, node);
+        const float limit = has ? best.t : ray.tmax;
+        float ln, rn;
+        bool lh, rh;
+        node_slabs(n, worg_inv, winv, ray.tmin, limit, ln, rn, lh, rh);
+        int next = -1;
+        int pending[2];
+        int pc = 0;
+        // order: nearer child first
+        const bool swap = rn < ln;
+        const int first = swap ? 1 : 0;
+        for (int k = 0; k < 2; ++k) {
+            const int side = k == 0 ? first : 1 - first;
+            const bool h = side == 0 ? lh : rh;
+            if (!h) continue;
+            const int c = side == 0 ? n.child.x : n.child.y;
+            const int cnt = side == 0 ? n.child.z : n.child.w;
+            if (c >= 0) {
+                pending[pc++] = c;
+                continue;
+            }
+            // instance leaves
+            for (int li = 0; li < cnt; ++li) {
+                const uint32_t ii = uint32_t(~c) + uint32_t(li);
+                const InstanceGpu &inst = s.instances[ii];
+                if ((inst.visibility & visibility) == 0u) continue;
+                const MeshGpu mesh = s.meshes[inst.mesh];
+                const Xform w2o = load_xform(inst.w2o);
+                const f3 o = xform_point(w2o, ray.o);
+                const f3 rdir = xform_direction(w2o, ray.d);
+                const f3 d = mk3(clamp_bvh_direction(rdir.x), clamp_bvh_direction(rdir.y), clamp_bvh_direction(rdir.z));
+                const f3 inv = mk3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+                const f3 org_inv = mk3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+                int bstack[kStackSize];
+                int bsp = 0;
+                int bnode = int(mesh.node_offset);
+                for (;;) {
+                    const BvhNodeGpu b = load_node(s.blas, bnode);
+                    const float blimit = has ? best.t : ray.tmax;
+                    float bln, brn;
+                    bool blh, brh;
+                    node_slabs(b, org_inv, inv, ray.tmin, blimit, bln, brn, blh, brh);
+                    int bpending[2];
+                    int bpc = 0;
+                    const bool bswap = brn < bln;
+                    const int bfirst = bswap ? 1 : 0;
+                    for (int k2 = 0; k2 < 2; ++k2) {
+                        const int side = k2 == 0 ? bfirst : 1 - bfirst;
+                        const bool h = side == 0 ? blh : brh;
+                        if (!h) continue;
+                        const int c2 = side == 0 ? b.child.x : b.child.y;
+                        const int cnt2 = side == 0 ? b.child.z : b.child.w;
+                        if (c2 >= 0) {
+                            bpending[bpc++] = int(mesh.node_offset) + c2;
+                            continue;
+                        }
+                        const uint32_t first_tri = mesh.tri_offset + uint32_t(~c2);
+                        for (int ti = 0; ti < cnt2; ++ti) {
+                            const float4 *tp = s.tris + 3u * (first_tri + uint32_t(ti));
+                            const float4 a = __ldg(tp), bb = __ldg(tp + 1), cc = __ldg(tp + 2);
+                            const uint32_t local = __float_as_uint(a.w);
+                            const uint32_t cp = mesh.prim_offset + local;
+                            if ((src_obj == ii && src_prim == cp) || (light_obj == ii && light_prim == cp)) continue;
+                            float t, u, v;
+                            const float tmax_test = has ? best.t : ray.tmax;
+                            if (!intersect_triangle(o, d, ray.tmin, tmax_test, ld3(a), ld3(bb), ld3(cc), t, u, v))
+                                continue;
+                            const bool later = ii > best.object || (ii == best.object && cp > best.cycles_prim);
+                            if (has && !(t < best.t || (t == best.t && later))) continue;
+                            has = true;
+                            best.t = t;
+                            best.u = u;
+                            best.v = v;
+                            best.instance = ii;
+                            best.prim = local;
+                            best.object = ii;
+                            best.cycles_prim = cp;
+                            if (any_hit) return true;
+                        }
+                    }
+                    if (bpc == 2) {
+                        if (bsp < kStackSize) bstack[bsp++] = bpending[1];
+                        bnode = bpending[0];
+                    } else if (bpc == 1) {
+                        bnode = bpending[0];
+                    } else {
+                        if (bsp == 0) break;
+                        bnode = bstack[--bsp];
+                    }
+                }
+            }
+        }
+        if (pc == 2) {
+            if (tsp < kStackSize) tstack[tsp++] = pending[1];
+            next = pending[0];
+        } else if (pc == 1) {
+            next = pending[0];
+        } else {
+            if (tsp == 0) break;
+            next = tstack[--tsp];
+        }
+        node = next;
+    }
+    return has;
+}
+
+// ---------------------------------------------------------- hit geometry
+
+struct SurfacePoint {
+    f3 position, object_position, ng, n;
+    f3 p0, p1, p2, wp0, wp1, wp2;
+    bool back_facing;
+    uint32_t instance, material, object, cycles_prim;
+};
+
+__device__ __forceinline__ f3 tri_interp(float u, float v, f3 a, f3 b, f3 c) {
+    return a * (1.0f - u - v) + b * u + c * v;
+}
+
+// FinalSupportTriangleSurfaceComponent::resolve (src/luisa/cycles_triangle_surface_component.cpp:9-95)
+// for instanced meshes.
+__device__ __forceinline__ SurfacePoint surface_point(const SceneView &s, const Hit &h, f3 ray_d) {
+    SurfacePoint sp;
+    const InstanceGpu &inst = s.instances[h.instance];
+    const MeshGpu mesh = s.meshes[inst.mesh];
+    const uint32_t *idx = s.indices + mesh.index_offset + 3u * h.prim;
+    const uint32_t i0 = idx[0], i1 = idx[1], i2 = idx[2];
+    const float *P = s.positions + 3u * mesh.vertex_offset;
+    sp.p0 = ld3(P + 3u * i0);
+    sp.p1 = ld3(P + 3u * i1);
+    sp.p2 = ld3(P + 3u * i2);
+    const Xform o2w = load_xform(inst.o2w);
+    const Xform nrm = load_xform(inst.nrm);
+    sp.wp0 = xform_point(o2w, sp.p0);
+    sp.wp1 = xform_point(o2w, sp.p1);
+    sp.wp2 = xform_point(o2w, sp.p2);
+    const f3 ogn = safe_normalize(cross(sp.p1 - sp.p0, sp.p2 - sp.p0), mk3(0.0f, 0.0f, 1.0f));
+    f3 ng = safe_normalize(xform_direction(nrm, ogn), -ray_d);
+    f3 osn = ogn;
+    if (mesh.smooth) {
+        const float *N = s.normals + 3u * mesh.vertex_offset;
+        osn = tri_interp(h.u, h.v, ld3(N + 3u * i0), ld3(N + 3u * i1), ld3(N + 3u * i2));
+    }
+    f3 n = safe_normalize(xform_direction(nrm, osn), ng);
+    sp.back_facing = dot(ng, -ray_d) < 0.0f;
+    if (sp.back_facing) {
+        ng = -ng;
+        n = -n;
+    }
+    if (dot(n, ng) < 0.0f) n = -n;
+    sp.ng = ng;
+    sp.n = n;
+    sp.object_position = sp.p0 + (sp.p1 - sp.p0) * h.u + (sp.p2 - sp.p0) * h.v;
+    sp.position = xform_point(o2w, sp.object_position);
+    sp.instance = h.instance;
+    sp.material = mesh.material_offset == kInvalid ? inst.material : s.tri_materials[mesh.material_offset + h.prim];
+    sp.object = h.object;
+    sp.cycles_prim = h.cycles_prim;
+    return sp;
+}
+
+// Wachter & Binder robust offset (Ray Tracing Gems ch. 6), the published
+// method behind Luisa's offset_ray_origin.
+__device__ __forceinline__ float offset_component(float p, float n) {
+    const float origin = 1.0f / 32.0f, float_scale = 1.0f / 65536.0f, int_scale = 256.0f;
+    const int of_i = static_cast<int>(int_scale * n);
+    const float p_i = __int_as_float(__float_as_int(p) + (p < 0.0f ? -of_i : of_i));
+    return fabsf(p) < origin ? p + float_scale * n : p_i;
+}
+
+// origin_with_explicit_self_exclusion (include/psycles/luisa/surface_ray.h:49-100).
+__device__ __forceinline__ f3 origin_with_self_exclusion(const SurfacePoint &sp, f3 oo, f3 od) {
+    const f3 v0 = sp.p0 - oo, v1 = sp.p1 - oo, v2 = sp.p2 - oo;
+    const f3 e0 = v2 - v0, e1 = v0 - v1, e2 = v1 - v2;
+    const float u = dot(cross(v2 + v0, e0), od);
+    const float v = dot(cross(v0 + v1, e1), od);
+    const float w = dot(cross(v1 + v2, e2), od);
+    const float eps = 1.1920928955078125e-07f * fabsf(u + v + w);
+    const float mn = minf_(u, minf_(v, w)), mx = maxf_(u, maxf_(v, w));
+    if ((mn >= eps) || (mx <= -eps)) return sp.position;
+    return mk3(offset_component(sp.position.x, sp.ng.x), offset_component(sp.position.y, sp.ng.y),
+               offset_component(sp.position.z, sp.ng.z));
+}
+
+// ------------------------------------------------------- light sampling
+
+__device__ __forceinline__ DistEntryGpu distribution_sample(const SceneView &s, float u) {
+    if (s.emitter_count == 0u) return {0.0f, 0.0f, 3u, 0u};
+    uint32_t first = 0u, length = s.emitter_count + 1u;
+    while (length > 0u) {
+        const uint32_t half = length >> 1u;
+        const uint32_t middle = first + half;
+        if (u < s.distribution[middle].cumulative) {
+            length = half;
+        } else {
+            first = middle + 1u;
+            length = length - half - 1u;
+        }
+    }
+    uint32_t selected = first > 0u ? first - 1u : 0u;
+    selected = min(selected, s.emitter_count - 1u);
+    return s.distribution[selected];
+}
+
+__device__ __forceinline__ float triangle_solid_angle(f3 r, f3 p0, f3 p1, f3 p2) {
+    const f3 a = normalize_or(p0 - r, mk3(1.0f, 0.0f, 0.0f));
+    const f3 b = normalize_or(p1 - r, mk3(0.0f, 1.0f, 0.0f));
+    const f3 c = normalize_or(p2 - r, mk3(0.0f, 0.0f, 1.0f));
+    const float num = fabsf(dot(a, cross(b, c)));
+    const float den = 1.0f + dot(a, b) + dot(b, c) + dot(c, a);
+    return 2.0f * atan2_(num, den);
+}
+__device__ __forceinline__ bool use_solid_angle(f3 r, f3 p0, f3 p1, f3 p2) {
+    const f3 e0 = p1 - p0, e1 = p2 - p0, e2 = p2 - p1;
+    const float longest = maxf_(dot(e0, e0), maxf_(dot(e1, e1), dot(e2, e2)));
+    const f3 un = cross(e0, e1);
+    const float nl2 = dot(un, un);
+    const float dist = dot(un, p0 - r) / maxf_(nl2, 1.0e-20f);
+    return nl2 > 1.0e-20f && longest > dist * dist;
+}
+struct TriPdf {
+    float value;
+    bool valid;
+};
+// triangle_directional_pdf (include/psycles/luisa/spherical_geometry.h:161-203).
+__device__ __forceinline__ TriPdf triangle_directional_pdf(f3 r, f3 lp, f3 p0, f3 p1, f3 p2) {
+    const f3 e0 = p1 - p0, e1 = p2 - p0;
+    const f3 un = cross(e0, e1);
+    const float da = sqrtf(maxf_(dot(un, un), 0.0f));
+    const float area = 0.5f * da;
+    const f3 nrm = un / maxf_(da, 1.0e-20f);
+    const f3 off = lp - r;
+    const float d2 = dot(off, off);
+    const f3 dir = off / sqrtf(maxf_(d2, 1.0e-20f));
+    const float cosine = fabsf(dot(nrm, -dir));
+    const bool sa = use_solid_angle(r, p0, p1, p2);
+    const float solid = triangle_solid_angle(r, p0, p1, p2);
+    const float area_pdf = d2 / maxf_(cosine * area, 1.0e-20f);
+    const float sa_pdf = 1.0f / maxf_(solid, 1.0e-20f);
+    const bool valid_area = area > 0.0f && d2 > 1.0e-12f && cosine > 0.0f;
+    return {sa ? sa_pdf : area_pdf, sa ? (valid_area && solid > 0.0f) : valid_area};
+}
+struct TriSample {
+    f3 position, direction;
+    float distance, pdf;
+    bool valid;
+};
+// sample_triangle (spherical_geometry.h:207-283).
+__device__ __forceinline__ TriSample sample_triangle(f3 r, f3 p0, f3 p1, f3 p2, f2 rnd) {
+    const float x = clampf_(rnd.x, 0.0f, 1.0f), y = clampf_(rnd.y, 0.0f, 1.0f);
+    f2 ab;
+    if (y > x) {
+        ab.x = 0.5f * x;
+        ab.y = y - ab.x;
+    } else {
+        ab.y = 0.5f * y;
+        ab.x = x - ab.y;
+    }
+    const f3 area_position = p0 * (1.0f - ab.x - ab.y) + p1 * ab.x + p2 * ab.y;
+    const f3 area_offset = area_position - r;
+    const float area_d2 = dot(area_offset, area_offset);
+    const float area_distance = sqrtf(maxf_(area_d2, 1.0e-20f));
+    const f3 area_direction = area_offset / area_distance;
+    TriSample out;
+    const bool sa = use_solid_angle(r, p0, p1, p2);
+    if (!sa) {
+        const TriPdf pdf = triangle_directional_pdf(r, area_position, p0, p1, p2);
+        out.position = area_position;
+        out.direction = area_direction;
+        out.distance = area_distance;
+        out.pdf = pdf.value;
+        out.valid = pdf.valid && area_d2 > 1.0e-12f;
+        return out;
+    }
+    const f3 a = normalize_or(p0 - r, mk3(1.0f, 0.0f, 0.0f));
+    const f3 b = normalize_or(p1 - r, mk3(0.0f, 1.0f, 0.0f));
+    const f3 c = normalize_or(p2 - r, mk3(0.0f, 0.0f, 1.0f));
+    const float cos_b = clampf_(dot(a, c), -1.0f, 1.0f);
+    const float cos_c = clampf_(dot(a, b), -1.0f, 1.0f);
+    const float solid = triangle_solid_angle(r, p0, p1, p2);
+    const f3 ab_n = normalize_or(cross(a, b), mk3(1.0f, 0.0f, 0.0f));
+    const f3 ac_n = normalize_or(cross(a, c), mk3(0.0f, 1.0f, 0.0f));
+    const float cos_alpha = clampf_(dot(ab_n, ac_n), -1.0f, 1.0f);
+    const float sin_alpha = sqrtf(maxf_(1.0f - cos_alpha * cos_alpha, 0.0f));
+    const float alpha = acos_(cos_alpha);
+    const float phi = x * solid - alpha;
+    const float sin_phi = sin_(phi), cos_phi = cos_(phi);
+    const float u = cos_phi - cos_alpha;
+    const float v = sin_phi + sin_alpha * cos_c;
+    const float num = (v * cos_phi - u * sin_phi) * cos_alpha - v;
+    const float den = (v * sin_phi + u * cos_phi) * sin_alpha;
+    const float safe_den = fabsf(den) > 1.0e-20f ? den : (den >= 0.0f ? 1.0e-20f : -1.0e-20f);
+    const float q = fabsf(den) <= 1.0e-20f ? 1.0f : num / safe_den;
+    const f3 tangent = normalize_or(c - a * cos_b, mk3(0.0f, 1.0f, 0.0f));
+    const f3 c_prime = normalize_or(a * clampf_(q, -1.0f, 1.0f) + tangent * sqrtf(maxf_(1.0f - q * q, 0.0f)), a);
+    const float z = 1.0f - y * (1.0f - dot(c_prime, b));
+    const f3 edge_dir = normalize_or(c_prime - b * dot(c_prime, b), a);
+    const f3 solid_dir = normalize_or(b * z + edge_dir * sqrtf(maxf_(1.0f - z * z, 0.0f)), b);
+    const f3 e01 = p1 - p0, e02 = p2 - p0;
+    const f3 pv = cross(solid_dir, e02);
+    const float det = dot(e01, pv);
+    const float safe_det = fabsf(det) > 1.0e-20f ? det : (det >= 0.0f ? 1.0e-20f : -1.0e-20f);
+    const float inv_det = 1.0f / safe_det;
+    const f3 tv = r - p0;
+    const float su = dot(tv, pv) * inv_det;
+    const f3 qv = cross(tv, e01);
+    const float sv = dot(solid_dir, qv) * inv_det;
+    const float sd = dot(e02, qv) * inv_det;
+    const f3 solid_position = r + solid_dir * sd;
+    const bool solid_valid = fabsf(det) > 1.0e-20f && sd > 0.0f && su >= -1.0e-5f && sv >= -1.0e-5f &&
+                             su + sv <= 1.0f + 1.0e-5f && solid > 0.0f;
+    const TriPdf pdf = triangle_directional_pdf(r, solid_position, p0, p1, p2);
+    out.position = solid_position;
+    out.direction = solid_dir;
+    out.distance = sd;
+    out.pdf = pdf.value;
+    out.valid = pdf.valid && solid_valid;
+    return out;
+}
+
+__device__ __forceinline__ bool samples_front(uint32_t m) { return m == 1u || m == 2u || m == 4u; }
+__device__ __forceinline__ bool samples_back(uint32_t m) { return m == 1u || m == 3u || m == 4u; }
+__device__ __forceinline__ bool sampled_side(uint32_t m, f3 ng, f3 dir) {
+    return dot(ng, -dir) < 0.0f ? samples_back(m) : samples_front(m);
+}
+
+__device__ __forceinline__ float emissive_forward_pdf(float selection_pdf, uint32_t sampling, f3 reference, f3 lp,
+                                                      f3 p0, f3 p1, f3 p2, f3 oriented_ng) {
+    const TriPdf pdf = triangle_directional_pdf(reference, lp, p0, p1, p2);
+    const f3 dir = normalize_or(lp - reference, mk3(0.0f, 0.0f, 1.0f));
+    const bool side = sampled_side(sampling, oriented_ng, dir);
+    const float area = 0.5f * length(cross(p1 - p0, p2 - p0));
+    const float value = pdf.value * selection_pdf;
+    return (sampling != 0u && side && pdf.valid && area > 0.0f && value > 0.0f) ? value : 0.0f;
+}
+
+struct AnalyticSample {
+    bool valid;
+    f3 direction, position;
+    float distance, pdf, eval_factor;
+};
+
+// include/psycles/luisa/analytic_light_sampling.h:84-108 (distant),
+// :549-603 (disk), :856-896 (pdf / eval factor), :309-345 (spot profile).
+__device__ __forceinline__ AnalyticSample sample_analytic(const psy_light_desc &l, f3 reference, f2 rnd) {
+    AnalyticSample out;
+    const bool normalize_power = (l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u;
+    if (l.type == PSY_LIGHT_DISTANT) {
+        const f3 az = ld3(l.axis_z);
+        const float half_angle = 0.5f * maxf_(l.angle, 0.0f);
+        const float sq = sin_(0.5f * half_angle);
+        const float omc = 2.0f * sq * sq;
+        const ConeSample c = sample_uniform_cone(-az, omc, rnd);
+        const bool finite = half_angle > 0.0f;
+        const float sh = sin_(half_angle);
+        const float disk_area = kPi * sh * sh;
+        out.eval_factor = (normalize_power && finite) ? 1.0f / maxf_(disk_area, 1.0e-20f) : 1.0f;
+        out.direction = -c.direction;
+        out.position = c.direction;
+        out.distance = 1.0e30f;
+        out.pdf = c.pdf;
+        out.valid = true;
+        return out;
+    }
+    const f3 center = ld3(l.position);
+    f3 ln = reference - center;
+    const float cd2 = dot(ln, ln);
+    const float cd = sqrtf(maxf_(cd2, 1.0e-30f));
+    ln = ln / cd;
+    const Basis b = make_orthonormals(ln);
+    const f2 disk = sample_uniform_disk(rnd);
+    const f3 position = center + (b.tangent * disk.x + b.bitangent * disk.y) * l.radius;
+    const f3 off = position - reference;
+    const float d2 = dot(off, off);
+    const float dist = sqrtf(maxf_(d2, 1.0e-30f));
+    const f3 dir = off / dist;
+    const float cosine = dot(ln, -dir);
+    const float r2 = l.radius * l.radius;
+    const float inv_area = r2 > 0.0f ? 1.0f / maxf_(r2 * kPi, 1.0e-20f) : 1.0f;
+    out.pdf = cosine > 0.0f ? inv_area * d2 / cosine : 0.0f;
+    const float area = r2 > 0.0f ? 4.0f * kPi * r2 : 4.0f;
+    float eval = (normalize_power ? 1.0f / maxf_(area, 1.0e-20f) : 1.0f) * kInvPi;
+    if (l.type == PSY_LIGHT_SPOT) {
+        const f3 ax = ld3(l.axis_x) * l.axis_scale[0];
+        const f3 ay = ld3(l.axis_y) * l.axis_scale[1];
+        const f3 az = ld3(l.axis_z) * l.axis_scale[2];
+        const f3 adj_x = cross(ay, az);
+        const float det = dot(ax, adj_x);
+        const bool valid = fabsf(det) > 1.0e-20f;
+        const float inv_det = 1.0f / (valid ? det : 1.0f);
+        const f3 rx = adj_x * inv_det, ry = cross(az, ax) * inv_det, rz = cross(ax, ay) * inv_det;
+        const f3 from_light = -dir;
+        f3 local = light_safe_normalize(mk3(dot(rx, from_light), dot(ry, from_light), dot(rz, from_light)),
+                                        mk3(0.0f, 0.0f, -1.0f));
+        local.z = -local.z;
+        const float cos_half = cos_(0.5f * l.spot_angle);
+        const float blend = (1.0f - cos_half) * l.spot_smooth;
+        const float ratio = blend != 0.0f ? (local.z - cos_half) / blend : 0.0f;
+        const float lin = clampf_(ratio, 0.0f, 1.0f);
+        const float smooth = lin * lin * (3.0f - 2.0f * lin);
+        const float hard = local.z >= cos_half ? 1.0f : 0.0f;
+        eval *= blend > 0.0f ? smooth : hard;
+    }
+    out.eval_factor = eval;
+    out.direction = dir;
+    out.position = position;
+    out.distance = dist;
+    out.valid = cd2 > 0.0f && cosine > 0.0f && eval != 0.0f;
+    return out;
+}
+
+}  // namespace psy

@@ -1,0 +1,1214 @@
+// Host side of libpsycles_cuda.so: the C ABI of include/psycles_cuda.h.
+//
+//   * host precompute: tabulated-Sobol LUT (src/sampling/tabulated_sobol.cpp),
+//     pixel-filter inverse CDF (src/sampling/pixel_filter.cpp), flat light
+//     distribution (src/sampling/light_distribution.cpp)
+//   * scene compile (LuisaPathTracerBackend::compile_scene,
+//     src/luisa/path_tracer_scene.cpp:50): flattening, binned-SAH BVH build
+//     per mesh plus an instance TLAS, emitter table, upload
+//   * sessions (LuisaRenderSession, src/luisa/path_tracer_session.cpp):
+//     film buffers, SampleRange validation, the wavefront render loop and
+//     pass readback
+// Compiled without FP contraction so the host tables are bit-identical to
+// the reference's construction.
+#include "psy_kernels.h"
+#include "psy_scene.h"
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_last_error;
+
+psy_status fail(psy_status status, const std::string &message) {
+    g_last_error = message;
+    return status;
+}
+
+#define PSY_CUDA_TRY(expr)                                                                        \
+    do {                                                                                          \
+        const cudaError_t err_ = (expr);                                                          \
+        if (err_ != cudaSuccess) {                                                                \
+            return fail(PSY_ERROR_CUDA, std::string(#expr ": ") + cudaGetErrorString(err_));      \
+        }                                                                                         \
+    } while (0)
+
+// ------------------------------------------------------------ Sobol LUT
+// Cycles' progressive multi-jittered 4-D table (tabulated_sobol.cpp:75-200).
+
+const uint32_t kXors[4][32] = {
+    {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u,
+     0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u},
+    {0x00000000u, 0x00000001u, 0x00000001u, 0x00000007u, 0x00000001u, 0x00000013u, 0x00000015u, 0x0000007fu,
+     0x00000001u, 0x00000103u, 0x00000105u, 0x0000070fu, 0x00000111u, 0x00001333u, 0x00001555u, 0x00007fffu,
+     0x00000001u, 0x00010003u, 0x00010005u, 0x0007000fu, 0x00010011u, 0x00130033u, 0x00150055u, 0x007f00ffu,
+     0x00010101u, 0x01030303u, 0x01050505u, 0x070f0f0fu, 0x01111111u, 0x13333333u, 0x15555555u, 0x7fffffffu},
+    {0x00000000u, 0x00000001u, 0x00000003u, 0x00000001u, 0x00000005u, 0x0000001fu, 0x0000002bu, 0x0000003du,
+     0x00000011u, 0x00000133u, 0x00000377u, 0x00000199u, 0x00000445u, 0x00001ccfu, 0x00002ddbu, 0x0000366du,
+     0x00000101u, 0x00010303u, 0x00030707u, 0x00010909u, 0x00051515u, 0x001f3f3fu, 0x002b6b6bu, 0x003dbdbdu,
+     0x00101011u, 0x01303033u, 0x03707077u, 0x01909099u, 0x04515145u, 0x1cf3f3cfu, 0x2db6b6dbu, 0x36dbdb6du},
+    {0x00000000u, 0x00000001u, 0x00000000u, 0x00000003u, 0x0000000du, 0x0000000cu, 0x00000005u, 0x0000004fu,
+     0x00000014u, 0x000000e7u, 0x00000329u, 0x0000039cu, 0x00000011u, 0x00001033u, 0x00000044u, 0x000030bbu,
+     0x0000d1cdu, 0x0000c2ecu, 0x00005415u, 0x0004fc3fu, 0x00015054u, 0x000e5c97u, 0x0032e5b9u, 0x0039725cu,
+     0x00000101u, 0x01000303u, 0x00000404u, 0x03000b0bu, 0x0d001d1du, 0x0c002c2cu, 0x05004545u, 0x4f00cfcfu},
+};
+
+uint32_t hp_hash(uint32_t v) {
+    v ^= v >> 16u;
+    v *= 0x21f0aaadu;
+    v ^= v >> 15u;
+    v *= 0xd35a2d97u;
+    v ^= v >> 15u;
+    return v ^ 0xe6fe3bebu;
+}
+float hp_float(uint32_t v) { return static_cast<float>(hp_hash(v)) * (1.0f / 4294967808.0f); }
+
+void sobol_pattern(float *pts, uint32_t size, uint32_t seed) {
+    uint32_t s = 0x44605a73u;
+    s ^= s << 19u;
+    uint32_t idx = hp_hash(seed ^ s);
+    for (int c = 0; c < 4; ++c) pts[c] = hp_float(idx++);
+    uint32_t log_n = 0u;
+    for (uint32_t n = 1u; n < size; ++log_n, n *= 2u) {
+        const float strata = static_cast<float>(n * 2u);
+        for (uint32_t i = 0u; i < n && n + i < size; ++i) {
+            uint32_t occ[4];
+            for (int c = 0; c < 4; ++c) occ[c] = static_cast<uint32_t>(pts[4 * (i ^ kXors[c][log_n]) + c] * strata);
+            for (int c = 0; c < 4; ++c)
+                pts[4 * (n + i) + c] = (static_cast<float>(occ[c] ^ 1u) + hp_float(idx++)) / strata;
+        }
+    }
+}
+
+bool sobol_size_valid(uint32_t s) { return s >= 256u && s <= 8192u && (s & (s - 1u)) == 0u; }
+
+// ------------------------------------------------------- pixel filter
+
+std::array<float, 1024> filter_table(uint32_t filter, float width) {
+    width = std::max(width, 1.0e-5f);
+    int kind = 0;
+    if (filter == PSY_FILTER_GAUSSIAN) {
+        kind = 1;
+        width *= 3.0f;
+    } else if (filter == PSY_FILTER_BLACKMAN_HARRIS) {
+        kind = 2;
+        width *= 2.0f;
+    }
+    auto f = [&](float v, float w) -> float {
+        if (kind == 1) {
+            v *= 6.0f / w;
+            return std::exp(-2.0f * v * v);
+        }
+        if (kind == 2) {
+            constexpr float two_pi = 6.28318530717958647692f;
+            v = two_pi * (v / w + 0.5f);
+            return 0.35875f - 0.48829f * std::cos(v) + 0.14128f * std::cos(2.0f * v) - 0.01168f * std::cos(3.0f * v);
+        }
+        return 1.0f;
+    };
+    constexpr size_t n = 1024u, res = n - 1u, half = (n - 1u) / 2u;
+    std::array<float, n> cdf{};
+    const float range = width * 0.5f;
+    for (size_t i = 0; i < res; ++i) {
+        const float v = range * static_cast<float>(i) / static_cast<float>(res - 1u);
+        cdf[i + 1u] = cdf[i] + std::fabs(f(v, width));
+    }
+    const float norm = cdf[res] == 0.0f ? 0.0f : 1.0f / cdf[res];
+    for (auto &v : cdf) v *= norm;
+    cdf[res] = 1.0f;
+    std::array<float, n> inv{};
+    for (size_t i = 0; i <= half; ++i) {
+        const float x = static_cast<float>(i) / static_cast<float>(half);
+        size_t index = static_cast<size_t>(std::upper_bound(cdf.begin(), cdf.end(), x) - cdf.begin());
+        float t = 0.0f;
+        if (index < res) t = (x - cdf[index]) / (cdf[index + 1u] - cdf[index]);
+        else index = res;
+        const float y = (static_cast<float>(index) + t) / static_cast<float>(n - 1u) * (2.0f * range);
+        inv[half + i] = 0.5f * (1.0f + y);
+        inv[half - i] = 0.5f * (1.0f - y);
+    }
+    return inv;
+}
+
+// ------------------------------------------------------------- geometry
+
+struct V3 {
+    float x, y, z;
+};
+V3 v3(float x, float y, float z) { return {x, y, z}; }
+V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+V3 crs(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+float dt(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+struct M34 {
+    V3 c0, c1, c2, c3;
+};
+M34 m34(const float *e) { return {{e[0], e[1], e[2]}, {e[4], e[5], e[6]}, {e[8], e[9], e[10]}, {e[12], e[13], e[14]}}; }
+V3 xaff(const M34 &m, V3 v, bool t) {
+    const float tx = t ? m.c3.x : 0.0f, ty = t ? m.c3.y : 0.0f, tz = t ? m.c3.z : 0.0f;
+    return {std::fma(v.x, m.c0.x, std::fma(v.y, m.c1.x, std::fma(v.z, m.c2.x, tx))),
+            std::fma(v.x, m.c0.y, std::fma(v.y, m.c1.y, std::fma(v.z, m.c2.y, ty))),
+            std::fma(v.x, m.c0.z, std::fma(v.y, m.c1.z, std::fma(v.z, m.c2.z, tz)))};
+}
+// Affine inverse in double precision with one rounding to float.
+M34 inverse34(const M34 &m) {
+    const double a00 = m.c0.x, a10 = m.c0.y, a20 = m.c0.z, a01 = m.c1.x, a11 = m.c1.y, a21 = m.c1.z;
+    const double a02 = m.c2.x, a12 = m.c2.y, a22 = m.c2.z, t0 = m.c3.x, t1 = m.c3.y, t2 = m.c3.z;
+    const double c00 = a11 * a22 - a12 * a21, c01 = a12 * a20 - a10 * a22, c02 = a10 * a21 - a11 * a20;
+    const double det = a00 * c00 + a01 * c01 + a02 * c02;
+    const double inv = det != 0.0 ? 1.0 / det : 0.0;
+    const double i00 = c00 * inv, i01 = (a02 * a21 - a01 * a22) * inv, i02 = (a01 * a12 - a02 * a11) * inv;
+    const double i10 = c01 * inv, i11 = (a00 * a22 - a02 * a20) * inv, i12 = (a02 * a10 - a00 * a12) * inv;
+    const double i20 = c02 * inv, i21 = (a01 * a20 - a00 * a21) * inv, i22 = (a00 * a11 - a01 * a10) * inv;
+    const double u0 = -(i00 * t0 + i01 * t1 + i02 * t2);
+    const double u1 = -(i10 * t0 + i11 * t1 + i12 * t2);
+    const double u2 = -(i20 * t0 + i21 * t1 + i22 * t2);
+    M34 r;
+    r.c0 = {float(i00), float(i10), float(i20)};
+    r.c1 = {float(i01), float(i11), float(i21)};
+    r.c2 = {float(i02), float(i12), float(i22)};
+    r.c3 = {float(u0), float(u1), float(u2)};
+    return r;
+}
+void store34(float *dst, const M34 &m) {
+    const V3 cols[4] = {m.c0, m.c1, m.c2, m.c3};
+    for (int c = 0; c < 4; ++c) {
+        dst[3 * c + 0] = cols[c].x;
+        dst[3 * c + 1] = cols[c].y;
+        dst[3 * c + 2] = cols[c].z;
+    }
+}
+
+// ------------------------------------------------------------ BVH build
+
+struct Box {
+    double lo[3] = {1e300, 1e300, 1e300};
+    double hi[3] = {-1e300, -1e300, -1e300};
+    void grow(const Box &b) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], b.lo[a]);
+            hi[a] = std::max(hi[a], b.hi[a]);
+        }
+    }
+    void grow(double x, double y, double z) {
+        const double p[3] = {x, y, z};
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], p[a]);
+            hi[a] = std::max(hi[a], p[a]);
+        }
+    }
+    bool empty() const { return lo[0] > hi[0]; }
+    double area() const {
+        if (empty()) return 0.0;
+        const double dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+        return 2.0 * (dx * dy + dy * dz + dz * dx);
+    }
+};
+
+struct Prim {
+    Box box;
+    double c[3];
+    uint32_t id;
+};
+
+// Pads a child box so that float slab tests never cull a triangle the
+// Pluecker predicate accepts: relative 1e-5 of the extent plus 1e-6 of the
+// coordinate magnitude, rounded outward.
+void padded(const Box &b, float lo[3], float hi[3]) {
+    for (int a = 0; a < 3; ++a) {
+        if (b.empty()) {
+            lo[a] = 1.0f;
+            hi[a] = -1.0f;
+            continue;
+        }
+        const double pad = 1e-5 * (b.hi[a] - b.lo[a]) + 1e-6 * std::max(std::fabs(b.lo[a]), std::fabs(b.hi[a])) + 1e-30;
+        lo[a] = std::nextafter(float(b.lo[a] - pad), -INFINITY);
+        hi[a] = std::nextafter(float(b.hi[a] + pad), INFINITY);
+    }
+}
+
+struct Builder {
+    std::vector<psy::BvhNodeGpu> nodes;
+    std::vector<Prim> prims;
+    uint32_t leaf_size = 4u;
+    bool leaf_is_id = false;  // TLAS: leaf link = ~prim id, count 1
+
+    struct Child {
+        Box box;
+        int link;
+        int count;
+    };
+
+    Child leaf(uint32_t begin, uint32_t end, const Box &box) {
+        if (leaf_is_id) return {box, ~int(prims[begin].id), 1};
+        return {box, ~int(begin), int(end - begin)};
+    }
+
+    Child build(uint32_t begin, uint32_t end, int depth) {
+        Box box, cbox;
+        for (uint32_t i = begin; i < end; ++i) {
+            box.grow(prims[i].box);
+            cbox.grow(prims[i].c[0], prims[i].c[1], prims[i].c[2]);
+        }
+        const uint32_t count = end - begin;
+        if (count <= leaf_size) return leaf(begin, end, box);
+        // binned SAH over the widest centroid axis
+        int axis = 0;
+        for (int a = 1; a < 3; ++a)
+            if (cbox.hi[a] - cbox.lo[a] > cbox.hi[axis] - cbox.lo[axis]) axis = a;
+        const double extent = cbox.hi[axis] - cbox.lo[axis];
+        uint32_t mid = begin + count / 2u;
+        bool done = false;
+        if (extent > 0.0 && depth < 60) {
+            constexpr int kBins = 16;
+            Box bins[kBins];
+            uint32_t counts[kBins] = {};
+            const double scale = kBins / extent;
+            auto bin_of = [&](const Prim &p) {
+                int b = int((p.c[axis] - cbox.lo[axis]) * scale);
+                return std::min(std::max(b, 0), kBins - 1);
+            };
+            for (uint32_t i = begin; i < end; ++i) {
+                const int b = bin_of(prims[i]);
+                bins[b].grow(prims[i].box);
+                counts[b]++;
+            }
+            double right_area[kBins];
+            uint32_t right_count[kBins];
+            Box acc;
+            uint32_t acc_n = 0u;
+            for (int b = kBins - 1; b > 0; --b) {
+                acc.grow(bins[b]);
+                acc_n += counts[b];
+                right_area[b] = acc.area();
+                right_count[b] = acc_n;
+            }
+            Box left;
+            uint32_t left_n = 0u;
+            double best = 1e300;
+            int best_split = -1;
+            for (int b = 1; b < kBins; ++b) {
+                left.grow(bins[b - 1]);
+                left_n += counts[b - 1];
+                if (left_n == 0u || right_count[b] == 0u) continue;
+                const double cost = left.area() * left_n + right_area[b] * right_count[b];
+                if (cost < best) {
+                    best = cost;
+                    best_split = b;
+                }
+            }
+            if (best_split > 0) {
+                auto it = std::partition(prims.begin() + begin, prims.begin() + end,
+                                         [&](const Prim &p) { return bin_of(p) < best_split; });
+                mid = uint32_t(it - prims.begin());
+                done = mid > begin && mid < end;
+            }
+        }
+        if (!done) {
+            mid = begin + count / 2u;
+            std::nth_element(prims.begin() + begin, prims.begin() + mid, prims.begin() + end,
+                             [&](const Prim &a, const Prim &b) {
+                                 return a.c[axis] < b.c[axis] || (a.c[axis] == b.c[axis] && a.id < b.id);
+                             });
+        }
+        const int index = int(nodes.size());
+        nodes.push_back({});
+        const Child l = build(begin, mid, depth + 1);
+        const Child r = build(mid, end, depth + 1);
+        write(index, l, r);
+        return {box, index, 0};
+    }
+
+    void write(int index, const Child &l, const Child &r) {
+        float llo[3], lhi[3], rlo[3], rhi[3];
+        padded(l.box, llo, lhi);
+        padded(r.box, rlo, rhi);
+        psy::BvhNodeGpu &n = nodes[size_t(index)];
+        n.x = make_float4(llo[0], lhi[0], rlo[0], rhi[0]);
+        n.y = make_float4(llo[1], lhi[1], rlo[1], rhi[1]);
+        n.z = make_float4(llo[2], lhi[2], rlo[2], rhi[2]);
+        n.child = make_int4(l.link, r.link, l.count, r.count);
+    }
+
+    // Root node: a single leaf still gets a two-child root (empty right).
+    Box build_root() {
+        nodes.clear();
+        Box box;
+        for (const auto &p : prims) box.grow(p.box);
+        if (prims.empty()) {
+            nodes.push_back({});
+            write(0, Child{Box{}, ~0, 0}, Child{Box{}, ~0, 0});
+            return box;
+        }
+        if (prims.size() <= leaf_size && !leaf_is_id) {
+            nodes.push_back({});
+            write(0, leaf(0u, uint32_t(prims.size()), box), Child{Box{}, ~0, 0});
+            return box;
+        }
+        if (prims.size() == 1u) {
+            nodes.push_back({});
+            write(0, leaf(0u, 1u, box), Child{Box{}, ~0, 0});
+            return box;
+        }
+        const Child root = build(0u, uint32_t(prims.size()), 0);
+        (void)root;
+        return box;
+    }
+};
+
+// ------------------------------------------------------------ device memory
+
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    ~DeviceBuffer() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        release();
+        bytes = n;
+        if (n == 0) return cudaSuccess;
+        return cudaMalloc(&ptr, n);
+    }
+    template <typename T>
+    cudaError_t upload(const std::vector<T> &v, cudaStream_t st) {
+        cudaError_t e = alloc(std::max<size_t>(v.size() * sizeof(T), 16));
+        if (e != cudaSuccess || v.empty()) return e;
+        return cudaMemcpyAsync(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+    }
+    template <typename T>
+    T *as() const {
+        return static_cast<T *>(ptr);
+    }
+};
+
+}  // namespace
+
+// ----------------------------------------------------------------- objects
+
+struct psy_context {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+};
+
+struct psy_scene {
+    psy_context *context = nullptr;
+    uint64_t revision = 0;
+    psy_camera_desc camera{};
+    std::vector<psy::MaterialGpu> materials;
+    std::vector<float> scalars, vectors;
+    DeviceBuffer tlas, blas, tris, instances, meshes, positions, normals, indices, tri_materials, material_buf, code,
+        scalar_buf, vector_buf, emitters, distribution, lights;
+    psy::SceneView view{};
+    uint64_t triangle_count = 0;
+    double build_ms = 0.0;
+};
+
+struct psy_session {
+    psy_scene *scene = nullptr;
+    psy_render_settings settings{};
+    psy::RenderParams params{};
+    uint32_t pixels = 0;
+    uint32_t total = 0;
+    uint32_t sobol_size = 0;
+    uint32_t rendered = 0;
+    std::atomic<bool> cancelled{false};
+    DeviceBuffer sobol, filter, combined, normal, albedo, sample_count;
+    // path state
+    uint32_t capacity = 0;
+    DeviceBuffer ray_o, ray_d, tp, rad, st, st2, sample, aov_n, aov_a, hit, hit_prim, sh_o, sh_d, sh_c, sh_ids,
+        sh_path, qa, qb, sq, counters, stats;
+    psy::PathBuffers paths{};
+    // trace
+    DeviceBuffer trace_buf;
+    bool trace_requested = false;
+    uint32_t trace_x = 0, trace_y = 0, trace_sample = 0;
+    psy_path_trace trace_host{};
+    psy_render_stats last_stats{};
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+};
+
+namespace {
+
+psy_status derive_params(psy_session *s, const psy_render_settings &r) {
+    if (r.full_width == 0u || r.full_height == 0u)
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "render extent must be non-empty");
+    const uint32_t ww = r.window_width ? r.window_width : r.full_width;
+    const uint32_t wh = r.window_height ? r.window_height : r.full_height;
+    if (uint64_t(r.window_x) + ww > r.full_width || uint64_t(r.window_y) + wh > r.full_height)
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "render window lies outside the full extent");
+    if (r.transparent_max_bounces > 255u || r.max_bounces > 250u || r.diffuse_bounces > 250u ||
+        r.glossy_bounces > 250u || r.transmission_bounces > 250u)
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "bounce limits above 250 are not supported");
+    if (r.direct_light_sampling > PSY_DIRECT_LIGHT_NEE)
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "unknown direct light sampling mode");
+    if (r.use_light_tree) return fail(PSY_ERROR_UNSUPPORTED, "light-tree sampling is not available in this build");
+    psy::RenderParams &p = s->params;
+    p.full_w = r.full_width;
+    p.full_h = r.full_height;
+    p.win_x = r.window_x;
+    p.win_y = r.window_y;
+    p.win_w = ww;
+    p.win_h = wh;
+    p.seed = r.seed;
+    p.transparent_background = r.transparent_background;
+    p.pass_alpha_threshold = r.pass_alpha_threshold;
+    // cycles_kernel_bounce_limits (src/luisa/cycles_integrator_limits.h:62-85)
+    p.maximum = r.max_bounces + 1u;
+    p.minimum = r.min_bounces + 1u;
+    p.max_diffuse = r.diffuse_bounces + 1u;
+    p.max_glossy = r.glossy_bounces + 1u;
+    p.max_transmission = r.transmission_bounces + 1u;
+    p.transparent_min = r.transparent_min_bounces + 1u;
+    p.transparent_max = r.transparent_max_bounces;
+    p.steps = std::min<uint32_t>(2u * p.maximum + std::max(p.transparent_max, 1u) + 1u, 1024u);
+    p.clamp_direct = r.sample_clamp_direct;
+    p.clamp_indirect = r.sample_clamp_indirect;
+    p.inv_rr_threshold = (!r.use_light_tree && r.light_sampling_threshold > 0.0f)
+                             ? r.film_exposure / r.light_sampling_threshold : 0.0f;
+    p.direct_mode = r.direct_light_sampling;
+    p.nee = r.next_event_estimation;
+    // camera parameters (src/luisa/path_tracer_kernel.cpp:225-280)
+    const psy_camera_desc &c = s->scene->camera;
+    const float aspect = static_cast<float>(std::max(r.full_width, 1u)) / static_cast<float>(std::max(r.full_height, 1u));
+    const bool hfit = c.sensor_fit == 1u || (c.sensor_fit == 0u && aspect >= 1.0f);
+    p.vtan = hfit ? std::tan(c.horizontal_field_of_view * 0.5f) / aspect : std::tan(c.field_of_view * 0.5f);
+    p.htan = p.vtan * aspect;
+    p.shift_x = c.lens_shift_x * (hfit ? 1.0f : 1.0f / aspect);
+    p.shift_y = c.lens_shift_y * (hfit ? aspect : 1.0f);
+    p.near_clip = c.near_clip;
+    p.far_clip = c.far_clip;
+    store34(p.cam, m34(c.camera_to_world));
+    s->pixels = ww * wh;
+    return PSY_OK;
+}
+
+psy_status ensure_capacity(psy_session *s, uint32_t n) {
+    if (s->capacity >= n) return PSY_OK;
+    const size_t f4 = sizeof(float4) * size_t(n), u4 = sizeof(uint4) * size_t(n), u1 = sizeof(uint32_t) * size_t(n);
+    PSY_CUDA_TRY(s->ray_o.alloc(f4));
+    PSY_CUDA_TRY(s->ray_d.alloc(f4));
+    PSY_CUDA_TRY(s->tp.alloc(f4));
+    PSY_CUDA_TRY(s->rad.alloc(f4));
+    PSY_CUDA_TRY(s->st.alloc(u4));
+    PSY_CUDA_TRY(s->st2.alloc(u4));
+    PSY_CUDA_TRY(s->sample.alloc(u1));
+    PSY_CUDA_TRY(s->aov_n.alloc(f4));
+    PSY_CUDA_TRY(s->aov_a.alloc(f4));
+    PSY_CUDA_TRY(s->hit.alloc(f4));
+    PSY_CUDA_TRY(s->hit_prim.alloc(u1));
+    PSY_CUDA_TRY(s->sh_o.alloc(f4));
+    PSY_CUDA_TRY(s->sh_d.alloc(f4));
+    PSY_CUDA_TRY(s->sh_c.alloc(f4));
+    PSY_CUDA_TRY(s->sh_ids.alloc(u4));
+    PSY_CUDA_TRY(s->sh_path.alloc(u1));
+    PSY_CUDA_TRY(s->qa.alloc(u1));
+    PSY_CUDA_TRY(s->qb.alloc(u1));
+    PSY_CUDA_TRY(s->sq.alloc(u1));
+    if (!s->counters.ptr) PSY_CUDA_TRY(s->counters.alloc(64));
+    if (!s->stats.ptr) PSY_CUDA_TRY(s->stats.alloc(64));
+    s->capacity = n;
+    psy::PathBuffers &b = s->paths;
+    b.ray_o = s->ray_o.as<float4>();
+    b.ray_d = s->ray_d.as<float4>();
+    b.tp = s->tp.as<float4>();
+    b.rad = s->rad.as<float4>();
+    b.st = s->st.as<uint4>();
+    b.st2 = s->st2.as<uint4>();
+    b.sample = s->sample.as<uint32_t>();
+    b.aov_n = s->aov_n.as<float4>();
+    b.aov_a = s->aov_a.as<float4>();
+    b.hit = s->hit.as<float4>();
+    b.hit_prim = s->hit_prim.as<uint32_t>();
+    b.sh_o = s->sh_o.as<float4>();
+    b.sh_d = s->sh_d.as<float4>();
+    b.sh_c = s->sh_c.as<float4>();
+    b.sh_ids = s->sh_ids.as<uint4>();
+    b.sh_path = s->sh_path.as<uint32_t>();
+    b.queue_in = s->qa.as<uint32_t>();
+    b.queue_out = s->qb.as<uint32_t>();
+    b.shadow_queue = s->sq.as<uint32_t>();
+    b.counters = s->counters.as<uint32_t>();
+    return PSY_OK;
+}
+
+psy_status clear_film(psy_session *s) {
+    cudaStream_t st = s->scene->context->stream;
+    const size_t n = s->pixels;
+    PSY_CUDA_TRY(s->combined.alloc(sizeof(float4) * n));
+    PSY_CUDA_TRY(s->normal.alloc(sizeof(float4) * n));
+    PSY_CUDA_TRY(s->albedo.alloc(sizeof(float4) * n));
+    PSY_CUDA_TRY(s->sample_count.alloc(sizeof(uint32_t) * n));
+    PSY_CUDA_TRY(cudaMemsetAsync(s->combined.ptr, 0, sizeof(float4) * n, st));
+    PSY_CUDA_TRY(cudaMemsetAsync(s->normal.ptr, 0, sizeof(float4) * n, st));
+    PSY_CUDA_TRY(cudaMemsetAsync(s->albedo.ptr, 0, sizeof(float4) * n, st));
+    PSY_CUDA_TRY(cudaMemsetAsync(s->sample_count.ptr, 0, sizeof(uint32_t) * n, st));
+    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    s->rendered = 0;
+    s->total = 0;
+    return PSY_OK;
+}
+
+constexpr uint32_t kDefaultCapacity = 1u << 22;  // 4M paths = 392 MB of state
+
+}  // namespace
+
+// ================================================================== C ABI
+
+extern "C" {
+
+const char *psy_last_error(void) { return g_last_error.c_str(); }
+uint32_t psy_abi_version(void) { return PSY_ABI_VERSION; }
+
+void psy_render_settings_default(psy_render_settings *r) {
+    if (!r) return;
+    std::memset(r, 0, sizeof(*r));
+    r->filter_width = 1.0f;
+    r->pass_alpha_threshold = 0.5f;
+    r->max_bounces = 12u;
+    r->diffuse_bounces = 4u;
+    r->glossy_bounces = 4u;
+    r->transmission_bounces = 12u;
+    r->transparent_max_bounces = 8u;
+    r->film_exposure = 1.0f;
+    r->light_sampling_threshold = 0.01f;
+    r->direct_light_sampling = PSY_DIRECT_LIGHT_MIS;
+    r->next_event_estimation = 1u;
+}
+
+uint32_t psy_sobol_sequence_size_for_samples(uint32_t samples) {
+    const uint32_t c = std::clamp(samples, 1u, 8192u);
+    uint32_t u = 1u;
+    if (c != 1u) u = 1u << (32u - static_cast<uint32_t>(__builtin_clz(c - 1u)));
+    return std::clamp(u, 256u, 8192u);
+}
+
+psy_status psy_sobol_generate_table(uint32_t size, float *out) {
+    if (!out) return fail(PSY_ERROR_INVALID_ARGUMENT, "null output");
+    if (!sobol_size_valid(size))
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "tabulated Sobol sequence size must be a power of two between 256 and 8192");
+    for (uint32_t pattern = 0; pattern < 256u; ++pattern) sobol_pattern(out + size_t(pattern) * size * 4u, size, pattern);
+    return PSY_OK;
+}
+
+psy_status psy_pixel_filter_table(uint32_t filter, float width, float *out) {
+    if (!out) return fail(PSY_ERROR_INVALID_ARGUMENT, "null output");
+    if (filter > PSY_FILTER_BLACKMAN_HARRIS) return fail(PSY_ERROR_INVALID_ARGUMENT, "unknown pixel filter");
+    const auto t = filter_table(filter, width);
+    std::memcpy(out, t.data(), sizeof(float) * t.size());
+    return PSY_OK;
+}
+
+psy_status psy_context_create(int device, psy_context **out) {
+    if (!out) return fail(PSY_ERROR_INVALID_ARGUMENT, "null output");
+    *out = nullptr;
+    int count = 0;
+    PSY_CUDA_TRY(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return fail(PSY_ERROR_INVALID_ARGUMENT, "no such CUDA device");
+    PSY_CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop{};
+    PSY_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) return fail(PSY_ERROR_UNSUPPORTED, "libpsycles_cuda is built for sm_100a (B200)");
+    auto c = std::make_unique<psy_context>();
+    c->device = device;
+    c->sms = prop.multiProcessorCount;
+    PSY_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    *out = c.release();
+    return PSY_OK;
+}
+
+void psy_context_destroy(psy_context *c) {
+    if (!c) return;
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scene **out) {
+    if (!ctx || !d || !out) return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    const auto t_begin = std::chrono::steady_clock::now();
+    PSY_CUDA_TRY(cudaSetDevice(ctx->device));
+    // ---- validation (SceneDatabase commits only valid snapshots)
+    for (uint32_t i = 0; i < d->instance_count; ++i) {
+        if (d->instances[i].mesh >= d->mesh_count) return fail(PSY_ERROR_INVALID_ARGUMENT, "instance mesh out of range");
+        if (d->instances[i].material >= d->material_count)
+            return fail(PSY_ERROR_INVALID_ARGUMENT, "instance material out of range");
+    }
+    for (uint32_t i = 0; i < d->mesh_count; ++i) {
+        const psy_mesh_desc &m = d->meshes[i];
+        if (m.triangle_count && (!m.indices || !m.positions))
+            return fail(PSY_ERROR_INVALID_ARGUMENT, "mesh without indices or positions");
+        for (uint64_t k = 0; k < 3ull * m.triangle_count; ++k)
+            if (m.indices[k] >= m.vertex_count) return fail(PSY_ERROR_INVALID_ARGUMENT, "mesh index out of range");
+        if (m.materials)
+            for (uint32_t k = 0; k < m.triangle_count; ++k)
+                if (m.materials[k] >= d->material_count)
+                    return fail(PSY_ERROR_INVALID_ARGUMENT, "triangle material out of range");
+        if (m.smooth && !m.normals) return fail(PSY_ERROR_INVALID_ARGUMENT, "smooth mesh without normals");
+    }
+    for (uint32_t i = 0; i < d->material_count; ++i) {
+        const psy_material_desc &m = d->materials[i];
+        if (m.closure_count == 0u || !m.closures || m.root >= m.closure_count)
+            return fail(PSY_ERROR_INVALID_ARGUMENT, "material without a valid closure root");
+        for (uint32_t k = 0; k < m.closure_count; ++k) {
+            const psy_closure_instruction &c = m.closures[k];
+            if (c.op > PSY_CLOSURE_MIX) return fail(PSY_ERROR_UNSUPPORTED, "closure operation outside the supported set");
+            if ((c.op == PSY_CLOSURE_ADD || c.op == PSY_CLOSURE_MIX) && (c.a >= m.closure_count || c.b >= m.closure_count))
+                return fail(PSY_ERROR_INVALID_ARGUMENT, "closure child out of range");
+            if ((c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_TRANSPARENT) &&
+                c.color >= m.vector_count)
+                return fail(PSY_ERROR_INVALID_ARGUMENT, "closure colour slot out of range");
+            if ((c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_MIX) && c.scalar >= m.scalar_count)
+                return fail(PSY_ERROR_INVALID_ARGUMENT, "closure scalar slot out of range");
+        }
+    }
+    for (uint32_t i = 0; i < d->light_count; ++i) {
+        const psy_light_desc &l = d->lights[i];
+        if (l.type == PSY_LIGHT_AREA) return fail(PSY_ERROR_UNSUPPORTED, "area lights are not available in this build");
+        if (l.type > PSY_LIGHT_DISTANT) return fail(PSY_ERROR_INVALID_ARGUMENT, "unknown light type");
+        if ((l.flags & PSY_LIGHT_FLAG_SPHERE) && l.radius > 0.0f)
+            return fail(PSY_ERROR_UNSUPPORTED, "spherical point lights are not available in this build");
+    }
+    auto sc = std::make_unique<psy_scene>();
+    sc->context = ctx;
+    sc->revision = d->revision;
+    sc->camera = d->camera;
+    cudaStream_t st = ctx->stream;
+
+    // ---- meshes: flatten, BLAS per mesh
+    std::vector<psy::MeshGpu> meshes(d->mesh_count);
+    std::vector<float> positions, normals;
+    std::vector<uint32_t> indices, tri_materials;
+    std::vector<psy::BvhNodeGpu> blas;
+    std::vector<float4> tris;
+    std::vector<Box> mesh_boxes(d->mesh_count);
+    uint32_t prim_offset = 0;
+    for (uint32_t i = 0; i < d->mesh_count; ++i) {
+        const psy_mesh_desc &m = d->meshes[i];
+        psy::MeshGpu &g = meshes[i];
+        g.vertex_offset = uint32_t(positions.size() / 3u);
+        g.index_offset = uint32_t(indices.size());
+        g.triangle_count = m.triangle_count;
+        g.prim_offset = prim_offset;
+        g.smooth = m.smooth ? 1u : 0u;
+        prim_offset += m.triangle_count;
+        positions.insert(positions.end(), m.positions, m.positions + 3ull * m.vertex_count);
+        if (m.smooth) normals.insert(normals.end(), m.normals, m.normals + 3ull * m.vertex_count);
+        else normals.resize(positions.size(), 0.0f);
+        indices.insert(indices.end(), m.indices, m.indices + 3ull * m.triangle_count);
+        if (m.materials) {
+            g.material_offset = uint32_t(tri_materials.size());
+            tri_materials.insert(tri_materials.end(), m.materials, m.materials + m.triangle_count);
+        } else {
+            g.material_offset = psy::kInvalidId;
+        }
+        Builder bld;
+        bld.prims.resize(m.triangle_count);
+        for (uint32_t k = 0; k < m.triangle_count; ++k) {
+            Prim &p = bld.prims[k];
+            for (int c = 0; c < 3; ++c) {
+                const float *v = m.positions + 3ull * m.indices[3ull * k + c];
+                p.box.grow(v[0], v[1], v[2]);
+            }
+            for (int a = 0; a < 3; ++a) p.c[a] = 0.5 * (p.box.lo[a] + p.box.hi[a]);
+            p.id = k;
+        }
+        mesh_boxes[i] = bld.build_root();
+        g.node_offset = uint32_t(blas.size());
+        g.tri_offset = uint32_t(tris.size() / 3u);
+        blas.insert(blas.end(), bld.nodes.begin(), bld.nodes.end());
+        for (const Prim &p : bld.prims) {
+            for (int c = 0; c < 3; ++c) {
+                const float *v = m.positions + 3ull * m.indices[3ull * p.id + c];
+                float w = 0.0f;
+                if (c == 0) std::memcpy(&w, &p.id, 4);
+                tris.push_back(make_float4(v[0], v[1], v[2], w));
+            }
+        }
+        sc->triangle_count += m.triangle_count;
+    }
+    if (blas.empty()) blas.push_back({});
+
+    // ---- instances + TLAS
+    std::vector<psy::InstanceGpu> instances(d->instance_count);
+    Builder tl;
+    tl.leaf_size = 1u;
+    tl.leaf_is_id = true;
+    std::vector<M34> o2w(d->instance_count);
+    for (uint32_t i = 0; i < d->instance_count; ++i) {
+        const psy_instance_desc &id = d->instances[i];
+        psy::InstanceGpu &g = instances[i];
+        o2w[i] = m34(id.object_to_world);
+        const M34 w2o = inverse34(o2w[i]);
+        M34 nrm;
+        nrm.c0 = {w2o.c0.x, w2o.c1.x, w2o.c2.x};
+        nrm.c1 = {w2o.c0.y, w2o.c1.y, w2o.c2.y};
+        nrm.c2 = {w2o.c0.z, w2o.c1.z, w2o.c2.z};
+        nrm.c3 = {0.0f, 0.0f, 0.0f};
+        store34(g.o2w, o2w[i]);
+        store34(g.w2o, w2o);
+        store34(g.nrm, nrm);
+        g.mesh = id.mesh;
+        g.material = id.material;
+        g.visibility = id.visibility;
+        const Box &mb = mesh_boxes[id.mesh];
+        if (mb.empty()) continue;
+        Prim p;
+        for (int corner = 0; corner < 8; ++corner) {
+            const double x = (corner & 1) ? mb.hi[0] : mb.lo[0];
+            const double y = (corner & 2) ? mb.hi[1] : mb.lo[1];
+            const double z = (corner & 4) ? mb.hi[2] : mb.lo[2];
+            const M34 &m = o2w[i];
+            const double wx = x * m.c0.x + y * m.c1.x + z * m.c2.x + m.c3.x;
+            const double wy = x * m.c0.y + y * m.c1.y + z * m.c2.y + m.c3.y;
+            const double wz = x * m.c0.z + y * m.c1.z + z * m.c2.z + m.c3.z;
+            p.box.grow(wx, wy, wz);
+        }
+        // relative widening for the float transform of the ray
+        for (int a = 0; a < 3; ++a) {
+            const double pad = 1e-5 * (p.box.hi[a] - p.box.lo[a]) + 1e-6 * std::max(std::fabs(p.box.lo[a]), std::fabs(p.box.hi[a]));
+            p.box.lo[a] -= pad;
+            p.box.hi[a] += pad;
+            p.c[a] = 0.5 * (p.box.lo[a] + p.box.hi[a]);
+        }
+        p.id = i;
+        tl.prims.push_back(p);
+    }
+    tl.build_root();
+
+    // ---- materials and parameter blocks
+    std::vector<psy_closure_instruction> code;
+    bool any_transparent = false;
+    for (uint32_t i = 0; i < d->material_count; ++i) {
+        const psy_material_desc &m = d->materials[i];
+        psy::MaterialGpu g{};
+        g.code_offset = uint32_t(code.size());
+        g.code_count = m.closure_count;
+        g.root = m.root;
+        g.scalar_offset = uint32_t(sc->scalars.size());
+        g.vector_offset = uint32_t(sc->vectors.size() / 3u);
+        g.emission_sampling = m.emission_sampling;
+        for (uint32_t k = 0; k < m.closure_count; ++k) {
+            if (m.closures[k].op == PSY_CLOSURE_EMISSION) g.has_emission = 1u;
+            if (m.closures[k].op == PSY_CLOSURE_TRANSPARENT) g.has_transparent = 1u;
+        }
+        any_transparent = any_transparent || g.has_transparent;
+        code.insert(code.end(), m.closures, m.closures + m.closure_count);
+        sc->scalars.insert(sc->scalars.end(), m.scalars, m.scalars + m.scalar_count);
+        sc->vectors.insert(sc->vectors.end(), m.vectors, m.vectors + 3ull * m.vector_count);
+        sc->materials.push_back(g);
+    }
+
+    // ---- emissive triangles + flat light distribution
+    // (src/sampling/light_distribution.cpp:25-150; emitter geometry as in
+    // src/luisa/path_kernel_emissive_triangle.cpp:80-150)
+    std::vector<psy::EmitterGpu> emitters;
+    std::vector<float> areas;
+    for (uint32_t i = 0; i < d->instance_count; ++i) {
+        const psy_instance_desc &id = d->instances[i];
+        const psy_mesh_desc &m = d->meshes[id.mesh];
+        const psy::InstanceGpu &g = instances[i];
+        M34 nrm;
+        nrm.c0 = {g.nrm[0], g.nrm[1], g.nrm[2]};
+        nrm.c1 = {g.nrm[3], g.nrm[4], g.nrm[5]};
+        nrm.c2 = {g.nrm[6], g.nrm[7], g.nrm[8]};
+        nrm.c3 = {0, 0, 0};
+        for (uint32_t k = 0; k < m.triangle_count; ++k) {
+            const uint32_t mi = m.materials ? m.materials[k] : id.material;
+            const psy::MaterialGpu &mat = sc->materials[mi];
+            if (!mat.has_emission || mat.emission_sampling == 0u) continue;
+            auto vert = [&](int c) {
+                const float *v = m.positions + 3ull * m.indices[3ull * k + c];
+                return v3(v[0], v[1], v[2]);
+            };
+            const V3 l0 = vert(0), l1 = vert(1), l2 = vert(2);
+            const V3 p0 = xaff(o2w[i], l0, true), p1 = xaff(o2w[i], l1, true), p2 = xaff(o2w[i], l2, true);
+            V3 ln = crs(sub(l1, l0), sub(l2, l0));
+            const float l2n = dt(ln, ln);
+            ln = l2n > 1.0e-20f ? V3{ln.x / std::sqrt(std::max(l2n, 1.0e-20f)), ln.y / std::sqrt(std::max(l2n, 1.0e-20f)),
+                                     ln.z / std::sqrt(std::max(l2n, 1.0e-20f))}
+                                : v3(0.0f, 0.0f, 1.0f);
+            V3 ng = xaff(nrm, ln, false);
+            const float g2 = dt(ng, ng);
+            ng = g2 > 1.0e-20f ? V3{ng.x / std::sqrt(std::max(g2, 1.0e-20f)), ng.y / std::sqrt(std::max(g2, 1.0e-20f)),
+                                    ng.z / std::sqrt(std::max(g2, 1.0e-20f))}
+                               : v3(0.0f, 0.0f, 1.0f);
+            const V3 cr = crs(sub(p1, p0), sub(p2, p0));
+            psy::EmitterGpu e{};
+            e.p0[0] = p0.x; e.p0[1] = p0.y; e.p0[2] = p0.z;
+            e.p1[0] = p1.x; e.p1[1] = p1.y; e.p1[2] = p1.z;
+            e.p2[0] = p2.x; e.p2[1] = p2.y; e.p2[2] = p2.z;
+            e.ng[0] = ng.x; e.ng[1] = ng.y; e.ng[2] = ng.z;
+            e.area = 0.5f * std::sqrt(dt(cr, cr));
+            e.material = mi;
+            e.object = i;
+            e.cycles_prim = meshes[id.mesh].prim_offset + k;
+            e.emission_sampling = mat.emission_sampling;
+            emitters.push_back(e);
+            areas.push_back(e.area);
+        }
+    }
+    std::vector<psy::DistEntryGpu> dist;
+    const uint32_t tri_n = uint32_t(areas.size()), light_n = d->light_count;
+    auto valid_area = [](float a) { return std::isfinite(a) && a > 0.0f ? a : 0.0f; };
+    float total = 0.0f;
+    for (uint32_t i = 0; i < tri_n; ++i) {
+        dist.push_back({total, 0.0f, 0u, i});
+        total += valid_area(areas[i]);
+    }
+    const float triangle_area = total;
+    const float light_area = light_n > 0u ? (total > 0.0f ? total / float(light_n) : 1.0f) : 0.0f;
+    for (uint32_t i = 0; i < light_n; ++i) {
+        dist.push_back({total, 0.0f, 1u, i});
+        total += light_area;
+    }
+    dist.push_back({total, 0.0f, 3u, 0u});
+    float triangle_area_pdf = 0.0f, light_selection_pdf = 0.0f;
+    if (triangle_area > 0.0f) {
+        triangle_area_pdf = 1.0f / triangle_area;
+        if (light_n > 0u) triangle_area_pdf *= 0.5f;
+    }
+    if (light_n > 0u) {
+        light_selection_pdf = 1.0f / float(light_n);
+        if (triangle_area > 0.0f) light_selection_pdf *= 0.5f;
+    }
+    for (uint32_t i = 0; i < tri_n; ++i) dist[i].selection_pdf = valid_area(areas[i]) * triangle_area_pdf;
+    for (uint32_t i = tri_n; i < tri_n + light_n; ++i) dist[i].selection_pdf = light_selection_pdf;
+    if (total > 0.0f) {
+        const float inv = 1.0f / total;
+        for (uint32_t i = 0; i < tri_n + light_n; ++i) dist[i].cumulative *= inv;
+        dist.back().cumulative = 1.0f;
+    }
+    std::vector<psy_light_desc> lights(d->lights, d->lights + d->light_count);
+
+    // ---- upload
+    PSY_CUDA_TRY(sc->tlas.upload(tl.nodes, st));
+    PSY_CUDA_TRY(sc->blas.upload(blas, st));
+    PSY_CUDA_TRY(sc->tris.upload(tris, st));
+    PSY_CUDA_TRY(sc->instances.upload(instances, st));
+    PSY_CUDA_TRY(sc->meshes.upload(meshes, st));
+    PSY_CUDA_TRY(sc->positions.upload(positions, st));
+    PSY_CUDA_TRY(sc->normals.upload(normals, st));
+    PSY_CUDA_TRY(sc->indices.upload(indices, st));
+    PSY_CUDA_TRY(sc->tri_materials.upload(tri_materials, st));
+    PSY_CUDA_TRY(sc->material_buf.upload(sc->materials, st));
+    PSY_CUDA_TRY(sc->code.upload(code, st));
+    PSY_CUDA_TRY(sc->scalar_buf.upload(sc->scalars, st));
+    PSY_CUDA_TRY(sc->vector_buf.upload(sc->vectors, st));
+    PSY_CUDA_TRY(sc->emitters.upload(emitters, st));
+    PSY_CUDA_TRY(sc->distribution.upload(dist, st));
+    PSY_CUDA_TRY(sc->lights.upload(lights, st));
+    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    psy::SceneView &v = sc->view;
+    v.tlas = sc->tlas.as<psy::BvhNodeGpu>();
+    v.blas = sc->blas.as<psy::BvhNodeGpu>();
+    v.tris = sc->tris.as<float4>();
+    v.instances = sc->instances.as<psy::InstanceGpu>();
+    v.meshes = sc->meshes.as<psy::MeshGpu>();
+    v.positions = sc->positions.as<float>();
+    v.normals = sc->normals.as<float>();
+    v.indices = sc->indices.as<uint32_t>();
+    v.tri_materials = sc->tri_materials.as<uint32_t>();
+    v.materials = sc->material_buf.as<psy::MaterialGpu>();
+    v.code = sc->code.as<psy_closure_instruction>();
+    v.scalars = sc->scalar_buf.as<float>();
+    v.vectors = sc->vector_buf.as<float>();
+    v.emitters = sc->emitters.as<psy::EmitterGpu>();
+    v.distribution = sc->distribution.as<psy::DistEntryGpu>();
+    v.lights = sc->lights.as<psy_light_desc>();
+    v.instance_count = tl.prims.empty() ? 0u : d->instance_count;
+    v.emitter_count = tri_n + light_n;
+    v.triangle_emitters = tri_n;
+    v.light_count = light_n;
+    v.triangle_area_pdf = triangle_area_pdf;
+    v.background[0] = d->background[0];
+    v.background[1] = d->background[1];
+    v.background[2] = d->background[2];
+    v.world_visibility = d->world_visibility;
+    v.any_transparent = any_transparent ? 1u : 0u;
+    sc->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
+    *out = sc.release();
+    return PSY_OK;
+}
+
+void psy_scene_destroy(psy_scene *s) {
+    if (!s) return;
+    cudaSetDevice(s->context->device);
+    delete s;
+}
+
+uint64_t psy_scene_source_revision(const psy_scene *s) { return s ? s->revision : 0u; }
+
+psy_status psy_scene_rebind_parameters(psy_scene *s, uint32_t material, const float *scalars, uint32_t scalar_count,
+                                       const float *vectors, uint32_t vector_count) {
+    if (!s) return fail(PSY_ERROR_INVALID_ARGUMENT, "null scene");
+    if (material >= s->materials.size()) return fail(PSY_ERROR_INVALID_ARGUMENT, "material out of range");
+    const psy::MaterialGpu &m = s->materials[material];
+    const uint32_t next_scalar =
+        material + 1 < s->materials.size() ? s->materials[material + 1].scalar_offset : uint32_t(s->scalars.size());
+    const uint32_t next_vector = material + 1 < s->materials.size() ? s->materials[material + 1].vector_offset
+                                                                    : uint32_t(s->vectors.size() / 3u);
+    if (scalar_count != next_scalar - m.scalar_offset || vector_count != next_vector - m.vector_offset)
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "parameter block layout differs from the compiled program");
+    if ((scalar_count && !scalars) || (vector_count && !vectors)) return fail(PSY_ERROR_INVALID_ARGUMENT, "null parameters");
+    cudaStream_t st = s->context->stream;
+    PSY_CUDA_TRY(cudaSetDevice(s->context->device));
+    if (scalar_count) {
+        std::memcpy(s->scalars.data() + m.scalar_offset, scalars, sizeof(float) * scalar_count);
+        PSY_CUDA_TRY(cudaMemcpyAsync(s->scalar_buf.as<float>() + m.scalar_offset, scalars, sizeof(float) * scalar_count,
+                                     cudaMemcpyHostToDevice, st));
+    }
+    if (vector_count) {
+        std::memcpy(s->vectors.data() + 3ull * m.vector_offset, vectors, sizeof(float) * 3u * vector_count);
+        PSY_CUDA_TRY(cudaMemcpyAsync(s->vector_buf.as<float>() + 3ull * m.vector_offset, vectors,
+                                     sizeof(float) * 3u * vector_count, cudaMemcpyHostToDevice, st));
+    }
+    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    return PSY_OK;
+}
+
+psy_status psy_session_create(psy_scene *scene, const psy_render_settings *settings, psy_session **out) {
+    if (!scene || !settings || !out) return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    PSY_CUDA_TRY(cudaSetDevice(scene->context->device));
+    auto s = std::make_unique<psy_session>();
+    s->scene = scene;
+    s->settings = *settings;
+    psy_status r = derive_params(s.get(), *settings);
+    if (r != PSY_OK) return r;
+    const auto table = filter_table(settings->pixel_filter, settings->filter_width);
+    std::vector<float> tv(table.begin(), table.end());
+    PSY_CUDA_TRY(s->filter.upload(tv, scene->context->stream));
+    s->params.filter = s->filter.as<float>();
+    if ((r = clear_film(s.get())) != PSY_OK) return r;
+    PSY_CUDA_TRY(s->trace_buf.alloc(sizeof(psy_path_trace)));
+    PSY_CUDA_TRY(cudaEventCreate(&s->ev_begin));
+    PSY_CUDA_TRY(cudaEventCreate(&s->ev_end));
+    *out = s.release();
+    return PSY_OK;
+}
+
+void psy_session_destroy(psy_session *s) {
+    if (!s) return;
+    cudaSetDevice(s->scene->context->device);
+    if (s->ev_begin) cudaEventDestroy(s->ev_begin);
+    if (s->ev_end) cudaEventDestroy(s->ev_end);
+    delete s;
+}
+
+psy_status psy_session_reset(psy_session *s, const psy_render_settings *settings) {
+    if (!s || !settings) return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    PSY_CUDA_TRY(cudaSetDevice(s->scene->context->device));
+    s->settings = *settings;
+    psy_status r = derive_params(s, *settings);
+    if (r != PSY_OK) return r;
+    const auto table = filter_table(settings->pixel_filter, settings->filter_width);
+    std::vector<float> tv(table.begin(), table.end());
+    PSY_CUDA_TRY(s->filter.upload(tv, s->scene->context->stream));
+    s->params.filter = s->filter.as<float>();
+    s->cancelled.store(false);
+    return clear_film(s);
+}
+
+void psy_session_cancel(psy_session *s) {
+    if (s) s->cancelled.store(true);
+}
+
+uint32_t psy_session_rendered_samples(const psy_session *s) { return s ? s->rendered : 0u; }
+
+psy_status psy_session_request_trace(psy_session *s, uint32_t x, uint32_t y, uint32_t sample) {
+    if (!s) return fail(PSY_ERROR_INVALID_ARGUMENT, "null session");
+    if (x >= s->params.full_w || y >= s->params.full_h) return fail(PSY_ERROR_INVALID_ARGUMENT, "trace pixel outside the film");
+    s->trace_requested = true;
+    s->trace_x = x;
+    s->trace_y = y;
+    s->trace_sample = sample;
+    std::memset(&s->trace_host, 0, sizeof(s->trace_host));
+    PSY_CUDA_TRY(cudaMemset(s->trace_buf.ptr, 0, sizeof(psy_path_trace)));
+    return PSY_OK;
+}
+
+psy_status psy_session_read_trace(psy_session *s, psy_path_trace *out) {
+    if (!s || !out) return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = s->trace_host;
+    return PSY_OK;
+}
+
+psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t count, uint32_t offset, uint32_t total) {
+    if (!s) return fail(PSY_ERROR_INVALID_ARGUMENT, "null session");
+    if (s->cancelled.load()) return fail(PSY_ERROR_CANCELLED, "session cancelled");
+    if (count == 0u) return fail(PSY_ERROR_RANGE, "empty sample range");
+    const uint64_t begin = uint64_t(first) + offset, end = begin + count;
+    if (total == 0u || end > total) return fail(PSY_ERROR_RANGE, "sample range beyond the render's total");
+    if (s->total != 0u && s->total != total) return fail(PSY_ERROR_STATE, "total sample count changed within the session");
+    psy_context *ctx = s->scene->context;
+    cudaStream_t st = ctx->stream;
+    PSY_CUDA_TRY(cudaSetDevice(ctx->device));
+    // Sobol table sized from the render's total (path_tracer_session.cpp:41-69)
+    const uint32_t size = psy_sobol_sequence_size_for_samples(total);
+    if (s->sobol_size != size) {
+        std::vector<float> table(size_t(size) * 256u * 4u);
+        psy_sobol_generate_table(size, table.data());
+        PSY_CUDA_TRY(s->sobol.upload(table, st));
+        s->sobol_size = size;
+    }
+    s->total = total;
+    psy::RenderParams p = s->params;
+    p.sobol = s->sobol.as<float4>();
+    p.sobol_size = s->sobol_size;
+    const uint32_t pixels = s->pixels;
+    uint32_t per_batch = std::max(1u, std::min(count, kDefaultCapacity / std::max(pixels, 1u)));
+    psy_status r = ensure_capacity(s, pixels * per_batch);
+    if (r != PSY_OK) return r;
+    psy_path_trace *trace = s->trace_requested ? s->trace_buf.as<psy_path_trace>() : nullptr;
+    PSY_CUDA_TRY(cudaMemsetAsync(s->stats.ptr, 0, 64, st));
+    psy_render_stats stats{};
+    PSY_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
+    const int sms = ctx->sms;
+    for (uint64_t sample = begin; sample < end;) {
+        if (s->cancelled.load()) return fail(PSY_ERROR_CANCELLED, "session cancelled");
+        const uint32_t n_samples = uint32_t(std::min<uint64_t>(per_batch, end - sample));
+        const uint32_t paths = pixels * n_samples;
+        uint32_t trace_path = psy::kInvalidId;
+        if (trace && s->trace_sample >= sample && s->trace_sample < sample + n_samples &&
+            s->trace_x >= p.win_x && s->trace_x < p.win_x + p.win_w && s->trace_y >= p.win_y &&
+            s->trace_y < p.win_y + p.win_h) {
+            const uint32_t local = (s->trace_y - p.win_y) * p.win_w + (s->trace_x - p.win_x);
+            trace_path = uint32_t(s->trace_sample - sample) * pixels + local;
+        }
+        psy::PathBuffers b = s->paths;
+        psy::launch_set_counters(st, b.counters, paths);
+        psy::launch_raygen(st, sms, p, b, pixels, paths, uint32_t(sample), trace_path, trace_path != psy::kInvalidId ? trace : nullptr);
+        stats.camera_rays += paths;
+        for (uint32_t step = 0; step < p.steps; ++step) {
+            psy::launch_intersect(st, sms, s->scene->view, b, paths);
+            psy::launch_shade(st, sms, s->scene->view, p, b, paths, step, trace_path, trace_path != psy::kInvalidId ? trace : nullptr);
+            psy::launch_count_rays(st, b.counters, s->stats.as<unsigned long long>());
+            psy::launch_shadow(st, sms, s->scene->view, p, b, paths, step, trace_path, trace_path != psy::kInvalidId ? trace : nullptr);
+            psy::launch_swap(st, b.counters);
+            std::swap(b.queue_in, b.queue_out);
+            stats.kernel_launches += 5u;
+            // every 4 steps, stop early once no path is left
+            if ((step & 3u) == 3u) {
+                uint32_t left = 0u;
+                PSY_CUDA_TRY(cudaMemcpyAsync(&left, b.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+                PSY_CUDA_TRY(cudaStreamSynchronize(st));
+                if (left == 0u) break;
+            }
+        }
+        psy::launch_film(st, sms, b, pixels, n_samples, s->combined.as<float4>(), s->normal.as<float4>(),
+                         s->albedo.as<float4>(), s->sample_count.as<uint32_t>(), trace_path,
+                         trace_path != psy::kInvalidId ? trace : nullptr);
+        stats.kernel_launches += 3u;
+        stats.batches += 1u;
+        sample += n_samples;
+    }
+    PSY_CUDA_TRY(cudaEventRecord(s->ev_end, st));
+    PSY_CUDA_TRY(cudaGetLastError());
+    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    float ms = 0.0f;
+    PSY_CUDA_TRY(cudaEventElapsedTime(&ms, s->ev_begin, s->ev_end));
+    unsigned long long counts[2] = {0, 0};
+    PSY_CUDA_TRY(cudaMemcpy(counts, s->stats.ptr, sizeof(counts), cudaMemcpyDeviceToHost));
+    stats.closest_rays = counts[0];
+    stats.path_segments = counts[0];
+    stats.shadow_rays = counts[1];
+    stats.ms_total = ms;
+    s->last_stats = stats;
+    s->rendered += count;
+    if (trace) {
+        PSY_CUDA_TRY(cudaMemcpy(&s->trace_host, trace, sizeof(psy_path_trace), cudaMemcpyDeviceToHost));
+    }
+    return PSY_OK;
+}
+
+psy_status psy_session_read_pass(psy_session *s, uint32_t pass_kind, float *out, uint64_t capacity, uint32_t *channels) {
+    if (!s || !out) return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    const uint64_t n = s->pixels;
+    const uint32_t ch = pass_kind == PSY_PASS_SAMPLE_COUNT ? 1u : 4u;
+    if (pass_kind != PSY_PASS_COMBINED && pass_kind != PSY_PASS_NORMAL && pass_kind != PSY_PASS_ALBEDO &&
+        pass_kind != PSY_PASS_DENOISING_NORMAL && pass_kind != PSY_PASS_DENOISING_ALBEDO &&
+        pass_kind != PSY_PASS_SAMPLE_COUNT)
+        return fail(PSY_ERROR_UNSUPPORTED, "pass kind not produced by this backend");
+    if (capacity < n * ch) return fail(PSY_ERROR_INVALID_ARGUMENT, "output buffer too small");
+    if (channels) *channels = ch;
+    PSY_CUDA_TRY(cudaSetDevice(s->scene->context->device));
+    std::vector<uint32_t> counts(n);
+    PSY_CUDA_TRY(cudaMemcpy(counts.data(), s->sample_count.ptr, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+    // write_passes fails when pixels disagree on the sample count
+    // (src/luisa/path_tracer_session.cpp:88-95)
+    for (uint64_t i = 0; i < n; ++i)
+        if (counts[i] != s->rendered) return fail(PSY_ERROR_STATE, "film sample counts disagree with the session");
+    if (pass_kind == PSY_PASS_SAMPLE_COUNT) {
+        for (uint64_t i = 0; i < n; ++i) out[i] = float(counts[i]);
+        return PSY_OK;
+    }
+    const void *src = pass_kind == PSY_PASS_COMBINED ? s->combined.ptr
+                      : (pass_kind == PSY_PASS_NORMAL || pass_kind == PSY_PASS_DENOISING_NORMAL) ? s->normal.ptr
+                                                                                                  : s->albedo.ptr;
+    PSY_CUDA_TRY(cudaMemcpy(out, src, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    const float exposure = s->settings.film_exposure;
+    for (uint64_t i = 0; i < n; ++i) {
+        const float den = float(std::max(counts[i], 1u));
+        float *v = out + 4 * i;
+        if (pass_kind == PSY_PASS_COMBINED) {
+            const float k = exposure / den;
+            v[0] *= k;
+            v[1] *= k;
+            v[2] *= k;
+            v[3] = std::clamp(1.0f - v[3] / den, 0.0f, 1.0f);
+        } else {
+            for (int c = 0; c < 4; ++c) v[c] /= den;
+        }
+    }
+    return PSY_OK;
+}
+
+psy_status psy_session_stats(const psy_session *s, psy_render_stats *out) {
+    if (!s || !out) return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = s->last_stats;
+    return PSY_OK;
+}
+
+psy_status psy_debug_sobol_samples(psy_context *ctx, uint32_t size, const uint32_t *queries, uint32_t count,
+                                   float *out_samples, uint32_t *out_indices) {
+    if (!ctx || !queries || !out_samples || !out_indices) return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    if (!sobol_size_valid(size)) return fail(PSY_ERROR_INVALID_ARGUMENT, "invalid Sobol sequence size");
+    if (count == 0u) return PSY_OK;
+    PSY_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    std::vector<float> table(size_t(size) * 256u * 4u);
+    psy_sobol_generate_table(size, table.data());
+    DeviceBuffer dt_, dq, ds, di;
+    PSY_CUDA_TRY(dt_.upload(table, st));
+    std::vector<uint32_t> q(queries, queries + 5ull * count);
+    PSY_CUDA_TRY(dq.upload(q, st));
+    PSY_CUDA_TRY(ds.alloc(sizeof(float4) * count));
+    PSY_CUDA_TRY(di.alloc(sizeof(uint32_t) * count));
+    psy::launch_debug_sobol(st, dt_.as<float4>(), size, dq.as<uint32_t>(), count, ds.as<float4>(), di.as<uint32_t>());
+    PSY_CUDA_TRY(cudaGetLastError());
+    PSY_CUDA_TRY(cudaMemcpyAsync(out_samples, ds.ptr, sizeof(float4) * count, cudaMemcpyDeviceToHost, st));
+    PSY_CUDA_TRY(cudaMemcpyAsync(out_indices, di.ptr, sizeof(uint32_t) * count, cudaMemcpyDeviceToHost, st));
+    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    return PSY_OK;
+}
+
+}  // extern "C"

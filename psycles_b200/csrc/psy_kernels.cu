@@ -1,0 +1,678 @@
+// Wavefront path-trace kernels for sm_100a.
+//
+// One render batch holds P window pixels x S samples = N paths whose state
+// lives in HBM as structure-of-arrays (PathBuffers).  Per path step:
+//   k_intersect  closest hit of every queued path (two-level BVH)
+//   k_shade      background / emission + forward MIS / roulette / AOV /
+//                NEE sample + BSDF evaluation (writes one shadow ray) /
+//                closure sample + path-state transition; survivors are
+//                compacted into the next queue with warp-aggregated atomics
+//   k_shadow     transmittance of the queued shadow rays, adds NEE radiance
+// and after the last step k_film adds each path's sample into the film in
+// sample order.  The kernels reproduce the Psycles Luisa megakernel
+// (src/luisa/path_kernel_pipeline.cpp:73-183) path by path: the queue order
+// never changes a path's result.
+#include "psy_device.cuh"
+#include "psy_kernels.h"
+
+namespace psy {
+
+// Warp-aggregated queue append: one atomic per warp, slots in lane order.
+// Every lane of the warp must call it (the callers' loops are warp-uniform).
+__device__ __forceinline__ uint32_t warp_push(uint32_t *counter, bool pred) {
+    const unsigned ballot = __ballot_sync(0xffffffffu, pred);
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0u;
+    if (lane == 0 && ballot != 0u) base = atomicAdd(counter, uint32_t(__popc(ballot)));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    return base + uint32_t(__popc(ballot & ((1u << lane) - 1u)));
+}
+
+__device__ __forceinline__ Xform xform12(const float *m) { return {ld3(m), ld3(m + 3), ld3(m + 6), ld3(m + 9)}; }
+
+__device__ __forceinline__ void set3(float *d, f3 v) {
+    d[0] = v.x;
+    d[1] = v.y;
+    d[2] = v.z;
+}
+
+// ------------------------------------------------------------------ raygen
+// begin_path_sample / construct_camera_ray (src/luisa/path_kernel_setup.cpp:485-700,
+// src/luisa/path_tracer_camera.cpp:10-246).
+__global__ void k_raygen(RenderParams p, PathBuffers b, uint32_t pixels, uint32_t paths, uint32_t sample_base,
+                         uint32_t trace_path, psy_path_trace *trace) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < paths; i += gridDim.x * blockDim.x) {
+        const uint32_t local = i % pixels;
+        const uint32_t sample = sample_base + i / pixels;
+        const uint32_t x = p.win_x + local % p.win_w;
+        const uint32_t y = p.win_y + local / p.win_w;
+        const uint32_t cycles_y = p.full_h - 1u - y;
+        const uint32_t rng_hash = pixel_hash(x, cycles_y, p.seed);
+        const float4 fs = sample_4d(p, sample, rng_hash, 0u);
+        const f2 filter = sample == 0u ? mk2(0.5f, 0.5f) : mk2(fs.x, fs.y);
+        const float jx = pixel_filter_sample(p.filter, filter.x);
+        const float jy = 1.0f - pixel_filter_sample(p.filter, filter.y);
+        const float W = static_cast<float>(p.full_w), H = static_cast<float>(p.full_h);
+        const float sx = 2.0f * (static_cast<float>(x) + jx) / W - 1.0f + 2.0f * p.shift_x;
+        const float sy = 1.0f - 2.0f * (static_cast<float>(y) + jy) / H + 2.0f * p.shift_y;
+        const f3 local_dir = normalize(mk3(sx * p.htan, sy * p.vtan, -1.0f));
+        const float clip_cos = -local_dir.z;
+        const Xform cam = xform12(p.cam);
+        f3 origin = xform_point(cam, mk3(0.0f));
+        const f3 dir = safe_normalize(xform_direction(cam, local_dir), mk3(0.0f, 0.0f, -1.0f));
+        const float safe_cos = maxf_(fabsf(clip_cos), 1.0e-20f);
+        const float near_t = p.near_clip / safe_cos;
+        const float far_t = (p.far_clip - p.near_clip) / safe_cos;
+        origin = origin + dir * near_t;
+        b.ray_o[i] = make_float4(origin.x, origin.y, origin.z, 0.0f);
+        b.ray_d[i] = make_float4(dir.x, dir.y, dir.z, far_t);
+        b.tp[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        b.rad[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        // initial_state (include/psycles/luisa/cycles_path_state.h:187-199)
+        b.st[i] = make_uint4(128u | 512u, 1u, 16u, 0u);
+        b.st2[i] = make_uint4(kSt2Delta, kInvalid, kInvalid, local);
+        b.sample[i] = sample;
+        b.aov_n[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        b.aov_a[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        b.queue_in[i] = i;
+        if (i == trace_path && trace) {
+            trace->pixel_x = x;
+            trace->pixel_y = y;
+            trace->sample = sample;
+            trace->rng_hash = rng_hash;
+            trace->filter[0] = filter.x;
+            trace->filter[1] = filter.y;
+            set3(trace->ray_origin, origin);
+            set3(trace->ray_direction, dir);
+            trace->valid = 1u;
+            trace->event_count = 0u;
+        }
+    }
+}
+
+// --------------------------------------------------------------- intersect
+// Cycles ray visibility of a path: contract_visibility (cycles_path_state.h:449-491).
+__device__ __forceinline__ uint32_t contract_visibility(uint32_t v) {
+    const uint32_t tv = (v & 2u) ? (v & ~(4u | 8u)) : v;
+    uint32_t r = 0u;
+    if (tv & 1u) r |= PSY_VISIBILITY_CAMERA;
+    if (tv & 2u) r |= PSY_VISIBILITY_TRANSMISSION;
+    if (tv & 4u) r |= PSY_VISIBILITY_DIFFUSE;
+    if (tv & 8u) r |= PSY_VISIBILITY_GLOSSY;
+    if (tv & 16u) r |= PSY_VISIBILITY_VOLUME_SCATTER;
+    return r;
+}
+
+__global__ void __launch_bounds__(256) k_intersect(SceneView s, PathBuffers b) {
+    const uint32_t count = b.counters[0];
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+        const uint32_t i = b.queue_in[q];
+        const float4 o = b.ray_o[i], d = b.ray_d[i];
+        const uint4 st = b.st[i];
+        const uint4 st2 = b.st2[i];
+        Ray ray{mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, d.w};
+        Hit h;
+        const bool hit = trace_closest(s, ray, contract_visibility(st.y), st2.y, st2.z, kInvalid, kInvalid, false, h);
+        b.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.instance));
+        b.hit_prim[i] = hit ? h.prim : kInvalid;
+    }
+}
+
+// ------------------------------------------------------------------- shade
+
+__device__ __forceinline__ float power_heuristic(float a, float c) {
+    const float a2 = a * a, c2 = c * c;
+    return a2 / maxf_(a2 + c2, 1.0e-20f);
+}
+
+// film_clamp_light (include/psycles/luisa/cycles_film_light.h:15-49).
+__device__ __forceinline__ f3 clamp_contribution(f3 c, uint32_t depth, const RenderParams &p) {
+    c = mk3(isfinite(c.x) ? c.x : 0.0f, isfinite(c.y) ? c.y : 0.0f, isfinite(c.z) ? c.z : 0.0f);
+    const float limit = depth > 0u ? p.clamp_indirect : p.clamp_direct;
+    const float mag = fabsf(c.x) + fabsf(c.y) + fabsf(c.z);
+    if (limit > 0.0f && mag > limit) return c * (limit / maxf_(mag, 1.0e-20f));
+    return c;
+}
+
+__device__ __forceinline__ float light_roulette_weight(f3 unshadowed, float random, float inv_threshold) {
+    const float m = max_abs_component(unshadowed);
+    const float pr = m * inv_threshold;
+    const bool roulette = inv_threshold > 0.0f && pr < 1.0f;
+    const bool survives = !roulette || random < pr;
+    const float inv_p = roulette ? 1.0f / maxf_(pr, 1.0e-20f) : 1.0f;
+    return survives ? inv_p : 0.0f;
+}
+
+constexpr uint32_t kFlagReflect = 1u, kFlagSingular = 2u, kFlagTransparent = 4u, kFlagImportanceBake = 8u,
+                   kFlagDiffuseAncestor = 16u, kFlagMisHadTransmission = 64u, kFlagMisSkip = 128u,
+                   kFlagSinglePassDone = 256u, kFlagTransparentBackground = 512u,
+                   kFlagTerminateOnNextSurface = 1024u, kFlagTerminateAfterTransparent = 4096u,
+                   kFlagSurfacePass = 1u << 18u, kFlagVolumePass = 1u << 19u;
+
+struct PathState {
+    uint32_t flag, visibility, bounce, diffuse_bounce, glossy_bounce, transmission_bounce, transparent_bounce,
+        rng_offset;
+};
+
+// cycles_path_state::next_surface (include/psycles/luisa/cycles_path_state.h:205-338).
+__device__ __forceinline__ PathState next_surface(const PathState &before, uint32_t label, uint32_t runtime,
+                                                  const RenderParams &p) {
+    if ((label & (kLabelTransparent | 512u)) != 0u) {
+        PathState t = before;
+        t.transparent_bounce += 1u;
+        t.rng_offset += 16u;
+        t.flag |= kFlagTransparent;
+        if (t.transparent_bounce >= p.transparent_max) t.flag |= kFlagTerminateOnNextSurface;
+        if ((runtime & 4096u) != 0u) t.flag |= kFlagMisSkip;
+        return t;
+    }
+    PathState s = before;
+    s.bounce += 1u;
+    s.rng_offset += 16u;
+    if (s.bounce >= p.maximum) s.flag |= kFlagTerminateAfterTransparent;
+    s.visibility = 0u;
+    s.flag &= ~(kFlagReflect | kFlagSingular | kFlagTransparent | kFlagImportanceBake | kFlagMisSkip |
+                kFlagMisHadTransmission);
+    const bool reflection = (label & kLabelReflect) != 0u;
+    const bool diffuse = (label & kLabelDiffuse) != 0u;
+    const bool glossy = (label & kLabelGlossy) != 0u;
+    const bool transmit_transparent = (label & 128u) != 0u;
+    if (reflection) s.flag |= kFlagReflect;
+    if (reflection || !transmit_transparent) s.flag &= ~kFlagTransparentBackground;
+    const bool diffuse_reflection = reflection && diffuse;
+    const bool glossy_reflection = reflection && !diffuse;
+    const bool transmission = !reflection;
+    if (diffuse_reflection) s.diffuse_bounce += 1u;
+    if (glossy_reflection) s.glossy_bounce += 1u;
+    if (transmission) s.transmission_bounce += 1u;
+    if (diffuse_reflection && s.diffuse_bounce >= p.max_diffuse) s.flag |= kFlagTerminateAfterTransparent;
+    if (glossy_reflection && s.glossy_bounce >= p.max_glossy) s.flag |= kFlagTerminateAfterTransparent;
+    if (transmission && s.transmission_bounce >= p.max_transmission) s.flag |= kFlagTerminateAfterTransparent;
+    if (transmission) s.visibility |= 2u;
+    s.visibility |= diffuse ? 4u : 8u;
+    if (diffuse) s.flag |= kFlagDiffuseAncestor;
+    if (!diffuse && !glossy) s.flag |= kFlagSingular | kFlagMisSkip;
+    if ((runtime & kRuntimeBsdfHasTransmission) != 0u) s.flag |= kFlagMisHadTransmission;
+    if ((s.flag & (kFlagSurfacePass | kFlagVolumePass)) == 0u && (s.flag & kFlagTransparentBackground) == 0u)
+        s.flag |= kFlagSurfacePass;
+    return s;
+}
+
+__device__ __forceinline__ PathState unpack_state(uint4 st, uint4 st2) {
+    return {st.x, st.y, st.w & 0xffu, (st.w >> 8) & 0xffu, (st.w >> 16) & 0xffu, st.w >> 24, st2.x & 0xffu, st.z};
+}
+
+__device__ __forceinline__ float next_float_up(float t) {
+    return t == 0.0f ? 1.17549435e-38f : __uint_as_float(__float_as_uint(t) + 1u);
+}
+
+__global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, PathBuffers b, uint32_t step,
+                                               uint32_t trace_path, psy_path_trace *trace) {
+    const uint32_t count = b.counters[0];
+    const uint32_t rounds = (count + gridDim.x * blockDim.x - 1u) / (gridDim.x * blockDim.x);
+    // Every lane runs the same number of rounds so the warp-aggregated queue
+    // pushes see the whole warp.
+    for (uint32_t r = 0; r < rounds; ++r) {
+        const uint32_t q = r * gridDim.x * blockDim.x + blockIdx.x * blockDim.x + threadIdx.x;
+        const bool active = q < count;
+        bool keep = false;
+        bool shadow = false;
+        uint32_t i = 0u;
+        float4 sh_o, sh_d, sh_c;
+        uint4 sh_ids;
+        if (active) {
+            i = b.queue_in[q];
+            psy_path_event *ev = nullptr;
+            if (trace && i == trace_path && step < PSY_TRACE_MAX_EVENTS) {
+                ev = &trace->events[step];
+                trace->event_count = step + 1u;
+            }
+            const float4 ro = b.ray_o[i], rd = b.ray_d[i];
+            Ray ray{mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z), ro.w, rd.w};
+            float4 tp4 = b.tp[i];
+            f3 throughput = mk3(tp4.x, tp4.y, tp4.z);
+            float previous_bsdf_pdf = tp4.w;
+            float4 rad4 = b.rad[i];
+            f3 radiance = mk3(rad4.x, rad4.y, rad4.z);
+            float transparency = rad4.w;
+            uint4 st = b.st[i];
+            uint4 st2 = b.st2[i];
+            PathState ps = unpack_state(st, st2);
+            bool previous_delta = (st2.x & kSt2Delta) != 0u;
+            bool primary_recorded = (st2.x & kSt2Primary) != 0u;
+            const bool terminate_on_next_surface = (st2.x & kSt2TermNext) != 0u;
+            const bool terminate_after_transparent = (st2.x & kSt2TermAfter) != 0u;
+            const uint32_t ray_visibility = contract_visibility(ps.visibility);
+            const uint32_t sample = b.sample[i];
+            const uint32_t local = st2.w;
+            const uint32_t x = p.win_x + local % p.win_w;
+            const uint32_t y = p.win_y + local / p.win_w;
+            const uint32_t rng_hash = pixel_hash(x, p.full_h - 1u - y, p.seed);
+            const float terminate_sample = sample_4d(p, sample, rng_hash, ps.rng_offset + 0u).x;
+            const float4 ls4 = sample_4d(p, sample, rng_hash, ps.rng_offset + 1u);
+            const f3 light_sample = mk3(ls4.x, ls4.y, ls4.z);
+            const float light_terminate = sample_4d(p, sample, rng_hash, ps.rng_offset + 2u).x;
+            const float4 bs4 = sample_4d(p, sample, rng_hash, ps.rng_offset + 3u);
+            const DistEntryGpu selected = distribution_sample(s, light_sample.z);
+            const float4 h4 = b.hit[i];
+            const uint32_t prim = b.hit_prim[i];
+            if (ev) {
+                ev->rng_offset = ps.rng_offset;
+                ev->random_terminate = terminate_sample;
+                set3(ev->random_light, light_sample);
+                ev->random_light_terminate = light_terminate;
+                set3(ev->random_bsdf, mk3(bs4.x, bs4.y, bs4.z));
+                ev->light_kind = selected.kind;
+                ev->light_index = selected.index;
+                const bool missed = prim == kInvalid;
+                ev->hit_t = missed ? 0.0f : h4.x;
+                ev->hit_u = missed ? 0.0f : h4.y;
+                ev->hit_v = missed ? 0.0f : h4.z;
+                ev->closure_index = kInvalid;
+                ev->hit_object = kInvalid;
+                ev->hit_primitive = kInvalid;
+            }
+            const uint32_t depth = ps.bounce;
+            bool alive = true;
+            if (prim == kInvalid) {
+                // BackgroundEventStage (src/luisa/path_kernel_background_event.cpp:14-160)
+                const f3 bg = ld3(s.background);
+                const f3 c = clamp_contribution(throughput * bg * 1.0f, depth, p);
+                const bool world_visible = (s.world_visibility & ray_visibility) != 0u;
+                const bool transparent_bg = p.transparent_background != 0u && (ps.flag & kFlagTransparentBackground) != 0u;
+                if (transparent_bg) {
+                    transparency += (throughput.x + throughput.y + throughput.z) * (1.0f / 3.0f);
+                } else if (world_visible) {
+                    radiance = radiance + c;
+                    if (ev) set3(ev->emission, c);
+                }
+                if (ev) ev->terminated = 1u;
+                alive = false;
+            } else {
+                Hit h;
+                h.t = h4.x;
+                h.u = h4.y;
+                h.v = h4.z;
+                h.instance = __float_as_uint(h4.w);
+                h.prim = prim;
+                h.object = h.instance;
+                h.cycles_prim = s.meshes[s.instances[h.instance].mesh].prim_offset + prim;
+                if (ev) {
+                    ev->hit_object = h.object;
+                    ev->hit_primitive = h.cycles_prim;
+                }
+                const SurfacePoint sp = surface_point(s, h, ray.d);
+                const MaterialGpu mat = s.materials[sp.material];
+                SurfaceClosures closures;
+                collect_surface(s, mat, sp.n, closures);
+                // SurfaceShadingStageImpl::emit (src/luisa/path_kernel_surface_shading.cpp:117-250)
+                float emission_weight = 1.0f;
+                if (p.nee && s.triangle_emitters > 0u && mat.emission_sampling != 0u && mat.has_emission) {
+                    const bool competing = depth > 0u && !previous_delta;
+                    const float selection_pdf =
+                        0.5f * length(cross(sp.wp1 - sp.wp0, sp.wp2 - sp.wp0)) * s.triangle_area_pdf;
+                    const float light_pdf = emissive_forward_pdf(selection_pdf, mat.emission_sampling, ray.o,
+                                                                 sp.position, sp.wp0, sp.wp1, sp.wp2, sp.ng);
+                    const bool available = light_pdf > 0.0f;
+                    if (p.direct_mode == PSY_DIRECT_LIGHT_NEE) emission_weight = (competing && available) ? 0.0f : 1.0f;
+                    else if (p.direct_mode == PSY_DIRECT_LIGHT_MIS)
+                        emission_weight = (competing && available) ? power_heuristic(previous_bsdf_pdf, light_pdf) : 1.0f;
+                }
+                const f3 ec = clamp_contribution(throughput * closures.emission * emission_weight, depth, p);
+                radiance = radiance + ec;
+                if (ev) set3(ev->emission, ec);
+                if (terminate_on_next_surface) {
+                    alive = false;
+                    if (ev) ev->terminated = 1u;
+                }
+                if (alive) {
+                    // continuation_probability (cycles_path_state.h:413-447)
+                    const bool tr_state = (ps.flag & kFlagTransparent) != 0u;
+                    const bool before_min = tr_state ? ps.transparent_bounce <= p.transparent_min : ps.bounce <= p.minimum;
+                    const float cp = before_min ? 1.0f : minf_(sqrtf(max_abs_component(throughput)), 1.0f);
+                    if (ev) ev->continuation_probability = cp;
+                    if (cp <= 0.0f) {
+                        alive = false;
+                    } else if (cp != 1.0f) {
+                        if (terminate_sample >= cp) alive = false;
+                        else throughput = throughput / cp;
+                    }
+                    if (!alive && ev) ev->terminated = 1u;
+                }
+                if (alive) {
+                    if (depth == 0u) {
+                        f3 aov_albedo, aov_normal, aov_transparency;
+                        surface_aov(closures, sp.n, aov_albedo, aov_normal, aov_transparency);
+                        const float4 a4 = b.aov_a[i];
+                        const f3 acc = mk3(a4.x, a4.y, a4.z) + throughput * aov_albedo;
+                        b.aov_a[i] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+                        const f3 alpha = clamp3(mk3(1.0f) - aov_transparency, 0.0f, 1.0f);
+                        const float average_alpha = (alpha.x + alpha.y + alpha.z) * (1.0f / 3.0f);
+                        const bool writes_normal = !primary_recorded && (p.pass_alpha_threshold == 0.0f ||
+                                                                         average_alpha >= p.pass_alpha_threshold);
+                        if (writes_normal) {
+                            b.aov_n[i] = make_float4(aov_normal.x, aov_normal.y, aov_normal.z, 0.0f);
+                            primary_recorded = true;
+                            ps.flag |= kFlagSinglePassDone;
+                        }
+                    }
+                    const uint32_t runtime = runtime_flags(closures, sp.back_facing);
+                    const uint32_t lobe_mask = terminate_after_transparent ? kEventTransparent : 0xffffffffu;
+                    const InstanceGpu &inst = s.instances[sp.instance];
+                    // Direct lighting (src/luisa/path_kernel_pipeline.cpp:160-172)
+                    if (p.nee && (runtime & kRuntimeBsdfHasEval) != 0u) {
+                        f3 lp = mk3(0.0f), ldir = mk3(0.0f);
+                        float ldist = 0.0f;
+                        bool distant = false;
+                        f3 surviving = mk3(0.0f);
+                        uint32_t light_obj = kInvalid, light_prim = kInvalid;
+                        bool emit = false;
+                        if (selected.kind == 0u) {
+                            // EmissiveMeshLightingComponent (src/luisa/path_kernel_nee_emissive_mesh.cpp:32-296)
+                            const EmitterGpu &em = s.emitters[selected.index];
+                            const TriSample ls = sample_triangle(sp.position, ld3(em.p0), ld3(em.p1), ld3(em.p2),
+                                                                 mk2(light_sample.x, light_sample.y));
+                            const bool side = sampled_side(em.emission_sampling, ld3(em.ng), ls.direction);
+                            const float pdf = ls.pdf * selected.selection_pdf;
+                            if (ls.valid && side && em.area > 0.0f && pdf > 0.0f) {
+                                const bool is_transmission = dot(ls.direction, sp.n) < 0.0f;
+                                const bool same_primitive = em.cycles_prim == sp.cycles_prim && em.object == sp.object;
+                                const f3 oriented = is_transmission ? -sp.ng : sp.ng;
+                                const bool reject_self = same_primitive && dot(ls.direction, oriented) > 0.0f;
+                                if (!reject_self) {
+                                    const f3 light_radiance = material_emission(s, s.materials[em.material]);
+                                    const Evaluation e = evaluate_mixture(closures, sp.n, ls.direction, lobe_mask, -1);
+                                    float mis = 1.0f;
+                                    if (p.direct_mode == PSY_DIRECT_LIGHT_FORWARD) mis = e.pdf <= 0.0f ? 1.0f : 0.0f;
+                                    else if (p.direct_mode == PSY_DIRECT_LIGHT_MIS) mis = power_heuristic(pdf, e.pdf);
+                                    const f3 weighted = e.f * light_radiance * (mis / pdf);
+                                    if (any_nonzero(weighted)) {
+                                        const f3 unshadowed = weighted * mk3(1.0f);
+                                        surviving = unshadowed *
+                                                    light_roulette_weight(unshadowed, light_terminate, p.inv_rr_threshold);
+                                        if (any_nonzero(surviving)) {
+                                            emit = true;
+                                            lp = ls.position;
+                                            light_obj = em.object;
+                                            light_prim = em.cycles_prim;
+                                            ldir = ls.direction;
+                                        }
+                                    }
+                                }
+                            }
+                        } else if (selected.kind == 1u) {
+                            // AnalyticLightingComponent (src/luisa/path_kernel_nee_analytic.cpp:98-428)
+                            const psy_light_desc &l = s.lights[selected.index];
+                            if (!(depth > l.max_bounces)) {
+                                const AnalyticSample a = sample_analytic(l, sp.position, mk2(light_sample.x, light_sample.y));
+                                const float light_pdf = a.pdf * selected.selection_pdf;
+                                if (a.valid && light_pdf > 0.0f) {
+                                    const f3 light_radiance = ld3(l.color) * (l.power * a.eval_factor);
+                                    const Evaluation e = evaluate_mixture(closures, sp.n, a.direction, lobe_mask, -1);
+                                    const f3 weighted = e.f * light_radiance * (1.0f / maxf_(light_pdf, 1.0e-20f));
+                                    if (any_nonzero(weighted)) {
+                                        const f3 unshadowed = weighted * mk3(1.0f);
+                                        surviving = unshadowed *
+                                                    light_roulette_weight(unshadowed, light_terminate, p.inv_rr_threshold);
+                                        if (any_nonzero(surviving)) {
+                                            emit = true;
+                                            lp = a.position;
+                                            ldir = a.direction;
+                                            distant = l.type == PSY_LIGHT_DISTANT;
+                                        }
+                                    }
+                                }
+                            }
+                        }
+                        if (emit) {
+                            // make_shadow_origin (src/luisa/path_kernel_surface_geometry.cpp:168-185)
+                            const Xform w2o = xform12(inst.w2o);
+                            const f3 so = origin_with_self_exclusion(sp, xform_point(w2o, sp.position),
+                                                                     xform_direction(w2o, ldir));
+                            const f3 off = lp - so;
+                            const float fd = sqrtf(maxf_(dot(off, off), 1.0e-20f));
+                            const f3 sdir = distant ? ldir : off / fd;
+                            ldist = distant ? 1.0e30f : fd;
+                            const f3 c = throughput * surviving;
+                            sh_o = make_float4(so.x, so.y, so.z, ldist);
+                            sh_d = make_float4(sdir.x, sdir.y, sdir.z, __uint_as_float(ps.transparent_bounce));
+                            sh_c = make_float4(c.x, c.y, c.z, __uint_as_float(depth));
+                            sh_ids = make_uint4(sp.object, sp.cycles_prim, light_obj, light_prim);
+                            shadow = true;
+                        }
+                    }
+                    // SurfaceScatterStageImpl::emit (src/luisa/path_kernel_surface_scatter.cpp:136-291)
+                    const SurfaceSample ss = sample_surface(closures, sp.n, sp.ng, -ray.d, bs4.z, mk2(bs4.x, bs4.y),
+                                                            lobe_mask);
+                    if (ev) {
+                        ev->closure_index = ss.closure_index;
+                        ev->bsdf_pdf = ss.eval.pdf;
+                        set3(ev->wi, ss.wi);
+                    }
+                    if (!ss.valid || ss.eval.pdf <= 0.0f) {
+                        alive = false;
+                    } else {
+                        const bool transparent = (ss.eval.events & kEventTransparent) != 0u;
+                        const bool singular = (ss.eval.events & kEventSingular) != 0u;
+                        const uint32_t label = label_from_events(ss.eval.events);
+                        throughput = throughput * (ss.eval.f / ss.eval.pdf);
+                        if (ev) {
+                            ev->label = label;
+                            set3(ev->throughput, throughput);
+                        }
+                        if (any_nan(throughput) || throughput.x < 0.0f || throughput.y < 0.0f || throughput.z < 0.0f) {
+                            alive = false;
+                        } else {
+                            ps = next_surface(ps, label, runtime, p);
+                            if (!transparent) {
+                                previous_bsdf_pdf = ss.eval.pdf;
+                                previous_delta = singular;
+                            }
+                            if (ev) {
+                                ev->bounce = ps.bounce;
+                                ev->transparent_bounce = ps.transparent_bounce;
+                                ev->flag = ps.flag;
+                                ev->visibility = ps.visibility;
+                            }
+                            if (transparent) {
+                                ray.tmin = next_float_up(h.t);
+                            } else {
+                                const f3 wi = normalize(ss.wi);
+                                const Xform w2o = xform12(inst.w2o);
+                                ray.o = origin_with_self_exclusion(sp, sp.object_position, xform_direction(w2o, wi));
+                                ray.d = wi;
+                                ray.tmin = 0.0f;
+                                ray.tmax = 1.0e30f;
+                            }
+                            keep = true;
+                            st2.y = sp.object;
+                            st2.z = sp.cycles_prim;
+                        }
+                    }
+                    if (!keep && ev) ev->terminated = 1u;
+                }
+            }
+            b.rad[i] = make_float4(radiance.x, radiance.y, radiance.z, transparency);
+            if (keep) {
+                b.ray_o[i] = make_float4(ray.o.x, ray.o.y, ray.o.z, ray.tmin);
+                b.ray_d[i] = make_float4(ray.d.x, ray.d.y, ray.d.z, ray.tmax);
+                b.tp[i] = make_float4(throughput.x, throughput.y, throughput.z, previous_bsdf_pdf);
+                b.st[i] = make_uint4(ps.flag, ps.visibility, ps.rng_offset,
+                                     ps.bounce | (ps.diffuse_bounce << 8) | (ps.glossy_bounce << 16) |
+                                         (ps.transmission_bounce << 24));
+                uint32_t bits = ps.transparent_bounce & 0xffu;
+                if (previous_delta) bits |= kSt2Delta;
+                if (primary_recorded) bits |= kSt2Primary;
+                if ((ps.flag & kFlagTerminateOnNextSurface) != 0u) bits |= kSt2TermNext;
+                if ((ps.flag & kFlagTerminateAfterTransparent) != 0u) bits |= kSt2TermAfter;
+                st2.x = bits;
+                b.st2[i] = st2;
+            }
+        }
+        const uint32_t slot = warp_push(&b.counters[1], active && keep);
+        if (active && keep) b.queue_out[slot] = i;
+        const uint32_t sslot = warp_push(&b.counters[2], active && shadow);
+        if (active && shadow) {
+            b.sh_o[sslot] = sh_o;
+            b.sh_d[sslot] = sh_d;
+            b.sh_c[sslot] = sh_c;
+            b.sh_ids[sslot] = sh_ids;
+            b.sh_path[sslot] = i;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ shadow
+// make_trace_shadow_callable (src/luisa/path_tracer_geometry.cpp:75-174).
+__global__ void __launch_bounds__(256) k_shadow(SceneView s, RenderParams p, PathBuffers b, uint32_t step,
+                                                uint32_t trace_path, psy_path_trace *trace) {
+    const uint32_t count = b.counters[2];
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+        const float4 o = b.sh_o[q], d = b.sh_d[q], c = b.sh_c[q];
+        const uint4 ids = b.sh_ids[q];
+        const uint32_t path = b.sh_path[q];
+        Ray ray{mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), 0.0f, o.w};
+        uint32_t transparent_depth = __float_as_uint(d.w);
+        const uint32_t depth = __float_as_uint(c.w);
+        f3 transmittance = mk3(1.0f);
+        if (!s.any_transparent) {
+            Hit h;
+            if (trace_closest(s, ray, PSY_VISIBILITY_SHADOW, ids.x, ids.y, ids.z, ids.w, true, h))
+                transmittance = mk3(0.0f);
+        } else {
+            for (uint32_t guard = 0; guard < 4096u; ++guard) {
+                Hit h;
+                if (!trace_closest(s, ray, PSY_VISIBILITY_SHADOW, ids.x, ids.y, ids.z, ids.w, false, h)) break;
+                if (transparent_depth >= p.transparent_max) {
+                    transmittance = mk3(0.0f);
+                    break;
+                }
+                const InstanceGpu &inst = s.instances[h.instance];
+                const MeshGpu mesh = s.meshes[inst.mesh];
+                const uint32_t mi = mesh.material_offset == kInvalid ? inst.material
+                                                                     : s.tri_materials[mesh.material_offset + h.prim];
+                const f3 t = clamp3(transparent_extinction(s, s.materials[mi]), 0.0f, 1.0f);
+                if (!(max_component(t) > 0.0f)) {
+                    transmittance = mk3(0.0f);
+                    break;
+                }
+                transmittance = transmittance * t;
+                transparent_depth += 1u;
+                ray.tmin = next_float_up(h.t);
+            }
+        }
+        f3 contribution = mk3(0.0f);
+        if (transmittance.x > 0.0f || transmittance.y > 0.0f || transmittance.z > 0.0f) {
+            contribution = clamp_contribution(mk3(c.x, c.y, c.z) * transmittance, depth, p);
+            float4 r = b.rad[path];
+            r.x += contribution.x;
+            r.y += contribution.y;
+            r.z += contribution.z;
+            b.rad[path] = r;
+        }
+        if (trace && path == trace_path && step < PSY_TRACE_MAX_EVENTS) set3(trace->events[step].nee, contribution);
+    }
+}
+
+// -------------------------------------------------------------------- film
+// accumulate_path_sample + write_film (src/luisa/path_kernel_setup.cpp:903-1062):
+// samples are added in sample order.
+__global__ void k_film(PathBuffers b, uint32_t pixels, uint32_t samples, float4 *combined, float4 *normal,
+                       float4 *albedo, uint32_t *sample_count, uint32_t trace_path, psy_path_trace *trace) {
+    for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < pixels; px += gridDim.x * blockDim.x) {
+        float4 c = combined[px], n = normal[px], a = albedo[px];
+        for (uint32_t k = 0; k < samples; ++k) {
+            const uint32_t i = k * pixels + px;
+            const float4 r = b.rad[i];
+            f3 rad = mk3(r.x, r.y, r.z);
+            if (any_nan(rad)) rad = mk3(0.0f);
+            c.x += rad.x;
+            c.y += rad.y;
+            c.z += rad.z;
+            c.w += r.w;
+            const float4 nn = b.aov_n[i], aa = b.aov_a[i];
+            n.x += nn.x;
+            n.y += nn.y;
+            n.z += nn.z;
+            n.w += 1.0f;
+            a.x += aa.x;
+            a.y += aa.y;
+            a.z += aa.z;
+            a.w += 1.0f;
+            if (trace && i == trace_path) set3(trace->radiance, rad);
+        }
+        combined[px] = c;
+        normal[px] = n;
+        albedo[px] = a;
+        sample_count[px] += samples;
+    }
+}
+
+__global__ void k_swap_counters(uint32_t *counters) {
+    counters[0] = counters[1];
+    counters[1] = 0u;
+    counters[2] = 0u;
+}
+
+__global__ void k_set_counters(uint32_t *counters, uint32_t n) {
+    counters[0] = n;
+    counters[1] = 0u;
+    counters[2] = 0u;
+}
+
+// Accumulates the number of rays traced by the queues of one step.
+__global__ void k_count_rays(const uint32_t *counters, unsigned long long *stats) {
+    stats[0] += counters[0];
+    stats[1] += counters[2];
+}
+
+__global__ void k_debug_sobol(const float4 *table, uint32_t size, const uint32_t *queries, uint32_t count, float4 *out,
+                              uint32_t *out_index) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const uint32_t *q = queries + 5u * i;
+    const uint32_t h = pixel_hash(q[0], q[1], q[2]);
+    const uint32_t idx = shuffled_sample_index(q[3], q[4], h, size);
+    out[i] = table[idx];
+    out_index[i] = idx;
+}
+
+// ----------------------------------------------------------------- launches
+
+int launch_grid(uint32_t work, int block, int sms) {
+    const uint32_t blocks = (work + uint32_t(block) - 1u) / uint32_t(block);
+    const uint32_t cap = uint32_t(sms) * 16u;
+    return int(blocks < 1u ? 1u : (blocks > cap ? cap : blocks));
+}
+
+void launch_raygen(cudaStream_t st, int sms, const RenderParams &p, const PathBuffers &b, uint32_t pixels,
+                   uint32_t paths, uint32_t sample_base, uint32_t trace_path, psy_path_trace *trace) {
+    k_raygen<<<launch_grid(paths, 256, sms), 256, 0, st>>>(p, b, pixels, paths, sample_base, trace_path, trace);
+}
+void launch_set_counters(cudaStream_t st, uint32_t *counters, uint32_t n) { k_set_counters<<<1, 1, 0, st>>>(counters, n); }
+void launch_intersect(cudaStream_t st, int sms, const SceneView &s, const PathBuffers &b, uint32_t max_work) {
+    k_intersect<<<launch_grid(max_work, 256, sms), 256, 0, st>>>(s, b);
+}
+void launch_shade(cudaStream_t st, int sms, const SceneView &s, const RenderParams &p, const PathBuffers &b,
+                  uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
+    k_shade<<<launch_grid(max_work, 128, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace);
+}
+void launch_shadow(cudaStream_t st, int sms, const SceneView &s, const RenderParams &p, const PathBuffers &b,
+                   uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
+    k_shadow<<<launch_grid(max_work, 256, sms), 256, 0, st>>>(s, p, b, step, trace_path, trace);
+}
+void launch_swap(cudaStream_t st, uint32_t *counters) { k_swap_counters<<<1, 1, 0, st>>>(counters); }
+void launch_count_rays(cudaStream_t st, const uint32_t *counters, unsigned long long *stats) {
+    k_count_rays<<<1, 1, 0, st>>>(counters, stats);
+}
+void launch_film(cudaStream_t st, int sms, const PathBuffers &b, uint32_t pixels, uint32_t samples, float4 *combined,
+                 float4 *normal, float4 *albedo, uint32_t *sample_count, uint32_t trace_path, psy_path_trace *trace) {
+    k_film<<<launch_grid(pixels, 256, sms), 256, 0, st>>>(b, pixels, samples, combined, normal, albedo, sample_count,
+                                                        trace_path, trace);
+}
+void launch_debug_sobol(cudaStream_t st, const float4 *table, uint32_t size, const uint32_t *queries, uint32_t count,
+                        float4 *out, uint32_t *out_index) {
+    k_debug_sobol<<<(count + 127u) / 128u, 128, 0, st>>>(table, size, queries, count, out, out_index);
+}
+
+}  // namespace psy

@@ -1,0 +1,139 @@
+// Device-resident scene and render parameters of the B200 path tracer.
+//
+// HBM layout (one allocation per array, all 16-byte aligned):
+//   tlas / blas   binary BVH nodes, 64 B each: three float4 hold the two
+//                 children's x/y/z slabs, one int4 the child links
+//   tris          leaf-ordered triangles of all meshes, 3 float4 per
+//                 triangle (48 B): object-space vertices, v0.w = local
+//                 primitive index bits
+//   positions / normals / indices  the meshes' shading data
+//   instances     InstanceGpu (object<->world transforms, mesh, material)
+//   materials / code / scalars / vectors  closure programs and their
+//                 parameter blocks (rebinding rewrites scalars/vectors)
+//   emitters / distribution  emissive triangles and the flat light CDF
+//   lights        analytic lights (psy_light_desc)
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/psycles_cuda.h"
+
+namespace psy {
+
+constexpr uint32_t kInvalidId = 0xffffffffu;
+
+struct alignas(16) BvhNodeGpu {
+    float4 x;    // left.lo.x, left.hi.x, right.lo.x, right.hi.x
+    float4 y;    // left.lo.y, left.hi.y, right.lo.y, right.hi.y
+    float4 z;    // left.lo.z, left.hi.z, right.lo.z, right.hi.z
+    int4 child;  // x/y: >= 0 inner node, < 0 leaf ~first; z/w: leaf counts
+};
+static_assert(sizeof(BvhNodeGpu) == 64, "BVH node is one 64-byte line");
+
+struct alignas(16) InstanceGpu {
+    float o2w[12];  // column-major c0, c1, c2, c3 (xyz each)
+    float w2o[12];
+    float nrm[12];  // normal-to-world columns (c3 unused)
+    uint32_t mesh, material, visibility, pad;
+};
+
+struct alignas(16) MeshGpu {
+    uint32_t node_offset;    // root of the mesh BLAS in `blas`
+    uint32_t tri_offset;     // first leaf triangle in `tris`
+    uint32_t triangle_count;
+    uint32_t prim_offset;    // Cycles primitive id of local primitive 0
+    uint32_t vertex_offset;  // into positions / normals (vertices)
+    uint32_t index_offset;   // into indices (uint32 elements)
+    uint32_t material_offset;  // into tri_materials, kInvalid = instance material
+    uint32_t smooth;
+};
+
+struct alignas(16) MaterialGpu {
+    uint32_t code_offset, code_count, root, scalar_offset;
+    uint32_t vector_offset, emission_sampling, has_emission, has_transparent;
+};
+
+struct alignas(16) EmitterGpu {
+    float p0[3], p1[3], p2[3], ng[3];
+    float area;
+    uint32_t material, object, cycles_prim;
+    uint32_t emission_sampling, pad0, pad1, pad2;
+};
+
+struct alignas(16) DistEntryGpu {
+    float cumulative, selection_pdf;
+    uint32_t kind, index;
+};
+
+struct SceneView {
+    const BvhNodeGpu *tlas;
+    const BvhNodeGpu *blas;
+    const float4 *tris;
+    const InstanceGpu *instances;
+    const MeshGpu *meshes;
+    const float *positions;
+    const float *normals;
+    const uint32_t *indices;
+    const uint32_t *tri_materials;
+    const MaterialGpu *materials;
+    const psy_closure_instruction *code;
+    const float *scalars;
+    const float *vectors;
+    const EmitterGpu *emitters;
+    const DistEntryGpu *distribution;
+    const psy_light_desc *lights;
+    uint32_t instance_count;
+    uint32_t emitter_count;   // distribution entries - 1 (triangles + lights)
+    uint32_t triangle_emitters;
+    uint32_t light_count;
+    float triangle_area_pdf;
+    float background[3];
+    uint32_t world_visibility;
+    uint32_t any_transparent;
+};
+
+struct RenderParams {
+    uint32_t full_w, full_h, win_x, win_y, win_w, win_h;
+    uint32_t seed, transparent_background;
+    float pass_alpha_threshold;
+    uint32_t maximum, minimum, max_diffuse, max_glossy, max_transmission;
+    uint32_t transparent_min, transparent_max, steps;
+    float clamp_direct, clamp_indirect, inv_rr_threshold;
+    uint32_t direct_mode, nee;
+    float cam[12];  // camera_to_world columns c0..c3
+    float htan, vtan, shift_x, shift_y, near_clip, far_clip;
+    const float4 *sobol;
+    uint32_t sobol_size;
+    const float *filter;  // 1024 entries
+};
+
+// Wavefront path state, structure of arrays over `capacity` paths.
+struct PathBuffers {
+    float4 *ray_o;    // origin, tmin
+    float4 *ray_d;    // direction, tmax
+    float4 *tp;       // throughput, previous bsdf pdf
+    float4 *rad;      // radiance, transparency
+    uint4 *st;        // flag, cycles visibility, rng_offset, packed counters
+    uint4 *st2;       // transparent bounce | bits, source object, source prim, pixel
+    uint32_t *sample; // absolute sample index
+    float4 *aov_n;    // first-surface normal
+    float4 *aov_a;    // albedo
+    float4 *hit;      // t, u, v, instance bits
+    uint32_t *hit_prim;
+    float4 *sh_o;     // shadow origin, tmax
+    float4 *sh_d;     // shadow direction, transparent depth bits
+    float4 *sh_c;     // unshadowed contribution
+    uint4 *sh_ids;    // source object, source prim, light object, light prim
+    uint32_t *sh_path;
+    uint32_t *queue_in;
+    uint32_t *queue_out;
+    uint32_t *shadow_queue;
+    uint32_t *counters;  // [0] in count, [1] out count, [2] shadow count, [3..] stats
+};
+
+// Packed counters of st.w: bounce | diffuse << 8 | glossy << 16 | transmission << 24.
+// st2.x: transparent bounce (bits 0-7), previous_delta (8), primary_recorded
+// (9), terminate_on_next_surface (10), terminate_after_transparent (11).
+constexpr uint32_t kSt2Delta = 1u << 8, kSt2Primary = 1u << 9, kSt2TermNext = 1u << 10, kSt2TermAfter = 1u << 11;
+
+}  // namespace psy

@@ -1,0 +1,449 @@
+"""Scene snapshots and the seeded synthetic workloads.
+
+`Scene` is the flattened SceneSnapshot the C ABI compiles
+(psy_scene_desc): meshes, instances, compiled materials, analytic lights,
+camera and a constant world colour.  `SceneDatabase.apply` mirrors the
+reference's transactional deltas (src/contract/scene.cpp:427): a delta is
+validated completely before a new revision is committed.
+
+Workloads (all generated from seeds; no external data):
+  * cornell_box()        closed box of 5 quads + a cube rotated 20 degrees
+                         about Y, 0.73 / 0.65 / 0.12 albedos, one 0.5 x 0.5
+                         emissive quad of strength 15, 40 degree pinhole
+  * procedural_scene()   64 instances of 8 geodesic spheres (2k-40k
+                         triangles, ~1M instanced), 32 random closure graphs,
+                         point / spot / sun lights, constant background
+  * many_light_scene()   ground + 200 boxes + emissive triangles scattered
+                         in a 20^3 volume with log-uniform strengths
+"""
+
+from __future__ import annotations
+
+import copy
+import ctypes
+import dataclasses
+import math
+
+import numpy as np
+
+from . import _abi
+from .materials import (CompiledMaterial, ShaderGraph, compile_surface_program, diffuse_material,
+                        emission_material, random_material)
+
+
+@dataclasses.dataclass
+class Mesh:
+    positions: np.ndarray            # float32 [V, 3]
+    indices: np.ndarray              # uint32 [T, 3]
+    normals: np.ndarray | None = None  # float32 [V, 3]
+    materials: np.ndarray | None = None  # uint32 [T]
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.indices.shape[0])
+
+
+@dataclasses.dataclass
+class Instance:
+    mesh: int
+    material: int
+    transform: np.ndarray = dataclasses.field(default_factory=lambda: np.eye(4, dtype=np.float32))
+    visibility: int = _abi.VIS_ALL
+
+
+@dataclasses.dataclass
+class Light:
+    type: int
+    color: tuple = (1.0, 1.0, 1.0)
+    power: float = 1.0
+    position: tuple = (0.0, 0.0, 0.0)
+    axis_x: tuple = (1.0, 0.0, 0.0)
+    axis_y: tuple = (0.0, 1.0, 0.0)
+    axis_z: tuple = (0.0, 0.0, 1.0)
+    axis_scale: tuple = (1.0, 1.0, 1.0)
+    radius: float = 0.0
+    size_u: float = 1.0
+    size_v: float = 1.0
+    spot_angle: float = math.pi / 4
+    spot_smooth: float = 0.0
+    angle: float = 0.0
+    flags: int = _abi.LIGHT_FLAG_NORMALIZE
+    max_bounces: int = 1024
+
+
+@dataclasses.dataclass
+class Camera:
+    transform: np.ndarray  # camera-to-world 4x4 (column vectors)
+    field_of_view: float = math.radians(40.0)
+    horizontal_field_of_view: float = math.radians(40.0)
+    sensor_fit: int = 2  # vertical
+    lens_shift_x: float = 0.0
+    lens_shift_y: float = 0.0
+    near_clip: float = 1.0e-4
+    far_clip: float = 1.0e5
+
+
+@dataclasses.dataclass
+class Scene:
+    meshes: list[Mesh]
+    instances: list[Instance]
+    materials: list[CompiledMaterial]
+    lights: list[Light]
+    camera: Camera
+    background: tuple = (0.0, 0.0, 0.0)
+    world_visibility: int = _abi.VIS_ALL
+    revision: int = 1
+
+    @property
+    def instanced_triangles(self) -> int:
+        return sum(self.meshes[i.mesh].triangle_count for i in self.instances)
+
+    def to_desc(self) -> "SceneDescHandle":
+        return SceneDescHandle(self)
+
+
+def _column_major(m: np.ndarray) -> list[float]:
+    """4x4 row-major numpy matrix (column vectors) -> Mat4f element order."""
+    return [float(v) for v in np.asarray(m, dtype=np.float64).T.reshape(-1)]
+
+
+class SceneDescHandle:
+    """A psy_scene_desc plus the arrays it points into (kept alive here)."""
+
+    def __init__(self, scene: Scene):
+        keep = []
+        meshes = (_abi.MeshDesc * max(len(scene.meshes), 1))()
+        for i, m in enumerate(scene.meshes):
+            p = np.ascontiguousarray(m.positions, dtype=np.float32)
+            idx = np.ascontiguousarray(m.indices, dtype=np.uint32)
+            n = None if m.normals is None else np.ascontiguousarray(m.normals, dtype=np.float32)
+            mats = None if m.materials is None else np.ascontiguousarray(m.materials, dtype=np.uint32)
+            keep += [p, idx, n, mats]
+            meshes[i].positions = _abi.ptr(p)
+            meshes[i].normals = _abi.ptr(n)
+            meshes[i].indices = _abi.ptr(idx, ctypes.c_uint32)
+            meshes[i].materials = _abi.ptr(mats, ctypes.c_uint32)
+            meshes[i].vertex_count = p.shape[0]
+            meshes[i].triangle_count = idx.shape[0]
+            meshes[i].smooth = 1 if n is not None else 0
+        instances = (_abi.InstanceDesc * max(len(scene.instances), 1))()
+        for i, inst in enumerate(scene.instances):
+            instances[i].object_to_world[:] = _column_major(inst.transform)
+            instances[i].mesh = inst.mesh
+            instances[i].material = inst.material
+            instances[i].visibility = inst.visibility
+        materials = (_abi.MaterialDesc * max(len(scene.materials), 1))()
+        for i, cm in enumerate(scene.materials):
+            code = np.ascontiguousarray(cm.program.closures, dtype=np.uint32)
+            sc = np.ascontiguousarray(cm.parameters.scalars, dtype=np.float32)
+            vc = np.ascontiguousarray(cm.parameters.vectors, dtype=np.float32).reshape(-1)
+            keep += [code, sc, vc]
+            materials[i].closures = code.ctypes.data_as(ctypes.POINTER(_abi.ClosureInstruction))
+            materials[i].closure_count = code.shape[0]
+            materials[i].root = cm.program.root
+            materials[i].scalars = _abi.ptr(sc)
+            materials[i].scalar_count = sc.shape[0]
+            materials[i].vectors = _abi.ptr(vc)
+            materials[i].vector_count = vc.shape[0] // 3
+            materials[i].emission_sampling = cm.emission_sampling
+        lights = (_abi.LightDesc * max(len(scene.lights), 1))()
+        for i, l in enumerate(scene.lights):
+            d = lights[i]
+            d.type, d.flags, d.max_bounces = l.type, l.flags, l.max_bounces
+            d.position[:] = l.position
+            d.axis_x[:] = l.axis_x
+            d.axis_y[:] = l.axis_y
+            d.axis_z[:] = l.axis_z
+            d.axis_scale[:] = l.axis_scale
+            d.color[:] = l.color
+            d.power, d.radius, d.size_u, d.size_v = l.power, l.radius, l.size_u, l.size_v
+            d.spot_angle, d.spot_smooth, d.angle = l.spot_angle, l.spot_smooth, l.angle
+        desc = _abi.SceneDesc()
+        desc.meshes, desc.instances, desc.materials, desc.lights = meshes, instances, materials, lights
+        desc.mesh_count = len(scene.meshes)
+        desc.instance_count = len(scene.instances)
+        desc.material_count = len(scene.materials)
+        desc.light_count = len(scene.lights)
+        cam = scene.camera
+        desc.camera.camera_to_world[:] = _column_major(cam.transform)
+        desc.camera.field_of_view = cam.field_of_view
+        desc.camera.horizontal_field_of_view = cam.horizontal_field_of_view
+        desc.camera.sensor_fit = cam.sensor_fit
+        desc.camera.lens_shift_x, desc.camera.lens_shift_y = cam.lens_shift_x, cam.lens_shift_y
+        desc.camera.near_clip, desc.camera.far_clip = cam.near_clip, cam.far_clip
+        desc.background[:] = scene.background
+        desc.world_visibility = scene.world_visibility
+        desc.revision = scene.revision
+        self.desc = desc
+        self._keep = (keep, meshes, instances, materials, lights)
+
+    @property
+    def pointer(self):
+        return ctypes.byref(self.desc)
+
+
+# ------------------------------------------------------------ transforms
+
+def translate(x, y, z) -> np.ndarray:
+    m = np.eye(4)
+    m[:3, 3] = (x, y, z)
+    return m
+
+
+def rotate_y(angle: float) -> np.ndarray:
+    c, s = math.cos(angle), math.sin(angle)
+    m = np.eye(4)
+    m[0, 0], m[0, 2], m[2, 0], m[2, 2] = c, s, -s, c
+    return m
+
+
+def scale(x, y, z) -> np.ndarray:
+    return np.diag([x, y, z, 1.0])
+
+
+def look_at(eye, target, up=(0.0, 1.0, 0.0)) -> np.ndarray:
+    """Camera-to-world matrix: the camera looks down its local -Z."""
+    eye, target, up = (np.asarray(v, dtype=np.float64) for v in (eye, target, up))
+    f = target - eye
+    f /= np.linalg.norm(f)
+    r = np.cross(f, up)
+    r /= np.linalg.norm(r)
+    u = np.cross(r, f)
+    m = np.eye(4)
+    m[:3, 0], m[:3, 1], m[:3, 2], m[:3, 3] = r, u, -f, eye
+    return m
+
+
+def random_rotation(rng: np.random.Generator) -> np.ndarray:
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    m = np.eye(4)
+    m[:3, :3] = [[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                 [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                 [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]]
+    return m
+
+
+# ----------------------------------------------------------------- meshes
+
+def quad(p0, p1, p2, p3) -> Mesh:
+    """Two triangles (p0, p1, p2), (p0, p2, p3)."""
+    pos = np.array([p0, p1, p2, p3], dtype=np.float32)
+    return Mesh(pos, np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+
+
+def box_mesh(size=1.0) -> Mesh:
+    h = size / 2.0
+    v = np.array([[-h, -h, -h], [h, -h, -h], [h, h, -h], [-h, h, -h],
+                  [-h, -h, h], [h, -h, h], [h, h, h], [-h, h, h]], dtype=np.float32)
+    faces = [(0, 3, 2, 1), (4, 5, 6, 7), (0, 4, 7, 3), (1, 2, 6, 5), (0, 1, 5, 4), (3, 7, 6, 2)]
+    idx = []
+    for a, b, c, d in faces:
+        idx += [(a, b, c), (a, c, d)]
+    return Mesh(v, np.array(idx, dtype=np.uint32))
+
+
+def geodesic_sphere(frequency: int) -> Mesh:
+    """Icosahedron with each face split into frequency^2 triangles, projected
+    to the unit sphere; smooth normals are the positions."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    verts = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t],
+                      [0, -1, -t], [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], dtype=np.float64)
+    verts /= np.linalg.norm(verts, axis=1, keepdims=True)
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+             (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    n = frequency
+    positions = []
+    indices = []
+    for a, b, c in faces:
+        A, B, C = verts[a], verts[b], verts[c]
+        base = len(positions)
+        row_start = []
+        for i in range(n + 1):
+            row_start.append(len(positions) - base)
+            for j in range(n + 1 - i):
+                p = A + (B - A) * (i / n) + (C - A) * (j / n)
+                positions.append(p / np.linalg.norm(p))
+        for i in range(n):
+            for j in range(n - i):
+                v0 = base + row_start[i] + j
+                v1 = base + row_start[i + 1] + j
+                v2 = base + row_start[i] + j + 1
+                indices.append((v0, v1, v2))
+                if j < n - i - 1:
+                    v3 = base + row_start[i + 1] + j + 1
+                    indices.append((v2, v1, v3))
+    pos = np.array(positions, dtype=np.float32)
+    return Mesh(pos, np.array(indices, dtype=np.uint32), normals=pos.copy())
+
+
+# --------------------------------------------------------------- workloads
+
+def _materials(graphs: list[ShaderGraph], sampling: int = _abi.EMISSION_AUTOMATIC) -> list[CompiledMaterial]:
+    out = []
+    for g in graphs:
+        program, block = compile_surface_program(g)
+        out.append(CompiledMaterial(g, program, block, sampling))
+    return out
+
+
+def cornell_box() -> Scene:
+    """Closed box of 5 axis-aligned quads (2x2x2) + a cube rotated 20 degrees
+    about Y; albedos 0.73 / 0.65 / 0.12 (grey, red, green); a 0.5 x 0.5
+    emissive quad of strength 15 under the ceiling; 40 degree pinhole."""
+    white = (0.73, 0.73, 0.73)
+    red = (0.65, 0.05, 0.05)
+    green = (0.12, 0.45, 0.15)
+    mats = _materials([diffuse_material(white), diffuse_material(red), diffuse_material(green),
+                       emission_material((1.0, 1.0, 1.0), 15.0)])
+    meshes = [
+        quad((-1, 0, -1), (-1, 0, 1), (1, 0, 1), (1, 0, -1)),    # floor, normal +y
+        quad((-1, 2, -1), (1, 2, -1), (1, 2, 1), (-1, 2, 1)),    # ceiling, normal -y
+        quad((-1, 0, -1), (1, 0, -1), (1, 2, -1), (-1, 2, -1)),  # back wall, normal +z
+        quad((-1, 0, -1), (-1, 2, -1), (-1, 2, 1), (-1, 0, 1)),  # left wall, normal +x
+        quad((1, 0, -1), (1, 0, 1), (1, 2, 1), (1, 2, -1)),      # right wall, normal -x
+        box_mesh(0.6),
+        quad((-0.25, 1.98, -0.25), (0.25, 1.98, -0.25), (0.25, 1.98, 0.25), (-0.25, 1.98, 0.25)),  # light
+    ]
+    cube_xf = translate(0.3, 0.3, -0.2) @ rotate_y(math.radians(20.0))
+    instances = [Instance(0, 0), Instance(1, 0), Instance(2, 0), Instance(3, 1), Instance(4, 2),
+                 Instance(5, 0, cube_xf), Instance(6, 3)]
+    cam = Camera(look_at((0.0, 1.0, 3.9), (0.0, 1.0, 0.0)), math.radians(40.0), math.radians(40.0), 0)
+    return Scene(meshes, instances, mats, [], cam, background=(0.0, 0.0, 0.0))
+
+
+def procedural_scene(seed: int = 0, frequencies=(10, 14, 18, 22, 27, 32, 38, 44), instances_per_mesh: int = 8,
+                     material_count: int = 32, lights_per_type: int = 6, light_types=None) -> Scene:
+    """64 seeded affine instances of 8 geodesic spheres (2k-40k triangles,
+    ~1M instanced triangles, smooth normals), 32 random closure graphs over
+    diffuse / emission / transparent / add / mix, point / spot / sun lights
+    and a constant world colour."""
+    rng = np.random.default_rng(seed)
+    meshes = [geodesic_sphere(f) for f in frequencies]
+    graphs = [random_material(rng, emission_probability=0.05) for _ in range(material_count)]
+    mats = _materials(graphs)
+    instances = []
+    for mi in range(len(meshes)):
+        for _ in range(instances_per_mesh):
+            s = rng.uniform(0.6, 1.8)
+            sx, sy, sz = s * rng.uniform(0.8, 1.25, 3)
+            t = rng.uniform((-9, 0.5, -9), (9, 6, 9))
+            xf = translate(*t) @ random_rotation(rng) @ scale(sx, sy, sz)
+            instances.append(Instance(mi, int(rng.integers(0, material_count)), xf))
+    if light_types is None:
+        light_types = (_abi.LIGHT_POINT, _abi.LIGHT_SPOT, _abi.LIGHT_DISTANT)
+    lights = []
+    for lt in light_types:
+        for _ in range(lights_per_type):
+            color = tuple(float(c) for c in rng.uniform(0.5, 1.0, 3))
+            if lt == _abi.LIGHT_DISTANT:
+                d = rng.normal(size=3)
+                d[1] = -abs(d[1]) - 0.5
+                d /= np.linalg.norm(d)
+                lights.append(Light(lt, color, float(rng.uniform(0.5, 2.0)), axis_z=tuple(d.tolist()),
+                                    angle=float(math.radians(rng.uniform(0.5, 5.0)))))
+            else:
+                pos = tuple(rng.uniform((-10, 7, -10), (10, 12, 10)).tolist())
+                xf = look_at(pos, (float(rng.uniform(-4, 4)), 0.0, float(rng.uniform(-4, 4))))
+                lights.append(Light(lt, color, float(rng.uniform(200.0, 800.0)), position=pos,
+                                    axis_x=tuple(xf[:3, 0].tolist()), axis_y=tuple(xf[:3, 1].tolist()),
+                                    axis_z=tuple(xf[:3, 2].tolist()),
+                                    spot_angle=float(math.radians(rng.uniform(30, 90))),
+                                    spot_smooth=float(rng.uniform(0.0, 0.5))))
+    cam = Camera(look_at((0.0, 9.0, 24.0), (0.0, 2.0, 0.0)), math.radians(40.0), math.radians(40.0), 0)
+    return Scene(meshes, instances, mats, lights, cam, background=(0.05, 0.06, 0.08))
+
+
+def many_light_scene(seed: int = 0, boxes: int = 200, emitters: int = 10000, emission_materials: int = 10000) -> Scene:
+    """Ground plane + 200 random boxes (2.4k triangles) + emissive triangles
+    scattered uniformly in a 20^3 volume with log-uniform strengths in
+    [1e-2, 1e2]; Lambertian albedo uniform in [0.2, 0.8]."""
+    rng = np.random.default_rng(seed)
+    mats_graphs = [diffuse_material(tuple(float(a) for a in rng.uniform(0.2, 0.8, 3))) for _ in range(16)]
+    strengths = 10.0 ** rng.uniform(-2.0, 2.0, emission_materials)
+    for s in strengths:
+        mats_graphs.append(emission_material(tuple(float(c) for c in rng.uniform(0.6, 1.0, 3)), float(s)))
+    mats = _materials(mats_graphs)
+    meshes = [quad((-30, 0, -30), (-30, 0, 30), (30, 0, 30), (30, 0, -30)), box_mesh(1.0)]
+    instances = [Instance(0, 0)]
+    for _ in range(boxes):
+        xf = translate(*rng.uniform((-10, 0.5, -10), (10, 3, 10))) @ rotate_y(float(rng.uniform(0, 2 * math.pi))) \
+            @ scale(*rng.uniform(0.3, 2.0, 3))
+        instances.append(Instance(1, int(rng.integers(0, 16)), xf))
+    centers = rng.uniform((-10, 0.5, -10), (10, 20.5, 10), (emitters, 3))
+    offsets = rng.normal(scale=0.15, size=(emitters, 3, 3))
+    pos = (centers[:, None, :] + offsets).reshape(-1, 3).astype(np.float32)
+    idx = np.arange(emitters * 3, dtype=np.uint32).reshape(-1, 3)
+    tri_mats = (16 + rng.integers(0, emission_materials, emitters)).astype(np.uint32)
+    meshes.append(Mesh(pos, idx, materials=tri_mats))
+    instances.append(Instance(2, 16))
+    cam = Camera(look_at((0.0, 12.0, 32.0), (0.0, 5.0, 0.0)), math.radians(45.0), math.radians(45.0), 0)
+    return Scene(meshes, instances, mats, [], cam, background=(0.0, 0.0, 0.0))
+
+
+def small_test_scene(seed: int = 0, transparent: bool = True, lights: bool = True) -> Scene:
+    """A few-hundred-triangle scene exercising every closure, instance
+    transforms, emissive meshes and point / spot / sun lights."""
+    rng = np.random.default_rng(seed)
+    graphs = [diffuse_material((0.7, 0.7, 0.7)), emission_material((1.0, 0.9, 0.8), 6.0)]
+    for _ in range(6):
+        graphs.append(random_material(rng, emission_probability=0.1,
+                                      transparent_probability=0.3 if transparent else 0.0))
+    mats = _materials(graphs)
+    meshes = [quad((-4, 0, -4), (-4, 0, 4), (4, 0, 4), (4, 0, -4)), geodesic_sphere(3), box_mesh(1.0),
+              quad((-0.5, 0, -0.5), (0.5, 0, -0.5), (0.5, 0, 0.5), (-0.5, 0, 0.5))]
+    instances = [Instance(0, 0), Instance(3, 1, translate(0.0, 3.5, 0.0) @ rotate_y(0.3) @ np.diag([1, -1, 1, 1]))]
+    for i in range(6):
+        xf = translate(*rng.uniform((-2.5, 0.5, -2.5), (2.5, 2.0, 2.5))) @ random_rotation(rng) \
+            @ scale(*rng.uniform(0.4, 1.0, 3))
+        instances.append(Instance(1 + (i % 2), 2 + i, xf))
+    ls = []
+    if lights:
+        ls = [Light(_abi.LIGHT_POINT, (1.0, 0.9, 0.8), 80.0, position=(2.0, 4.0, 1.0)),
+              Light(_abi.LIGHT_SPOT, (0.8, 0.9, 1.0), 120.0, position=(-2.0, 4.5, 2.0),
+                    axis_x=(1, 0, 0), axis_y=(0, 0, 1), axis_z=(0, 1, 0), spot_angle=math.radians(70),
+                    spot_smooth=0.3),
+              Light(_abi.LIGHT_DISTANT, (1.0, 1.0, 0.9), 1.5, axis_z=(0.3, -0.9, 0.2), angle=math.radians(3.0))]
+    cam = Camera(look_at((0.0, 3.0, 9.0), (0.0, 1.0, 0.0)), math.radians(40.0), math.radians(40.0), 0)
+    return Scene(meshes, instances, mats, ls, cam, background=(0.1, 0.12, 0.15))
+
+
+def render_settings(width: int, height: int, max_bounces: int = 4, seed: int = 0, **overrides) -> _abi.RenderSettings:
+    s = _abi.default_settings()
+    s.full_width, s.full_height = width, height
+    s.max_bounces = max_bounces
+    s.seed = seed
+    for k, v in overrides.items():
+        setattr(s, k, v)
+    return s
+
+
+class SceneDatabase:
+    """Atomic snapshot store: apply() validates the whole delta and commits a
+    new revision, or raises and keeps the previous snapshot."""
+
+    def __init__(self, scene: Scene):
+        self.snapshot = scene
+
+    def apply(self, material_graphs: dict[int, ShaderGraph] | None = None,
+              instance_transforms: dict[int, np.ndarray] | None = None) -> Scene:
+        nxt = copy.copy(self.snapshot)
+        nxt.materials = list(self.snapshot.materials)
+        nxt.instances = list(self.snapshot.instances)
+        for index, graph in (material_graphs or {}).items():
+            if not 0 <= index < len(nxt.materials):
+                raise ValueError(f"material {index} does not exist")
+            program, block = compile_surface_program(graph)
+            nxt.materials[index] = CompiledMaterial(graph, program, block, nxt.materials[index].emission_sampling)
+        for index, xf in (instance_transforms or {}).items():
+            if not 0 <= index < len(nxt.instances):
+                raise ValueError(f"instance {index} does not exist")
+            xf = np.asarray(xf, dtype=np.float64)
+            if xf.shape != (4, 4) or not np.isfinite(xf).all():
+                raise ValueError("instance transform must be a finite 4x4 matrix")
+            nxt.instances[index] = dataclasses.replace(nxt.instances[index], transform=xf)
+        nxt.revision = self.snapshot.revision + 1
+        self.snapshot = nxt
+        return nxt

@@ -1,0 +1,113 @@
+"""The CPU oracle pinned to the reference's golden vectors: the tabulated
+Sobol LUT fingerprint and rows (tests/test_tabulated_sobol.cpp), the device
+Sobol probe bits and shuffled indices (tests/test_luisa_sobol_fallback.cpp),
+the cosine-hemisphere cases (tests/test_luisa_cycles_sample_mapping.cpp),
+the path-state transitions (tests/test_luisa_cycles_path_state.cpp), and the
+tables the reference's own sampling code produces (oracle/_ref)."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def test_sobol_table_fingerprint(oracle_lib, golden):
+    assert oracle_lib.oracle_sobol_fingerprint(256) == golden["sobol"]["table256_fnv1a"]
+    t = np.zeros(256 * 256 * 4, np.float32)
+    oracle_lib.oracle_sobol_table(256, _p(t))
+    bits = t.view(np.uint32).reshape(-1, 4)
+    assert bits[0].tolist() == golden["sobol"]["table256_row0_bits"]
+    assert bits[1].tolist() == golden["sobol"]["table256_row1_bits"]
+
+
+@pytest.mark.parametrize("samples,size", [(1, 256), (16, 256), (64, 256), (256, 256), (257, 512),
+                                          (4096, 4096), (5000, 8192), (100000, 8192)])
+def test_sequence_size_for_samples(oracle_lib, samples, size):
+    assert oracle_lib.oracle_sobol_sequence_size(samples) == size
+
+
+def test_device_sobol_probe(oracle_lib, golden):
+    probe = golden["sobol"]["device_probe"]
+    t = np.zeros(256 * 256 * 4, np.float32)
+    oracle_lib.oracle_sobol_table(256, _p(t))
+    rows = t.view(np.uint32).reshape(-1, 4)
+    x, y = probe["pixel"]
+    h = oracle_lib.oracle_pixel_hash(x, y, probe["seed"]) & 0xFFFFFFFF
+    assert h == probe["rng_hash"]
+    for (sample, dim), bits, index in zip(probe["queries"], probe["expected_bits"], probe["shuffled_indices"]):
+        i = oracle_lib.oracle_shuffled_sample_index(sample, dim, h, 256)
+        assert i == index
+        assert rows[i].tolist() == bits
+
+
+def test_cosine_hemisphere_cases(oracle_lib, golden):
+    cases = golden["sample_mapping"]["cosine_hemisphere"]
+    tol = golden["sample_mapping"]["tolerance"]
+    assert len(cases) >= 4
+    for c in cases:
+        n = np.array(c["normal"], np.float32)
+        r = np.array(c["random"], np.float32)
+        d = np.zeros(3, np.float32)
+        pdf = np.zeros(1, np.float32)
+        oracle_lib.oracle_sample_cosine_hemisphere(_p(n), _p(r), _p(d), _p(pdf))
+        exp = np.array(c["direction"], np.float32)
+        assert np.all(np.abs(d - exp) <= tol * np.maximum(1.0, np.maximum(np.abs(d), np.abs(exp)))), (d, exp)
+        assert abs(pdf[0] - c["pdf"]) <= tol * max(1.0, abs(c["pdf"]))
+
+
+def test_path_state_transitions(oracle_lib, golden):
+    ps = golden["path_state"]
+    names = ["flag", "visibility", "bounce", "diffuse_bounce", "glossy_bounce", "transmission_bounce",
+             "transparent_bounce", "rng_offset"]
+    results = {}
+    for c in ps["cases"]:
+        state = np.array(c["state"], np.uint32)
+        limits = np.array(c["limits"], np.uint32)
+        out = np.zeros(8, np.uint32)
+        oracle_lib.oracle_next_surface(_p(state), c["label"], c["runtime"], _p(limits), _p(out))
+        got = dict(zip(names, out.tolist()))
+        results[c["name"]] = out
+        for k, v in c["expect"].items():
+            if k == "contract_visibility":
+                assert oracle_lib.oracle_contract_visibility(got["visibility"]) == v
+            else:
+                assert got[k] == v, (c["name"], k, got[k], v)
+    # two transparent transitions consume two 16-dimension blocks
+    once = results["transparent"]
+    limits = np.array([8, 8, 8, 8, 8], np.uint32)
+    out = np.zeros(8, np.uint32)
+    oracle_lib.oracle_next_surface(_p(once), 32, 8 | 1024, _p(limits), _p(out))
+    tw = ps["transparent_twice"]
+    assert out[7] == tw["rng_offset"] and out[7] + 1 == tw["light_dimension"]
+    assert out[2] == tw["bounce"] and out[6] == tw["transparent_bounce"]
+    assert oracle_lib.oracle_contract_visibility(2 | 4 | 8) == ps["contract_visibility_transmit_diffuse_glossy"]
+
+
+def test_pixel_filter_tables_match_reference(oracle_lib, golden):
+    ref = golden["reference_tables"]["pixel_filter_bits_every37"]
+    for key, bits in ref.items():
+        f, w = key.split(":")
+        t = np.zeros(1024, np.float32)
+        oracle_lib.oracle_pixel_filter_table(int(f), ctypes.c_float(float(w)), _p(t))
+        assert t.view(np.uint32)[::37].tolist() == bits, key
+
+
+def test_reference_library_tables_when_built():
+    """Cross-checks against the reference's own sampling code compiled into
+    oracle/_ref (present where the reference tree was available)."""
+    if not oracle.REF_LIB.exists():
+        pytest.skip("oracle/_ref not built")
+    ref = ctypes.CDLL(str(oracle.REF_LIB))
+    lib = oracle.load()
+    for size in (256, 512):
+        a = np.zeros(size * 256 * 4, np.float32)
+        b = np.zeros_like(a)
+        lib.oracle_sobol_table(size, _p(a))
+        assert ref.ref_sobol_generate_table(size, _p(b)) == 0
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
