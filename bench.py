@@ -1,0 +1,354 @@
+"""Throughput benchmark of the B200 path tracer.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+                    [--config procedural|cornell|many_light] [--spp S]
+
+Workload (default): the procedural mesh scene -- 64 seeded affine instances
+of 8 geodesic spheres (997,920 instanced fp32 triangles, smooth normals), 32
+random closure graphs over diffuse / emission / transparent / add / mix,
+point / spot / sun lights, constant world colour -- rendered at 1920x1080,
+64 spp, max 8 bounces.  One step renders that whole frame
+(RenderSession.render_samples over all 64 samples).  The metric is
+samples/s (pixels x spp / render seconds) with rays/s beside it.
+
+`value` is device time (CUDA events on the session stream around each
+render_samples call, max over ranks); `e2e` is the public API per step:
+compile_scene from host arrays (geometry upload + BVH build), create_session,
+render_samples, and the read of every pass back to host memory.  Under
+torchrun each rank renders its own frame (seed = rank) on its own GPU: the
+work shards by frame with no data-path collective (weak scaling).
+
+--impl reference times the reference path's CPU restatement (the oracle,
+all host threads) on a bounded row band of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CONFIGS = {
+    "procedural": dict(width=1920, height=1080, spp=64, bounces=8),
+    "cornell": dict(width=256, height=256, spp=16, bounces=4),
+    "many_light": dict(width=1280, height=720, spp=32, bounces=6),
+}
+
+
+def make_scene(name: str, seed: int = 0):
+    from psycles_b200 import scenes
+    if name == "procedural":
+        return scenes.procedural_scene(seed=0)
+    if name == "cornell":
+        return scenes.cornell_box()
+    return scenes.many_light_scene(seed=0)
+
+
+def workload_config(args, scene) -> dict:
+    c = CONFIGS[args.config]
+    return {"workload": f"{args.config} scene {c['width']}x{c['height']} {args.spp} spp max {c['bounces']} bounces",
+            "width": c["width"], "height": c["height"], "spp": args.spp, "max_bounces": c["bounces"],
+            "instanced_triangles": scene.instanced_triangles, "instances": len(scene.instances),
+            "materials": len(scene.materials), "analytic_lights": len(scene.lights),
+            "l2_policy": "scene geometry + BVH (~150 MB) and per-path state (~400 MB) exceed the 126 MB L2"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "fallback": True}
+
+
+def cpu_baseline(args, scene, seconds_budget: float = 15.0) -> dict:
+    """The oracle (CPU restatement of the reference path) on a bounded row band."""
+    from oracle.oracle import OracleFilm
+    from psycles_b200 import scenes
+    c = CONFIGS[args.config]
+    desc = scene.to_desc()
+    cores = os.cpu_count() or 1
+    rows, spp = 8, 1
+    while True:
+        st = scenes.render_settings(c["width"], c["height"], max_bounces=c["bounces"], window_y=c["height"] // 2,
+                                    window_height=rows)
+        film = OracleFilm(st)
+        t0 = time.perf_counter()
+        film.render(desc, 0, spp, args.spp, threads=cores)
+        dt = time.perf_counter() - t0
+        if dt * 2.5 > seconds_budget or rows >= c["height"] // 2:
+            break
+        rows = min(rows * 2, c["height"] // 2)
+    samples = c["width"] * rows * spp
+    return {"value": samples / dt, "unit": "samples/s", "cores": cores, "kind": "port",
+            "sample": f"{c['width']}x{rows} centre rows, samples {0}..{spp - 1} of {args.spp}, "
+                      f"{samples} samples in {dt:.2f} s (scene prep + BVH build included)"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    scene = make_scene(args.config)
+    base = cpu_baseline(args, scene)
+    times = []
+    for _ in range(args.warmup + args.steps):
+        b = cpu_baseline(args, scene, seconds_budget=max(4.0, 40.0 / max(args.steps + args.warmup, 1)))
+        times.append(b["value"])
+    vals = times[args.warmup:]
+    value = statistics.mean(vals)
+    c = CONFIGS[args.config]
+    line = {"impl": "reference", "metric": "samples/s", "value": value, "unit": "samples/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": c["width"] * c["height"] * args.spp / value * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args, scene),
+            "cpu_baseline": {"value": value, "unit": "samples/s", "cores": base["cores"], "kind": "port",
+                             "sample": base["sample"]},
+            "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def scene_bytes(scene) -> int:
+    total = 0
+    for m in scene.meshes:
+        total += m.positions.nbytes + m.indices.nbytes
+        total += 0 if m.normals is None else m.normals.nbytes
+        total += 0 if m.materials is None else m.materials.nbytes
+    total += len(scene.instances) * 80
+    for cm in scene.materials:
+        total += cm.program.closures.nbytes + cm.parameters.scalars.nbytes + cm.parameters.vectors.nbytes
+    return total
+
+
+def run_cuda(args) -> None:
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist = dist_mod
+    from psycles_b200 import _abi, scenes
+    from psycles_b200.backend import CudaPathTracerBackend, SampleRange
+
+    c = CONFIGS[args.config]
+    scene = make_scene(args.config)
+    backend = CudaPathTracerBackend(local)
+    settings = lambda: scenes.render_settings(c["width"], c["height"], max_bounces=c["bounces"], seed=rank)
+    comp = backend.compile_scene(scene)
+    if not comp.ok():
+        raise SystemExit(f"compile_scene failed: {comp.diagnostics}")
+    session = backend.create_session(comp.scene, settings())
+    pixels = c["width"] * c["height"]
+    samples_per_step = pixels * args.spp
+
+    def step():
+        session.reset(settings())
+        ok = session.render_samples(SampleRange(0, args.spp, 0, args.spp))
+        if not ok:
+            raise SystemExit(f"render failed: {session.diagnostics}")
+        return session.stats()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    ms, rays, launches, seg = [], 0, 0, 0
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            s = step()
+            ms.append(s.ms_total)
+            rays += s.closest_rays + s.shadow_rays
+            launches += s.kernel_launches
+            seg += s.path_segments
+        wall = time.perf_counter() - t0
+    barrier()
+    device_s = max_over_ranks(sum(ms) / 1e3)
+    value = samples_per_step * args.steps * world / device_s
+    rays_per_s = max_over_ranks(rays / (sum(ms) / 1e3)) * world if rays else 0.0
+
+    # roofline of the dominant kernel (closest-hit traversal): algorithmic
+    # bytes per ray = ray 32 B + path state 32 B + queue index 4 B read,
+    # hit 20 B written, plus the scene's unique geometry once per launch.
+    peaks = measured_peaks()
+    kernel = {}
+    if args.kernel_timing:
+        kernel = kernel_profile(args, backend, comp.scene, settings())
+
+    # e2e: host arrays -> compile_scene -> render -> passes in host memory
+    e2e_ms = []
+    d2h = 0
+    for _ in range(max(1, min(args.steps, 2))):
+        barrier()
+        t0 = time.perf_counter()
+        comp2 = backend.compile_scene(scene)
+        sess2 = backend.create_session(comp2.scene, settings())
+        assert sess2.render_samples(SampleRange(0, args.spp, 0, args.spp))
+        d2h = 0
+        for p in sess2.passes:
+            d2h += sess2.read_pass(p.kind).nbytes
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        sess2.close()
+        comp2.scene.close()
+    e2e_s = max_over_ranks(statistics.mean(e2e_ms) / 1e3)
+    e2e_value = samples_per_step * world / e2e_s
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    line = {
+        "metric": "samples/s", "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": device_s * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args, scene),
+        "rays_per_s": rays_per_s, "wall_s": wall,
+        "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": scene_bytes(scene),
+                "d2h_bytes_per_step": d2h, "includes": "compile_scene (upload + BVH build), render, pass readback"},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    if kernel:
+        line["roofline"] = kernel["roofline"]
+        line["kernels"] = kernel["kernels"]
+    if args.cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, scene)
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def kernel_profile(args, backend, compiled, settings) -> dict:
+    """Per-kernel device time of one render with CUDA events around each
+    launch class (psy_session profile mode)."""
+    from psycles_b200 import _abi
+    from psycles_b200.backend import SampleRange
+    lib = backend.context.lib
+    if not hasattr(lib, "psy_session_profile"):
+        return {}
+    sess = backend.create_session(compiled, settings)
+    prof = _abi.KernelProfile()
+    _abi.check(lib.psy_session_set_profiling(sess.handle, 1))
+    assert sess.render_samples(SampleRange(0, args.spp, 0, args.spp))
+    _abi.check(lib.psy_session_profile(sess.handle, __import__("ctypes").byref(prof)))
+    sess.close()
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    kernels = {}
+    for name in ("raygen", "intersect", "shade", "shadow", "film"):
+        launches = getattr(prof, f"{name}_launches")
+        ms = getattr(prof, f"{name}_ms")
+        nbytes = getattr(prof, f"{name}_bytes")
+        kernels[name] = {"launches": launches, "ms": ms,
+                         "gbs": (nbytes / (ms / 1e3) / 1e9) if ms > 0 else 0.0, "algorithmic_bytes": nbytes}
+    top = max(kernels, key=lambda k: kernels[k]["ms"])
+    k = kernels[top]
+    achieved = k["gbs"]
+    return {"kernels": kernels,
+            "roofline": {"kernel": f"k_{top}", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None,
+                         "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if not peaks.get("fallback")
+                         else "fallback 6.65 TB/s"}}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--config", default="procedural", choices=sorted(CONFIGS))
+    ap.add_argument("--spp", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-kernel-timing", dest="kernel_timing", action="store_false")
+    args = ap.parse_args()
+    if args.spp is None:
+        args.spp = CONFIGS[args.config]["spp"]
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_cuda(args)
+
+
+if __name__ == "__main__":
+    main()

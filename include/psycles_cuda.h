@@ -380,6 +380,37 @@ typedef struct psy_render_stats {
 psy_status psy_session_stats(const psy_session *session,
                              psy_render_stats *out);
 
+/* Per-kernel-class device time of the last render_samples call in profiling
+ * mode (CUDA events around every launch; one host synchronisation per path
+ * step) and the algorithmic HBM bytes each class moved: the path-state,
+ * ray, hit, queue, shadow and film records it must read and write, counted
+ * from the live queue sizes.  No reference counterpart: measurement
+ * support for the roofline report. */
+typedef struct psy_kernel_profile {
+    uint32_t raygen_launches;
+    uint32_t intersect_launches;
+    uint32_t shade_launches;
+    uint32_t shadow_launches;
+    uint32_t film_launches;
+    uint32_t reserved;
+    float raygen_ms;
+    float intersect_ms;
+    float shade_ms;
+    float shadow_ms;
+    float film_ms;
+    float reserved_ms;
+    double raygen_bytes;
+    double intersect_bytes;
+    double shade_bytes;
+    double shadow_bytes;
+    double film_bytes;
+    double reserved_bytes;
+} psy_kernel_profile;
+
+psy_status psy_session_set_profiling(psy_session *session, uint32_t enabled);
+psy_status psy_session_profile(const psy_session *session,
+                               psy_kernel_profile *out);
+
 /* ------------------------------------------- host precompute (no GPU) -- */
 
 /* tabulated_sobol::sequence_size_for_samples

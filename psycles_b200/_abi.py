@@ -122,6 +122,15 @@ class RenderStats(ctypes.Structure):
                 ("kernel_launches", ctypes.c_uint32), ("batches", ctypes.c_uint32)]
 
 
+class KernelProfile(ctypes.Structure):
+    _fields_ = [(n + "_launches", ctypes.c_uint32) for n in ("raygen", "intersect", "shade", "shadow", "film")] + [
+        ("reserved", ctypes.c_uint32)] + [
+        (n + "_ms", ctypes.c_float) for n in ("raygen", "intersect", "shade", "shadow", "film")] + [
+        ("reserved_ms", ctypes.c_float)] + [
+        (n + "_bytes", ctypes.c_double) for n in ("raygen", "intersect", "shade", "shadow", "film")] + [
+        ("reserved_bytes", ctypes.c_double)]
+
+
 # Entry points declared by include/psycles_cuda.h: (name, restype, argtypes).
 SIGNATURES = [
     ("psy_last_error", ctypes.c_char_p, []),
@@ -147,6 +156,8 @@ SIGNATURES = [
     ("psy_session_request_trace", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
     ("psy_session_read_trace", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PathTrace)]),
     ("psy_session_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RenderStats)]),
+    ("psy_session_set_profiling", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    ("psy_session_profile", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(KernelProfile)]),
     ("psy_sobol_sequence_size_for_samples", ctypes.c_uint32, [ctypes.c_uint32]),
     ("psy_sobol_generate_table", ctypes.c_int, [ctypes.c_uint32, c_float_p]),
     ("psy_pixel_filter_table", ctypes.c_int, [ctypes.c_uint32, ctypes.c_float, c_float_p]),

@@ -487,133 +487,144 @@ __device__ __forceinline__ BvhNodeGpu load_node(const BvhNodeGpu *nodes, int idx
     return n;
 }
 
-constexpr int kStackSize = 64;
+constexpr int kStackSize = 48;
+
+// Stack entries carry a 2-bit tag: a TLAS node, a BLAS node (global index),
+// an instance to enter, or the marker that returns to the world ray.
+constexpr uint32_t kTagTlas = 0u, kTagBlas = 1u << 30, kTagInstance = 2u << 30, kTagLeave = 3u << 30;
+constexpr uint32_t kTagMask = 3u << 30;
+
+struct SlabRay {
+    f3 o, d, inv, oinv;  // origin, clamped direction, reciprocal, origin * reciprocal
+};
+
+__device__ __forceinline__ SlabRay make_slab_ray(f3 o, f3 raw) {
+    SlabRay r;
+    r.o = o;
+    r.d = mk3(clamp_bvh_direction(raw.x), clamp_bvh_direction(raw.y), clamp_bvh_direction(raw.z));
+    r.inv = mk3(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
+    r.oinv = mk3(o.x * r.inv.x, o.y * r.inv.y, o.z * r.inv.z);
+    return r;
+}
+
+// Two-level traversal in one loop: TLAS and BLAS nodes share the loop body
+// so the lanes of a warp stay on the same instruction stream while their
+// rays sit at different levels.  Every triangle accepted by the Pluecker
+// predicate in [tmin, tmax] (tmax shrinks through `tmax`) that is neither
+// the source nor the light identity is handed to `on_hit(instance, local,
+// cycles_prim, t, u, v)`; a true return ends the traversal.
+template <typename OnHit>
+__device__ __forceinline__ void traverse_scene(const SceneView &s, const Ray &ray, uint32_t visibility,
+                                               uint32_t src_obj, uint32_t src_prim, uint32_t light_obj,
+                                               uint32_t light_prim, float &tmax, OnHit on_hit) {
+    if (s.instance_count == 0u) return;
+    const SlabRay world = make_slab_ray(ray.o, ray.d);
+    SlabRay cur = world;
+    uint32_t stack[kStackSize];
+    int sp = 0;
+    uint32_t node = kTagTlas;  // TLAS root
+    uint32_t inst = kInvalid, blas_base = 0u, tri_base = 0u, prim_offset = 0u;
+    for (;;) {
+        const uint32_t tag = node & kTagMask;
+        const uint32_t idx = node & ~kTagMask;
+        if (tag == kTagInstance) {
+            const InstanceGpu &in = s.instances[idx];
+            if ((in.visibility & visibility) != 0u) {
+                const MeshGpu mesh = s.meshes[in.mesh];
+                const Xform w2o = load_xform(in.w2o);
+                cur = make_slab_ray(xform_point(w2o, ray.o), xform_direction(w2o, ray.d));
+                inst = idx;
+                blas_base = mesh.node_offset;
+                tri_base = mesh.tri_offset;
+                prim_offset = mesh.prim_offset;
+                if (sp < kStackSize) stack[sp++] = kTagLeave;
+                node = kTagBlas | mesh.node_offset;
+                continue;
+            }
+            if (sp == 0) return;
+            node = stack[--sp];
+            continue;
+        }
+        if (tag == kTagLeave) {
+            cur = world;
+            inst = kInvalid;
+            if (sp == 0) return;
+            node = stack[--sp];
+            continue;
+        }
+        const bool blas = tag == kTagBlas;
+        const BvhNodeGpu n = load_node(blas ? s.blas : s.tlas, int(idx));
+        float ln, rn;
+        bool lh, rh;
+        node_slabs(n, cur.oinv, cur.inv, ray.tmin, tmax, ln, rn, lh, rh);
+        uint32_t next[2];
+        int nc = 0;
+        const bool right_first = rn < ln;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int side = (k == 0) == right_first ? 1 : 0;
+            if (!(side == 0 ? lh : rh)) continue;
+            const int link = side == 0 ? n.child.x : n.child.y;
+            const int count = side == 0 ? n.child.z : n.child.w;
+            if (link >= 0) {
+                next[nc++] = blas ? (kTagBlas | (blas_base + uint32_t(link))) : uint32_t(link);
+                continue;
+            }
+            if (!blas) {
+                if (count > 0) next[nc++] = kTagInstance | uint32_t(~link);
+                continue;
+            }
+            const uint32_t first = tri_base + uint32_t(~link);
+            for (int t = 0; t < count; ++t) {
+                const float4 *tp = s.tris + 3u * (first + uint32_t(t));
+                const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                const uint32_t local = __float_as_uint(a.w);
+                const uint32_t cp = prim_offset + local;
+                if ((src_obj == inst && src_prim == cp) || (light_obj == inst && light_prim == cp)) continue;
+                float th, u, v;
+                if (!intersect_triangle(cur.o, cur.d, ray.tmin, tmax, ld3(a), ld3(b), ld3(c), th, u, v)) continue;
+                if (on_hit(inst, local, cp, th, u, v)) return;
+            }
+        }
+        if (nc == 2) {
+            if (sp < kStackSize) stack[sp++] = next[1];
+            node = next[0];
+        } else if (nc == 1) {
+            node = next[0];
+        } else {
+            if (sp == 0) return;
+            node = stack[--sp];
+        }
+    }
+}
 
 // Closest hit of the whole scene under the Cycles predicate
 // (UnifiedSceneTraversalComponent::trace, src/luisa/path_kernel_scene_traversal.cpp:301-490):
 // closed [tmin, tmax], exclusion of the source and light identities, and
-// equal distances resolved to the greatest (object, primitive).  `any_hit`
-// returns at the first accepted candidate (opaque shadow rays).
+// equal distances resolved to the greatest (object, primitive).
 __device__ __forceinline__ bool trace_closest(const SceneView &s, const Ray &ray, uint32_t visibility,
                                               uint32_t src_obj, uint32_t src_prim, uint32_t light_obj,
-                                              uint32_t light_prim, bool any_hit, Hit &best) {
+                                              uint32_t light_prim, Hit &best) {
     bool has = false;
     best.t = ray.tmax;
     best.u = best.v = 0.0f;
     best.instance = best.prim = best.object = best.cycles_prim = kInvalid;
-    // world-space ray for the TLAS
-    const f3 wd = mk3(clamp_bvh_direction(ray.d.x), clamp_bvh_direction(ray.d.y), clamp_bvh_direction(ray.d.z));
-    const f3 winv = mk3(1.0f / wd.x, 1.0f / wd.y, 1.0f / wd.z);
-    const f3 worg_inv = mk3(ray.o.x * winv.x, ray.o.y * winv.y, ray.o.z * winv.z);
-    int tstack[kStackSize];
-    int tsp = 0;
-    int node = 0;
-    if (s.instance_count == 0u) return false;
-    for (;;) {
-        // TLAS: nodes whose children are instances (leaf count 1, index ~i)
-        const BvhNodeGpu n = load_node(s.tlas, node);
-        const float limit = has ? best.t : ray.tmax;
-        float ln, rn;
-        bool lh, rh;
-        node_slabs(n, worg_inv, winv, ray.tmin, limit, ln, rn, lh, rh);
-        int next = -1;
-        int pending[2];
-        int pc = 0;
-        // order: nearer child first
-        const bool swap = rn < ln;
-        const int first = swap ? 1 : 0;
-        for (int k = 0; k < 2; ++k) {
-            const int side = k == 0 ? first : 1 - first;
-            const bool h = side == 0 ? lh : rh;
-            if (!h) continue;
-            const int c = side == 0 ? n.child.x : n.child.y;
-            const int cnt = side == 0 ? n.child.z : n.child.w;
-            if (c >= 0) {
-                pending[pc++] = c;
-                continue;
-            }
-            // instance leaves
-            for (int li = 0; li < cnt; ++li) {
-                const uint32_t ii = uint32_t(~c) + uint32_t(li);
-                const InstanceGpu &inst = s.instances[ii];
-                if ((inst.visibility & visibility) == 0u) continue;
-                const MeshGpu mesh = s.meshes[inst.mesh];
-                const Xform w2o = load_xform(inst.w2o);
-                const f3 o = xform_point(w2o, ray.o);
-                const f3 rdir = xform_direction(w2o, ray.d);
-                const f3 d = mk3(clamp_bvh_direction(rdir.x), clamp_bvh_direction(rdir.y), clamp_bvh_direction(rdir.z));
-                const f3 inv = mk3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-                const f3 org_inv = mk3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
-                int bstack[kStackSize];
-                int bsp = 0;
-                int bnode = int(mesh.node_offset);
-                for (;;) {
-                    const BvhNodeGpu b = load_node(s.blas, bnode);
-                    const float blimit = has ? best.t : ray.tmax;
-                    float bln, brn;
-                    bool blh, brh;
-                    node_slabs(b, org_inv, inv, ray.tmin, blimit, bln, brn, blh, brh);
-                    int bpending[2];
-                    int bpc = 0;
-                    const bool bswap = brn < bln;
-                    const int bfirst = bswap ? 1 : 0;
-                    for (int k2 = 0; k2 < 2; ++k2) {
-                        const int side = k2 == 0 ? bfirst : 1 - bfirst;
-                        const bool h = side == 0 ? blh : brh;
-                        if (!h) continue;
-                        const int c2 = side == 0 ? b.child.x : b.child.y;
-                        const int cnt2 = side == 0 ? b.child.z : b.child.w;
-                        if (c2 >= 0) {
-                            bpending[bpc++] = int(mesh.node_offset) + c2;
-                            continue;
-                        }
-                        const uint32_t first_tri = mesh.tri_offset + uint32_t(~c2);
-                        for (int ti = 0; ti < cnt2; ++ti) {
-                            const float4 *tp = s.tris + 3u * (first_tri + uint32_t(ti));
-                            const float4 a = __ldg(tp), bb = __ldg(tp + 1), cc = __ldg(tp + 2);
-                            const uint32_t local = __float_as_uint(a.w);
-                            const uint32_t cp = mesh.prim_offset + local;
-                            if ((src_obj == ii && src_prim == cp) || (light_obj == ii && light_prim == cp)) continue;
-                            float t, u, v;
-                            const float tmax_test = has ? best.t : ray.tmax;
-                            if (!intersect_triangle(o, d, ray.tmin, tmax_test, ld3(a), ld3(bb), ld3(cc), t, u, v))
-                                continue;
-                            const bool later = ii > best.object || (ii == best.object && cp > best.cycles_prim);
-                            if (has && !(t < best.t || (t == best.t && later))) continue;
-                            has = true;
-                            best.t = t;
-                            best.u = u;
-                            best.v = v;
-                            best.instance = ii;
-                            best.prim = local;
-                            best.object = ii;
-                            best.cycles_prim = cp;
-                            if (any_hit) return true;
-                        }
-                    }
-                    if (bpc == 2) {
-                        if (bsp < kStackSize) bstack[bsp++] = bpending[1];
-                        bnode = bpending[0];
-                    } else if (bpc == 1) {
-                        bnode = bpending[0];
-                    } else {
-                        if (bsp == 0) break;
-                        bnode = bstack[--bsp];
-                    }
-                }
-            }
-        }
-        if (pc == 2) {
-            if (tsp < kStackSize) tstack[tsp++] = pending[1];
-            next = pending[0];
-        } else if (pc == 1) {
-            next = pending[0];
-        } else {
-            if (tsp == 0) break;
-            next = tstack[--tsp];
-        }
-        node = next;
-    }
+    float tmax = ray.tmax;
+    traverse_scene(s, ray, visibility, src_obj, src_prim, light_obj, light_prim, tmax,
+                   [&](uint32_t ii, uint32_t local, uint32_t cp, float t, float u, float v) {
+                       const bool later = ii > best.object || (ii == best.object && cp > best.cycles_prim);
+                       if (has && !(t < best.t || (t == best.t && later))) return false;
+                       has = true;
+                       best.t = t;
+                       best.u = u;
+                       best.v = v;
+                       best.instance = ii;
+                       best.prim = local;
+                       best.object = ii;
+                       best.cycles_prim = cp;
+                       tmax = t;
+                       return false;
+                   });
     return has;
 }
 

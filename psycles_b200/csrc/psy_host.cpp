@@ -444,6 +444,9 @@ struct psy_session {
     psy_path_trace trace_host{};
     psy_render_stats last_stats{};
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+    bool profiling = false;
+    psy_kernel_profile profile{};
+    cudaEvent_t ev_k[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -1002,6 +1005,8 @@ psy_status psy_session_create(psy_scene *scene, const psy_render_settings *setti
     PSY_CUDA_TRY(s->trace_buf.alloc(sizeof(psy_path_trace)));
     PSY_CUDA_TRY(cudaEventCreate(&s->ev_begin));
     PSY_CUDA_TRY(cudaEventCreate(&s->ev_end));
+    PSY_CUDA_TRY(cudaEventCreate(&s->ev_k[0]));
+    PSY_CUDA_TRY(cudaEventCreate(&s->ev_k[1]));
     *out = s.release();
     return PSY_OK;
 }
@@ -1011,6 +1016,8 @@ void psy_session_destroy(psy_session *s) {
     cudaSetDevice(s->scene->context->device);
     if (s->ev_begin) cudaEventDestroy(s->ev_begin);
     if (s->ev_end) cudaEventDestroy(s->ev_end);
+    for (cudaEvent_t e : s->ev_k)
+        if (e) cudaEventDestroy(e);
     delete s;
 }
 
@@ -1083,6 +1090,32 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
     psy_render_stats stats{};
     PSY_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
     const int sms = ctx->sms;
+    const bool prof = s->profiling;
+    if (prof) std::memset(&s->profile, 0, sizeof(s->profile));
+    // Times one launch class when profiling: events on both sides, then a
+    // synchronisation so the queue sizes the byte model needs are final.
+    auto timed = [&](auto &&launch, uint32_t &launches, float &ms) -> psy_status {
+        if (!prof) {
+            launch();
+            return PSY_OK;
+        }
+        PSY_CUDA_TRY(cudaEventRecord(s->ev_k[0], st));
+        launch();
+        PSY_CUDA_TRY(cudaEventRecord(s->ev_k[1], st));
+        PSY_CUDA_TRY(cudaEventSynchronize(s->ev_k[1]));
+        float t = 0.0f;
+        PSY_CUDA_TRY(cudaEventElapsedTime(&t, s->ev_k[0], s->ev_k[1]));
+        ms += t;
+        launches += 1u;
+        return PSY_OK;
+    };
+    auto read_counters = [&](uint32_t *c3) -> psy_status {
+        PSY_CUDA_TRY(cudaMemcpyAsync(c3, s->paths.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        PSY_CUDA_TRY(cudaStreamSynchronize(st));
+        return PSY_OK;
+    };
+    psy_kernel_profile &pf = s->profile;
+    psy_status ps = PSY_OK;
     for (uint64_t sample = begin; sample < end;) {
         if (s->cancelled.load()) return fail(PSY_ERROR_CANCELLED, "session cancelled");
         const uint32_t n_samples = uint32_t(std::min<uint64_t>(per_batch, end - sample));
@@ -1094,15 +1127,31 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
             const uint32_t local = (s->trace_y - p.win_y) * p.win_w + (s->trace_x - p.win_x);
             trace_path = uint32_t(s->trace_sample - sample) * pixels + local;
         }
+        psy_path_trace *tr = trace_path != psy::kInvalidId ? trace : nullptr;
         psy::PathBuffers b = s->paths;
         psy::launch_set_counters(st, b.counters, paths);
-        psy::launch_raygen(st, sms, p, b, pixels, paths, uint32_t(sample), trace_path, trace_path != psy::kInvalidId ? trace : nullptr);
+        if ((ps = timed([&] { psy::launch_raygen(st, sms, p, b, pixels, paths, uint32_t(sample), trace_path, tr); },
+                        pf.raygen_launches, pf.raygen_ms)) != PSY_OK)
+            return ps;
+        pf.raygen_bytes += 164.0 * paths;
         stats.camera_rays += paths;
         for (uint32_t step = 0; step < p.steps; ++step) {
-            psy::launch_intersect(st, sms, s->scene->view, b, paths);
-            psy::launch_shade(st, sms, s->scene->view, p, b, paths, step, trace_path, trace_path != psy::kInvalidId ? trace : nullptr);
+            uint32_t c3[3] = {0u, 0u, 0u};
+            if (prof && (ps = read_counters(c3)) != PSY_OK) return ps;
+            if ((ps = timed([&] { psy::launch_intersect(st, sms, s->scene->view, b, paths); }, pf.intersect_launches,
+                            pf.intersect_ms)) != PSY_OK)
+                return ps;
+            pf.intersect_bytes += 88.0 * c3[0];
+            if ((ps = timed([&] { psy::launch_shade(st, sms, s->scene->view, p, b, paths, step, trace_path, tr); },
+                            pf.shade_launches, pf.shade_ms)) != PSY_OK)
+                return ps;
             psy::launch_count_rays(st, b.counters, s->stats.as<unsigned long long>());
-            psy::launch_shadow(st, sms, s->scene->view, p, b, paths, step, trace_path, trace_path != psy::kInvalidId ? trace : nullptr);
+            if (prof && (ps = read_counters(c3)) != PSY_OK) return ps;
+            pf.shade_bytes += 304.0 * c3[0] + 68.0 * c3[2];
+            if ((ps = timed([&] { psy::launch_shadow(st, sms, s->scene->view, p, b, paths, step, trace_path, tr); },
+                            pf.shadow_launches, pf.shadow_ms)) != PSY_OK)
+                return ps;
+            pf.shadow_bytes += 100.0 * c3[2];
             psy::launch_swap(st, b.counters);
             std::swap(b.queue_in, b.queue_out);
             stats.kernel_launches += 5u;
@@ -1114,9 +1163,12 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
                 if (left == 0u) break;
             }
         }
-        psy::launch_film(st, sms, b, pixels, n_samples, s->combined.as<float4>(), s->normal.as<float4>(),
-                         s->albedo.as<float4>(), s->sample_count.as<uint32_t>(), trace_path,
-                         trace_path != psy::kInvalidId ? trace : nullptr);
+        if ((ps = timed([&] {
+                 psy::launch_film(st, sms, b, pixels, n_samples, s->combined.as<float4>(), s->normal.as<float4>(),
+                                  s->albedo.as<float4>(), s->sample_count.as<uint32_t>(), trace_path, tr);
+             }, pf.film_launches, pf.film_ms)) != PSY_OK)
+            return ps;
+        pf.film_bytes += 48.0 * paths + 104.0 * pixels;
         stats.kernel_launches += 3u;
         stats.batches += 1u;
         sample += n_samples;
@@ -1179,6 +1231,18 @@ psy_status psy_session_read_pass(psy_session *s, uint32_t pass_kind, float *out,
             for (int c = 0; c < 4; ++c) v[c] /= den;
         }
     }
+    return PSY_OK;
+}
+
+psy_status psy_session_set_profiling(psy_session *s, uint32_t enabled) {
+    if (!s) return fail(PSY_ERROR_INVALID_ARGUMENT, "null session");
+    s->profiling = enabled != 0u;
+    return PSY_OK;
+}
+
+psy_status psy_session_profile(const psy_session *s, psy_kernel_profile *out) {
+    if (!s || !out) return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = s->profile;
     return PSY_OK;
 }
 

@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(256) k_intersect(SceneView s, PathBuffers b) {
         const uint4 st2 = b.st2[i];
         Ray ray{mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, d.w};
         Hit h;
-        const bool hit = trace_closest(s, ray, contract_visibility(st.y), st2.y, st2.z, kInvalid, kInvalid, false, h);
+        const bool hit = trace_closest(s, ray, contract_visibility(st.y), st2.y, st2.z, kInvalid, kInvalid, h);
         b.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.instance));
         b.hit_prim[i] = hit ? h.prim : kInvalid;
     }
@@ -523,7 +523,115 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
 }
 
 // ------------------------------------------------------------------ shadow
-// make_trace_shadow_callable (src/luisa/path_tracer_geometry.cpp:75-174).
+// make_trace_shadow_callable (src/luisa/path_tracer_geometry.cpp:75-174)
+// iterates closest hits: a transparent surface multiplies its extinction
+// and advances tmin past its distance, an opaque one or the
+// transparent_max_bounces budget blocks the ray.  The transmittance that
+// loop produces depends only on the set of surfaces in [0, tmax]: zero if
+// any is opaque or if more than (max - depth) surfaces lie on it, else the
+// product in distance order (coincident distances count once, the greatest
+// identity standing for them).  The kernel computes it with one any-hit
+// traversal: it stops at the first opaque surface, collects transparent
+// ones, and multiplies them sorted by distance.  A ray whose surface count
+// outgrows the collector falls back to the iterated closest hit.
+
+constexpr int kShadowList = 8;
+
+__device__ __forceinline__ uint32_t surface_material(const SceneView &s, uint32_t instance, uint32_t local) {
+    const InstanceGpu &inst = s.instances[instance];
+    const MeshGpu mesh = s.meshes[inst.mesh];
+    return mesh.material_offset == kInvalid ? inst.material : s.tri_materials[mesh.material_offset + local];
+}
+
+__device__ f3 shadow_iterated(const SceneView &s, const RenderParams &p, Ray ray, uint4 ids, uint32_t depth) {
+    f3 transmittance = mk3(1.0f);
+    for (uint32_t guard = 0; guard < 4096u; ++guard) {
+        Hit h;
+        if (!trace_closest(s, ray, PSY_VISIBILITY_SHADOW, ids.x, ids.y, ids.z, ids.w, h)) return transmittance;
+        if (depth >= p.transparent_max) return mk3(0.0f);
+        const f3 t = clamp3(transparent_extinction(s, s.materials[surface_material(s, h.instance, h.prim)]), 0.0f, 1.0f);
+        if (!(max_component(t) > 0.0f)) return mk3(0.0f);
+        transmittance = transmittance * t;
+        depth += 1u;
+        ray.tmin = h.t == 0.0f ? 1.17549435e-38f : __uint_as_float(__float_as_uint(h.t) + 1u);
+    }
+    return mk3(0.0f);
+}
+
+__device__ __forceinline__ f3 shadow_transmittance(const SceneView &s, const RenderParams &p, const Ray &ray,
+                                                   uint4 ids, uint32_t depth) {
+    float tmax = ray.tmax;
+    if (!s.any_transparent) {
+        bool blocked = false;
+        traverse_scene(s, ray, PSY_VISIBILITY_SHADOW, ids.x, ids.y, ids.z, ids.w, tmax,
+                       [&](uint32_t, uint32_t, uint32_t, float, float, float) {
+                           blocked = true;
+                           return true;
+                       });
+        return blocked ? mk3(0.0f) : mk3(1.0f);
+    }
+    float lt[kShadowList];
+    uint32_t lo[kShadowList], lp[kShadowList], lm[kShadowList];
+    int n = 0;
+    bool blocked = false, overflow = false;
+    traverse_scene(s, ray, PSY_VISIBILITY_SHADOW, ids.x, ids.y, ids.z, ids.w, tmax,
+                   [&](uint32_t ii, uint32_t local, uint32_t cp, float t, float, float) {
+                       const uint32_t mi = surface_material(s, ii, local);
+                       const MaterialGpu m = s.materials[mi];
+                       if (!m.has_transparent) {
+                           blocked = true;
+                           return true;
+                       }
+                       for (int k = 0; k < n; ++k) {
+                           if (lt[k] == t) {  // coincident: keep the greatest identity
+                               if (ii > lo[k] || (ii == lo[k] && cp > lp[k])) {
+                                   lo[k] = ii;
+                                   lp[k] = cp;
+                                   lm[k] = mi;
+                               }
+                               return false;
+                           }
+                       }
+                       if (n == kShadowList) {
+                           overflow = true;
+                           return true;
+                       }
+                       lt[n] = t;
+                       lo[n] = ii;
+                       lp[n] = cp;
+                       lm[n] = mi;
+                       ++n;
+                       return false;
+                   });
+    if (blocked) return mk3(0.0f);
+    const uint32_t budget = depth >= p.transparent_max ? 0u : p.transparent_max - depth;
+    if (overflow) {
+        if (uint32_t(kShadowList) > budget) return mk3(0.0f);
+        return shadow_iterated(s, p, ray, ids, depth);
+    }
+    if (uint32_t(n) > budget) return mk3(0.0f);
+    // insertion sort by distance, then multiply in that order
+    for (int i = 1; i < n; ++i) {
+        const float kt = lt[i];
+        const uint32_t km = lm[i];
+        int j = i - 1;
+        while (j >= 0 && lt[j] > kt) {
+            lt[j + 1] = lt[j];
+            lm[j + 1] = lm[j];
+            --j;
+        }
+        lt[j + 1] = kt;
+        lm[j + 1] = km;
+    }
+    f3 transmittance = mk3(1.0f);
+    for (int i = 0; i < n; ++i) {
+        const f3 t = clamp3(transparent_extinction(s, s.materials[lm[i]]), 0.0f, 1.0f);
+        if (!(max_component(t) > 0.0f)) return mk3(0.0f);
+        transmittance = transmittance * t;
+    }
+    return transmittance;
+}
+
 __global__ void __launch_bounds__(256) k_shadow(SceneView s, RenderParams p, PathBuffers b, uint32_t step,
                                                 uint32_t trace_path, psy_path_trace *trace) {
     const uint32_t count = b.counters[2];
@@ -531,36 +639,9 @@ __global__ void __launch_bounds__(256) k_shadow(SceneView s, RenderParams p, Pat
         const float4 o = b.sh_o[q], d = b.sh_d[q], c = b.sh_c[q];
         const uint4 ids = b.sh_ids[q];
         const uint32_t path = b.sh_path[q];
-        Ray ray{mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), 0.0f, o.w};
-        uint32_t transparent_depth = __float_as_uint(d.w);
+        const Ray ray{mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), 0.0f, o.w};
         const uint32_t depth = __float_as_uint(c.w);
-        f3 transmittance = mk3(1.0f);
-        if (!s.any_transparent) {
-            Hit h;
-            if (trace_closest(s, ray, PSY_VISIBILITY_SHADOW, ids.x, ids.y, ids.z, ids.w, true, h))
-                transmittance = mk3(0.0f);
-        } else {
-            for (uint32_t guard = 0; guard < 4096u; ++guard) {
-                Hit h;
-                if (!trace_closest(s, ray, PSY_VISIBILITY_SHADOW, ids.x, ids.y, ids.z, ids.w, false, h)) break;
-                if (transparent_depth >= p.transparent_max) {
-                    transmittance = mk3(0.0f);
-                    break;
-                }
-                const InstanceGpu &inst = s.instances[h.instance];
-                const MeshGpu mesh = s.meshes[inst.mesh];
-                const uint32_t mi = mesh.material_offset == kInvalid ? inst.material
-                                                                     : s.tri_materials[mesh.material_offset + h.prim];
-                const f3 t = clamp3(transparent_extinction(s, s.materials[mi]), 0.0f, 1.0f);
-                if (!(max_component(t) > 0.0f)) {
-                    transmittance = mk3(0.0f);
-                    break;
-                }
-                transmittance = transmittance * t;
-                transparent_depth += 1u;
-                ray.tmin = next_float_up(h.t);
-            }
-        }
+        const f3 transmittance = shadow_transmittance(s, p, ray, ids, __float_as_uint(d.w));
         f3 contribution = mk3(0.0f);
         if (transmittance.x > 0.0f || transmittance.y > 0.0f || transmittance.z > 0.0f) {
             contribution = clamp_contribution(mk3(c.x, c.y, c.z) * transmittance, depth, p);
