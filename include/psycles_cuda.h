@@ -296,6 +296,22 @@ psy_status psy_session_render_samples(psy_session *session, uint32_t first,
                                       uint32_t count, uint32_t offset,
                                       uint32_t total);
 
+/* Allocation-free render_samples, for callers that cannot allocate device
+ * memory at render time (a plugin inside a host application's fixed memory
+ * budget, work issued into a stream the caller does not own, a real-time
+ * viewport thread).  No counterpart in the reference.  Renders the same
+ * samples with the same kernels as psy_session_render_samples, but the path
+ * state lives in static device arrays (about 17 MiB that every GPU loading
+ * the library holds until exit) and the session's Sobol table is not used:
+ * at most 65536 window pixels and renders of at most 256 total samples
+ * (PSY_ERROR_RANGE beyond).  It calls no cudaMalloc or cudaFree.  The first
+ * call on a device takes the arrays' device addresses and fills the static
+ * Sobol table; make it before any stream capture.  All calls share the
+ * arrays: calls that overlap on the GPU race. */
+psy_status psy_session_render_samples_static(psy_session *session,
+                                             uint32_t first, uint32_t count,
+                                             uint32_t offset, uint32_t total);
+
 /* RenderSession::cancel (render.h:169); callable from any thread. */
 void psy_session_cancel(psy_session *session);
 

@@ -149,6 +149,8 @@ SIGNATURES = [
     ("psy_session_reset", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RenderSettings)]),
     ("psy_session_render_samples", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    ("psy_session_render_samples_static", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
     ("psy_session_cancel", None, [ctypes.c_void_p]),
     ("psy_session_read_pass", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_uint32, c_float_p, ctypes.c_uint64, c_uint32_p]),

@@ -13,6 +13,7 @@
 // the reference's construction.
 #include "psy_kernels.h"
 #include "psy_scene.h"
+#include "psy_static.h"
 
 #include <algorithm>
 #include <array>
@@ -1189,6 +1190,126 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
     if (trace) {
         PSY_CUDA_TRY(cudaMemcpy(&s->trace_host, trace, sizeof(psy_path_trace), cudaMemcpyDeviceToHost));
     }
+    return PSY_OK;
+}
+
+// Allocation-free render for callers that cannot allocate device memory at
+// render time.  Same kernels and sample order as psy_session_render_samples;
+// the wavefront state and the Sobol table come from static device arrays
+// (psy_static.cu).  The first call on a device takes the arrays' addresses
+// and fills the table; make that first call before any stream capture.
+// Calls share the arrays: overlapping calls on the GPU race.
+psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uint32_t count, uint32_t offset,
+                                             uint32_t total) {
+    if (!s) return fail(PSY_ERROR_INVALID_ARGUMENT, "null session");
+    if (s->cancelled.load()) return fail(PSY_ERROR_CANCELLED, "session cancelled");
+    if (count == 0u) return fail(PSY_ERROR_RANGE, "empty sample range");
+    const uint64_t begin = uint64_t(first) + offset, end = begin + count;
+    if (total == 0u || end > total) return fail(PSY_ERROR_RANGE, "sample range beyond the render's total");
+    if (s->total != 0u && s->total != total) return fail(PSY_ERROR_STATE, "total sample count changed within the session");
+    if (psy_sobol_sequence_size_for_samples(total) != psy::kStaticSobolSize)
+        return fail(PSY_ERROR_RANGE, "the static render supports renders of at most 256 total samples");
+    if (s->pixels > psy::kStaticMaxPaths)
+        return fail(PSY_ERROR_RANGE, "the static render supports windows of at most 65536 pixels");
+    psy_context *ctx = s->scene->context;
+    cudaStream_t st = ctx->stream;
+    PSY_CUDA_TRY(cudaSetDevice(ctx->device));
+    void *base = nullptr;
+    float4 *sobol = nullptr;
+    bool first_use = false;
+    PSY_CUDA_TRY(psy::static_scratch(ctx->device, &base, &sobol, &first_use));
+    if (first_use) {
+        float pattern[psy::kStaticSobolSize * 4u];  // one 4 KiB pattern at a time, no heap
+        for (uint32_t k = 0; k < 256u; ++k) {
+            sobol_pattern(pattern, psy::kStaticSobolSize, k);
+            PSY_CUDA_TRY(cudaMemcpy(sobol + size_t(k) * psy::kStaticSobolSize, pattern, sizeof(pattern),
+                                    cudaMemcpyHostToDevice));
+        }
+    }
+    // carve the static bytes into the wavefront arrays
+    unsigned char *cursor = static_cast<unsigned char *>(base);
+    auto carve = [&](size_t bytes) {
+        unsigned char *p = cursor;
+        cursor += (bytes + 255u) & ~size_t(255u);
+        return p;
+    };
+    const size_t n = psy::kStaticMaxPaths;
+    psy::PathBuffers b{};
+    b.ray_o = reinterpret_cast<float4 *>(carve(16 * n));
+    b.ray_d = reinterpret_cast<float4 *>(carve(16 * n));
+    b.tp = reinterpret_cast<float4 *>(carve(16 * n));
+    b.rad = reinterpret_cast<float4 *>(carve(16 * n));
+    b.st = reinterpret_cast<uint4 *>(carve(16 * n));
+    b.st2 = reinterpret_cast<uint4 *>(carve(16 * n));
+    b.sample = reinterpret_cast<uint32_t *>(carve(4 * n));
+    b.aov_n = reinterpret_cast<float4 *>(carve(16 * n));
+    b.aov_a = reinterpret_cast<float4 *>(carve(16 * n));
+    b.hit = reinterpret_cast<float4 *>(carve(16 * n));
+    b.hit_prim = reinterpret_cast<uint32_t *>(carve(4 * n));
+    b.sh_o = reinterpret_cast<float4 *>(carve(16 * n));
+    b.sh_d = reinterpret_cast<float4 *>(carve(16 * n));
+    b.sh_c = reinterpret_cast<float4 *>(carve(16 * n));
+    b.sh_ids = reinterpret_cast<uint4 *>(carve(16 * n));
+    b.sh_path = reinterpret_cast<uint32_t *>(carve(4 * n));
+    b.queue_in = reinterpret_cast<uint32_t *>(carve(4 * n));
+    b.queue_out = reinterpret_cast<uint32_t *>(carve(4 * n));
+    b.shadow_queue = reinterpret_cast<uint32_t *>(carve(4 * n));
+    b.counters = reinterpret_cast<uint32_t *>(carve(64));
+    unsigned long long *ray_stats = reinterpret_cast<unsigned long long *>(reinterpret_cast<unsigned char *>(b.counters) + 64);
+    // the ray counters accumulate: clear them; every other array is written
+    // before it is read within the call
+    PSY_CUDA_TRY(cudaMemsetAsync(ray_stats, 0, 2 * sizeof(unsigned long long), st));
+    psy::RenderParams p = s->params;
+    p.sobol = sobol;
+    p.sobol_size = psy::kStaticSobolSize;
+    s->total = total;
+    const uint32_t pixels = s->pixels;
+    const uint32_t per_batch = std::max(1u, std::min(count, psy::kStaticMaxPaths / std::max(pixels, 1u)));
+    const int sms = ctx->sms;
+    psy_render_stats stats{};
+    PSY_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
+    for (uint64_t sample = begin; sample < end;) {
+        if (s->cancelled.load()) return fail(PSY_ERROR_CANCELLED, "session cancelled");
+        const uint32_t n_samples = uint32_t(std::min<uint64_t>(per_batch, end - sample));
+        const uint32_t paths = pixels * n_samples;
+        psy::PathBuffers bb = b;
+        psy::launch_set_counters(st, bb.counters, paths);
+        psy::launch_raygen(st, sms, p, bb, pixels, paths, uint32_t(sample), psy::kInvalidId, nullptr);
+        stats.camera_rays += paths;
+        for (uint32_t step = 0; step < p.steps; ++step) {
+            psy::launch_intersect(st, sms, s->scene->view, bb, paths);
+            psy::launch_shade(st, sms, s->scene->view, p, bb, paths, step, psy::kInvalidId, nullptr);
+            psy::launch_count_rays(st, bb.counters, ray_stats);
+            psy::launch_shadow(st, sms, s->scene->view, p, bb, paths, step, psy::kInvalidId, nullptr);
+            psy::launch_swap(st, bb.counters);
+            std::swap(bb.queue_in, bb.queue_out);
+            stats.kernel_launches += 5u;
+            if ((step & 3u) == 3u) {
+                uint32_t left = 0u;
+                PSY_CUDA_TRY(cudaMemcpyAsync(&left, bb.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+                PSY_CUDA_TRY(cudaStreamSynchronize(st));
+                if (left == 0u) break;
+            }
+        }
+        psy::launch_film(st, sms, bb, pixels, n_samples, s->combined.as<float4>(), s->normal.as<float4>(),
+                         s->albedo.as<float4>(), s->sample_count.as<uint32_t>(), psy::kInvalidId, nullptr);
+        stats.kernel_launches += 3u;
+        stats.batches += 1u;
+        sample += n_samples;
+    }
+    PSY_CUDA_TRY(cudaEventRecord(s->ev_end, st));
+    PSY_CUDA_TRY(cudaGetLastError());
+    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    float ms = 0.0f;
+    PSY_CUDA_TRY(cudaEventElapsedTime(&ms, s->ev_begin, s->ev_end));
+    unsigned long long counts[2] = {0, 0};
+    PSY_CUDA_TRY(cudaMemcpy(counts, ray_stats, sizeof(counts), cudaMemcpyDeviceToHost));
+    stats.closest_rays = counts[0];
+    stats.path_segments = counts[0];
+    stats.shadow_rays = counts[1];
+    stats.ms_total = ms;
+    s->last_stats = stats;
+    s->rendered += count;
     return PSY_OK;
 }
 
