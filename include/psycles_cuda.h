@@ -136,6 +136,7 @@ typedef enum psy_light_type {
 
 #define PSY_LIGHT_FLAG_SPHERE 1u      /* point/spot radius is a sphere */
 #define PSY_LIGHT_FLAG_NORMALIZE 2u   /* divide power by emitter area */
+#define PSY_LIGHT_FLAG_ELLIPSE 4u     /* area light: ellipse, else rectangle */
 
 /* Analytic light (LightGpu, src/luisa/path_tracer_types.h:142). */
 typedef struct psy_light_desc {
@@ -156,6 +157,7 @@ typedef struct psy_light_desc {
     float spot_angle;
     float spot_smooth;
     float angle;                 /* sun angular diameter */
+    float spread;                /* area light spread; pi = full */
 } psy_light_desc;
 
 /* contract::CameraDesc (include/psycles/contract/scene.h:347),

@@ -907,6 +907,87 @@ static AnalyticSample sample_point_or_spot(const psy_light_desc &l, float3 refer
     return g;
 }
 
+// Area lights with full spread: rectangle_solid_angle_context /
+// sample_rectangle_solid_angle (analytic_light_sampling.h:605-793) and
+// AreaLightSampling::from_position (src/luisa/area_light_sampling.cpp:494-642).
+static float safe_div(float a, float b) { return b != 0.0f ? a / b : 0.0f; }
+static AnalyticSample sample_area(const psy_light_desc &l, float3 reference, float2 rnd) {
+    AnalyticSample out{false, f3(0.0f), f3(l.position[0], l.position[1], l.position[2]), 0.0f, 0.0f, 0.0f};
+    const float3 center = f3(l.position[0], l.position[1], l.position[2]);
+    const float3 au = f3(l.axis_x[0], l.axis_x[1], l.axis_x[2]);
+    const float3 av = f3(l.axis_y[0], l.axis_y[1], l.axis_y[2]);
+    const float3 az = f3(l.axis_z[0], l.axis_z[1], l.axis_z[2]);
+    const float lu = l.size_u, lv = l.size_v;
+    const bool ellipse = (l.flags & PSY_LIGHT_FLAG_ELLIPSE) != 0u;
+    const float3 normal = -az;
+    if (!(dot(center - reference, normal) <= 0.0f)) return out;
+    float3 position = center;
+    float pdf = 0.0f;
+    if (!ellipse) {
+        float3 z = cross(au, av);
+        const float3 co = center - reference;
+        float z0 = dot(co, z);
+        if (z0 > 0.0f) {
+            z = -z;
+            z0 = -z0;
+        }
+        const float cu = dot(co, au), cv = dot(co, av);
+        const float x0 = cu - 0.5f * lu, x1 = cu + 0.5f * lu, y0 = cv - 0.5f * lv, y1 = cv + 0.5f * lv;
+        float e[4] = {-y0, x1, y1, -x0};
+        for (float &v : e) v = v / std::sqrt(v * v + z0 * z0);
+        float g[4];
+        for (int k = 0; k < 4; ++k) g[k] = asin_(clampf(-e[k] * e[(k + 1) & 3], -1.0f, 1.0f));
+        const float solid = -(g[0] + g[1] + g[2] + g[3]);
+        const float min_e2 = minf(minf(e[0] * e[0], e[1] * e[1]), minf(e[2] * e[2], e[3] * e[3]));
+        const float cd = length(co);
+        const float planar = safe_div(-(cd * cd * cd), z0 * lu * lv);
+        pdf = (solid < 1.0e-5f || min_e2 > 0.99999f) ? planar : 1.0f / solid;
+        const float b0 = e[0], b1 = e[2];
+        const float alpha = rnd.x * solid + g[2] + g[3];
+        const float fu = safe_div(cos_(alpha) * b0 + b1, sin_(alpha));
+        float cos_u = std::copysign(1.0f / std::sqrt(fu * fu + b0 * b0), fu);
+        cos_u = clampf(cos_u, -1.0f, 1.0f);
+        float su = -(cos_u * z0) / maxf(std::sqrt(maxf(1.0f - cos_u * cos_u, 0.0f)), 1.0e-7f);
+        su = clampf(su, x0, x1);
+        const float du2 = su * su + z0 * z0;
+        const float h0 = y0 / std::sqrt(du2 + y0 * y0);
+        const float h1 = y1 / std::sqrt(du2 + y1 * y1);
+        const float hv = h0 + rnd.y * (h1 - h0);
+        const float hv2 = hv * hv;
+        const float sv = hv2 < 1.0f - 1.0e-6f ? hv * std::sqrt(du2 / (1.0f - hv2)) : y1;
+        position = reference + au * su + av * sv + z * z0;
+    } else {
+        const float2 disk = sample_uniform_disk(rnd);
+        position = center + au * (0.5f * lu * disk.x) + av * (0.5f * lv * disk.y);
+        pdf = 4.0f * kInvPi / (lu * lv);
+    }
+    const float3 off = position - reference;
+    const float d2 = dot(off, off);
+    const float dist = std::sqrt(maxf(d2, 0.0f));
+    const float3 dir = off / maxf(dist, 1.0e-30f);
+    if (ellipse) {
+        const float cosine = dot(normal, -dir);
+        pdf *= cosine > 0.0f ? d2 / cosine : 0.0f;
+    }
+    float area = lu * lv;
+    if (ellipse) area *= 0.25f * kPi;
+    const bool normalize_power = (l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u;
+    const float inv_area = (normalize_power && area != 0.0f) ? safe_div(1.0f, area) : 1.0f;
+    const float factor = kInvPi * inv_area * 1.0f;
+    const float3 inplane = position - center;
+    const float u = dot(inplane, au), v = dot(inplane, av);
+    const float eu = (0.5f + 1.0e-7f) * lu + 1.0e-6f, ev = (0.5f + 1.0e-7f) * lv + 1.0e-6f;
+    const bool inside = ellipse ? (u * u / (eu * eu) + v * v / (ev * ev) <= 1.0f)
+                                : (std::fabs(u) <= eu && std::fabs(v) <= ev);
+    out.valid = inside && factor > 0.0f;
+    out.direction = dir;
+    out.position = position;
+    out.distance = dist;
+    out.pdf = pdf;
+    out.eval_factor = factor;
+    return out;
+}
+
 // --------------------------------------------------------------- shadow
 
 // make_trace_shadow_callable (src/luisa/path_tracer_geometry.cpp:75-174):
@@ -1291,9 +1372,10 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
                 // AnalyticLightingComponent (src/luisa/path_kernel_nee_analytic.cpp:98-428)
                 const psy_light_desc &l = s.lights[selected.index];
                 if (!(depth > l.max_bounces)) {
-                    AnalyticSample a = l.type == PSY_LIGHT_DISTANT
-                                           ? sample_distant(l, f2(light_sample.x, light_sample.y))
-                                           : sample_point_or_spot(l, sp.position, f2(light_sample.x, light_sample.y));
+                    const float2 lxy = f2(light_sample.x, light_sample.y);
+                    AnalyticSample a = l.type == PSY_LIGHT_DISTANT ? sample_distant(l, lxy)
+                                       : l.type == PSY_LIGHT_AREA  ? sample_area(l, sp.position, lxy)
+                                                                    : sample_point_or_spot(l, sp.position, lxy);
                     const float light_pdf = a.pdf * selected.selection_pdf;
                     if (a.valid && light_pdf > 0.0f) {
                         const float3 light_radiance = f3(l.color[0], l.color[1], l.color[2]) * (l.power * a.eval_factor);

@@ -46,8 +46,22 @@ def _stale(target: pathlib.Path, deps: list[pathlib.Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(force: bool = False, verbose_ptxas: bool = False) -> pathlib.Path:
-    BUILD.mkdir(exist_ok=True)
+def build(force: bool = False, verbose_ptxas: bool = False, defines: tuple[str, ...] = (),
+          out: pathlib.Path | None = None, build_dir: pathlib.Path | None = None) -> pathlib.Path:
+    """Compiles the library; `defines` (NAME=VALUE) set the kernel tuning
+    macros, `out` / `build_dir` redirect the artefacts."""
+    global OUT, BUILD
+    out_path, build_path = OUT, BUILD
+    if out is not None:
+        OUT, BUILD = pathlib.Path(out), pathlib.Path(build_dir or pathlib.Path(out).parent / "_build")
+    try:
+        return _build(force, verbose_ptxas, [f"-D{d}" for d in defines])
+    finally:
+        OUT, BUILD = out_path, build_path
+
+
+def _build(force: bool, verbose_ptxas: bool, defs: list[str]) -> pathlib.Path:
+    BUILD.mkdir(exist_ok=True, parents=True)
     headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "psycles_cuda.h"]
     objects = []
     for src in SOURCES_CU:
@@ -55,13 +69,13 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> pathlib.Path:
         objects.append(obj)
         if force or _stale(obj, [CSRC / src] + headers):
             extra = ["-Xptxas", "-v"] if verbose_ptxas else []
-            _run([NVCC, *ARCH, *NVCC_FLAGS, *extra, "-c", str(CSRC / src), "-o", str(obj)])
+            _run([NVCC, *ARCH, *NVCC_FLAGS, *defs, *extra, "-c", str(CSRC / src), "-o", str(obj)])
     cxx = shutil.which("g++") or "g++"
     for src in SOURCES_CPP:
         obj = BUILD / (src + ".o")
         objects.append(obj)
         if force or _stale(obj, [CSRC / src] + headers):
-            _run([cxx, *CXX_FLAGS, f"-I{CUDA_HOME / 'include'}", "-c", str(CSRC / src), "-o", str(obj)])
+            _run([cxx, *CXX_FLAGS, *defs, f"-I{CUDA_HOME / 'include'}", "-c", str(CSRC / src), "-o", str(obj)])
     if force or _stale(OUT, objects):
         _run([NVCC, *ARCH, "-shared", "-o", str(OUT), *map(str, objects), "-lcudart"])
     return OUT

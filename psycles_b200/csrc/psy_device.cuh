@@ -507,56 +507,79 @@ __device__ __forceinline__ SlabRay make_slab_ray(f3 o, f3 raw) {
     return r;
 }
 
-// Two-level traversal in one loop: TLAS and BLAS nodes share the loop body
+// Resumable two-level traversal.  TLAS and BLAS nodes share one loop body
 // so the lanes of a warp stay on the same instruction stream while their
-// rays sit at different levels.  Every triangle accepted by the Pluecker
-// predicate in [tmin, tmax] (tmax shrinks through `tmax`) that is neither
-// the source nor the light identity is handed to `on_hit(instance, local,
-// cycles_prim, t, u, v)`; a true return ends the traversal.
-template <typename OnHit>
-__device__ __forceinline__ void traverse_scene(const SceneView &s, const Ray &ray, uint32_t visibility,
-                                               uint32_t src_obj, uint32_t src_prim, uint32_t light_obj,
-                                               uint32_t light_prim, float &tmax, OnHit on_hit) {
-    if (s.instance_count == 0u) return;
-    const SlabRay world = make_slab_ray(ray.o, ray.d);
-    SlabRay cur = world;
+// rays sit at different levels; the state lives in registers (stack in
+// local memory) so a persistent kernel can advance a ray a few nodes at a
+// time and hand the lane a new ray when it finishes.  Every triangle
+// accepted by the Pluecker predicate in [tmin, tmax] (`tmax` shrinks as the
+// visitor requests) that is neither the source nor the light identity is
+// handed to `on_hit(instance, local, cycles_prim, t, u, v)`; a true return
+// ends the traversal.
+struct TraversalState {
+    Ray ray;      // world ray
+    SlabRay cur;  // slab ray of the current level
+    float tmax;
+    uint32_t node, sp, inst, blas_base, tri_base, prim_offset;
+    uint32_t visibility, src_obj, src_prim, light_obj, light_prim;
     uint32_t stack[kStackSize];
-    int sp = 0;
-    uint32_t node = kTagTlas;  // TLAS root
-    uint32_t inst = kInvalid, blas_base = 0u, tri_base = 0u, prim_offset = 0u;
-    for (;;) {
-        const uint32_t tag = node & kTagMask;
-        const uint32_t idx = node & ~kTagMask;
+};
+
+__device__ __forceinline__ void traversal_begin(TraversalState &t, const SceneView &s, const Ray &ray,
+                                                uint32_t visibility, uint32_t src_obj, uint32_t src_prim,
+                                                uint32_t light_obj, uint32_t light_prim) {
+    t.ray = ray;
+    t.cur = make_slab_ray(ray.o, ray.d);
+    t.tmax = ray.tmax;
+    t.node = s.instance_count == 0u ? kTagLeave : kTagTlas;
+    t.sp = 0u;
+    t.inst = kInvalid;
+    t.blas_base = t.tri_base = t.prim_offset = 0u;
+    t.visibility = visibility;
+    t.src_obj = src_obj;
+    t.src_prim = src_prim;
+    t.light_obj = light_obj;
+    t.light_prim = light_prim;
+}
+
+// Advances at most `budget` loop iterations; true once the traversal ended.
+template <typename OnHit>
+__device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneView &s, int budget, OnHit on_hit) {
+    for (int it = 0; it < budget; ++it) {
+        const uint32_t tag = t.node & kTagMask;
+        const uint32_t idx = t.node & ~kTagMask;
         if (tag == kTagInstance) {
             const InstanceGpu &in = s.instances[idx];
-            if ((in.visibility & visibility) != 0u) {
+            if ((in.visibility & t.visibility) != 0u) {
                 const MeshGpu mesh = s.meshes[in.mesh];
                 const Xform w2o = load_xform(in.w2o);
-                cur = make_slab_ray(xform_point(w2o, ray.o), xform_direction(w2o, ray.d));
-                inst = idx;
-                blas_base = mesh.node_offset;
-                tri_base = mesh.tri_offset;
-                prim_offset = mesh.prim_offset;
-                if (sp < kStackSize) stack[sp++] = kTagLeave;
-                node = kTagBlas | mesh.node_offset;
+                t.cur = make_slab_ray(xform_point(w2o, t.ray.o), xform_direction(w2o, t.ray.d));
+                t.inst = idx;
+                t.blas_base = mesh.node_offset;
+                t.tri_base = mesh.tri_offset;
+                t.prim_offset = mesh.prim_offset;
+                if (t.sp < uint32_t(kStackSize)) t.stack[t.sp++] = kTagLeave;
+                t.node = kTagBlas | mesh.node_offset;
                 continue;
             }
-            if (sp == 0) return;
-            node = stack[--sp];
+            if (t.sp == 0u) return true;
+            t.node = t.stack[--t.sp];
             continue;
         }
         if (tag == kTagLeave) {
-            cur = world;
-            inst = kInvalid;
-            if (sp == 0) return;
-            node = stack[--sp];
+            if (t.inst != kInvalid) {
+                t.cur = make_slab_ray(t.ray.o, t.ray.d);
+                t.inst = kInvalid;
+            }
+            if (t.sp == 0u) return true;
+            t.node = t.stack[--t.sp];
             continue;
         }
         const bool blas = tag == kTagBlas;
         const BvhNodeGpu n = load_node(blas ? s.blas : s.tlas, int(idx));
         float ln, rn;
         bool lh, rh;
-        node_slabs(n, cur.oinv, cur.inv, ray.tmin, tmax, ln, rn, lh, rh);
+        node_slabs(n, t.cur.oinv, t.cur.inv, t.ray.tmin, t.tmax, ln, rn, lh, rh);
         uint32_t next[2];
         int nc = 0;
         const bool right_first = rn < ln;
@@ -567,34 +590,52 @@ __device__ __forceinline__ void traverse_scene(const SceneView &s, const Ray &ra
             const int link = side == 0 ? n.child.x : n.child.y;
             const int count = side == 0 ? n.child.z : n.child.w;
             if (link >= 0) {
-                next[nc++] = blas ? (kTagBlas | (blas_base + uint32_t(link))) : uint32_t(link);
+                next[nc++] = blas ? (kTagBlas | (t.blas_base + uint32_t(link))) : uint32_t(link);
                 continue;
             }
             if (!blas) {
                 if (count > 0) next[nc++] = kTagInstance | uint32_t(~link);
                 continue;
             }
-            const uint32_t first = tri_base + uint32_t(~link);
-            for (int t = 0; t < count; ++t) {
-                const float4 *tp = s.tris + 3u * (first + uint32_t(t));
+            const uint32_t first = t.tri_base + uint32_t(~link);
+            for (int q = 0; q < count; ++q) {
+                const float4 *tp = s.tris + 3u * (first + uint32_t(q));
                 const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
                 const uint32_t local = __float_as_uint(a.w);
-                const uint32_t cp = prim_offset + local;
-                if ((src_obj == inst && src_prim == cp) || (light_obj == inst && light_prim == cp)) continue;
+                const uint32_t cp = t.prim_offset + local;
+                if ((t.src_obj == t.inst && t.src_prim == cp) || (t.light_obj == t.inst && t.light_prim == cp)) continue;
                 float th, u, v;
-                if (!intersect_triangle(cur.o, cur.d, ray.tmin, tmax, ld3(a), ld3(b), ld3(c), th, u, v)) continue;
-                if (on_hit(inst, local, cp, th, u, v)) return;
+                if (!intersect_triangle(t.cur.o, t.cur.d, t.ray.tmin, t.tmax, ld3(a), ld3(b), ld3(c), th, u, v))
+                    continue;
+                if (on_hit(t.inst, local, cp, th, u, v)) return true;
             }
         }
         if (nc == 2) {
-            if (sp < kStackSize) stack[sp++] = next[1];
-            node = next[0];
+            if (t.sp < uint32_t(kStackSize)) t.stack[t.sp++] = next[1];
+            t.node = next[0];
         } else if (nc == 1) {
-            node = next[0];
+            t.node = next[0];
         } else {
-            if (sp == 0) return;
-            node = stack[--sp];
+            if (t.sp == 0u) return true;
+            t.node = t.stack[--t.sp];
         }
+    }
+    return false;
+}
+
+// Whole traversal in one call.
+template <typename OnHit>
+__device__ __forceinline__ void traverse_scene(const SceneView &s, const Ray &ray, uint32_t visibility,
+                                               uint32_t src_obj, uint32_t src_prim, uint32_t light_obj,
+                                               uint32_t light_prim, float &tmax, OnHit on_hit) {
+    TraversalState t;
+    traversal_begin(t, s, ray, visibility, src_obj, src_prim, light_obj, light_prim);
+    t.tmax = tmax;
+    while (!traversal_steps(t, s, 1 << 30, [&](uint32_t ii, uint32_t local, uint32_t cp, float th, float u, float v) {
+        const bool stop = on_hit(ii, local, cp, th, u, v);
+        t.tmax = tmax;
+        return stop;
+    })) {
     }
 }
 
@@ -884,6 +925,89 @@ __device__ __forceinline__ AnalyticSample sample_analytic(const psy_light_desc &
         out.distance = 1.0e30f;
         out.pdf = c.pdf;
         out.valid = true;
+        return out;
+    }
+    if (l.type == PSY_LIGHT_AREA) {
+        // AreaLightSampling::from_position, full spread
+        // (src/luisa/area_light_sampling.cpp:494-642; analytic_light_sampling.h:605-793)
+        out.valid = false;
+        out.eval_factor = 0.0f;
+        const f3 center = ld3(l.position), au = ld3(l.axis_x), av = ld3(l.axis_y), az = ld3(l.axis_z);
+        const float lu = l.size_u, lv = l.size_v;
+        const bool ellipse = (l.flags & PSY_LIGHT_FLAG_ELLIPSE) != 0u;
+        const f3 normal = -az;
+        out.position = center;
+        out.direction = mk3(0.0f);
+        out.distance = 0.0f;
+        out.pdf = 0.0f;
+        if (!(dot(center - reference, normal) <= 0.0f)) return out;
+        f3 position;
+        float pdf;
+        if (!ellipse) {
+            f3 z = cross(au, av);
+            const f3 co = center - reference;
+            float z0 = dot(co, z);
+            if (z0 > 0.0f) {
+                z = -z;
+                z0 = -z0;
+            }
+            const float cu = dot(co, au), cv = dot(co, av);
+            const float x0 = cu - 0.5f * lu, x1 = cu + 0.5f * lu, y0 = cv - 0.5f * lv, y1 = cv + 0.5f * lv;
+            float e[4] = {-y0, x1, y1, -x0};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) e[k] = e[k] / sqrtf(e[k] * e[k] + z0 * z0);
+            float g[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) g[k] = asin_(clampf_(-e[k] * e[(k + 1) & 3], -1.0f, 1.0f));
+            const float solid = -(g[0] + g[1] + g[2] + g[3]);
+            const float min_e2 = minf_(minf_(e[0] * e[0], e[1] * e[1]), minf_(e[2] * e[2], e[3] * e[3]));
+            const float cd = length(co);
+            const float pden = z0 * lu * lv;
+            const float planar = pden != 0.0f ? -(cd * cd * cd) / pden : 0.0f;
+            pdf = (solid < 1.0e-5f || min_e2 > 0.99999f) ? planar : 1.0f / solid;
+            const float b0 = e[0], b1 = e[2];
+            const float alpha = rnd.x * solid + g[2] + g[3];
+            const float sa = sin_(alpha);
+            const float fu = sa != 0.0f ? (cos_(alpha) * b0 + b1) / sa : 0.0f;
+            float cos_u = copysignf(1.0f / sqrtf(fu * fu + b0 * b0), fu);
+            cos_u = clampf_(cos_u, -1.0f, 1.0f);
+            float su = -(cos_u * z0) / maxf_(sqrtf(maxf_(1.0f - cos_u * cos_u, 0.0f)), 1.0e-7f);
+            su = clampf_(su, x0, x1);
+            const float du2 = su * su + z0 * z0;
+            const float h0 = y0 / sqrtf(du2 + y0 * y0);
+            const float h1 = y1 / sqrtf(du2 + y1 * y1);
+            const float hv = h0 + rnd.y * (h1 - h0);
+            const float hv2 = hv * hv;
+            const float sv = hv2 < 1.0f - 1.0e-6f ? hv * sqrtf(du2 / (1.0f - hv2)) : y1;
+            position = reference + au * su + av * sv + z * z0;
+        } else {
+            const f2 disk = sample_uniform_disk(rnd);
+            position = center + au * (0.5f * lu * disk.x) + av * (0.5f * lv * disk.y);
+            pdf = 4.0f * kInvPi / (lu * lv);
+        }
+        const f3 off = position - reference;
+        const float d2 = dot(off, off);
+        const float dist = sqrtf(maxf_(d2, 0.0f));
+        const f3 dir = off / maxf_(dist, 1.0e-30f);
+        if (ellipse) {
+            const float cosine = dot(normal, -dir);
+            pdf *= cosine > 0.0f ? d2 / cosine : 0.0f;
+        }
+        float area = lu * lv;
+        if (ellipse) area *= 0.25f * kPi;
+        const float inv_area = (normalize_power && area != 0.0f) ? 1.0f / area : 1.0f;
+        const float factor = kInvPi * inv_area * 1.0f;
+        const f3 inplane = position - center;
+        const float u = dot(inplane, au), v = dot(inplane, av);
+        const float eu = (0.5f + 1.0e-7f) * lu + 1.0e-6f, ev = (0.5f + 1.0e-7f) * lv + 1.0e-6f;
+        const bool inside = ellipse ? (u * u / (eu * eu) + v * v / (ev * ev) <= 1.0f)
+                                    : (fabsf(u) <= eu && fabsf(v) <= ev);
+        out.valid = inside && factor > 0.0f;
+        out.direction = dir;
+        out.position = position;
+        out.distance = dist;
+        out.pdf = pdf;
+        out.eval_factor = factor;
         return out;
     }
     const f3 center = ld3(l.position);

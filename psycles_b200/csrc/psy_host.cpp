@@ -239,10 +239,14 @@ void padded(const Box &b, float lo[3], float hi[3]) {
     }
 }
 
+#ifndef PSY_LEAF_SIZE
+#define PSY_LEAF_SIZE 1u
+#endif
+
 struct Builder {
     std::vector<psy::BvhNodeGpu> nodes;
     std::vector<Prim> prims;
-    uint32_t leaf_size = 4u;
+    uint32_t leaf_size = PSY_LEAF_SIZE;
     bool leaf_is_id = false;  // TLAS: leaf link = ~prim id, count 1
 
     struct Child {
@@ -686,7 +690,10 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     }
     for (uint32_t i = 0; i < d->light_count; ++i) {
         const psy_light_desc &l = d->lights[i];
-        if (l.type == PSY_LIGHT_AREA) return fail(PSY_ERROR_UNSUPPORTED, "area lights are not available in this build");
+        if (l.type == PSY_LIGHT_AREA && !(l.spread >= 3.14159165f))
+            return fail(PSY_ERROR_UNSUPPORTED, "area lights with a spread below pi are not available in this build");
+        if (l.type == PSY_LIGHT_AREA && !(l.size_u > 0.0f && l.size_v > 0.0f))
+            return fail(PSY_ERROR_INVALID_ARGUMENT, "area light with an empty size");
         if (l.type > PSY_LIGHT_DISTANT) return fail(PSY_ERROR_INVALID_ARGUMENT, "unknown light type");
         if ((l.flags & PSY_LIGHT_FLAG_SPHERE) && l.radius > 0.0f)
             return fail(PSY_ERROR_UNSUPPORTED, "spherical point lights are not available in this build");

@@ -103,18 +103,84 @@ __device__ __forceinline__ uint32_t contract_visibility(uint32_t v) {
     return r;
 }
 
-__global__ void __launch_bounds__(256) k_intersect(SceneView s, PathBuffers b) {
+// Persistent closest-hit kernel: each lane owns one ray at a time and, when
+// it finishes, the warp refills its idle lanes from a global fetch counter
+// (one atomic per warp), so lanes do not wait for the warp's longest ray.
+#ifndef PSY_TRAVERSAL_BUDGET
+#define PSY_TRAVERSAL_BUDGET 12
+#endif
+#ifndef PSY_INTERSECT_MIN_BLOCKS
+#define PSY_INTERSECT_MIN_BLOCKS 6
+#endif
+#ifndef PSY_SHADOW_MIN_BLOCKS
+#define PSY_SHADOW_MIN_BLOCKS 5
+#endif
+// Nodes a lane advances between refills of idle lanes.
+constexpr int kTraversalBudget = PSY_TRAVERSAL_BUDGET;
+constexpr uint32_t kFullMask = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Hands the next queue slot below `count` to every lane with `need`, or
+// kInvalid.  Warp-uniform: every lane calls it, and `exhausted` (uniform
+// across the warp) stops further atomics once the queue is used up.
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t *fetch_counter, uint32_t count, bool need, bool &exhausted) {
+    if (exhausted) return kInvalid;
+    const unsigned mask = __ballot_sync(kFullMask, need);
+    if (mask == 0u) return kInvalid;
+    uint32_t base = 0u;
+    if (lane_id() == 0u) base = atomicAdd(fetch_counter, uint32_t(__popc(mask)));
+    base = __shfl_sync(kFullMask, base, 0);
+    if (base + uint32_t(__popc(mask)) >= count) exhausted = true;
+    if (!need) return kInvalid;
+    const uint32_t q = base + uint32_t(__popc(mask & ((1u << lane_id()) - 1u)));
+    return q < count ? q : kInvalid;
+}
+
+__global__ void __launch_bounds__(128, PSY_INTERSECT_MIN_BLOCKS) k_intersect(SceneView s, PathBuffers b) {
     const uint32_t count = b.counters[0];
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
-        const uint32_t i = b.queue_in[q];
-        const float4 o = b.ray_o[i], d = b.ray_d[i];
-        const uint4 st = b.st[i];
-        const uint4 st2 = b.st2[i];
-        Ray ray{mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, d.w};
-        Hit h;
-        const bool hit = trace_closest(s, ray, contract_visibility(st.y), st2.y, st2.z, kInvalid, kInvalid, h);
-        b.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.instance));
-        b.hit_prim[i] = hit ? h.prim : kInvalid;
+    TraversalState t;
+    Hit best;
+    bool has = false, active = false, exhausted = false;
+    uint32_t path = 0u;
+    for (;;) {
+        const uint32_t q = warp_fetch(&b.counters[3], count, !active, exhausted);
+        if (q != kInvalid) {
+            path = b.queue_in[q];
+            const float4 o = b.ray_o[path], d = b.ray_d[path];
+            const uint32_t vis = b.st[path].y;
+            const uint4 st2 = b.st2[path];
+            const Ray ray{mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, d.w};
+            traversal_begin(t, s, ray, contract_visibility(vis), st2.y, st2.z, kInvalid, kInvalid);
+            has = false;
+            best.t = ray.tmax;
+            best.u = best.v = 0.0f;
+            best.instance = best.prim = best.object = best.cycles_prim = kInvalid;
+            active = true;
+        }
+        if (!__any_sync(kFullMask, active)) break;
+        if (active) {
+            const bool done = traversal_steps(t, s, kTraversalBudget,
+                                              [&](uint32_t ii, uint32_t local, uint32_t cp, float th, float u, float v) {
+                const bool later = ii > best.object || (ii == best.object && cp > best.cycles_prim);
+                if (has && !(th < best.t || (th == best.t && later))) return false;
+                has = true;
+                best.t = th;
+                best.u = u;
+                best.v = v;
+                best.instance = ii;
+                best.prim = local;
+                best.object = ii;
+                best.cycles_prim = cp;
+                t.tmax = th;
+                return false;
+            });
+            if (done) {
+                b.hit[path] = make_float4(best.t, best.u, best.v, __uint_as_float(best.instance));
+                b.hit_prim[path] = has ? best.prim : kInvalid;
+                active = false;
+            }
+        }
     }
 }
 
@@ -543,7 +609,7 @@ __device__ __forceinline__ uint32_t surface_material(const SceneView &s, uint32_
     return mesh.material_offset == kInvalid ? inst.material : s.tri_materials[mesh.material_offset + local];
 }
 
-__device__ f3 shadow_iterated(const SceneView &s, const RenderParams &p, Ray ray, uint4 ids, uint32_t depth) {
+__device__ __noinline__ f3 shadow_iterated(const SceneView &s, const RenderParams &p, Ray ray, uint4 ids, uint32_t depth) {
     f3 transmittance = mk3(1.0f);
     for (uint32_t guard = 0; guard < 4096u; ++guard) {
         Hit h;
@@ -632,16 +698,105 @@ __device__ __forceinline__ f3 shadow_transmittance(const SceneView &s, const Ren
     return transmittance;
 }
 
-__global__ void __launch_bounds__(256) k_shadow(SceneView s, RenderParams p, PathBuffers b, uint32_t step,
+// Persistent any-hit shadow kernel (same refill scheme as k_intersect).
+// Opaque-only scenes stop at the first accepted candidate; otherwise
+// transparent hits are collected per lane and resolved as in
+// shadow_transmittance once the traversal ends.
+__global__ void __launch_bounds__(128, PSY_SHADOW_MIN_BLOCKS) k_shadow(SceneView s, RenderParams p, PathBuffers b, uint32_t step,
                                                 uint32_t trace_path, psy_path_trace *trace) {
     const uint32_t count = b.counters[2];
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
-        const float4 o = b.sh_o[q], d = b.sh_d[q], c = b.sh_c[q];
-        const uint4 ids = b.sh_ids[q];
-        const uint32_t path = b.sh_path[q];
-        const Ray ray{mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), 0.0f, o.w};
+    TraversalState t;
+    bool active = false, exhausted = false, blocked = false, overflow = false;
+    uint32_t q_cur = 0u;
+    float lt[kShadowList];
+    uint32_t lo[kShadowList], lp[kShadowList], lm[kShadowList];
+    int n = 0;
+    for (;;) {
+        const uint32_t q = warp_fetch(&b.counters[4], count, !active, exhausted);
+        if (q != kInvalid) {
+            q_cur = q;
+            const float4 o = b.sh_o[q], d = b.sh_d[q];
+            const uint4 ids = b.sh_ids[q];
+            const Ray ray{mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), 0.0f, o.w};
+            traversal_begin(t, s, ray, PSY_VISIBILITY_SHADOW, ids.x, ids.y, ids.z, ids.w);
+            blocked = overflow = false;
+            n = 0;
+            active = true;
+        }
+        if (!__any_sync(kFullMask, active)) break;
+        if (!active) continue;
+        bool done;
+        if (!s.any_transparent) {
+            done = traversal_steps(t, s, kTraversalBudget, [&](uint32_t, uint32_t, uint32_t, float, float, float) {
+                blocked = true;
+                return true;
+            });
+        } else {
+            done = traversal_steps(t, s, kTraversalBudget,
+                                   [&](uint32_t ii, uint32_t local, uint32_t cp, float th, float, float) {
+                const uint32_t mi = surface_material(s, ii, local);
+                if (!s.materials[mi].has_transparent) {
+                    blocked = true;
+                    return true;
+                }
+                for (int k = 0; k < n; ++k) {
+                    if (lt[k] == th) {
+                        if (ii > lo[k] || (ii == lo[k] && cp > lp[k])) {
+                            lo[k] = ii;
+                            lp[k] = cp;
+                            lm[k] = mi;
+                        }
+                        return false;
+                    }
+                }
+                if (n == kShadowList) {
+                    overflow = true;
+                    return true;
+                }
+                lt[n] = th;
+                lo[n] = ii;
+                lp[n] = cp;
+                lm[n] = mi;
+                ++n;
+                return false;
+            });
+        }
+        if (!done) continue;
+        active = false;
+        const float4 d = b.sh_d[q_cur], c = b.sh_c[q_cur];
         const uint32_t depth = __float_as_uint(c.w);
-        const f3 transmittance = shadow_transmittance(s, p, ray, ids, __float_as_uint(d.w));
+        const uint32_t tdepth = __float_as_uint(d.w);
+        f3 transmittance = mk3(0.0f);
+        if (!blocked) {
+            const uint32_t budget = tdepth >= p.transparent_max ? 0u : p.transparent_max - tdepth;
+            if (overflow) {
+                if (uint32_t(kShadowList) <= budget)
+                    transmittance = shadow_iterated(s, p, t.ray, b.sh_ids[q_cur], tdepth);
+            } else if (uint32_t(n) <= budget) {
+                for (int i = 1; i < n; ++i) {
+                    const float kt = lt[i];
+                    const uint32_t km = lm[i];
+                    int j = i - 1;
+                    while (j >= 0 && lt[j] > kt) {
+                        lt[j + 1] = lt[j];
+                        lm[j + 1] = lm[j];
+                        --j;
+                    }
+                    lt[j + 1] = kt;
+                    lm[j + 1] = km;
+                }
+                transmittance = mk3(1.0f);
+                for (int i = 0; i < n; ++i) {
+                    const f3 e = clamp3(transparent_extinction(s, s.materials[lm[i]]), 0.0f, 1.0f);
+                    if (!(max_component(e) > 0.0f)) {
+                        transmittance = mk3(0.0f);
+                        break;
+                    }
+                    transmittance = transmittance * e;
+                }
+            }
+        }
+        const uint32_t path = b.sh_path[q_cur];
         f3 contribution = mk3(0.0f);
         if (transmittance.x > 0.0f || transmittance.y > 0.0f || transmittance.z > 0.0f) {
             contribution = clamp_contribution(mk3(c.x, c.y, c.z) * transmittance, depth, p);
@@ -693,12 +848,16 @@ __global__ void k_swap_counters(uint32_t *counters) {
     counters[0] = counters[1];
     counters[1] = 0u;
     counters[2] = 0u;
+    counters[3] = 0u;
+    counters[4] = 0u;
 }
 
 __global__ void k_set_counters(uint32_t *counters, uint32_t n) {
     counters[0] = n;
     counters[1] = 0u;
     counters[2] = 0u;
+    counters[3] = 0u;
+    counters[4] = 0u;
 }
 
 // Accumulates the number of rays traced by the queues of one step.
@@ -731,8 +890,16 @@ void launch_raygen(cudaStream_t st, int sms, const RenderParams &p, const PathBu
     k_raygen<<<launch_grid(paths, 256, sms), 256, 0, st>>>(p, b, pixels, paths, sample_base, trace_path, trace);
 }
 void launch_set_counters(cudaStream_t st, uint32_t *counters, uint32_t n) { k_set_counters<<<1, 1, 0, st>>>(counters, n); }
+// Persistent kernels: enough resident warps to fill every SM (bounded by the
+// work so small queues launch few blocks).
+int persistent_grid(uint32_t work, int sms) {
+    const uint32_t blocks = (work + 127u) / 128u;
+    const uint32_t cap = uint32_t(sms) * 12u;
+    return int(blocks < 1u ? 1u : (blocks > cap ? cap : blocks));
+}
+
 void launch_intersect(cudaStream_t st, int sms, const SceneView &s, const PathBuffers &b, uint32_t max_work) {
-    k_intersect<<<launch_grid(max_work, 256, sms), 256, 0, st>>>(s, b);
+    k_intersect<<<persistent_grid(max_work, sms), 128, 0, st>>>(s, b);
 }
 void launch_shade(cudaStream_t st, int sms, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                   uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
@@ -740,7 +907,7 @@ void launch_shade(cudaStream_t st, int sms, const SceneView &s, const RenderPara
 }
 void launch_shadow(cudaStream_t st, int sms, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                    uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
-    k_shadow<<<launch_grid(max_work, 256, sms), 256, 0, st>>>(s, p, b, step, trace_path, trace);
+    k_shadow<<<persistent_grid(max_work, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace);
 }
 void launch_swap(cudaStream_t st, uint32_t *counters) { k_swap_counters<<<1, 1, 0, st>>>(counters); }
 void launch_count_rays(cudaStream_t st, const uint32_t *counters, unsigned long long *stats) {

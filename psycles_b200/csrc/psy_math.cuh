@@ -96,6 +96,7 @@ __device__ __forceinline__ f3 light_safe_normalize(f3 value, f3 fallback) {
 __device__ __forceinline__ float sin_(float x) { return static_cast<float>(sin(static_cast<double>(x))); }
 __device__ __forceinline__ float cos_(float x) { return static_cast<float>(cos(static_cast<double>(x))); }
 __device__ __forceinline__ float acos_(float x) { return static_cast<float>(acos(static_cast<double>(x))); }
+__device__ __forceinline__ float asin_(float x) { return static_cast<float>(asin(static_cast<double>(x))); }
 __device__ __forceinline__ float atan2_(float y, float x) {
     return static_cast<float>(atan2(static_cast<double>(y), static_cast<double>(x)));
 }

@@ -67,6 +67,7 @@ class Light:
     spot_angle: float = math.pi / 4
     spot_smooth: float = 0.0
     angle: float = 0.0
+    spread: float = math.pi
     flags: int = _abi.LIGHT_FLAG_NORMALIZE
     max_bounces: int = 1024
 
@@ -157,7 +158,7 @@ class SceneDescHandle:
             d.axis_scale[:] = l.axis_scale
             d.color[:] = l.color
             d.power, d.radius, d.size_u, d.size_v = l.power, l.radius, l.size_u, l.size_v
-            d.spot_angle, d.spot_smooth, d.angle = l.spot_angle, l.spot_smooth, l.angle
+            d.spot_angle, d.spot_smooth, d.angle, d.spread = l.spot_angle, l.spot_smooth, l.angle, l.spread
         desc = _abi.SceneDesc()
         desc.meshes, desc.instances, desc.materials, desc.lights = meshes, instances, materials, lights
         desc.mesh_count = len(scene.meshes)
@@ -333,7 +334,7 @@ def procedural_scene(seed: int = 0, frequencies=(10, 14, 18, 22, 27, 32, 38, 44)
             xf = translate(*t) @ random_rotation(rng) @ scale(sx, sy, sz)
             instances.append(Instance(mi, int(rng.integers(0, material_count)), xf))
     if light_types is None:
-        light_types = (_abi.LIGHT_POINT, _abi.LIGHT_SPOT, _abi.LIGHT_DISTANT)
+        light_types = (_abi.LIGHT_POINT, _abi.LIGHT_SPOT, _abi.LIGHT_DISTANT, _abi.LIGHT_AREA)
     lights = []
     for lt in light_types:
         for _ in range(lights_per_type):
@@ -347,11 +348,16 @@ def procedural_scene(seed: int = 0, frequencies=(10, 14, 18, 22, 27, 32, 38, 44)
             else:
                 pos = tuple(rng.uniform((-10, 7, -10), (10, 12, 10)).tolist())
                 xf = look_at(pos, (float(rng.uniform(-4, 4)), 0.0, float(rng.uniform(-4, 4))))
+                flags = _abi.LIGHT_FLAG_NORMALIZE
+                if lt == _abi.LIGHT_AREA and rng.random() < 0.5:
+                    flags |= _abi.LIGHT_FLAG_ELLIPSE
                 lights.append(Light(lt, color, float(rng.uniform(200.0, 800.0)), position=pos,
                                     axis_x=tuple(xf[:3, 0].tolist()), axis_y=tuple(xf[:3, 1].tolist()),
                                     axis_z=tuple(xf[:3, 2].tolist()),
                                     spot_angle=float(math.radians(rng.uniform(30, 90))),
-                                    spot_smooth=float(rng.uniform(0.0, 0.5))))
+                                    spot_smooth=float(rng.uniform(0.0, 0.5)),
+                                    size_u=float(rng.uniform(0.5, 3.0)), size_v=float(rng.uniform(0.5, 3.0)),
+                                    flags=flags))
     cam = Camera(look_at((0.0, 9.0, 24.0), (0.0, 2.0, 0.0)), math.radians(40.0), math.radians(40.0), 0)
     return Scene(meshes, instances, mats, lights, cam, background=(0.05, 0.06, 0.08))
 
@@ -405,7 +411,12 @@ def small_test_scene(seed: int = 0, transparent: bool = True, lights: bool = Tru
               Light(_abi.LIGHT_SPOT, (0.8, 0.9, 1.0), 120.0, position=(-2.0, 4.5, 2.0),
                     axis_x=(1, 0, 0), axis_y=(0, 0, 1), axis_z=(0, 1, 0), spot_angle=math.radians(70),
                     spot_smooth=0.3),
-              Light(_abi.LIGHT_DISTANT, (1.0, 1.0, 0.9), 1.5, axis_z=(0.3, -0.9, 0.2), angle=math.radians(3.0))]
+              Light(_abi.LIGHT_DISTANT, (1.0, 1.0, 0.9), 1.5, axis_z=(0.3, -0.9, 0.2), angle=math.radians(3.0)),
+              Light(_abi.LIGHT_AREA, (0.9, 1.0, 0.9), 60.0, position=(3.0, 3.0, -1.0), axis_x=(1, 0, 0),
+                    axis_y=(0, 0, 1), axis_z=(0, 1, 0), size_u=1.5, size_v=0.8),
+              Light(_abi.LIGHT_AREA, (1.0, 0.8, 0.9), 40.0, position=(-3.0, 2.5, -1.5), axis_x=(0, 0, 1),
+                    axis_y=(0, 1, 0), axis_z=(1, 0, 0), size_u=1.0, size_v=1.2,
+                    flags=_abi.LIGHT_FLAG_NORMALIZE | _abi.LIGHT_FLAG_ELLIPSE)]
     cam = Camera(look_at((0.0, 3.0, 9.0), (0.0, 1.0, 0.0)), math.radians(40.0), math.radians(40.0), 0)
     return Scene(meshes, instances, mats, ls, cam, background=(0.1, 0.12, 0.15))
 
