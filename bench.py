@@ -40,7 +40,7 @@ sys.path.insert(0, str(ROOT))
 CONFIGS = {
     "procedural": dict(width=1920, height=1080, spp=64, bounces=8),
     "cornell": dict(width=256, height=256, spp=16, bounces=4),
-    "many_light": dict(width=1280, height=720, spp=32, bounces=6),
+    "many_light": dict(width=1280, height=720, spp=32, bounces=6, light_tree=1),
 }
 
 
@@ -59,6 +59,7 @@ def workload_config(args, scene) -> dict:
             "width": c["width"], "height": c["height"], "spp": args.spp, "max_bounces": c["bounces"],
             "instanced_triangles": scene.instanced_triangles, "instances": len(scene.instances),
             "materials": len(scene.materials), "analytic_lights": len(scene.lights),
+            "light_selection": "light tree" if c.get("light_tree") else "flat distribution",
             "l2_policy": "scene geometry + BVH (~150 MB) and per-path state (~400 MB) exceed the 126 MB L2"}
 
 
@@ -133,6 +134,7 @@ def cpu_baseline(args, scene, seconds_budget: float = 15.0) -> dict:
     rows, spp = 8, 1
     while True:
         st = scenes.render_settings(c["width"], c["height"], max_bounces=c["bounces"], window_y=c["height"] // 2,
+                                    use_light_tree=c.get("light_tree", 0),
                                     window_height=rows)
         film = OracleFilm(st)
         t0 = time.perf_counter()
@@ -200,7 +202,8 @@ def run_cuda(args) -> None:
     c = CONFIGS[args.config]
     scene = make_scene(args.config)
     backend = CudaPathTracerBackend(local)
-    settings = lambda: scenes.render_settings(c["width"], c["height"], max_bounces=c["bounces"], seed=rank)
+    settings = lambda: scenes.render_settings(c["width"], c["height"], max_bounces=c["bounces"], seed=rank,
+                                              use_light_tree=c.get("light_tree", 0))
     comp = backend.compile_scene(scene)
     if not comp.ok():
         raise SystemExit(f"compile_scene failed: {comp.diagnostics}")

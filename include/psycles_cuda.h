@@ -452,6 +452,18 @@ psy_status psy_debug_sobol_samples(psy_context *context,
                                    const uint32_t *queries, uint32_t count,
                                    float *out_samples, uint32_t *out_indices);
 
+/* Evaluates the compiled scene's many-light tree on the device for `count`
+ * shading points: light_tree.surface_sample and light_tree.surface_pdf
+ * (src/luisa/path_tracer_light_tree.cpp:547-760).  `queries` holds 8 floats
+ * per point: position xyz, random u, shading normal xyz, has-transmission
+ * (0 or 1).  Writes the selected emitter identity (emissive triangles first,
+ * then analytic lights; 0xffffffff for none) with its selection pdf, and the
+ * reverse pdf of emitter `pdf_emitters[i]` from the same point.  Fails with
+ * PSY_ERROR_UNSUPPORTED when the scene has no usable tree. */
+psy_status psy_debug_light_tree(psy_scene *scene,
+                                const float *queries, const uint32_t *pdf_emitters, uint32_t count,
+                                uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,8 +11,10 @@
 #include "../include/psycles_cuda.h"
 #include "oracle_math.h"
 #include "oracle_sampling.h"
+#include "oracle_light_tree.h"
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <memory>
 #include <thread>
@@ -79,6 +81,11 @@ struct Scene {
     float3 background{};
     uint32_t world_visibility{PSY_VISIBILITY_ALL};
     bool brute_force{false};
+    // many-light tree over the same emitters (triangles, then lights) and
+    // the (object, primitive) -> emitter lookup of forward hits
+    lt::LightTree tree;
+    bool tree_usable{false};
+    std::vector<std::array<uint32_t, 3>> tree_lookup;
 };
 
 // Median-split binary BVH over one mesh (object space).  The oracle's BVH
@@ -436,6 +443,24 @@ static float3 material_emission(const Material &mat) {
     for (const auto &t : traced)
         if (t.op == PSY_CLOSURE_EMISSION) r += t.weight;
     return r;
+}
+
+// estimate_surface_emission (src/compiler/surface_program.cpp:244-330):
+// bottom-up over the instructions; emission colour x strength, add a + b,
+// mix a (1 - f) + b f with the factor as authored; a forward or missing
+// operand counts as one.
+static float3 emission_estimate(const Material &mat) {
+    std::vector<float3> e;
+    for (const psy_closure_instruction &c : mat.code) {
+        auto operand = [&](uint32_t id) { return id < e.size() ? e[id] : f3(1.0f); };
+        float3 v = f3(0.0f);
+        if (c.op == PSY_CLOSURE_EMISSION) v = mat.vectors[c.color] * mat.scalars[c.scalar];
+        else if (c.op == PSY_CLOSURE_ADD) v = operand(c.a) + operand(c.b);
+        else if (c.op == PSY_CLOSURE_MIX)
+            v = operand(c.a) * (1.0f - mat.scalars[c.scalar]) + operand(c.b) * mat.scalars[c.scalar];
+        e.push_back(v);
+    }
+    return mat.root < e.size() ? e[mat.root] : f3(0.0f);
 }
 
 static bool program_has(const Material &mat, uint32_t op) {
@@ -1019,6 +1044,7 @@ struct Settings {
     psy_render_settings raw;
     uint32_t maximum, minimum, max_diffuse, max_glossy, max_transmission, transparent_min, transparent_max, steps;
     float inv_rr_threshold;
+    bool use_light_tree;
     float htan, vtan, shift_x, shift_y;
     std::array<float, 1024> filter;
     SobolTable sobol;
@@ -1040,6 +1066,8 @@ static void derive_settings(Settings &st, const Scene &s, const psy_render_setti
     st.steps = static_cast<uint32_t>(std::min<uint64_t>(required, 1024ull));
     st.inv_rr_threshold = (!r.use_light_tree && r.light_sampling_threshold > 0.0f)
                               ? r.film_exposure / r.light_sampling_threshold : 0.0f;
+    // path_tracer_kernel.cpp:206-209: the tree is used only when it exists
+    st.use_light_tree = r.use_light_tree != 0u && s.tree_usable;
     const float aspect = static_cast<float>(std::max(r.full_width, 1u)) / static_cast<float>(std::max(r.full_height, 1u));
     const bool hfit = s.camera.sensor_fit == 1u || (s.camera.sensor_fit == 0u && aspect >= 1.0f);
     st.vtan = hfit ? std::tan(s.camera.horizontal_field_of_view * 0.5f) / aspect
@@ -1171,6 +1199,15 @@ static void trace_set3(float *dst, float3 v) {
 // (src/luisa/path_kernel_setup.cpp:485-700), PathKernelPipeline::emit
 // (src/luisa/path_kernel_pipeline.cpp:73-183) and accumulate_path_sample
 // (path_kernel_setup.cpp:903-997).
+// make_triangle_emitter_callable (path_tracer_light_tree.cpp:762-797): the
+// emitter identity of an emissive (object, primitive), or invalid.
+static uint32_t tree_emitter(const Scene &s, uint32_t object, uint32_t primitive) {
+    const std::array<uint32_t, 3> key{object, primitive, 0u};
+    auto it = std::lower_bound(s.tree_lookup.begin(), s.tree_lookup.end(), key);
+    if (it != s.tree_lookup.end() && (*it)[0] == object && (*it)[1] == primitive) return (*it)[2];
+    return lt::kLtInvalid;
+}
+
 static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, uint32_t y, uint32_t sample,
                               psy_path_trace *trace) {
     const psy_render_settings &r = st.raw;
@@ -1216,6 +1253,7 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
     float transparency = 0.0f;
     float previous_bsdf_pdf = 0.0f;
     bool previous_delta = true;
+    float3 previous_mis_normal = f3(0.0f);
     bool primary_recorded = false;
     bool terminate_on_next_surface = false, terminate_after_transparent = false;
     uint32_t ray_visibility = PSY_VISIBILITY_CAMERA;
@@ -1240,7 +1278,9 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
         const float terminate_sample = st.sobol.sample_4d(sample, rng_hash, ps.rng_offset + kDimTerminate).x;
         const float4 ls4 = st.sobol.sample_4d(sample, rng_hash, ps.rng_offset + kDimLight);
         const float3 light_sample = f3(ls4.x, ls4.y, ls4.z);
-        const DistEntry selected = distribution_sample(s, light_sample.z);
+        // with the light tree the pick needs the shading point (below)
+        DistEntry selected = st.use_light_tree ? DistEntry{0.0f, 0.0f, kKindSentinel, 0u}
+                                               : distribution_sample(s, light_sample.z);
         const float light_terminate = st.sobol.sample_4d(sample, rng_hash, ps.rng_offset + kDimLightTerminate).x;
         const float4 bs4 = st.sobol.sample_4d(sample, rng_hash, ps.rng_offset + kDimBsdf);
         const float3 bsdf_sample = f3(bs4.x, bs4.y, bs4.z);
@@ -1284,7 +1324,10 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
         float emission_weight = 1.0f;
         if (nee && !s.emitters.empty() && mat.emission_sampling != 0u && mat.has_emission) {
             const bool competing = depth > 0u && !previous_delta;
-            const float selection_pdf = 0.5f * length(cross(sp.wp1 - sp.wp0, sp.wp2 - sp.wp0)) * s.triangle_area_pdf;
+            float selection_pdf = 0.5f * length(cross(sp.wp1 - sp.wp0, sp.wp2 - sp.wp0)) * s.triangle_area_pdf;
+            if (st.use_light_tree)  // light_tree.forward_pdf (path_tracer_light_tree.cpp:785-823)
+                selection_pdf = lt::tree_pdf(s.tree, tree_emitter(s, sp.object, sp.cycles_prim), ray.o,
+                                             previous_mis_normal, (ps.flag & kFlagMisHadTransmission) != 0u);
             const float light_pdf = emissive_forward_pdf(selection_pdf, mat.emission_sampling, ray.o, sp.position,
                                                          sp.wp0, sp.wp1, sp.wp2, sp.ng);
             const bool available = light_pdf > 0.0f;
@@ -1327,6 +1370,20 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
             }
         }
         const uint32_t runtime = runtime_flags(closures, sp.back_facing);
+        if (st.use_light_tree) {
+            // light_tree.surface_sample after shading (path_kernel_pipeline.cpp:150-159)
+            float pdf = 0.0f;
+            const uint32_t slot = lt::tree_sample(s.tree, light_sample.z, sp.position, sp.n,
+                                                  (runtime & kRuntimeBsdfHasTransmission) != 0u, pdf);
+            if (slot != lt::kLtInvalid && s.tree.emitters[slot].emitter_id < s.emitter_count) {
+                selected = s.distribution[s.tree.emitters[slot].emitter_id];
+                selected.selection_pdf = pdf;
+            }
+            if (ev) {
+                ev->light_kind = selected.kind;
+                ev->light_index = selected.index;
+            }
+        }
         // SurfaceGeometryStage lobe mask (path_kernel_surface_geometry.cpp:62-84)
         const uint32_t lobe_mask = terminate_after_transparent ? kEventTransparent : 0xffffffffu;
         // Direct lighting (path_kernel_pipeline.cpp:160-172)
@@ -1435,6 +1492,7 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
         if (!transparent) {
             previous_bsdf_pdf = ss.eval.pdf;
             previous_delta = singular;
+            previous_mis_normal = sp.n;
         }
         if (ev) {
             ev->bounce = ps.bounce;
@@ -1578,6 +1636,27 @@ static std::unique_ptr<Scene> prepare_scene(const psy_scene_desc *d, bool brute_
         for (uint32_t i = 0; i < s->emitter_count; ++i) s->distribution[i].cumulative *= inv;
         s->distribution.back().cumulative = 1.0f;
     }
+    // Light tree over the same population (path_tracer_light_sampling_scene.cpp:154-240):
+    // triangles carry identities 0..T-1, analytic lights T..T+L-1.
+    std::vector<lt::LtEmitter> population;
+    for (uint32_t i = 0; i < tri_count; ++i) {
+        const Emitter &e = s->emitters[i];
+        const float3 estimate = emission_estimate(s->materials[e.material]);
+        const float p0[3] = {e.p0.x, e.p0.y, e.p0.z}, p1[3] = {e.p1.x, e.p1.y, e.p1.z},
+                    p2[3] = {e.p2.x, e.p2.y, e.p2.z}, em[3] = {estimate.x, estimate.y, estimate.z};
+        const mat4 &m = s->instances[e.instance].o2w;
+        const bool mirror = dot(m.c0, cross(m.c1, m.c2)) < 0.0f;
+        population.push_back(lt::lt_triangle_emitter(i, p0, p1, p2, em, e.emission_sampling, mirror));
+    }
+    for (uint32_t i = 0; i < light_count; ++i) population.push_back(lt::lt_analytic_emitter(tri_count + i, &s->lights[i]));
+    if (!population.empty()) {
+        s->tree = lt::lt_build(population, 8u);
+        const lt::LightTree &t = s->tree;
+        s->tree_usable = t.root < t.nodes.size() && !t.emitters.empty() && t.emitter_to_tree.size() == t.emitters.size() &&
+                         t.emitter_to_leaf.size() == t.emitters.size() && t.nodes[t.root].measure.energy > 0.0f;
+    }
+    for (uint32_t i = 0; i < tri_count; ++i) s->tree_lookup.push_back({s->emitters[i].object, s->emitters[i].cycles_prim, i});
+    std::sort(s->tree_lookup.begin(), s->tree_lookup.end());
     return s;
 }
 
@@ -1726,5 +1805,103 @@ void oracle_scene_closest(const void *scene, const float *rays8, uint32_t count,
     }
 }
 
+
+
+// Light-tree build over emitter records, with the record layout and outputs
+// of the reference shim's ref_build_light_tree (oracle/ref_shim.cpp) so a
+// test compares the two word for word.
+static void put_measure(const lt::LtMeasure &m, float *o) {
+    for (int k = 0; k < 3; ++k) {
+        o[k] = m.bounds.lo[k];
+        o[3 + k] = m.bounds.hi[k];
+        o[7 + k] = m.orientation.axis[k];
+    }
+    o[6] = m.bounds.empty ? 1.0f : 0.0f;
+    o[10] = m.orientation.theta_o;
+    o[11] = m.orientation.theta_e;
+    o[12] = m.orientation.empty ? 1.0f : 0.0f;
+    o[13] = m.energy;
+}
+
+int oracle_build_light_tree(const float *in, uint32_t n, uint32_t max_leaf, uint32_t node_capacity, float *node_measure,
+                            uint32_t *node_topology, float *emitter_measure, uint32_t *emitter_ids, uint32_t *to_tree,
+                            uint32_t *to_leaf, uint32_t *root, uint32_t *node_count) {
+    std::vector<lt::LtEmitter> source(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *r = in + 20u * i;
+        lt::LtEmitter &e = source[i];
+        for (int k = 0; k < 3; ++k) {
+            e.measure.bounds.lo[k] = r[k];
+            e.measure.bounds.hi[k] = r[3 + k];
+            e.measure.orientation.axis[k] = r[7 + k];
+            e.centroid[k] = r[14 + k];
+        }
+        e.measure.bounds.empty = r[6] != 0.0f;
+        e.measure.orientation.theta_o = r[10];
+        e.measure.orientation.theta_e = r[11];
+        e.measure.orientation.empty = r[12] != 0.0f;
+        e.measure.energy = r[13];
+        e.distant = r[17] != 0.0f;
+        e.emitter_id = static_cast<uint32_t>(r[18]);
+    }
+    try {
+        const lt::LightTree t = lt::lt_build(source, max_leaf);
+        if (t.nodes.size() > node_capacity) return 2;
+        for (size_t k = 0; k < t.nodes.size(); ++k) {
+            const lt::LtNode &nd = t.nodes[k];
+            put_measure(nd.measure, node_measure + 14u * k);
+            uint32_t *w = node_topology + 6u * k;
+            w[0] = nd.parent;
+            w[1] = nd.left;
+            w[2] = nd.right;
+            w[3] = nd.first;
+            w[4] = nd.count;
+            w[5] = nd.kind;
+        }
+        for (size_t k = 0; k < t.emitters.size(); ++k) {
+            put_measure(t.emitters[k].measure, emitter_measure + 14u * k);
+            emitter_ids[k] = t.emitters[k].emitter_id;
+        }
+        for (size_t k = 0; k < t.emitter_to_tree.size(); ++k) {
+            to_tree[k] = t.emitter_to_tree[k];
+            to_leaf[k] = t.emitter_to_leaf[k];
+        }
+        *root = t.root;
+        *node_count = static_cast<uint32_t>(t.nodes.size());
+        return 0;
+    } catch (...) {
+        return 1;
+    }
+}
+
+// Light-tree selection over a prepared scene (oracle_scene_create) for
+// `count` shading points.  queries: 8 floats per point (position xyz,
+// random u, normal xyz, has_transmission 0/1).  Writes the selected emitter
+// identity (0xffffffff for none) with its selection pdf, and the reverse pdf
+// of emitter pdf_emitters[i] from the same point.  Returns 1 when the scene
+// has no usable tree.
+int oracle_light_tree_query(const void *scene, const float *queries, const uint32_t *pdf_emitters, uint32_t count,
+                            uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf) {
+    const Scene &s = *static_cast<const Scene *>(scene);
+    if (!s.tree_usable) return 1;
+    for (uint32_t i = 0; i < count; ++i) {
+        const float *q = queries + 8u * i;
+        const float3 p = f3(q[0], q[1], q[2]), n = f3(q[4], q[5], q[6]);
+        const bool tr = q[7] != 0.0f;
+        float pdf = 0.0f;
+        const uint32_t slot = lt::tree_sample(s.tree, q[3], p, n, tr, pdf);
+        out_emitters[i] = slot == lt::kLtInvalid ? slot : s.tree.emitters[slot].emitter_id;
+        out_sample_pdf[i] = slot == lt::kLtInvalid ? 0.0f : pdf;
+        out_reverse_pdf[i] = lt::tree_pdf(s.tree, pdf_emitters[i], p, n, tr);
+    }
+    return 0;
+}
+
+uint32_t oracle_scene_emitter_count(const void *scene) { return static_cast<const Scene *>(scene)->emitter_count; }
+
+// Emitter identity of an emissive (object, cycles primitive) pair.
+uint32_t oracle_light_tree_triangle_emitter(const void *scene, uint32_t object, uint32_t primitive) {
+    return tree_emitter(*static_cast<const Scene *>(scene), object, primitive);
+}
 
 }  // extern "C"

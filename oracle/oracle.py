@@ -39,6 +39,12 @@ def load() -> ctypes.CDLL:
         lib.oracle_scene_create.argtypes = [vp, ctypes.c_int]
         lib.oracle_scene_destroy.argtypes = [vp]
         lib.oracle_scene_closest.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
+        lib.oracle_light_tree_query.argtypes = [vp, vp, vp, ctypes.c_uint32, vp, vp, vp]
+        lib.oracle_light_tree_query.restype = ctypes.c_int
+        lib.oracle_light_tree_triangle_emitter.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32]
+        lib.oracle_light_tree_triangle_emitter.restype = ctypes.c_uint32
+        lib.oracle_scene_emitter_count.argtypes = [vp]
+        lib.oracle_scene_emitter_count.restype = ctypes.c_uint32
         lib.oracle_pixel_filter_table.argtypes = [ctypes.c_uint32, ctypes.c_float, vp]
         lib.oracle_sample_cosine_hemisphere.argtypes = [vp, vp, vp, vp]
         lib.oracle_next_surface.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
@@ -112,8 +118,101 @@ class OracleScene:
         self.lib.oracle_scene_closest(self.handle, _p(rays), rays.shape[0], visibility, _p(tuv), _p(ids))
         return tuv, ids
 
+    def light_tree_query(self, queries: np.ndarray, pdf_emitters: np.ndarray):
+        """(selected emitter, its selection pdf, reverse pdf of pdf_emitters)
+        per shading point; queries are (position, u, normal, transmission)."""
+        q = np.ascontiguousarray(queries, np.float32).reshape(-1, 8)
+        e = np.ascontiguousarray(pdf_emitters, np.uint32)
+        sel = np.zeros(q.shape[0], np.uint32)
+        spdf = np.zeros(q.shape[0], np.float32)
+        rpdf = np.zeros(q.shape[0], np.float32)
+        if self.lib.oracle_light_tree_query(self.handle, _p(q), _p(e), q.shape[0], _p(sel), _p(spdf), _p(rpdf)) != 0:
+            raise RuntimeError("scene has no usable light tree")
+        return sel, spdf, rpdf
+
+    def emitter_count(self) -> int:
+        """Emissive triangles + analytic lights of the prepared scene."""
+        return int(self.lib.oracle_scene_emitter_count(self.handle))
+
+    def triangle_emitter(self, obj: int, prim: int) -> int:
+        return int(self.lib.oracle_light_tree_triangle_emitter(self.handle, obj, prim))
+
     def __del__(self):
         try:
             self.lib.oracle_scene_destroy(self.handle)
         except Exception:
             pass
+
+
+# ----------------------------------------------------------------- light tree
+
+def light_tree_emitter_records(seed: int, count: int) -> np.ndarray:
+    """Seeded emitter records (20 floats each, the layout of
+    oracle_build_light_tree / ref_build_light_tree): triangle-, point-, spot-
+    and distant-like measures, a few invalid ones, shared centroids for the
+    tie-breaks, and identities in shuffled order."""
+    rng = np.random.default_rng(seed)
+    rec = np.zeros((count, 20), np.float32)
+    kinds = rng.integers(0, 6, count)
+    for i in range(count):
+        k = int(kinds[i])
+        c = rng.uniform(-10.0, 10.0, 3).astype(np.float32)
+        if i > 2 and rng.uniform() < 0.1:
+            c = rec[rng.integers(0, i), 14:17].copy()
+        half = rng.uniform(0.0, 1.0, 3).astype(np.float32)
+        axis = rng.normal(size=3)
+        axis = (axis / np.linalg.norm(axis)).astype(np.float32)
+        energy = np.float32(rng.uniform(0.01, 5.0))
+        lo, hi, empty_b = c - half, c + half, 0.0
+        theta_o, theta_e, distant = np.float32(np.pi / 2), np.float32(np.pi / 2), 0.0
+        if k == 0:    # one-sided triangle
+            theta_o = np.float32(0.0)
+        elif k == 1:  # point light
+            theta_o = np.float32(np.pi)
+        elif k == 2:  # spot light
+            theta_o, theta_e = np.float32(0.0), np.float32(rng.uniform(0.05, 1.5))
+        elif k == 3:  # distant light
+            lo, hi, empty_b, distant = np.zeros(3), np.zeros(3), 1.0, 1.0
+            theta_o, theta_e = np.float32(0.0), np.float32(rng.uniform(0.0, 0.3))
+        elif k == 4 and rng.uniform() < 0.3:  # emits nothing
+            energy = np.float32(0.0)
+        rec[i, 0:3], rec[i, 3:6], rec[i, 6] = lo, hi, empty_b
+        rec[i, 7:10], rec[i, 10], rec[i, 11], rec[i, 12] = axis, theta_o, theta_e, 0.0
+        rec[i, 13], rec[i, 14:17], rec[i, 17] = energy, c, distant
+    rec[:, 18] = rng.permutation(count).astype(np.float32)
+    return rec
+
+
+def build_light_tree(lib: ctypes.CDLL, symbol: str, records: np.ndarray, max_leaf: int = 8) -> dict:
+    """Runs oracle_build_light_tree or ref_build_light_tree on `records`."""
+    n = records.shape[0]
+    cap = 2 * n + 4
+    node_m = np.zeros((cap, 14), np.float32)
+    node_t = np.zeros((cap, 6), np.uint32)
+    em_m = np.zeros((n, 14), np.float32)
+    em_id = np.zeros(n, np.uint32)
+    to_tree = np.zeros(n, np.uint32)
+    to_leaf = np.zeros(n, np.uint32)
+    root = ctypes.c_uint32(0)
+    nodes = ctypes.c_uint32(0)
+    fn = getattr(lib, symbol)
+    fn.restype = ctypes.c_int
+    rc = fn(_p(np.ascontiguousarray(records, np.float32)), ctypes.c_uint32(n), ctypes.c_uint32(max_leaf),
+            ctypes.c_uint32(cap), _p(node_m), _p(node_t), _p(em_m), _p(em_id), _p(to_tree), _p(to_leaf),
+            ctypes.byref(root), ctypes.byref(nodes))
+    if rc != 0:
+        raise RuntimeError(f"{symbol} failed with {rc}")
+    k = nodes.value
+    return {"node_measure": node_m[:k], "node_topology": node_t[:k], "emitter_measure": em_m,
+            "emitter_ids": em_id, "to_tree": to_tree, "to_leaf": to_leaf, "root": root.value}
+
+
+def light_tree_fingerprint(tree: dict) -> int:
+    """FNV-1a 64 over every output word of a tree build."""
+    h = 14695981039346656037
+    parts = [tree["node_measure"].view(np.uint32), tree["node_topology"], tree["emitter_measure"].view(np.uint32),
+             tree["emitter_ids"], tree["to_tree"], tree["to_leaf"], np.array([tree["root"]], np.uint32)]
+    for part in parts:
+        for b in np.ascontiguousarray(part).tobytes():
+            h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h

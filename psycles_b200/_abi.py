@@ -165,6 +165,8 @@ SIGNATURES = [
     ("psy_pixel_filter_table", ctypes.c_int, [ctypes.c_uint32, ctypes.c_float, c_float_p]),
     ("psy_debug_sobol_samples", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_uint32, c_uint32_p, ctypes.c_uint32, c_float_p, c_uint32_p]),
+    ("psy_debug_light_tree", ctypes.c_int,
+     [ctypes.c_void_p, c_float_p, c_uint32_p, ctypes.c_uint32, c_uint32_p, c_float_p, c_float_p]),
 ]
 
 def default_settings() -> RenderSettings:

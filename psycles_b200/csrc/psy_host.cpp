@@ -12,6 +12,7 @@
 // Compiled without FP contraction so the host tables are bit-identical to
 // the reference's construction.
 #include "psy_kernels.h"
+#include "psy_light_tree.h"
 #include "psy_scene.h"
 #include "psy_static.h"
 
@@ -421,7 +422,7 @@ struct psy_scene {
     std::vector<psy::MaterialGpu> materials;
     std::vector<float> scalars, vectors;
     DeviceBuffer tlas, blas, tris, instances, meshes, positions, normals, indices, tri_materials, material_buf, code,
-        scalar_buf, vector_buf, emitters, distribution, lights;
+        scalar_buf, vector_buf, emitters, distribution, lights, lt_nodes, lt_emitters, lt_mapping, lt_lookup;
     psy::SceneView view{};
     uint64_t triangle_count = 0;
     double build_ms = 0.0;
@@ -439,7 +440,7 @@ struct psy_session {
     DeviceBuffer sobol, filter, combined, normal, albedo, sample_count;
     // path state
     uint32_t capacity = 0;
-    DeviceBuffer ray_o, ray_d, tp, rad, st, st2, sample, aov_n, aov_a, hit, hit_prim, sh_o, sh_d, sh_c, sh_ids,
+    DeviceBuffer ray_o, ray_d, tp, rad, st, st2, sample, aov_n, aov_a, mis_n, hit, hit_prim, sh_o, sh_d, sh_c, sh_ids,
         sh_path, qa, qb, sq, counters, stats;
     psy::PathBuffers paths{};
     // trace
@@ -468,7 +469,6 @@ psy_status derive_params(psy_session *s, const psy_render_settings &r) {
         return fail(PSY_ERROR_INVALID_ARGUMENT, "bounce limits above 250 are not supported");
     if (r.direct_light_sampling > PSY_DIRECT_LIGHT_NEE)
         return fail(PSY_ERROR_INVALID_ARGUMENT, "unknown direct light sampling mode");
-    if (r.use_light_tree) return fail(PSY_ERROR_UNSUPPORTED, "light-tree sampling is not available in this build");
     psy::RenderParams &p = s->params;
     p.full_w = r.full_width;
     p.full_h = r.full_height;
@@ -494,6 +494,10 @@ psy_status derive_params(psy_session *s, const psy_render_settings &r) {
                              ? r.film_exposure / r.light_sampling_threshold : 0.0f;
     p.direct_mode = r.direct_light_sampling;
     p.nee = r.next_event_estimation;
+    // the tree is used only where the scene has one
+    // (src/luisa/path_tracer_kernel.cpp:206-209)
+    p.use_light_tree = (r.use_light_tree && s->scene->view.lt_node_count > 0u && s->scene->view.lt_emitter_count > 0u)
+                           ? 1u : 0u;
     // camera parameters (src/luisa/path_tracer_kernel.cpp:225-280)
     const psy_camera_desc &c = s->scene->camera;
     const float aspect = static_cast<float>(std::max(r.full_width, 1u)) / static_cast<float>(std::max(r.full_height, 1u));
@@ -521,6 +525,7 @@ psy_status ensure_capacity(psy_session *s, uint32_t n) {
     PSY_CUDA_TRY(s->sample.alloc(u1));
     PSY_CUDA_TRY(s->aov_n.alloc(f4));
     PSY_CUDA_TRY(s->aov_a.alloc(f4));
+    PSY_CUDA_TRY(s->mis_n.alloc(f4));
     PSY_CUDA_TRY(s->hit.alloc(f4));
     PSY_CUDA_TRY(s->hit_prim.alloc(u1));
     PSY_CUDA_TRY(s->sh_o.alloc(f4));
@@ -544,6 +549,7 @@ psy_status ensure_capacity(psy_session *s, uint32_t n) {
     b.sample = s->sample.as<uint32_t>();
     b.aov_n = s->aov_n.as<float4>();
     b.aov_a = s->aov_a.as<float4>();
+    b.mis_n = s->mis_n.as<float4>();
     b.hit = s->hit.as<float4>();
     b.hit_prim = s->hit_prim.as<uint32_t>();
     b.sh_o = s->sh_o.as<float4>();
@@ -575,7 +581,35 @@ psy_status clear_film(psy_session *s) {
     return PSY_OK;
 }
 
-constexpr uint32_t kDefaultCapacity = 1u << 22;  // 4M paths = 392 MB of state
+constexpr uint32_t kDefaultCapacity = 1u << 22;  // 4M paths = 408 MB of state
+
+// Emission estimate of a closure program for the light tree
+// (estimate_surface_emission, src/compiler/surface_program.cpp:244-330): one
+// estimate per instruction in program order -- emission colour x strength,
+// add a + b, mix a (1 - f) + b f with the unclamped factor -- where an
+// operand that is not an earlier instruction counts as one.
+void emission_estimate(const psy_material_desc &m, float out[3]) {
+    std::vector<std::array<float, 3>> est;
+    est.reserve(m.closure_count);
+    auto dep = [&](uint32_t id) { return id < est.size() ? est[id] : std::array<float, 3>{1.0f, 1.0f, 1.0f}; };
+    for (uint32_t i = 0; i < m.closure_count; ++i) {
+        const psy_closure_instruction &c = m.closures[i];
+        std::array<float, 3> e{0.0f, 0.0f, 0.0f};
+        if (c.op == PSY_CLOSURE_EMISSION) {
+            const float strength = m.scalars[c.scalar];
+            for (int k = 0; k < 3; ++k) e[k] = m.vectors[3u * c.color + k] * strength;
+        } else if (c.op == PSY_CLOSURE_ADD) {
+            const auto a = dep(c.a), b = dep(c.b);
+            for (int k = 0; k < 3; ++k) e[k] = a[k] + b[k];
+        } else if (c.op == PSY_CLOSURE_MIX) {
+            const auto a = dep(c.a), b = dep(c.b);
+            const float f = m.scalars[c.scalar];
+            for (int k = 0; k < 3; ++k) e[k] = a[k] * (1.0f - f) + b[k] * f;
+        }
+        est.push_back(e);
+    }
+    for (int k = 0; k < 3; ++k) out[k] = m.root < est.size() ? est[m.root][k] : 0.0f;
+}
 
 }  // namespace
 
@@ -910,6 +944,66 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     }
     std::vector<psy_light_desc> lights(d->lights, d->lights + d->light_count);
 
+    // ---- many-light tree over the same emitter population
+    // (src/luisa/path_tracer_light_sampling_scene.cpp:160-240)
+    std::vector<psy::LtNodeGpu> lt_nodes;
+    std::vector<psy::LtEmitterGpu> lt_emitters;
+    std::vector<uint2> lt_mapping;
+    std::vector<uint4> lt_lookup;
+    uint32_t lt_root = 0u;
+    {
+        std::vector<psy::LtEmitter> source;
+        source.reserve(emitters.size() + lights.size());
+        for (uint32_t i = 0; i < tri_n; ++i) {
+            const psy::EmitterGpu &e = emitters[i];
+            float estimate[3] = {0.0f, 0.0f, 0.0f};
+            const psy_material_desc &m = d->materials[e.material];
+            emission_estimate(m, estimate);
+            const M34 &xf = o2w[e.object];
+            const float det = dt(xf.c0, crs(xf.c1, xf.c2));
+            source.push_back(psy::lt_triangle_emitter(i, e.p0, e.p1, e.p2, estimate, e.emission_sampling, det < 0.0f));
+        }
+        for (uint32_t i = 0; i < light_n; ++i) source.push_back(psy::lt_analytic_emitter(tri_n + i, &lights[i]));
+        if (!source.empty()) {
+            const psy::LightTree tree = psy::lt_build(source, 8u);
+            const bool usable = tree.root < tree.nodes.size() && tree.emitter_to_tree.size() == tree.emitters.size() &&
+                                tree.nodes[tree.root].measure.energy > 0.0f;
+            if (usable) {
+                auto flags = [](const psy::LtMeasure &m, bool distant) {
+                    return (!m.bounds.empty ? psy::kLtFlagBounds : 0u) |
+                           (!m.orientation.empty ? psy::kLtFlagOrientation : 0u) | (distant ? psy::kLtFlagDistant : 0u);
+                };
+                auto pack = [](const psy::LtMeasure &m, float4 &a, float4 &b, float4 &c) {
+                    a = make_float4(m.bounds.lo[0], m.bounds.lo[1], m.bounds.lo[2], m.energy);
+                    b = make_float4(m.bounds.hi[0], m.bounds.hi[1], m.bounds.hi[2], m.orientation.theta_o);
+                    c = make_float4(m.orientation.axis[0], m.orientation.axis[1], m.orientation.axis[2],
+                                    m.orientation.theta_e);
+                };
+                for (const psy::LtNode &n : tree.nodes) {
+                    psy::LtNodeGpu g{};
+                    pack(n.measure, g.min_energy, g.max_theta_o, g.axis_theta_e);
+                    g.topology = make_uint4(n.parent, n.left, n.right, n.kind);
+                    g.emitters = make_uint4(n.first, n.count, flags(n.measure, n.kind == psy::kLtDistant), 0u);
+                    lt_nodes.push_back(g);
+                }
+                for (const psy::LtEmitter &e : tree.emitters) {
+                    psy::LtEmitterGpu g{};
+                    pack(e.measure, g.min_energy, g.max_theta_o, g.axis_theta_e);
+                    g.identity = make_uint4(e.emitter_id, flags(e.measure, e.distant), 0u, 0u);
+                    lt_emitters.push_back(g);
+                }
+                for (size_t id = 0; id < tree.emitters.size(); ++id)
+                    lt_mapping.push_back(make_uint2(tree.emitter_to_tree[id], tree.emitter_to_leaf[id]));
+                for (uint32_t i = 0; i < tri_n; ++i)
+                    lt_lookup.push_back(make_uint4(emitters[i].object, emitters[i].cycles_prim, i, 0u));
+                std::sort(lt_lookup.begin(), lt_lookup.end(), [](const uint4 &a, const uint4 &b) {
+                    return a.x < b.x || (a.x == b.x && (a.y < b.y || (a.y == b.y && a.z < b.z)));
+                });
+                lt_root = tree.root;
+            }
+        }
+    }
+
     // ---- upload
     PSY_CUDA_TRY(sc->tlas.upload(tl.nodes, st));
     PSY_CUDA_TRY(sc->blas.upload(blas, st));
@@ -927,6 +1021,10 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->emitters.upload(emitters, st));
     PSY_CUDA_TRY(sc->distribution.upload(dist, st));
     PSY_CUDA_TRY(sc->lights.upload(lights, st));
+    PSY_CUDA_TRY(sc->lt_nodes.upload(lt_nodes, st));
+    PSY_CUDA_TRY(sc->lt_emitters.upload(lt_emitters, st));
+    PSY_CUDA_TRY(sc->lt_mapping.upload(lt_mapping, st));
+    PSY_CUDA_TRY(sc->lt_lookup.upload(lt_lookup, st));
     PSY_CUDA_TRY(cudaStreamSynchronize(st));
     psy::SceneView &v = sc->view;
     v.tlas = sc->tlas.as<psy::BvhNodeGpu>();
@@ -955,6 +1053,14 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     v.background[2] = d->background[2];
     v.world_visibility = d->world_visibility;
     v.any_transparent = any_transparent ? 1u : 0u;
+    v.lt_nodes = sc->lt_nodes.as<psy::LtNodeGpu>();
+    v.lt_emitters = sc->lt_emitters.as<psy::LtEmitterGpu>();
+    v.lt_mapping = sc->lt_mapping.as<uint2>();
+    v.lt_lookup = sc->lt_lookup.as<uint4>();
+    v.lt_node_count = uint32_t(lt_nodes.size());
+    v.lt_emitter_count = uint32_t(lt_emitters.size());
+    v.lt_lookup_count = uint32_t(lt_lookup.size());
+    v.lt_root = lt_root;
     sc->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
     *out = sc.release();
     return PSY_OK;
@@ -1251,6 +1357,7 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
     b.sample = reinterpret_cast<uint32_t *>(carve(4 * n));
     b.aov_n = reinterpret_cast<float4 *>(carve(16 * n));
     b.aov_a = reinterpret_cast<float4 *>(carve(16 * n));
+    b.mis_n = reinterpret_cast<float4 *>(carve(16 * n));
     b.hit = reinterpret_cast<float4 *>(carve(16 * n));
     b.hit_prim = reinterpret_cast<uint32_t *>(carve(4 * n));
     b.sh_o = reinterpret_cast<float4 *>(carve(16 * n));
@@ -1399,6 +1506,33 @@ psy_status psy_debug_sobol_samples(psy_context *ctx, uint32_t size, const uint32
     PSY_CUDA_TRY(cudaGetLastError());
     PSY_CUDA_TRY(cudaMemcpyAsync(out_samples, ds.ptr, sizeof(float4) * count, cudaMemcpyDeviceToHost, st));
     PSY_CUDA_TRY(cudaMemcpyAsync(out_indices, di.ptr, sizeof(uint32_t) * count, cudaMemcpyDeviceToHost, st));
+    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    return PSY_OK;
+}
+
+psy_status psy_debug_light_tree(psy_scene *scene, const float *queries, const uint32_t *pdf_emitters, uint32_t count,
+                                uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf) {
+    if (!scene || !queries || !pdf_emitters || !out_emitters || !out_sample_pdf || !out_reverse_pdf)
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    if (scene->view.lt_node_count == 0u || scene->view.lt_emitter_count == 0u)
+        return fail(PSY_ERROR_UNSUPPORTED, "scene has no usable light tree");
+    if (count == 0u) return PSY_OK;
+    PSY_CUDA_TRY(cudaSetDevice(scene->context->device));
+    cudaStream_t st = scene->context->stream;
+    DeviceBuffer dq, de, ds, dsp, drp;
+    std::vector<float> q(queries, queries + 8ull * count);
+    std::vector<uint32_t> e(pdf_emitters, pdf_emitters + count);
+    PSY_CUDA_TRY(dq.upload(q, st));
+    PSY_CUDA_TRY(de.upload(e, st));
+    PSY_CUDA_TRY(ds.alloc(sizeof(uint32_t) * count));
+    PSY_CUDA_TRY(dsp.alloc(sizeof(float) * count));
+    PSY_CUDA_TRY(drp.alloc(sizeof(float) * count));
+    psy::launch_debug_light_tree(st, scene->view, dq.as<float4>(), de.as<uint32_t>(), count, ds.as<uint32_t>(),
+                                 dsp.as<float>(), drp.as<float>());
+    PSY_CUDA_TRY(cudaGetLastError());
+    PSY_CUDA_TRY(cudaMemcpyAsync(out_emitters, ds.ptr, sizeof(uint32_t) * count, cudaMemcpyDeviceToHost, st));
+    PSY_CUDA_TRY(cudaMemcpyAsync(out_sample_pdf, dsp.ptr, sizeof(float) * count, cudaMemcpyDeviceToHost, st));
+    PSY_CUDA_TRY(cudaMemcpyAsync(out_reverse_pdf, drp.ptr, sizeof(float) * count, cudaMemcpyDeviceToHost, st));
     PSY_CUDA_TRY(cudaStreamSynchronize(st));
     return PSY_OK;
 }

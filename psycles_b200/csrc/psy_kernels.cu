@@ -14,6 +14,7 @@
 // never changes a path's result.
 #include "psy_device.cuh"
 #include "psy_kernels.h"
+#include "psy_light_tree.cuh"
 
 namespace psy {
 
@@ -74,6 +75,7 @@ __global__ void k_raygen(RenderParams p, PathBuffers b, uint32_t pixels, uint32_
         b.sample[i] = sample;
         b.aov_n[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         b.aov_a[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        b.mis_n[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         b.queue_in[i] = i;
         if (i == trace_path && trace) {
             trace->pixel_x = x;
@@ -319,7 +321,8 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
             const f3 light_sample = mk3(ls4.x, ls4.y, ls4.z);
             const float light_terminate = sample_4d(p, sample, rng_hash, ps.rng_offset + 2u).x;
             const float4 bs4 = sample_4d(p, sample, rng_hash, ps.rng_offset + 3u);
-            const DistEntryGpu selected = distribution_sample(s, light_sample.z);
+            DistEntryGpu selected = p.use_light_tree ? DistEntryGpu{0.0f, 0.0f, 3u, 0u}
+                                                     : distribution_sample(s, light_sample.z);
             const float4 h4 = b.hit[i];
             const uint32_t prim = b.hit_prim[i];
             if (ev) {
@@ -375,8 +378,14 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
                 float emission_weight = 1.0f;
                 if (p.nee && s.triangle_emitters > 0u && mat.emission_sampling != 0u && mat.has_emission) {
                     const bool competing = depth > 0u && !previous_delta;
-                    const float selection_pdf =
+                    float selection_pdf =
                         0.5f * length(cross(sp.wp1 - sp.wp0, sp.wp2 - sp.wp0)) * s.triangle_area_pdf;
+                    if (p.use_light_tree) {
+                        // light_tree.forward_pdf (src/luisa/path_tracer_light_tree.cpp:799-838)
+                        const float4 mn = b.mis_n[i];
+                        selection_pdf = lt_pdf(s, lt_triangle_emitter(s, sp.object, sp.cycles_prim), ray.o,
+                                               mk3(mn.x, mn.y, mn.z), (ps.flag & kFlagMisHadTransmission) != 0u);
+                    }
                     const float light_pdf = emissive_forward_pdf(selection_pdf, mat.emission_sampling, ray.o,
                                                                  sp.position, sp.wp0, sp.wp1, sp.wp2, sp.ng);
                     const bool available = light_pdf > 0.0f;
@@ -423,6 +432,15 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
                         }
                     }
                     const uint32_t runtime = runtime_flags(closures, sp.back_facing);
+                    if (p.use_light_tree) {
+                        // light-tree pick after shading (src/luisa/path_kernel_pipeline.cpp:150-159)
+                        selected = lt_sample(s, light_sample.z, sp.position, sp.n,
+                                             (runtime & kRuntimeBsdfHasTransmission) != 0u);
+                        if (ev) {
+                            ev->light_kind = selected.kind;
+                            ev->light_index = selected.index;
+                        }
+                    }
                     const uint32_t lobe_mask = terminate_after_transparent ? kEventTransparent : 0xffffffffu;
                     const InstanceGpu &inst = s.instances[sp.instance];
                     // Direct lighting (src/luisa/path_kernel_pipeline.cpp:160-172)
@@ -533,6 +551,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
                             if (!transparent) {
                                 previous_bsdf_pdf = ss.eval.pdf;
                                 previous_delta = singular;
+                                b.mis_n[i] = make_float4(sp.n.x, sp.n.y, sp.n.z, 0.0f);
                             }
                             if (ev) {
                                 ev->bounce = ps.bounce;
@@ -877,6 +896,20 @@ __global__ void k_debug_sobol(const float4 *table, uint32_t size, const uint32_t
     out_index[i] = idx;
 }
 
+__global__ void k_debug_light_tree(SceneView s, const float4 *queries, const uint32_t *pdf_emitters, uint32_t count,
+                                   uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float4 a = queries[2u * i], b = queries[2u * i + 1u];
+    const f3 point = mk3(a.x, a.y, a.z), n = mk3(b.x, b.y, b.z);
+    const bool tr = b.w != 0.0f;
+    const DistEntryGpu e = lt_sample(s, a.w, point, n, tr);
+    const bool valid = e.kind == 0u || e.kind == 1u;
+    out_emitters[i] = valid ? (e.kind == 0u ? e.index : s.triangle_emitters + e.index) : kInvalid;
+    out_sample_pdf[i] = valid ? e.selection_pdf : 0.0f;
+    out_reverse_pdf[i] = lt_pdf(s, pdf_emitters[i], point, n, tr);
+}
+
 // ----------------------------------------------------------------- launches
 
 int launch_grid(uint32_t work, int block, int sms) {
@@ -917,6 +950,11 @@ void launch_film(cudaStream_t st, int sms, const PathBuffers &b, uint32_t pixels
                  float4 *normal, float4 *albedo, uint32_t *sample_count, uint32_t trace_path, psy_path_trace *trace) {
     k_film<<<launch_grid(pixels, 256, sms), 256, 0, st>>>(b, pixels, samples, combined, normal, albedo, sample_count,
                                                         trace_path, trace);
+}
+void launch_debug_light_tree(cudaStream_t st, const SceneView &s, const float4 *queries, const uint32_t *pdf_emitters,
+                             uint32_t count, uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf) {
+    k_debug_light_tree<<<(count + 127u) / 128u, 128, 0, st>>>(s, queries, pdf_emitters, count, out_emitters,
+                                                               out_sample_pdf, out_reverse_pdf);
 }
 void launch_debug_sobol(cudaStream_t st, const float4 *table, uint32_t size, const uint32_t *queries, uint32_t count,
                         float4 *out, uint32_t *out_index) {

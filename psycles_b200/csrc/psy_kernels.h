@@ -20,6 +20,8 @@ void launch_swap(cudaStream_t st, uint32_t *counters);
 void launch_count_rays(cudaStream_t st, const uint32_t *counters, unsigned long long *stats);
 void launch_film(cudaStream_t st, int sms, const PathBuffers &b, uint32_t pixels, uint32_t samples, float4 *combined,
                  float4 *normal, float4 *albedo, uint32_t *sample_count, uint32_t trace_path, psy_path_trace *trace);
+void launch_debug_light_tree(cudaStream_t st, const SceneView &s, const float4 *queries, const uint32_t *pdf_emitters,
+                             uint32_t count, uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf);
 void launch_debug_sobol(cudaStream_t st, const float4 *table, uint32_t size, const uint32_t *queries, uint32_t count,
                         float4 *out, uint32_t *out_index);
 

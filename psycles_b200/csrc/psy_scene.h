@@ -17,6 +17,7 @@
 #include <cstdint>
 
 #include "../../include/psycles_cuda.h"
+#include "psy_light_tree.h"
 
 namespace psy {
 
@@ -90,6 +91,12 @@ struct SceneView {
     float background[3];
     uint32_t world_visibility;
     uint32_t any_transparent;
+    // many-light tree (empty when the scene has no emitter with energy)
+    const LtNodeGpu *lt_nodes;
+    const LtEmitterGpu *lt_emitters;
+    const uint2 *lt_mapping;  // emitter id -> (tree emitter, leaf node)
+    const uint4 *lt_lookup;   // sorted (object, primitive, emitter id)
+    uint32_t lt_node_count, lt_emitter_count, lt_lookup_count, lt_root;
 };
 
 struct RenderParams {
@@ -99,7 +106,7 @@ struct RenderParams {
     uint32_t maximum, minimum, max_diffuse, max_glossy, max_transmission;
     uint32_t transparent_min, transparent_max, steps;
     float clamp_direct, clamp_indirect, inv_rr_threshold;
-    uint32_t direct_mode, nee;
+    uint32_t direct_mode, nee, use_light_tree;
     float cam[12];  // camera_to_world columns c0..c3
     float htan, vtan, shift_x, shift_y, near_clip, far_clip;
     const float4 *sobol;
@@ -118,6 +125,7 @@ struct PathBuffers {
     uint32_t *sample; // absolute sample index
     float4 *aov_n;    // first-surface normal
     float4 *aov_a;    // albedo
+    float4 *mis_n;    // shading normal of the last non-transparent scatter (light-tree MIS)
     float4 *hit;      // t, u, v, instance bits
     uint32_t *hit_prim;
     float4 *sh_o;     // shadow origin, tmax

@@ -23,6 +23,12 @@ import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
 REPO = HERE.parent.parent
+sys.path.insert(0, str(REPO))
+
+from oracle import oracle  # noqa: E402  (seeded emitter records, tree outputs)
+
+# (seed, emitter count) of the light-tree build fixtures
+LIGHT_TREE_CASES = [(1, 12), (2, 100), (3, 1000), (4, 1), (5, 3), (6, 7), (7, 9), (8, 4000)]
 
 
 def _hex_list(text: str) -> list[int]:
@@ -139,6 +145,14 @@ def reference_tables() -> dict:
         "triangle_area_pdf_bits": int(pdfs.view(np.uint32)[0]),
         "light_selection_pdf_bits": int(pdfs.view(np.uint32)[1]),
     }
+    # build_cycles_light_tree over seeded emitter populations: a fingerprint
+    # of every output word, and the node count.
+    cases = []
+    for seed, count in LIGHT_TREE_CASES:
+        tree = oracle.build_light_tree(lib, "ref_build_light_tree", oracle.light_tree_emitter_records(seed, count))
+        cases.append({"seed": seed, "count": count, "nodes": int(len(tree["node_topology"])),
+                      "root": int(tree["root"]), "fingerprint": oracle.light_tree_fingerprint(tree)})
+    out["light_tree"] = cases
     return out
 
 

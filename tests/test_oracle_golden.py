@@ -111,3 +111,56 @@ def test_reference_library_tables_when_built():
         lib.oracle_sobol_table(size, _p(a))
         assert ref.ref_sobol_generate_table(size, _p(b)) == 0
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_light_tree_build_matches_reference_fixtures(oracle_lib, golden):
+    """The oracle's build_cycles_light_tree restatement reproduces every
+    output word (nodes, measures, emitter order, mappings) the reference
+    builder produced for seeded populations (src/sampling/light_tree.cpp)."""
+    cases = golden["reference_tables"]["light_tree"]
+    assert len(cases) >= 6
+    for case in cases:
+        tree = oracle.build_light_tree(oracle_lib, "oracle_build_light_tree",
+                                       oracle.light_tree_emitter_records(case["seed"], case["count"]))
+        assert len(tree["node_topology"]) == case["nodes"], case
+        assert tree["root"] == case["root"], case
+        assert oracle.light_tree_fingerprint(tree) == case["fingerprint"], case
+
+
+def test_light_tree_structure_invariants(oracle_lib):
+    """Parent / child links, leaf ranges and the two identity mappings are
+    consistent; distant emitters sit in the root's right branch."""
+    rec = oracle.light_tree_emitter_records(11, 300)
+    t = oracle.build_light_tree(oracle_lib, "oracle_build_light_tree", rec)
+    topo = t["node_topology"]
+    root = t["root"]
+    assert topo[root][0] == 0xFFFFFFFF and topo[root][5] == 0
+    distant_node = topo[root][2]
+    assert topo[distant_node][5] == 2
+    n = rec.shape[0]
+    by_id = rec[np.argsort(rec[:, 18])]
+    seen = np.zeros(n, bool)
+    for idx, (parent, left, right, first, count, kind) in enumerate(topo):
+        if kind == 0:
+            assert topo[left][0] == idx and topo[right][0] == idx
+        else:
+            for slot in range(first, first + count):
+                eid = t["emitter_ids"][slot]
+                assert not seen[eid]
+                seen[eid] = True
+                assert t["to_tree"][eid] == slot and t["to_leaf"][eid] == idx
+                assert (by_id[eid, 17] != 0.0) == (idx == distant_node)
+    assert seen.all()
+
+
+def test_light_tree_against_reference_library_when_built(oracle_lib):
+    """Fresh populations (not in the fixtures) against oracle/_ref."""
+    if not oracle.REF_LIB.exists():
+        pytest.skip("oracle/_ref not built")
+    ref = ctypes.CDLL(str(oracle.REF_LIB))
+    for seed, count in [(21, 2), (22, 17), (23, 640), (24, 2500)]:
+        rec = oracle.light_tree_emitter_records(seed, count)
+        for max_leaf in (1, 8):
+            a = oracle.build_light_tree(oracle_lib, "oracle_build_light_tree", rec, max_leaf)
+            b = oracle.build_light_tree(ref, "ref_build_light_tree", rec, max_leaf)
+            assert oracle.light_tree_fingerprint(a) == oracle.light_tree_fingerprint(b), (seed, count, max_leaf)
