@@ -137,13 +137,14 @@ typedef enum psy_light_type {
 #define PSY_LIGHT_FLAG_SPHERE 1u      /* point/spot radius is a sphere */
 #define PSY_LIGHT_FLAG_NORMALIZE 2u   /* divide power by emitter area */
 #define PSY_LIGHT_FLAG_ELLIPSE 4u     /* area light: ellipse, else rectangle */
+#define PSY_LIGHT_FLAG_USE_MIS 8u     /* LightDesc::use_mis (contract default on) */
 
 /* Analytic light (LightGpu, src/luisa/path_tracer_types.h:142). */
 typedef struct psy_light_desc {
     uint32_t type;
-    uint32_t flags;
+    uint32_t flags;              /* PSY_LIGHT_FLAG_*; bits 16-31 reserved (0) */
     uint32_t max_bounces;
-    uint32_t reserved;
+    uint32_t visibility;         /* LightDesc::visibility_mask, PSY_VISIBILITY_* */
     float position[3];
     float axis_x[3];
     float axis_y[3];

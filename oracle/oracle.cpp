@@ -1013,6 +1013,115 @@ static AnalyticSample sample_area(const psy_light_desc &l, float3 reference, flo
     return out;
 }
 
+// Derived light flags (path_tracer_scene.cpp:1787-1830): effective use_mis
+// (lamps with a finite extent) and forward intersectability.
+constexpr uint32_t kLightUseMis = 1u << 30, kLightForward = 1u << 31;
+
+// rectangle_solid_angle_context(...).pdf (analytic_light_sampling.h): the
+// directional pdf of the spherical rectangle, planar limit for tiny or
+// grazing rectangles.
+static float rectangle_pdf(float3 reference, float3 center, float3 au, float lu, float3 av, float lv) {
+    const float3 co = center - reference;
+    float z0 = dot(co, cross(au, av));
+    if (z0 > 0.0f) z0 = -z0;
+    const float cu = dot(co, au), cv = dot(co, av);
+    const float x0 = cu - 0.5f * lu, x1 = cu + 0.5f * lu, y0 = cv - 0.5f * lv, y1 = cv + 0.5f * lv;
+    float e[4] = {-y0, x1, y1, -x0};
+    for (float &v : e) v = v / std::sqrt(v * v + z0 * z0);
+    float angles[4];
+    for (int k = 0; k < 4; ++k) angles[k] = asin_(clampf(-e[k] * e[(k + 1) & 3], -1.0f, 1.0f));
+    const float solid = -(angles[0] + angles[1] + angles[2] + angles[3]);
+    const float min_e2 = minf(minf(e[0] * e[0], e[1] * e[1]), minf(e[2] * e[2], e[3] * e[3]));
+    const float cd = length(co);
+    const float planar = safe_div(-(cd * cd * cd), z0 * lu * lv);
+    return (solid < 1.0e-5f || min_e2 > 0.99999f) ? planar : 1.0f / solid;
+}
+
+struct LampHit {
+    bool valid;
+    uint32_t index;
+    float distance, pdf, eval_factor;
+};
+
+// intersect_area (analytic_light_intersection.h:268-353) with the pdf and
+// factor of AreaLightSampling::from_intersection (area_light_sampling.cpp:644-727)
+// at full spread: front side, strictly inside (tmin, tmax).
+static bool lamp_area(const psy_light_desc &l, const Ray &ray, float tmin, float tmax, LampHit &out) {
+    const float3 center = f3(l.position[0], l.position[1], l.position[2]);
+    const float3 au = f3(l.axis_x[0], l.axis_x[1], l.axis_x[2]);
+    const float3 av = f3(l.axis_y[0], l.axis_y[1], l.axis_y[2]);
+    const float3 normal = -f3(l.axis_z[0], l.axis_z[1], l.axis_z[2]);
+    const bool ellipse = (l.flags & PSY_LIGHT_FLAG_ELLIPSE) != 0u;
+    const float denom = dot(ray.d, normal);
+    const float t = safe_div(dot(center - ray.o, normal), denom);
+    const float3 inplane = (ray.o + ray.d * t) - center;
+    const float u = safe_div(dot(inplane, au), l.size_u);
+    const float v = safe_div(dot(inplane, av), l.size_v);
+    bool inside = u >= -0.5f && u <= 0.5f && v >= -0.5f && v <= 0.5f;
+    if (ellipse) inside = inside && u * u + v * v <= 0.25f;
+    if (!(denom < 0.0f && t > tmin && t < tmax && inside)) return false;
+    float pdf;
+    if (ellipse) {
+        const float cosine = dot(normal, -ray.d);
+        pdf = 4.0f * kInvPi / (l.size_u * l.size_v) * (cosine > 0.0f ? t * t / cosine : 0.0f);
+    } else {
+        pdf = rectangle_pdf(ray.o, center, au, l.size_u, av, l.size_v);
+    }
+    float area = l.size_u * l.size_v;
+    if (ellipse) area *= 0.25f * kPi;
+    const bool normalize_power = (l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u;
+    const float eval = kInvPi * ((normalize_power && area != 0.0f) ? safe_div(1.0f, area) : 1.0f) * 1.0f;
+    if (!(area > 0.0f && eval > 0.0f)) return false;
+    out = {true, 0u, t, pdf, eval};
+    return true;
+}
+
+// intersect_point / intersect_spot, oriented-disk case (analytic_light_intersection.h:33-266):
+// the disk of `radius` faces the ray origin.
+static bool lamp_disk(const psy_light_desc &l, const Ray &ray, float tmin, float tmax, LampHit &out) {
+    const float3 center = f3(l.position[0], l.position[1], l.position[2]);
+    const float3 offset = ray.o - center;
+    const float3 n = light_safe_normalize(offset, -ray.d);
+    const float plane = dot(offset, n);
+    const float cosine = dot(n, -ray.d);
+    const float t = safe_div(plane, cosine);
+    const float3 radial = (ray.o + ray.d * t) - center;
+    const bool hit = plane * cosine > 0.0f && t >= 0.0f && dot(radial, radial) < l.radius * l.radius && t > tmin &&
+                     t < tmax && l.radius > 0.0f;
+    if (!hit) return false;
+    float eval = point_eval_factor(l.radius, (l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u);
+    if (l.type == PSY_LIGHT_SPOT) {
+        eval *= spot_attenuation(l, -ray.d);
+        if (!(dot(ray.d, offset) < 0.0f)) return false;
+    }
+    if (!(eval > 0.0f)) return false;
+    out = {true, 0u, t, point_disk_pdf(t * t, cosine, l.radius), eval};
+    return true;
+}
+
+// ClosestEventStageImpl's lamp loop (src/luisa/path_kernel_closest_event.cpp:56-230):
+// the nearest eligible lamp strictly before `event_distance`, ties to the
+// lower index.
+static LampHit closest_lamp(const Scene &s, const Ray &ray, float tmin, float event_distance, uint32_t ray_visibility,
+                            uint32_t excluded) {
+    LampHit best{false, kInvalid, event_distance, 0.0f, 0.0f};
+    const bool camera_path = (ray_visibility & PSY_VISIBILITY_CAMERA) != 0u;
+    for (uint32_t i = 0; i < s.lights.size(); ++i) {
+        const psy_light_desc &l = s.lights[i];
+        if (l.type == PSY_LIGHT_DISTANT || i == excluded) continue;
+        if ((l.visibility & ray_visibility) == 0u) continue;
+        if (!camera_path && (l.flags & kLightUseMis) == 0u) continue;
+        LampHit h{};
+        const bool ok = l.type == PSY_LIGHT_AREA ? lamp_area(l, ray, tmin, best.distance, h)
+                                                 : lamp_disk(l, ray, tmin, best.distance, h);
+        if (ok) {
+            best = h;
+            best.index = i;
+        }
+    }
+    return best;
+}
+
 // --------------------------------------------------------------- shadow
 
 // make_trace_shadow_callable (src/luisa/path_tracer_geometry.cpp:75-174):
@@ -1083,6 +1192,18 @@ static void derive_settings(Settings &st, const Scene &s, const psy_render_setti
 static float power_heuristic(float a, float b) {
     const float a2 = a * a, b2 = b * b;
     return a2 / maxf(a2 + b2, 1.0e-20f);
+}
+
+// forward_light_weight / nee_light_weight (src/luisa/path_tracer_lighting.cpp:35-72).
+static float forward_light_weight(uint32_t mode, float forward_pdf, float nee_pdf, bool competing, bool available) {
+    if (mode == PSY_DIRECT_LIGHT_FORWARD) return 1.0f;
+    if (mode == PSY_DIRECT_LIGHT_NEE) return (competing && available) ? 0.0f : 1.0f;
+    return (competing && available) ? power_heuristic(forward_pdf, nee_pdf) : 1.0f;
+}
+static float nee_light_weight(uint32_t mode, float nee_pdf, float forward_pdf) {
+    if (mode == PSY_DIRECT_LIGHT_NEE) return 1.0f;
+    if (mode == PSY_DIRECT_LIGHT_FORWARD) return forward_pdf <= 0.0f ? 1.0f : 0.0f;
+    return power_heuristic(nee_pdf, forward_pdf);
 }
 
 // film_clamp_light (include/psycles/luisa/cycles_film_light.h:15-49).
@@ -1194,6 +1315,11 @@ static void trace_set3(float *dst, float3 v) {
     dst[1] = v.y;
     dst[2] = v.z;
 }
+static void trace_add3(float *dst, float3 v) {
+    dst[0] += v.x;
+    dst[1] += v.y;
+    dst[2] += v.z;
+}
 
 // One camera sample through the path loop: begin_path_sample
 // (src/luisa/path_kernel_setup.cpp:485-700), PathKernelPipeline::emit
@@ -1259,8 +1385,12 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
     uint32_t ray_visibility = PSY_VISIBILITY_CAMERA;
     uint32_t ray_events = 0u;
     Identity source;
-    const bool nee = r.next_event_estimation != 0u;
-    const uint32_t mode = r.direct_light_sampling;
+    // path_tracer_kernel.cpp:206-223: NEE only when a light can be picked and
+    // the mode is not forward path tracing; without it every emitter is
+    // weighted as forward path tracing.
+    const bool available = st.use_light_tree ? !s.tree.emitters.empty() : s.emitter_count > 0u;
+    const bool nee = r.next_event_estimation != 0u && r.direct_light_sampling != PSY_DIRECT_LIGHT_FORWARD && available;
+    const uint32_t mode = nee ? r.direct_light_sampling : PSY_DIRECT_LIGHT_FORWARD;
 
     for (uint32_t step = 0u; step < st.steps; ++step) {
         psy_path_event *ev = nullptr;
@@ -1301,6 +1431,43 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
             }
         }
         const uint32_t depth = ps.bounce;
+        // Lamps in front of the mesh event are transparent events: they add
+        // their emission, count a transparent bounce and move tmin past
+        // themselves, without a new bounce or new Sobol dimensions
+        // (path_kernel_pipeline.cpp:78-126, path_kernel_forward_light.cpp:14-118).
+        bool lamp_terminated = false;
+        {
+            const float event_distance = hit.valid ? hit.t : ray.tmax;
+            uint32_t excluded = kInvalid;
+            float tmin = ray.tmin;
+            for (;;) {
+                const LampHit lh = closest_lamp(s, ray, tmin, event_distance, ray_visibility, excluded);
+                if (!lh.valid) break;
+                float selection_pdf = s.light_selection_pdf;
+                if (st.use_light_tree)
+                    selection_pdf = lt::tree_pdf(s.tree, static_cast<uint32_t>(s.emitters.size()) + lh.index, ray.o,
+                                                 previous_mis_normal, (ps.flag & kFlagMisHadTransmission) != 0u);
+                const float light_pdf = lh.pdf * selection_pdf;
+                const bool competing = depth > 0u && !previous_delta;
+                const float w = forward_light_weight(mode, previous_bsdf_pdf, light_pdf, competing, light_pdf > 0.0f);
+                const psy_light_desc &l = s.lights[lh.index];
+                const float3 lr = f3(l.color[0], l.color[1], l.color[2]) * (l.power * lh.eval_factor);
+                const float3 c = clamp_contribution(throughput * lr * w, depth, st);
+                radiance += c;
+                if (ev) trace_add3(ev->emission, c);
+                ps.transparent_bounce += 1u;
+                tmin = lh.distance == 0.0f ? std::numeric_limits<float>::min() : bits_float(float_bits(lh.distance) + 1u);
+                excluded = lh.index;
+                if (ps.transparent_bounce >= st.transparent_max) {
+                    lamp_terminated = true;
+                    break;
+                }
+            }
+        }
+        if (lamp_terminated) {
+            if (ev) ev->terminated = 1u;
+            break;
+        }
         if (!hit.valid) {
             // BackgroundEventStage (src/luisa/path_kernel_background_event.cpp:14-160):
             // the constant world is not part of the light distribution, so
@@ -1312,7 +1479,7 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
                 transparency += (throughput.x + throughput.y + throughput.z) * (1.0f / 3.0f);
             } else if (world_visible) {
                 radiance += c;
-                if (ev) trace_set3(ev->emission, c);
+                if (ev) trace_add3(ev->emission, c);
             }
             if (ev) ev->terminated = 1u;
             break;
@@ -1330,14 +1497,12 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
                                              previous_mis_normal, (ps.flag & kFlagMisHadTransmission) != 0u);
             const float light_pdf = emissive_forward_pdf(selection_pdf, mat.emission_sampling, ray.o, sp.position,
                                                          sp.wp0, sp.wp1, sp.wp2, sp.ng);
-            const bool available = light_pdf > 0.0f;
-            if (mode == PSY_DIRECT_LIGHT_FORWARD) emission_weight = 1.0f;
-            else if (mode == PSY_DIRECT_LIGHT_NEE) emission_weight = (competing && available) ? 0.0f : 1.0f;
-            else emission_weight = (competing && available) ? power_heuristic(previous_bsdf_pdf, light_pdf) : 1.0f;
+            const bool light_available = light_pdf > 0.0f;
+            emission_weight = forward_light_weight(mode, previous_bsdf_pdf, light_pdf, competing, light_available);
         }
         const float3 emission_contribution = clamp_contribution(throughput * closures.emission * emission_weight, depth, st);
         radiance += emission_contribution;
-        if (ev) trace_set3(ev->emission, emission_contribution);
+        if (ev) trace_add3(ev->emission, emission_contribution);
         if (terminate_on_next_surface) {
             if (ev) ev->terminated = 1u;
             break;
@@ -1405,8 +1570,7 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
                         const float3 light_radiance = material_emission(s.materials[em.material]);
                         const Evaluation e = evaluate_mixture(closures, sp.n, ls.direction, lobe_mask, -1);
                         float mis = 1.0f;
-                        if (mode == PSY_DIRECT_LIGHT_FORWARD) mis = e.pdf <= 0.0f ? 1.0f : 0.0f;
-                        else if (mode == PSY_DIRECT_LIGHT_MIS) mis = power_heuristic(pdf, e.pdf);
+                        mis = nee_light_weight(mode, pdf, e.pdf);
                         const float3 weighted = e.f * light_radiance * (mis / pdf);
                         if (any_nonzero(weighted)) {
                             const float3 unshadowed = weighted * f3(1.0f);
@@ -1437,7 +1601,9 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
                     if (a.valid && light_pdf > 0.0f) {
                         const float3 light_radiance = f3(l.color[0], l.color[1], l.color[2]) * (l.power * a.eval_factor);
                         const Evaluation e = evaluate_mixture(closures, sp.n, a.direction, lobe_mask, -1);
-                        const float3 weighted = e.f * light_radiance * (1.0f / maxf(light_pdf, 1.0e-20f));
+                        // MIS only for lamps a BSDF ray can also hit (path_kernel_nee_analytic.cpp:286-292)
+                        const float mis = (l.flags & kLightForward) != 0u ? nee_light_weight(mode, light_pdf, e.pdf) : 1.0f;
+                        const float3 weighted = e.f * light_radiance * (mis / maxf(light_pdf, 1.0e-20f));
                         if (any_nonzero(weighted)) {
                             const float3 unshadowed = weighted * f3(1.0f);
                             const float3 surviving = unshadowed * light_roulette_weight(unshadowed, light_terminate, st.inv_rr_threshold);
@@ -1569,6 +1735,16 @@ static std::unique_ptr<Scene> prepare_scene(const psy_scene_desc *d, bool brute_
         s->instances.push_back(inst);
     }
     s->lights.assign(d->lights, d->lights + d->light_count);
+    for (psy_light_desc &l : s->lights) {
+        bool extent = true;  // path_tracer_scene.cpp:1787-1830
+        if (l.type == PSY_LIGHT_POINT || l.type == PSY_LIGHT_SPOT) extent = l.radius > 0.0f;
+        if (l.type == PSY_LIGHT_AREA) extent = l.size_u != 0.0f && l.size_v != 0.0f && l.spread > 0.0f;
+        if (l.type == PSY_LIGHT_DISTANT) extent = l.angle > 0.0f;
+        if ((l.flags & PSY_LIGHT_FLAG_USE_MIS) != 0u && extent) {
+            l.flags |= kLightUseMis;
+            if (l.type != PSY_LIGHT_DISTANT) l.flags |= kLightForward;
+        }
+    }
     s->camera = d->camera;
     s->background = f3(d->background[0], d->background[1], d->background[2]);
     s->world_visibility = d->world_visibility;

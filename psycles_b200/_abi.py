@@ -21,7 +21,7 @@ STATUS_NAMES = {
 
 CLOSURE_NULL, CLOSURE_DIFFUSE, CLOSURE_EMISSION, CLOSURE_TRANSPARENT, CLOSURE_ADD, CLOSURE_MIX = range(6)
 LIGHT_POINT, LIGHT_SPOT, LIGHT_AREA, LIGHT_DISTANT = range(4)
-LIGHT_FLAG_SPHERE, LIGHT_FLAG_NORMALIZE, LIGHT_FLAG_ELLIPSE = 1, 2, 4
+LIGHT_FLAG_SPHERE, LIGHT_FLAG_NORMALIZE, LIGHT_FLAG_ELLIPSE, LIGHT_FLAG_USE_MIS = 1, 2, 4, 8
 VIS_CAMERA, VIS_DIFFUSE, VIS_GLOSSY, VIS_TRANSMISSION, VIS_SHADOW, VIS_VOLUME = 1, 2, 4, 8, 16, 32
 VIS_ALL = 63
 EMISSION_NONE, EMISSION_AUTOMATIC, EMISSION_FRONT, EMISSION_BACK, EMISSION_FRONT_BACK = range(5)
@@ -57,7 +57,7 @@ class MaterialDesc(ctypes.Structure):
 
 class LightDesc(ctypes.Structure):
     _fields_ = [("type", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("max_bounces", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32), ("position", ctypes.c_float * 3), ("axis_x", ctypes.c_float * 3),
+                ("visibility", ctypes.c_uint32), ("position", ctypes.c_float * 3), ("axis_x", ctypes.c_float * 3),
                 ("axis_y", ctypes.c_float * 3), ("axis_z", ctypes.c_float * 3), ("axis_scale", ctypes.c_float * 3),
                 ("color", ctypes.c_float * 3), ("power", ctypes.c_float), ("radius", ctypes.c_float),
                 ("size_u", ctypes.c_float), ("size_v", ctypes.c_float), ("spot_angle", ctypes.c_float),

@@ -905,6 +905,79 @@ struct AnalyticSample {
     float distance, pdf, eval_factor;
 };
 
+// rectangle_solid_angle_context (include/psycles/luisa/analytic_light_sampling.h:
+// Ureña et al. spherical rectangle seen from `reference`, with the planar pdf
+// limit for tiny or grazing rectangles).
+struct RectContext {
+    f3 z;
+    float z0, x0, x1, y0, y1;
+    float e[4], g[4];
+    float solid, pdf;
+};
+
+__device__ __forceinline__ RectContext rect_context(f3 reference, f3 center, f3 au, float lu, f3 av, float lv) {
+    RectContext c;
+    c.z = cross(au, av);
+    const f3 co = center - reference;
+    c.z0 = dot(co, c.z);
+    if (c.z0 > 0.0f) {
+        c.z = -c.z;
+        c.z0 = -c.z0;
+    }
+    const float cu = dot(co, au), cv = dot(co, av);
+    c.x0 = cu - 0.5f * lu;
+    c.x1 = cu + 0.5f * lu;
+    c.y0 = cv - 0.5f * lv;
+    c.y1 = cv + 0.5f * lv;
+    c.e[0] = -c.y0;
+    c.e[1] = c.x1;
+    c.e[2] = c.y1;
+    c.e[3] = -c.x0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c.e[k] = c.e[k] / sqrtf(c.e[k] * c.e[k] + c.z0 * c.z0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c.g[k] = asin_(clampf_(-c.e[k] * c.e[(k + 1) & 3], -1.0f, 1.0f));
+    c.solid = -(c.g[0] + c.g[1] + c.g[2] + c.g[3]);
+    const float min_e2 =
+        minf_(minf_(c.e[0] * c.e[0], c.e[1] * c.e[1]), minf_(c.e[2] * c.e[2], c.e[3] * c.e[3]));
+    const float cd = length(co);
+    const float pden = c.z0 * lu * lv;
+    const float planar = pden != 0.0f ? -(cd * cd * cd) / pden : 0.0f;
+    c.pdf = (c.solid < 1.0e-5f || min_e2 > 0.99999f) ? planar : 1.0f / c.solid;
+    return c;
+}
+
+// point_eval_factor (analytic_light_sampling.h:880-896): 1/(pi area) with
+// the sphere's area for a finite radius and 4 for a delta point.
+__device__ __forceinline__ float point_eval_factor(const psy_light_desc &l) {
+    const float r2 = l.radius * l.radius;
+    const float area = r2 > 0.0f ? 4.0f * kPi * r2 : 4.0f;
+    return ((l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u ? 1.0f / maxf_(area, 1.0e-20f) : 1.0f) * kInvPi;
+}
+
+// spot_light_to_local + spot_light_attenuation (analytic_light_sampling.h:309-345)
+// for the direction `from_light` leaving the lamp.
+__device__ __forceinline__ float spot_attenuation(const psy_light_desc &l, f3 from_light) {
+    const f3 ax = ld3(l.axis_x) * l.axis_scale[0];
+    const f3 ay = ld3(l.axis_y) * l.axis_scale[1];
+    const f3 az = ld3(l.axis_z) * l.axis_scale[2];
+    const f3 adj_x = cross(ay, az);
+    const float det = dot(ax, adj_x);
+    const bool valid = fabsf(det) > 1.0e-20f;
+    const float inv_det = 1.0f / (valid ? det : 1.0f);
+    const f3 rx = adj_x * inv_det, ry = cross(az, ax) * inv_det, rz = cross(ax, ay) * inv_det;
+    f3 local = light_safe_normalize(mk3(dot(rx, from_light), dot(ry, from_light), dot(rz, from_light)),
+                                    mk3(0.0f, 0.0f, -1.0f));
+    local.z = -local.z;
+    const float cos_half = cos_(0.5f * l.spot_angle);
+    const float blend = (1.0f - cos_half) * l.spot_smooth;
+    const float ratio = blend != 0.0f ? (local.z - cos_half) / blend : 0.0f;
+    const float lin = clampf_(ratio, 0.0f, 1.0f);
+    const float smooth = lin * lin * (3.0f - 2.0f * lin);
+    const float hard = local.z >= cos_half ? 1.0f : 0.0f;
+    return blend > 0.0f ? smooth : hard;
+}
+
 // include/psycles/luisa/analytic_light_sampling.h:84-108 (distant),
 // :549-603 (disk), :856-896 (pdf / eval factor), :309-345 (spot profile).
 __device__ __forceinline__ AnalyticSample sample_analytic(const psy_light_desc &l, f3 reference, f2 rnd) {
@@ -944,29 +1017,13 @@ __device__ __forceinline__ AnalyticSample sample_analytic(const psy_light_desc &
         f3 position;
         float pdf;
         if (!ellipse) {
-            f3 z = cross(au, av);
-            const f3 co = center - reference;
-            float z0 = dot(co, z);
-            if (z0 > 0.0f) {
-                z = -z;
-                z0 = -z0;
-            }
-            const float cu = dot(co, au), cv = dot(co, av);
-            const float x0 = cu - 0.5f * lu, x1 = cu + 0.5f * lu, y0 = cv - 0.5f * lv, y1 = cv + 0.5f * lv;
-            float e[4] = {-y0, x1, y1, -x0};
-#pragma unroll
-            for (int k = 0; k < 4; ++k) e[k] = e[k] / sqrtf(e[k] * e[k] + z0 * z0);
-            float g[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) g[k] = asin_(clampf_(-e[k] * e[(k + 1) & 3], -1.0f, 1.0f));
-            const float solid = -(g[0] + g[1] + g[2] + g[3]);
-            const float min_e2 = minf_(minf_(e[0] * e[0], e[1] * e[1]), minf_(e[2] * e[2], e[3] * e[3]));
-            const float cd = length(co);
-            const float pden = z0 * lu * lv;
-            const float planar = pden != 0.0f ? -(cd * cd * cd) / pden : 0.0f;
-            pdf = (solid < 1.0e-5f || min_e2 > 0.99999f) ? planar : 1.0f / solid;
-            const float b0 = e[0], b1 = e[2];
-            const float alpha = rnd.x * solid + g[2] + g[3];
+            const RectContext c = rect_context(reference, center, au, lu, av, lv);
+            const f3 z = c.z;
+            const float z0 = c.z0, x0 = c.x0, x1 = c.x1, y0 = c.y0, y1 = c.y1;
+            pdf = c.pdf;
+            const float solid = c.solid;
+            const float b0 = c.e[0], b1 = c.e[2];
+            const float alpha = rnd.x * solid + c.g[2] + c.g[3];
             const float sa = sin_(alpha);
             const float fu = sa != 0.0f ? (cos_(alpha) * b0 + b1) / sa : 0.0f;
             float cos_u = copysignf(1.0f / sqrtf(fu * fu + b0 * b0), fu);
@@ -1026,35 +1083,103 @@ __device__ __forceinline__ AnalyticSample sample_analytic(const psy_light_desc &
     const float r2 = l.radius * l.radius;
     const float inv_area = r2 > 0.0f ? 1.0f / maxf_(r2 * kPi, 1.0e-20f) : 1.0f;
     out.pdf = cosine > 0.0f ? inv_area * d2 / cosine : 0.0f;
-    const float area = r2 > 0.0f ? 4.0f * kPi * r2 : 4.0f;
-    float eval = (normalize_power ? 1.0f / maxf_(area, 1.0e-20f) : 1.0f) * kInvPi;
-    if (l.type == PSY_LIGHT_SPOT) {
-        const f3 ax = ld3(l.axis_x) * l.axis_scale[0];
-        const f3 ay = ld3(l.axis_y) * l.axis_scale[1];
-        const f3 az = ld3(l.axis_z) * l.axis_scale[2];
-        const f3 adj_x = cross(ay, az);
-        const float det = dot(ax, adj_x);
-        const bool valid = fabsf(det) > 1.0e-20f;
-        const float inv_det = 1.0f / (valid ? det : 1.0f);
-        const f3 rx = adj_x * inv_det, ry = cross(az, ax) * inv_det, rz = cross(ax, ay) * inv_det;
-        const f3 from_light = -dir;
-        f3 local = light_safe_normalize(mk3(dot(rx, from_light), dot(ry, from_light), dot(rz, from_light)),
-                                        mk3(0.0f, 0.0f, -1.0f));
-        local.z = -local.z;
-        const float cos_half = cos_(0.5f * l.spot_angle);
-        const float blend = (1.0f - cos_half) * l.spot_smooth;
-        const float ratio = blend != 0.0f ? (local.z - cos_half) / blend : 0.0f;
-        const float lin = clampf_(ratio, 0.0f, 1.0f);
-        const float smooth = lin * lin * (3.0f - 2.0f * lin);
-        const float hard = local.z >= cos_half ? 1.0f : 0.0f;
-        eval *= blend > 0.0f ? smooth : hard;
-    }
+    float eval = point_eval_factor(l);
+    if (l.type == PSY_LIGHT_SPOT) eval *= spot_attenuation(l, -dir);
     out.eval_factor = eval;
     out.direction = dir;
     out.position = position;
     out.distance = dist;
     out.valid = cd2 > 0.0f && cosine > 0.0f && eval != 0.0f;
     return out;
+}
+
+
+// ------------------------------------------------- forward lamp events
+
+// A lamp in front of the committed mesh event: ClosestEventStageImpl's lamp
+// loop (src/luisa/path_kernel_closest_event.cpp:56-230) over the
+// intersections of include/psycles/luisa/analytic_light_intersection.h.
+struct LampHit {
+    bool valid;
+    uint32_t index;
+    float distance, pdf, eval_factor;
+};
+
+// intersect_area (analytic_light_intersection.h:268-353) at full spread:
+// strictly inside (tmin, tmax), front side only; the directional pdf of
+// AreaLightSampling::from_intersection (src/luisa/area_light_sampling.cpp:644-727).
+__device__ __forceinline__ bool intersect_area_lamp(const psy_light_desc &l, f3 o, f3 d, float tmin, float tmax,
+                                                    float &distance, float &pdf, float &eval) {
+    const f3 center = ld3(l.position), au = ld3(l.axis_x), av = ld3(l.axis_y);
+    const f3 normal = -ld3(l.axis_z);
+    const float lu = l.size_u, lv = l.size_v;
+    const bool ellipse = (l.flags & PSY_LIGHT_FLAG_ELLIPSE) != 0u;
+    const float dn = dot(d, normal);
+    const float num = dot(center - o, normal);
+    distance = dn != 0.0f ? num / dn : 0.0f;
+    const f3 inplane = (o + d * distance) - center;
+    const float u = lu != 0.0f ? dot(inplane, au) / lu : 0.0f;
+    const float v = lv != 0.0f ? dot(inplane, av) / lv : 0.0f;
+    const bool inside = u >= -0.5f && u <= 0.5f && v >= -0.5f && v <= 0.5f && (!ellipse || u * u + v * v <= 0.25f);
+    if (!(dn < 0.0f && distance > tmin && distance < tmax && inside)) return false;
+    if (!ellipse) {
+        pdf = rect_context(o, center, au, lu, av, lv).pdf;
+    } else {
+        const float cosine = dot(normal, -d);
+        pdf = 4.0f * kInvPi / (lu * lv) * (cosine > 0.0f ? (distance * distance) / cosine : 0.0f);
+    }
+    float area = lu * lv;
+    if (ellipse) area *= 0.25f * kPi;
+    const float inv_area = ((l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u && area != 0.0f) ? 1.0f / area : 1.0f;
+    eval = kInvPi * inv_area * 1.0f;
+    return area > 0.0f && eval > 0.0f;
+}
+
+// intersect_point / intersect_spot (analytic_light_intersection.h:33-266)
+// for the oriented-disk geometry (radius > 0, not a sphere): the disk faces
+// the ray origin.
+__device__ __forceinline__ bool intersect_disk_lamp(const psy_light_desc &l, f3 o, f3 d, float tmin, float tmax,
+                                                    float &distance, float &pdf, float &eval) {
+    const f3 center = ld3(l.position);
+    const f3 offset = o - center;
+    const f3 ln = light_safe_normalize(offset, -d);
+    const float plane = dot(offset, ln);
+    const float cosine = dot(ln, -d);
+    distance = cosine != 0.0f ? plane / cosine : 0.0f;
+    const f3 radial = (o + d * distance) - center;
+    const float r2 = l.radius * l.radius;
+    const bool hit = plane * cosine > 0.0f && distance >= 0.0f && dot(radial, radial) < r2 && distance > tmin &&
+                     distance < tmax;
+    if (!(hit && l.radius > 0.0f)) return false;
+    const float inv_area = r2 > 0.0f ? 1.0f / maxf_(r2 * kPi, 1.0e-20f) : 1.0f;
+    pdf = cosine > 0.0f ? inv_area * (distance * distance) / cosine : 0.0f;
+    eval = point_eval_factor(l);
+    if (l.type == PSY_LIGHT_SPOT) {
+        eval *= spot_attenuation(l, -d);
+        if (!(dot(d, offset) < 0.0f)) return false;
+    }
+    return eval > 0.0f;
+}
+
+// Nearest eligible lamp strictly inside (tmin, event_distance); ties keep the
+// lower index.  Eligibility: the lamp's visibility covers the ray, the ray
+// is a camera ray or the lamp takes part in MIS, and it is not the lamp the
+// previous event hit.
+__device__ __forceinline__ LampHit closest_lamp(const SceneView &s, f3 o, f3 d, float tmin, float event_distance,
+                                                uint32_t ray_visibility, uint32_t excluded) {
+    LampHit best{false, kInvalid, event_distance, 0.0f, 0.0f};
+    const bool camera_path = (ray_visibility & PSY_VISIBILITY_CAMERA) != 0u;
+    for (uint32_t li = 0; li < s.light_count; ++li) {
+        const psy_light_desc &l = s.lights[li];
+        if (l.type == PSY_LIGHT_DISTANT) continue;
+        const bool use_mis = (l.flags & kLightFlagUseMis) != 0u;
+        if (!((l.visibility & ray_visibility) != 0u && (camera_path || use_mis) && li != excluded)) continue;
+        float distance = 0.0f, pdf = 0.0f, eval = 0.0f;
+        const bool hit = l.type == PSY_LIGHT_AREA ? intersect_area_lamp(l, o, d, tmin, best.distance, distance, pdf, eval)
+                                                  : intersect_disk_lamp(l, o, d, tmin, best.distance, distance, pdf, eval);
+        if (hit) best = LampHit{true, li, distance, pdf, eval};
+    }
+    return best;
 }
 
 }  // namespace psy

@@ -492,12 +492,16 @@ psy_status derive_params(psy_session *s, const psy_render_settings &r) {
     p.clamp_indirect = r.sample_clamp_indirect;
     p.inv_rr_threshold = (!r.use_light_tree && r.light_sampling_threshold > 0.0f)
                              ? r.film_exposure / r.light_sampling_threshold : 0.0f;
-    p.direct_mode = r.direct_light_sampling;
-    p.nee = r.next_event_estimation;
-    // the tree is used only where the scene has one
-    // (src/luisa/path_tracer_kernel.cpp:206-209)
-    p.use_light_tree = (r.use_light_tree && s->scene->view.lt_node_count > 0u && s->scene->view.lt_emitter_count > 0u)
-                           ? 1u : 0u;
+    // the tree is used only where the scene has one; NEE runs only when a
+    // light can be picked and the mode is not forward path tracing, and
+    // without NEE every emitter is weighted as forward path tracing
+    // (src/luisa/path_tracer_kernel.cpp:206-223)
+    const psy::SceneView &sv = s->scene->view;
+    p.use_light_tree = (r.use_light_tree && sv.lt_node_count > 0u && sv.lt_emitter_count > 0u) ? 1u : 0u;
+    const bool available = p.use_light_tree ? sv.lt_emitter_count > 0u : sv.emitter_count > 0u;
+    const bool nee = r.next_event_estimation != 0u && r.direct_light_sampling != PSY_DIRECT_LIGHT_FORWARD && available;
+    p.nee = nee ? 1u : 0u;
+    p.direct_mode = nee ? r.direct_light_sampling : PSY_DIRECT_LIGHT_FORWARD;
     // camera parameters (src/luisa/path_tracer_kernel.cpp:225-280)
     const psy_camera_desc &c = s->scene->camera;
     const float aspect = static_cast<float>(std::max(r.full_width, 1u)) / static_cast<float>(std::max(r.full_height, 1u));
@@ -729,6 +733,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         if (l.type == PSY_LIGHT_AREA && !(l.size_u > 0.0f && l.size_v > 0.0f))
             return fail(PSY_ERROR_INVALID_ARGUMENT, "area light with an empty size");
         if (l.type > PSY_LIGHT_DISTANT) return fail(PSY_ERROR_INVALID_ARGUMENT, "unknown light type");
+        if ((l.flags >> 16) != 0u) return fail(PSY_ERROR_INVALID_ARGUMENT, "reserved light flag bits are set");
         if ((l.flags & PSY_LIGHT_FLAG_SPHERE) && l.radius > 0.0f)
             return fail(PSY_ERROR_UNSUPPORTED, "spherical point lights are not available in this build");
     }
@@ -943,6 +948,16 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         dist.back().cumulative = 1.0f;
     }
     std::vector<psy_light_desc> lights(d->lights, d->lights + d->light_count);
+    // effective use_mis and forward intersectability (path_tracer_scene.cpp:1787-1830)
+    for (psy_light_desc &l : lights) {
+        bool extent = true;
+        if (l.type == PSY_LIGHT_POINT || l.type == PSY_LIGHT_SPOT) extent = l.radius > 0.0f;
+        else if (l.type == PSY_LIGHT_AREA) extent = l.size_u != 0.0f && l.size_v != 0.0f && l.spread > 0.0f;
+        else if (l.type == PSY_LIGHT_DISTANT) extent = l.angle > 0.0f;
+        const bool mis = (l.flags & PSY_LIGHT_FLAG_USE_MIS) != 0u && extent;
+        if (mis) l.flags |= psy::kLightFlagUseMis;
+        if (mis && l.type != PSY_LIGHT_DISTANT) l.flags |= psy::kLightFlagForward;
+    }
 
     // ---- many-light tree over the same emitter population
     // (src/luisa/path_tracer_light_sampling_scene.cpp:160-240)
@@ -1048,6 +1063,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     v.triangle_emitters = tri_n;
     v.light_count = light_n;
     v.triangle_area_pdf = triangle_area_pdf;
+    v.light_selection_pdf = light_selection_pdf;
     v.background[0] = d->background[0];
     v.background[1] = d->background[1];
     v.background[2] = d->background[2];

@@ -31,6 +31,11 @@ __device__ __forceinline__ uint32_t warp_push(uint32_t *counter, bool pred) {
 
 __device__ __forceinline__ Xform xform12(const float *m) { return {ld3(m), ld3(m + 3), ld3(m + 6), ld3(m + 9)}; }
 
+__device__ __forceinline__ void add3(float *d, f3 v) {
+    d[0] += v.x;
+    d[1] += v.y;
+    d[2] += v.z;
+}
 __device__ __forceinline__ void set3(float *d, f3 v) {
     d[0] = v.x;
     d[1] = v.y;
@@ -193,6 +198,20 @@ __device__ __forceinline__ float power_heuristic(float a, float c) {
     return a2 / maxf_(a2 + c2, 1.0e-20f);
 }
 
+// forward_light_weight / nee_light_weight (src/luisa/path_tracer_lighting.cpp:35-72)
+// for the effective direct-light mode.
+__device__ __forceinline__ float forward_light_weight(uint32_t mode, float forward_pdf, float nee_pdf, bool competing,
+                                                      bool nee_available) {
+    if (mode == PSY_DIRECT_LIGHT_FORWARD) return 1.0f;
+    if (mode == PSY_DIRECT_LIGHT_NEE) return (competing && nee_available) ? 0.0f : 1.0f;
+    return (competing && nee_available) ? power_heuristic(forward_pdf, nee_pdf) : 1.0f;
+}
+__device__ __forceinline__ float nee_light_weight(uint32_t mode, float nee_pdf, float forward_pdf) {
+    if (mode == PSY_DIRECT_LIGHT_NEE) return 1.0f;
+    if (mode == PSY_DIRECT_LIGHT_FORWARD) return forward_pdf <= 0.0f ? 1.0f : 0.0f;
+    return power_heuristic(nee_pdf, forward_pdf);
+}
+
 // film_clamp_light (include/psycles/luisa/cycles_film_light.h:15-49).
 __device__ __forceinline__ f3 clamp_contribution(f3 c, uint32_t depth, const RenderParams &p) {
     c = mk3(isfinite(c.x) ? c.x : 0.0f, isfinite(c.y) ? c.y : 0.0f, isfinite(c.z) ? c.z : 0.0f);
@@ -343,7 +362,44 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
             }
             const uint32_t depth = ps.bounce;
             bool alive = true;
-            if (prim == kInvalid) {
+            if (s.light_count > 0u) {
+                // Lamps in front of the mesh event are transparent events that
+                // add their emission without a new bounce or new dimensions
+                // (src/luisa/path_kernel_pipeline.cpp:78-126,
+                // src/luisa/path_kernel_forward_light.cpp:14-118).
+                const float event_distance = prim == kInvalid ? ray.tmax : h4.x;
+                uint32_t excluded = kInvalid;
+                float tmin = ray.tmin;
+                for (uint32_t guard = 0; guard <= s.light_count && alive; ++guard) {
+                    const LampHit lh = closest_lamp(s, ray.o, ray.d, tmin, event_distance, ray_visibility, excluded);
+                    if (!lh.valid) break;
+                    float selection_pdf = s.light_selection_pdf;
+                    if (p.use_light_tree) {
+                        const float4 mn = b.mis_n[i];
+                        selection_pdf = lt_pdf(s, s.triangle_emitters + lh.index, ray.o, mk3(mn.x, mn.y, mn.z),
+                                               (ps.flag & kFlagMisHadTransmission) != 0u);
+                    }
+                    const float light_pdf = lh.pdf * selection_pdf;
+                    const bool competing = depth > 0u && !previous_delta;
+                    const float w = forward_light_weight(p.direct_mode, previous_bsdf_pdf, light_pdf, competing,
+                                                         light_pdf > 0.0f);
+                    const psy_light_desc &l = s.lights[lh.index];
+                    const f3 lr = ld3(l.color) * (l.power * lh.eval_factor);
+                    const f3 c = clamp_contribution(throughput * lr * w, depth, p);
+                    radiance = radiance + c;
+                    if (ev) add3(ev->emission, c);
+                    ps.transparent_bounce += 1u;
+                    tmin = next_float_up(lh.distance);
+                    excluded = lh.index;
+                    if (ps.transparent_bounce >= p.transparent_max) {
+                        alive = false;
+                        if (ev) ev->terminated = 1u;
+                    }
+                }
+            }
+            if (!alive) {
+                // a lamp event used up the transparent budget
+            } else if (prim == kInvalid) {
                 // BackgroundEventStage (src/luisa/path_kernel_background_event.cpp:14-160)
                 const f3 bg = ld3(s.background);
                 const f3 c = clamp_contribution(throughput * bg * 1.0f, depth, p);
@@ -353,7 +409,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
                     transparency += (throughput.x + throughput.y + throughput.z) * (1.0f / 3.0f);
                 } else if (world_visible) {
                     radiance = radiance + c;
-                    if (ev) set3(ev->emission, c);
+                    if (ev) add3(ev->emission, c);
                 }
                 if (ev) ev->terminated = 1u;
                 alive = false;
@@ -389,13 +445,11 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
                     const float light_pdf = emissive_forward_pdf(selection_pdf, mat.emission_sampling, ray.o,
                                                                  sp.position, sp.wp0, sp.wp1, sp.wp2, sp.ng);
                     const bool available = light_pdf > 0.0f;
-                    if (p.direct_mode == PSY_DIRECT_LIGHT_NEE) emission_weight = (competing && available) ? 0.0f : 1.0f;
-                    else if (p.direct_mode == PSY_DIRECT_LIGHT_MIS)
-                        emission_weight = (competing && available) ? power_heuristic(previous_bsdf_pdf, light_pdf) : 1.0f;
+                    emission_weight = forward_light_weight(p.direct_mode, previous_bsdf_pdf, light_pdf, competing, available);
                 }
                 const f3 ec = clamp_contribution(throughput * closures.emission * emission_weight, depth, p);
                 radiance = radiance + ec;
-                if (ev) set3(ev->emission, ec);
+                if (ev) add3(ev->emission, ec);
                 if (terminate_on_next_surface) {
                     alive = false;
                     if (ev) ev->terminated = 1u;
@@ -466,9 +520,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
                                 if (!reject_self) {
                                     const f3 light_radiance = material_emission(s, s.materials[em.material]);
                                     const Evaluation e = evaluate_mixture(closures, sp.n, ls.direction, lobe_mask, -1);
-                                    float mis = 1.0f;
-                                    if (p.direct_mode == PSY_DIRECT_LIGHT_FORWARD) mis = e.pdf <= 0.0f ? 1.0f : 0.0f;
-                                    else if (p.direct_mode == PSY_DIRECT_LIGHT_MIS) mis = power_heuristic(pdf, e.pdf);
+                                    const float mis = nee_light_weight(p.direct_mode, pdf, e.pdf);
                                     const f3 weighted = e.f * light_radiance * (mis / pdf);
                                     if (any_nonzero(weighted)) {
                                         const f3 unshadowed = weighted * mk3(1.0f);
@@ -493,7 +545,11 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
                                 if (a.valid && light_pdf > 0.0f) {
                                     const f3 light_radiance = ld3(l.color) * (l.power * a.eval_factor);
                                     const Evaluation e = evaluate_mixture(closures, sp.n, a.direction, lobe_mask, -1);
-                                    const f3 weighted = e.f * light_radiance * (1.0f / maxf_(light_pdf, 1.0e-20f));
+                                    // MIS only for lamps a BSDF ray can also hit
+                                    // (path_kernel_nee_analytic.cpp:286-292)
+                                    const float mis = (l.flags & kLightFlagForward) != 0u
+                                                          ? nee_light_weight(p.direct_mode, light_pdf, e.pdf) : 1.0f;
+                                    const f3 weighted = e.f * light_radiance * (mis / maxf_(light_pdf, 1.0e-20f));
                                     if (any_nonzero(weighted)) {
                                         const f3 unshadowed = weighted * mk3(1.0f);
                                         surviving = unshadowed *

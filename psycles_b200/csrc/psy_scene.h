@@ -23,6 +23,12 @@ namespace psy {
 
 constexpr uint32_t kInvalidId = 0xffffffffu;
 
+// Light flags the host derives at compile (src/luisa/path_tracer_scene.cpp:1787-1830):
+// the effective use_mis (MIS only for lamps with a finite extent) and
+// whether BSDF / camera rays can hit the lamp.
+constexpr uint32_t kLightFlagUseMis = 1u << 30;
+constexpr uint32_t kLightFlagForward = 1u << 31;
+
 struct alignas(16) BvhNodeGpu {
     float4 x;    // left.lo.x, left.hi.x, right.lo.x, right.hi.x
     float4 y;    // left.lo.y, left.hi.y, right.lo.y, right.hi.y
@@ -88,6 +94,7 @@ struct SceneView {
     uint32_t triangle_emitters;
     uint32_t light_count;
     float triangle_area_pdf;
+    float light_selection_pdf;
     float background[3];
     uint32_t world_visibility;
     uint32_t any_transparent;

@@ -70,6 +70,8 @@ class Light:
     spread: float = math.pi
     flags: int = _abi.LIGHT_FLAG_NORMALIZE
     max_bounces: int = 1024
+    use_mis: bool = True            # LightDesc::use_mis
+    visibility: int = _abi.VIS_ALL  # LightDesc::visibility_mask
 
 
 @dataclasses.dataclass
@@ -150,7 +152,8 @@ class SceneDescHandle:
         lights = (_abi.LightDesc * max(len(scene.lights), 1))()
         for i, l in enumerate(scene.lights):
             d = lights[i]
-            d.type, d.flags, d.max_bounces = l.type, l.flags, l.max_bounces
+            d.type, d.max_bounces, d.visibility = l.type, l.max_bounces, l.visibility
+            d.flags = l.flags | (_abi.LIGHT_FLAG_USE_MIS if l.use_mis else 0)
             d.position[:] = l.position
             d.axis_x[:] = l.axis_x
             d.axis_y[:] = l.axis_y
@@ -351,7 +354,9 @@ def procedural_scene(seed: int = 0, frequencies=(10, 14, 18, 22, 27, 32, 38, 44)
                 flags = _abi.LIGHT_FLAG_NORMALIZE
                 if lt == _abi.LIGHT_AREA and rng.random() < 0.5:
                     flags |= _abi.LIGHT_FLAG_ELLIPSE
-                lights.append(Light(lt, color, float(rng.uniform(200.0, 800.0)), position=pos,
+                # half of the point / spot lamps have a finite (disk) radius
+                radius = float(rng.uniform(0.1, 0.5)) if rng.random() < 0.5 else 0.0
+                lights.append(Light(lt, color, float(rng.uniform(200.0, 800.0)), position=pos, radius=radius,
                                     axis_x=tuple(xf[:3, 0].tolist()), axis_y=tuple(xf[:3, 1].tolist()),
                                     axis_z=tuple(xf[:3, 2].tolist()),
                                     spot_angle=float(math.radians(rng.uniform(30, 90))),
@@ -407,8 +412,8 @@ def small_test_scene(seed: int = 0, transparent: bool = True, lights: bool = Tru
         instances.append(Instance(1 + (i % 2), 2 + i, xf))
     ls = []
     if lights:
-        ls = [Light(_abi.LIGHT_POINT, (1.0, 0.9, 0.8), 80.0, position=(2.0, 4.0, 1.0)),
-              Light(_abi.LIGHT_SPOT, (0.8, 0.9, 1.0), 120.0, position=(-2.0, 4.5, 2.0),
+        ls = [Light(_abi.LIGHT_POINT, (1.0, 0.9, 0.8), 80.0, position=(2.0, 4.0, 1.0), radius=0.3),
+              Light(_abi.LIGHT_SPOT, (0.8, 0.9, 1.0), 120.0, position=(-2.0, 4.5, 2.0), radius=0.25,
                     axis_x=(1, 0, 0), axis_y=(0, 0, 1), axis_z=(0, 1, 0), spot_angle=math.radians(70),
                     spot_smooth=0.3),
               Light(_abi.LIGHT_DISTANT, (1.0, 1.0, 0.9), 1.5, axis_z=(0.3, -0.9, 0.2), angle=math.radians(3.0)),
@@ -419,6 +424,46 @@ def small_test_scene(seed: int = 0, transparent: bool = True, lights: bool = Tru
                     flags=_abi.LIGHT_FLAG_NORMALIZE | _abi.LIGHT_FLAG_ELLIPSE)]
     cam = Camera(look_at((0.0, 3.0, 9.0), (0.0, 1.0, 0.0)), math.radians(40.0), math.radians(40.0), 0)
     return Scene(meshes, instances, mats, ls, cam, background=(0.1, 0.12, 0.15))
+
+
+def lamp_scene(seed: int = 0) -> Scene:
+    """Lamps in view: rectangle and ellipse area lamps (two stacked along the
+    view axis, one facing away), finite-radius point and spot disks, a delta
+    point and a sun, over a floor with boxes and a transparent pane; camera
+    and BSDF rays hit the lamps directly."""
+    rng = np.random.default_rng(seed)
+    pane = ShaderGraph()
+    pane.set_output(pane.transparent_bsdf((0.8, 0.9, 0.8)))
+    graphs = [diffuse_material((0.7, 0.7, 0.7)), pane]
+    for _ in range(3):
+        graphs.append(random_material(rng, emission_probability=0.0, transparent_probability=0.2))
+    mats = _materials(graphs)
+    meshes = [quad((-6, 0, -6), (-6, 0, 6), (6, 0, 6), (6, 0, -6)), box_mesh(1.0),
+              quad((-1, 0, 0), (1, 0, 0), (1, 2, 0), (-1, 2, 0))]
+    instances = [Instance(0, 0), Instance(2, 1, translate(0.5, 0.0, 1.5))]
+    for k in range(4):
+        xf = translate(*rng.uniform((-3, 0.5, -3), (3, 1.5, 1))) @ rotate_y(float(rng.uniform(0, 6.28)))
+        instances.append(Instance(1, 2 + (k % 3), xf))
+    ls = [
+        Light(_abi.LIGHT_AREA, (1.0, 0.9, 0.8), 30.0, position=(-1.5, 2.0, -2.0), size_u=1.2, size_v=0.8,
+              axis_x=(1, 0, 0), axis_y=(0, 1, 0), axis_z=(0, 0, -1)),
+        Light(_abi.LIGHT_AREA, (0.8, 0.9, 1.0), 25.0, position=(-1.3, 2.1, -3.0), size_u=1.0, size_v=1.0,
+              axis_x=(1, 0, 0), axis_y=(0, 1, 0), axis_z=(0, 0, -1),
+              flags=_abi.LIGHT_FLAG_NORMALIZE | _abi.LIGHT_FLAG_ELLIPSE),
+        Light(_abi.LIGHT_AREA, (0.9, 1.0, 0.9), 40.0, position=(1.8, 1.5, -1.0), size_u=0.9, size_v=0.6,
+              axis_x=(1, 0, 0), axis_y=(0, 1, 0), axis_z=(0, 0, 1)),
+        Light(_abi.LIGHT_AREA, (1.0, 1.0, 1.0), 20.0, position=(0.0, 3.5, 0.0), size_u=2.0, size_v=2.0,
+              axis_x=(1, 0, 0), axis_y=(0, 0, 1), axis_z=(0, 1, 0), flags=0),
+        Light(_abi.LIGHT_POINT, (1.0, 0.8, 0.6), 60.0, position=(2.5, 2.5, -2.0), radius=0.35),
+        Light(_abi.LIGHT_SPOT, (0.6, 0.8, 1.0), 90.0, position=(-2.5, 3.0, 0.5), radius=0.3,
+              axis_x=(1, 0, 0), axis_y=(0, 0, 1), axis_z=(0.3, 1, 0.2), spot_angle=math.radians(80), spot_smooth=0.4),
+        Light(_abi.LIGHT_POINT, (0.9, 0.9, 1.0), 15.0, position=(0.5, 1.0, -0.5)),
+        Light(_abi.LIGHT_DISTANT, (1.0, 1.0, 0.9), 0.8, axis_z=(0.2, -0.9, -0.3), angle=math.radians(4.0)),
+        Light(_abi.LIGHT_AREA, (1.0, 0.5, 0.5), 10.0, position=(0.0, 1.2, -4.0), size_u=1.0, size_v=1.0,
+              axis_x=(1, 0, 0), axis_y=(0, 1, 0), axis_z=(0, 0, -1), use_mis=False),
+    ]
+    cam = Camera(look_at((0.0, 2.0, 7.0), (0.0, 1.5, -1.0)), math.radians(45.0), math.radians(45.0), 0)
+    return Scene(meshes, instances, mats, ls, cam, background=(0.05, 0.05, 0.08))
 
 
 def render_settings(width: int, height: int, max_bounces: int = 4, seed: int = 0, **overrides) -> _abi.RenderSettings:
