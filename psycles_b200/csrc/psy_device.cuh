@@ -980,7 +980,7 @@ __device__ __forceinline__ float spot_attenuation(const psy_light_desc &l, f3 fr
 
 // include/psycles/luisa/analytic_light_sampling.h:84-108 (distant),
 // :549-603 (disk), :856-896 (pdf / eval factor), :309-345 (spot profile).
-__device__ __forceinline__ AnalyticSample sample_analytic(const psy_light_desc &l, f3 reference, f2 rnd) {
+__device__ __noinline__ AnalyticSample sample_analytic(const psy_light_desc &l, f3 reference, f2 rnd) {
     AnalyticSample out;
     const bool normalize_power = (l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u;
     if (l.type == PSY_LIGHT_DISTANT) {
@@ -1165,13 +1165,22 @@ __device__ __forceinline__ bool intersect_disk_lamp(const psy_light_desc &l, f3 
 // lower index.  Eligibility: the lamp's visibility covers the ray, the ray
 // is a camera ray or the lamp takes part in MIS, and it is not the lamp the
 // previous event hit.
-__device__ __forceinline__ LampHit closest_lamp(const SceneView &s, f3 o, f3 d, float tmin, float event_distance,
+__device__ __noinline__ LampHit closest_lamp(const SceneView &s, f3 o, f3 d, float tmin, float event_distance,
                                                 uint32_t ray_visibility, uint32_t excluded) {
     LampHit best{false, kInvalid, event_distance, 0.0f, 0.0f};
     const bool camera_path = (ray_visibility & PSY_VISIBILITY_CAMERA) != 0u;
-    for (uint32_t li = 0; li < s.light_count; ++li) {
+    for (uint32_t k = 0; k < s.lamp_count; ++k) {
+        // Bounding-sphere rejection with a margin well above the float
+        // error of the test, so no lamp the exact test accepts is skipped.
+        const float4 bound = s.lamp_bounds[k];
+        const f3 oc = mk3(bound.x, bound.y, bound.z) - o;
+        const float tca = dot(oc, d);
+        const float oc2 = dot(oc, oc);
+        const float miss2 = oc2 - tca * tca;
+        if (miss2 > bound.w * 1.0625f + oc2 * 1.0e-5f) continue;
+        if (tca < 0.0f && oc2 > bound.w * 1.0625f + 1.0e-6f) continue;
+        const uint32_t li = s.lamp_ids[k];
         const psy_light_desc &l = s.lights[li];
-        if (l.type == PSY_LIGHT_DISTANT) continue;
         const bool use_mis = (l.flags & kLightFlagUseMis) != 0u;
         if (!((l.visibility & ray_visibility) != 0u && (camera_path || use_mis) && li != excluded)) continue;
         float distance = 0.0f, pdf = 0.0f, eval = 0.0f;

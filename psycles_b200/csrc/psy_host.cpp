@@ -422,7 +422,8 @@ struct psy_scene {
     std::vector<psy::MaterialGpu> materials;
     std::vector<float> scalars, vectors;
     DeviceBuffer tlas, blas, tris, instances, meshes, positions, normals, indices, tri_materials, material_buf, code,
-        scalar_buf, vector_buf, emitters, distribution, lights, lt_nodes, lt_emitters, lt_mapping, lt_lookup;
+        scalar_buf, vector_buf, emitters, distribution, lights, lamp_bounds, lamp_ids, lt_nodes, lt_emitters, lt_mapping,
+        lt_lookup;
     psy::SceneView view{};
     uint64_t triangle_count = 0;
     double build_ms = 0.0;
@@ -1036,6 +1037,31 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->emitters.upload(emitters, st));
     PSY_CUDA_TRY(sc->distribution.upload(dist, st));
     PSY_CUDA_TRY(sc->lights.upload(lights, st));
+    // lamps a ray can hit, in light order, with a bounding sphere each
+    std::vector<float4> lamp_bounds;
+    std::vector<uint32_t> lamp_ids;
+    for (uint32_t i = 0; i < light_n; ++i) {
+        const psy_light_desc &l = lights[i];
+        double r2 = -1.0;
+        if (l.type == PSY_LIGHT_AREA && l.size_u * l.size_v != 0.0f) {
+            double hu2 = 0.0, hv2 = 0.0, huv = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                const double hu = 0.5 * double(l.size_u) * double(l.axis_x[k]);
+                const double hv = 0.5 * double(l.size_v) * double(l.axis_y[k]);
+                hu2 += hu * hu;
+                hv2 += hv * hv;
+                huv += hu * hv;
+            }
+            r2 = hu2 + hv2 + 2.0 * std::fabs(huv);
+        } else if ((l.type == PSY_LIGHT_POINT || l.type == PSY_LIGHT_SPOT) && l.radius > 0.0f) {
+            r2 = double(l.radius) * double(l.radius);
+        }
+        if (r2 < 0.0) continue;
+        lamp_bounds.push_back(make_float4(l.position[0], l.position[1], l.position[2], float(r2 * (1.0 + 1.0e-6))));
+        lamp_ids.push_back(i);
+    }
+    PSY_CUDA_TRY(sc->lamp_bounds.upload(lamp_bounds, st));
+    PSY_CUDA_TRY(sc->lamp_ids.upload(lamp_ids, st));
     PSY_CUDA_TRY(sc->lt_nodes.upload(lt_nodes, st));
     PSY_CUDA_TRY(sc->lt_emitters.upload(lt_emitters, st));
     PSY_CUDA_TRY(sc->lt_mapping.upload(lt_mapping, st));
@@ -1058,6 +1084,9 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     v.emitters = sc->emitters.as<psy::EmitterGpu>();
     v.distribution = sc->distribution.as<psy::DistEntryGpu>();
     v.lights = sc->lights.as<psy_light_desc>();
+    v.lamp_bounds = sc->lamp_bounds.as<float4>();
+    v.lamp_ids = sc->lamp_ids.as<uint32_t>();
+    v.lamp_count = uint32_t(lamp_ids.size());
     v.instance_count = tl.prims.empty() ? 0u : d->instance_count;
     v.emitter_count = tri_n + light_n;
     v.triangle_emitters = tri_n;

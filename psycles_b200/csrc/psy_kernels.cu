@@ -119,6 +119,9 @@ __device__ __forceinline__ uint32_t contract_visibility(uint32_t v) {
 #ifndef PSY_INTERSECT_MIN_BLOCKS
 #define PSY_INTERSECT_MIN_BLOCKS 6
 #endif
+#ifndef PSY_SHADE_MIN_BLOCKS
+#define PSY_SHADE_MIN_BLOCKS 3
+#endif
 #ifndef PSY_SHADOW_MIN_BLOCKS
 #define PSY_SHADOW_MIN_BLOCKS 5
 #endif
@@ -144,7 +147,7 @@ __device__ __forceinline__ uint32_t warp_fetch(uint32_t *fetch_counter, uint32_t
     return q < count ? q : kInvalid;
 }
 
-__global__ void __launch_bounds__(128, PSY_INTERSECT_MIN_BLOCKS) k_intersect(SceneView s, PathBuffers b) {
+__global__ void __launch_bounds__(128, PSY_INTERSECT_MIN_BLOCKS) k_intersect(const __grid_constant__ SceneView s, const __grid_constant__ PathBuffers b) {
     const uint32_t count = b.counters[0];
     TraversalState t;
     Hit best;
@@ -293,7 +296,11 @@ __device__ __forceinline__ float next_float_up(float t) {
     return t == 0.0f ? 1.17549435e-38f : __uint_as_float(__float_as_uint(t) + 1u);
 }
 
-__global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, PathBuffers b, uint32_t step,
+// kTrace selects the variant that records the per-path trace; the render
+// variant carries no trace code.
+template <bool kTrace>
+__global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS) k_shade(const __grid_constant__ SceneView s, const __grid_constant__ RenderParams p,
+                                                                    const __grid_constant__ PathBuffers b, uint32_t step,
                                                uint32_t trace_path, psy_path_trace *trace) {
     const uint32_t count = b.counters[0];
     const uint32_t rounds = (count + gridDim.x * blockDim.x - 1u) / (gridDim.x * blockDim.x);
@@ -310,7 +317,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
         if (active) {
             i = b.queue_in[q];
             psy_path_event *ev = nullptr;
-            if (trace && i == trace_path && step < PSY_TRACE_MAX_EVENTS) {
+            if (kTrace && trace && i == trace_path && step < PSY_TRACE_MAX_EVENTS) {
                 ev = &trace->events[step];
                 trace->event_count = step + 1u;
             }
@@ -362,7 +369,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
             }
             const uint32_t depth = ps.bounce;
             bool alive = true;
-            if (s.light_count > 0u) {
+            if (s.lamp_count > 0u) {
                 // Lamps in front of the mesh event are transparent events that
                 // add their emission without a new bounce or new dimensions
                 // (src/luisa/path_kernel_pipeline.cpp:78-126,
@@ -370,7 +377,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, RenderParams p, Path
                 const float event_distance = prim == kInvalid ? ray.tmax : h4.x;
                 uint32_t excluded = kInvalid;
                 float tmin = ray.tmin;
-                for (uint32_t guard = 0; guard <= s.light_count && alive; ++guard) {
+                for (uint32_t guard = 0; guard <= s.lamp_count && alive; ++guard) {
                     const LampHit lh = closest_lamp(s, ray.o, ray.d, tmin, event_distance, ray_visibility, excluded);
                     if (!lh.valid) break;
                     float selection_pdf = s.light_selection_pdf;
@@ -777,7 +784,8 @@ __device__ __forceinline__ f3 shadow_transmittance(const SceneView &s, const Ren
 // Opaque-only scenes stop at the first accepted candidate; otherwise
 // transparent hits are collected per lane and resolved as in
 // shadow_transmittance once the traversal ends.
-__global__ void __launch_bounds__(128, PSY_SHADOW_MIN_BLOCKS) k_shadow(SceneView s, RenderParams p, PathBuffers b, uint32_t step,
+__global__ void __launch_bounds__(128, PSY_SHADOW_MIN_BLOCKS) k_shadow(const __grid_constant__ SceneView s, const __grid_constant__ RenderParams p,
+                                                                      const __grid_constant__ PathBuffers b, uint32_t step,
                                                 uint32_t trace_path, psy_path_trace *trace) {
     const uint32_t count = b.counters[2];
     TraversalState t;
@@ -952,7 +960,7 @@ __global__ void k_debug_sobol(const float4 *table, uint32_t size, const uint32_t
     out_index[i] = idx;
 }
 
-__global__ void k_debug_light_tree(SceneView s, const float4 *queries, const uint32_t *pdf_emitters, uint32_t count,
+__global__ void k_debug_light_tree(const __grid_constant__ SceneView s, const float4 *queries, const uint32_t *pdf_emitters, uint32_t count,
                                    uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
@@ -992,7 +1000,10 @@ void launch_intersect(cudaStream_t st, int sms, const SceneView &s, const PathBu
 }
 void launch_shade(cudaStream_t st, int sms, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                   uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
-    k_shade<<<launch_grid(max_work, 128, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace);
+    if (trace)
+        k_shade<true><<<launch_grid(max_work, 128, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace);
+    else
+        k_shade<false><<<launch_grid(max_work, 128, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace);
 }
 void launch_shadow(cudaStream_t st, int sms, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                    uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {

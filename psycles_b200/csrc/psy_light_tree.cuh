@@ -63,7 +63,7 @@ __device__ __forceinline__ f2 lt_bounded_importance(f3 n, bool has_transmission,
 }
 
 // measure_importance (path_tracer_light_tree.cpp:195-277).
-__device__ __forceinline__ f2 lt_measure_importance(float4 min_energy, float4 max_theta_o, float4 axis_theta_e,
+__device__ __noinline__ f2 lt_measure_importance(float4 min_energy, float4 max_theta_o, float4 axis_theta_e,
                                                     uint32_t flags, f3 point, f3 n, bool has_transmission) {
     f2 result = {0.0f, 0.0f};
     const bool has_orientation = (flags & kLtFlagOrientation) != 0u;
@@ -202,7 +202,7 @@ __device__ __forceinline__ void lt_select_leaf(const SceneView &s, const LtNodeG
 
 // make_sample_callable, surface case (path_tracer_light_tree.cpp:547-637):
 // the selected emitter's distribution entry with the tree's selection pdf.
-__device__ __forceinline__ DistEntryGpu lt_sample(const SceneView &s, float u, f3 point, f3 n, bool tr) {
+__device__ __noinline__ DistEntryGpu lt_sample(const SceneView &s, float u, f3 point, f3 n, bool tr) {
     DistEntryGpu result{0.0f, 0.0f, 3u, 0u};
     if (s.lt_node_count == 0u || s.lt_emitter_count == 0u || s.lt_root >= s.lt_node_count) return result;
     float random = clampf_(u, 0.0f, 1.0f);
@@ -235,7 +235,7 @@ __device__ __forceinline__ DistEntryGpu lt_sample(const SceneView &s, float u, f
 }
 
 // make_pdf_callable, surface case (path_tracer_light_tree.cpp:639-760).
-__device__ __forceinline__ float lt_pdf(const SceneView &s, uint32_t emitter_id, f3 point, f3 n, bool tr) {
+__device__ __noinline__ float lt_pdf(const SceneView &s, uint32_t emitter_id, f3 point, f3 n, bool tr) {
     if (s.lt_node_count == 0u || s.lt_emitter_count == 0u || emitter_id >= s.lt_emitter_count) return 0.0f;
     const uint2 mapping = s.lt_mapping[emitter_id];
     const uint32_t target = mapping.x;

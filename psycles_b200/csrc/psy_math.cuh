@@ -92,12 +92,14 @@ __device__ __forceinline__ f3 light_safe_normalize(f3 value, f3 fallback) {
 
 // Transcendentals on the sampling path are evaluated in double precision
 // and rounded once to float, so the kernels and a CPU evaluation of the same
-// expression agree bit for bit.
-__device__ __forceinline__ float sin_(float x) { return static_cast<float>(sin(static_cast<double>(x))); }
-__device__ __forceinline__ float cos_(float x) { return static_cast<float>(cos(static_cast<double>(x))); }
-__device__ __forceinline__ float acos_(float x) { return static_cast<float>(acos(static_cast<double>(x))); }
-__device__ __forceinline__ float asin_(float x) { return static_cast<float>(asin(static_cast<double>(x))); }
-__device__ __forceinline__ float atan2_(float y, float x) {
+// expression agree bit for bit.  They are out of line: each double-precision
+// routine is long, and one copy per call site would overflow the
+// instruction cache of the shading kernel.
+__device__ __noinline__ float sin_(float x) { return static_cast<float>(sin(static_cast<double>(x))); }
+__device__ __noinline__ float cos_(float x) { return static_cast<float>(cos(static_cast<double>(x))); }
+__device__ __noinline__ float acos_(float x) { return static_cast<float>(acos(static_cast<double>(x))); }
+__device__ __noinline__ float asin_(float x) { return static_cast<float>(asin(static_cast<double>(x))); }
+__device__ __noinline__ float atan2_(float y, float x) {
     return static_cast<float>(atan2(static_cast<double>(y), static_cast<double>(x)));
 }
 

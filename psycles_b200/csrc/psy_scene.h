@@ -93,6 +93,11 @@ struct SceneView {
     uint32_t emitter_count;   // distribution entries - 1 (triangles + lights)
     uint32_t triangle_emitters;
     uint32_t light_count;
+    // lamps a ray can hit (area lamps, finite point / spot disks) in light
+    // order: bounding sphere (centre, radius^2) and light index
+    const float4 *lamp_bounds;
+    const uint32_t *lamp_ids;
+    uint32_t lamp_count;
     float triangle_area_pdf;
     float light_selection_pdf;
     float background[3];
