@@ -46,6 +46,7 @@ typedef enum psy_status {
 typedef struct psy_context psy_context;
 typedef struct psy_scene psy_scene;
 typedef struct psy_session psy_session;
+typedef struct psy_batch psy_batch;
 
 /* ---------------------------------------------------------------- scene -- */
 
@@ -284,6 +285,11 @@ psy_status psy_session_create(psy_scene *scene,
                               const psy_render_settings *settings,
                               psy_session **out);
 void psy_session_destroy(psy_session *session);
+/* Renders the session's scene through `camera` (NULL: the scene's own
+ * camera) and clears the film.  No counterpart in the reference, where a
+ * camera move is a new SceneSnapshot revision recompiled by compile_scene;
+ * here a viewport moves without touching the resident scene. */
+psy_status psy_session_set_camera(psy_session *session, const psy_camera_desc *camera);
 /* RenderSession::reset (render.h:167): clears the film. */
 psy_status psy_session_reset(psy_session *session,
                              const psy_render_settings *settings);
@@ -441,6 +447,52 @@ psy_status psy_sobol_generate_table(uint32_t sequence_size, float *out);
 /* sampling::make_pixel_filter_table (src/sampling/pixel_filter.cpp:30):
  * writes 1024 floats. */
 psy_status psy_pixel_filter_table(uint32_t filter, float width, float *out);
+
+/* ------------------------------------------------- batched wavefronts -- */
+/* A batch renders sample ranges of many sessions in shared wavefronts:
+ * camera paths of every session fill one path state of `path_capacity`
+ * paths, and each kernel reads the scene and parameters of its path's
+ * session.  No counterpart in the reference, whose sessions dispatch
+ * separately (LuisaRenderSession::render_samples,
+ * src/luisa/path_tracer_session.cpp:272-397); each session's result is the
+ * one render_samples gives, bit for bit, because every pixel adds its
+ * samples to the film one at a time in sample order. */
+typedef struct psy_batch_config {
+    uint32_t path_capacity;      /* paths per wavefront; 0 = 4 Mi; grown to the largest window */
+    uint32_t max_jobs;           /* sessions per psy_batch_render call; 0 = 256 */
+    uint32_t use_graph;          /* 1: each wavefront replays one captured CUDA graph */
+    uint32_t check_interval;     /* without graphs: host check of live paths every N steps (0 = 4) */
+} psy_batch_config;
+
+typedef struct psy_batch_stats {
+    uint64_t samples;            /* pixel samples rendered by the last call */
+    uint64_t closest_rays;
+    uint64_t shadow_rays;
+    float ms_total;              /* device time of the last call */
+    uint32_t wavefronts;
+    uint32_t jobs;
+    uint32_t graph_launches;
+    uint32_t kernel_launches;    /* launched directly or as graph nodes */
+} psy_batch_stats;
+
+psy_status psy_batch_create(psy_context *context, const psy_batch_config *config, psy_batch **out);
+void psy_batch_destroy(psy_batch *batch);
+/* Renders, for each i < n, sessions[i]'s sample range (first[i], count[i],
+ * offset[i], total[i]) with the validation and film result of
+ * psy_session_render_samples.  Sessions must belong to the batch's context;
+ * a session listed twice is rejected.  Per-path traces are not recorded.  A
+ * session cancelled during the call stops at the next wavefront and the
+ * call returns PSY_ERROR_CANCELLED after finishing the others. */
+psy_status psy_batch_render(psy_batch *batch, psy_session *const *sessions, const uint32_t *first,
+                            const uint32_t *count, const uint32_t *offset, const uint32_t *total, uint32_t n);
+psy_status psy_batch_get_stats(const psy_batch *batch, psy_batch_stats *out);
+/* The wavefront plan of a batch, without a GPU: for n jobs of pixels[i]
+ * window pixels and samples[i] samples, the items of each wavefront of at
+ * most `capacity` paths.  Writes up to max_items records of 6 words (job,
+ * wavefront, path_begin, first sample offset, samples, film_begin) and the
+ * item count; PSY_ERROR_RANGE when max_items is too small. */
+psy_status psy_batch_plan(const uint32_t *pixels, const uint32_t *samples, uint32_t n, uint32_t capacity,
+                          uint32_t *out_items, uint32_t max_items, uint32_t *out_count);
 
 /* ------------------------------------------------ device probes (GPU) -- */
 

@@ -131,6 +131,17 @@ class KernelProfile(ctypes.Structure):
         ("reserved_bytes", ctypes.c_double)]
 
 
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("path_capacity", ctypes.c_uint32), ("max_jobs", ctypes.c_uint32), ("use_graph", ctypes.c_uint32),
+                ("check_interval", ctypes.c_uint32)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_uint64), ("closest_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
+                ("ms_total", ctypes.c_float), ("wavefronts", ctypes.c_uint32), ("jobs", ctypes.c_uint32),
+                ("graph_launches", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32)]
+
+
 # Entry points declared by include/psycles_cuda.h: (name, restype, argtypes).
 SIGNATURES = [
     ("psy_last_error", ctypes.c_char_p, []),
@@ -165,6 +176,14 @@ SIGNATURES = [
     ("psy_pixel_filter_table", ctypes.c_int, [ctypes.c_uint32, ctypes.c_float, c_float_p]),
     ("psy_debug_sobol_samples", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_uint32, c_uint32_p, ctypes.c_uint32, c_float_p, c_uint32_p]),
+    ("psy_session_set_camera", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("psy_batch_create", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    ("psy_batch_destroy", None, [ctypes.c_void_p]),
+    ("psy_batch_render", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), c_uint32_p, c_uint32_p,
+                                        c_uint32_p, c_uint32_p, ctypes.c_uint32]),
+    ("psy_batch_get_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchStats)]),
+    ("psy_batch_plan", ctypes.c_int, [c_uint32_p, c_uint32_p, ctypes.c_uint32, ctypes.c_uint32, c_uint32_p,
+                                      ctypes.c_uint32, c_uint32_p]),
     ("psy_debug_light_tree", ctypes.c_int,
      [ctypes.c_void_p, c_float_p, c_uint32_p, ctypes.c_uint32, c_uint32_p, c_float_p, c_float_p]),
 ]

@@ -170,6 +170,13 @@ class RenderSession:
     def cancel(self) -> None:
         self.lib.psy_session_cancel(self.handle)
 
+    def set_camera(self, camera) -> None:
+        """Renders through `camera` (a scenes.Camera; None restores the
+        scene's) and clears the film."""
+        from .scenes import camera_desc
+        desc = camera_desc(camera) if camera is not None else None
+        _abi.check(self.lib.psy_session_set_camera(self.handle, ctypes.byref(desc) if desc is not None else None))
+
     def render_samples(self, samples: SampleRange, output: OutputSink | None = None) -> bool:
         with self._lock:
             status = self.lib.psy_session_render_samples(self.handle, samples.first, samples.count,
@@ -251,3 +258,61 @@ class CudaPathTracerBackend:
         if status != _abi.PSY_OK:
             return None
         return RenderSession(compiled, h, settings, list(passes or DEFAULT_PASSES))
+
+
+class BatchRenderer:
+    """Sample ranges of many sessions rendered in shared wavefronts
+    (psy_batch_*).  Each session ends exactly as its own render_samples call
+    would leave it; the batch only shares the path state and the launches."""
+
+    def __init__(self, context: Context, path_capacity: int = 0, max_jobs: int = 0, use_graph: bool = True,
+                 check_interval: int = 0):
+        self.context = context
+        self.lib = context.lib
+        cfg = _abi.BatchConfig(path_capacity, max_jobs, 1 if use_graph else 0, check_interval)
+        h = ctypes.c_void_p()
+        _abi.check(self.lib.psy_batch_create(context.handle, ctypes.byref(cfg), ctypes.byref(h)))
+        self.handle = h
+
+    def render(self, work: list[tuple[RenderSession, SampleRange]]) -> bool:
+        n = len(work)
+        sessions = (ctypes.c_void_p * n)(*[s.handle for s, _ in work])
+        cols = [np.array([getattr(r, f) for _, r in work], np.uint32) for f in ("first", "count", "offset", "total")]
+        status = self.lib.psy_batch_render(self.handle, sessions, *[_abi.ptr(c, ctypes.c_uint32) for c in cols], n)
+        if status != _abi.PSY_OK:
+            message = self.lib.psy_last_error().decode()
+            for s, _ in work:
+                s.diagnostics.append(RenderDiagnostic(message))
+            return False
+        return True
+
+    def stats(self) -> _abi.BatchStats:
+        s = _abi.BatchStats()
+        _abi.check(self.lib.psy_batch_get_stats(self.handle, ctypes.byref(s)))
+        return s
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.psy_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_plan(pixels: list[int], samples: list[int], capacity: int) -> np.ndarray:
+    """psy_batch_plan: rows (job, wavefront, path_begin, first sample offset,
+    samples, film_begin) of the batch wavefront plan; needs no GPU."""
+    lib = _abi.load()
+    px = np.ascontiguousarray(pixels, np.uint32)
+    sp = np.ascontiguousarray(samples, np.uint32)
+    count = ctypes.c_uint32()
+    lib.psy_batch_plan(_abi.ptr(px, ctypes.c_uint32), _abi.ptr(sp, ctypes.c_uint32), len(px), capacity, None, 0,
+                       ctypes.byref(count))
+    out = np.zeros((max(count.value, 1), 6), np.uint32)
+    _abi.check(lib.psy_batch_plan(_abi.ptr(px, ctypes.c_uint32), _abi.ptr(sp, ctypes.c_uint32), len(px), capacity,
+                                  _abi.ptr(out, ctypes.c_uint32), count.value, ctypes.byref(count)))
+    return out[:count.value]

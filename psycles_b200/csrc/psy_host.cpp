@@ -11,6 +11,7 @@
 //     pass readback
 // Compiled without FP contraction so the host tables are bit-identical to
 // the reference's construction.
+#include "psy_host_internal.h"
 #include "psy_kernels.h"
 #include "psy_light_tree.h"
 #include "psy_scene.h"
@@ -29,7 +30,7 @@
 #include <string>
 #include <vector>
 
-namespace {
+namespace psy::host {
 
 thread_local std::string g_last_error;
 
@@ -38,13 +39,69 @@ psy_status fail(psy_status status, const std::string &message) {
     return status;
 }
 
-#define PSY_CUDA_TRY(expr)                                                                        \
-    do {                                                                                          \
-        const cudaError_t err_ = (expr);                                                          \
-        if (err_ != cudaSuccess) {                                                                \
-            return fail(PSY_ERROR_CUDA, std::string(#expr ": ") + cudaGetErrorString(err_));      \
-        }                                                                                         \
-    } while (0)
+psy_status PathArena::ensure(uint32_t n, bool with_job) {
+    if (capacity >= n && (!with_job || job.ptr)) return PSY_OK;
+    const uint32_t c = std::max(n, capacity);
+    const size_t f4 = sizeof(float4) * size_t(c), u4 = sizeof(uint4) * size_t(c), u1 = sizeof(uint32_t) * size_t(c);
+    PSY_CUDA_TRY(ray_o.alloc(f4));
+    PSY_CUDA_TRY(ray_d.alloc(f4));
+    PSY_CUDA_TRY(tp.alloc(f4));
+    PSY_CUDA_TRY(rad.alloc(f4));
+    PSY_CUDA_TRY(st.alloc(u4));
+    PSY_CUDA_TRY(st2.alloc(u4));
+    PSY_CUDA_TRY(sample.alloc(u1));
+    PSY_CUDA_TRY(aov_n.alloc(f4));
+    PSY_CUDA_TRY(aov_a.alloc(f4));
+    PSY_CUDA_TRY(mis_n.alloc(f4));
+    PSY_CUDA_TRY(hit.alloc(f4));
+    PSY_CUDA_TRY(hit_prim.alloc(u1));
+    PSY_CUDA_TRY(sh_o.alloc(f4));
+    PSY_CUDA_TRY(sh_d.alloc(f4));
+    PSY_CUDA_TRY(sh_c.alloc(f4));
+    PSY_CUDA_TRY(sh_ids.alloc(u4));
+    PSY_CUDA_TRY(sh_path.alloc(u1));
+    PSY_CUDA_TRY(qa.alloc(u1));
+    PSY_CUDA_TRY(qb.alloc(u1));
+    PSY_CUDA_TRY(sq.alloc(u1));
+    if (with_job) PSY_CUDA_TRY(job.alloc(u1));
+    if (!counters.ptr) PSY_CUDA_TRY(counters.alloc(64));
+    if (!stats.ptr) PSY_CUDA_TRY(stats.alloc(64));
+    capacity = c;
+    PathBuffers &b = view;
+    b.ray_o = ray_o.as<float4>();
+    b.ray_d = ray_d.as<float4>();
+    b.tp = tp.as<float4>();
+    b.rad = rad.as<float4>();
+    b.st = st.as<uint4>();
+    b.st2 = st2.as<uint4>();
+    b.sample = sample.as<uint32_t>();
+    b.aov_n = aov_n.as<float4>();
+    b.aov_a = aov_a.as<float4>();
+    b.mis_n = mis_n.as<float4>();
+    b.hit = hit.as<float4>();
+    b.hit_prim = hit_prim.as<uint32_t>();
+    b.sh_o = sh_o.as<float4>();
+    b.sh_d = sh_d.as<float4>();
+    b.sh_c = sh_c.as<float4>();
+    b.sh_ids = sh_ids.as<uint4>();
+    b.sh_path = sh_path.as<uint32_t>();
+    b.queue_in = qa.as<uint32_t>();
+    b.queue_out = qb.as<uint32_t>();
+    b.shadow_queue = sq.as<uint32_t>();
+    b.counters = counters.as<uint32_t>();
+    b.job = job.ptr ? job.as<uint32_t>() : nullptr;
+    return PSY_OK;
+}
+
+size_t PathArena::bytes_per_path(bool with_job) {
+    return 10u * sizeof(float4) + 4u * sizeof(uint4) + (7u + (with_job ? 1u : 0u)) * sizeof(uint32_t);
+}
+
+}  // namespace psy::host
+
+using namespace psy::host;
+
+namespace {
 
 // ------------------------------------------------------------ Sobol LUT
 // Cycles' progressive multi-jittered 4-D table (tabulated_sobol.cpp:75-200).
@@ -373,88 +430,9 @@ struct Builder {
     }
 };
 
-// ------------------------------------------------------------ device memory
-
-struct DeviceBuffer {
-    void *ptr = nullptr;
-    size_t bytes = 0;
-    DeviceBuffer() = default;
-    DeviceBuffer(const DeviceBuffer &) = delete;
-    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
-    ~DeviceBuffer() { release(); }
-    void release() {
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
-    }
-    cudaError_t alloc(size_t n) {
-        release();
-        bytes = n;
-        if (n == 0) return cudaSuccess;
-        return cudaMalloc(&ptr, n);
-    }
-    template <typename T>
-    cudaError_t upload(const std::vector<T> &v, cudaStream_t st) {
-        cudaError_t e = alloc(std::max<size_t>(v.size() * sizeof(T), 16));
-        if (e != cudaSuccess || v.empty()) return e;
-        return cudaMemcpyAsync(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
-    }
-    template <typename T>
-    T *as() const {
-        return static_cast<T *>(ptr);
-    }
-};
 
 }  // namespace
 
-// ----------------------------------------------------------------- objects
-
-struct psy_context {
-    int device = 0;
-    int sms = 148;
-    cudaStream_t stream = nullptr;
-};
-
-struct psy_scene {
-    psy_context *context = nullptr;
-    uint64_t revision = 0;
-    psy_camera_desc camera{};
-    std::vector<psy::MaterialGpu> materials;
-    std::vector<float> scalars, vectors;
-    DeviceBuffer tlas, blas, tris, instances, meshes, positions, normals, indices, tri_materials, material_buf, code,
-        scalar_buf, vector_buf, emitters, distribution, lights, lamp_bounds, lamp_ids, lt_nodes, lt_emitters, lt_mapping,
-        lt_lookup;
-    psy::SceneView view{};
-    uint64_t triangle_count = 0;
-    double build_ms = 0.0;
-};
-
-struct psy_session {
-    psy_scene *scene = nullptr;
-    psy_render_settings settings{};
-    psy::RenderParams params{};
-    uint32_t pixels = 0;
-    uint32_t total = 0;
-    uint32_t sobol_size = 0;
-    uint32_t rendered = 0;
-    std::atomic<bool> cancelled{false};
-    DeviceBuffer sobol, filter, combined, normal, albedo, sample_count;
-    // path state
-    uint32_t capacity = 0;
-    DeviceBuffer ray_o, ray_d, tp, rad, st, st2, sample, aov_n, aov_a, mis_n, hit, hit_prim, sh_o, sh_d, sh_c, sh_ids,
-        sh_path, qa, qb, sq, counters, stats;
-    psy::PathBuffers paths{};
-    // trace
-    DeviceBuffer trace_buf;
-    bool trace_requested = false;
-    uint32_t trace_x = 0, trace_y = 0, trace_sample = 0;
-    psy_path_trace trace_host{};
-    psy_render_stats last_stats{};
-    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
-    bool profiling = false;
-    psy_kernel_profile profile{};
-    cudaEvent_t ev_k[2] = {nullptr, nullptr};
-};
 
 namespace {
 
@@ -504,7 +482,7 @@ psy_status derive_params(psy_session *s, const psy_render_settings &r) {
     p.nee = nee ? 1u : 0u;
     p.direct_mode = nee ? r.direct_light_sampling : PSY_DIRECT_LIGHT_FORWARD;
     // camera parameters (src/luisa/path_tracer_kernel.cpp:225-280)
-    const psy_camera_desc &c = s->scene->camera;
+    const psy_camera_desc &c = s->has_camera ? s->camera : s->scene->camera;
     const float aspect = static_cast<float>(std::max(r.full_width, 1u)) / static_cast<float>(std::max(r.full_height, 1u));
     const bool hfit = c.sensor_fit == 1u || (c.sensor_fit == 0u && aspect >= 1.0f);
     p.vtan = hfit ? std::tan(c.horizontal_field_of_view * 0.5f) / aspect : std::tan(c.field_of_view * 0.5f);
@@ -519,54 +497,7 @@ psy_status derive_params(psy_session *s, const psy_render_settings &r) {
 }
 
 psy_status ensure_capacity(psy_session *s, uint32_t n) {
-    if (s->capacity >= n) return PSY_OK;
-    const size_t f4 = sizeof(float4) * size_t(n), u4 = sizeof(uint4) * size_t(n), u1 = sizeof(uint32_t) * size_t(n);
-    PSY_CUDA_TRY(s->ray_o.alloc(f4));
-    PSY_CUDA_TRY(s->ray_d.alloc(f4));
-    PSY_CUDA_TRY(s->tp.alloc(f4));
-    PSY_CUDA_TRY(s->rad.alloc(f4));
-    PSY_CUDA_TRY(s->st.alloc(u4));
-    PSY_CUDA_TRY(s->st2.alloc(u4));
-    PSY_CUDA_TRY(s->sample.alloc(u1));
-    PSY_CUDA_TRY(s->aov_n.alloc(f4));
-    PSY_CUDA_TRY(s->aov_a.alloc(f4));
-    PSY_CUDA_TRY(s->mis_n.alloc(f4));
-    PSY_CUDA_TRY(s->hit.alloc(f4));
-    PSY_CUDA_TRY(s->hit_prim.alloc(u1));
-    PSY_CUDA_TRY(s->sh_o.alloc(f4));
-    PSY_CUDA_TRY(s->sh_d.alloc(f4));
-    PSY_CUDA_TRY(s->sh_c.alloc(f4));
-    PSY_CUDA_TRY(s->sh_ids.alloc(u4));
-    PSY_CUDA_TRY(s->sh_path.alloc(u1));
-    PSY_CUDA_TRY(s->qa.alloc(u1));
-    PSY_CUDA_TRY(s->qb.alloc(u1));
-    PSY_CUDA_TRY(s->sq.alloc(u1));
-    if (!s->counters.ptr) PSY_CUDA_TRY(s->counters.alloc(64));
-    if (!s->stats.ptr) PSY_CUDA_TRY(s->stats.alloc(64));
-    s->capacity = n;
-    psy::PathBuffers &b = s->paths;
-    b.ray_o = s->ray_o.as<float4>();
-    b.ray_d = s->ray_d.as<float4>();
-    b.tp = s->tp.as<float4>();
-    b.rad = s->rad.as<float4>();
-    b.st = s->st.as<uint4>();
-    b.st2 = s->st2.as<uint4>();
-    b.sample = s->sample.as<uint32_t>();
-    b.aov_n = s->aov_n.as<float4>();
-    b.aov_a = s->aov_a.as<float4>();
-    b.mis_n = s->mis_n.as<float4>();
-    b.hit = s->hit.as<float4>();
-    b.hit_prim = s->hit_prim.as<uint32_t>();
-    b.sh_o = s->sh_o.as<float4>();
-    b.sh_d = s->sh_d.as<float4>();
-    b.sh_c = s->sh_c.as<float4>();
-    b.sh_ids = s->sh_ids.as<uint4>();
-    b.sh_path = s->sh_path.as<uint32_t>();
-    b.queue_in = s->qa.as<uint32_t>();
-    b.queue_out = s->qb.as<uint32_t>();
-    b.shadow_queue = s->sq.as<uint32_t>();
-    b.counters = s->counters.as<uint32_t>();
-    return PSY_OK;
+    return s->arena.ensure(n, false);
 }
 
 psy_status clear_film(psy_session *s) {
@@ -1194,6 +1125,17 @@ psy_status psy_session_reset(psy_session *s, const psy_render_settings *settings
     return clear_film(s);
 }
 
+psy_status psy_session_set_camera(psy_session *s, const psy_camera_desc *camera) {
+    if (!s) return fail(PSY_ERROR_INVALID_ARGUMENT, "null session");
+    PSY_CUDA_TRY(cudaSetDevice(s->scene->context->device));
+    s->has_camera = camera != nullptr;
+    if (camera) s->camera = *camera;
+    psy_status r = derive_params(s, s->settings);
+    if (r != PSY_OK) return r;
+    s->params.filter = s->filter.as<float>();
+    return clear_film(s);
+}
+
 void psy_session_cancel(psy_session *s) {
     if (s) s->cancelled.store(true);
 }
@@ -1218,7 +1160,10 @@ psy_status psy_session_read_trace(psy_session *s, psy_path_trace *out) {
     return PSY_OK;
 }
 
-psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t count, uint32_t offset, uint32_t total) {
+}  // extern "C"
+
+psy_status psy::host::prepare_render(psy_session *s, uint32_t first, uint32_t count, uint32_t offset, uint32_t total,
+                                      psy::RenderParams *out) {
     if (!s) return fail(PSY_ERROR_INVALID_ARGUMENT, "null session");
     if (s->cancelled.load()) return fail(PSY_ERROR_CANCELLED, "session cancelled");
     if (count == 0u) return fail(PSY_ERROR_RANGE, "empty sample range");
@@ -1226,26 +1171,37 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
     if (total == 0u || end > total) return fail(PSY_ERROR_RANGE, "sample range beyond the render's total");
     if (s->total != 0u && s->total != total) return fail(PSY_ERROR_STATE, "total sample count changed within the session");
     psy_context *ctx = s->scene->context;
-    cudaStream_t st = ctx->stream;
     PSY_CUDA_TRY(cudaSetDevice(ctx->device));
     // Sobol table sized from the render's total (path_tracer_session.cpp:41-69)
     const uint32_t size = psy_sobol_sequence_size_for_samples(total);
     if (s->sobol_size != size) {
         std::vector<float> table(size_t(size) * 256u * 4u);
         psy_sobol_generate_table(size, table.data());
-        PSY_CUDA_TRY(s->sobol.upload(table, st));
+        PSY_CUDA_TRY(s->sobol.upload(table, ctx->stream));
         s->sobol_size = size;
     }
     s->total = total;
-    psy::RenderParams p = s->params;
-    p.sobol = s->sobol.as<float4>();
-    p.sobol_size = s->sobol_size;
+    *out = s->params;
+    out->sobol = s->sobol.as<float4>();
+    out->sobol_size = s->sobol_size;
+    return PSY_OK;
+}
+
+extern "C" {
+
+psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t count, uint32_t offset, uint32_t total) {
+    psy::RenderParams p;
+    const psy_status prepared = prepare_render(s, first, count, offset, total, &p);
+    if (prepared != PSY_OK) return prepared;
+    const uint64_t begin = uint64_t(first) + offset, end = begin + count;
+    psy_context *ctx = s->scene->context;
+    cudaStream_t st = ctx->stream;
     const uint32_t pixels = s->pixels;
     uint32_t per_batch = std::max(1u, std::min(count, kDefaultCapacity / std::max(pixels, 1u)));
     psy_status r = ensure_capacity(s, pixels * per_batch);
     if (r != PSY_OK) return r;
     psy_path_trace *trace = s->trace_requested ? s->trace_buf.as<psy_path_trace>() : nullptr;
-    PSY_CUDA_TRY(cudaMemsetAsync(s->stats.ptr, 0, 64, st));
+    PSY_CUDA_TRY(cudaMemsetAsync(s->arena.stats.ptr, 0, 64, st));
     psy_render_stats stats{};
     PSY_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
     const int sms = ctx->sms;
@@ -1269,7 +1225,7 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
         return PSY_OK;
     };
     auto read_counters = [&](uint32_t *c3) -> psy_status {
-        PSY_CUDA_TRY(cudaMemcpyAsync(c3, s->paths.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        PSY_CUDA_TRY(cudaMemcpyAsync(c3, s->arena.view.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         PSY_CUDA_TRY(cudaStreamSynchronize(st));
         return PSY_OK;
     };
@@ -1287,7 +1243,7 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
             trace_path = uint32_t(s->trace_sample - sample) * pixels + local;
         }
         psy_path_trace *tr = trace_path != psy::kInvalidId ? trace : nullptr;
-        psy::PathBuffers b = s->paths;
+        psy::PathBuffers b = s->arena.view;
         psy::launch_set_counters(st, b.counters, paths);
         if ((ps = timed([&] { psy::launch_raygen(st, sms, p, b, pixels, paths, uint32_t(sample), trace_path, tr); },
                         pf.raygen_launches, pf.raygen_ms)) != PSY_OK)
@@ -1304,7 +1260,7 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
             if ((ps = timed([&] { psy::launch_shade(st, sms, s->scene->view, p, b, paths, step, trace_path, tr); },
                             pf.shade_launches, pf.shade_ms)) != PSY_OK)
                 return ps;
-            psy::launch_count_rays(st, b.counters, s->stats.as<unsigned long long>());
+            psy::launch_count_rays(st, b.counters, s->arena.stats.as<unsigned long long>());
             if (prof && (ps = read_counters(c3)) != PSY_OK) return ps;
             pf.shade_bytes += 304.0 * c3[0] + 68.0 * c3[2];
             if ((ps = timed([&] { psy::launch_shadow(st, sms, s->scene->view, p, b, paths, step, trace_path, tr); },
@@ -1338,7 +1294,7 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
     float ms = 0.0f;
     PSY_CUDA_TRY(cudaEventElapsedTime(&ms, s->ev_begin, s->ev_end));
     unsigned long long counts[2] = {0, 0};
-    PSY_CUDA_TRY(cudaMemcpy(counts, s->stats.ptr, sizeof(counts), cudaMemcpyDeviceToHost));
+    PSY_CUDA_TRY(cudaMemcpy(counts, s->arena.stats.ptr, sizeof(counts), cudaMemcpyDeviceToHost));
     stats.closest_rays = counts[0];
     stats.path_segments = counts[0];
     stats.shadow_rays = counts[1];

@@ -1,0 +1,127 @@
+// Host objects shared by the translation units of libpsycles_cuda.so: the
+// opaque handles of the C ABI (context, compiled scene, session), device
+// buffers, the wavefront path-state arena and error reporting.
+#pragma once
+
+#include "../../include/psycles_cuda.h"
+#include "psy_scene.h"
+
+#include <cuda_runtime.h>
+
+struct psy_session;
+
+#include <algorithm>
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace psy::host {
+
+// Records `message` as psy_last_error() of this thread and returns `status`.
+psy_status fail(psy_status status, const std::string &message);
+
+// Validates a SampleRange against a session (path_tracer_session.cpp:275-292),
+// uploads the Sobol table sized from `total` and returns the render
+// parameters of the range.
+psy_status prepare_render(psy_session *s, uint32_t first, uint32_t count, uint32_t offset, uint32_t total,
+                          RenderParams *out);
+
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    ~DeviceBuffer() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        release();
+        bytes = n;
+        if (n == 0) return cudaSuccess;
+        return cudaMalloc(&ptr, n);
+    }
+    template <typename T>
+    cudaError_t upload(const std::vector<T> &v, cudaStream_t st) {
+        cudaError_t e = alloc(std::max<size_t>(v.size() * sizeof(T), 16));
+        if (e != cudaSuccess || v.empty()) return e;
+        return cudaMemcpyAsync(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+    }
+    template <typename T>
+    T *as() const {
+        return static_cast<T *>(ptr);
+    }
+};
+
+// Wavefront path state over `capacity` paths (structure of arrays); the
+// per-path job array only for batched wavefronts.
+struct PathArena {
+    uint32_t capacity = 0;
+    DeviceBuffer ray_o, ray_d, tp, rad, st, st2, sample, aov_n, aov_a, mis_n, hit, hit_prim, sh_o, sh_d, sh_c, sh_ids,
+        sh_path, qa, qb, sq, job, counters, stats;
+    PathBuffers view{};
+    psy_status ensure(uint32_t n, bool with_job);
+    static size_t bytes_per_path(bool with_job);
+};
+
+}  // namespace psy::host
+
+#define PSY_CUDA_TRY(expr)                                                                          \
+    do {                                                                                            \
+        const cudaError_t err_ = (expr);                                                            \
+        if (err_ != cudaSuccess) {                                                                  \
+            return psy::host::fail(PSY_ERROR_CUDA, std::string(#expr ": ") + cudaGetErrorString(err_)); \
+        }                                                                                           \
+    } while (0)
+
+struct psy_context {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+};
+
+struct psy_scene {
+    psy_context *context = nullptr;
+    uint64_t revision = 0;
+    psy_camera_desc camera{};
+    std::vector<psy::MaterialGpu> materials;
+    std::vector<float> scalars, vectors;
+    psy::host::DeviceBuffer tlas, blas, tris, instances, meshes, positions, normals, indices, tri_materials, material_buf, code,
+        scalar_buf, vector_buf, emitters, distribution, lights, lamp_bounds, lamp_ids, lt_nodes, lt_emitters, lt_mapping,
+        lt_lookup;
+    psy::SceneView view{};
+    uint64_t triangle_count = 0;
+    double build_ms = 0.0;
+};
+
+struct psy_session {
+    psy_scene *scene = nullptr;
+    psy_render_settings settings{};
+    psy::RenderParams params{};
+    bool has_camera = false;      // psy_session_set_camera override
+    psy_camera_desc camera{};
+    uint32_t pixels = 0;
+    uint32_t total = 0;
+    uint32_t sobol_size = 0;
+    uint32_t rendered = 0;
+    std::atomic<bool> cancelled{false};
+    psy::host::DeviceBuffer sobol, filter, combined, normal, albedo, sample_count;
+    // path state
+    psy::host::PathArena arena;
+    // trace
+    psy::host::DeviceBuffer trace_buf;
+    bool trace_requested = false;
+    uint32_t trace_x = 0, trace_y = 0, trace_sample = 0;
+    psy_path_trace trace_host{};
+    psy_render_stats last_stats{};
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+    bool profiling = false;
+    psy_kernel_profile profile{};
+    cudaEvent_t ev_k[2] = {nullptr, nullptr};
+};
+

@@ -45,55 +45,83 @@ __device__ __forceinline__ void set3(float *d, f3 v) {
 // ------------------------------------------------------------------ raygen
 // begin_path_sample / construct_camera_ray (src/luisa/path_kernel_setup.cpp:485-700,
 // src/luisa/path_tracer_camera.cpp:10-246).
+__device__ __forceinline__ void raygen_path(const RenderParams &p, const PathBuffers &b, uint32_t i, uint32_t local,
+                                            uint32_t sample, uint32_t trace_path, psy_path_trace *trace) {
+    const uint32_t x = p.win_x + local % p.win_w;
+    const uint32_t y = p.win_y + local / p.win_w;
+    const uint32_t cycles_y = p.full_h - 1u - y;
+    const uint32_t rng_hash = pixel_hash(x, cycles_y, p.seed);
+    const float4 fs = sample_4d(p, sample, rng_hash, 0u);
+    const f2 filter = sample == 0u ? mk2(0.5f, 0.5f) : mk2(fs.x, fs.y);
+    const float jx = pixel_filter_sample(p.filter, filter.x);
+    const float jy = 1.0f - pixel_filter_sample(p.filter, filter.y);
+    const float W = static_cast<float>(p.full_w), H = static_cast<float>(p.full_h);
+    const float sx = 2.0f * (static_cast<float>(x) + jx) / W - 1.0f + 2.0f * p.shift_x;
+    const float sy = 1.0f - 2.0f * (static_cast<float>(y) + jy) / H + 2.0f * p.shift_y;
+    const f3 local_dir = normalize(mk3(sx * p.htan, sy * p.vtan, -1.0f));
+    const float clip_cos = -local_dir.z;
+    const Xform cam = xform12(p.cam);
+    f3 origin = xform_point(cam, mk3(0.0f));
+    const f3 dir = safe_normalize(xform_direction(cam, local_dir), mk3(0.0f, 0.0f, -1.0f));
+    const float safe_cos = maxf_(fabsf(clip_cos), 1.0e-20f);
+    const float near_t = p.near_clip / safe_cos;
+    const float far_t = (p.far_clip - p.near_clip) / safe_cos;
+    origin = origin + dir * near_t;
+    b.ray_o[i] = make_float4(origin.x, origin.y, origin.z, 0.0f);
+    b.ray_d[i] = make_float4(dir.x, dir.y, dir.z, far_t);
+    b.tp[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    b.rad[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    // initial_state (include/psycles/luisa/cycles_path_state.h:187-199)
+    b.st[i] = make_uint4(128u | 512u, 1u, 16u, 0u);
+    b.st2[i] = make_uint4(kSt2Delta, kInvalid, kInvalid, local);
+    b.sample[i] = sample;
+    b.aov_n[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    b.aov_a[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    b.mis_n[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    b.queue_in[i] = i;
+    if (i == trace_path && trace) {
+        trace->pixel_x = x;
+        trace->pixel_y = y;
+        trace->sample = sample;
+        trace->rng_hash = rng_hash;
+        trace->filter[0] = filter.x;
+        trace->filter[1] = filter.y;
+        set3(trace->ray_origin, origin);
+        set3(trace->ray_direction, dir);
+        trace->valid = 1u;
+        trace->event_count = 0u;
+    }
+}
+
 __global__ void k_raygen(RenderParams p, PathBuffers b, uint32_t pixels, uint32_t paths, uint32_t sample_base,
                          uint32_t trace_path, psy_path_trace *trace) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < paths; i += gridDim.x * blockDim.x)
+        raygen_path(p, b, i, i % pixels, sample_base + i / pixels, trace_path, trace);
+}
+
+// The item of a batched wavefront that holds `index` (items sorted by the
+// field `begin` selects).
+template <typename Begin>
+__device__ __forceinline__ uint32_t find_item(const BatchItem *items, uint32_t n, uint32_t index, Begin begin) {
+    uint32_t lo = 0u, hi = n;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (begin(items[mid]) <= index) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Camera rays of every item of a batched wavefront; records each path's job.
+// The wavefront's shape comes from device memory (round[0] paths, round[2]
+// items) so one captured launch serves every wavefront.
+__global__ void k_raygen_batch(const JobGpu *jobs, const BatchItem *items, const uint32_t *round, PathBuffers b) {
+    const uint32_t paths = round[0], item_count = round[2];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < paths; i += gridDim.x * blockDim.x) {
-        const uint32_t local = i % pixels;
-        const uint32_t sample = sample_base + i / pixels;
-        const uint32_t x = p.win_x + local % p.win_w;
-        const uint32_t y = p.win_y + local / p.win_w;
-        const uint32_t cycles_y = p.full_h - 1u - y;
-        const uint32_t rng_hash = pixel_hash(x, cycles_y, p.seed);
-        const float4 fs = sample_4d(p, sample, rng_hash, 0u);
-        const f2 filter = sample == 0u ? mk2(0.5f, 0.5f) : mk2(fs.x, fs.y);
-        const float jx = pixel_filter_sample(p.filter, filter.x);
-        const float jy = 1.0f - pixel_filter_sample(p.filter, filter.y);
-        const float W = static_cast<float>(p.full_w), H = static_cast<float>(p.full_h);
-        const float sx = 2.0f * (static_cast<float>(x) + jx) / W - 1.0f + 2.0f * p.shift_x;
-        const float sy = 1.0f - 2.0f * (static_cast<float>(y) + jy) / H + 2.0f * p.shift_y;
-        const f3 local_dir = normalize(mk3(sx * p.htan, sy * p.vtan, -1.0f));
-        const float clip_cos = -local_dir.z;
-        const Xform cam = xform12(p.cam);
-        f3 origin = xform_point(cam, mk3(0.0f));
-        const f3 dir = safe_normalize(xform_direction(cam, local_dir), mk3(0.0f, 0.0f, -1.0f));
-        const float safe_cos = maxf_(fabsf(clip_cos), 1.0e-20f);
-        const float near_t = p.near_clip / safe_cos;
-        const float far_t = (p.far_clip - p.near_clip) / safe_cos;
-        origin = origin + dir * near_t;
-        b.ray_o[i] = make_float4(origin.x, origin.y, origin.z, 0.0f);
-        b.ray_d[i] = make_float4(dir.x, dir.y, dir.z, far_t);
-        b.tp[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-        b.rad[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        // initial_state (include/psycles/luisa/cycles_path_state.h:187-199)
-        b.st[i] = make_uint4(128u | 512u, 1u, 16u, 0u);
-        b.st2[i] = make_uint4(kSt2Delta, kInvalid, kInvalid, local);
-        b.sample[i] = sample;
-        b.aov_n[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        b.aov_a[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        b.mis_n[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        b.queue_in[i] = i;
-        if (i == trace_path && trace) {
-            trace->pixel_x = x;
-            trace->pixel_y = y;
-            trace->sample = sample;
-            trace->rng_hash = rng_hash;
-            trace->filter[0] = filter.x;
-            trace->filter[1] = filter.y;
-            set3(trace->ray_origin, origin);
-            set3(trace->ray_direction, dir);
-            trace->valid = 1u;
-            trace->event_count = 0u;
-        }
+        const BatchItem it = items[find_item(items, item_count, i, [](const BatchItem &t) { return t.path_begin; })];
+        const uint32_t r = i - it.path_begin;
+        b.job[i] = it.job;
+        raygen_path(jobs[it.job].p, b, i, r % it.pixels, it.sample_base + r / it.pixels, kInvalid, nullptr);
     }
 }
 
@@ -147,16 +175,23 @@ __device__ __forceinline__ uint32_t warp_fetch(uint32_t *fetch_counter, uint32_t
     return q < count ? q : kInvalid;
 }
 
-__global__ void __launch_bounds__(128, PSY_INTERSECT_MIN_BLOCKS) k_intersect(const __grid_constant__ SceneView s, const __grid_constant__ PathBuffers b) {
+// kMulti: paths of a batched wavefront, each traced in its job's scene.
+template <bool kMulti>
+__global__ void __launch_bounds__(128, PSY_INTERSECT_MIN_BLOCKS)
+    k_intersect(const __grid_constant__ SceneView s_arg, const __grid_constant__ PathBuffers b, const JobGpu *jobs) {
     const uint32_t count = b.counters[0];
     TraversalState t;
     Hit best;
     bool has = false, active = false, exhausted = false;
-    uint32_t path = 0u;
+    uint32_t path = 0u, job = 0u;
     for (;;) {
         const uint32_t q = warp_fetch(&b.counters[3], count, !active, exhausted);
         if (q != kInvalid) {
             path = b.queue_in[q];
+            if (kMulti) job = b.job[path];
+        }
+        const SceneView &s = kMulti ? jobs[job].s : s_arg;
+        if (q != kInvalid) {
             const float4 o = b.ray_o[path], d = b.ray_d[path];
             const uint32_t vis = b.st[path].y;
             const uint4 st2 = b.st2[path];
@@ -298,10 +333,13 @@ __device__ __forceinline__ float next_float_up(float t) {
 
 // kTrace selects the variant that records the per-path trace; the render
 // variant carries no trace code.
-template <bool kTrace>
-__global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS) k_shade(const __grid_constant__ SceneView s, const __grid_constant__ RenderParams p,
-                                                                    const __grid_constant__ PathBuffers b, uint32_t step,
-                                               uint32_t trace_path, psy_path_trace *trace) {
+// kMulti: paths of a batched wavefront, each shaded with its job's scene and
+// parameters.
+template <bool kTrace, bool kMulti>
+__global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
+    k_shade(const __grid_constant__ SceneView s_arg, const __grid_constant__ RenderParams p_arg,
+            const __grid_constant__ PathBuffers b, uint32_t step, uint32_t trace_path, psy_path_trace *trace,
+            const JobGpu *jobs) {
     const uint32_t count = b.counters[0];
     const uint32_t rounds = (count + gridDim.x * blockDim.x - 1u) / (gridDim.x * blockDim.x);
     // Every lane runs the same number of rounds so the warp-aggregated queue
@@ -316,6 +354,9 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS) k_shade(const __gri
         uint4 sh_ids;
         if (active) {
             i = b.queue_in[q];
+            const uint32_t job = kMulti ? b.job[i] : 0u;
+            const SceneView &s = kMulti ? jobs[job].s : s_arg;
+            const RenderParams &p = kMulti ? jobs[job].p : p_arg;
             psy_path_event *ev = nullptr;
             if (kTrace && trace && i == trace_path && step < PSY_TRACE_MAX_EVENTS) {
                 ev = &trace->events[step];
@@ -784,18 +825,24 @@ __device__ __forceinline__ f3 shadow_transmittance(const SceneView &s, const Ren
 // Opaque-only scenes stop at the first accepted candidate; otherwise
 // transparent hits are collected per lane and resolved as in
 // shadow_transmittance once the traversal ends.
-__global__ void __launch_bounds__(128, PSY_SHADOW_MIN_BLOCKS) k_shadow(const __grid_constant__ SceneView s, const __grid_constant__ RenderParams p,
-                                                                      const __grid_constant__ PathBuffers b, uint32_t step,
-                                                uint32_t trace_path, psy_path_trace *trace) {
+// kMulti: shadow rays of a batched wavefront, each in its path's job.
+template <bool kMulti>
+__global__ void __launch_bounds__(128, PSY_SHADOW_MIN_BLOCKS)
+    k_shadow(const __grid_constant__ SceneView s_arg, const __grid_constant__ RenderParams p_arg,
+             const __grid_constant__ PathBuffers b, uint32_t step, uint32_t trace_path, psy_path_trace *trace,
+             const JobGpu *jobs) {
     const uint32_t count = b.counters[2];
     TraversalState t;
     bool active = false, exhausted = false, blocked = false, overflow = false;
-    uint32_t q_cur = 0u;
+    uint32_t q_cur = 0u, job = 0u;
     float lt[kShadowList];
     uint32_t lo[kShadowList], lp[kShadowList], lm[kShadowList];
     int n = 0;
     for (;;) {
         const uint32_t q = warp_fetch(&b.counters[4], count, !active, exhausted);
+        if (kMulti && q != kInvalid) job = b.job[b.sh_path[q]];
+        const SceneView &s = kMulti ? jobs[job].s : s_arg;
+        const RenderParams &p = kMulti ? jobs[job].p : p_arg;
         if (q != kInvalid) {
             q_cur = q;
             const float4 o = b.sh_o[q], d = b.sh_d[q];
@@ -896,34 +943,75 @@ __global__ void __launch_bounds__(128, PSY_SHADOW_MIN_BLOCKS) k_shadow(const __g
 // -------------------------------------------------------------------- film
 // accumulate_path_sample + write_film (src/luisa/path_kernel_setup.cpp:903-1062):
 // samples are added in sample order.
+// One window pixel: its samples of the batch added to the film in sample
+// order, one at a time, so the film does not depend on how the samples were
+// grouped into batches.
+__device__ __forceinline__ void film_pixel(const PathBuffers &b, uint32_t px, uint32_t pixels, uint32_t samples,
+                                           uint32_t path_begin, float4 *combined, float4 *normal, float4 *albedo,
+                                           uint32_t *sample_count, uint32_t trace_path, psy_path_trace *trace) {
+    float4 c = combined[px], n = normal[px], a = albedo[px];
+    for (uint32_t k = 0; k < samples; ++k) {
+        const uint32_t i = path_begin + k * pixels + px;
+        const float4 r = b.rad[i];
+        f3 rad = mk3(r.x, r.y, r.z);
+        if (any_nan(rad)) rad = mk3(0.0f);
+        c.x += rad.x;
+        c.y += rad.y;
+        c.z += rad.z;
+        c.w += r.w;
+        const float4 nn = b.aov_n[i], aa = b.aov_a[i];
+        n.x += nn.x;
+        n.y += nn.y;
+        n.z += nn.z;
+        n.w += 1.0f;
+        a.x += aa.x;
+        a.y += aa.y;
+        a.z += aa.z;
+        a.w += 1.0f;
+        if (trace && i == trace_path) set3(trace->radiance, rad);
+    }
+    combined[px] = c;
+    normal[px] = n;
+    albedo[px] = a;
+    sample_count[px] += samples;
+}
+
 __global__ void k_film(PathBuffers b, uint32_t pixels, uint32_t samples, float4 *combined, float4 *normal,
                        float4 *albedo, uint32_t *sample_count, uint32_t trace_path, psy_path_trace *trace) {
-    for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < pixels; px += gridDim.x * blockDim.x) {
-        float4 c = combined[px], n = normal[px], a = albedo[px];
-        for (uint32_t k = 0; k < samples; ++k) {
-            const uint32_t i = k * pixels + px;
-            const float4 r = b.rad[i];
-            f3 rad = mk3(r.x, r.y, r.z);
-            if (any_nan(rad)) rad = mk3(0.0f);
-            c.x += rad.x;
-            c.y += rad.y;
-            c.z += rad.z;
-            c.w += r.w;
-            const float4 nn = b.aov_n[i], aa = b.aov_a[i];
-            n.x += nn.x;
-            n.y += nn.y;
-            n.z += nn.z;
-            n.w += 1.0f;
-            a.x += aa.x;
-            a.y += aa.y;
-            a.z += aa.z;
-            a.w += 1.0f;
-            if (trace && i == trace_path) set3(trace->radiance, rad);
-        }
-        combined[px] = c;
-        normal[px] = n;
-        albedo[px] = a;
-        sample_count[px] += samples;
+    for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < pixels; px += gridDim.x * blockDim.x)
+        film_pixel(b, px, pixels, samples, 0u, combined, normal, albedo, sample_count, trace_path, trace);
+}
+
+// Film of every item of a batched wavefront (a job appears in at most one
+// item per wavefront, so its pixels have one writer).
+__global__ void k_film_batch(const JobGpu *jobs, const BatchItem *items, const uint32_t *round, PathBuffers b) {
+    const uint32_t film_pixels = round[1], item_count = round[2];
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < film_pixels; g += gridDim.x * blockDim.x) {
+        const BatchItem it = items[find_item(items, item_count, g, [](const BatchItem &t) { return t.film_begin; })];
+        const JobGpu &j = jobs[it.job];
+        film_pixel(b, g - it.film_begin, it.pixels, it.samples, it.path_begin, j.combined, j.normal, j.albedo,
+                   j.sample_count, kInvalid, nullptr);
+    }
+}
+
+// Start of a batched wavefront: the wavefront `*cursor` of a planned call
+// becomes current (its header and items copied to the fixed buffers every
+// later kernel reads), the queue counters are set, and the cursor advances.
+// One block.
+__global__ void k_begin_round(uint32_t *counters, uint32_t *round, BatchItem *items, const uint32_t *plan_rounds,
+                              const BatchItem *plan_items, uint32_t *cursor, uint32_t max_items) {
+    const uint32_t w = *cursor;
+    const uint32_t n = plan_rounds[4u * w + 2u];
+    for (uint32_t k = threadIdx.x; k < n && k < max_items; k += blockDim.x)
+        items[k] = plan_items[size_t(w) * max_items + k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        round[0] = plan_rounds[4u * w];
+        round[1] = plan_rounds[4u * w + 1u];
+        round[2] = n;
+        counters[0] = round[0];
+        counters[1] = counters[2] = counters[3] = counters[4] = 0u;
+        *cursor = w + 1u;
     }
 }
 
@@ -996,18 +1084,22 @@ int persistent_grid(uint32_t work, int sms) {
 }
 
 void launch_intersect(cudaStream_t st, int sms, const SceneView &s, const PathBuffers &b, uint32_t max_work) {
-    k_intersect<<<persistent_grid(max_work, sms), 128, 0, st>>>(s, b);
+    k_intersect<false><<<persistent_grid(max_work, sms), 128, 0, st>>>(s, b, nullptr);
 }
 void launch_shade(cudaStream_t st, int sms, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                   uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
     if (trace)
-        k_shade<true><<<launch_grid(max_work, 128, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace);
+        k_shade<true, false><<<launch_grid(max_work, 128, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr);
     else
-        k_shade<false><<<launch_grid(max_work, 128, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace);
+        k_shade<false, false><<<launch_grid(max_work, 128, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr);
 }
 void launch_shadow(cudaStream_t st, int sms, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                    uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
-    k_shadow<<<persistent_grid(max_work, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace);
+    k_shadow<false><<<persistent_grid(max_work, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr);
+}
+void launch_begin_round(cudaStream_t st, uint32_t *counters, uint32_t *round, BatchItem *items,
+                        const uint32_t *plan_rounds, const BatchItem *plan_items, uint32_t *cursor, uint32_t max_items) {
+    k_begin_round<<<1, 256, 0, st>>>(counters, round, items, plan_rounds, plan_items, cursor, max_items);
 }
 void launch_swap(cudaStream_t st, uint32_t *counters) { k_swap_counters<<<1, 1, 0, st>>>(counters); }
 void launch_count_rays(cudaStream_t st, const uint32_t *counters, unsigned long long *stats) {
@@ -1018,6 +1110,29 @@ void launch_film(cudaStream_t st, int sms, const PathBuffers &b, uint32_t pixels
     k_film<<<launch_grid(pixels, 256, sms), 256, 0, st>>>(b, pixels, samples, combined, normal, albedo, sample_count,
                                                         trace_path, trace);
 }
+// Batched wavefront: every kernel reads each path's job record.
+void launch_raygen_batch(cudaStream_t st, int sms, const JobGpu *jobs, const BatchItem *items, const uint32_t *round,
+                         const PathBuffers &b, uint32_t max_paths) {
+    k_raygen_batch<<<launch_grid(max_paths, 256, sms), 256, 0, st>>>(jobs, items, round, b);
+}
+void launch_intersect_batch(cudaStream_t st, int sms, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work) {
+    k_intersect<true><<<persistent_grid(max_work, sms), 128, 0, st>>>(SceneView{}, b, jobs);
+}
+void launch_shade_batch(cudaStream_t st, int sms, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work,
+                        uint32_t step) {
+    k_shade<false, true><<<launch_grid(max_work, 128, sms), 128, 0, st>>>(SceneView{}, RenderParams{}, b, step,
+                                                                           kInvalid, nullptr, jobs);
+}
+void launch_shadow_batch(cudaStream_t st, int sms, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work,
+                         uint32_t step) {
+    k_shadow<true><<<persistent_grid(max_work, sms), 128, 0, st>>>(SceneView{}, RenderParams{}, b, step, kInvalid,
+                                                                    nullptr, jobs);
+}
+void launch_film_batch(cudaStream_t st, int sms, const JobGpu *jobs, const BatchItem *items, const uint32_t *round,
+                       const PathBuffers &b, uint32_t max_pixels) {
+    k_film_batch<<<launch_grid(max_pixels, 256, sms), 256, 0, st>>>(jobs, items, round, b);
+}
+
 void launch_debug_light_tree(cudaStream_t st, const SceneView &s, const float4 *queries, const uint32_t *pdf_emitters,
                              uint32_t count, uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf) {
     k_debug_light_tree<<<(count + 127u) / 128u, 128, 0, st>>>(s, queries, pdf_emitters, count, out_emitters,

@@ -149,6 +149,25 @@ struct PathBuffers {
     uint32_t *queue_out;
     uint32_t *shadow_queue;
     uint32_t *counters;  // [0] in count, [1] out count, [2] shadow count, [3..] stats
+    uint32_t *job;       // batched wavefronts: the job of each path
+};
+
+// One job of a batched wavefront: a session's render parameters, its scene
+// and its film.  Paths of many jobs share the path state; each path reads
+// its job's record.
+struct alignas(16) JobGpu {
+    RenderParams p;
+    SceneView s;
+    float4 *combined, *normal, *albedo;
+    uint32_t *sample_count;
+};
+
+// A block of paths of one job in a batched wavefront: samples
+// [sample_base, sample_base + samples) over the job's `pixels` window
+// pixels, laid out sample-major from path_begin.  film_begin is the item's
+// first pixel in the batch-wide pixel numbering the film kernel walks.
+struct BatchItem {
+    uint32_t job, path_begin, pixels, samples, sample_base, film_begin, pad0, pad1;
 };
 
 // Packed counters of st.w: bounce | diffuse << 8 | glossy << 16 | transmission << 24.

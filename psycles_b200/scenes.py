@@ -110,6 +110,18 @@ def _column_major(m: np.ndarray) -> list[float]:
     return [float(v) for v in np.asarray(m, dtype=np.float64).T.reshape(-1)]
 
 
+def camera_desc(cam: "Camera") -> _abi.CameraDesc:
+    """contract::CameraDesc of a Camera (perspective)."""
+    c = _abi.CameraDesc()
+    c.camera_to_world[:] = _column_major(cam.transform)
+    c.field_of_view = cam.field_of_view
+    c.horizontal_field_of_view = cam.horizontal_field_of_view
+    c.sensor_fit = cam.sensor_fit
+    c.lens_shift_x, c.lens_shift_y = cam.lens_shift_x, cam.lens_shift_y
+    c.near_clip, c.far_clip = cam.near_clip, cam.far_clip
+    return c
+
+
 class SceneDescHandle:
     """A psy_scene_desc plus the arrays it points into (kept alive here)."""
 
@@ -169,12 +181,7 @@ class SceneDescHandle:
         desc.material_count = len(scene.materials)
         desc.light_count = len(scene.lights)
         cam = scene.camera
-        desc.camera.camera_to_world[:] = _column_major(cam.transform)
-        desc.camera.field_of_view = cam.field_of_view
-        desc.camera.horizontal_field_of_view = cam.horizontal_field_of_view
-        desc.camera.sensor_fit = cam.sensor_fit
-        desc.camera.lens_shift_x, desc.camera.lens_shift_y = cam.lens_shift_x, cam.lens_shift_y
-        desc.camera.near_clip, desc.camera.far_clip = cam.near_clip, cam.far_clip
+        desc.camera = camera_desc(cam)
         desc.background[:] = scene.background
         desc.world_visibility = scene.world_visibility
         desc.revision = scene.revision
