@@ -47,6 +47,7 @@ typedef struct psy_context psy_context;
 typedef struct psy_scene psy_scene;
 typedef struct psy_session psy_session;
 typedef struct psy_batch psy_batch;
+typedef struct psy_server psy_server;
 
 /* ---------------------------------------------------------------- scene -- */
 
@@ -493,6 +494,81 @@ psy_status psy_batch_get_stats(const psy_batch *batch, psy_batch_stats *out);
  * item count; PSY_ERROR_RANGE when max_items is too small. */
 psy_status psy_batch_plan(const uint32_t *pixels, const uint32_t *samples, uint32_t n, uint32_t capacity,
                           uint32_t *out_items, uint32_t max_items, uint32_t *out_count);
+
+/* ----------------------------------------------------------- serving -- */
+/* A render server: a request loop thread over resident scenes that admits
+ * jobs against an HBM budget and renders all running jobs in shared
+ * wavefronts (continuous batching: a job submitted while others run joins
+ * the next wavefront).  No counterpart in the reference.  A job's passes
+ * equal those of a session rendering the same settings and samples alone.
+ * Scenes stay owned by the caller and must outlive their jobs; they must
+ * belong to the server's context, and the caller issues no other work on
+ * that context while the server runs except psy_scene_compile. */
+typedef struct psy_server_config {
+    uint64_t hbm_budget_bytes;   /* scenes + job films/tables + path state; 0 = 120 GiB */
+    uint32_t path_capacity;      /* paths per wavefront; 0 = 4 Mi */
+    uint32_t max_running;        /* jobs sharing the wavefronts; 0 = 256 */
+    uint32_t use_graph;          /* 1: wavefronts replay a captured CUDA graph */
+    uint32_t reserved;
+} psy_server_config;
+
+#define PSY_JOB_QUEUED 0u
+#define PSY_JOB_RUNNING 1u
+#define PSY_JOB_DONE 2u
+#define PSY_JOB_FAILED 3u
+#define PSY_JOB_CANCELLED 4u
+
+typedef struct psy_job_info {
+    uint32_t state;              /* PSY_JOB_* */
+    int32_t status;              /* psy_status of a failed job */
+    uint32_t samples_done;
+    uint32_t samples_total;
+    double submit_ms;            /* since the server started */
+    double admit_ms;
+    double done_ms;
+} psy_job_info;
+
+typedef struct psy_server_stats {
+    uint64_t jobs_submitted;
+    uint64_t jobs_done;
+    uint64_t jobs_failed;
+    uint64_t samples;            /* pixel samples issued */
+    uint64_t wavefronts;
+    uint64_t bytes_in_use;       /* admitted against the budget */
+    uint64_t bytes_peak;
+    double busy_ms;              /* wall time with work on the GPU */
+    double latency_p50_ms;       /* submit -> done over finished jobs */
+    double latency_p99_ms;
+    uint32_t latency_jobs;
+    uint32_t reserved;
+} psy_server_stats;
+
+psy_status psy_server_create(psy_context *context, const psy_server_config *config, psy_server **out);
+/* Stops the loop after the wavefronts in flight; queued jobs are dropped. */
+void psy_server_destroy(psy_server *server);
+/* Queues a job rendering `samples` samples of `scene` with `settings`
+ * (window and all) through `camera` (NULL: the scene's camera).  A job whose
+ * bytes cannot fit the budget even alone fails with PSY_ERROR_OUT_OF_MEMORY. */
+psy_status psy_server_submit(psy_server *server, psy_scene *scene, const psy_render_settings *settings,
+                             const psy_camera_desc *camera, uint32_t samples, uint64_t *job);
+/* A parameter-only material edit (psy_scene_rebind_parameters) ordered
+ * with the jobs: applied once no running job uses the scene, before any job
+ * submitted after it is admitted. */
+psy_status psy_server_rebind_parameters(psy_server *server, psy_scene *scene, uint32_t material,
+                                        const float *scalars, uint32_t scalar_count,
+                                        const float *vectors, uint32_t vector_count);
+psy_status psy_server_poll(psy_server *server, uint64_t job, psy_job_info *out);
+/* Waits for a job to end (bounded); PSY_ERROR_TIMEOUT if it has not. */
+psy_status psy_server_wait(psy_server *server, uint64_t job, uint32_t timeout_ms);
+/* A finished job's pass, as psy_session_read_pass. */
+psy_status psy_server_read_pass(psy_server *server, uint64_t job, uint32_t pass_kind, float *out,
+                                uint64_t capacity, uint32_t *channels);
+/* Frees a finished job's film and returns its bytes to the budget. */
+psy_status psy_server_release(psy_server *server, uint64_t job);
+psy_status psy_server_cancel(psy_server *server, uint64_t job);
+psy_status psy_server_get_stats(psy_server *server, psy_server_stats *out);
+/* Device bytes of a compiled scene (what a server counts against its budget). */
+uint64_t psy_scene_device_bytes(const psy_scene *scene);
 
 /* ------------------------------------------------ device probes (GPU) -- */
 

@@ -14,6 +14,8 @@ c_float_p = ctypes.POINTER(ctypes.c_float)
 c_uint32_p = ctypes.POINTER(ctypes.c_uint32)
 
 PSY_OK = 0
+(PSY_ERROR_INVALID_ARGUMENT, PSY_ERROR_OUT_OF_MEMORY, PSY_ERROR_CUDA, PSY_ERROR_CANCELLED, PSY_ERROR_RANGE,
+ PSY_ERROR_UNSUPPORTED, PSY_ERROR_STATE, PSY_ERROR_TIMEOUT) = range(1, 9)
 STATUS_NAMES = {
     0: "ok", 1: "invalid argument", 2: "out of memory", 3: "cuda error", 4: "cancelled",
     5: "range", 6: "unsupported", 7: "state", 8: "timeout",
@@ -142,6 +144,27 @@ class BatchStats(ctypes.Structure):
                 ("graph_launches", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("path_capacity", ctypes.c_uint32),
+                ("max_running", ctypes.c_uint32), ("use_graph", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class JobInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_uint32), ("status", ctypes.c_int32), ("samples_done", ctypes.c_uint32),
+                ("samples_total", ctypes.c_uint32), ("submit_ms", ctypes.c_double), ("admit_ms", ctypes.c_double),
+                ("done_ms", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("jobs_submitted", "jobs_done", "jobs_failed", "samples", "wavefronts",
+                                               "bytes_in_use", "bytes_peak")] + [
+        ("busy_ms", ctypes.c_double), ("latency_p50_ms", ctypes.c_double), ("latency_p99_ms", ctypes.c_double),
+        ("latency_jobs", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
+
+
 # Entry points declared by include/psycles_cuda.h: (name, restype, argtypes).
 SIGNATURES = [
     ("psy_last_error", ctypes.c_char_p, []),
@@ -184,6 +207,21 @@ SIGNATURES = [
     ("psy_batch_get_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchStats)]),
     ("psy_batch_plan", ctypes.c_int, [c_uint32_p, c_uint32_p, ctypes.c_uint32, ctypes.c_uint32, c_uint32_p,
                                       ctypes.c_uint32, c_uint32_p]),
+    ("psy_server_create", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerConfig),
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    ("psy_server_destroy", None, [ctypes.c_void_p]),
+    ("psy_server_submit", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]),
+    ("psy_server_rebind_parameters", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, c_float_p,
+                                                    ctypes.c_uint32, c_float_p, ctypes.c_uint32]),
+    ("psy_server_poll", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(JobInfo)]),
+    ("psy_server_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32]),
+    ("psy_server_read_pass", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, c_float_p,
+                                            ctypes.c_uint64, c_uint32_p]),
+    ("psy_server_release", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("psy_server_cancel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("psy_server_get_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    ("psy_scene_device_bytes", ctypes.c_uint64, [ctypes.c_void_p]),
     ("psy_debug_light_tree", ctypes.c_int,
      [ctypes.c_void_p, c_float_p, c_uint32_p, ctypes.c_uint32, c_uint32_p, c_float_p, c_float_p]),
 ]

@@ -316,3 +316,71 @@ def batch_plan(pixels: list[int], samples: list[int], capacity: int) -> np.ndarr
     _abi.check(lib.psy_batch_plan(_abi.ptr(px, ctypes.c_uint32), _abi.ptr(sp, ctypes.c_uint32), len(px), capacity,
                                   _abi.ptr(out, ctypes.c_uint32), count.value, ctypes.byref(count)))
     return out[:count.value]
+
+
+class RenderServer:
+    """psy_server_*: a request loop over resident scenes with HBM-budget
+    admission and continuous batching of all running jobs."""
+
+    def __init__(self, context: Context, hbm_budget_bytes: int = 0, path_capacity: int = 0, max_running: int = 0,
+                 use_graph: bool = True):
+        self.context = context
+        self.lib = context.lib
+        cfg = _abi.ServerConfig(hbm_budget_bytes, path_capacity, max_running, 1 if use_graph else 0, 0)
+        h = ctypes.c_void_p()
+        _abi.check(self.lib.psy_server_create(context.handle, ctypes.byref(cfg), ctypes.byref(h)))
+        self.handle = h
+
+    def submit(self, compiled: CompiledScene, settings: _abi.RenderSettings, samples: int, camera=None) -> int:
+        from .scenes import camera_desc
+        cam = camera_desc(camera) if camera is not None else None
+        job = ctypes.c_uint64()
+        _abi.check(self.lib.psy_server_submit(self.handle, compiled.handle, ctypes.byref(settings),
+                                              ctypes.byref(cam) if cam is not None else None, samples,
+                                              ctypes.byref(job)))
+        return int(job.value)
+
+    def rebind_parameters(self, compiled: CompiledScene, material: int, scalars, vectors) -> None:
+        sc = np.ascontiguousarray(scalars, dtype=np.float32).reshape(-1)
+        vc = np.ascontiguousarray(vectors, dtype=np.float32).reshape(-1)
+        _abi.check(self.lib.psy_server_rebind_parameters(self.handle, compiled.handle, material, _abi.ptr(sc), sc.size,
+                                                         _abi.ptr(vc), vc.size // 3))
+
+    def poll(self, job: int) -> _abi.JobInfo:
+        info = _abi.JobInfo()
+        _abi.check(self.lib.psy_server_poll(self.handle, job, ctypes.byref(info)))
+        return info
+
+    def wait(self, job: int, timeout_ms: int = 60000) -> int:
+        """The psy_status of the job's end (PSY_ERROR_TIMEOUT if still running)."""
+        return int(self.lib.psy_server_wait(self.handle, job, timeout_ms))
+
+    def read_pass(self, job: int, kind: int, width: int, height: int) -> np.ndarray:
+        ch = 1 if kind == _abi.PASS_SAMPLE_COUNT else 4
+        out = np.zeros((height, width, ch), dtype=np.float32)
+        channels = ctypes.c_uint32()
+        _abi.check(self.lib.psy_server_read_pass(self.handle, job, kind, _abi.ptr(out), out.size,
+                                                 ctypes.byref(channels)))
+        return out
+
+    def release(self, job: int) -> None:
+        _abi.check(self.lib.psy_server_release(self.handle, job))
+
+    def cancel(self, job: int) -> None:
+        _abi.check(self.lib.psy_server_cancel(self.handle, job))
+
+    def stats(self) -> _abi.ServerStats:
+        s = _abi.ServerStats()
+        _abi.check(self.lib.psy_server_get_stats(self.handle, ctypes.byref(s)))
+        return s
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.psy_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -31,7 +31,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-prec-div=true",
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-Wextra"]
 
 SOURCES_CU = ["psy_kernels.cu", "psy_static.cu"]
-SOURCES_CPP = ["psy_host.cpp", "psy_light_tree.cpp", "psy_batch.cpp"]
+SOURCES_CPP = ["psy_host.cpp", "psy_light_tree.cpp", "psy_engine.cpp", "psy_batch.cpp", "psy_server.cpp"]
 
 
 def _run(cmd: list[str]) -> None:

@@ -1162,6 +1162,27 @@ psy_status psy_session_read_trace(psy_session *s, psy_path_trace *out) {
 
 }  // extern "C"
 
+uint64_t psy::host::scene_device_bytes(const psy_scene *s) {
+    uint64_t n = 0u;
+    for (const DeviceBuffer *b : {&s->tlas, &s->blas, &s->tris, &s->instances, &s->meshes, &s->positions, &s->normals,
+                                  &s->indices, &s->tri_materials, &s->material_buf, &s->code, &s->scalar_buf,
+                                  &s->vector_buf, &s->emitters, &s->distribution, &s->lights, &s->lamp_bounds,
+                                  &s->lamp_ids, &s->lt_nodes, &s->lt_emitters, &s->lt_mapping, &s->lt_lookup})
+        n += b->bytes;
+    return n;
+}
+
+psy::JobGpu psy::host::session_job(const psy_session *s, const psy::RenderParams &p) {
+    psy::JobGpu j{};
+    j.p = p;
+    j.s = s->scene->view;
+    j.combined = s->combined.as<float4>();
+    j.normal = s->normal.as<float4>();
+    j.albedo = s->albedo.as<float4>();
+    j.sample_count = s->sample_count.as<uint32_t>();
+    return j;
+}
+
 psy_status psy::host::prepare_render(psy_session *s, uint32_t first, uint32_t count, uint32_t offset, uint32_t total,
                                       psy::RenderParams *out) {
     if (!s) return fail(PSY_ERROR_INVALID_ARGUMENT, "null session");

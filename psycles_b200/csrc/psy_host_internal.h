@@ -28,6 +28,12 @@ psy_status fail(psy_status status, const std::string &message);
 psy_status prepare_render(psy_session *s, uint32_t first, uint32_t count, uint32_t offset, uint32_t total,
                           RenderParams *out);
 
+// Device bytes a compiled scene holds (geometry, BVH, materials, lights, tree).
+uint64_t scene_device_bytes(const psy_scene *s);
+
+// The job record of a session for a multi-job wavefront.
+JobGpu session_job(const psy_session *s, const RenderParams &p);
+
 struct DeviceBuffer {
     void *ptr = nullptr;
     size_t bytes = 0;
