@@ -288,15 +288,225 @@ def run_cuda(args) -> None:
                 "d2h_bytes_per_step": d2h, "includes": "compile_scene (upload + BVH build), render, pass readback"},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
+        "tuning": __import__("psycles_b200.autotune", fromlist=["get_tuning"]).get_tuning(backend),
     }
     if kernel:
         line["roofline"] = kernel["roofline"]
         line["kernels"] = kernel["kernels"]
+    if args.serving and args.config == "procedural":
+        line["viewports"] = run_viewports(backend, comp.scene)
+        line["serving"] = run_serving(backend)
     if args.cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, scene)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------ serving
+
+SERVING_SIZES = [(256, 256), (512, 512), (1024, 768), (1920, 1080)]
+
+
+def _random_camera(rng):
+    import math
+    from psycles_b200 import scenes
+    eye = (float(rng.uniform(-14, 14)), float(rng.uniform(2, 10)), float(rng.uniform(12, 24)))
+    target = (float(rng.uniform(-3, 3)), 2.0, float(rng.uniform(-3, 3)))
+    return scenes.Camera(scenes.look_at(eye, target), math.radians(45), math.radians(45), 0)
+
+
+def _parameter_edit(rng, material):
+    """Same-structure edit of a compiled material: random RGB slots and
+    mix factors (a parameter-only rebind)."""
+    import numpy as np
+    sc = material.parameters.scalars.copy()
+    vc = rng.uniform(0.05, 0.95, material.parameters.vectors.shape).astype(np.float32)
+    if sc.size:
+        sc = rng.uniform(0.0, 1.0, sc.shape).astype(np.float32)
+    return sc, vc
+
+
+def serving_workload(seed: int, jobs: int, rate: float):
+    """The serving stream: Poisson arrivals at `rate` jobs/s over 4 resident
+    procedural scenes (8-64 instances, 125k-1M triangles), resolution drawn
+    from {256^2, 512^2, 1024x768, 1920x1080}, spp uniform in 1-64, random
+    camera poses; 30 % of jobs preceded by a parameter-only material edit and
+    5 % by a structural graph edit (a recompiled material)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(jobs):
+        t += float(rng.exponential(1.0 / rate))
+        w, h = SERVING_SIZES[int(rng.integers(0, len(SERVING_SIZES)))]
+        u = float(rng.random())
+        out.append({"arrival": t, "scene": int(rng.integers(0, 4)), "width": w, "height": h,
+                    "spp": int(rng.integers(1, 65)), "camera": _random_camera(rng),
+                    "edit": "structural" if u < 0.05 else ("parameters" if u < 0.35 else None),
+                    "edit_seed": int(rng.integers(0, 1 << 30)), "seed": k})
+    return out
+
+
+def run_serving(backend, jobs: int = 32, rate: float = 200.0, capacity: int = 0) -> dict:
+    """The same job stream through the render server (continuous batching)
+    and through plain one-session-per-job renders; both arms read every pass
+    back.  Latency is arrival -> passes in host memory."""
+    import numpy as np
+    from psycles_b200 import _abi, scenes
+    from psycles_b200.backend import RenderServer, SampleRange
+    from psycles_b200.materials import random_material
+
+    base = [scenes.procedural_scene(seed=k, instances_per_mesh=ipm) for k, ipm in enumerate((1, 2, 4, 8))]
+    stream = serving_workload(7, jobs, rate)
+    passes = (_abi.PASS_COMBINED, _abi.PASS_NORMAL, _abi.PASS_ALBEDO, _abi.PASS_SAMPLE_COUNT)
+    total_samples = sum(j["width"] * j["height"] * j["spp"] for j in stream)
+    structural = {}  # job index -> recompiled scene (built before the clock starts: the same for both arms)
+    for i, j in enumerate(stream):
+        if j["edit"] == "structural":
+            rng = np.random.default_rng(j["edit_seed"])
+            db = scenes.SceneDatabase(base[j["scene"]])
+            m = int(rng.integers(0, len(base[j["scene"]].materials)))
+            structural[i] = db.apply(material_graphs={m: random_material(rng, emission_probability=0.0)})
+
+    def settings(j):
+        return scenes.render_settings(j["width"], j["height"], max_bounces=8, seed=j["seed"])
+
+    def arm(serve: bool) -> dict:
+        compiled = [backend.compile_scene(sc).scene for sc in base]
+        recompiled = {i: backend.compile_scene(sc).scene for i, sc in structural.items()}
+        current = list(compiled)
+        latencies, t_done = [], 0.0
+        server = RenderServer(backend.context, path_capacity=capacity) if serve else None
+        ids = [None] * len(stream)
+        edits = [(i, j) for i, j in enumerate(stream)]
+
+        def apply_edit(i, j):
+            if j["edit"] == "structural":
+                current[j["scene"]] = recompiled[i]
+            elif j["edit"] == "parameters":
+                rng = np.random.default_rng(j["edit_seed"])
+                sc = base[j["scene"]]
+                m = int(rng.integers(0, len(sc.materials)))
+                scal, vec = _parameter_edit(rng, sc.materials[m])
+                if serve:
+                    server.rebind_parameters(current[j["scene"]], m, scal, vec)
+                else:
+                    current[j["scene"]].rebind_parameters(m, scal, vec)
+
+        t0 = time.perf_counter()
+        if serve:
+            def submitter():
+                for i, j in edits:
+                    delay = j["arrival"] - (time.perf_counter() - t0)
+                    if delay > 0:
+                        time.sleep(delay)
+                    apply_edit(i, j)
+                    ids[i] = server.submit(current[j["scene"]], settings(j), j["spp"], camera=j["camera"])
+            th = threading.Thread(target=submitter)
+            th.start()
+            for i, j in enumerate(stream):
+                while ids[i] is None:
+                    time.sleep(0.0005)
+                assert server.wait(ids[i], 600000) == _abi.PSY_OK
+                for k in passes:
+                    server.read_pass(ids[i], k, j["width"], j["height"])
+                server.release(ids[i])
+                now = time.perf_counter() - t0
+                latencies.append((now - j["arrival"]) * 1e3)
+                t_done = now
+            th.join()
+            st = server.stats()
+            extra = {"wavefronts": int(st.wavefronts), "server_p50_ms": st.latency_p50_ms,
+                     "server_p99_ms": st.latency_p99_ms, "bytes_peak": int(st.bytes_peak)}
+            server.close()
+        else:
+            for i, j in edits:
+                delay = j["arrival"] - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                apply_edit(i, j)
+                sess = backend.create_session(current[j["scene"]], settings(j))
+                sess.set_camera(j["camera"])
+                assert sess.render_samples(SampleRange(0, j["spp"], 0, j["spp"])), sess.diagnostics
+                for k in passes:
+                    sess.read_pass(k)
+                sess.close()
+                now = time.perf_counter() - t0
+                latencies.append((now - j["arrival"]) * 1e3)
+                t_done = now
+            extra = {}
+        for c in list(compiled) + list(recompiled.values()):
+            c.close()
+        lat = np.array(latencies)
+        return dict({"samples_per_s": total_samples / t_done, "wall_s": t_done,
+                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}, **extra)
+
+    plain = arm(False)
+    served = arm(True)
+    return {"workload": f"{jobs} jobs, Poisson arrivals at {rate:g}/s over 4 resident procedural scenes "
+                        "(125k-1M triangles); sizes 256^2..1920x1080, spp U[1,64], 8 bounces; 30% parameter "
+                        "edits, 5% structural edits; every pass read back",
+            "samples": total_samples, "path_capacity": capacity, "server": served, "plain": plain,
+            "server_vs_plain": served["samples_per_s"] / plain["samples_per_s"]}
+
+
+def run_viewports(backend, compiled, count: int = 64, capacity: int = 0) -> dict:
+    """64 concurrent viewport renders of the procedural scene from random
+    camera poses (128^2 .. 1920x1080, 1-16 spp): one batched call (shared
+    wavefronts, each replayed as a captured CUDA graph) against the same
+    sessions rendered one after another.  Both arms check out bit-identical."""
+    import numpy as np
+    from psycles_b200 import _abi, scenes
+    from psycles_b200.backend import BatchRenderer, SampleRange
+    rng = np.random.default_rng(11)
+    sizes = [(128, 128), (256, 256), (512, 512), (1024, 768), (1920, 1080)]
+    views = []
+    for _ in range(count):
+        w, h = sizes[int(rng.integers(0, len(sizes)))]
+        views.append((w, h, int(rng.integers(1, 17)), _random_camera(rng)))
+    total = sum(w * h * spp for w, h, spp, _ in views)
+
+    def sessions():
+        out = []
+        for w, h, spp, cam in views:
+            s = backend.create_session(compiled, scenes.render_settings(w, h, max_bounces=8))
+            s.set_camera(cam)
+            out.append((s, spp))
+        return out
+
+    ss = sessions()
+    t0 = time.perf_counter()
+    dev = 0.0
+    for s, spp in ss:
+        assert s.render_samples(SampleRange(0, spp, 0, spp))
+        dev += s.stats().ms_total
+    plain_wall = time.perf_counter() - t0
+    ref = [s.read_pass(_abi.PASS_COMBINED) for s, _ in ss]
+    for s, _ in ss:
+        s.close()
+    batch = BatchRenderer(backend.context, path_capacity=capacity, use_graph=True)
+    warm = sessions()
+    assert batch.render([(s, SampleRange(0, spp, 0, spp)) for s, spp in warm])
+    for s, _ in warm:
+        s.close()
+    bs = sessions()
+    t0 = time.perf_counter()
+    assert batch.render([(s, SampleRange(0, spp, 0, spp)) for s, spp in bs])
+    batch_wall = time.perf_counter() - t0
+    st = batch.stats()
+    same = all(np.array_equal(s.read_pass(_abi.PASS_COMBINED).view(np.uint32), r.view(np.uint32))
+               for (s, _), r in zip(bs, ref))
+    for s, _ in bs:
+        s.close()
+    batch.close()
+    return {"workload": f"{count} viewports of the procedural scene, random poses, 128^2..1920x1080, 1-16 spp",
+            "samples": total, "path_capacity": capacity,
+            "batched": {"samples_per_s": total / batch_wall, "device_samples_per_s": total / (st.ms_total / 1e3),
+                        "wall_s": batch_wall, "wavefronts": int(st.wavefronts), "graph_launches": int(st.graph_launches)},
+            "plain": {"samples_per_s": total / plain_wall, "device_samples_per_s": total / (dev / 1e3),
+                      "wall_s": plain_wall},
+            "batched_vs_plain": plain_wall / batch_wall, "identical": bool(same)}
 
 
 def kernel_profile(args, backend, compiled, settings) -> dict:
@@ -342,6 +552,8 @@ def main() -> None:
     ap.add_argument("--spp", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-kernel-timing", dest="kernel_timing", action="store_false")
+    ap.add_argument("--no-serving", dest="serving", action="store_false",
+                    help="skip the batched-viewport and serving-stream measurements")
     args = ap.parse_args()
     if args.spp is None:
         args.spp = CONFIGS[args.config]["spp"]

@@ -449,6 +449,21 @@ psy_status psy_sobol_generate_table(uint32_t sequence_size, float *out);
  * writes 1024 floats. */
 psy_status psy_pixel_filter_table(uint32_t filter, float width, float *out);
 
+/* Launch and capacity tuning of a context (what psycles_b200.autotune
+ * searches).  No counterpart in the reference, whose dispatch size is
+ * max_samples_per_dispatch.  Zero fields take the defaults. */
+typedef struct psy_tuning {
+    uint32_t path_capacity;            /* paths per session wavefront; 0 = 16 Mi */
+    uint32_t stream_blocks_per_sm;     /* grid cap of grid-stride kernels; 0 = 16 */
+    uint32_t traversal_blocks_per_sm;  /* persistent closest-hit / shadow grid; 0 = 12 */
+    uint32_t shade_blocks_per_sm;      /* shading grid cap; 0 = 32 */
+    uint32_t sort_threshold;           /* sort shading queues of at least this many paths by material;
+                                          0 = never, 0xffffffff = the default 65536 */
+} psy_tuning;
+
+psy_status psy_context_set_tuning(psy_context *context, const psy_tuning *tuning);
+psy_status psy_context_get_tuning(const psy_context *context, psy_tuning *tuning);
+
 /* ------------------------------------------------- batched wavefronts -- */
 /* A batch renders sample ranges of many sessions in shared wavefronts:
  * camera paths of every session fill one path state of `path_capacity`
@@ -459,7 +474,7 @@ psy_status psy_pixel_filter_table(uint32_t filter, float width, float *out);
  * one render_samples gives, bit for bit, because every pixel adds its
  * samples to the film one at a time in sample order. */
 typedef struct psy_batch_config {
-    uint32_t path_capacity;      /* paths per wavefront; 0 = 4 Mi; grown to the largest window */
+    uint32_t path_capacity;      /* paths per wavefront; 0 = the context's (16 Mi); grown to the largest window */
     uint32_t max_jobs;           /* sessions per psy_batch_render call; 0 = 256 */
     uint32_t use_graph;          /* 1: each wavefront replays one captured CUDA graph */
     uint32_t check_interval;     /* without graphs: host check of live paths every N steps (0 = 4) */
@@ -506,7 +521,7 @@ psy_status psy_batch_plan(const uint32_t *pixels, const uint32_t *samples, uint3
  * that context while the server runs except psy_scene_compile. */
 typedef struct psy_server_config {
     uint64_t hbm_budget_bytes;   /* scenes + job films/tables + path state; 0 = 120 GiB */
-    uint32_t path_capacity;      /* paths per wavefront; 0 = 4 Mi */
+    uint32_t path_capacity;      /* paths per wavefront; 0 = the context's (16 Mi) */
     uint32_t max_running;        /* jobs sharing the wavefronts; 0 = 256 */
     uint32_t use_graph;          /* 1: wavefronts replay a captured CUDA graph */
     uint32_t reserved;

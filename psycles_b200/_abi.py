@@ -133,6 +133,11 @@ class KernelProfile(ctypes.Structure):
         ("reserved_bytes", ctypes.c_double)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("path_capacity", "stream_blocks_per_sm", "traversal_blocks_per_sm",
+                                               "shade_blocks_per_sm", "sort_threshold")]
+
+
 class BatchConfig(ctypes.Structure):
     _fields_ = [("path_capacity", ctypes.c_uint32), ("max_jobs", ctypes.c_uint32), ("use_graph", ctypes.c_uint32),
                 ("check_interval", ctypes.c_uint32)]
@@ -200,6 +205,8 @@ SIGNATURES = [
     ("psy_debug_sobol_samples", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_uint32, c_uint32_p, ctypes.c_uint32, c_float_p, c_uint32_p]),
     ("psy_session_set_camera", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("psy_context_set_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
+    ("psy_context_get_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
     ("psy_batch_create", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchConfig), ctypes.POINTER(ctypes.c_void_p)]),
     ("psy_batch_destroy", None, [ctypes.c_void_p]),
     ("psy_batch_render", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), c_uint32_p, c_uint32_p,

@@ -13,7 +13,6 @@ using namespace psy::host;
 
 namespace {
 
-constexpr uint32_t kDefaultBatchCapacity = 1u << 22;
 constexpr uint32_t kDefaultMaxJobs = 256u;
 
 }  // namespace
@@ -33,7 +32,7 @@ psy_status psy_batch_create(psy_context *context, const psy_batch_config *config
     auto b = std::make_unique<psy_batch>();
     b->context = context;
     if (config) b->config = *config;
-    if (b->config.path_capacity == 0u) b->config.path_capacity = kDefaultBatchCapacity;
+    if (b->config.path_capacity == 0u) b->config.path_capacity = context->path_capacity;
     if (b->config.max_jobs == 0u) b->config.max_jobs = kDefaultMaxJobs;
     if (b->config.check_interval == 0u) b->config.check_interval = 4u;
     if (b->config.max_jobs > 65536u) return fail(PSY_ERROR_INVALID_ARGUMENT, "batch: at most 65536 jobs");

@@ -98,7 +98,7 @@ psy_status WavefrontEngine::ensure_plan_room(size_t waves) {
 // last live path find empty queues and return at once.
 uint32_t WavefrontEngine::issue(uint32_t steps, bool allow_exit, psy_status &status) {
     cudaStream_t st = context_->stream;
-    const int sms = context_->sms;
+    const LaunchConfig &lc = context_->launch;
     const JobGpu *jt = jobs_.as<JobGpu>();
     const BatchItem *it = items_.as<BatchItem>();
     const uint32_t *rd = round_.as<uint32_t>();
@@ -107,13 +107,13 @@ uint32_t WavefrontEngine::issue(uint32_t steps, bool allow_exit, psy_status &sta
     status = PSY_OK;
     launch_begin_round(st, b.counters, round_.as<uint32_t>(), items_.as<BatchItem>(), plan_rounds_.as<uint32_t>(),
                        plan_items_.as<BatchItem>(), cursor_.as<uint32_t>(), max_jobs_);
-    launch_raygen_batch(st, sms, jt, it, rd, b, cap);
+    launch_raygen_batch(st, lc, jt, it, rd, b, cap);
     uint32_t launches = 2u;
     for (uint32_t step = 0; step < steps; ++step) {
-        launch_intersect_batch(st, sms, jt, b, cap);
-        launch_shade_batch(st, sms, jt, b, cap, step);
+        launch_intersect_batch(st, lc, jt, b, cap);
+        launch_shade_batch(st, lc, jt, b, cap, step);
         launch_count_rays(st, b.counters, arena_.stats.as<unsigned long long>());
-        launch_shadow_batch(st, sms, jt, b, cap, step);
+        launch_shadow_batch(st, lc, jt, b, cap, step);
         launch_swap(st, b.counters);
         std::swap(b.queue_in, b.queue_out);
         launches += 5u;
@@ -127,7 +127,7 @@ uint32_t WavefrontEngine::issue(uint32_t steps, bool allow_exit, psy_status &sta
             if (left == 0u) break;
         }
     }
-    launch_film_batch(st, sms, jt, it, rd, b, cap);
+    launch_film_batch(st, lc, jt, it, rd, b, cap);
     return launches + 1u;
 }
 

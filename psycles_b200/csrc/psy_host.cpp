@@ -64,6 +64,12 @@ psy_status PathArena::ensure(uint32_t n, bool with_job) {
     PSY_CUDA_TRY(qb.alloc(u1));
     PSY_CUDA_TRY(sq.alloc(u1));
     if (with_job) PSY_CUDA_TRY(job.alloc(u1));
+    PSY_CUDA_TRY(sort_keys.alloc(u1));
+    PSY_CUDA_TRY(queue_sorted.alloc(u1));
+    if (!sort_hist.ptr) {
+        PSY_CUDA_TRY(sort_hist.alloc(2u * psy::kSortBuckets * sizeof(uint32_t)));
+        PSY_CUDA_TRY(cudaMemset(sort_hist.ptr, 0, 2u * psy::kSortBuckets * sizeof(uint32_t)));
+    }
     if (!counters.ptr) PSY_CUDA_TRY(counters.alloc(64));
     if (!stats.ptr) PSY_CUDA_TRY(stats.alloc(64));
     capacity = c;
@@ -90,11 +96,15 @@ psy_status PathArena::ensure(uint32_t n, bool with_job) {
     b.shadow_queue = sq.as<uint32_t>();
     b.counters = counters.as<uint32_t>();
     b.job = job.ptr ? job.as<uint32_t>() : nullptr;
+    b.sort_keys = sort_keys.as<uint32_t>();
+    b.queue_sorted = queue_sorted.as<uint32_t>();
+    b.sort_hist = sort_hist.as<uint32_t>();
+    b.sort_offsets = b.sort_hist + psy::kSortBuckets;
     return PSY_OK;
 }
 
 size_t PathArena::bytes_per_path(bool with_job) {
-    return 10u * sizeof(float4) + 4u * sizeof(uint4) + (7u + (with_job ? 1u : 0u)) * sizeof(uint32_t);
+    return 10u * sizeof(float4) + 4u * sizeof(uint4) + (9u + (with_job ? 1u : 0u)) * sizeof(uint32_t);
 }
 
 }  // namespace psy::host
@@ -517,7 +527,6 @@ psy_status clear_film(psy_session *s) {
     return PSY_OK;
 }
 
-constexpr uint32_t kDefaultCapacity = 1u << 22;  // 4M paths = 408 MB of state
 
 // Emission estimate of a closure program for the light tree
 // (estimate_surface_emission, src/compiler/surface_program.cpp:244-330): one
@@ -608,8 +617,34 @@ psy_status psy_context_create(int device, psy_context **out) {
     auto c = std::make_unique<psy_context>();
     c->device = device;
     c->sms = prop.multiProcessorCount;
+    c->launch.sms = c->sms;
     PSY_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     *out = c.release();
+    return PSY_OK;
+}
+
+psy_status psy_context_set_tuning(psy_context *c, const psy_tuning *t) {
+    if (!c || !t) return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    if (t->stream_blocks_per_sm > 64u || t->traversal_blocks_per_sm > 64u || t->shade_blocks_per_sm > 64u)
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "at most 64 blocks per SM");
+    if (t->path_capacity > (1u << 26)) return fail(PSY_ERROR_INVALID_ARGUMENT, "path capacity above 64 Mi");
+    const psy::LaunchConfig defaults;
+    c->path_capacity = t->path_capacity ? t->path_capacity : (1u << 24);
+    c->launch.stream_blocks_per_sm = t->stream_blocks_per_sm ? t->stream_blocks_per_sm : defaults.stream_blocks_per_sm;
+    c->launch.traversal_blocks_per_sm =
+        t->traversal_blocks_per_sm ? t->traversal_blocks_per_sm : defaults.traversal_blocks_per_sm;
+    c->launch.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : defaults.shade_blocks_per_sm;
+    c->launch.sort_threshold = t->sort_threshold == 0xffffffffu ? defaults.sort_threshold : t->sort_threshold;
+    return PSY_OK;
+}
+
+psy_status psy_context_get_tuning(const psy_context *c, psy_tuning *t) {
+    if (!c || !t) return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    t->path_capacity = c->path_capacity;
+    t->stream_blocks_per_sm = c->launch.stream_blocks_per_sm;
+    t->traversal_blocks_per_sm = c->launch.traversal_blocks_per_sm;
+    t->shade_blocks_per_sm = c->launch.shade_blocks_per_sm;
+    t->sort_threshold = c->launch.sort_threshold;
     return PSY_OK;
 }
 
@@ -1218,14 +1253,14 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
     psy_context *ctx = s->scene->context;
     cudaStream_t st = ctx->stream;
     const uint32_t pixels = s->pixels;
-    uint32_t per_batch = std::max(1u, std::min(count, kDefaultCapacity / std::max(pixels, 1u)));
+    uint32_t per_batch = std::max(1u, std::min(count, ctx->path_capacity / std::max(pixels, 1u)));
     psy_status r = ensure_capacity(s, pixels * per_batch);
     if (r != PSY_OK) return r;
     psy_path_trace *trace = s->trace_requested ? s->trace_buf.as<psy_path_trace>() : nullptr;
     PSY_CUDA_TRY(cudaMemsetAsync(s->arena.stats.ptr, 0, 64, st));
     psy_render_stats stats{};
     PSY_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
-    const int sms = ctx->sms;
+    const psy::LaunchConfig &lc = ctx->launch;
     const bool prof = s->profiling;
     if (prof) std::memset(&s->profile, 0, sizeof(s->profile));
     // Times one launch class when profiling: events on both sides, then a
@@ -1266,7 +1301,7 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
         psy_path_trace *tr = trace_path != psy::kInvalidId ? trace : nullptr;
         psy::PathBuffers b = s->arena.view;
         psy::launch_set_counters(st, b.counters, paths);
-        if ((ps = timed([&] { psy::launch_raygen(st, sms, p, b, pixels, paths, uint32_t(sample), trace_path, tr); },
+        if ((ps = timed([&] { psy::launch_raygen(st, lc, p, b, pixels, paths, uint32_t(sample), trace_path, tr); },
                         pf.raygen_launches, pf.raygen_ms)) != PSY_OK)
             return ps;
         pf.raygen_bytes += 164.0 * paths;
@@ -1274,17 +1309,17 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
         for (uint32_t step = 0; step < p.steps; ++step) {
             uint32_t c3[3] = {0u, 0u, 0u};
             if (prof && (ps = read_counters(c3)) != PSY_OK) return ps;
-            if ((ps = timed([&] { psy::launch_intersect(st, sms, s->scene->view, b, paths); }, pf.intersect_launches,
+            if ((ps = timed([&] { psy::launch_intersect(st, lc, s->scene->view, b, paths); }, pf.intersect_launches,
                             pf.intersect_ms)) != PSY_OK)
                 return ps;
             pf.intersect_bytes += 88.0 * c3[0];
-            if ((ps = timed([&] { psy::launch_shade(st, sms, s->scene->view, p, b, paths, step, trace_path, tr); },
+            if ((ps = timed([&] { psy::launch_shade(st, lc, s->scene->view, p, b, paths, step, trace_path, tr); },
                             pf.shade_launches, pf.shade_ms)) != PSY_OK)
                 return ps;
             psy::launch_count_rays(st, b.counters, s->arena.stats.as<unsigned long long>());
             if (prof && (ps = read_counters(c3)) != PSY_OK) return ps;
             pf.shade_bytes += 304.0 * c3[0] + 68.0 * c3[2];
-            if ((ps = timed([&] { psy::launch_shadow(st, sms, s->scene->view, p, b, paths, step, trace_path, tr); },
+            if ((ps = timed([&] { psy::launch_shadow(st, lc, s->scene->view, p, b, paths, step, trace_path, tr); },
                             pf.shadow_launches, pf.shadow_ms)) != PSY_OK)
                 return ps;
             pf.shadow_bytes += 100.0 * c3[2];
@@ -1300,7 +1335,7 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
             }
         }
         if ((ps = timed([&] {
-                 psy::launch_film(st, sms, b, pixels, n_samples, s->combined.as<float4>(), s->normal.as<float4>(),
+                 psy::launch_film(st, lc, b, pixels, n_samples, s->combined.as<float4>(), s->normal.as<float4>(),
                                   s->albedo.as<float4>(), s->sample_count.as<uint32_t>(), trace_path, tr);
              }, pf.film_launches, pf.film_ms)) != PSY_OK)
             return ps;
@@ -1401,7 +1436,9 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
     s->total = total;
     const uint32_t pixels = s->pixels;
     const uint32_t per_batch = std::max(1u, std::min(count, psy::kStaticMaxPaths / std::max(pixels, 1u)));
-    const int sms = ctx->sms;
+    // the static path state has no sort buffers
+    psy::LaunchConfig lc = ctx->launch;
+    lc.sort_threshold = 0u;
     psy_render_stats stats{};
     PSY_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
     for (uint64_t sample = begin; sample < end;) {
@@ -1410,13 +1447,13 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
         const uint32_t paths = pixels * n_samples;
         psy::PathBuffers bb = b;
         psy::launch_set_counters(st, bb.counters, paths);
-        psy::launch_raygen(st, sms, p, bb, pixels, paths, uint32_t(sample), psy::kInvalidId, nullptr);
+        psy::launch_raygen(st, lc, p, bb, pixels, paths, uint32_t(sample), psy::kInvalidId, nullptr);
         stats.camera_rays += paths;
         for (uint32_t step = 0; step < p.steps; ++step) {
-            psy::launch_intersect(st, sms, s->scene->view, bb, paths);
-            psy::launch_shade(st, sms, s->scene->view, p, bb, paths, step, psy::kInvalidId, nullptr);
+            psy::launch_intersect(st, lc, s->scene->view, bb, paths);
+            psy::launch_shade(st, lc, s->scene->view, p, bb, paths, step, psy::kInvalidId, nullptr);
             psy::launch_count_rays(st, bb.counters, ray_stats);
-            psy::launch_shadow(st, sms, s->scene->view, p, bb, paths, step, psy::kInvalidId, nullptr);
+            psy::launch_shadow(st, lc, s->scene->view, p, bb, paths, step, psy::kInvalidId, nullptr);
             psy::launch_swap(st, bb.counters);
             std::swap(bb.queue_in, bb.queue_out);
             stats.kernel_launches += 5u;
@@ -1427,7 +1464,7 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
                 if (left == 0u) break;
             }
         }
-        psy::launch_film(st, sms, bb, pixels, n_samples, s->combined.as<float4>(), s->normal.as<float4>(),
+        psy::launch_film(st, lc, bb, pixels, n_samples, s->combined.as<float4>(), s->normal.as<float4>(),
                          s->albedo.as<float4>(), s->sample_count.as<uint32_t>(), psy::kInvalidId, nullptr);
         stats.kernel_launches += 3u;
         stats.batches += 1u;

@@ -4,6 +4,7 @@
 #pragma once
 
 #include "../../include/psycles_cuda.h"
+#include "psy_kernels.h"
 #include "psy_scene.h"
 
 #include <cuda_runtime.h>
@@ -69,7 +70,7 @@ struct DeviceBuffer {
 struct PathArena {
     uint32_t capacity = 0;
     DeviceBuffer ray_o, ray_d, tp, rad, st, st2, sample, aov_n, aov_a, mis_n, hit, hit_prim, sh_o, sh_d, sh_c, sh_ids,
-        sh_path, qa, qb, sq, job, counters, stats;
+        sh_path, qa, qb, sq, job, sort_keys, queue_sorted, sort_hist, counters, stats;
     PathBuffers view{};
     psy_status ensure(uint32_t n, bool with_job);
     static size_t bytes_per_path(bool with_job);
@@ -89,6 +90,8 @@ struct psy_context {
     int device = 0;
     int sms = 148;
     cudaStream_t stream = nullptr;
+    psy::LaunchConfig launch;      // psy_context_set_tuning
+    uint32_t path_capacity = 1u << 24;  // 16 Mi paths, about 3.9 GB of path state
 };
 
 struct psy_scene {

@@ -331,6 +331,77 @@ __device__ __forceinline__ float next_float_up(float t) {
     return t == 0.0f ? 1.17549435e-38f : __uint_as_float(__float_as_uint(t) + 1u);
 }
 
+// ------------------------------------------------------ sort by material
+__device__ __forceinline__ uint32_t surface_material(const SceneView &s, uint32_t instance, uint32_t local);
+
+// Queues of at least `threshold` paths are grouped by material before
+// shading, so a warp mostly runs one closure program: a bucket per queue
+// entry (misses in bucket 0, hits by material and job hashed into the other
+// buckets), a histogram, its exclusive scan and a scatter.  Order inside a
+// bucket is arbitrary; no path's result depends on the queue order.
+template <bool kMulti>
+__global__ void k_sort_count(const __grid_constant__ SceneView s_arg, const __grid_constant__ PathBuffers b,
+                             const JobGpu *jobs, uint32_t threshold) {
+    __shared__ uint32_t local[kSortBuckets];
+    const uint32_t count = b.counters[0];
+    if (count < threshold) return;
+    for (uint32_t k = threadIdx.x; k < kSortBuckets; k += blockDim.x) local[k] = 0u;
+    __syncthreads();
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+        const uint32_t i = b.queue_in[q];
+        const uint32_t prim = b.hit_prim[i];
+        uint32_t key = 0u;
+        if (prim != kInvalid) {
+            const uint32_t job = kMulti ? b.job[i] : 0u;
+            const SceneView &s = kMulti ? jobs[job].s : s_arg;
+            const uint32_t mat = surface_material(s, __float_as_uint(b.hit[i].w), prim);
+            key = 1u + (mat + job * 977u) % (kSortBuckets - 1u);
+        }
+        b.sort_keys[q] = key;
+        atomicAdd(&local[key], 1u);
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < kSortBuckets; k += blockDim.x)
+        if (local[k]) atomicAdd(&b.sort_hist[k], local[k]);
+}
+
+// One block of 1024 threads: offsets = exclusive scan of the histogram,
+// which is cleared for the next sort.
+__global__ void k_sort_scan(const __grid_constant__ PathBuffers b, uint32_t threshold) {
+    __shared__ uint32_t part[1024];
+    if (b.counters[0] < threshold) return;
+    constexpr uint32_t kPer = kSortBuckets / 1024u;
+    const uint32_t t = threadIdx.x;
+    uint32_t v[kPer], sum = 0u;
+    for (uint32_t k = 0; k < kPer; ++k) {
+        v[k] = b.sort_hist[t * kPer + k];
+        sum += v[k];
+    }
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t d = 1u; d < 1024u; d <<= 1) {  // inclusive Hillis-Steele scan
+        const uint32_t add = t >= d ? part[t - d] : 0u;
+        __syncthreads();
+        part[t] += add;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - sum;
+    for (uint32_t k = 0; k < kPer; ++k) {
+        b.sort_offsets[t * kPer + k] = run;
+        run += v[k];
+        b.sort_hist[t * kPer + k] = 0u;
+    }
+}
+
+__global__ void k_sort_scatter(const __grid_constant__ PathBuffers b, uint32_t threshold) {
+    const uint32_t count = b.counters[0];
+    if (count < threshold) return;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+        const uint32_t pos = atomicAdd(&b.sort_offsets[b.sort_keys[q]], 1u);
+        b.queue_sorted[pos] = b.queue_in[q];
+    }
+}
+
 // kTrace selects the variant that records the per-path trace; the render
 // variant carries no trace code.
 // kMulti: paths of a batched wavefront, each shaded with its job's scene and
@@ -339,8 +410,9 @@ template <bool kTrace, bool kMulti>
 __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
     k_shade(const __grid_constant__ SceneView s_arg, const __grid_constant__ RenderParams p_arg,
             const __grid_constant__ PathBuffers b, uint32_t step, uint32_t trace_path, psy_path_trace *trace,
-            const JobGpu *jobs) {
+            const JobGpu *jobs, uint32_t sort_threshold) {
     const uint32_t count = b.counters[0];
+    const uint32_t *queue = (sort_threshold != 0u && count >= sort_threshold) ? b.queue_sorted : b.queue_in;
     const uint32_t rounds = (count + gridDim.x * blockDim.x - 1u) / (gridDim.x * blockDim.x);
     // Every lane runs the same number of rounds so the warp-aggregated queue
     // pushes see the whole warp.
@@ -353,7 +425,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
         float4 sh_o, sh_d, sh_c;
         uint4 sh_ids;
         if (active) {
-            i = b.queue_in[q];
+            i = queue[q];
             const uint32_t job = kMulti ? b.job[i] : 0u;
             const SceneView &s = kMulti ? jobs[job].s : s_arg;
             const RenderParams &p = kMulti ? jobs[job].p : p_arg;
@@ -1064,38 +1136,53 @@ __global__ void k_debug_light_tree(const __grid_constant__ SceneView s, const fl
 
 // ----------------------------------------------------------------- launches
 
-int launch_grid(uint32_t work, int block, int sms) {
+int launch_grid(uint32_t work, int block, const LaunchConfig &lc) {
     const uint32_t blocks = (work + uint32_t(block) - 1u) / uint32_t(block);
-    const uint32_t cap = uint32_t(sms) * 16u;
+    const uint32_t cap = uint32_t(lc.sms) * lc.stream_blocks_per_sm;
     return int(blocks < 1u ? 1u : (blocks > cap ? cap : blocks));
 }
 
-void launch_raygen(cudaStream_t st, int sms, const RenderParams &p, const PathBuffers &b, uint32_t pixels,
+void launch_raygen(cudaStream_t st, const LaunchConfig &lc, const RenderParams &p, const PathBuffers &b, uint32_t pixels,
                    uint32_t paths, uint32_t sample_base, uint32_t trace_path, psy_path_trace *trace) {
-    k_raygen<<<launch_grid(paths, 256, sms), 256, 0, st>>>(p, b, pixels, paths, sample_base, trace_path, trace);
+    k_raygen<<<launch_grid(paths, 256, lc), 256, 0, st>>>(p, b, pixels, paths, sample_base, trace_path, trace);
 }
 void launch_set_counters(cudaStream_t st, uint32_t *counters, uint32_t n) { k_set_counters<<<1, 1, 0, st>>>(counters, n); }
 // Persistent kernels: enough resident warps to fill every SM (bounded by the
 // work so small queues launch few blocks).
-int persistent_grid(uint32_t work, int sms) {
+int shade_grid(uint32_t work, const LaunchConfig &lc) {
     const uint32_t blocks = (work + 127u) / 128u;
-    const uint32_t cap = uint32_t(sms) * 12u;
+    const uint32_t cap = uint32_t(lc.sms) * lc.shade_blocks_per_sm;
+    return int(blocks < 1u ? 1u : (blocks > cap ? cap : blocks));
+}
+template <bool kMulti>
+void launch_sort(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const PathBuffers &b, const JobGpu *jobs,
+                 uint32_t max_work) {
+    k_sort_count<kMulti><<<launch_grid(max_work, 256, lc), 256, 0, st>>>(s, b, jobs, lc.sort_threshold);
+    k_sort_scan<<<1, 1024, 0, st>>>(b, lc.sort_threshold);
+    k_sort_scatter<<<launch_grid(max_work, 256, lc), 256, 0, st>>>(b, lc.sort_threshold);
+}
+int persistent_grid(uint32_t work, const LaunchConfig &lc) {
+    const uint32_t blocks = (work + 127u) / 128u;
+    const uint32_t cap = uint32_t(lc.sms) * lc.traversal_blocks_per_sm;
     return int(blocks < 1u ? 1u : (blocks > cap ? cap : blocks));
 }
 
-void launch_intersect(cudaStream_t st, int sms, const SceneView &s, const PathBuffers &b, uint32_t max_work) {
-    k_intersect<false><<<persistent_grid(max_work, sms), 128, 0, st>>>(s, b, nullptr);
+void launch_intersect(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const PathBuffers &b, uint32_t max_work) {
+    k_intersect<false><<<persistent_grid(max_work, lc), 128, 0, st>>>(s, b, nullptr);
 }
-void launch_shade(cudaStream_t st, int sms, const SceneView &s, const RenderParams &p, const PathBuffers &b,
+void launch_shade(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                   uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
+    if (lc.sort_threshold) launch_sort<false>(st, lc, s, b, nullptr, max_work);
     if (trace)
-        k_shade<true, false><<<launch_grid(max_work, 128, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr);
+        k_shade<true, false><<<shade_grid(max_work, lc), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr,
+                                                                     lc.sort_threshold);
     else
-        k_shade<false, false><<<launch_grid(max_work, 128, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr);
+        k_shade<false, false><<<shade_grid(max_work, lc), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr,
+                                                                      lc.sort_threshold);
 }
-void launch_shadow(cudaStream_t st, int sms, const SceneView &s, const RenderParams &p, const PathBuffers &b,
+void launch_shadow(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                    uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
-    k_shadow<false><<<persistent_grid(max_work, sms), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr);
+    k_shadow<false><<<persistent_grid(max_work, lc), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr);
 }
 void launch_begin_round(cudaStream_t st, uint32_t *counters, uint32_t *round, BatchItem *items,
                         const uint32_t *plan_rounds, const BatchItem *plan_items, uint32_t *cursor, uint32_t max_items) {
@@ -1105,32 +1192,33 @@ void launch_swap(cudaStream_t st, uint32_t *counters) { k_swap_counters<<<1, 1, 
 void launch_count_rays(cudaStream_t st, const uint32_t *counters, unsigned long long *stats) {
     k_count_rays<<<1, 1, 0, st>>>(counters, stats);
 }
-void launch_film(cudaStream_t st, int sms, const PathBuffers &b, uint32_t pixels, uint32_t samples, float4 *combined,
+void launch_film(cudaStream_t st, const LaunchConfig &lc, const PathBuffers &b, uint32_t pixels, uint32_t samples, float4 *combined,
                  float4 *normal, float4 *albedo, uint32_t *sample_count, uint32_t trace_path, psy_path_trace *trace) {
-    k_film<<<launch_grid(pixels, 256, sms), 256, 0, st>>>(b, pixels, samples, combined, normal, albedo, sample_count,
+    k_film<<<launch_grid(pixels, 256, lc), 256, 0, st>>>(b, pixels, samples, combined, normal, albedo, sample_count,
                                                         trace_path, trace);
 }
 // Batched wavefront: every kernel reads each path's job record.
-void launch_raygen_batch(cudaStream_t st, int sms, const JobGpu *jobs, const BatchItem *items, const uint32_t *round,
+void launch_raygen_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const BatchItem *items, const uint32_t *round,
                          const PathBuffers &b, uint32_t max_paths) {
-    k_raygen_batch<<<launch_grid(max_paths, 256, sms), 256, 0, st>>>(jobs, items, round, b);
+    k_raygen_batch<<<launch_grid(max_paths, 256, lc), 256, 0, st>>>(jobs, items, round, b);
 }
-void launch_intersect_batch(cudaStream_t st, int sms, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work) {
-    k_intersect<true><<<persistent_grid(max_work, sms), 128, 0, st>>>(SceneView{}, b, jobs);
+void launch_intersect_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work) {
+    k_intersect<true><<<persistent_grid(max_work, lc), 128, 0, st>>>(SceneView{}, b, jobs);
 }
-void launch_shade_batch(cudaStream_t st, int sms, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work,
+void launch_shade_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work,
                         uint32_t step) {
-    k_shade<false, true><<<launch_grid(max_work, 128, sms), 128, 0, st>>>(SceneView{}, RenderParams{}, b, step,
-                                                                           kInvalid, nullptr, jobs);
+    if (lc.sort_threshold) launch_sort<true>(st, lc, SceneView{}, b, jobs, max_work);
+    k_shade<false, true><<<shade_grid(max_work, lc), 128, 0, st>>>(SceneView{}, RenderParams{}, b, step, kInvalid,
+                                                                 nullptr, jobs, lc.sort_threshold);
 }
-void launch_shadow_batch(cudaStream_t st, int sms, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work,
+void launch_shadow_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work,
                          uint32_t step) {
-    k_shadow<true><<<persistent_grid(max_work, sms), 128, 0, st>>>(SceneView{}, RenderParams{}, b, step, kInvalid,
+    k_shadow<true><<<persistent_grid(max_work, lc), 128, 0, st>>>(SceneView{}, RenderParams{}, b, step, kInvalid,
                                                                     nullptr, jobs);
 }
-void launch_film_batch(cudaStream_t st, int sms, const JobGpu *jobs, const BatchItem *items, const uint32_t *round,
+void launch_film_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const BatchItem *items, const uint32_t *round,
                        const PathBuffers &b, uint32_t max_pixels) {
-    k_film_batch<<<launch_grid(max_pixels, 256, sms), 256, 0, st>>>(jobs, items, round, b);
+    k_film_batch<<<launch_grid(max_pixels, 256, lc), 256, 0, st>>>(jobs, items, round, b);
 }
 
 void launch_debug_light_tree(cudaStream_t st, const SceneView &s, const float4 *queries, const uint32_t *pdf_emitters,

@@ -150,7 +150,12 @@ struct PathBuffers {
     uint32_t *shadow_queue;
     uint32_t *counters;  // [0] in count, [1] out count, [2] shadow count, [3..] stats
     uint32_t *job;       // batched wavefronts: the job of each path
+    // shading-queue sort by material: per-queue-entry bucket, the sorted
+    // queue, and kSortBuckets-word histogram / offset arrays
+    uint32_t *sort_keys, *queue_sorted, *sort_hist, *sort_offsets;
 };
+
+constexpr uint32_t kSortBuckets = 2048u;
 
 // One job of a batched wavefront: a session's render parameters, its scene
 // and its film.  Paths of many jobs share the path state; each path reads

@@ -32,7 +32,6 @@ using namespace psy::host;
 namespace {
 
 constexpr uint64_t kDefaultBudget = 120ull << 30;
-constexpr uint32_t kDefaultCapacity = 1u << 22;
 constexpr uint32_t kDefaultRunning = 256u;
 
 struct Job {
@@ -317,7 +316,7 @@ psy_status psy_server_create(psy_context *context, const psy_server_config *conf
     sv->context = context;
     if (config) sv->config = *config;
     if (sv->config.hbm_budget_bytes == 0u) sv->config.hbm_budget_bytes = kDefaultBudget;
-    if (sv->config.path_capacity == 0u) sv->config.path_capacity = kDefaultCapacity;
+    if (sv->config.path_capacity == 0u) sv->config.path_capacity = context->path_capacity;
     if (sv->config.max_running == 0u) sv->config.max_running = kDefaultRunning;
     if (sv->config.max_running > 65536u) return fail(PSY_ERROR_INVALID_ARGUMENT, "server: at most 65536 running jobs");
     const psy_status r = sv->engine.init(context, sv->config.path_capacity, sv->config.max_running,
