@@ -186,9 +186,8 @@ def scene_bytes(scene) -> int:
 
 
 def run_cuda(args) -> None:
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from psycles_b200 import dist as pdist
+    rank, world, local = pdist.rank_env()
     dist = None
     if world > 1:
         import torch
@@ -202,8 +201,8 @@ def run_cuda(args) -> None:
     c = CONFIGS[args.config]
     scene = make_scene(args.config)
     backend = CudaPathTracerBackend(local)
-    settings = lambda: scenes.render_settings(c["width"], c["height"], max_bounces=c["bounces"], seed=rank,
-                                              use_light_tree=c.get("light_tree", 0))
+    settings = lambda: scenes.render_settings(c["width"], c["height"], max_bounces=c["bounces"],
+                                              seed=pdist.frame_seed(rank), use_light_tree=c.get("light_tree", 0))
     comp = backend.compile_scene(scene)
     if not comp.ok():
         raise SystemExit(f"compile_scene failed: {comp.diagnostics}")
@@ -223,12 +222,7 @@ def run_cuda(args) -> None:
             dist.barrier()
 
     def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        import torch
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return pdist.max_over_ranks(v, device=f"cuda:{local}")
 
     for _ in range(args.warmup):
         step()

@@ -6,9 +6,10 @@
 // A loop thread admits jobs from its head while the HBM budget and the job
 // slots allow: a job gets a session (film, Sobol and filter tables) and a
 // slot of the wavefront engine's job table.  Every wavefront takes samples
-// from all running jobs (continuous batching: a job admitted while others
-// are on the GPU joins the next wavefront), so small and large jobs share
-// the device.  Two wavefronts are in flight: the host plans and admits for
+// from the running jobs in admission order -- the oldest job takes all the
+// samples that fit and younger jobs backfill the rest (continuous batching:
+// a job admitted while others are on the GPU joins the next wavefront), so
+// small jobs share the device with large ones without delaying them.  Two wavefronts are in flight: the host plans and admits for
 // the next while the GPU runs the current one.  A job is done once the
 // wavefront holding its last samples has finished.  Because every pixel
 // adds its samples in order, a job's passes are the same alone and in any
@@ -189,7 +190,6 @@ struct psy_server {
         cudaSetDevice(context->device);
         for (auto &f : flight) cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming);
         uint64_t wave_counter = 0, finished_wave = 0;
-        uint32_t rr = 0;
         double busy_since = -1.0;
         for (;;) {
             {
@@ -227,7 +227,8 @@ struct psy_server {
             if (!plan.empty()) {
                 std::vector<psy::BatchItem> items;
                 uint32_t film = 0u;
-                const uint32_t paths = plan_wavefront(plan, rr++ % uint32_t(plan.size()), engine.capacity(), items, film);
+                // oldest job first, the others backfill the capacity it leaves
+                const uint32_t paths = plan_wavefront(plan, 0u, engine.capacity(), items, film);
                 EnginePlan ep;
                 ep.add(items, paths, film, engine.max_jobs());
                 EngineRun run;
