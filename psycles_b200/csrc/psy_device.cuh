@@ -487,6 +487,41 @@ __device__ __forceinline__ BvhNodeGpu load_node(const BvhNodeGpu *nodes, int idx
     return n;
 }
 
+// Slab test of the four children of a wide node, with the conservative
+// bounds of the binary test; empty slots never hit.
+__device__ __forceinline__ void wide_slabs(const WideNodeGpu &n, f3 oinv, f3 inv, float tmin, float tmax,
+                                           float near[4], bool hit[4]) {
+    const float lx[4] = {n.lox.x, n.lox.y, n.lox.z, n.lox.w}, hx[4] = {n.hix.x, n.hix.y, n.hix.z, n.hix.w};
+    const float ly[4] = {n.loy.x, n.loy.y, n.loy.z, n.loy.w}, hy[4] = {n.hiy.x, n.hiy.y, n.hiy.z, n.hiy.w};
+    const float lz[4] = {n.loz.x, n.loz.y, n.loz.z, n.loz.w}, hz[4] = {n.hiz.x, n.hiz.y, n.hiz.z, n.hiz.w};
+    const int lk[4] = {n.link.x, n.link.y, n.link.z, n.link.w}, ct[4] = {n.count.x, n.count.y, n.count.z, n.count.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float x0 = fmaf(lx[k], inv.x, -oinv.x), x1 = fmaf(hx[k], inv.x, -oinv.x);
+        const float y0 = fmaf(ly[k], inv.y, -oinv.y), y1 = fmaf(hy[k], inv.y, -oinv.y);
+        const float z0 = fmaf(lz[k], inv.z, -oinv.z), z1 = fmaf(hz[k], inv.z, -oinv.z);
+        const float nr = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+        const float fr = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
+        near[k] = nr;
+        hit[k] = (nr <= fr * 1.00000095367431640625f + 1.0e-30f || nr <= fr) && (lk[k] >= 0 || ct[k] > 0);
+    }
+}
+
+__device__ __forceinline__ WideNodeGpu load_wide_node(const WideNodeGpu *nodes, uint32_t idx) {
+    const float4 *p = reinterpret_cast<const float4 *>(nodes + idx);
+    WideNodeGpu n;
+    n.lox = __ldg(p + 0);
+    n.hix = __ldg(p + 1);
+    n.loy = __ldg(p + 2);
+    n.hiy = __ldg(p + 3);
+    n.loz = __ldg(p + 4);
+    n.hiz = __ldg(p + 5);
+    const int4 *q = reinterpret_cast<const int4 *>(p + 6);
+    n.link = __ldg(q);
+    n.count = __ldg(q + 1);
+    return n;
+}
+
 constexpr int kStackSize = 48;
 
 // Stack entries carry a 2-bit tag: a TLAS node, a BLAS node (global index),
@@ -576,49 +611,69 @@ __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneVi
             continue;
         }
         const bool blas = tag == kTagBlas;
-        const BvhNodeGpu n = load_node(blas ? s.blas : s.tlas, int(idx));
-        float ln, rn;
-        bool lh, rh;
-        node_slabs(n, t.cur.oinv, t.cur.inv, t.ray.tmin, t.tmax, ln, rn, lh, rh);
-        uint32_t next[2];
-        int nc = 0;
-        const bool right_first = rn < ln;
+        const WideNodeGpu n = load_wide_node(blas ? s.blas : s.tlas, idx);
+        float near[4];
+        bool hit[4];
+        wide_slabs(n, t.cur.oinv, t.cur.inv, t.ray.tmin, t.tmax, near, hit);
+        const int lk[4] = {n.link.x, n.link.y, n.link.z, n.link.w}, ct[4] = {n.count.x, n.count.y, n.count.z, n.count.w};
+        // leaves first: their triangles may shrink tmax before the inner
+        // children are ordered
+        if (blas) {
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int side = (k == 0) == right_first ? 1 : 0;
-            if (!(side == 0 ? lh : rh)) continue;
-            const int link = side == 0 ? n.child.x : n.child.y;
-            const int count = side == 0 ? n.child.z : n.child.w;
-            if (link >= 0) {
-                next[nc++] = blas ? (kTagBlas | (t.blas_base + uint32_t(link))) : uint32_t(link);
-                continue;
-            }
-            if (!blas) {
-                if (count > 0) next[nc++] = kTagInstance | uint32_t(~link);
-                continue;
-            }
-            const uint32_t first = t.tri_base + uint32_t(~link);
-            for (int q = 0; q < count; ++q) {
-                const float4 *tp = s.tris + 3u * (first + uint32_t(q));
-                const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-                const uint32_t local = __float_as_uint(a.w);
-                const uint32_t cp = t.prim_offset + local;
-                if ((t.src_obj == t.inst && t.src_prim == cp) || (t.light_obj == t.inst && t.light_prim == cp)) continue;
-                float th, u, v;
-                if (!intersect_triangle(t.cur.o, t.cur.d, t.ray.tmin, t.tmax, ld3(a), ld3(b), ld3(c), th, u, v))
-                    continue;
-                if (on_hit(t.inst, local, cp, th, u, v)) return true;
+            for (int k = 0; k < 4; ++k) {
+                if (!hit[k] || lk[k] >= 0) continue;
+                const uint32_t first = t.tri_base + uint32_t(~lk[k]);
+                for (int q = 0; q < ct[k]; ++q) {
+                    const float4 *tp = s.tris + 3u * (first + uint32_t(q));
+                    const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                    const uint32_t local = __float_as_uint(a.w);
+                    const uint32_t cp = t.prim_offset + local;
+                    if ((t.src_obj == t.inst && t.src_prim == cp) || (t.light_obj == t.inst && t.light_prim == cp))
+                        continue;
+                    float th, u, v;
+                    if (!intersect_triangle(t.cur.o, t.cur.d, t.ray.tmin, t.tmax, ld3(a), ld3(b), ld3(c), th, u, v))
+                        continue;
+                    if (on_hit(t.inst, local, cp, th, u, v)) return true;
+                }
             }
         }
-        if (nc == 2) {
-            if (t.sp < uint32_t(kStackSize)) t.stack[t.sp++] = next[1];
-            t.node = next[0];
-        } else if (nc == 1) {
-            t.node = next[0];
-        } else {
+        // inner children (and TLAS instances) nearest first: sort the four
+        // (distance, entry) pairs, misses last
+        float key[4];
+        uint32_t val[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const bool inner = lk[k] >= 0;
+            const bool take = hit[k] && near[k] <= t.tmax && (inner || !blas);
+            key[k] = take ? near[k] : __int_as_float(0x7f800000);
+            val[k] = inner ? (blas ? (kTagBlas | (t.blas_base + uint32_t(lk[k]))) : uint32_t(lk[k]))
+                           : (kTagInstance | uint32_t(~lk[k]));
+        }
+#define PSY_CSWAP(i, j)                         \
+    if (key[j] < key[i]) {                      \
+        const float tk = key[i];                \
+        key[i] = key[j];                        \
+        key[j] = tk;                            \
+        const uint32_t tv = val[i];             \
+        val[i] = val[j];                        \
+        val[j] = tv;                            \
+    }
+        PSY_CSWAP(0, 1)
+        PSY_CSWAP(2, 3)
+        PSY_CSWAP(0, 2)
+        PSY_CSWAP(1, 3)
+        PSY_CSWAP(1, 2)
+#undef PSY_CSWAP
+        const float kInf = __int_as_float(0x7f800000);
+        if (key[0] == kInf) {
             if (t.sp == 0u) return true;
             t.node = t.stack[--t.sp];
+            continue;
         }
+#pragma unroll
+        for (int k = 3; k >= 1; --k)
+            if (key[k] != kInf && t.sp < uint32_t(kStackSize)) t.stack[t.sp++] = val[k];
+        t.node = val[0];
     }
     return false;
 }

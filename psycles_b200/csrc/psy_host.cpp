@@ -414,6 +414,90 @@ struct Builder {
         n.child = make_int4(l.link, r.link, l.count, r.count);
     }
 
+    // The 4-wide BVH of the binary nodes: starting from a binary node's two
+    // children, the inner child of largest surface area is replaced by its
+    // own two children until four children (or only leaves) remain; then
+    // every inner child is collapsed the same way.  Child boxes are the
+    // binary build's padded boxes, so the slab test stays conservative.
+    std::vector<psy::WideNodeGpu> widen() const {
+        std::vector<psy::WideNodeGpu> wide;
+        wide.reserve(nodes.size() / 2u + 1u);
+        collapse(0, wide);
+        return wide;
+    }
+
+    struct WideChild {
+        float lo[3], hi[3];
+        int link, count;
+        double area() const {
+            if (lo[0] > hi[0]) return -1.0;
+            const double dx = double(hi[0]) - lo[0], dy = double(hi[1]) - lo[1], dz = double(hi[2]) - lo[2];
+            return dx * dy + dy * dz + dz * dx;
+        }
+    };
+
+    WideChild child_of(int node, int side) const {
+        const psy::BvhNodeGpu &n = nodes[size_t(node)];
+        WideChild c;
+        if (side == 0) {
+            c.lo[0] = n.x.x, c.hi[0] = n.x.y, c.lo[1] = n.y.x, c.hi[1] = n.y.y, c.lo[2] = n.z.x, c.hi[2] = n.z.y;
+            c.link = n.child.x, c.count = n.child.z;
+        } else {
+            c.lo[0] = n.x.z, c.hi[0] = n.x.w, c.lo[1] = n.y.z, c.hi[1] = n.y.w, c.lo[2] = n.z.z, c.hi[2] = n.z.w;
+            c.link = n.child.y, c.count = n.child.w;
+        }
+        return c;
+    }
+
+    int collapse(int node, std::vector<psy::WideNodeGpu> &wide) const {
+        WideChild kids[4] = {child_of(node, 0), child_of(node, 1), {}, {}};
+        int n = 2;
+        while (n < 4) {
+            int best = -1;
+            double best_area = -2.0;
+            for (int k = 0; k < n; ++k)
+                if (kids[k].link >= 0 && kids[k].area() > best_area) {
+                    best = k;
+                    best_area = kids[k].area();
+                }
+            if (best < 0) break;
+            const int inner = kids[best].link;
+            kids[best] = child_of(inner, 0);
+            kids[n++] = child_of(inner, 1);
+        }
+        const int index = int(wide.size());
+        wide.push_back({});
+        int links[4], counts[4];
+        float lo[3][4], hi[3][4];
+        for (int k = 0; k < 4; ++k) {
+            if (k < n) {
+                for (int a = 0; a < 3; ++a) {
+                    lo[a][k] = kids[k].lo[a];
+                    hi[a][k] = kids[k].hi[a];
+                }
+                links[k] = kids[k].link >= 0 ? collapse(kids[k].link, wide) : kids[k].link;
+                counts[k] = kids[k].link >= 0 ? 0 : kids[k].count;
+            } else {
+                for (int a = 0; a < 3; ++a) {
+                    lo[a][k] = 1.0f;
+                    hi[a][k] = -1.0f;
+                }
+                links[k] = -1;
+                counts[k] = 0;
+            }
+        }
+        psy::WideNodeGpu &w = wide[size_t(index)];
+        w.lox = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+        w.hix = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+        w.loy = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+        w.hiy = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+        w.loz = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+        w.hiz = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+        w.link = make_int4(links[0], links[1], links[2], links[3]);
+        w.count = make_int4(counts[0], counts[1], counts[2], counts[3]);
+        return index;
+    }
+
     // Root node: a single leaf still gets a two-child root (empty right).
     Box build_root() {
         nodes.clear();
@@ -507,7 +591,7 @@ psy_status derive_params(psy_session *s, const psy_render_settings &r) {
 }
 
 psy_status ensure_capacity(psy_session *s, uint32_t n) {
-    return s->arena.ensure(n, false);
+    return s->scene->context->arena.ensure(n, false);
 }
 
 psy_status clear_film(psy_session *s) {
@@ -714,7 +798,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     std::vector<psy::MeshGpu> meshes(d->mesh_count);
     std::vector<float> positions, normals;
     std::vector<uint32_t> indices, tri_materials;
-    std::vector<psy::BvhNodeGpu> blas;
+    std::vector<psy::WideNodeGpu> blas;
     std::vector<float4> tris;
     std::vector<Box> mesh_boxes(d->mesh_count);
     uint32_t prim_offset = 0;
@@ -751,7 +835,8 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         mesh_boxes[i] = bld.build_root();
         g.node_offset = uint32_t(blas.size());
         g.tri_offset = uint32_t(tris.size() / 3u);
-        blas.insert(blas.end(), bld.nodes.begin(), bld.nodes.end());
+        const std::vector<psy::WideNodeGpu> wide = bld.widen();
+        blas.insert(blas.end(), wide.begin(), wide.end());
         for (const Prim &p : bld.prims) {
             for (int c = 0; c < 3; ++c) {
                 const float *v = m.positions + 3ull * m.indices[3ull * p.id + c];
@@ -987,7 +1072,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     }
 
     // ---- upload
-    PSY_CUDA_TRY(sc->tlas.upload(tl.nodes, st));
+    PSY_CUDA_TRY(sc->tlas.upload(tl.widen(), st));
     PSY_CUDA_TRY(sc->blas.upload(blas, st));
     PSY_CUDA_TRY(sc->tris.upload(tris, st));
     PSY_CUDA_TRY(sc->instances.upload(instances, st));
@@ -1034,8 +1119,8 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->lt_lookup.upload(lt_lookup, st));
     PSY_CUDA_TRY(cudaStreamSynchronize(st));
     psy::SceneView &v = sc->view;
-    v.tlas = sc->tlas.as<psy::BvhNodeGpu>();
-    v.blas = sc->blas.as<psy::BvhNodeGpu>();
+    v.tlas = sc->tlas.as<psy::WideNodeGpu>();
+    v.blas = sc->blas.as<psy::WideNodeGpu>();
     v.tris = sc->tris.as<float4>();
     v.instances = sc->instances.as<psy::InstanceGpu>();
     v.meshes = sc->meshes.as<psy::MeshGpu>();
@@ -1251,13 +1336,14 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
     if (prepared != PSY_OK) return prepared;
     const uint64_t begin = uint64_t(first) + offset, end = begin + count;
     psy_context *ctx = s->scene->context;
+    std::lock_guard<std::mutex> render_lock(ctx->render_mutex);
     cudaStream_t st = ctx->stream;
     const uint32_t pixels = s->pixels;
     uint32_t per_batch = std::max(1u, std::min(count, ctx->path_capacity / std::max(pixels, 1u)));
     psy_status r = ensure_capacity(s, pixels * per_batch);
     if (r != PSY_OK) return r;
     psy_path_trace *trace = s->trace_requested ? s->trace_buf.as<psy_path_trace>() : nullptr;
-    PSY_CUDA_TRY(cudaMemsetAsync(s->arena.stats.ptr, 0, 64, st));
+    PSY_CUDA_TRY(cudaMemsetAsync(ctx->arena.stats.ptr, 0, 64, st));
     psy_render_stats stats{};
     PSY_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
     const psy::LaunchConfig &lc = ctx->launch;
@@ -1281,7 +1367,7 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
         return PSY_OK;
     };
     auto read_counters = [&](uint32_t *c3) -> psy_status {
-        PSY_CUDA_TRY(cudaMemcpyAsync(c3, s->arena.view.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        PSY_CUDA_TRY(cudaMemcpyAsync(c3, ctx->arena.view.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         PSY_CUDA_TRY(cudaStreamSynchronize(st));
         return PSY_OK;
     };
@@ -1299,7 +1385,7 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
             trace_path = uint32_t(s->trace_sample - sample) * pixels + local;
         }
         psy_path_trace *tr = trace_path != psy::kInvalidId ? trace : nullptr;
-        psy::PathBuffers b = s->arena.view;
+        psy::PathBuffers b = ctx->arena.view;
         psy::launch_set_counters(st, b.counters, paths);
         if ((ps = timed([&] { psy::launch_raygen(st, lc, p, b, pixels, paths, uint32_t(sample), trace_path, tr); },
                         pf.raygen_launches, pf.raygen_ms)) != PSY_OK)
@@ -1316,7 +1402,7 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
             if ((ps = timed([&] { psy::launch_shade(st, lc, s->scene->view, p, b, paths, step, trace_path, tr); },
                             pf.shade_launches, pf.shade_ms)) != PSY_OK)
                 return ps;
-            psy::launch_count_rays(st, b.counters, s->arena.stats.as<unsigned long long>());
+            psy::launch_count_rays(st, b.counters, ctx->arena.stats.as<unsigned long long>());
             if (prof && (ps = read_counters(c3)) != PSY_OK) return ps;
             pf.shade_bytes += 304.0 * c3[0] + 68.0 * c3[2];
             if ((ps = timed([&] { psy::launch_shadow(st, lc, s->scene->view, p, b, paths, step, trace_path, tr); },
@@ -1350,7 +1436,7 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
     float ms = 0.0f;
     PSY_CUDA_TRY(cudaEventElapsedTime(&ms, s->ev_begin, s->ev_end));
     unsigned long long counts[2] = {0, 0};
-    PSY_CUDA_TRY(cudaMemcpy(counts, s->arena.stats.ptr, sizeof(counts), cudaMemcpyDeviceToHost));
+    PSY_CUDA_TRY(cudaMemcpy(counts, ctx->arena.stats.ptr, sizeof(counts), cudaMemcpyDeviceToHost));
     stats.closest_rays = counts[0];
     stats.path_segments = counts[0];
     stats.shadow_rays = counts[1];

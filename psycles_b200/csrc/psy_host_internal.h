@@ -13,6 +13,7 @@ struct psy_session;
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -92,6 +93,11 @@ struct psy_context {
     cudaStream_t stream = nullptr;
     psy::LaunchConfig launch;      // psy_context_set_tuning
     uint32_t path_capacity = 1u << 24;  // 16 Mi paths, about 3.9 GB of path state
+    // Path state shared by every session of the context: their renders run
+    // on the context's one stream and render_samples is synchronous, so
+    // they never overlap; the mutex orders renders from different threads.
+    psy::host::PathArena arena;
+    std::mutex render_mutex;
 };
 
 struct psy_scene {
@@ -120,8 +126,7 @@ struct psy_session {
     uint32_t rendered = 0;
     std::atomic<bool> cancelled{false};
     psy::host::DeviceBuffer sobol, filter, combined, normal, albedo, sample_count;
-    // path state
-    psy::host::PathArena arena;
+    // path state: the context's shared arena (psy_context::arena)
     // trace
     psy::host::DeviceBuffer trace_buf;
     bool trace_requested = false;

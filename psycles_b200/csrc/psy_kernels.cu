@@ -14,6 +14,8 @@
 // never changes a path's result.
 #include "psy_device.cuh"
 #include "psy_kernels.h"
+
+#include <algorithm>
 #include "psy_light_tree.cuh"
 
 namespace psy {
@@ -151,7 +153,7 @@ __device__ __forceinline__ uint32_t contract_visibility(uint32_t v) {
 #define PSY_SHADE_MIN_BLOCKS 3
 #endif
 #ifndef PSY_SHADOW_MIN_BLOCKS
-#define PSY_SHADOW_MIN_BLOCKS 5
+#define PSY_SHADOW_MIN_BLOCKS 4
 #endif
 // Nodes a lane advances between refills of idle lanes.
 constexpr int kTraversalBudget = PSY_TRAVERSAL_BUDGET;
@@ -393,12 +395,40 @@ __global__ void k_sort_scan(const __grid_constant__ PathBuffers b, uint32_t thre
     }
 }
 
-__global__ void k_sort_scatter(const __grid_constant__ PathBuffers b, uint32_t threshold) {
+// Scatter in three passes over each block's contiguous chunk of the queue:
+// ranks inside the block from warp-aggregated shared-memory atomics (stored
+// beside the 11-bit bucket), one global reservation per non-empty bucket
+// per block, then the writes.  Global atomics drop from one per path to one
+// per bucket and block.
+__global__ void __launch_bounds__(256) k_sort_scatter(const __grid_constant__ PathBuffers b, uint32_t threshold) {
+    __shared__ uint32_t hist[kSortBuckets];
     const uint32_t count = b.counters[0];
     if (count < threshold) return;
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
-        const uint32_t pos = atomicAdd(&b.sort_offsets[b.sort_keys[q]], 1u);
-        b.queue_sorted[pos] = b.queue_in[q];
+    const uint32_t chunk = (count + gridDim.x - 1u) / gridDim.x;
+    const uint32_t begin = blockIdx.x * chunk;
+    const uint32_t end = min(count, begin + chunk);
+    for (uint32_t k = threadIdx.x; k < kSortBuckets; k += blockDim.x) hist[k] = 0u;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = begin; base < end; base += blockDim.x) {
+        const uint32_t q = base + threadIdx.x;
+        const bool live = q < end;
+        const uint32_t key = live ? b.sort_keys[q] : kSortBuckets;  // sentinel outside the histogram
+        const uint32_t peers = __match_any_sync(kFullMask, key);
+        const uint32_t leader = __ffs(peers) - 1u;
+        const uint32_t rank_in_warp = __popc(peers & ((1u << lane) - 1u));
+        uint32_t first = 0u;
+        if (live && lane == leader) first = atomicAdd(&hist[key], __popc(peers));
+        first = __shfl_sync(peers, first, leader);
+        if (live) b.sort_keys[q] = key | ((first + rank_in_warp) << 11);
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < kSortBuckets; k += blockDim.x)
+        if (hist[k]) hist[k] = atomicAdd(&b.sort_offsets[k], hist[k]);
+    __syncthreads();
+    for (uint32_t q = begin + threadIdx.x; q < end; q += blockDim.x) {
+        const uint32_t packed = b.sort_keys[q];
+        b.queue_sorted[hist[packed & (kSortBuckets - 1u)] + (packed >> 11)] = b.queue_in[q];
     }
 }
 
@@ -1159,7 +1189,9 @@ void launch_sort(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, co
                  uint32_t max_work) {
     k_sort_count<kMulti><<<launch_grid(max_work, 256, lc), 256, 0, st>>>(s, b, jobs, lc.sort_threshold);
     k_sort_scan<<<1, 1024, 0, st>>>(b, lc.sort_threshold);
-    k_sort_scatter<<<launch_grid(max_work, 256, lc), 256, 0, st>>>(b, lc.sort_threshold);
+    // ranks are packed in 21 bits: keep every block's chunk below 2^20 paths
+    const int scatter_blocks = std::max(launch_grid(max_work, 256, lc), int((max_work >> 20) + 1u));
+    k_sort_scatter<<<scatter_blocks, 256, 0, st>>>(b, lc.sort_threshold);
 }
 int persistent_grid(uint32_t work, const LaunchConfig &lc) {
     const uint32_t blocks = (work + 127u) / 128u;

@@ -1,8 +1,9 @@
 // Device-resident scene and render parameters of the B200 path tracer.
 //
 // HBM layout (one allocation per array, all 16-byte aligned):
-//   tlas / blas   binary BVH nodes, 64 B each: three float4 hold the two
-//                 children's x/y/z slabs, one int4 the child links
+//   tlas / blas   4-wide BVH nodes, 128 B each (two 64-byte lines): six
+//                 float4 hold the four children's x/y/z slabs lane by
+//                 lane, two int4 the child links and leaf counts
 //   tris          leaf-ordered triangles of all meshes, 3 float4 per
 //                 triangle (48 B): object-space vertices, v0.w = local
 //                 primitive index bits
@@ -36,6 +37,17 @@ struct alignas(16) BvhNodeGpu {
     int4 child;  // x/y: >= 0 inner node, < 0 leaf ~first; z/w: leaf counts
 };
 static_assert(sizeof(BvhNodeGpu) == 64, "BVH node is one 64-byte line");
+
+// 4-wide node, collapsed from the binary build: child k's slabs in lane k.
+// link >= 0: inner node (relative to the BVH's first node); link < 0 with
+// count > 0: a leaf (~first triangle, or ~instance in the TLAS); count 0
+// with link < 0: an empty slot.
+struct alignas(16) WideNodeGpu {
+    float4 lox, hix, loy, hiy, loz, hiz;
+    int4 link;
+    int4 count;
+};
+static_assert(sizeof(WideNodeGpu) == 128, "wide BVH node is two 64-byte lines");
 
 struct alignas(16) InstanceGpu {
     float o2w[12];  // column-major c0, c1, c2, c3 (xyz each)
@@ -73,8 +85,8 @@ struct alignas(16) DistEntryGpu {
 };
 
 struct SceneView {
-    const BvhNodeGpu *tlas;
-    const BvhNodeGpu *blas;
+    const WideNodeGpu *tlas;
+    const WideNodeGpu *blas;
     const float4 *tris;
     const InstanceGpu *instances;
     const MeshGpu *meshes;
