@@ -459,6 +459,8 @@ typedef struct psy_tuning {
     uint32_t shade_blocks_per_sm;      /* shading grid cap; 0 = 32 */
     uint32_t sort_threshold;           /* sort shading queues of at least this many paths by material;
                                           0 = never, 0xffffffff = the default 65536 */
+    uint32_t shadow_sort_threshold;    /* sort shadow queues of at least this many rays by direction;
+                                          0 = never (the default), 0xffffffff = the default */
 } psy_tuning;
 
 psy_status psy_context_set_tuning(psy_context *context, const psy_tuning *tuning);

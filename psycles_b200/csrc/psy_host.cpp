@@ -310,6 +310,12 @@ void padded(const Box &b, float lo[3], float hi[3]) {
 #ifndef PSY_LEAF_SIZE
 #define PSY_LEAF_SIZE 1u
 #endif
+#ifndef PSY_SAH_BINS
+#define PSY_SAH_BINS 32
+#endif
+#ifndef PSY_SAH_AXES
+#define PSY_SAH_AXES 3
+#endif
 
 struct Builder {
     std::vector<psy::BvhNodeGpu> nodes;
@@ -336,54 +342,59 @@ struct Builder {
         }
         const uint32_t count = end - begin;
         if (count <= leaf_size) return leaf(begin, end, box);
-        // binned SAH over the widest centroid axis
+        // binned SAH: PSY_SAH_BINS bins on every axis with a centroid extent
+        // (PSY_SAH_AXES 1: the widest axis only)
         int axis = 0;
         for (int a = 1; a < 3; ++a)
             if (cbox.hi[a] - cbox.lo[a] > cbox.hi[axis] - cbox.lo[axis]) axis = a;
-        const double extent = cbox.hi[axis] - cbox.lo[axis];
         uint32_t mid = begin + count / 2u;
         bool done = false;
-        if (extent > 0.0 && depth < 60) {
-            constexpr int kBins = 16;
-            Box bins[kBins];
-            uint32_t counts[kBins] = {};
-            const double scale = kBins / extent;
-            auto bin_of = [&](const Prim &p) {
-                int b = int((p.c[axis] - cbox.lo[axis]) * scale);
-                return std::min(std::max(b, 0), kBins - 1);
-            };
-            for (uint32_t i = begin; i < end; ++i) {
-                const int b = bin_of(prims[i]);
-                bins[b].grow(prims[i].box);
-                counts[b]++;
-            }
-            double right_area[kBins];
-            uint32_t right_count[kBins];
-            Box acc;
-            uint32_t acc_n = 0u;
-            for (int b = kBins - 1; b > 0; --b) {
-                acc.grow(bins[b]);
-                acc_n += counts[b];
-                right_area[b] = acc.area();
-                right_count[b] = acc_n;
-            }
-            Box left;
-            uint32_t left_n = 0u;
+        if (depth < 60) {
+            constexpr int kBins = PSY_SAH_BINS;
             double best = 1e300;
-            int best_split = -1;
-            for (int b = 1; b < kBins; ++b) {
-                left.grow(bins[b - 1]);
-                left_n += counts[b - 1];
-                if (left_n == 0u || right_count[b] == 0u) continue;
-                const double cost = left.area() * left_n + right_area[b] * right_count[b];
-                if (cost < best) {
-                    best = cost;
-                    best_split = b;
+            int best_split = -1, best_axis = -1;
+            for (int a = 0; a < 3; ++a) {
+                if (PSY_SAH_AXES == 1 && a != axis) continue;
+                const double extent = cbox.hi[a] - cbox.lo[a];
+                if (!(extent > 0.0)) continue;
+                Box bins[kBins];
+                uint32_t counts[kBins] = {};
+                const double scale = kBins / extent;
+                for (uint32_t i = begin; i < end; ++i) {
+                    const int bn = std::min(std::max(int((prims[i].c[a] - cbox.lo[a]) * scale), 0), kBins - 1);
+                    bins[bn].grow(prims[i].box);
+                    counts[bn]++;
+                }
+                double right_area[kBins];
+                uint32_t right_count[kBins];
+                Box acc;
+                uint32_t acc_n = 0u;
+                for (int bn = kBins - 1; bn > 0; --bn) {
+                    acc.grow(bins[bn]);
+                    acc_n += counts[bn];
+                    right_area[bn] = acc.area();
+                    right_count[bn] = acc_n;
+                }
+                Box left;
+                uint32_t left_n = 0u;
+                for (int bn = 1; bn < kBins; ++bn) {
+                    left.grow(bins[bn - 1]);
+                    left_n += counts[bn - 1];
+                    if (left_n == 0u || right_count[bn] == 0u) continue;
+                    const double cost = left.area() * left_n + right_area[bn] * right_count[bn];
+                    if (cost < best) {
+                        best = cost;
+                        best_split = bn;
+                        best_axis = a;
+                    }
                 }
             }
             if (best_split > 0) {
-                auto it = std::partition(prims.begin() + begin, prims.begin() + end,
-                                         [&](const Prim &p) { return bin_of(p) < best_split; });
+                const int a = best_axis;
+                const double scale = kBins / (cbox.hi[a] - cbox.lo[a]);
+                auto it = std::partition(prims.begin() + begin, prims.begin() + end, [&](const Prim &p) {
+                    return std::min(std::max(int((p.c[a] - cbox.lo[a]) * scale), 0), kBins - 1) < best_split;
+                });
                 mid = uint32_t(it - prims.begin());
                 done = mid > begin && mid < end;
             }
@@ -719,6 +730,8 @@ psy_status psy_context_set_tuning(psy_context *c, const psy_tuning *t) {
         t->traversal_blocks_per_sm ? t->traversal_blocks_per_sm : defaults.traversal_blocks_per_sm;
     c->launch.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : defaults.shade_blocks_per_sm;
     c->launch.sort_threshold = t->sort_threshold == 0xffffffffu ? defaults.sort_threshold : t->sort_threshold;
+    c->launch.shadow_sort_threshold =
+        t->shadow_sort_threshold == 0xffffffffu ? defaults.shadow_sort_threshold : t->shadow_sort_threshold;
     return PSY_OK;
 }
 
@@ -729,6 +742,7 @@ psy_status psy_context_get_tuning(const psy_context *c, psy_tuning *t) {
     t->traversal_blocks_per_sm = c->launch.traversal_blocks_per_sm;
     t->shade_blocks_per_sm = c->launch.shade_blocks_per_sm;
     t->sort_threshold = c->launch.sort_threshold;
+    t->shadow_sort_threshold = c->launch.shadow_sort_threshold;
     return PSY_OK;
 }
 
@@ -1525,6 +1539,7 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
     // the static path state has no sort buffers
     psy::LaunchConfig lc = ctx->launch;
     lc.sort_threshold = 0u;
+    lc.shadow_sort_threshold = 0u;
     psy_render_stats stats{};
     PSY_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
     for (uint64_t sample = begin; sample < end;) {

@@ -144,7 +144,7 @@ __device__ __forceinline__ uint32_t contract_visibility(uint32_t v) {
 // it finishes, the warp refills its idle lanes from a global fetch counter
 // (one atomic per warp), so lanes do not wait for the warp's longest ray.
 #ifndef PSY_TRAVERSAL_BUDGET
-#define PSY_TRAVERSAL_BUDGET 12
+#define PSY_TRAVERSAL_BUDGET 24
 #endif
 #ifndef PSY_INTERSECT_MIN_BLOCKS
 #define PSY_INTERSECT_MIN_BLOCKS 6
@@ -369,9 +369,10 @@ __global__ void k_sort_count(const __grid_constant__ SceneView s_arg, const __gr
 
 // One block of 1024 threads: offsets = exclusive scan of the histogram,
 // which is cleared for the next sort.
-__global__ void k_sort_scan(const __grid_constant__ PathBuffers b, uint32_t threshold) {
+// `counter`: 0 sorts the shading queue, 2 the shadow queue.
+__global__ void k_sort_scan(const __grid_constant__ PathBuffers b, uint32_t threshold, uint32_t counter) {
     __shared__ uint32_t part[1024];
-    if (b.counters[0] < threshold) return;
+    if (b.counters[counter] < threshold) return;
     constexpr uint32_t kPer = kSortBuckets / 1024u;
     const uint32_t t = threadIdx.x;
     uint32_t v[kPer], sum = 0u;
@@ -400,9 +401,12 @@ __global__ void k_sort_scan(const __grid_constant__ PathBuffers b, uint32_t thre
 // beside the 11-bit bucket), one global reservation per non-empty bucket
 // per block, then the writes.  Global atomics drop from one per path to one
 // per bucket and block.
-__global__ void __launch_bounds__(256) k_sort_scatter(const __grid_constant__ PathBuffers b, uint32_t threshold) {
+// The shading queue sorts its path indices; the shadow queue sorts its
+// slot numbers (a permutation k_shadow reads its rays through).
+__global__ void __launch_bounds__(256) k_sort_scatter(const __grid_constant__ PathBuffers b, uint32_t threshold,
+                                                      uint32_t counter) {
     __shared__ uint32_t hist[kSortBuckets];
-    const uint32_t count = b.counters[0];
+    const uint32_t count = b.counters[counter];
     if (count < threshold) return;
     const uint32_t chunk = (count + gridDim.x - 1u) / gridDim.x;
     const uint32_t begin = blockIdx.x * chunk;
@@ -428,8 +432,37 @@ __global__ void __launch_bounds__(256) k_sort_scatter(const __grid_constant__ Pa
     __syncthreads();
     for (uint32_t q = begin + threadIdx.x; q < end; q += blockDim.x) {
         const uint32_t packed = b.sort_keys[q];
-        b.queue_sorted[hist[packed & (kSortBuckets - 1u)] + (packed >> 11)] = b.queue_in[q];
+        b.queue_sorted[hist[packed & (kSortBuckets - 1u)] + (packed >> 11)] = counter == 0u ? b.queue_in[q] : q;
     }
+}
+
+// Shadow rays grouped by direction (octahedral map of the direction into a
+// 45 x 45 grid), so a warp's rays head the same way -- mostly towards the
+// same light from nearby points.
+__global__ void k_sort_count_shadow(const __grid_constant__ PathBuffers b, uint32_t threshold) {
+    __shared__ uint32_t local[kSortBuckets];
+    const uint32_t count = b.counters[2];
+    if (count < threshold) return;
+    for (uint32_t k = threadIdx.x; k < kSortBuckets; k += blockDim.x) local[k] = 0u;
+    __syncthreads();
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+        const float4 d = b.sh_d[q];
+        const float l1 = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
+        float u = l1 > 0.0f ? d.x / l1 : 0.0f, v = l1 > 0.0f ? d.y / l1 : 0.0f;
+        if (d.z < 0.0f) {
+            const float uu = (1.0f - fabsf(v)) * (u >= 0.0f ? 1.0f : -1.0f);
+            v = (1.0f - fabsf(u)) * (v >= 0.0f ? 1.0f : -1.0f);
+            u = uu;
+        }
+        const uint32_t iu = min(44u, uint32_t(fmaxf(u * 0.5f + 0.5f, 0.0f) * 45.0f));
+        const uint32_t iv = min(44u, uint32_t(fmaxf(v * 0.5f + 0.5f, 0.0f) * 45.0f));
+        const uint32_t key = iv * 45u + iu;
+        b.sort_keys[q] = key;
+        atomicAdd(&local[key], 1u);
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < kSortBuckets; k += blockDim.x)
+        if (local[k]) atomicAdd(&b.sort_hist[k], local[k]);
 }
 
 // kTrace selects the variant that records the per-path trace; the render
@@ -932,8 +965,9 @@ template <bool kMulti>
 __global__ void __launch_bounds__(128, PSY_SHADOW_MIN_BLOCKS)
     k_shadow(const __grid_constant__ SceneView s_arg, const __grid_constant__ RenderParams p_arg,
              const __grid_constant__ PathBuffers b, uint32_t step, uint32_t trace_path, psy_path_trace *trace,
-             const JobGpu *jobs) {
+             const JobGpu *jobs, uint32_t sort_threshold) {
     const uint32_t count = b.counters[2];
+    const bool sorted = sort_threshold != 0u && count >= sort_threshold;
     TraversalState t;
     bool active = false, exhausted = false, blocked = false, overflow = false;
     uint32_t q_cur = 0u, job = 0u;
@@ -941,7 +975,8 @@ __global__ void __launch_bounds__(128, PSY_SHADOW_MIN_BLOCKS)
     uint32_t lo[kShadowList], lp[kShadowList], lm[kShadowList];
     int n = 0;
     for (;;) {
-        const uint32_t q = warp_fetch(&b.counters[4], count, !active, exhausted);
+        uint32_t q = warp_fetch(&b.counters[4], count, !active, exhausted);
+        if (sorted && q != kInvalid) q = b.queue_sorted[q];
         if (kMulti && q != kInvalid) job = b.job[b.sh_path[q]];
         const SceneView &s = kMulti ? jobs[job].s : s_arg;
         const RenderParams &p = kMulti ? jobs[job].p : p_arg;
@@ -1188,10 +1223,17 @@ template <bool kMulti>
 void launch_sort(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const PathBuffers &b, const JobGpu *jobs,
                  uint32_t max_work) {
     k_sort_count<kMulti><<<launch_grid(max_work, 256, lc), 256, 0, st>>>(s, b, jobs, lc.sort_threshold);
-    k_sort_scan<<<1, 1024, 0, st>>>(b, lc.sort_threshold);
+    k_sort_scan<<<1, 1024, 0, st>>>(b, lc.sort_threshold, 0u);
     // ranks are packed in 21 bits: keep every block's chunk below 2^20 paths
     const int scatter_blocks = std::max(launch_grid(max_work, 256, lc), int((max_work >> 20) + 1u));
-    k_sort_scatter<<<scatter_blocks, 256, 0, st>>>(b, lc.sort_threshold);
+    k_sort_scatter<<<scatter_blocks, 256, 0, st>>>(b, lc.sort_threshold, 0u);
+}
+void launch_shadow_sort(cudaStream_t st, const LaunchConfig &lc, const PathBuffers &b, uint32_t max_work) {
+    const uint32_t thr = lc.shadow_sort_threshold;
+    k_sort_count_shadow<<<launch_grid(max_work, 256, lc), 256, 0, st>>>(b, thr);
+    k_sort_scan<<<1, 1024, 0, st>>>(b, thr, 2u);
+    const int scatter_blocks = std::max(launch_grid(max_work, 256, lc), int((max_work >> 20) + 1u));
+    k_sort_scatter<<<scatter_blocks, 256, 0, st>>>(b, thr, 2u);
 }
 int persistent_grid(uint32_t work, const LaunchConfig &lc) {
     const uint32_t blocks = (work + 127u) / 128u;
@@ -1214,7 +1256,9 @@ void launch_shade(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, c
 }
 void launch_shadow(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                    uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
-    k_shadow<false><<<persistent_grid(max_work, lc), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr);
+    if (lc.shadow_sort_threshold) launch_shadow_sort(st, lc, b, max_work);
+    k_shadow<false><<<persistent_grid(max_work, lc), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr,
+                                                                   lc.shadow_sort_threshold);
 }
 void launch_begin_round(cudaStream_t st, uint32_t *counters, uint32_t *round, BatchItem *items,
                         const uint32_t *plan_rounds, const BatchItem *plan_items, uint32_t *cursor, uint32_t max_items) {
@@ -1245,8 +1289,9 @@ void launch_shade_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *j
 }
 void launch_shadow_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work,
                          uint32_t step) {
+    if (lc.shadow_sort_threshold) launch_shadow_sort(st, lc, b, max_work);
     k_shadow<true><<<persistent_grid(max_work, lc), 128, 0, st>>>(SceneView{}, RenderParams{}, b, step, kInvalid,
-                                                                    nullptr, jobs);
+                                                                  nullptr, jobs, lc.shadow_sort_threshold);
 }
 void launch_film_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const BatchItem *items, const uint32_t *round,
                        const PathBuffers &b, uint32_t max_pixels) {

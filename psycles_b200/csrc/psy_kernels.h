@@ -15,6 +15,7 @@ struct LaunchConfig {
     uint32_t traversal_blocks_per_sm = 12;  // persistent closest-hit and shadow kernels
     uint32_t shade_blocks_per_sm = 32;
     uint32_t sort_threshold = 1u << 16;     // 0: never sort
+    uint32_t shadow_sort_threshold = 0;     // shadow queue by direction (off: it measured slower); 0: never
 };
 
 int launch_grid(uint32_t work, int block, const LaunchConfig &lc);
