@@ -919,12 +919,116 @@ static AnalyticSample sample_distant(const psy_light_desc &l, float2 rnd) {
     const float3 dir = -c.direction;
     return {true, dir, -dir, 1.0e30f, c.pdf, eval};
 }
-// sample_point_light / sample_spot_light for delta and disk point sources
-// (:898-1105); sphere-shaped sources are not in the subset.
-static AnalyticSample sample_point_or_spot(const psy_light_desc &l, float3 reference, float2 rnd) {
+// spot_one_minus_cosine_larger_spread (:355-376), with 1/sqrt for rsqrt.
+static float spot_spread_cap(const psy_light_desc &l) {
+    const float t = tan_(0.5f * l.spot_angle);
+    const float ts2 = maxf(l.axis_scale[0] * l.axis_scale[0], l.axis_scale[1] * l.axis_scale[1]);
+    const float as2 = l.axis_scale[2] * l.axis_scale[2];
+    return 1.0f - 1.0f / std::sqrt(1.0f + t * t * ts2 / maxf(as2, 1.0e-30f));
+}
+
+struct SphereHit {
+    bool valid;
+    float distance;
+    float3 position;
+};
+
+// intersect_sphere (:192-239).
+static SphereHit intersect_sphere(float3 o, float3 d, float tmin, float tmax, float3 c, float r) {
+    const float3 co = c - o;
+    const float r2 = r * r;
+    const float cd2 = dot(co, co);
+    const float pd = dot(co, d);
+    const float3 perp = co - d * pd;
+    const float pp2 = dot(perp, perp);
+    const float dist = pd - std::copysign(std::sqrt(maxf(r2 - pp2, 0.0f)), cd2 - r2);
+    const bool valid = !(cd2 > r2 && pd < 0.0f) && pp2 <= r2 && dist > tmin && dist < tmax;
+    return {valid, dist, o + d * dist};
+}
+
+// sample_uniform_sphere (cycles_sample_mapping.h:380-387).
+static float3 sample_uniform_sphere(float2 u) {
+    const float z = 1.0f - 2.0f * u.x;
+    const float r = std::sqrt(maxf(1.0f - z * z, 0.0f));
+    const float phi = 2.0f * kPi * u.y;
+    return f3(r * cos_(phi), r * sin_(phi), z);
+}
+
+// sample_sphere_geometry (:430-548).
+static AnalyticSample sample_sphere(float3 reference, float3 n, bool transmission, float3 center, float r,
+                                    float3 outside_axis, float outside_omc, bool intersect_sampled, float2 rnd) {
+    const float r2 = r * r;
+    float3 ln = reference - center;
+    const float cd2 = dot(ln, ln);
+    const float cd = std::sqrt(maxf(cd2, 1.0e-30f));
+    ln = ln / cd;
+    float3 dir = f3(0.0f);
+    float cosine = 1.0f, pdf = 0.0f, dist = 0.0f;
+    float3 pos = reference;
+    bool known = false;
+    bool valid = r > 0.0f && cd2 > 0.0f;
+    if (cd2 > r2) {
+        const ConeSample c = sample_uniform_cone(outside_axis, outside_omc, rnd);
+        dir = c.direction;
+        cosine = c.cosine;
+        pdf = c.pdf;
+        if (intersect_sampled) {
+            const SphereHit h = intersect_sphere(reference, dir, 0.0f, 1.0e30f, center, r);
+            valid = valid && h.valid;
+            dist = h.distance;
+            pos = h.position;
+            known = h.valid;
+        }
+    } else {
+        if (transmission) {
+            dir = sample_uniform_sphere(rnd);
+            pdf = 0.5f * kInvTwoPi;
+        } else {
+            const HemisphereSample hs = sample_cosine_hemisphere(n, rnd);
+            dir = hs.direction;
+            pdf = hs.pdf;
+        }
+        cosine = -dot(dir, ln);
+    }
+    if (!known) {
+        dist = cd * cosine - std::copysign(std::sqrt(maxf(r2 - cd2 + cd2 * cosine * cosine, 0.0f)), cd2 - r2);
+        pos = reference + dir * dist;
+    }
+    const float3 normal = light_safe_normalize(pos - center, -dir);
+    return {valid, dir, normal * r + center, dist, pdf, 0.0f};
+}
+
+// sample_point_light / sample_spot_light (:898-1105): delta, disk and
+// sphere sources.
+static AnalyticSample sample_point_or_spot(const psy_light_desc &l, float3 reference, float3 shading_n,
+                                           bool transmission, float2 rnd) {
     const float3 center = f3(l.position[0], l.position[1], l.position[2]);
-    AnalyticSample g = sample_disk(reference, center, l.radius, rnd);
     const bool normalize_power = (l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u;
+    if ((l.flags & PSY_LIGHT_FLAG_SPHERE) != 0u && l.radius > 0.0f) {
+        const float3 off = reference - center;
+        const float cd2 = dot(off, off);
+        const float r2 = l.radius * l.radius;
+        const float3 ln = light_safe_normalize(off, f3(0.0f, 0.0f, -1.0f));
+        const float sphere_cap = sin_squared_to_one_minus_cosine(r2 / maxf(cd2, 1.0e-30f));
+        float3 axis = -ln;
+        float cap = sphere_cap;
+        bool spread = false;
+        if (l.type == PSY_LIGHT_SPOT) {
+            const float spot_cap = spot_spread_cap(l);
+            spread = cd2 > r2 && !(sphere_cap < spot_cap);
+            if (spread) {
+                axis = f3(l.axis_z[0], l.axis_z[1], l.axis_z[2]);
+                cap = spot_cap;
+            }
+        }
+        AnalyticSample g = sample_sphere(reference, shading_n, transmission, center, l.radius, axis, cap, spread, rnd);
+        float eval = point_eval_factor(l.radius, normalize_power);
+        if (l.type == PSY_LIGHT_SPOT && cd2 > r2) eval *= spot_attenuation(l, -g.direction);
+        g.eval_factor = eval;
+        if (l.type == PSY_LIGHT_SPOT) g.valid = g.valid && eval != 0.0f;
+        return g;
+    }
+    AnalyticSample g = sample_disk(reference, center, l.radius, rnd);
     float eval = point_eval_factor(l.radius, normalize_power);
     if (l.type == PSY_LIGHT_SPOT) eval *= spot_attenuation(l, -g.direction);
     g.eval_factor = eval;
@@ -1078,9 +1182,37 @@ static bool lamp_area(const psy_light_desc &l, const Ray &ray, float tmin, float
 
 // intersect_point / intersect_spot, oriented-disk case (analytic_light_intersection.h:33-266):
 // the disk of `radius` faces the ray origin.
-static bool lamp_disk(const psy_light_desc &l, const Ray &ray, float tmin, float tmax, LampHit &out) {
+static bool lamp_disk(const psy_light_desc &l, const Ray &ray, float tmin, float tmax, float3 mis_n,
+                      bool had_transmission, LampHit &out) {
     const float3 center = f3(l.position[0], l.position[1], l.position[2]);
     const float3 offset = ray.o - center;
+    if ((l.flags & PSY_LIGHT_FLAG_SPHERE) != 0u) {
+        // sphere geometry with sphere_light_pdf (analytic_light_sampling.h:282-307)
+        if (!(l.radius > 0.0f)) return false;
+        const float cd2 = dot(offset, offset);
+        const float r2 = l.radius * l.radius;
+        float cap = sin_squared_to_one_minus_cosine(r2 / maxf(cd2, 1.0e-30f));
+        if (l.type == PSY_LIGHT_SPOT) cap = minf(cap, spot_spread_cap(l));
+        const SphereHit h = intersect_sphere(ray.o, ray.d, tmin, tmax, center, l.radius);
+        if (!h.valid) return false;
+        float pdf;
+        if (cd2 > r2) {
+            pdf = kInvTwoPi / maxf(cap, 1.0e-30f);
+        } else if (had_transmission) {
+            pdf = 0.5f * kInvTwoPi;
+        } else {
+            const float c = dot(mis_n, ray.d);
+            pdf = c > 0.0f ? c * kInvPi : 0.0f;
+        }
+        float eval = point_eval_factor(l.radius, (l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u);
+        if (l.type == PSY_LIGHT_SPOT) {
+            if (cd2 > r2) eval *= spot_attenuation(l, -ray.d);
+            if (!(dot(ray.d, offset) < 0.0f)) return false;
+        }
+        if (!(eval > 0.0f)) return false;
+        out = {true, 0u, h.distance, pdf, eval};
+        return true;
+    }
     const float3 n = light_safe_normalize(offset, -ray.d);
     const float plane = dot(offset, n);
     const float cosine = dot(n, -ray.d);
@@ -1103,7 +1235,7 @@ static bool lamp_disk(const psy_light_desc &l, const Ray &ray, float tmin, float
 // the nearest eligible lamp strictly before `event_distance`, ties to the
 // lower index.
 static LampHit closest_lamp(const Scene &s, const Ray &ray, float tmin, float event_distance, uint32_t ray_visibility,
-                            uint32_t excluded) {
+                            uint32_t excluded, float3 mis_n, bool had_transmission) {
     LampHit best{false, kInvalid, event_distance, 0.0f, 0.0f};
     const bool camera_path = (ray_visibility & PSY_VISIBILITY_CAMERA) != 0u;
     for (uint32_t i = 0; i < s.lights.size(); ++i) {
@@ -1113,7 +1245,7 @@ static LampHit closest_lamp(const Scene &s, const Ray &ray, float tmin, float ev
         if (!camera_path && (l.flags & kLightUseMis) == 0u) continue;
         LampHit h{};
         const bool ok = l.type == PSY_LIGHT_AREA ? lamp_area(l, ray, tmin, best.distance, h)
-                                                 : lamp_disk(l, ray, tmin, best.distance, h);
+                                                 : lamp_disk(l, ray, tmin, best.distance, mis_n, had_transmission, h);
         if (ok) {
             best = h;
             best.index = i;
@@ -1441,7 +1573,8 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
             uint32_t excluded = kInvalid;
             float tmin = ray.tmin;
             for (;;) {
-                const LampHit lh = closest_lamp(s, ray, tmin, event_distance, ray_visibility, excluded);
+                const LampHit lh = closest_lamp(s, ray, tmin, event_distance, ray_visibility, excluded,
+                                                previous_mis_normal, (ps.flag & kFlagMisHadTransmission) != 0u);
                 if (!lh.valid) break;
                 float selection_pdf = s.light_selection_pdf;
                 if (st.use_light_tree)
@@ -1496,7 +1629,10 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
                 selection_pdf = lt::tree_pdf(s.tree, tree_emitter(s, sp.object, sp.cycles_prim), ray.o,
                                              previous_mis_normal, (ps.flag & kFlagMisHadTransmission) != 0u);
             const float light_pdf = emissive_forward_pdf(selection_pdf, mat.emission_sampling, ray.o, sp.position,
-                                                         sp.wp0, sp.wp1, sp.wp2, sp.ng);
+                                                         sp.wp0, sp.wp1, sp.wp2,
+                                                         // the geometric normal before the back-face flip
+                                                         // (path_kernel_surface_shading.cpp:130-134)
+                                                         sp.back_facing ? -sp.ng : sp.ng);
             const bool light_available = light_pdf > 0.0f;
             emission_weight = forward_light_weight(mode, previous_bsdf_pdf, light_pdf, competing, light_available);
         }
@@ -1596,7 +1732,8 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
                     const float2 lxy = f2(light_sample.x, light_sample.y);
                     AnalyticSample a = l.type == PSY_LIGHT_DISTANT ? sample_distant(l, lxy)
                                        : l.type == PSY_LIGHT_AREA  ? sample_area(l, sp.position, lxy)
-                                                                    : sample_point_or_spot(l, sp.position, lxy);
+                                                                    : sample_point_or_spot(l, sp.position, sp.n,
+                                                                                           (runtime & kRuntimeBsdfHasTransmission) != 0u, lxy);
                     const float light_pdf = a.pdf * selected.selection_pdf;
                     if (a.valid && light_pdf > 0.0f) {
                         const float3 light_radiance = f3(l.color[0], l.color[1], l.color[2]) * (l.power * a.eval_factor);

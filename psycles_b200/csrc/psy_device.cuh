@@ -960,6 +960,102 @@ struct AnalyticSample {
     float distance, pdf, eval_factor;
 };
 
+// ---------------------------------------------------------- sphere lamps
+// sin_squared_to_one_minus_cosine (include/psycles/luisa/cycles_sample_mapping.h).
+__device__ __forceinline__ float sin2_to_one_minus_cos(float s2) {
+    return s2 > 0.0004f ? 1.0f - sqrtf(maxf_(1.0f - s2, 0.0f)) : 0.5f * s2;
+}
+
+// spot_one_minus_cosine_larger_spread (analytic_light_sampling.h:355-376); the
+// reciprocal square root is an IEEE 1/sqrt.
+__device__ __forceinline__ float spot_spread_cap(const psy_light_desc &l) {
+    const float t = tan_(0.5f * l.spot_angle);
+    const float ts2 = maxf_(l.axis_scale[0] * l.axis_scale[0], l.axis_scale[1] * l.axis_scale[1]);
+    const float as2 = l.axis_scale[2] * l.axis_scale[2];
+    return 1.0f - 1.0f / sqrtf(1.0f + t * t * ts2 / maxf_(as2, 1.0e-30f));
+}
+
+struct SphereHit {
+    bool valid;
+    float distance;
+    f3 position;
+};
+
+// intersect_sphere (analytic_light_sampling.h:192-239): open interval, the
+// far side only from inside.
+__device__ __forceinline__ SphereHit intersect_sphere(f3 o, f3 d, float tmin, float tmax, f3 c, float r) {
+    const f3 co = c - o;
+    const float r2 = r * r;
+    const float cd2 = dot(co, co);
+    const float pd = dot(co, d);
+    const f3 perp = co - d * pd;
+    const float pp2 = dot(perp, perp);
+    const float dist = pd - copysignf(sqrtf(maxf_(r2 - pp2, 0.0f)), cd2 - r2);
+    const bool valid = !(cd2 > r2 && pd < 0.0f) && pp2 <= r2 && dist > tmin && dist < tmax;
+    return {valid, dist, o + d * dist};
+}
+
+// sample_uniform_sphere (cycles_sample_mapping.h:380-387).
+__device__ __forceinline__ f3 sample_uniform_sphere(f2 u) {
+    const float z = 1.0f - 2.0f * u.x;
+    const float r = sqrtf(maxf_(1.0f - z * z, 0.0f));
+    const float phi = 2.0f * kPi * u.y;
+    return mk3(r * cos_(phi), r * sin_(phi), z);
+}
+
+// sample_sphere_geometry (analytic_light_sampling.h:430-548): a cone towards
+// the sphere from outside (optionally around another axis, then intersected),
+// the shading hemisphere or the whole sphere from inside.
+__device__ __forceinline__ AnalyticSample sample_sphere(f3 reference, f3 n, bool transmission, f3 center, float r,
+                                                        f3 outside_axis, float outside_omc, bool intersect_sampled,
+                                                        f2 rnd) {
+    AnalyticSample out;
+    const float r2 = r * r;
+    f3 ln = reference - center;
+    const float cd2 = dot(ln, ln);
+    const float cd = sqrtf(maxf_(cd2, 1.0e-30f));
+    ln = ln / cd;
+    const bool outside = cd2 > r2;
+    f3 dir = mk3(0.0f);
+    float cosine = 1.0f, pdf = 0.0f, dist = 0.0f;
+    f3 pos = reference;
+    bool known = false;
+    bool valid = r > 0.0f && cd2 > 0.0f;
+    if (outside) {
+        const ConeSample c = sample_uniform_cone(outside_axis, outside_omc, rnd);
+        dir = c.direction;
+        cosine = c.cosine;
+        pdf = c.pdf;
+        if (intersect_sampled) {
+            const SphereHit h = intersect_sphere(reference, dir, 0.0f, 1.0e30f, center, r);
+            valid = valid && h.valid;
+            dist = h.distance;
+            pos = h.position;
+            known = h.valid;
+        }
+    } else {
+        if (transmission) {
+            dir = sample_uniform_sphere(rnd);
+            pdf = 0.5f * kInvTwoPi;
+        } else {
+            dir = sample_cosine_hemisphere(n, rnd, &pdf);
+        }
+        cosine = -dot(dir, ln);
+    }
+    if (!known) {
+        dist = cd * cosine - copysignf(sqrtf(maxf_(r2 - cd2 + cd2 * cosine * cosine, 0.0f)), cd2 - r2);
+        pos = reference + dir * dist;
+    }
+    const f3 normal = light_safe_normalize(pos - center, -dir);
+    out.valid = valid;
+    out.direction = dir;
+    out.position = normal * r + center;
+    out.distance = dist;
+    out.pdf = pdf;
+    out.eval_factor = 0.0f;
+    return out;
+}
+
 // rectangle_solid_angle_context (include/psycles/luisa/analytic_light_sampling.h:
 // Ureña et al. spherical rectangle seen from `reference`, with the planar pdf
 // limit for tiny or grazing rectangles).
@@ -1035,7 +1131,8 @@ __device__ __forceinline__ float spot_attenuation(const psy_light_desc &l, f3 fr
 
 // include/psycles/luisa/analytic_light_sampling.h:84-108 (distant),
 // :549-603 (disk), :856-896 (pdf / eval factor), :309-345 (spot profile).
-__device__ __noinline__ AnalyticSample sample_analytic(const psy_light_desc &l, f3 reference, f2 rnd) {
+__device__ __noinline__ AnalyticSample sample_analytic(const psy_light_desc &l, f3 reference, f3 shading_n,
+                                                       bool transmission, f2 rnd) {
     AnalyticSample out;
     const bool normalize_power = (l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u;
     if (l.type == PSY_LIGHT_DISTANT) {
@@ -1122,6 +1219,33 @@ __device__ __noinline__ AnalyticSample sample_analytic(const psy_light_desc &l, 
         out.eval_factor = factor;
         return out;
     }
+    if ((l.flags & PSY_LIGHT_FLAG_SPHERE) != 0u && l.radius > 0.0f) {
+        // sample_point_light / sample_spot_light, sphere geometry
+        // (analytic_light_sampling.h:898-1105)
+        const f3 center = ld3(l.position);
+        const f3 off = reference - center;
+        const float cd2 = dot(off, off);
+        const float r2 = l.radius * l.radius;
+        const f3 ln = light_safe_normalize(off, mk3(0.0f, 0.0f, -1.0f));
+        const float sphere_cap = sin2_to_one_minus_cos(r2 / maxf_(cd2, 1.0e-30f));
+        f3 axis = -ln;
+        float cap = sphere_cap;
+        bool spread = false;
+        if (l.type == PSY_LIGHT_SPOT) {
+            const float spot_cap = spot_spread_cap(l);
+            spread = cd2 > r2 && !(sphere_cap < spot_cap);
+            if (spread) {
+                axis = ld3(l.axis_z);
+                cap = spot_cap;
+            }
+        }
+        out = sample_sphere(reference, shading_n, transmission, center, l.radius, axis, cap, spread, rnd);
+        float eval = point_eval_factor(l);
+        if (l.type == PSY_LIGHT_SPOT && cd2 > r2) eval *= spot_attenuation(l, -out.direction);
+        out.eval_factor = eval;
+        if (l.type == PSY_LIGHT_SPOT) out.valid = out.valid && eval != 0.0f;
+        return out;
+    }
     const f3 center = ld3(l.position);
     f3 ln = reference - center;
     const float cd2 = dot(ln, ln);
@@ -1194,9 +1318,37 @@ __device__ __forceinline__ bool intersect_area_lamp(const psy_light_desc &l, f3 
 // for the oriented-disk geometry (radius > 0, not a sphere): the disk faces
 // the ray origin.
 __device__ __forceinline__ bool intersect_disk_lamp(const psy_light_desc &l, f3 o, f3 d, float tmin, float tmax,
-                                                    float &distance, float &pdf, float &eval) {
+                                                    f3 mis_n, bool had_transmission, float &distance, float &pdf,
+                                                    float &eval) {
     const f3 center = ld3(l.position);
     const f3 offset = o - center;
+    if ((l.flags & PSY_LIGHT_FLAG_SPHERE) != 0u) {
+        // intersect_point / intersect_spot, sphere geometry, with
+        // sphere_light_pdf (analytic_light_intersection.h:33-266,
+        // analytic_light_sampling.h:282-307)
+        if (!(l.radius > 0.0f)) return false;
+        const float cd2 = dot(offset, offset);
+        const float r2 = l.radius * l.radius;
+        float cap = sin2_to_one_minus_cos(r2 / maxf_(cd2, 1.0e-30f));
+        if (l.type == PSY_LIGHT_SPOT) cap = minf_(cap, spot_spread_cap(l));
+        const SphereHit h = intersect_sphere(o, d, tmin, tmax, center, l.radius);
+        if (!h.valid) return false;
+        distance = h.distance;
+        if (cd2 > r2) {
+            pdf = kInvTwoPi / maxf_(cap, 1.0e-30f);
+        } else if (had_transmission) {
+            pdf = 0.5f * kInvTwoPi;
+        } else {
+            const float c = dot(mis_n, d);
+            pdf = c > 0.0f ? c * kInvPi : 0.0f;
+        }
+        eval = point_eval_factor(l);
+        if (l.type == PSY_LIGHT_SPOT) {
+            if (cd2 > r2) eval *= spot_attenuation(l, -d);
+            if (!(dot(d, offset) < 0.0f)) return false;
+        }
+        return eval > 0.0f;
+    }
     const f3 ln = light_safe_normalize(offset, -d);
     const float plane = dot(offset, ln);
     const float cosine = dot(ln, -d);
@@ -1221,7 +1373,8 @@ __device__ __forceinline__ bool intersect_disk_lamp(const psy_light_desc &l, f3 
 // is a camera ray or the lamp takes part in MIS, and it is not the lamp the
 // previous event hit.
 __device__ __noinline__ LampHit closest_lamp(const SceneView &s, f3 o, f3 d, float tmin, float event_distance,
-                                                uint32_t ray_visibility, uint32_t excluded) {
+                                             uint32_t ray_visibility, uint32_t excluded, f3 mis_n,
+                                             bool had_transmission) {
     LampHit best{false, kInvalid, event_distance, 0.0f, 0.0f};
     const bool camera_path = (ray_visibility & PSY_VISIBILITY_CAMERA) != 0u;
     for (uint32_t k = 0; k < s.lamp_count; ++k) {
@@ -1240,7 +1393,8 @@ __device__ __noinline__ LampHit closest_lamp(const SceneView &s, f3 o, f3 d, flo
         if (!((l.visibility & ray_visibility) != 0u && (camera_path || use_mis) && li != excluded)) continue;
         float distance = 0.0f, pdf = 0.0f, eval = 0.0f;
         const bool hit = l.type == PSY_LIGHT_AREA ? intersect_area_lamp(l, o, d, tmin, best.distance, distance, pdf, eval)
-                                                  : intersect_disk_lamp(l, o, d, tmin, best.distance, distance, pdf, eval);
+                                                  : intersect_disk_lamp(l, o, d, tmin, best.distance, mis_n,
+                                                                        had_transmission, distance, pdf, eval);
         if (hit) best = LampHit{true, li, distance, pdf, eval};
     }
     return best;

@@ -799,8 +799,6 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
             return fail(PSY_ERROR_INVALID_ARGUMENT, "area light with an empty size");
         if (l.type > PSY_LIGHT_DISTANT) return fail(PSY_ERROR_INVALID_ARGUMENT, "unknown light type");
         if ((l.flags >> 16) != 0u) return fail(PSY_ERROR_INVALID_ARGUMENT, "reserved light flag bits are set");
-        if ((l.flags & PSY_LIGHT_FLAG_SPHERE) && l.radius > 0.0f)
-            return fail(PSY_ERROR_UNSUPPORTED, "spherical point lights are not available in this build");
     }
     auto sc = std::make_unique<psy_scene>();
     sc->context = ctx;

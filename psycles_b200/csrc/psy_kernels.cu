@@ -554,14 +554,14 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                 uint32_t excluded = kInvalid;
                 float tmin = ray.tmin;
                 for (uint32_t guard = 0; guard <= s.lamp_count && alive; ++guard) {
-                    const LampHit lh = closest_lamp(s, ray.o, ray.d, tmin, event_distance, ray_visibility, excluded);
+                    const float4 mn = b.mis_n[i];
+                    const LampHit lh = closest_lamp(s, ray.o, ray.d, tmin, event_distance, ray_visibility, excluded,
+                                                    mk3(mn.x, mn.y, mn.z), (ps.flag & kFlagMisHadTransmission) != 0u);
                     if (!lh.valid) break;
                     float selection_pdf = s.light_selection_pdf;
-                    if (p.use_light_tree) {
-                        const float4 mn = b.mis_n[i];
+                    if (p.use_light_tree)
                         selection_pdf = lt_pdf(s, s.triangle_emitters + lh.index, ray.o, mk3(mn.x, mn.y, mn.z),
                                                (ps.flag & kFlagMisHadTransmission) != 0u);
-                    }
                     const float light_pdf = lh.pdf * selection_pdf;
                     const bool competing = depth > 0u && !previous_delta;
                     const float w = forward_light_weight(p.direct_mode, previous_bsdf_pdf, light_pdf, competing,
@@ -626,7 +626,10 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                                                mk3(mn.x, mn.y, mn.z), (ps.flag & kFlagMisHadTransmission) != 0u);
                     }
                     const float light_pdf = emissive_forward_pdf(selection_pdf, mat.emission_sampling, ray.o,
-                                                                 sp.position, sp.wp0, sp.wp1, sp.wp2, sp.ng);
+                                                                 sp.position, sp.wp0, sp.wp1, sp.wp2,
+                                                                 // the geometric normal before the back-face
+                                                                 // flip (path_kernel_surface_shading.cpp:130-134)
+                                                                 sp.back_facing ? -sp.ng : sp.ng);
                     const bool available = light_pdf > 0.0f;
                     emission_weight = forward_light_weight(p.direct_mode, previous_bsdf_pdf, light_pdf, competing, available);
                 }
@@ -723,7 +726,9 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                             // AnalyticLightingComponent (src/luisa/path_kernel_nee_analytic.cpp:98-428)
                             const psy_light_desc &l = s.lights[selected.index];
                             if (!(depth > l.max_bounces)) {
-                                const AnalyticSample a = sample_analytic(l, sp.position, mk2(light_sample.x, light_sample.y));
+                                const AnalyticSample a =
+                                    sample_analytic(l, sp.position, sp.n, (runtime & kRuntimeBsdfHasTransmission) != 0u,
+                                                    mk2(light_sample.x, light_sample.y));
                                 const float light_pdf = a.pdf * selected.selection_pdf;
                                 if (a.valid && light_pdf > 0.0f) {
                                     const f3 light_radiance = ld3(l.color) * (l.power * a.eval_factor);

@@ -361,8 +361,11 @@ def procedural_scene(seed: int = 0, frequencies=(10, 14, 18, 22, 27, 32, 38, 44)
                 flags = _abi.LIGHT_FLAG_NORMALIZE
                 if lt == _abi.LIGHT_AREA and rng.random() < 0.5:
                     flags |= _abi.LIGHT_FLAG_ELLIPSE
-                # half of the point / spot lamps have a finite (disk) radius
+                # half of the point / spot lamps have a finite radius, as a
+                # disk or (LightDesc::is_sphere) a sphere
                 radius = float(rng.uniform(0.1, 0.5)) if rng.random() < 0.5 else 0.0
+                if lt in (_abi.LIGHT_POINT, _abi.LIGHT_SPOT) and radius > 0.0 and rng.random() < 0.5:
+                    flags |= _abi.LIGHT_FLAG_SPHERE
                 lights.append(Light(lt, color, float(rng.uniform(200.0, 800.0)), position=pos, radius=radius,
                                     axis_x=tuple(xf[:3, 0].tolist()), axis_y=tuple(xf[:3, 1].tolist()),
                                     axis_z=tuple(xf[:3, 2].tolist()),
@@ -468,6 +471,12 @@ def lamp_scene(seed: int = 0) -> Scene:
         Light(_abi.LIGHT_DISTANT, (1.0, 1.0, 0.9), 0.8, axis_z=(0.2, -0.9, -0.3), angle=math.radians(4.0)),
         Light(_abi.LIGHT_AREA, (1.0, 0.5, 0.5), 10.0, position=(0.0, 1.2, -4.0), size_u=1.0, size_v=1.0,
               axis_x=(1, 0, 0), axis_y=(0, 1, 0), axis_z=(0, 0, -1), use_mis=False),
+        # sphere lamps (LightDesc::is_sphere)
+        Light(_abi.LIGHT_POINT, (0.7, 1.0, 0.8), 50.0, position=(-0.8, 2.8, -1.5), radius=0.4,
+              flags=_abi.LIGHT_FLAG_NORMALIZE | _abi.LIGHT_FLAG_SPHERE),
+        Light(_abi.LIGHT_SPOT, (1.0, 0.9, 0.6), 70.0, position=(2.2, 3.2, 1.0), radius=0.35,
+              axis_x=(1, 0, 0), axis_y=(0, 0, 1), axis_z=(-0.3, 1, -0.2), spot_angle=math.radians(60), spot_smooth=0.2,
+              flags=_abi.LIGHT_FLAG_NORMALIZE | _abi.LIGHT_FLAG_SPHERE),
     ]
     cam = Camera(look_at((0.0, 2.0, 7.0), (0.0, 1.5, -1.0)), math.radians(45.0), math.radians(45.0), 0)
     return Scene(meshes, instances, mats, ls, cam, background=(0.05, 0.05, 0.08))
