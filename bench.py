@@ -253,16 +253,24 @@ def run_cuda(args) -> None:
     # e2e: host arrays -> compile_scene -> render -> passes in host memory
     e2e_ms = []
     d2h = 0
+    phases = {}
     for _ in range(max(1, min(args.steps, 2))):
         barrier()
         t0 = time.perf_counter()
         comp2 = backend.compile_scene(scene)
+        t1 = time.perf_counter()
         sess2 = backend.create_session(comp2.scene, settings())
         assert sess2.render_samples(SampleRange(0, args.spp, 0, args.spp))
+        t2 = time.perf_counter()
         d2h = 0
         for p in sess2.passes:
             d2h += sess2.read_pass(p.kind).nbytes
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        t3 = time.perf_counter()
+        e2e_ms.append((t3 - t0) * 1e3)
+        bs = comp2.scene.build_stats()
+        phases = {"compile_ms": (t1 - t0) * 1e3, "session_render_ms": (t2 - t1) * 1e3, "readback_ms": (t3 - t2) * 1e3,
+                  "build": {n: (round(getattr(bs, n), 3) if isinstance(getattr(bs, n), float) else getattr(bs, n))
+                            for n, _ in bs._fields_}}
         sess2.close()
         comp2.scene.close()
     e2e_s = max_over_ranks(statistics.mean(e2e_ms) / 1e3)
@@ -279,7 +287,8 @@ def run_cuda(args) -> None:
         "config": workload_config(args, scene),
         "rays_per_s": rays_per_s, "wall_s": wall,
         "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": scene_bytes(scene),
-                "d2h_bytes_per_step": d2h, "includes": "compile_scene (upload + BVH build), render, pass readback"},
+                "d2h_bytes_per_step": d2h, "includes": "compile_scene (upload + BVH build), render, pass readback",
+                "phases": phases},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
         "tuning": __import__("psycles_b200.autotune", fromlist=["get_tuning"]).get_tuning(backend),

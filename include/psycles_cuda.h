@@ -269,6 +269,24 @@ void psy_scene_destroy(psy_scene *scene);
 /* CompiledScene::source_revision (render.h:153). */
 uint64_t psy_scene_source_revision(const psy_scene *scene);
 
+/* Wall-clock phases of psy_scene_compile, the BVH build and upload times
+ * the reference reports apart from render time (VALIDATION.md:751-755).
+ * The light tree is built the first time a session of the scene asks for
+ * it (use_light_tree), and again after a parameter edit of an emissive
+ * material once built; light_tree_ms is its latest build. */
+typedef struct psy_scene_build_stats {
+    double total_ms;        /* psy_scene_compile, validation to upload */
+    double validate_ms;
+    double blas_ms;         /* per-mesh BVH builds, parallel over meshes */
+    double tlas_ms;
+    double emitters_ms;     /* materials, emissive triangles, flat distribution */
+    double upload_ms;
+    double light_tree_ms;
+    uint32_t build_threads; /* host threads of the BLAS builds */
+    uint32_t light_tree_builds;
+} psy_scene_build_stats;
+psy_status psy_scene_get_build_stats(const psy_scene *scene, psy_scene_build_stats *out);
+
 /* Parameter-only material edit: the MaterialLibrary `parameters_rebound`
  * outcome (src/compiler/material_library.cpp:51-97) applied on the device.
  * Rewrites the material's parameter block in place; no BVH or program

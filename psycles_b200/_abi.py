@@ -170,6 +170,12 @@ class ServerStats(ctypes.Structure):
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
 
 
+class SceneBuildStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("total_ms", "validate_ms", "blas_ms", "tlas_ms", "emitters_ms",
+                                               "upload_ms", "light_tree_ms")] + [
+        ("build_threads", ctypes.c_uint32), ("light_tree_builds", ctypes.c_uint32)]
+
+
 # Entry points declared by include/psycles_cuda.h: (name, restype, argtypes).
 SIGNATURES = [
     ("psy_last_error", ctypes.c_char_p, []),
@@ -180,6 +186,7 @@ SIGNATURES = [
     ("psy_scene_compile", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SceneDesc), ctypes.POINTER(ctypes.c_void_p)]),
     ("psy_scene_destroy", None, [ctypes.c_void_p]),
     ("psy_scene_source_revision", ctypes.c_uint64, [ctypes.c_void_p]),
+    ("psy_scene_get_build_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SceneBuildStats)]),
     ("psy_scene_rebind_parameters", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_uint32, c_float_p, ctypes.c_uint32, c_float_p, ctypes.c_uint32]),
     ("psy_session_create", ctypes.c_int,

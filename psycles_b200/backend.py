@@ -119,6 +119,15 @@ class CompiledScene:
     def source_revision(self) -> int:
         return int(self.lib.psy_scene_source_revision(self.handle))
 
+    def build_stats(self) -> _abi.SceneBuildStats:
+        """Phase times of compile_scene and of the latest light-tree build."""
+        st = _abi.SceneBuildStats()
+        _abi.check(self.lib.psy_scene_get_build_stats(self.handle, ctypes.byref(st)))
+        return st
+
+    def device_bytes(self) -> int:
+        return int(self.lib.psy_scene_device_bytes(self.handle))
+
     def rebind_parameters(self, material: int, scalars: np.ndarray, vectors: np.ndarray) -> None:
         """Parameter-only edit: rewrites one material's parameter block on the device."""
         sc = np.ascontiguousarray(scalars, dtype=np.float32).reshape(-1)

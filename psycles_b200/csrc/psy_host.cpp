@@ -28,6 +28,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace psy::host {
@@ -541,6 +542,20 @@ struct Builder {
 
 namespace {
 
+// Light selection of a render from the scene's current tables: the tree is
+// used only where the scene has one; NEE runs only when a light can be
+// picked and the mode is not forward path tracing, and without NEE every
+// emitter is weighted as forward path tracing
+// (src/luisa/path_tracer_kernel.cpp:206-223).  Re-applied before every
+// render, so a tree rebuilt by a parameter edit is picked up.
+void apply_light_selection(psy::RenderParams &p, const psy_render_settings &r, const psy::SceneView &sv) {
+    p.use_light_tree = (r.use_light_tree && sv.lt_node_count > 0u && sv.lt_emitter_count > 0u) ? 1u : 0u;
+    const bool available = p.use_light_tree ? sv.lt_emitter_count > 0u : sv.emitter_count > 0u;
+    const bool nee = r.next_event_estimation != 0u && r.direct_light_sampling != PSY_DIRECT_LIGHT_FORWARD && available;
+    p.nee = nee ? 1u : 0u;
+    p.direct_mode = nee ? r.direct_light_sampling : PSY_DIRECT_LIGHT_FORWARD;
+}
+
 psy_status derive_params(psy_session *s, const psy_render_settings &r) {
     if (r.full_width == 0u || r.full_height == 0u)
         return fail(PSY_ERROR_INVALID_ARGUMENT, "render extent must be non-empty");
@@ -576,16 +591,11 @@ psy_status derive_params(psy_session *s, const psy_render_settings &r) {
     p.clamp_indirect = r.sample_clamp_indirect;
     p.inv_rr_threshold = (!r.use_light_tree && r.light_sampling_threshold > 0.0f)
                              ? r.film_exposure / r.light_sampling_threshold : 0.0f;
-    // the tree is used only where the scene has one; NEE runs only when a
-    // light can be picked and the mode is not forward path tracing, and
-    // without NEE every emitter is weighted as forward path tracing
-    // (src/luisa/path_tracer_kernel.cpp:206-223)
-    const psy::SceneView &sv = s->scene->view;
-    p.use_light_tree = (r.use_light_tree && sv.lt_node_count > 0u && sv.lt_emitter_count > 0u) ? 1u : 0u;
-    const bool available = p.use_light_tree ? sv.lt_emitter_count > 0u : sv.emitter_count > 0u;
-    const bool nee = r.next_event_estimation != 0u && r.direct_light_sampling != PSY_DIRECT_LIGHT_FORWARD && available;
-    p.nee = nee ? 1u : 0u;
-    p.direct_mode = nee ? r.direct_light_sampling : PSY_DIRECT_LIGHT_FORWARD;
+    if (r.use_light_tree) {
+        const psy_status built = ensure_light_tree(s->scene);
+        if (built != PSY_OK) return built;
+    }
+    apply_light_selection(p, r, s->scene->view);
     // camera parameters (src/luisa/path_tracer_kernel.cpp:225-280)
     const psy_camera_desc &c = s->has_camera ? s->camera : s->scene->camera;
     const float aspect = static_cast<float>(std::max(r.full_width, 1u)) / static_cast<float>(std::max(r.full_height, 1u));
@@ -651,7 +661,135 @@ void emission_estimate(const psy_material_desc &m, float out[3]) {
     for (int k = 0; k < 3; ++k) out[k] = m.root < est.size() ? est[m.root][k] : 0.0f;
 }
 
+// Runs body(i) for every i in [0, n) on up to 32 host threads that pull
+// indices from a shared counter; `threads` receives the count used.  An
+// exception in a body (out of host memory) becomes PSY_ERROR_OUT_OF_MEMORY.
+template <typename F>
+psy_status parallel_for(uint32_t n, uint32_t *threads, F &&body) {
+    const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint32_t count = std::max(1u, std::min({hw, n, 32u}));
+    std::atomic<uint32_t> next{0u};
+    std::atomic<bool> failed{false};
+    auto worker = [&]() {
+        for (uint32_t i; !failed.load() && (i = next.fetch_add(1u)) < n;) {
+            try {
+                body(i);
+            } catch (...) {
+                failed.store(true);
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < count; ++t) pool.emplace_back(worker);
+    worker();
+    for (std::thread &t : pool) t.join();
+    if (threads) *threads = count;
+    return failed.load() ? fail(PSY_ERROR_OUT_OF_MEMORY, "host memory exhausted while building the scene") : PSY_OK;
+}
+
+// The many-light tree over the scene's emitter population -- emissive
+// triangles in emitter order, then the analytic lights -- built from the
+// host copies and uploaded (src/luisa/path_tracer_light_sampling_scene.cpp:
+// 160-240).  A tree whose root carries no energy is left empty, and
+// sessions then select lights from the flat distribution.
+psy_status build_light_tree(psy_scene *sc) {
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<psy::LtNodeGpu> lt_nodes;
+    std::vector<psy::LtEmitterGpu> lt_emitters;
+    std::vector<uint2> lt_mapping;
+    std::vector<uint4> lt_lookup;
+    uint32_t lt_root = 0u;
+    const std::vector<psy::EmitterGpu> &emitters = sc->emitters_host;
+    const uint32_t tri_n = uint32_t(emitters.size()), light_n = uint32_t(sc->lights_host.size());
+    // estimate_surface_emission per material (a property of the program and
+    // its parameter block)
+    std::vector<std::array<float, 3>> estimates(sc->materials.size());
+    for (size_t i = 0; i < sc->materials.size(); ++i) {
+        const psy::MaterialGpu &g = sc->materials[i];
+        psy_material_desc m{};
+        m.closures = sc->code_host.data() + g.code_offset;
+        m.closure_count = g.code_count;
+        m.root = g.root;
+        m.scalars = sc->scalars.data() + g.scalar_offset;
+        m.vectors = sc->vectors.data() + 3ull * g.vector_offset;
+        if (g.has_emission) emission_estimate(m, estimates[i].data());
+        else estimates[i] = {0.0f, 0.0f, 0.0f};
+    }
+    std::vector<psy::LtEmitter> source;
+    source.reserve(tri_n + light_n);
+    for (uint32_t i = 0; i < tri_n; ++i) {
+        const psy::EmitterGpu &e = emitters[i];
+        source.push_back(psy::lt_triangle_emitter(i, e.p0, e.p1, e.p2, estimates[e.material].data(), e.emission_sampling,
+                                                  sc->instance_mirrored[e.object] != 0u));
+    }
+    for (uint32_t i = 0; i < light_n; ++i) source.push_back(psy::lt_analytic_emitter(tri_n + i, &sc->lights_host[i]));
+    if (!source.empty()) {
+        const psy::LightTree tree = psy::lt_build(source, 8u);
+        const bool usable = tree.root < tree.nodes.size() && tree.emitter_to_tree.size() == tree.emitters.size() &&
+                            tree.nodes[tree.root].measure.energy > 0.0f;
+        if (usable) {
+            auto flags = [](const psy::LtMeasure &m, bool distant) {
+                return (!m.bounds.empty ? psy::kLtFlagBounds : 0u) | (!m.orientation.empty ? psy::kLtFlagOrientation : 0u) |
+                       (distant ? psy::kLtFlagDistant : 0u);
+            };
+            auto pack = [](const psy::LtMeasure &m, float4 &a, float4 &b, float4 &c) {
+                a = make_float4(m.bounds.lo[0], m.bounds.lo[1], m.bounds.lo[2], m.energy);
+                b = make_float4(m.bounds.hi[0], m.bounds.hi[1], m.bounds.hi[2], m.orientation.theta_o);
+                c = make_float4(m.orientation.axis[0], m.orientation.axis[1], m.orientation.axis[2], m.orientation.theta_e);
+            };
+            lt_nodes.reserve(tree.nodes.size());
+            for (const psy::LtNode &n : tree.nodes) {
+                psy::LtNodeGpu g{};
+                pack(n.measure, g.min_energy, g.max_theta_o, g.axis_theta_e);
+                g.topology = make_uint4(n.parent, n.left, n.right, n.kind);
+                g.emitters = make_uint4(n.first, n.count, flags(n.measure, n.kind == psy::kLtDistant), 0u);
+                lt_nodes.push_back(g);
+            }
+            lt_emitters.reserve(tree.emitters.size());
+            for (const psy::LtEmitter &e : tree.emitters) {
+                psy::LtEmitterGpu g{};
+                pack(e.measure, g.min_energy, g.max_theta_o, g.axis_theta_e);
+                g.identity = make_uint4(e.emitter_id, flags(e.measure, e.distant), 0u, 0u);
+                lt_emitters.push_back(g);
+            }
+            for (size_t id = 0; id < tree.emitters.size(); ++id)
+                lt_mapping.push_back(make_uint2(tree.emitter_to_tree[id], tree.emitter_to_leaf[id]));
+            for (uint32_t i = 0; i < tri_n; ++i)
+                lt_lookup.push_back(make_uint4(emitters[i].object, emitters[i].cycles_prim, i, 0u));
+            std::sort(lt_lookup.begin(), lt_lookup.end(), [](const uint4 &a, const uint4 &b) {
+                return a.x < b.x || (a.x == b.x && (a.y < b.y || (a.y == b.y && a.z < b.z)));
+            });
+            lt_root = tree.root;
+        }
+    }
+    cudaStream_t st = sc->context->stream;
+    PSY_CUDA_TRY(cudaSetDevice(sc->context->device));
+    PSY_CUDA_TRY(sc->lt_nodes.upload(lt_nodes, st));
+    PSY_CUDA_TRY(sc->lt_emitters.upload(lt_emitters, st));
+    PSY_CUDA_TRY(sc->lt_mapping.upload(lt_mapping, st));
+    PSY_CUDA_TRY(sc->lt_lookup.upload(lt_lookup, st));
+    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    psy::SceneView &v = sc->view;
+    v.lt_nodes = sc->lt_nodes.as<psy::LtNodeGpu>();
+    v.lt_emitters = sc->lt_emitters.as<psy::LtEmitterGpu>();
+    v.lt_mapping = sc->lt_mapping.as<uint2>();
+    v.lt_lookup = sc->lt_lookup.as<uint4>();
+    v.lt_node_count = uint32_t(lt_nodes.size());
+    v.lt_emitter_count = uint32_t(lt_emitters.size());
+    v.lt_lookup_count = uint32_t(lt_lookup.size());
+    v.lt_root = lt_root;
+    sc->light_tree_built = true;
+    sc->stats.light_tree_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    sc->stats.light_tree_builds++;
+    return PSY_OK;
+}
+
 }  // namespace
+
+psy_status psy::host::ensure_light_tree(psy_scene *sc) {
+    std::lock_guard<std::mutex> lock(sc->light_tree_mutex);
+    return sc->light_tree_built ? PSY_OK : build_light_tree(sc);
+}
 
 // ================================================================== C ABI
 
@@ -805,14 +943,53 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     sc->revision = d->revision;
     sc->camera = d->camera;
     cudaStream_t st = ctx->stream;
+    auto t_phase = std::chrono::steady_clock::now();
+    auto lap = [&t_phase]() {
+        const auto now = std::chrono::steady_clock::now();
+        const double ms = std::chrono::duration<double, std::milli>(now - t_phase).count();
+        t_phase = now;
+        return ms;
+    };
+    sc->stats.validate_ms = lap();
 
-    // ---- meshes: flatten, BLAS per mesh
+    // ---- meshes: flatten, then one BLAS per mesh (meshes build in parallel;
+    // each build is sequential and deterministic, so the result does not
+    // depend on the thread count)
     std::vector<psy::MeshGpu> meshes(d->mesh_count);
     std::vector<float> positions, normals;
     std::vector<uint32_t> indices, tri_materials;
     std::vector<psy::WideNodeGpu> blas;
     std::vector<float4> tris;
     std::vector<Box> mesh_boxes(d->mesh_count);
+    std::vector<std::vector<psy::WideNodeGpu>> mesh_wide(d->mesh_count);
+    std::vector<std::vector<uint32_t>> mesh_order(d->mesh_count);
+    {
+        std::vector<uint32_t> by_size(d->mesh_count);
+        for (uint32_t i = 0; i < d->mesh_count; ++i) by_size[i] = i;
+        std::stable_sort(by_size.begin(), by_size.end(), [d](uint32_t a, uint32_t b) {
+            return d->meshes[a].triangle_count > d->meshes[b].triangle_count;
+        });
+        const psy_status built = parallel_for(d->mesh_count, &sc->stats.build_threads, [&](uint32_t job) {
+            const uint32_t i = by_size[job];
+            const psy_mesh_desc &m = d->meshes[i];
+            Builder bld;
+            bld.prims.resize(m.triangle_count);
+            for (uint32_t k = 0; k < m.triangle_count; ++k) {
+                Prim &p = bld.prims[k];
+                for (int c = 0; c < 3; ++c) {
+                    const float *v = m.positions + 3ull * m.indices[3ull * k + c];
+                    p.box.grow(v[0], v[1], v[2]);
+                }
+                for (int a = 0; a < 3; ++a) p.c[a] = 0.5 * (p.box.lo[a] + p.box.hi[a]);
+                p.id = k;
+            }
+            mesh_boxes[i] = bld.build_root();
+            mesh_wide[i] = bld.widen();
+            mesh_order[i].resize(bld.prims.size());
+            for (size_t k = 0; k < bld.prims.size(); ++k) mesh_order[i][k] = bld.prims[k].id;
+        });
+        if (built != PSY_OK) return built;
+    }
     uint32_t prim_offset = 0;
     for (uint32_t i = 0; i < d->mesh_count; ++i) {
         const psy_mesh_desc &m = d->meshes[i];
@@ -833,33 +1010,22 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         } else {
             g.material_offset = psy::kInvalidId;
         }
-        Builder bld;
-        bld.prims.resize(m.triangle_count);
-        for (uint32_t k = 0; k < m.triangle_count; ++k) {
-            Prim &p = bld.prims[k];
-            for (int c = 0; c < 3; ++c) {
-                const float *v = m.positions + 3ull * m.indices[3ull * k + c];
-                p.box.grow(v[0], v[1], v[2]);
-            }
-            for (int a = 0; a < 3; ++a) p.c[a] = 0.5 * (p.box.lo[a] + p.box.hi[a]);
-            p.id = k;
-        }
-        mesh_boxes[i] = bld.build_root();
         g.node_offset = uint32_t(blas.size());
         g.tri_offset = uint32_t(tris.size() / 3u);
-        const std::vector<psy::WideNodeGpu> wide = bld.widen();
-        blas.insert(blas.end(), wide.begin(), wide.end());
-        for (const Prim &p : bld.prims) {
+        blas.insert(blas.end(), mesh_wide[i].begin(), mesh_wide[i].end());
+        std::vector<psy::WideNodeGpu>().swap(mesh_wide[i]);
+        for (const uint32_t id : mesh_order[i]) {
             for (int c = 0; c < 3; ++c) {
-                const float *v = m.positions + 3ull * m.indices[3ull * p.id + c];
+                const float *v = m.positions + 3ull * m.indices[3ull * id + c];
                 float w = 0.0f;
-                if (c == 0) std::memcpy(&w, &p.id, 4);
+                if (c == 0) std::memcpy(&w, &id, 4);
                 tris.push_back(make_float4(v[0], v[1], v[2], w));
             }
         }
         sc->triangle_count += m.triangle_count;
     }
     if (blas.empty()) blas.push_back({});
+    sc->stats.blas_ms = lap();
 
     // ---- instances + TLAS
     std::vector<psy::InstanceGpu> instances(d->instance_count);
@@ -907,6 +1073,10 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         tl.prims.push_back(p);
     }
     tl.build_root();
+    sc->instance_mirrored.resize(d->instance_count);
+    for (uint32_t i = 0; i < d->instance_count; ++i)
+        sc->instance_mirrored[i] = dt(o2w[i].c0, crs(o2w[i].c1, o2w[i].c2)) < 0.0f ? 1u : 0u;
+    sc->stats.tlas_ms = lap();
 
     // ---- materials and parameter blocks
     std::vector<psy_closure_instruction> code;
@@ -1023,65 +1193,10 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         if (mis && l.type != PSY_LIGHT_DISTANT) l.flags |= psy::kLightFlagForward;
     }
 
-    // ---- many-light tree over the same emitter population
-    // (src/luisa/path_tracer_light_sampling_scene.cpp:160-240)
-    std::vector<psy::LtNodeGpu> lt_nodes;
-    std::vector<psy::LtEmitterGpu> lt_emitters;
-    std::vector<uint2> lt_mapping;
-    std::vector<uint4> lt_lookup;
-    uint32_t lt_root = 0u;
-    {
-        std::vector<psy::LtEmitter> source;
-        source.reserve(emitters.size() + lights.size());
-        for (uint32_t i = 0; i < tri_n; ++i) {
-            const psy::EmitterGpu &e = emitters[i];
-            float estimate[3] = {0.0f, 0.0f, 0.0f};
-            const psy_material_desc &m = d->materials[e.material];
-            emission_estimate(m, estimate);
-            const M34 &xf = o2w[e.object];
-            const float det = dt(xf.c0, crs(xf.c1, xf.c2));
-            source.push_back(psy::lt_triangle_emitter(i, e.p0, e.p1, e.p2, estimate, e.emission_sampling, det < 0.0f));
-        }
-        for (uint32_t i = 0; i < light_n; ++i) source.push_back(psy::lt_analytic_emitter(tri_n + i, &lights[i]));
-        if (!source.empty()) {
-            const psy::LightTree tree = psy::lt_build(source, 8u);
-            const bool usable = tree.root < tree.nodes.size() && tree.emitter_to_tree.size() == tree.emitters.size() &&
-                                tree.nodes[tree.root].measure.energy > 0.0f;
-            if (usable) {
-                auto flags = [](const psy::LtMeasure &m, bool distant) {
-                    return (!m.bounds.empty ? psy::kLtFlagBounds : 0u) |
-                           (!m.orientation.empty ? psy::kLtFlagOrientation : 0u) | (distant ? psy::kLtFlagDistant : 0u);
-                };
-                auto pack = [](const psy::LtMeasure &m, float4 &a, float4 &b, float4 &c) {
-                    a = make_float4(m.bounds.lo[0], m.bounds.lo[1], m.bounds.lo[2], m.energy);
-                    b = make_float4(m.bounds.hi[0], m.bounds.hi[1], m.bounds.hi[2], m.orientation.theta_o);
-                    c = make_float4(m.orientation.axis[0], m.orientation.axis[1], m.orientation.axis[2],
-                                    m.orientation.theta_e);
-                };
-                for (const psy::LtNode &n : tree.nodes) {
-                    psy::LtNodeGpu g{};
-                    pack(n.measure, g.min_energy, g.max_theta_o, g.axis_theta_e);
-                    g.topology = make_uint4(n.parent, n.left, n.right, n.kind);
-                    g.emitters = make_uint4(n.first, n.count, flags(n.measure, n.kind == psy::kLtDistant), 0u);
-                    lt_nodes.push_back(g);
-                }
-                for (const psy::LtEmitter &e : tree.emitters) {
-                    psy::LtEmitterGpu g{};
-                    pack(e.measure, g.min_energy, g.max_theta_o, g.axis_theta_e);
-                    g.identity = make_uint4(e.emitter_id, flags(e.measure, e.distant), 0u, 0u);
-                    lt_emitters.push_back(g);
-                }
-                for (size_t id = 0; id < tree.emitters.size(); ++id)
-                    lt_mapping.push_back(make_uint2(tree.emitter_to_tree[id], tree.emitter_to_leaf[id]));
-                for (uint32_t i = 0; i < tri_n; ++i)
-                    lt_lookup.push_back(make_uint4(emitters[i].object, emitters[i].cycles_prim, i, 0u));
-                std::sort(lt_lookup.begin(), lt_lookup.end(), [](const uint4 &a, const uint4 &b) {
-                    return a.x < b.x || (a.x == b.x && (a.y < b.y || (a.y == b.y && a.z < b.z)));
-                });
-                lt_root = tree.root;
-            }
-        }
-    }
+    sc->code_host = code;
+    sc->emitters_host = emitters;
+    sc->lights_host = lights;
+    sc->stats.emitters_ms = lap();
 
     // ---- upload
     PSY_CUDA_TRY(sc->tlas.upload(tl.widen(), st));
@@ -1125,10 +1240,6 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     }
     PSY_CUDA_TRY(sc->lamp_bounds.upload(lamp_bounds, st));
     PSY_CUDA_TRY(sc->lamp_ids.upload(lamp_ids, st));
-    PSY_CUDA_TRY(sc->lt_nodes.upload(lt_nodes, st));
-    PSY_CUDA_TRY(sc->lt_emitters.upload(lt_emitters, st));
-    PSY_CUDA_TRY(sc->lt_mapping.upload(lt_mapping, st));
-    PSY_CUDA_TRY(sc->lt_lookup.upload(lt_lookup, st));
     PSY_CUDA_TRY(cudaStreamSynchronize(st));
     psy::SceneView &v = sc->view;
     v.tlas = sc->tlas.as<psy::WideNodeGpu>();
@@ -1161,15 +1272,9 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     v.background[2] = d->background[2];
     v.world_visibility = d->world_visibility;
     v.any_transparent = any_transparent ? 1u : 0u;
-    v.lt_nodes = sc->lt_nodes.as<psy::LtNodeGpu>();
-    v.lt_emitters = sc->lt_emitters.as<psy::LtEmitterGpu>();
-    v.lt_mapping = sc->lt_mapping.as<uint2>();
-    v.lt_lookup = sc->lt_lookup.as<uint4>();
-    v.lt_node_count = uint32_t(lt_nodes.size());
-    v.lt_emitter_count = uint32_t(lt_emitters.size());
-    v.lt_lookup_count = uint32_t(lt_lookup.size());
-    v.lt_root = lt_root;
-    sc->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
+    // the light tree is built on first use (ensure_light_tree)
+    sc->stats.upload_ms = lap();
+    sc->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
     *out = sc.release();
     return PSY_OK;
 }
@@ -1207,6 +1312,18 @@ psy_status psy_scene_rebind_parameters(psy_scene *s, uint32_t material, const fl
                                      sizeof(float) * 3u * vector_count, cudaMemcpyHostToDevice, st));
     }
     PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    // the light tree's energies follow the emission estimates: rebuild a
+    // built tree when an emissive material changes, as a recompile would
+    if (m.has_emission) {
+        std::lock_guard<std::mutex> lock(s->light_tree_mutex);
+        if (s->light_tree_built) return build_light_tree(s);
+    }
+    return PSY_OK;
+}
+
+psy_status psy_scene_get_build_stats(const psy_scene *s, psy_scene_build_stats *out) {
+    if (!s || !out) return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = s->stats;
     return PSY_OK;
 }
 
@@ -1335,6 +1452,7 @@ psy_status psy::host::prepare_render(psy_session *s, uint32_t first, uint32_t co
     }
     s->total = total;
     *out = s->params;
+    apply_light_selection(*out, s->settings, s->scene->view);
     out->sobol = s->sobol.as<float4>();
     out->sobol_size = s->sobol_size;
     return PSY_OK;
@@ -1529,6 +1647,7 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
     // before it is read within the call
     PSY_CUDA_TRY(cudaMemsetAsync(ray_stats, 0, 2 * sizeof(unsigned long long), st));
     psy::RenderParams p = s->params;
+    apply_light_selection(p, s->settings, s->scene->view);
     p.sobol = sobol;
     p.sobol_size = psy::kStaticSobolSize;
     s->total = total;
@@ -1672,6 +1791,8 @@ psy_status psy_debug_light_tree(psy_scene *scene, const float *queries, const ui
                                 uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf) {
     if (!scene || !queries || !pdf_emitters || !out_emitters || !out_sample_pdf || !out_reverse_pdf)
         return fail(PSY_ERROR_INVALID_ARGUMENT, "null argument");
+    const psy_status built = ensure_light_tree(scene);
+    if (built != PSY_OK) return built;
     if (scene->view.lt_node_count == 0u || scene->view.lt_emitter_count == 0u)
         return fail(PSY_ERROR_UNSUPPORTED, "scene has no usable light tree");
     if (count == 0u) return PSY_OK;

@@ -33,6 +33,10 @@ psy_status prepare_render(psy_session *s, uint32_t first, uint32_t count, uint32
 // Device bytes a compiled scene holds (geometry, BVH, materials, lights, tree).
 uint64_t scene_device_bytes(const psy_scene *s);
 
+// Builds the scene's many-light tree unless it is built already (it is built
+// on first use, not by psy_scene_compile).
+psy_status ensure_light_tree(psy_scene *s);
+
 // The job record of a session for a multi-job wavefront.
 JobGpu session_job(const psy_session *s, const RenderParams &p);
 
@@ -111,7 +115,16 @@ struct psy_scene {
         lt_lookup;
     psy::SceneView view{};
     uint64_t triangle_count = 0;
-    double build_ms = 0.0;
+    psy_scene_build_stats stats{};
+    // What the light tree is built from, kept on the host: it is built on
+    // first use (a session with use_light_tree) and rebuilt when a
+    // parameter edit changes an emissive material's estimate.
+    std::vector<psy::EmitterGpu> emitters_host;
+    std::vector<psy_light_desc> lights_host;
+    std::vector<psy_closure_instruction> code_host;
+    std::vector<uint8_t> instance_mirrored;  // object-to-world determinant < 0
+    std::mutex light_tree_mutex;
+    bool light_tree_built = false;
 };
 
 struct psy_session {

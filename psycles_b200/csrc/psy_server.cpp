@@ -127,7 +127,24 @@ struct psy_server {
                 continue;
             }
             Job &j = *it->second;
-            const uint64_t scene_extra = scene_bytes.count(j.scene) ? 0u : psy_scene_device_bytes(j.scene);
+            // a job that selects lights from the tree builds it first, so
+            // its bytes are counted with the scene's
+            if (j.settings.use_light_tree) {
+                const psy_status built = ensure_light_tree(j.scene);
+                if (built != PSY_OK) {
+                    j.state = PSY_JOB_FAILED;
+                    j.status = built;
+                    j.done_ms = now_ms();
+                    ++jobs_failed;
+                    fifo.pop_front();
+                    done_cv.notify_all();
+                    continue;
+                }
+            }
+            const uint64_t scene_now = psy_scene_device_bytes(j.scene);
+            const auto counted = scene_bytes.find(j.scene);
+            const uint64_t scene_extra =
+                counted == scene_bytes.end() ? scene_now : scene_now - std::min(scene_now, counted->second);
             const uint64_t need = j.bytes + scene_extra;
             uint64_t resident = fixed_bytes;
             for (const auto &kv : scene_bytes) resident += kv.second;
@@ -164,7 +181,7 @@ struct psy_server {
                 continue;
             }
             free_slots.pop_back();
-            if (scene_extra) scene_bytes[j.scene] = scene_extra;
+            if (scene_extra) scene_bytes[j.scene] = scene_now;
             bytes_in_use += need;
             bytes_peak = std::max(bytes_peak, bytes_in_use);
             j.session = s;

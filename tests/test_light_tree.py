@@ -170,3 +170,39 @@ def test_tree_trace_light_picks_bit_exact(backend):
             g, o = gt.events[k], ot.events[k]
             assert (g.light_kind, g.light_index) == (o.light_kind, o.light_index), (x, y, s, k)
         assert np.allclose(np.array(gt.radiance), np.array(ot.radiance), rtol=2e-6, atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_tree_built_on_first_use_and_rebuilt_after_emission_edit(backend):
+    """compile_scene leaves the tree unbuilt; the first session that selects
+    lights from it builds it.  A parameter edit of an emissive material
+    rebuilds a built tree, and the render afterwards equals a render of the
+    scene compiled with the edited parameters, bit for bit."""
+    import copy
+    scene = tree_scene_small()
+    st = scenes.render_settings(64, 48, max_bounces=4, use_light_tree=1)
+    comp = backend.compile_scene(scene).scene
+    assert comp.build_stats().light_tree_builds == 0
+    flat = backend.create_session(comp, scenes.render_settings(64, 48, max_bounces=4))
+    assert flat.render_samples(SampleRange(0, 1, 0, 1))
+    assert comp.build_stats().light_tree_builds == 0
+    before_bytes = comp.device_bytes()
+    sess = backend.create_session(comp, st)
+    assert comp.build_stats().light_tree_builds == 1 and comp.device_bytes() > before_bytes
+    k = next(i for i, m in enumerate(scene.materials) if m.program.has_emission and m.parameters.scalars.size)
+    sc = scene.materials[k].parameters.scalars * np.float32(3.0)
+    vc = scene.materials[k].parameters.vectors[::-1].copy()
+    comp.rebind_parameters(k, sc, vc)
+    assert comp.build_stats().light_tree_builds == 2
+    sess.reset(st)
+    assert sess.render_samples(SampleRange(0, 4, 0, 4)), sess.diagnostics
+    edited = copy.deepcopy(scene)
+    edited.materials[k].parameters.scalars[:] = sc
+    edited.materials[k].parameters.vectors[:] = vc
+    comp2 = backend.compile_scene(edited).scene
+    ref = backend.create_session(comp2, st)
+    assert ref.render_samples(SampleRange(0, 4, 0, 4)), ref.diagnostics
+    for kind in PASSES:
+        assert np.array_equal(sess.read_pass(kind).view(np.uint32), ref.read_pass(kind).view(np.uint32)), kind
+    stats = comp2.build_stats()
+    assert stats.total_ms > 0.0 and stats.build_threads >= 1 and stats.light_tree_ms > 0.0
