@@ -291,8 +291,10 @@ struct Evaluation {
 };
 
 // surface_closure_evaluation_contribution + accumulator
-// (src/luisa/surface_closure_evaluation.cpp:71-438).
-__device__ __forceinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, f3 shading_normal, f3 outgoing_raw,
+// (src/luisa/surface_closure_evaluation.cpp:71-438).  Out of line: the
+// shading kernel calls it for the light sample and for the BSDF sample, and
+// a single copy keeps the kernel's code within the instruction cache.
+__device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, f3 shading_normal, f3 outgoing_raw,
                                                        uint32_t lobe_mask, int selected) {
     const f3 outgoing = safe_normalize(outgoing_raw, shading_normal);
     Evaluation e{mk3(0.0f), 0.0f, 0u};
@@ -966,14 +968,9 @@ __device__ __forceinline__ float sin2_to_one_minus_cos(float s2) {
     return s2 > 0.0004f ? 1.0f - sqrtf(maxf_(1.0f - s2, 0.0f)) : 0.5f * s2;
 }
 
-// spot_one_minus_cosine_larger_spread (analytic_light_sampling.h:355-376); the
-// reciprocal square root is an IEEE 1/sqrt.
-__device__ __forceinline__ float spot_spread_cap(const psy_light_desc &l) {
-    const float t = tan_(0.5f * l.spot_angle);
-    const float ts2 = maxf_(l.axis_scale[0] * l.axis_scale[0], l.axis_scale[1] * l.axis_scale[1]);
-    const float as2 = l.axis_scale[2] * l.axis_scale[2];
-    return 1.0f - 1.0f / sqrtf(1.0f + t * t * ts2 / maxf_(as2, 1.0e-30f));
-}
+// spot_one_minus_cosine_larger_spread (analytic_light_sampling.h:355-376),
+// a per-lamp constant.
+__device__ __forceinline__ float spot_spread_cap(const LampConstGpu &c) { return c.spot_rz.w; }
 
 struct SphereHit {
     bool valid;
@@ -1098,30 +1095,21 @@ __device__ __forceinline__ RectContext rect_context(f3 reference, f3 center, f3 
     return c;
 }
 
-// point_eval_factor (analytic_light_sampling.h:880-896): 1/(pi area) with
-// the sphere's area for a finite radius and 4 for a delta point.
-__device__ __forceinline__ float point_eval_factor(const psy_light_desc &l) {
-    const float r2 = l.radius * l.radius;
-    const float area = r2 > 0.0f ? 4.0f * kPi * r2 : 4.0f;
-    return ((l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u ? 1.0f / maxf_(area, 1.0e-20f) : 1.0f) * kInvPi;
-}
+// point_eval_factor (analytic_light_sampling.h:880-896), a per-lamp constant.
+__device__ __forceinline__ float point_eval_factor(const LampConstGpu &c) { return c.factors.x; }
 
 // spot_light_to_local + spot_light_attenuation (analytic_light_sampling.h:309-345)
-// for the direction `from_light` leaving the lamp.
-__device__ __forceinline__ float spot_attenuation(const psy_light_desc &l, f3 from_light) {
-    const f3 ax = ld3(l.axis_x) * l.axis_scale[0];
-    const f3 ay = ld3(l.axis_y) * l.axis_scale[1];
-    const f3 az = ld3(l.axis_z) * l.axis_scale[2];
-    const f3 adj_x = cross(ay, az);
-    const float det = dot(ax, adj_x);
-    const bool valid = fabsf(det) > 1.0e-20f;
-    const float inv_det = 1.0f / (valid ? det : 1.0f);
-    const f3 rx = adj_x * inv_det, ry = cross(az, ax) * inv_det, rz = cross(ax, ay) * inv_det;
+// for the direction `from_light` leaving the lamp; the inverse axes and the
+// cone constants are the lamp's.
+__device__ __forceinline__ float spot_attenuation(const LampConstGpu &c, f3 from_light) {
+    const f3 rx = mk3(c.spot_rx.x, c.spot_rx.y, c.spot_rx.z);
+    const f3 ry = mk3(c.spot_ry.x, c.spot_ry.y, c.spot_ry.z);
+    const f3 rz = mk3(c.spot_rz.x, c.spot_rz.y, c.spot_rz.z);
     f3 local = light_safe_normalize(mk3(dot(rx, from_light), dot(ry, from_light), dot(rz, from_light)),
                                     mk3(0.0f, 0.0f, -1.0f));
     local.z = -local.z;
-    const float cos_half = cos_(0.5f * l.spot_angle);
-    const float blend = (1.0f - cos_half) * l.spot_smooth;
+    const float cos_half = c.spot_rx.w;
+    const float blend = c.spot_ry.w;
     const float ratio = blend != 0.0f ? (local.z - cos_half) / blend : 0.0f;
     const float lin = clampf_(ratio, 0.0f, 1.0f);
     const float smooth = lin * lin * (3.0f - 2.0f * lin);
@@ -1131,20 +1119,14 @@ __device__ __forceinline__ float spot_attenuation(const psy_light_desc &l, f3 fr
 
 // include/psycles/luisa/analytic_light_sampling.h:84-108 (distant),
 // :549-603 (disk), :856-896 (pdf / eval factor), :309-345 (spot profile).
-__device__ __noinline__ AnalyticSample sample_analytic(const psy_light_desc &l, f3 reference, f3 shading_n,
-                                                       bool transmission, f2 rnd) {
+__device__ __noinline__ AnalyticSample sample_analytic(const psy_light_desc &l, const LampConstGpu &lc, f3 reference,
+                                                       f3 shading_n, bool transmission, f2 rnd) {
     AnalyticSample out;
     const bool normalize_power = (l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u;
     if (l.type == PSY_LIGHT_DISTANT) {
         const f3 az = ld3(l.axis_z);
-        const float half_angle = 0.5f * maxf_(l.angle, 0.0f);
-        const float sq = sin_(0.5f * half_angle);
-        const float omc = 2.0f * sq * sq;
-        const ConeSample c = sample_uniform_cone(-az, omc, rnd);
-        const bool finite = half_angle > 0.0f;
-        const float sh = sin_(half_angle);
-        const float disk_area = kPi * sh * sh;
-        out.eval_factor = (normalize_power && finite) ? 1.0f / maxf_(disk_area, 1.0e-20f) : 1.0f;
+        const ConeSample c = sample_uniform_cone(-az, lc.factors.y, rnd);
+        out.eval_factor = lc.factors.z;
         out.direction = -c.direction;
         out.position = c.direction;
         out.distance = 1.0e30f;
@@ -1232,7 +1214,7 @@ __device__ __noinline__ AnalyticSample sample_analytic(const psy_light_desc &l, 
         float cap = sphere_cap;
         bool spread = false;
         if (l.type == PSY_LIGHT_SPOT) {
-            const float spot_cap = spot_spread_cap(l);
+            const float spot_cap = spot_spread_cap(lc);
             spread = cd2 > r2 && !(sphere_cap < spot_cap);
             if (spread) {
                 axis = ld3(l.axis_z);
@@ -1240,8 +1222,8 @@ __device__ __noinline__ AnalyticSample sample_analytic(const psy_light_desc &l, 
             }
         }
         out = sample_sphere(reference, shading_n, transmission, center, l.radius, axis, cap, spread, rnd);
-        float eval = point_eval_factor(l);
-        if (l.type == PSY_LIGHT_SPOT && cd2 > r2) eval *= spot_attenuation(l, -out.direction);
+        float eval = point_eval_factor(lc);
+        if (l.type == PSY_LIGHT_SPOT && cd2 > r2) eval *= spot_attenuation(lc, -out.direction);
         out.eval_factor = eval;
         if (l.type == PSY_LIGHT_SPOT) out.valid = out.valid && eval != 0.0f;
         return out;
@@ -1262,8 +1244,8 @@ __device__ __noinline__ AnalyticSample sample_analytic(const psy_light_desc &l, 
     const float r2 = l.radius * l.radius;
     const float inv_area = r2 > 0.0f ? 1.0f / maxf_(r2 * kPi, 1.0e-20f) : 1.0f;
     out.pdf = cosine > 0.0f ? inv_area * d2 / cosine : 0.0f;
-    float eval = point_eval_factor(l);
-    if (l.type == PSY_LIGHT_SPOT) eval *= spot_attenuation(l, -dir);
+    float eval = point_eval_factor(lc);
+    if (l.type == PSY_LIGHT_SPOT) eval *= spot_attenuation(lc, -dir);
     out.eval_factor = eval;
     out.direction = dir;
     out.position = position;
@@ -1317,9 +1299,9 @@ __device__ __forceinline__ bool intersect_area_lamp(const psy_light_desc &l, f3 
 // intersect_point / intersect_spot (analytic_light_intersection.h:33-266)
 // for the oriented-disk geometry (radius > 0, not a sphere): the disk faces
 // the ray origin.
-__device__ __forceinline__ bool intersect_disk_lamp(const psy_light_desc &l, f3 o, f3 d, float tmin, float tmax,
-                                                    f3 mis_n, bool had_transmission, float &distance, float &pdf,
-                                                    float &eval) {
+__device__ __forceinline__ bool intersect_disk_lamp(const psy_light_desc &l, const LampConstGpu &lc, f3 o, f3 d,
+                                                    float tmin, float tmax, f3 mis_n, bool had_transmission,
+                                                    float &distance, float &pdf, float &eval) {
     const f3 center = ld3(l.position);
     const f3 offset = o - center;
     if ((l.flags & PSY_LIGHT_FLAG_SPHERE) != 0u) {
@@ -1330,7 +1312,7 @@ __device__ __forceinline__ bool intersect_disk_lamp(const psy_light_desc &l, f3 
         const float cd2 = dot(offset, offset);
         const float r2 = l.radius * l.radius;
         float cap = sin2_to_one_minus_cos(r2 / maxf_(cd2, 1.0e-30f));
-        if (l.type == PSY_LIGHT_SPOT) cap = minf_(cap, spot_spread_cap(l));
+        if (l.type == PSY_LIGHT_SPOT) cap = minf_(cap, spot_spread_cap(lc));
         const SphereHit h = intersect_sphere(o, d, tmin, tmax, center, l.radius);
         if (!h.valid) return false;
         distance = h.distance;
@@ -1342,9 +1324,9 @@ __device__ __forceinline__ bool intersect_disk_lamp(const psy_light_desc &l, f3 
             const float c = dot(mis_n, d);
             pdf = c > 0.0f ? c * kInvPi : 0.0f;
         }
-        eval = point_eval_factor(l);
+        eval = point_eval_factor(lc);
         if (l.type == PSY_LIGHT_SPOT) {
-            if (cd2 > r2) eval *= spot_attenuation(l, -d);
+            if (cd2 > r2) eval *= spot_attenuation(lc, -d);
             if (!(dot(d, offset) < 0.0f)) return false;
         }
         return eval > 0.0f;
@@ -1360,9 +1342,9 @@ __device__ __forceinline__ bool intersect_disk_lamp(const psy_light_desc &l, f3 
     if (!(hit && l.radius > 0.0f)) return false;
     const float inv_area = r2 > 0.0f ? 1.0f / maxf_(r2 * kPi, 1.0e-20f) : 1.0f;
     pdf = cosine > 0.0f ? inv_area * (distance * distance) / cosine : 0.0f;
-    eval = point_eval_factor(l);
+    eval = point_eval_factor(lc);
     if (l.type == PSY_LIGHT_SPOT) {
-        eval *= spot_attenuation(l, -d);
+        eval *= spot_attenuation(lc, -d);
         if (!(dot(d, offset) < 0.0f)) return false;
     }
     return eval > 0.0f;
@@ -1393,7 +1375,7 @@ __device__ __noinline__ LampHit closest_lamp(const SceneView &s, f3 o, f3 d, flo
         if (!((l.visibility & ray_visibility) != 0u && (camera_path || use_mis) && li != excluded)) continue;
         float distance = 0.0f, pdf = 0.0f, eval = 0.0f;
         const bool hit = l.type == PSY_LIGHT_AREA ? intersect_area_lamp(l, o, d, tmin, best.distance, distance, pdf, eval)
-                                                  : intersect_disk_lamp(l, o, d, tmin, best.distance, mis_n,
+                                                  : intersect_disk_lamp(l, s.lamp_consts[li], o, d, tmin, best.distance, mis_n,
                                                                         had_transmission, distance, pdf, eval);
         if (hit) best = LampHit{true, li, distance, pdf, eval};
     }

@@ -661,6 +661,55 @@ void emission_estimate(const psy_material_desc &m, float out[3]) {
     for (int k = 0; k < 3; ++k) out[k] = m.root < est.size() ? est[m.root][k] : 0.0f;
 }
 
+// The per-lamp constants of the sampling kernels, in the kernels' float
+// expressions and operation order (the library is compiled without FP
+// contraction); transcendentals are evaluated in double and rounded once,
+// as the kernels' own are (analytic_light_sampling.h:84-108, 309-376,
+// 880-896).
+psy::LampConstGpu lamp_constants(const psy_light_desc &l) {
+    constexpr float kPiF = 3.1415926535897932f, kInvPiF = 0.31830988618379067154f;
+    auto rounded = [](double v) { return static_cast<float>(v); };
+    auto maxf = [](float a, float b) { return a > b ? a : b; };
+    psy::LampConstGpu c{};
+    float ax[3], ay[3], az[3];
+    for (int k = 0; k < 3; ++k) {
+        ax[k] = l.axis_x[k] * l.axis_scale[0];
+        ay[k] = l.axis_y[k] * l.axis_scale[1];
+        az[k] = l.axis_z[k] * l.axis_scale[2];
+    }
+    auto cross = [](const float a[3], const float b[3], float o[3]) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    float adj_x[3], adj_y[3], adj_z[3];
+    cross(ay, az, adj_x);
+    cross(az, ax, adj_y);
+    cross(ax, ay, adj_z);
+    const float det = ax[0] * adj_x[0] + ax[1] * adj_x[1] + ax[2] * adj_x[2];
+    const float inv_det = 1.0f / (std::fabs(det) > 1.0e-20f ? det : 1.0f);
+    const float cos_half = rounded(std::cos(static_cast<double>(0.5f * l.spot_angle)));
+    const float blend = (1.0f - cos_half) * l.spot_smooth;
+    const float t = rounded(std::tan(static_cast<double>(0.5f * l.spot_angle)));
+    const float ts2 = maxf(l.axis_scale[0] * l.axis_scale[0], l.axis_scale[1] * l.axis_scale[1]);
+    const float as2 = l.axis_scale[2] * l.axis_scale[2];
+    const float spread_cap = 1.0f - 1.0f / std::sqrt(1.0f + t * t * ts2 / maxf(as2, 1.0e-30f));
+    c.spot_rx = make_float4(adj_x[0] * inv_det, adj_x[1] * inv_det, adj_x[2] * inv_det, cos_half);
+    c.spot_ry = make_float4(adj_y[0] * inv_det, adj_y[1] * inv_det, adj_y[2] * inv_det, blend);
+    c.spot_rz = make_float4(adj_z[0] * inv_det, adj_z[1] * inv_det, adj_z[2] * inv_det, spread_cap);
+    const bool normalize_power = (l.flags & PSY_LIGHT_FLAG_NORMALIZE) != 0u;
+    const float r2 = l.radius * l.radius;
+    const float area = r2 > 0.0f ? 4.0f * kPiF * r2 : 4.0f;
+    c.factors.x = (normalize_power ? 1.0f / maxf(area, 1.0e-20f) : 1.0f) * kInvPiF;
+    const float half_angle = 0.5f * maxf(l.angle, 0.0f);
+    const float sq = rounded(std::sin(static_cast<double>(0.5f * half_angle)));
+    c.factors.y = 2.0f * sq * sq;
+    const float sh = rounded(std::sin(static_cast<double>(half_angle)));
+    const float disk_area = kPiF * sh * sh;
+    c.factors.z = (normalize_power && half_angle > 0.0f) ? 1.0f / maxf(disk_area, 1.0e-20f) : 1.0f;
+    return c;
+}
+
 // Runs body(i) for every i in [0, n) on up to 32 host threads that pull
 // indices from a shared counter; `threads` receives the count used.  An
 // exception in a body (out of host memory) becomes PSY_ERROR_OUT_OF_MEMORY.
@@ -1215,6 +1264,10 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->emitters.upload(emitters, st));
     PSY_CUDA_TRY(sc->distribution.upload(dist, st));
     PSY_CUDA_TRY(sc->lights.upload(lights, st));
+    std::vector<psy::LampConstGpu> lamp_consts;
+    lamp_consts.reserve(lights.size());
+    for (const psy_light_desc &l : lights) lamp_consts.push_back(lamp_constants(l));
+    PSY_CUDA_TRY(sc->lamp_consts.upload(lamp_consts, st));
     // lamps a ray can hit, in light order, with a bounding sphere each
     std::vector<float4> lamp_bounds;
     std::vector<uint32_t> lamp_ids;
@@ -1259,6 +1312,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     v.distribution = sc->distribution.as<psy::DistEntryGpu>();
     v.lights = sc->lights.as<psy_light_desc>();
     v.lamp_bounds = sc->lamp_bounds.as<float4>();
+    v.lamp_consts = sc->lamp_consts.as<psy::LampConstGpu>();
     v.lamp_ids = sc->lamp_ids.as<uint32_t>();
     v.lamp_count = uint32_t(lamp_ids.size());
     v.instance_count = tl.prims.empty() ? 0u : d->instance_count;
@@ -1415,7 +1469,7 @@ uint64_t psy::host::scene_device_bytes(const psy_scene *s) {
     uint64_t n = 0u;
     for (const DeviceBuffer *b : {&s->tlas, &s->blas, &s->tris, &s->instances, &s->meshes, &s->positions, &s->normals,
                                   &s->indices, &s->tri_materials, &s->material_buf, &s->code, &s->scalar_buf,
-                                  &s->vector_buf, &s->emitters, &s->distribution, &s->lights, &s->lamp_bounds,
+                                  &s->vector_buf, &s->emitters, &s->distribution, &s->lights, &s->lamp_consts, &s->lamp_bounds,
                                   &s->lamp_ids, &s->lt_nodes, &s->lt_emitters, &s->lt_mapping, &s->lt_lookup})
         n += b->bytes;
     return n;

@@ -111,8 +111,8 @@ struct psy_scene {
     std::vector<psy::MaterialGpu> materials;
     std::vector<float> scalars, vectors;
     psy::host::DeviceBuffer tlas, blas, tris, instances, meshes, positions, normals, indices, tri_materials, material_buf, code,
-        scalar_buf, vector_buf, emitters, distribution, lights, lamp_bounds, lamp_ids, lt_nodes, lt_emitters, lt_mapping,
-        lt_lookup;
+        scalar_buf, vector_buf, emitters, distribution, lights, lamp_consts, lamp_bounds, lamp_ids, lt_nodes, lt_emitters,
+        lt_mapping, lt_lookup;
     psy::SceneView view{};
     uint64_t triangle_count = 0;
     psy_scene_build_stats stats{};

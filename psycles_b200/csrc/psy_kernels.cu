@@ -691,6 +691,13 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                         f3 surviving = mk3(0.0f);
                         uint32_t light_obj = kInvalid, light_prim = kInvalid;
                         bool emit = false;
+                        // The light sample of either kind, then one BSDF
+                        // evaluation, MIS weight and light roulette shared by
+                        // both (a warp's lanes that picked triangles and lamps
+                        // evaluate together).
+                        bool sampled = false, weigh_mis = true;
+                        f3 light_radiance = mk3(0.0f);
+                        float light_pdf = 0.0f, pdf_divisor = 1.0f;
                         if (selected.kind == 0u) {
                             // EmissiveMeshLightingComponent (src/luisa/path_kernel_nee_emissive_mesh.cpp:32-296)
                             const EmitterGpu &em = s.emitters[selected.index];
@@ -704,22 +711,14 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                                 const f3 oriented = is_transmission ? -sp.ng : sp.ng;
                                 const bool reject_self = same_primitive && dot(ls.direction, oriented) > 0.0f;
                                 if (!reject_self) {
-                                    const f3 light_radiance = material_emission(s, s.materials[em.material]);
-                                    const Evaluation e = evaluate_mixture(closures, sp.n, ls.direction, lobe_mask, -1);
-                                    const float mis = nee_light_weight(p.direct_mode, pdf, e.pdf);
-                                    const f3 weighted = e.f * light_radiance * (mis / pdf);
-                                    if (any_nonzero(weighted)) {
-                                        const f3 unshadowed = weighted * mk3(1.0f);
-                                        surviving = unshadowed *
-                                                    light_roulette_weight(unshadowed, light_terminate, p.inv_rr_threshold);
-                                        if (any_nonzero(surviving)) {
-                                            emit = true;
-                                            lp = ls.position;
-                                            light_obj = em.object;
-                                            light_prim = em.cycles_prim;
-                                            ldir = ls.direction;
-                                        }
-                                    }
+                                    sampled = true;
+                                    light_radiance = material_emission(s, s.materials[em.material]);
+                                    light_pdf = pdf;
+                                    pdf_divisor = pdf;
+                                    lp = ls.position;
+                                    light_obj = em.object;
+                                    light_prim = em.cycles_prim;
+                                    ldir = ls.direction;
                                 }
                             }
                         } else if (selected.kind == 1u) {
@@ -727,29 +726,33 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                             const psy_light_desc &l = s.lights[selected.index];
                             if (!(depth > l.max_bounces)) {
                                 const AnalyticSample a =
-                                    sample_analytic(l, sp.position, sp.n, (runtime & kRuntimeBsdfHasTransmission) != 0u,
+                                    sample_analytic(l, s.lamp_consts[selected.index], sp.position, sp.n,
+                                                    (runtime & kRuntimeBsdfHasTransmission) != 0u,
                                                     mk2(light_sample.x, light_sample.y));
-                                const float light_pdf = a.pdf * selected.selection_pdf;
-                                if (a.valid && light_pdf > 0.0f) {
-                                    const f3 light_radiance = ld3(l.color) * (l.power * a.eval_factor);
-                                    const Evaluation e = evaluate_mixture(closures, sp.n, a.direction, lobe_mask, -1);
+                                const float pdf = a.pdf * selected.selection_pdf;
+                                if (a.valid && pdf > 0.0f) {
+                                    sampled = true;
+                                    light_radiance = ld3(l.color) * (l.power * a.eval_factor);
+                                    light_pdf = pdf;
+                                    pdf_divisor = maxf_(pdf, 1.0e-20f);
                                     // MIS only for lamps a BSDF ray can also hit
                                     // (path_kernel_nee_analytic.cpp:286-292)
-                                    const float mis = (l.flags & kLightFlagForward) != 0u
-                                                          ? nee_light_weight(p.direct_mode, light_pdf, e.pdf) : 1.0f;
-                                    const f3 weighted = e.f * light_radiance * (mis / maxf_(light_pdf, 1.0e-20f));
-                                    if (any_nonzero(weighted)) {
-                                        const f3 unshadowed = weighted * mk3(1.0f);
-                                        surviving = unshadowed *
-                                                    light_roulette_weight(unshadowed, light_terminate, p.inv_rr_threshold);
-                                        if (any_nonzero(surviving)) {
-                                            emit = true;
-                                            lp = a.position;
-                                            ldir = a.direction;
-                                            distant = l.type == PSY_LIGHT_DISTANT;
-                                        }
-                                    }
+                                    weigh_mis = (l.flags & kLightFlagForward) != 0u;
+                                    lp = a.position;
+                                    ldir = a.direction;
+                                    distant = l.type == PSY_LIGHT_DISTANT;
                                 }
+                            }
+                        }
+                        if (sampled) {
+                            const Evaluation e = evaluate_mixture(closures, sp.n, ldir, lobe_mask, -1);
+                            const float mis = weigh_mis ? nee_light_weight(p.direct_mode, light_pdf, e.pdf) : 1.0f;
+                            const f3 weighted = e.f * light_radiance * (mis / pdf_divisor);
+                            if (any_nonzero(weighted)) {
+                                const f3 unshadowed = weighted * mk3(1.0f);
+                                surviving =
+                                    unshadowed * light_roulette_weight(unshadowed, light_terminate, p.inv_rr_threshold);
+                                emit = any_nonzero(surviving);
                             }
                         }
                         if (emit) {

@@ -99,7 +99,6 @@ __device__ __noinline__ float sin_(float x) { return static_cast<float>(sin(stat
 __device__ __noinline__ float cos_(float x) { return static_cast<float>(cos(static_cast<double>(x))); }
 __device__ __noinline__ float acos_(float x) { return static_cast<float>(acos(static_cast<double>(x))); }
 __device__ __noinline__ float asin_(float x) { return static_cast<float>(asin(static_cast<double>(x))); }
-__device__ __noinline__ float tan_(float x) { return static_cast<float>(tan(static_cast<double>(x))); }
 __device__ __noinline__ float atan2_(float y, float x) {
     return static_cast<float>(atan2(static_cast<double>(y), static_cast<double>(x)));
 }

@@ -84,6 +84,19 @@ struct alignas(16) DistEntryGpu {
     uint32_t kind, index;
 };
 
+// Per-lamp constants of analytic_light_sampling.h that depend on the lamp
+// alone, computed once on the host with the kernels' float expressions
+// (transcendentals in double, rounded once): the inverse of the spot axes
+// (spot_light_to_local, :309-329) with cos(spot_angle / 2) and the smooth
+// blend (:331-345), the spot spread cap (:355-376), point_eval_factor
+// (:880-896), and the distant lamp's cone and eval factor (:84-108).
+struct alignas(16) LampConstGpu {
+    float4 spot_rx;  // xyz: first row of the inverse spot axes; w: cos(spot_angle / 2)
+    float4 spot_ry;  // w: (1 - cos(spot_angle / 2)) * spot_smooth
+    float4 spot_rz;  // w: one minus cosine of the spot's spread cone
+    float4 factors;  // x: point eval factor, y: distant cone one minus cosine, z: distant eval factor
+};
+
 struct SceneView {
     const WideNodeGpu *tlas;
     const WideNodeGpu *blas;
@@ -108,6 +121,7 @@ struct SceneView {
     // lamps a ray can hit (area lamps, finite point / spot disks) in light
     // order: bounding sphere (centre, radius^2) and light index
     const float4 *lamp_bounds;
+    const LampConstGpu *lamp_consts;  // one per light
     const uint32_t *lamp_ids;
     uint32_t lamp_count;
     float triangle_area_pdf;
