@@ -457,71 +457,51 @@ __device__ __forceinline__ Xform load_xform(const float *m) {
     return {ld3(m), ld3(m + 3), ld3(m + 6), ld3(m + 9)};
 }
 
-// Slab test of both children of a binary node.  Boxes are padded at build
-// time and the far bound widened by a relative 2^-20, so a triangle that the
-// Pluecker predicate accepts inside [tmin, tmax] is never culled.
-__device__ __forceinline__ void node_slabs(const BvhNodeGpu &n, f3 org_inv, f3 inv, float tmin, float tmax,
-                                           float &lnear, float &rnear, bool &lhit, bool &rhit) {
-    const float lx0 = fmaf(n.x.x, inv.x, -org_inv.x), lx1 = fmaf(n.x.y, inv.x, -org_inv.x);
-    const float ly0 = fmaf(n.y.x, inv.y, -org_inv.y), ly1 = fmaf(n.y.y, inv.y, -org_inv.y);
-    const float lz0 = fmaf(n.z.x, inv.z, -org_inv.z), lz1 = fmaf(n.z.y, inv.z, -org_inv.z);
-    const float rx0 = fmaf(n.x.z, inv.x, -org_inv.x), rx1 = fmaf(n.x.w, inv.x, -org_inv.x);
-    const float ry0 = fmaf(n.y.z, inv.y, -org_inv.y), ry1 = fmaf(n.y.w, inv.y, -org_inv.y);
-    const float rz0 = fmaf(n.z.z, inv.z, -org_inv.z), rz1 = fmaf(n.z.w, inv.z, -org_inv.z);
-    const float ln = fmaxf(fmaxf(fminf(lx0, lx1), fminf(ly0, ly1)), fmaxf(fminf(lz0, lz1), tmin));
-    const float lf = fminf(fminf(fmaxf(lx0, lx1), fmaxf(ly0, ly1)), fminf(fmaxf(lz0, lz1), tmax));
-    const float rn = fmaxf(fmaxf(fminf(rx0, rx1), fminf(ry0, ry1)), fmaxf(fminf(rz0, rz1), tmin));
-    const float rf = fminf(fminf(fmaxf(rx0, rx1), fmaxf(ry0, ry1)), fminf(fmaxf(rz0, rz1), tmax));
-    lhit = ln <= lf * 1.00000095367431640625f + 1.0e-30f || ln <= lf;
-    rhit = rn <= rf * 1.00000095367431640625f + 1.0e-30f || rn <= rf;
-    lnear = ln;
-    rnear = rn;
-}
+// A wide node as one ray sees it: per axis the plane a ray of that
+// direction sign enters through (near) and leaves through (far).
+struct WideNodeRay {
+    float4 nx, fx, ny, fy, nz, fz;
+    int4 link, count;
+};
 
-__device__ __forceinline__ BvhNodeGpu load_node(const BvhNodeGpu *nodes, int idx) {
+// Loads a wide node with its planes ordered by the ray's direction signs
+// (`neg` bit a set where the direction's component a is negative), so the
+// slab test needs no min / max per axis.
+__device__ __forceinline__ WideNodeRay load_wide_node(const WideNodeGpu *nodes, uint32_t idx, uint32_t neg) {
     const float4 *p = reinterpret_cast<const float4 *>(nodes + idx);
-    BvhNodeGpu n;
-    n.x = __ldg(p + 0);
-    n.y = __ldg(p + 1);
-    n.z = __ldg(p + 2);
-    const float4 c = __ldg(p + 3);
-    n.child = make_int4(__float_as_int(c.x), __float_as_int(c.y), __float_as_int(c.z), __float_as_int(c.w));
-    return n;
-}
-
-// Slab test of the four children of a wide node, with the conservative
-// bounds of the binary test; empty slots never hit.
-__device__ __forceinline__ void wide_slabs(const WideNodeGpu &n, f3 oinv, f3 inv, float tmin, float tmax,
-                                           float near[4], bool hit[4]) {
-    const float lx[4] = {n.lox.x, n.lox.y, n.lox.z, n.lox.w}, hx[4] = {n.hix.x, n.hix.y, n.hix.z, n.hix.w};
-    const float ly[4] = {n.loy.x, n.loy.y, n.loy.z, n.loy.w}, hy[4] = {n.hiy.x, n.hiy.y, n.hiy.z, n.hiy.w};
-    const float lz[4] = {n.loz.x, n.loz.y, n.loz.z, n.loz.w}, hz[4] = {n.hiz.x, n.hiz.y, n.hiz.z, n.hiz.w};
-    const int lk[4] = {n.link.x, n.link.y, n.link.z, n.link.w}, ct[4] = {n.count.x, n.count.y, n.count.z, n.count.w};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const float x0 = fmaf(lx[k], inv.x, -oinv.x), x1 = fmaf(hx[k], inv.x, -oinv.x);
-        const float y0 = fmaf(ly[k], inv.y, -oinv.y), y1 = fmaf(hy[k], inv.y, -oinv.y);
-        const float z0 = fmaf(lz[k], inv.z, -oinv.z), z1 = fmaf(hz[k], inv.z, -oinv.z);
-        const float nr = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
-        const float fr = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
-        near[k] = nr;
-        hit[k] = (nr <= fr * 1.00000095367431640625f + 1.0e-30f || nr <= fr) && (lk[k] >= 0 || ct[k] > 0);
-    }
-}
-
-__device__ __forceinline__ WideNodeGpu load_wide_node(const WideNodeGpu *nodes, uint32_t idx) {
-    const float4 *p = reinterpret_cast<const float4 *>(nodes + idx);
-    WideNodeGpu n;
-    n.lox = __ldg(p + 0);
-    n.hix = __ldg(p + 1);
-    n.loy = __ldg(p + 2);
-    n.hiy = __ldg(p + 3);
-    n.loz = __ldg(p + 4);
-    n.hiz = __ldg(p + 5);
+    const uint32_t sx = neg & 1u, sy = (neg >> 1) & 1u, sz = (neg >> 2) & 1u;
+    WideNodeRay n;
+    n.nx = __ldg(p + sx);
+    n.fx = __ldg(p + (1u - sx));
+    n.ny = __ldg(p + 2u + sy);
+    n.fy = __ldg(p + (3u - sy));
+    n.nz = __ldg(p + 4u + sz);
+    n.fz = __ldg(p + (5u - sz));
     const int4 *q = reinterpret_cast<const int4 *>(p + 6);
     n.link = __ldg(q);
     n.count = __ldg(q + 1);
     return n;
+}
+
+// Slab test of the four children of a wide node, conservative as the
+// boxes are padded at build time and the far bound is widened by a
+// relative 2^-20.  Empty slots hold +inf planes on every axis, which give
+// an entry distance of +inf or an exit distance of -inf, so they never hit.
+__device__ __forceinline__ void wide_slabs(const WideNodeRay &n, f3 oinv, f3 inv, float tmin, float tmax,
+                                           float near[4], bool hit[4]) {
+    const float nx[4] = {n.nx.x, n.nx.y, n.nx.z, n.nx.w}, fx[4] = {n.fx.x, n.fx.y, n.fx.z, n.fx.w};
+    const float ny[4] = {n.ny.x, n.ny.y, n.ny.z, n.ny.w}, fy[4] = {n.fy.x, n.fy.y, n.fy.z, n.fy.w};
+    const float nz[4] = {n.nz.x, n.nz.y, n.nz.z, n.nz.w}, fz[4] = {n.fz.x, n.fz.y, n.fz.z, n.fz.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float x0 = fmaf(nx[k], inv.x, -oinv.x), x1 = fmaf(fx[k], inv.x, -oinv.x);
+        const float y0 = fmaf(ny[k], inv.y, -oinv.y), y1 = fmaf(fy[k], inv.y, -oinv.y);
+        const float z0 = fmaf(nz[k], inv.z, -oinv.z), z1 = fmaf(fz[k], inv.z, -oinv.z);
+        const float nr = fmaxf(fmaxf(x0, y0), fmaxf(z0, tmin));
+        const float fr = fminf(fminf(x1, y1), fminf(z1, tmax));
+        near[k] = nr;
+        hit[k] = nr <= fr * 1.00000095367431640625f + 1.0e-30f || nr <= fr;
+    }
 }
 
 constexpr int kStackSize = 48;
@@ -533,6 +513,7 @@ constexpr uint32_t kTagMask = 3u << 30;
 
 struct SlabRay {
     f3 o, d, inv, oinv;  // origin, clamped direction, reciprocal, origin * reciprocal
+    uint32_t neg;        // bit a: direction component a is negative
 };
 
 __device__ __forceinline__ SlabRay make_slab_ray(f3 o, f3 raw) {
@@ -541,6 +522,7 @@ __device__ __forceinline__ SlabRay make_slab_ray(f3 o, f3 raw) {
     r.d = mk3(clamp_bvh_direction(raw.x), clamp_bvh_direction(raw.y), clamp_bvh_direction(raw.z));
     r.inv = mk3(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
     r.oinv = mk3(o.x * r.inv.x, o.y * r.inv.y, o.z * r.inv.z);
+    r.neg = (r.d.x < 0.0f ? 1u : 0u) | (r.d.y < 0.0f ? 2u : 0u) | (r.d.z < 0.0f ? 4u : 0u);
     return r;
 }
 
@@ -613,7 +595,7 @@ __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneVi
             continue;
         }
         const bool blas = tag == kTagBlas;
-        const WideNodeGpu n = load_wide_node(blas ? s.blas : s.tlas, idx);
+        const WideNodeRay n = load_wide_node(blas ? s.blas : s.tlas, idx, t.cur.neg);
         float near[4];
         bool hit[4];
         wide_slabs(n, t.cur.oinv, t.cur.inv, t.ray.tmin, t.tmax, near, hit);

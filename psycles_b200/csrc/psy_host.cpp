@@ -481,8 +481,10 @@ struct Builder {
         wide.push_back({});
         int links[4], counts[4];
         float lo[3][4], hi[3][4];
+        // empty slots (and empty leaves) get +inf planes on every axis: the
+        // traversal's slab test then misses them for any ray direction
         for (int k = 0; k < 4; ++k) {
-            if (k < n) {
+            if (k < n && (kids[k].link >= 0 || kids[k].count > 0)) {
                 for (int a = 0; a < 3; ++a) {
                     lo[a][k] = kids[k].lo[a];
                     hi[a][k] = kids[k].hi[a];
@@ -491,8 +493,8 @@ struct Builder {
                 counts[k] = kids[k].link >= 0 ? 0 : kids[k].count;
             } else {
                 for (int a = 0; a < 3; ++a) {
-                    lo[a][k] = 1.0f;
-                    hi[a][k] = -1.0f;
+                    lo[a][k] = INFINITY;
+                    hi[a][k] = INFINITY;
                 }
                 links[k] = -1;
                 counts[k] = 0;
