@@ -336,14 +336,42 @@ __device__ __forceinline__ float next_float_up(float t) {
 // ------------------------------------------------------ sort by material
 __device__ __forceinline__ uint32_t surface_material(const SceneView &s, uint32_t instance, uint32_t local);
 
-// Queues of at least `threshold` paths are grouped by material before
-// shading, so a warp mostly runs one closure program: a bucket per queue
-// entry (misses in bucket 0, hits by material and job hashed into the other
-// buckets), a histogram, its exclusive scan and a scatter.  Order inside a
-// bucket is arbitrary; no path's result depends on the queue order.
+// The kind of lamp a path's next-event sample will take under the flat
+// light distribution, estimated from the same random number the shading
+// kernel draws (the lamps share the distribution's tail equally): 1
+// emissive triangle, 2 sun, 3 / 4 rectangle / ellipse, 5 delta point or
+// spot, 6 disk, 7 sphere; 0 without a flat-distribution pick.  Only the
+// queue order depends on it, so an estimate at a bin edge costs
+// coherence, never a result.
+__device__ __forceinline__ uint32_t nee_kind_hint(const SceneView &s, const RenderParams &p, const PathBuffers &b,
+                                                  uint32_t i) {
+    if (p.use_light_tree || !p.nee || s.emitter_count == 0u) return 0u;
+    const uint4 st = b.st[i];
+    const uint32_t local = b.st2[i].w;
+    const uint32_t x = p.win_x + local % p.win_w, y = p.win_y + local / p.win_w;
+    const uint32_t rng_hash = pixel_hash(x, p.full_h - 1u - y, p.seed);
+    const float u = sample_4d(p, b.sample[i], rng_hash, st.z + 1u).z;
+    const uint32_t tri_n = s.triangle_emitters, light_n = s.light_count;
+    const float c0 = tri_n > 0u ? s.distribution[tri_n].cumulative : 0.0f;
+    if (light_n == 0u || u < c0) return 1u;
+    const uint32_t li = min(uint32_t((u - c0) / fmaxf(1.0f - c0, 1.0e-20f) * float(light_n)), light_n - 1u);
+    const psy_light_desc &l = s.lights[li];
+    if (l.type == PSY_LIGHT_DISTANT) return 2u;
+    if (l.type == PSY_LIGHT_AREA) return (l.flags & PSY_LIGHT_FLAG_ELLIPSE) != 0u ? 4u : 3u;
+    if (!(l.radius > 0.0f)) return 5u;
+    return (l.flags & PSY_LIGHT_FLAG_SPHERE) != 0u ? 7u : 6u;
+}
+
+// Queues of at least `threshold` paths are grouped before shading by
+// material and by the kind of lamp the path's next-event sample takes, so
+// a warp mostly runs one closure program and one light-sampling branch: a
+// bucket per queue entry (misses in bucket 0, hits by material, lamp kind
+// and job hashed into the other buckets), a histogram, its exclusive scan
+// and a scatter.  Order inside a bucket is arbitrary; no path's result
+// depends on the queue order.
 template <bool kMulti>
-__global__ void k_sort_count(const __grid_constant__ SceneView s_arg, const __grid_constant__ PathBuffers b,
-                             const JobGpu *jobs, uint32_t threshold) {
+__global__ void k_sort_count(const __grid_constant__ SceneView s_arg, const __grid_constant__ RenderParams p_arg,
+                             const __grid_constant__ PathBuffers b, const JobGpu *jobs, uint32_t threshold) {
     __shared__ uint32_t local[kSortBuckets];
     const uint32_t count = b.counters[0];
     if (count < threshold) return;
@@ -356,8 +384,9 @@ __global__ void k_sort_count(const __grid_constant__ SceneView s_arg, const __gr
         if (prim != kInvalid) {
             const uint32_t job = kMulti ? b.job[i] : 0u;
             const SceneView &s = kMulti ? jobs[job].s : s_arg;
+            const RenderParams &p = kMulti ? jobs[job].p : p_arg;
             const uint32_t mat = surface_material(s, __float_as_uint(b.hit[i].w), prim);
-            key = 1u + (mat + job * 977u) % (kSortBuckets - 1u);
+            key = 1u + (mat * 8u + nee_kind_hint(s, p, b, i) + job * 977u) % (kSortBuckets - 1u);
         }
         b.sort_keys[q] = key;
         atomicAdd(&local[key], 1u);
@@ -1228,9 +1257,9 @@ int shade_grid(uint32_t work, const LaunchConfig &lc) {
     return int(blocks < 1u ? 1u : (blocks > cap ? cap : blocks));
 }
 template <bool kMulti>
-void launch_sort(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const PathBuffers &b, const JobGpu *jobs,
-                 uint32_t max_work) {
-    k_sort_count<kMulti><<<launch_grid(max_work, 256, lc), 256, 0, st>>>(s, b, jobs, lc.sort_threshold);
+void launch_sort(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const RenderParams &p, const PathBuffers &b,
+                 const JobGpu *jobs, uint32_t max_work) {
+    k_sort_count<kMulti><<<launch_grid(max_work, 256, lc), 256, 0, st>>>(s, p, b, jobs, lc.sort_threshold);
     k_sort_scan<<<1, 1024, 0, st>>>(b, lc.sort_threshold, 0u);
     // ranks are packed in 21 bits: keep every block's chunk below 2^20 paths
     const int scatter_blocks = std::max(launch_grid(max_work, 256, lc), int((max_work >> 20) + 1u));
@@ -1254,7 +1283,7 @@ void launch_intersect(cudaStream_t st, const LaunchConfig &lc, const SceneView &
 }
 void launch_shade(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                   uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
-    if (lc.sort_threshold) launch_sort<false>(st, lc, s, b, nullptr, max_work);
+    if (lc.sort_threshold) launch_sort<false>(st, lc, s, p, b, nullptr, max_work);
     if (trace)
         k_shade<true, false><<<shade_grid(max_work, lc), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr,
                                                                      lc.sort_threshold);
@@ -1291,7 +1320,7 @@ void launch_intersect_batch(cudaStream_t st, const LaunchConfig &lc, const JobGp
 }
 void launch_shade_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work,
                         uint32_t step) {
-    if (lc.sort_threshold) launch_sort<true>(st, lc, SceneView{}, b, jobs, max_work);
+    if (lc.sort_threshold) launch_sort<true>(st, lc, SceneView{}, RenderParams{}, b, jobs, max_work);
     k_shade<false, true><<<shade_grid(max_work, lc), 128, 0, st>>>(SceneView{}, RenderParams{}, b, step, kInvalid,
                                                                  nullptr, jobs, lc.sort_threshold);
 }
