@@ -479,6 +479,8 @@ typedef struct psy_tuning {
                                           0 = never, 0xffffffff = the default 65536 */
     uint32_t shadow_sort_threshold;    /* sort shadow queues of at least this many rays by direction;
                                           0 = never (the default), 0xffffffff = the default */
+    uint32_t ray_sort_threshold;       /* sort closest-hit queues of at least this many rays by origin
+                                          cell and octant; 0 = never (the default), 0xffffffff = the default */
 } psy_tuning;
 
 psy_status psy_context_set_tuning(psy_context *context, const psy_tuning *tuning);

@@ -135,7 +135,8 @@ class KernelProfile(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("path_capacity", "stream_blocks_per_sm", "traversal_blocks_per_sm",
-                                               "shade_blocks_per_sm", "sort_threshold", "shadow_sort_threshold")]
+                                               "shade_blocks_per_sm", "sort_threshold", "shadow_sort_threshold",
+                                               "ray_sort_threshold")]
 
 
 class BatchConfig(ctypes.Structure):

@@ -27,6 +27,7 @@ CANDIDATES = {
     "path_capacity": (1 << 20, 1 << 22, 1 << 23, 1 << 24),
     "sort_threshold": (0, 1 << 16, 1 << 20),
     "shadow_sort_threshold": (0, 1 << 16, 1 << 20),
+    "ray_sort_threshold": (0, 1 << 16, 1 << 20),
     "traversal_blocks_per_sm": (8, 12, 16),
     "shade_blocks_per_sm": (8, 16, 32),
 }

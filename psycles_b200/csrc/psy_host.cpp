@@ -921,6 +921,8 @@ psy_status psy_context_set_tuning(psy_context *c, const psy_tuning *t) {
     c->launch.sort_threshold = t->sort_threshold == 0xffffffffu ? defaults.sort_threshold : t->sort_threshold;
     c->launch.shadow_sort_threshold =
         t->shadow_sort_threshold == 0xffffffffu ? defaults.shadow_sort_threshold : t->shadow_sort_threshold;
+    c->launch.ray_sort_threshold =
+        t->ray_sort_threshold == 0xffffffffu ? defaults.ray_sort_threshold : t->ray_sort_threshold;
     return PSY_OK;
 }
 
@@ -932,6 +934,7 @@ psy_status psy_context_get_tuning(const psy_context *c, psy_tuning *t) {
     t->shade_blocks_per_sm = c->launch.shade_blocks_per_sm;
     t->sort_threshold = c->launch.sort_threshold;
     t->shadow_sort_threshold = c->launch.shadow_sort_threshold;
+    t->ray_sort_threshold = c->launch.ray_sort_threshold;
     return PSY_OK;
 }
 
@@ -1124,6 +1127,8 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         tl.prims.push_back(p);
     }
     tl.build_root();
+    Box world;
+    for (const Prim &p : tl.prims) world.grow(p.box);
     sc->instance_mirrored.resize(d->instance_count);
     for (uint32_t i = 0; i < d->instance_count; ++i)
         sc->instance_mirrored[i] = dt(o2w[i].c0, crs(o2w[i].c1, o2w[i].c2)) < 0.0f ? 1u : 0u;
@@ -1315,6 +1320,11 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     v.lights = sc->lights.as<psy_light_desc>();
     v.lamp_bounds = sc->lamp_bounds.as<float4>();
     v.lamp_consts = sc->lamp_consts.as<psy::LampConstGpu>();
+    if (!world.empty())
+        for (int a = 0; a < 3; ++a) {
+            (&v.world_lo.x)[a] = float(world.lo[a]);
+            (&v.world_hi.x)[a] = float(world.hi[a]);
+        }
     v.lamp_ids = sc->lamp_ids.as<uint32_t>();
     v.lamp_count = uint32_t(lamp_ids.size());
     v.instance_count = tl.prims.empty() ? 0u : d->instance_count;
@@ -1713,6 +1723,7 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
     psy::LaunchConfig lc = ctx->launch;
     lc.sort_threshold = 0u;
     lc.shadow_sort_threshold = 0u;
+    lc.ray_sort_threshold = 0u;
     psy_render_stats stats{};
     PSY_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
     for (uint64_t sample = begin; sample < end;) {

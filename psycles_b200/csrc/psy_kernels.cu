@@ -180,8 +180,10 @@ __device__ __forceinline__ uint32_t warp_fetch(uint32_t *fetch_counter, uint32_t
 // kMulti: paths of a batched wavefront, each traced in its job's scene.
 template <bool kMulti>
 __global__ void __launch_bounds__(128, PSY_INTERSECT_MIN_BLOCKS)
-    k_intersect(const __grid_constant__ SceneView s_arg, const __grid_constant__ PathBuffers b, const JobGpu *jobs) {
+    k_intersect(const __grid_constant__ SceneView s_arg, const __grid_constant__ PathBuffers b, const JobGpu *jobs,
+                uint32_t sort_threshold) {
     const uint32_t count = b.counters[0];
+    const bool sorted = sort_threshold != 0u && count >= sort_threshold;
     TraversalState t;
     Hit best;
     bool has = false, active = false, exhausted = false;
@@ -189,7 +191,7 @@ __global__ void __launch_bounds__(128, PSY_INTERSECT_MIN_BLOCKS)
     for (;;) {
         const uint32_t q = warp_fetch(&b.counters[3], count, !active, exhausted);
         if (q != kInvalid) {
-            path = b.queue_in[q];
+            path = sorted ? b.queue_sorted[q] : b.queue_in[q];
             if (kMulti) job = b.job[path];
         }
         const SceneView &s = kMulti ? jobs[job].s : s_arg;
@@ -463,6 +465,40 @@ __global__ void __launch_bounds__(256) k_sort_scatter(const __grid_constant__ Pa
         const uint32_t packed = b.sort_keys[q];
         b.queue_sorted[hist[packed & (kSortBuckets - 1u)] + (packed >> 11)] = counter == 0u ? b.queue_in[q] : q;
     }
+}
+
+// Closest-hit rays grouped by where they start and where they head: the
+// direction octant and an 8 x 8 x 4 cell of the scene's bounds around the
+// origin, so a warp's rays walk the same part of the BVH.  Rays of a
+// batched wavefront are grouped per job as well.
+template <bool kMulti>
+__global__ void k_sort_count_rays(const __grid_constant__ SceneView s_arg, const __grid_constant__ PathBuffers b,
+                                  const JobGpu *jobs, uint32_t threshold) {
+    __shared__ uint32_t local[kSortBuckets];
+    const uint32_t count = b.counters[0];
+    if (count < threshold) return;
+    for (uint32_t k = threadIdx.x; k < kSortBuckets; k += blockDim.x) local[k] = 0u;
+    __syncthreads();
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+        const uint32_t i = b.queue_in[q];
+        const uint32_t job = kMulti ? b.job[i] : 0u;
+        const SceneView &s = kMulti ? jobs[job].s : s_arg;
+        const float4 o = b.ray_o[i], d = b.ray_d[i];
+        auto cell = [](float v, float lo, float hi, float n) {
+            const float f = hi > lo ? (v - lo) / (hi - lo) : 0.0f;
+            return uint32_t(fminf(fmaxf(f * n, 0.0f), n - 1.0f));
+        };
+        const uint32_t cx = cell(o.x, s.world_lo.x, s.world_hi.x, 8.0f);
+        const uint32_t cy = cell(o.y, s.world_lo.y, s.world_hi.y, 8.0f);
+        const uint32_t cz = cell(o.z, s.world_lo.z, s.world_hi.z, 4.0f);
+        const uint32_t octant = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+        const uint32_t key = ((octant << 8 | cz << 6 | cy << 3 | cx) + job * 977u) & (kSortBuckets - 1u);
+        b.sort_keys[q] = key;
+        atomicAdd(&local[key], 1u);
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < kSortBuckets; k += blockDim.x)
+        if (local[k]) atomicAdd(&b.sort_hist[k], local[k]);
 }
 
 // Shadow rays grouped by direction (octahedral map of the direction into a
@@ -1278,8 +1314,18 @@ int persistent_grid(uint32_t work, const LaunchConfig &lc) {
     return int(blocks < 1u ? 1u : (blocks > cap ? cap : blocks));
 }
 
+template <bool kMulti>
+void launch_ray_sort(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const PathBuffers &b, const JobGpu *jobs,
+                     uint32_t max_work) {
+    const uint32_t thr = lc.ray_sort_threshold;
+    k_sort_count_rays<kMulti><<<launch_grid(max_work, 256, lc), 256, 0, st>>>(s, b, jobs, thr);
+    k_sort_scan<<<1, 1024, 0, st>>>(b, thr, 0u);
+    const int scatter_blocks = std::max(launch_grid(max_work, 256, lc), int((max_work >> 20) + 1u));
+    k_sort_scatter<<<scatter_blocks, 256, 0, st>>>(b, thr, 0u);
+}
 void launch_intersect(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const PathBuffers &b, uint32_t max_work) {
-    k_intersect<false><<<persistent_grid(max_work, lc), 128, 0, st>>>(s, b, nullptr);
+    if (lc.ray_sort_threshold) launch_ray_sort<false>(st, lc, s, b, nullptr, max_work);
+    k_intersect<false><<<persistent_grid(max_work, lc), 128, 0, st>>>(s, b, nullptr, lc.ray_sort_threshold);
 }
 void launch_shade(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                   uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
@@ -1316,7 +1362,8 @@ void launch_raygen_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *
     k_raygen_batch<<<launch_grid(max_paths, 256, lc), 256, 0, st>>>(jobs, items, round, b);
 }
 void launch_intersect_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work) {
-    k_intersect<true><<<persistent_grid(max_work, lc), 128, 0, st>>>(SceneView{}, b, jobs);
+    if (lc.ray_sort_threshold) launch_ray_sort<true>(st, lc, SceneView{}, b, jobs, max_work);
+    k_intersect<true><<<persistent_grid(max_work, lc), 128, 0, st>>>(SceneView{}, b, jobs, lc.ray_sort_threshold);
 }
 void launch_shade_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work,
                         uint32_t step) {

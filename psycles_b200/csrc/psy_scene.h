@@ -122,6 +122,7 @@ struct SceneView {
     // order: bounding sphere (centre, radius^2) and light index
     const float4 *lamp_bounds;
     const LampConstGpu *lamp_consts;  // one per light
+    float4 world_lo, world_hi;        // bounds of the instances (xyz)
     const uint32_t *lamp_ids;
     uint32_t lamp_count;
     float triangle_area_pdf;

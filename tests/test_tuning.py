@@ -22,7 +22,7 @@ def _render(backend, compiled, st, spp):
 
 
 @pytest.mark.parametrize("tuning", [
-    {"sort_threshold": 1, "shadow_sort_threshold": 1},
+    {"sort_threshold": 1, "shadow_sort_threshold": 1, "ray_sort_threshold": 1},
     {"sort_threshold": 1, "shadow_sort_threshold": 0, "path_capacity": 3000, "traversal_blocks_per_sm": 2,
      "shade_blocks_per_sm": 1},
     {"stream_blocks_per_sm": 1, "traversal_blocks_per_sm": 64, "shade_blocks_per_sm": 64},
