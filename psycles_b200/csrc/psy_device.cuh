@@ -500,16 +500,12 @@ __device__ __forceinline__ void wide_slabs(const WideNodeRay &n, f3 oinv, f3 inv
         const float nr = fmaxf(fmaxf(x0, y0), fmaxf(z0, tmin));
         const float fr = fminf(fminf(x1, y1), fminf(z1, tmax));
         near[k] = nr;
-        hit[k] = nr <= fr * 1.00000095367431640625f + 1.0e-30f || nr <= fr;
+        hit[k] = nr <= fmaxf(fmaf(fr, 1.00000095367431640625f, 1.0e-30f), fr);
     }
 }
 
 constexpr int kStackSize = 48;
 
-// Stack entries carry a 2-bit tag: a TLAS node, a BLAS node (global index),
-// an instance to enter, or the marker that returns to the world ray.
-constexpr uint32_t kTagTlas = 0u, kTagBlas = 1u << 30, kTagInstance = 2u << 30, kTagLeave = 3u << 30;
-constexpr uint32_t kTagMask = 3u << 30;
 
 struct SlabRay {
     f3 o, d, inv, oinv;  // origin, clamped direction, reciprocal, origin * reciprocal
@@ -539,7 +535,7 @@ struct TraversalState {
     Ray ray;      // world ray
     SlabRay cur;  // slab ray of the current level
     float tmax;
-    uint32_t node, sp, inst, blas_base, tri_base, prim_offset;
+    uint32_t node, sp, inst, prim_offset;
     uint32_t visibility, src_obj, src_prim, light_obj, light_prim;
     uint32_t stack[kStackSize];
 };
@@ -553,7 +549,7 @@ __device__ __forceinline__ void traversal_begin(TraversalState &t, const SceneVi
     t.node = s.instance_count == 0u ? kTagLeave : kTagTlas;
     t.sp = 0u;
     t.inst = kInvalid;
-    t.blas_base = t.tri_base = t.prim_offset = 0u;
+    t.prim_offset = 0u;
     t.visibility = visibility;
     t.src_obj = src_obj;
     t.src_prim = src_prim;
@@ -574,8 +570,6 @@ __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneVi
                 const Xform w2o = load_xform(in.w2o);
                 t.cur = make_slab_ray(xform_point(w2o, t.ray.o), xform_direction(w2o, t.ray.d));
                 t.inst = idx;
-                t.blas_base = mesh.node_offset;
-                t.tri_base = mesh.tri_offset;
                 t.prim_offset = mesh.prim_offset;
                 if (t.sp < uint32_t(kStackSize)) t.stack[t.sp++] = kTagLeave;
                 t.node = kTagBlas | mesh.node_offset;
@@ -599,14 +593,17 @@ __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneVi
         float near[4];
         bool hit[4];
         wide_slabs(n, t.cur.oinv, t.cur.inv, t.ray.tmin, t.tmax, near, hit);
-        const int lk[4] = {n.link.x, n.link.y, n.link.z, n.link.w}, ct[4] = {n.count.x, n.count.y, n.count.z, n.count.w};
+        // a slot's link is a ready stack entry (tagged global node index or
+        // tagged instance) when its count is 0, else its first triangle
+        const uint32_t lk[4] = {uint32_t(n.link.x), uint32_t(n.link.y), uint32_t(n.link.z), uint32_t(n.link.w)};
+        const int ct[4] = {n.count.x, n.count.y, n.count.z, n.count.w};
         // leaves first: their triangles may shrink tmax before the inner
         // children are ordered
         if (blas) {
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                if (!hit[k] || lk[k] >= 0) continue;
-                const uint32_t first = t.tri_base + uint32_t(~lk[k]);
+                if (!hit[k] || ct[k] == 0) continue;
+                const uint32_t first = lk[k];
                 for (int q = 0; q < ct[k]; ++q) {
                     const float4 *tp = s.tris + 3u * (first + uint32_t(q));
                     const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
@@ -627,11 +624,9 @@ __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneVi
         uint32_t val[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            const bool inner = lk[k] >= 0;
-            const bool take = hit[k] && near[k] <= t.tmax && (inner || !blas);
+            const bool take = hit[k] && near[k] <= t.tmax && ct[k] == 0;
             key[k] = take ? near[k] : __int_as_float(0x7f800000);
-            val[k] = inner ? (blas ? (kTagBlas | (t.blas_base + uint32_t(lk[k]))) : uint32_t(lk[k]))
-                           : (kTagInstance | uint32_t(~lk[k]));
+            val[k] = lk[k];
         }
 #define PSY_CSWAP(i, j)                         \
     if (key[j] < key[i]) {                      \

@@ -489,14 +489,26 @@ struct Builder {
                     lo[a][k] = kids[k].lo[a];
                     hi[a][k] = kids[k].hi[a];
                 }
-                links[k] = kids[k].link >= 0 ? collapse(kids[k].link, wide) : kids[k].link;
-                counts[k] = kids[k].link >= 0 ? 0 : kids[k].count;
+                // the traversal pushes a count-0 slot's link as it is: a
+                // tagged node index (BLAS indices are made global when the
+                // meshes are concatenated) or a tagged instance; a leaf of
+                // triangles keeps its first primitive (made global likewise)
+                if (kids[k].link >= 0) {
+                    links[k] = int((leaf_is_id ? psy::kTagTlas : psy::kTagBlas) | uint32_t(collapse(kids[k].link, wide)));
+                    counts[k] = 0;
+                } else if (leaf_is_id) {
+                    links[k] = int(psy::kTagInstance | uint32_t(~kids[k].link));
+                    counts[k] = 0;
+                } else {
+                    links[k] = ~kids[k].link;
+                    counts[k] = kids[k].count;
+                }
             } else {
                 for (int a = 0; a < 3; ++a) {
                     lo[a][k] = INFINITY;
                     hi[a][k] = INFINITY;
                 }
-                links[k] = -1;
+                links[k] = int(psy::kInvalidId);
                 counts[k] = 0;
             }
         }
@@ -1066,6 +1078,17 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         }
         g.node_offset = uint32_t(blas.size());
         g.tri_offset = uint32_t(tris.size() / 3u);
+        // global node and triangle indices of the mesh's links
+        for (psy::WideNodeGpu &w : mesh_wide[i]) {
+            int *lk = &w.link.x;
+            const int *ct = &w.count.x;
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t v = uint32_t(lk[k]);
+                if (ct[k] > 0) lk[k] = int(v + g.tri_offset);
+                else if (v != psy::kInvalidId && (v & psy::kTagMask) == psy::kTagBlas)
+                    lk[k] = int(psy::kTagBlas | ((v & ~psy::kTagMask) + g.node_offset));
+            }
+        }
         blas.insert(blas.end(), mesh_wide[i].begin(), mesh_wide[i].end());
         std::vector<psy::WideNodeGpu>().swap(mesh_wide[i]);
         for (const uint32_t id : mesh_order[i]) {

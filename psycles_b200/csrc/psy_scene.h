@@ -42,6 +42,16 @@ static_assert(sizeof(BvhNodeGpu) == 64, "BVH node is one 64-byte line");
 // link >= 0: inner node (relative to the BVH's first node); link < 0 with
 // count > 0: a leaf (~first triangle, or ~instance in the TLAS); count 0
 // with link < 0: an empty slot.
+// Traversal stack entries carry a 2-bit tag: a TLAS node, a BLAS node
+// (global index), an instance to enter, or the marker that returns to the
+// world ray.
+constexpr uint32_t kTagTlas = 0u, kTagBlas = 1u << 30, kTagInstance = 2u << 30, kTagLeave = 3u << 30;
+constexpr uint32_t kTagMask = 3u << 30;
+
+// Four children of a wide BVH node: boxes as six planes of four lanes, and
+// per child either a ready stack entry (count 0: a tagged global node index
+// or, in the TLAS, a tagged instance) or the first of `count` triangles in
+// the global triangle array.  Empty slots have +inf planes and count 0.
 struct alignas(16) WideNodeGpu {
     float4 lox, hix, loy, hiy, loz, hiz;
     int4 link;
