@@ -507,6 +507,12 @@ __device__ __forceinline__ void wide_slabs(const WideNodeRay &n, f3 oinv, f3 inv
 constexpr int kStackSize = 48;
 
 
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 struct SlabRay {
     f3 o, d, inv, oinv;  // origin, clamped direction, reciprocal, origin * reciprocal
     uint32_t neg;        // bit a: direction component a is negative
@@ -516,7 +522,10 @@ __device__ __forceinline__ SlabRay make_slab_ray(f3 o, f3 raw) {
     SlabRay r;
     r.o = o;
     r.d = mk3(clamp_bvh_direction(raw.x), clamp_bvh_direction(raw.y), clamp_bvh_direction(raw.z));
-    r.inv = mk3(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
+    // the slab test only has to be conservative, which its padding and far
+    // widening keep with the hardware's approximate reciprocal (relative
+    // error below 2^-22); the triangle test uses the clamped direction itself
+    r.inv = mk3(rcp_approx(r.d.x), rcp_approx(r.d.y), rcp_approx(r.d.z));
     r.oinv = mk3(o.x * r.inv.x, o.y * r.inv.y, o.z * r.inv.z);
     r.neg = (r.d.x < 0.0f ? 1u : 0u) | (r.d.y < 0.0f ? 2u : 0u) | (r.d.z < 0.0f ? 4u : 0u);
     return r;
