@@ -421,9 +421,11 @@ def run_serving(backend, jobs: int = 32, rate: float = 200.0, capacity: int = 0)
             th.join()
             st = server.stats()
             extra = {"wavefronts": int(st.wavefronts), "server_p50_ms": st.latency_p50_ms,
-                     "server_p99_ms": st.latency_p99_ms, "bytes_peak": int(st.bytes_peak)}
+                     "server_p99_ms": st.latency_p99_ms, "bytes_peak": int(st.bytes_peak),
+                     "device_busy_s": st.busy_ms / 1e3}
             server.close()
         else:
+            device_ms = 0.0
             for i, j in edits:
                 delay = j["arrival"] - (time.perf_counter() - t0)
                 if delay > 0:
@@ -432,13 +434,14 @@ def run_serving(backend, jobs: int = 32, rate: float = 200.0, capacity: int = 0)
                 sess = backend.create_session(current[j["scene"]], settings(j))
                 sess.set_camera(j["camera"])
                 assert sess.render_samples(SampleRange(0, j["spp"], 0, j["spp"])), sess.diagnostics
+                device_ms += sess.stats().ms_total
                 for k in passes:
                     sess.read_pass(k)
                 sess.close()
                 now = time.perf_counter() - t0
                 latencies.append((now - j["arrival"]) * 1e3)
                 t_done = now
-            extra = {}
+            extra = {"device_busy_s": device_ms / 1e3}
         for c in list(compiled) + list(recompiled.values()):
             c.close()
         lat = np.array(latencies)

@@ -629,7 +629,7 @@ psy_status ensure_capacity(psy_session *s, uint32_t n) {
     return s->scene->context->arena.ensure(n, false);
 }
 
-psy_status clear_film(psy_session *s) {
+psy_status clear_film(psy_session *s, bool sync = true) {
     cudaStream_t st = s->scene->context->stream;
     const size_t n = s->pixels;
     PSY_CUDA_TRY(s->combined.alloc(sizeof(float4) * n));
@@ -640,7 +640,7 @@ psy_status clear_film(psy_session *s) {
     PSY_CUDA_TRY(cudaMemsetAsync(s->normal.ptr, 0, sizeof(float4) * n, st));
     PSY_CUDA_TRY(cudaMemsetAsync(s->albedo.ptr, 0, sizeof(float4) * n, st));
     PSY_CUDA_TRY(cudaMemsetAsync(s->sample_count.ptr, 0, sizeof(uint32_t) * n, st));
-    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    if (sync) PSY_CUDA_TRY(cudaStreamSynchronize(st));
     s->rendered = 0;
     s->total = 0;
     return PSY_OK;
@@ -724,6 +724,23 @@ psy::LampConstGpu lamp_constants(const psy_light_desc &l) {
     return c;
 }
 
+// Argument checks of a parameter-only edit: the material exists and the
+// new block has the compiled block's layout.
+psy_status check_rebind(const psy_scene *s, uint32_t material, const float *scalars, uint32_t scalar_count,
+                        const float *vectors, uint32_t vector_count) {
+    if (!s) return fail(PSY_ERROR_INVALID_ARGUMENT, "null scene");
+    if (material >= s->materials.size()) return fail(PSY_ERROR_INVALID_ARGUMENT, "material out of range");
+    const psy::MaterialGpu &m = s->materials[material];
+    const uint32_t next_scalar =
+        material + 1 < s->materials.size() ? s->materials[material + 1].scalar_offset : uint32_t(s->scalars.size());
+    const uint32_t next_vector = material + 1 < s->materials.size() ? s->materials[material + 1].vector_offset
+                                                                    : uint32_t(s->vectors.size() / 3u);
+    if (scalar_count != next_scalar - m.scalar_offset || vector_count != next_vector - m.vector_offset)
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "parameter block layout differs from the compiled program");
+    if ((scalar_count && !scalars) || (vector_count && !vectors)) return fail(PSY_ERROR_INVALID_ARGUMENT, "null parameters");
+    return PSY_OK;
+}
+
 // Runs body(i) for every i in [0, n) on up to 32 host threads that pull
 // indices from a shared counter; `threads` receives the count used.  An
 // exception in a body (out of host memory) becomes PSY_ERROR_OUT_OF_MEMORY.
@@ -750,12 +767,29 @@ psy_status parallel_for(uint32_t n, uint32_t *threads, F &&body) {
     return failed.load() ? fail(PSY_ERROR_OUT_OF_MEMORY, "host memory exhausted while building the scene") : PSY_OK;
 }
 
+// Uploads `v` into a new device buffer that takes the place of `slot`; the
+// buffer it replaces joins the scene's retired list.
+// The new buffer is stream-ordered on the context's stream, and the host
+// copy it is uploaded from stays alive with the retired list, so the caller
+// need not wait for the upload.
+template <typename T>
+cudaError_t replace_buffer(psy_scene *sc, DeviceBuffer &slot, const std::vector<T> &v) {
+    auto source = std::make_shared<const std::vector<T>>(v);
+    auto fresh = std::make_unique<DeviceBuffer>(sc->context->stream);
+    const cudaError_t e = fresh->upload(*source, sc->context->stream);
+    if (e != cudaSuccess) return e;
+    slot.swap(*fresh);
+    if (fresh->ptr) sc->retired.push_back(std::move(fresh));
+    sc->retired_host.push_back(std::move(source));
+    return cudaSuccess;
+}
+
 // The many-light tree over the scene's emitter population -- emissive
 // triangles in emitter order, then the analytic lights -- built from the
 // host copies and uploaded (src/luisa/path_tracer_light_sampling_scene.cpp:
 // 160-240).  A tree whose root carries no energy is left empty, and
 // sessions then select lights from the flat distribution.
-psy_status build_light_tree(psy_scene *sc) {
+psy_status build_light_tree(psy_scene *sc, bool sync = true) {
     const auto t0 = std::chrono::steady_clock::now();
     std::vector<psy::LtNodeGpu> lt_nodes;
     std::vector<psy::LtEmitterGpu> lt_emitters;
@@ -827,11 +861,13 @@ psy_status build_light_tree(psy_scene *sc) {
     }
     cudaStream_t st = sc->context->stream;
     PSY_CUDA_TRY(cudaSetDevice(sc->context->device));
-    PSY_CUDA_TRY(sc->lt_nodes.upload(lt_nodes, st));
-    PSY_CUDA_TRY(sc->lt_emitters.upload(lt_emitters, st));
-    PSY_CUDA_TRY(sc->lt_mapping.upload(lt_mapping, st));
-    PSY_CUDA_TRY(sc->lt_lookup.upload(lt_lookup, st));
-    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    // new buffers; a tree built before is retired, not freed, as queued
+    // work may still read it
+    PSY_CUDA_TRY(replace_buffer(sc, sc->lt_nodes, lt_nodes));
+    PSY_CUDA_TRY(replace_buffer(sc, sc->lt_emitters, lt_emitters));
+    PSY_CUDA_TRY(replace_buffer(sc, sc->lt_mapping, lt_mapping));
+    PSY_CUDA_TRY(replace_buffer(sc, sc->lt_lookup, lt_lookup));
+    if (sync) PSY_CUDA_TRY(cudaStreamSynchronize(st));
     psy::SceneView &v = sc->view;
     v.lt_nodes = sc->lt_nodes.as<psy::LtNodeGpu>();
     v.lt_emitters = sc->lt_emitters.as<psy::LtEmitterGpu>();
@@ -848,6 +884,38 @@ psy_status build_light_tree(psy_scene *sc) {
 }
 
 }  // namespace
+
+psy_status psy::host::rebind_parameters_versioned(psy_scene *s, uint32_t material, const float *scalars,
+                                                  uint32_t scalar_count, const float *vectors, uint32_t vector_count) {
+    const psy_status valid = check_rebind(s, material, scalars, scalar_count, vectors, vector_count);
+    if (valid != PSY_OK) return valid;
+    const psy::MaterialGpu &m = s->materials[material];
+    PSY_CUDA_TRY(cudaSetDevice(s->context->device));
+    if (scalar_count) std::memcpy(s->scalars.data() + m.scalar_offset, scalars, sizeof(float) * scalar_count);
+    if (vector_count) std::memcpy(s->vectors.data() + 3ull * m.vector_offset, vectors, sizeof(float) * 3u * vector_count);
+    PSY_CUDA_TRY(replace_buffer(s, s->scalar_buf, s->scalars));
+    PSY_CUDA_TRY(replace_buffer(s, s->vector_buf, s->vectors));
+    s->view.scalars = s->scalar_buf.as<float>();
+    s->view.vectors = s->vector_buf.as<float>();
+    if (m.has_emission) {
+        std::lock_guard<std::mutex> lock(s->light_tree_mutex);
+        if (s->light_tree_built) {
+            const psy_status r = build_light_tree(s, false);
+            if (r != PSY_OK) return r;
+        }
+    }
+    if (!s->uploads_done) PSY_CUDA_TRY(cudaEventCreateWithFlags(&s->uploads_done, cudaEventDisableTiming));
+    PSY_CUDA_TRY(cudaEventRecord(s->uploads_done, s->context->stream));
+    return PSY_OK;
+}
+
+void psy::host::release_retired(psy_scene *s) {
+    if (!s || (s->retired.empty() && s->retired_host.empty())) return;
+    cudaSetDevice(s->context->device);
+    s->retired.clear();  // stream-ordered frees: after all work queued so far
+    // host sources go once their uploads have run
+    if (!s->uploads_done || cudaEventQuery(s->uploads_done) == cudaSuccess) s->retired_host.clear();
+}
 
 psy_status psy::host::ensure_light_tree(psy_scene *sc) {
     std::lock_guard<std::mutex> lock(sc->light_tree_mutex);
@@ -910,6 +978,13 @@ psy_status psy_context_create(int device, psy_context **out) {
     cudaDeviceProp prop{};
     PSY_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10) return fail(PSY_ERROR_UNSUPPORTED, "libpsycles_cuda is built for sm_100a (B200)");
+    // stream-ordered buffers (render-server sessions, edited parameter
+    // blocks) come from the device's default pool; freed memory stays in the
+    // pool for the next job instead of going back to the driver
+    cudaMemPool_t pool = nullptr;
+    PSY_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;
+    PSY_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     auto c = std::make_unique<psy_context>();
     c->device = device;
     c->sms = prop.multiProcessorCount;
@@ -1289,6 +1364,10 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->tri_materials.upload(tri_materials, st));
     PSY_CUDA_TRY(sc->material_buf.upload(sc->materials, st));
     PSY_CUDA_TRY(sc->code.upload(code, st));
+    // parameter blocks are replaced by edits while work may still read them:
+    // stream-ordered, so retiring them never waits on the device
+    sc->scalar_buf.ordered = st;
+    sc->vector_buf.ordered = st;
     PSY_CUDA_TRY(sc->scalar_buf.upload(sc->scalars, st));
     PSY_CUDA_TRY(sc->vector_buf.upload(sc->vectors, st));
     PSY_CUDA_TRY(sc->emitters.upload(emitters, st));
@@ -1371,6 +1450,10 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
 void psy_scene_destroy(psy_scene *s) {
     if (!s) return;
     cudaSetDevice(s->context->device);
+    if (s->uploads_done) {
+        cudaEventSynchronize(s->uploads_done);
+        cudaEventDestroy(s->uploads_done);
+    }
     delete s;
 }
 
@@ -1378,16 +1461,9 @@ uint64_t psy_scene_source_revision(const psy_scene *s) { return s ? s->revision 
 
 psy_status psy_scene_rebind_parameters(psy_scene *s, uint32_t material, const float *scalars, uint32_t scalar_count,
                                        const float *vectors, uint32_t vector_count) {
-    if (!s) return fail(PSY_ERROR_INVALID_ARGUMENT, "null scene");
-    if (material >= s->materials.size()) return fail(PSY_ERROR_INVALID_ARGUMENT, "material out of range");
+    const psy_status valid = check_rebind(s, material, scalars, scalar_count, vectors, vector_count);
+    if (valid != PSY_OK) return valid;
     const psy::MaterialGpu &m = s->materials[material];
-    const uint32_t next_scalar =
-        material + 1 < s->materials.size() ? s->materials[material + 1].scalar_offset : uint32_t(s->scalars.size());
-    const uint32_t next_vector = material + 1 < s->materials.size() ? s->materials[material + 1].vector_offset
-                                                                    : uint32_t(s->vectors.size() / 3u);
-    if (scalar_count != next_scalar - m.scalar_offset || vector_count != next_vector - m.vector_offset)
-        return fail(PSY_ERROR_INVALID_ARGUMENT, "parameter block layout differs from the compiled program");
-    if ((scalar_count && !scalars) || (vector_count && !vectors)) return fail(PSY_ERROR_INVALID_ARGUMENT, "null parameters");
     cudaStream_t st = s->context->stream;
     PSY_CUDA_TRY(cudaSetDevice(s->context->device));
     if (scalar_count) {
@@ -1405,8 +1481,14 @@ psy_status psy_scene_rebind_parameters(psy_scene *s, uint32_t material, const fl
     // built tree when an emissive material changes, as a recompile would
     if (m.has_emission) {
         std::lock_guard<std::mutex> lock(s->light_tree_mutex);
-        if (s->light_tree_built) return build_light_tree(s);
+        if (s->light_tree_built) {
+            const psy_status r = build_light_tree(s);
+            if (r != PSY_OK) return r;
+        }
     }
+    // renders through a session are synchronous: nothing queued reads the
+    // replaced tree any more
+    release_retired(s);
     return PSY_OK;
 }
 
@@ -1438,6 +1520,40 @@ psy_status psy_session_create(psy_scene *scene, const psy_render_settings *setti
     *out = s.release();
     return PSY_OK;
 }
+
+}  // extern "C"
+
+psy_status psy::host::create_server_session(psy_scene *scene, const psy_render_settings &settings,
+                                            const psy_camera_desc *camera, psy_session **out) {
+    *out = nullptr;
+    PSY_CUDA_TRY(cudaSetDevice(scene->context->device));
+    cudaStream_t st = scene->context->stream;
+    auto s = std::make_unique<psy_session>();
+    s->scene = scene;
+    s->settings = settings;
+    for (DeviceBuffer *b : {&s->sobol, &s->filter, &s->combined, &s->normal, &s->albedo, &s->sample_count, &s->trace_buf})
+        b->ordered = st;
+    s->has_camera = camera != nullptr;
+    if (camera) s->camera = *camera;
+    psy_status r = derive_params(s.get(), settings);
+    if (r != PSY_OK) return r;
+    // (copies from pageable host memory are staged before the call returns,
+    // so the temporary tables may go at once)
+    const auto table = filter_table(settings.pixel_filter, settings.filter_width);
+    const std::vector<float> tv(table.begin(), table.end());
+    PSY_CUDA_TRY(s->filter.upload(tv, st));
+    s->params.filter = s->filter.as<float>();
+    if ((r = clear_film(s.get(), false)) != PSY_OK) return r;
+    PSY_CUDA_TRY(s->trace_buf.alloc(sizeof(psy_path_trace)));
+    PSY_CUDA_TRY(cudaEventCreate(&s->ev_begin));
+    PSY_CUDA_TRY(cudaEventCreate(&s->ev_end));
+    PSY_CUDA_TRY(cudaEventCreate(&s->ev_k[0]));
+    PSY_CUDA_TRY(cudaEventCreate(&s->ev_k[1]));
+    *out = s.release();
+    return PSY_OK;
+}
+
+extern "C" {
 
 void psy_session_destroy(psy_session *s) {
     if (!s) return;

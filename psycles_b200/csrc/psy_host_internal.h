@@ -13,6 +13,7 @@ struct psy_session;
 
 #include <algorithm>
 #include <atomic>
+#include <memory>
 #include <mutex>
 #include <cstddef>
 #include <cstdint>
@@ -37,18 +38,43 @@ uint64_t scene_device_bytes(const psy_scene *s);
 // on first use, not by psy_scene_compile).
 psy_status ensure_light_tree(psy_scene *s);
 
+// Parameter-only material edit that leaves the device data of work already
+// queued intact: the parameter block (and a rebuilt light tree) go to new
+// device buffers and the scene's view points at them; the old buffers are
+// kept until release_retired.  Work planned afterwards sees the edit.
+psy_status rebind_parameters_versioned(psy_scene *s, uint32_t material, const float *scalars, uint32_t scalar_count,
+                                       const float *vectors, uint32_t vector_count);
+// Frees the buffers earlier edits retired; no queued work may read them.
+void release_retired(psy_scene *s);
+
 // The job record of a session for a multi-job wavefront.
 JobGpu session_job(const psy_session *s, const RenderParams &p);
 
+// psy_session_create (+ psy_session_set_camera when `camera` is set) for a
+// render server: the session's buffers are stream-ordered and nothing waits
+// for the context's stream, so admitting a job does not stall wavefronts in
+// flight.
+psy_status create_server_session(psy_scene *scene, const psy_render_settings &settings, const psy_camera_desc *camera,
+                                 psy_session **out);
+
+// Device memory.  A buffer bound to a stream (`ordered`) is allocated and
+// freed in that stream's order (cudaMallocAsync / cudaFreeAsync), so
+// freeing it neither waits for nor disturbs work queued on other buffers;
+// otherwise cudaMalloc / cudaFree.
 struct DeviceBuffer {
     void *ptr = nullptr;
     size_t bytes = 0;
+    cudaStream_t ordered = nullptr;
     DeviceBuffer() = default;
+    explicit DeviceBuffer(cudaStream_t st) : ordered(st) {}
     DeviceBuffer(const DeviceBuffer &) = delete;
     DeviceBuffer &operator=(const DeviceBuffer &) = delete;
     ~DeviceBuffer() { release(); }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) {
+            if (ordered) cudaFreeAsync(ptr, ordered);
+            else cudaFree(ptr);
+        }
         ptr = nullptr;
         bytes = 0;
     }
@@ -56,7 +82,7 @@ struct DeviceBuffer {
         release();
         bytes = n;
         if (n == 0) return cudaSuccess;
-        return cudaMalloc(&ptr, n);
+        return ordered ? cudaMallocAsync(&ptr, n, ordered) : cudaMalloc(&ptr, n);
     }
     template <typename T>
     cudaError_t upload(const std::vector<T> &v, cudaStream_t st) {
@@ -67,6 +93,11 @@ struct DeviceBuffer {
     template <typename T>
     T *as() const {
         return static_cast<T *>(ptr);
+    }
+    void swap(DeviceBuffer &o) noexcept {
+        std::swap(ptr, o.ptr);
+        std::swap(bytes, o.bytes);
+        std::swap(ordered, o.ordered);
     }
 };
 
@@ -125,6 +156,10 @@ struct psy_scene {
     std::vector<uint8_t> instance_mirrored;  // object-to-world determinant < 0
     std::mutex light_tree_mutex;
     bool light_tree_built = false;
+    // device buffers replaced by edits while work still read them
+    std::vector<std::unique_ptr<psy::host::DeviceBuffer>> retired;
+    std::vector<std::shared_ptr<const void>> retired_host;  // host sources of uploads not yet waited for
+    cudaEvent_t uploads_done = nullptr;                      // recorded after the latest edit's uploads
 };
 
 struct psy_session {

@@ -9,12 +9,16 @@
 // from the running jobs in admission order -- the oldest job takes all the
 // samples that fit and younger jobs backfill the rest (continuous batching:
 // a job admitted while others are on the GPU joins the next wavefront), so
-// small jobs share the device with large ones without delaying them.  Two wavefronts are in flight: the host plans and admits for
-// the next while the GPU runs the current one.  A job is done once the
-// wavefront holding its last samples has finished.  Because every pixel
-// adds its samples in order, a job's passes are the same alone and in any
-// mix.  An edit waits at the head of the FIFO until no running job uses its
-// scene, so each job sees one parameter state.
+// small jobs share the device with large ones without delaying them.  Two
+// wavefronts are in flight: the host plans and admits for the next while
+// the GPU runs the current one.  A job is done once the wavefront holding
+// its last samples has finished.  Because every pixel adds its samples in
+// order, a job's passes are the same alone and in any mix.  An edit takes
+// effect when it reaches the head of the FIFO, without waiting for running
+// jobs: it writes a new copy of the scene's parameter block (and of a light
+// tree it changes), running jobs keep reading the copy they were admitted
+// with, and the old copy is freed once no running job uses the scene -- so
+// each job sees exactly the edits submitted before it.
 #include "psy_engine.h"
 
 #include <algorithm>
@@ -25,6 +29,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <thread>
 #include <vector>
 
@@ -86,6 +91,7 @@ struct psy_server {
     std::deque<Request> fifo;
     std::map<uint64_t, std::unique_ptr<Job>> jobs;
     std::map<const psy_scene *, uint64_t> scene_bytes;
+    std::set<psy_scene *> retired_scenes;  // scenes holding buffers that running jobs read
     std::vector<uint32_t> free_slots;
     uint64_t next_id = 1;
     uint64_t bytes_in_use = 0, bytes_peak = 0, fixed_bytes = 0;
@@ -106,13 +112,18 @@ struct psy_server {
         while (!fifo.empty()) {
             Request &head = fifo.front();
             if (head.edit) {
-                const psy_scene *sc = head.edit->scene;
-                if (std::any_of(running.begin(), running.end(), [sc](const Job *j) { return j->scene == sc; })) return;
+                // running jobs keep the parameter block they were admitted
+                // with; jobs admitted from here on see the edit
+                psy_scene *sc = head.edit->scene;
                 const Edit &e = *head.edit;
-                const psy_status r = psy_scene_rebind_parameters(head.edit->scene, e.material, e.scalars.data(),
+                const psy_status r = rebind_parameters_versioned(sc, e.material, e.scalars.data(),
                                                                  uint32_t(e.scalars.size()), e.vectors.data(),
                                                                  uint32_t(e.vectors.size() / 3u));
                 if (r != PSY_OK) loop_error = std::string("edit rejected: ") + psy_last_error();
+                if (std::none_of(running.begin(), running.end(), [sc](const Job *j) { return j->scene == sc; }))
+                    release_retired(sc);
+                else
+                    retired_scenes.insert(sc);
                 fifo.pop_front();
                 continue;
             }
@@ -160,8 +171,7 @@ struct psy_server {
             if (bytes_in_use + need > config.hbm_budget_bytes || free_slots.empty()) return;
             // admission: the job's session holds its film and tables
             psy_session *s = nullptr;
-            psy_status r = psy_session_create(j.scene, &j.settings, &s);
-            if (r == PSY_OK && j.has_camera) r = psy_session_set_camera(s, &j.camera);
+            psy_status r = create_server_session(j.scene, j.settings, j.has_camera ? &j.camera : nullptr, &s);
             psy::RenderParams p{};
             if (r == PSY_OK) r = prepare_render(s, 0u, j.samples, 0u, j.samples, &p);
             const uint32_t slot = free_slots.back();
@@ -312,7 +322,20 @@ struct psy_server {
                     it = running.erase(it);
                     any = true;
                 }
-                if (any) done_cv.notify_all();
+                if (any) {
+                    // buffers replaced by edits are freed once no running
+                    // job reads their scene
+                    for (auto it = retired_scenes.begin(); it != retired_scenes.end();) {
+                        psy_scene *sc = *it;
+                        if (std::any_of(running.begin(), running.end(), [sc](const Job *j) { return j->scene == sc; })) {
+                            ++it;
+                            continue;
+                        }
+                        release_retired(sc);
+                        it = retired_scenes.erase(it);
+                    }
+                    done_cv.notify_all();
+                }
             }
         }
         for (auto &f : flight) {

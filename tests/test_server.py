@@ -128,3 +128,32 @@ def test_cancel_and_errors(backend):
         server.release(12345)
     assert server.wait(long_job, 1) == _abi.PSY_OK
     server.close()
+
+
+def test_emissive_edit_while_a_tree_job_runs(backend):
+    """An edit of an emissive material reaches the server while a job that
+    samples the light tree is running: that job keeps the tree and the
+    parameter block it was admitted with, the next job sees the edited
+    ones, each equal to a session alone on a scene compiled with the same
+    parameters."""
+    import copy
+    scene = scenes.small_test_scene(seed=3)
+    k = next(i for i, m in enumerate(scene.materials) if m.program.has_emission and m.parameters.scalars.size)
+    sc = scene.materials[k].parameters.scalars * np.float32(2.5)
+    vc = scene.materials[k].parameters.vectors[::-1].copy()
+    comp = backend.compile_scene(scene).scene
+    st_a = scenes.render_settings(160, 120, max_bounces=5, use_light_tree=1)
+    st_b = scenes.render_settings(48, 40, max_bounces=5, use_light_tree=1)
+    server = RenderServer(backend.context, path_capacity=40000)
+    a = server.submit(comp, st_a, 32)
+    server.rebind_parameters(comp, k, sc, vc)
+    b = server.submit(comp, st_b, 4)
+    ra, rb = _from_server(server, a, 160, 120), _from_server(server, b, 48, 40)
+    server.close()
+    ref_a = _alone(backend, backend.compile_scene(scene).scene, st_a, 32)
+    edited = copy.deepcopy(scene)
+    edited.materials[k].parameters.scalars[:] = sc
+    edited.materials[k].parameters.vectors[:] = vc
+    ref_b = _alone(backend, backend.compile_scene(edited).scene, st_b, 4)
+    assert _same(ra, ref_a)
+    assert _same(rb, ref_b)
