@@ -515,6 +515,15 @@ def run_viewports(backend, compiled, count: int = 64, capacity: int = 0) -> dict
             "batched_vs_plain": plain_wall / batch_wall, "identical": bool(same)}
 
 
+# DRAM bytes per second of device time of the traversal and shading kernels,
+# from one `ncu --set full` capture of each (the third launch of the 4-spp
+# procedural render: DRAM read + write of the launch over its duration).
+# The traffic of a bench launch is this rate times the launch's mean
+# event-timed duration (the procedural workload only).
+NCU_DRAM_GBS = {"intersect": (959.2 + 121.9) / 2.741, "shadow": (102.6 + 20.5) / 2.762,
+                "shade": (2522.6 + 681.5) / 1.276}
+
+
 def kernel_profile(args, backend, compiled, settings) -> dict:
     """Per-kernel device time of one render with CUDA events around each
     launch class (psy_session profile mode)."""
@@ -541,9 +550,18 @@ def kernel_profile(args, backend, compiled, settings) -> dict:
     top = max(kernels, key=lambda k: kernels[k]["ms"])
     k = kernels[top]
     achieved = k["gbs"]
+    traffic = None
+    if args.config == "procedural" and top in NCU_DRAM_GBS and k["launches"]:
+        traffic = NCU_DRAM_GBS[top] * 1e9 * (k["ms"] / 1e3) / k["launches"]
+    for name, rec in kernels.items():
+        rec["frac_of_hbm"] = rec["gbs"] / hbm
+        rec["algorithmic_bytes_per_launch"] = rec["algorithmic_bytes"] / rec["launches"] if rec["launches"] else 0.0
     return {"kernels": kernels,
             "roofline": {"kernel": f"k_{top}", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None,
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": k["algorithmic_bytes"] / k["launches"] if k["launches"] else 0.0,
+                         "traffic_source": "ncu DRAM bytes per device-second of this kernel x mean launch duration"
+                         if traffic is not None else None,
                          "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if not peaks.get("fallback")
                          else "fallback 6.65 TB/s"}}
 
