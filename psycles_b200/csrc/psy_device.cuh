@@ -567,7 +567,10 @@ __device__ __forceinline__ void traversal_begin(TraversalState &t, const SceneVi
 }
 
 // Advances at most `budget` loop iterations; true once the traversal ended.
-template <typename OnHit>
+// kNearFirst orders a node's hit children nearest first (closest hit);
+// without it they are pushed in slot order (any-hit queries, which visit
+// every candidate or stop at the first blocker regardless of order).
+template <bool kNearFirst = true, typename OnHit>
 __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneView &s, int budget, OnHit on_hit) {
     for (int it = 0; it < budget; ++it) {
         const uint32_t tag = t.node & kTagMask;
@@ -627,41 +630,56 @@ __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneVi
                 }
             }
         }
-        // inner children (and TLAS instances) nearest first: sort the four
-        // (distance, entry) pairs, misses last
-        float key[4];
-        uint32_t val[4];
+        if constexpr (!kNearFirst) {
+            uint32_t next = kInvalid;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const bool take = hit[k] && near[k] <= t.tmax && ct[k] == 0;
-            key[k] = take ? near[k] : __int_as_float(0x7f800000);
-            val[k] = lk[k];
-        }
-#define PSY_CSWAP(i, j)                         \
-    if (key[j] < key[i]) {                      \
-        const float tk = key[i];                \
-        key[i] = key[j];                        \
-        key[j] = tk;                            \
-        const uint32_t tv = val[i];             \
-        val[i] = val[j];                        \
-        val[j] = tv;                            \
+            for (int k = 0; k < 4; ++k) {
+                if (!(hit[k] && near[k] <= t.tmax && ct[k] == 0)) continue;
+                if (next != kInvalid && t.sp < uint32_t(kStackSize)) t.stack[t.sp++] = next;
+                next = lk[k];
+            }
+            if (next == kInvalid) {
+                if (t.sp == 0u) return true;
+                next = t.stack[--t.sp];
+            }
+            t.node = next;
+        } else {
+            // inner children (and TLAS instances) nearest first: sort the four
+            // (distance, entry) pairs, misses last
+            float key[4];
+            uint32_t val[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const bool take = hit[k] && near[k] <= t.tmax && ct[k] == 0;
+                key[k] = take ? near[k] : __int_as_float(0x7f800000);
+                val[k] = lk[k];
+            }
+#define PSY_CSWAP(i, j)                 \
+    if (key[j] < key[i]) {              \
+        const float tk = key[i];        \
+        key[i] = key[j];                \
+        key[j] = tk;                    \
+        const uint32_t tv = val[i];     \
+        val[i] = val[j];                \
+        val[j] = tv;                    \
     }
-        PSY_CSWAP(0, 1)
-        PSY_CSWAP(2, 3)
-        PSY_CSWAP(0, 2)
-        PSY_CSWAP(1, 3)
-        PSY_CSWAP(1, 2)
+            PSY_CSWAP(0, 1)
+            PSY_CSWAP(2, 3)
+            PSY_CSWAP(0, 2)
+            PSY_CSWAP(1, 3)
+            PSY_CSWAP(1, 2)
 #undef PSY_CSWAP
-        const float kInf = __int_as_float(0x7f800000);
-        if (key[0] == kInf) {
-            if (t.sp == 0u) return true;
-            t.node = t.stack[--t.sp];
-            continue;
-        }
+            const float kInf = __int_as_float(0x7f800000);
+            if (key[0] == kInf) {
+                if (t.sp == 0u) return true;
+                t.node = t.stack[--t.sp];
+                continue;
+            }
 #pragma unroll
-        for (int k = 3; k >= 1; --k)
-            if (key[k] != kInf && t.sp < uint32_t(kStackSize)) t.stack[t.sp++] = val[k];
-        t.node = val[0];
+            for (int k = 3; k >= 1; --k)
+                if (key[k] != kInf && t.sp < uint32_t(kStackSize)) t.stack[t.sp++] = val[k];
+            t.node = val[0];
+        }
     }
     return false;
 }

@@ -1067,13 +1067,13 @@ __global__ void __launch_bounds__(128, PSY_SHADOW_MIN_BLOCKS)
         if (!active) continue;
         bool done;
         if (!s.any_transparent) {
-            done = traversal_steps(t, s, kTraversalBudget, [&](uint32_t, uint32_t, uint32_t, float, float, float) {
+            done = traversal_steps<false>(t, s, kTraversalBudget, [&](uint32_t, uint32_t, uint32_t, float, float, float) {
                 blocked = true;
                 return true;
             });
         } else {
-            done = traversal_steps(t, s, kTraversalBudget,
-                                   [&](uint32_t ii, uint32_t local, uint32_t cp, float th, float, float) {
+            done = traversal_steps<false>(t, s, kTraversalBudget,
+                                          [&](uint32_t ii, uint32_t local, uint32_t cp, float th, float, float) {
                 const uint32_t mi = surface_material(s, ii, local);
                 if (!s.materials[mi].has_transparent) {
                     blocked = true;
