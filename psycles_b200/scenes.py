@@ -122,6 +122,44 @@ def camera_desc(cam: "Camera") -> _abi.CameraDesc:
     return c
 
 
+def _material_descs(mats) -> tuple:
+    """psy_material_desc array of `mats`: every program, scalar block and
+    vector block concatenated into one array each, and the descriptors
+    filled as one structured numpy array (a scene may hold thousands of
+    materials; per-material ctypes pointers would dominate its flattening)."""
+    n = max(len(mats), 1)
+    codes = [np.ascontiguousarray(cm.program.closures, dtype=np.uint32).reshape(-1, 5) for cm in mats]
+    scal = [np.ascontiguousarray(cm.parameters.scalars, dtype=np.float32).reshape(-1) for cm in mats]
+    vecs = [np.ascontiguousarray(cm.parameters.vectors, dtype=np.float32).reshape(-1) for cm in mats]
+    code_all = np.concatenate(codes) if codes else np.zeros((1, 5), np.uint32)
+    scal_all = np.concatenate(scal + [np.zeros(1, np.float32)])
+    vec_all = np.concatenate(vecs + [np.zeros(3, np.float32)])
+    c_counts = np.array([c.shape[0] for c in codes], np.uint64)
+    s_counts = np.array([s.size for s in scal], np.uint64)
+    v_counts = np.array([v.size for v in vecs], np.uint64)
+    start = lambda counts: np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.uint64) if len(counts) else counts
+    rec = np.zeros(n, dtype=_MATERIAL_DESC_DTYPE)
+    if mats:
+        rec["closures"] = np.uint64(code_all.ctypes.data) + start(c_counts) * np.uint64(20)
+        rec["closure_count"] = c_counts
+        rec["root"] = [cm.program.root for cm in mats]
+        rec["scalars"] = np.uint64(scal_all.ctypes.data) + start(s_counts) * np.uint64(4)
+        rec["scalar_count"] = s_counts
+        rec["vector_count"] = v_counts // np.uint64(3)
+        rec["vectors"] = np.uint64(vec_all.ctypes.data) + start(v_counts) * np.uint64(4)
+        rec["emission_sampling"] = [cm.emission_sampling for cm in mats]
+    descs = (_abi.MaterialDesc * n).from_buffer(rec)
+    return descs, [rec, code_all, scal_all, vec_all]
+
+
+# psy_material_desc of include/psycles_cuda.h on LP64 hosts (48 bytes)
+_MATERIAL_DESC_DTYPE = np.dtype({
+    "names": ["closures", "closure_count", "root", "scalars", "scalar_count", "vector_count", "vectors",
+              "emission_sampling", "reserved"],
+    "formats": [np.uint64, np.uint32, np.uint32, np.uint64, np.uint32, np.uint32, np.uint64, np.uint32, np.uint32],
+    "offsets": [0, 8, 12, 16, 24, 28, 32, 40, 44], "itemsize": 48})
+
+
 class SceneDescHandle:
     """A psy_scene_desc plus the arrays it points into (kept alive here)."""
 
@@ -147,20 +185,8 @@ class SceneDescHandle:
             instances[i].mesh = inst.mesh
             instances[i].material = inst.material
             instances[i].visibility = inst.visibility
-        materials = (_abi.MaterialDesc * max(len(scene.materials), 1))()
-        for i, cm in enumerate(scene.materials):
-            code = np.ascontiguousarray(cm.program.closures, dtype=np.uint32)
-            sc = np.ascontiguousarray(cm.parameters.scalars, dtype=np.float32)
-            vc = np.ascontiguousarray(cm.parameters.vectors, dtype=np.float32).reshape(-1)
-            keep += [code, sc, vc]
-            materials[i].closures = code.ctypes.data_as(ctypes.POINTER(_abi.ClosureInstruction))
-            materials[i].closure_count = code.shape[0]
-            materials[i].root = cm.program.root
-            materials[i].scalars = _abi.ptr(sc)
-            materials[i].scalar_count = sc.shape[0]
-            materials[i].vectors = _abi.ptr(vc)
-            materials[i].vector_count = vc.shape[0] // 3
-            materials[i].emission_sampling = cm.emission_sampling
+        materials, material_arrays = _material_descs(scene.materials)
+        keep += material_arrays
         lights = (_abi.LightDesc * max(len(scene.lights), 1))()
         for i, l in enumerate(scene.lights):
             d = lights[i]
