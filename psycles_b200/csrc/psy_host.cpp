@@ -990,6 +990,7 @@ psy_status psy_context_create(int device, psy_context **out) {
     c->sms = prop.multiProcessorCount;
     c->launch.sms = c->sms;
     PSY_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    PSY_CUDA_TRY(cudaStreamCreateWithFlags(&c->readback, cudaStreamNonBlocking));
     *out = c.release();
     return PSY_OK;
 }
@@ -1027,7 +1028,10 @@ psy_status psy_context_get_tuning(const psy_context *c, psy_tuning *t) {
 
 void psy_context_destroy(psy_context *c) {
     if (!c) return;
+    cudaSetDevice(c->device);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->readback) cudaStreamDestroy(c->readback);
+    if (c->readback_host) cudaFreeHost(c->readback_host);
     delete c;
 }
 
@@ -1258,9 +1262,11 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     // ---- emissive triangles + flat light distribution
     // (src/sampling/light_distribution.cpp:25-150; emitter geometry as in
     // src/luisa/path_kernel_emissive_triangle.cpp:80-150)
-    std::vector<psy::EmitterGpu> emitters;
-    std::vector<float> areas;
-    for (uint32_t i = 0; i < d->instance_count; ++i) {
+    // per instance in parallel, concatenated in instance order
+    std::vector<std::vector<psy::EmitterGpu>> instance_emitters(d->instance_count);
+    uint32_t emitter_threads = 0u;
+    const psy_status emit_status = parallel_for(d->instance_count, &emitter_threads, [&](uint32_t i) {
+        std::vector<psy::EmitterGpu> &out_e = instance_emitters[i];
         const psy_instance_desc &id = d->instances[i];
         const psy_mesh_desc &m = d->meshes[id.mesh];
         const psy::InstanceGpu &g = instances[i];
@@ -1300,10 +1306,17 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
             e.object = i;
             e.cycles_prim = meshes[id.mesh].prim_offset + k;
             e.emission_sampling = mat.emission_sampling;
+            out_e.push_back(e);
+        }
+    });
+    if (emit_status != PSY_OK) return emit_status;
+    std::vector<psy::EmitterGpu> emitters;
+    std::vector<float> areas;
+    for (const std::vector<psy::EmitterGpu> &v : instance_emitters)
+        for (const psy::EmitterGpu &e : v) {
             emitters.push_back(e);
             areas.push_back(e.area);
         }
-    }
     std::vector<psy::DistEntryGpu> dist;
     const uint32_t tri_n = uint32_t(areas.size()), light_n = d->light_count;
     auto valid_area = [](float a) { return std::isfinite(a) && a > 0.0f ? a : 0.0f; };
@@ -1920,35 +1933,37 @@ psy_status psy_session_read_pass(psy_session *s, uint32_t pass_kind, float *out,
         return fail(PSY_ERROR_UNSUPPORTED, "pass kind not produced by this backend");
     if (capacity < n * ch) return fail(PSY_ERROR_INVALID_ARGUMENT, "output buffer too small");
     if (channels) *channels = ch;
-    PSY_CUDA_TRY(cudaSetDevice(s->scene->context->device));
-    std::vector<uint32_t> counts(n);
-    PSY_CUDA_TRY(cudaMemcpy(counts.data(), s->sample_count.ptr, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
-    // write_passes fails when pixels disagree on the sample count
-    // (src/luisa/path_tracer_session.cpp:88-95)
-    for (uint64_t i = 0; i < n; ++i)
-        if (counts[i] != s->rendered) return fail(PSY_ERROR_STATE, "film sample counts disagree with the session");
-    if (pass_kind == PSY_PASS_SAMPLE_COUNT) {
-        for (uint64_t i = 0; i < n; ++i) out[i] = float(counts[i]);
-        return PSY_OK;
+    psy_context *ctx = s->scene->context;
+    PSY_CUDA_TRY(cudaSetDevice(ctx->device));
+    std::lock_guard<std::mutex> lock(ctx->readback_mutex);
+    cudaStream_t st = ctx->readback;
+    const size_t bytes = sizeof(float) * ch * n;
+    if (ctx->readback_pass.bytes < std::max<size_t>(bytes, 16)) PSY_CUDA_TRY(ctx->readback_pass.alloc(std::max<size_t>(bytes, 16)));
+    if (!ctx->readback_flag.ptr) PSY_CUDA_TRY(ctx->readback_flag.alloc(16));
+    if (ctx->readback_host_bytes < std::max<size_t>(bytes, 16)) {
+        if (ctx->readback_host) PSY_CUDA_TRY(cudaFreeHost(ctx->readback_host));
+        ctx->readback_host = nullptr;
+        ctx->readback_host_bytes = 0;
+        PSY_CUDA_TRY(cudaMallocHost(&ctx->readback_host, std::max<size_t>(bytes, 16)));
+        ctx->readback_host_bytes = std::max<size_t>(bytes, 16);
     }
+    // write_passes fails when pixels disagree on the sample count
+    // (src/luisa/path_tracer_session.cpp:88-95); checked on the device
+    psy::launch_check_counts(st, s->sample_count.as<uint32_t>(), uint32_t(n), s->rendered, ctx->readback_flag.as<uint32_t>());
+    uint32_t *flag = static_cast<uint32_t *>(ctx->readback_host);
+    PSY_CUDA_TRY(cudaMemcpyAsync(flag, ctx->readback_flag.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    if (*flag != 0u) return fail(PSY_ERROR_STATE, "film sample counts disagree with the session");
     const void *src = pass_kind == PSY_PASS_COMBINED ? s->combined.ptr
                       : (pass_kind == PSY_PASS_NORMAL || pass_kind == PSY_PASS_DENOISING_NORMAL) ? s->normal.ptr
                                                                                                   : s->albedo.ptr;
-    PSY_CUDA_TRY(cudaMemcpy(out, src, sizeof(float4) * n, cudaMemcpyDeviceToHost));
-    const float exposure = s->settings.film_exposure;
-    for (uint64_t i = 0; i < n; ++i) {
-        const float den = float(std::max(counts[i], 1u));
-        float *v = out + 4 * i;
-        if (pass_kind == PSY_PASS_COMBINED) {
-            const float k = exposure / den;
-            v[0] *= k;
-            v[1] *= k;
-            v[2] *= k;
-            v[3] = std::clamp(1.0f - v[3] / den, 0.0f, 1.0f);
-        } else {
-            for (int c = 0; c < 4; ++c) v[c] /= den;
-        }
-    }
+    const uint32_t kind = pass_kind == PSY_PASS_SAMPLE_COUNT ? 2u : (pass_kind == PSY_PASS_COMBINED ? 0u : 1u);
+    psy::launch_resolve_pass(st, static_cast<const float4 *>(src), s->sample_count.as<uint32_t>(), uint32_t(n), kind,
+                             s->settings.film_exposure, ctx->readback_pass.as<float>());
+    PSY_CUDA_TRY(cudaGetLastError());
+    PSY_CUDA_TRY(cudaMemcpyAsync(ctx->readback_host, ctx->readback_pass.ptr, bytes, cudaMemcpyDeviceToHost, st));
+    PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    std::memcpy(out, ctx->readback_host, bytes);
     return PSY_OK;
 }
 

@@ -133,6 +133,14 @@ struct psy_context {
     // they never overlap; the mutex orders renders from different threads.
     psy::host::PathArena arena;
     std::mutex render_mutex;
+    // pass readback: its own stream (films are complete when read, so it
+    // need not wait for renders queued on `stream`), a device buffer for the
+    // resolved pass and pinned host staging
+    cudaStream_t readback = nullptr;
+    psy::host::DeviceBuffer readback_pass, readback_flag;
+    void *readback_host = nullptr;
+    size_t readback_host_bytes = 0;
+    std::mutex readback_mutex;
 };
 
 struct psy_scene {

@@ -1247,6 +1247,43 @@ __global__ void k_count_rays(const uint32_t *counters, unsigned long long *stats
     stats[1] += counters[2];
 }
 
+__global__ void k_check_counts(const uint32_t *counts, uint32_t n, uint32_t expected, uint32_t *mismatch) {
+    bool bad = false;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        bad = bad || counts[i] != expected;
+    if (__any_sync(kFullMask, bad) && (threadIdx.x & 31u) == 0u) atomicOr(mismatch, 1u);
+}
+
+// write_passes (src/luisa/path_tracer_session.cpp:71-270): Combined = sum x
+// exposure / samples with alpha 1 - transparency / samples clamped to [0, 1];
+// Normal and Albedo = sum / samples; Sample Count as a float.
+__global__ void k_resolve_pass(const float4 *film, const uint32_t *counts, uint32_t n, uint32_t kind, float exposure,
+                               float *out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t c = counts[i];
+        if (kind == 2u) {
+            out[i] = float(c);
+            continue;
+        }
+        const float den = float(c > 1u ? c : 1u);
+        float4 v = film[i];
+        if (kind == 0u) {
+            const float k = exposure / den;
+            v.x *= k;
+            v.y *= k;
+            v.z *= k;
+            const float a = 1.0f - v.w / den;
+            v.w = a < 0.0f ? 0.0f : (1.0f < a ? 1.0f : a);
+        } else {
+            v.x /= den;
+            v.y /= den;
+            v.z /= den;
+            v.w /= den;
+        }
+        reinterpret_cast<float4 *>(out)[i] = v;
+    }
+}
+
 __global__ void k_debug_sobol(const float4 *table, uint32_t size, const uint32_t *queries, uint32_t count, float4 *out,
                               uint32_t *out_index) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1350,6 +1387,16 @@ void launch_begin_round(cudaStream_t st, uint32_t *counters, uint32_t *round, Ba
 void launch_swap(cudaStream_t st, uint32_t *counters) { k_swap_counters<<<1, 1, 0, st>>>(counters); }
 void launch_count_rays(cudaStream_t st, const uint32_t *counters, unsigned long long *stats) {
     k_count_rays<<<1, 1, 0, st>>>(counters, stats);
+}
+void launch_check_counts(cudaStream_t st, const uint32_t *counts, uint32_t n, uint32_t expected, uint32_t *mismatch) {
+    cudaMemsetAsync(mismatch, 0, sizeof(uint32_t), st);
+    const uint32_t blocks = n == 0u ? 1u : (n + 255u) / 256u;
+    k_check_counts<<<blocks < 1184u ? blocks : 1184u, 256, 0, st>>>(counts, n, expected, mismatch);
+}
+void launch_resolve_pass(cudaStream_t st, const float4 *film, const uint32_t *counts, uint32_t n, uint32_t kind,
+                         float exposure, float *out) {
+    const uint32_t blocks = n == 0u ? 1u : (n + 255u) / 256u;
+    k_resolve_pass<<<blocks < 2368u ? blocks : 2368u, 256, 0, st>>>(film, counts, n, kind, exposure, out);
 }
 void launch_film(cudaStream_t st, const LaunchConfig &lc, const PathBuffers &b, uint32_t pixels, uint32_t samples, float4 *combined,
                  float4 *normal, float4 *albedo, uint32_t *sample_count, uint32_t trace_path, psy_path_trace *trace) {

@@ -32,6 +32,13 @@ void launch_swap(cudaStream_t st, uint32_t *counters);
 void launch_begin_round(cudaStream_t st, uint32_t *counters, uint32_t *round, BatchItem *items,
                         const uint32_t *plan_rounds, const BatchItem *plan_items, uint32_t *cursor, uint32_t max_items);
 void launch_count_rays(cudaStream_t st, const uint32_t *counters, unsigned long long *stats);
+// Pass readback: `mismatch` (one word, cleared first) is set when a pixel's
+// sample count differs from `expected`; the resolve writes a pass as the
+// film's consumer sees it (kind: 0 Combined, 1 Normal / Albedo, 2 Sample
+// Count), float4 per pixel (one float for the sample count).
+void launch_check_counts(cudaStream_t st, const uint32_t *counts, uint32_t n, uint32_t expected, uint32_t *mismatch);
+void launch_resolve_pass(cudaStream_t st, const float4 *film, const uint32_t *counts, uint32_t n, uint32_t kind,
+                         float exposure, float *out);
 void launch_film(cudaStream_t st, const LaunchConfig &lc, const PathBuffers &b, uint32_t pixels, uint32_t samples, float4 *combined,
                  float4 *normal, float4 *albedo, uint32_t *sample_count, uint32_t trace_path, psy_path_trace *trace);
 // Batched wavefront.  round (device memory): paths, film pixels, items.
