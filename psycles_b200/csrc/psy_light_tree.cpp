@@ -12,6 +12,8 @@
 #include <cmath>
 #include <limits>
 #include <stdexcept>
+#include <thread>
+#include <vector>
 
 #include "../../include/psycles_cuda.h"
 
@@ -111,24 +113,35 @@ struct Bucket {
     uint32_t count = 0u;
 };
 
+// Subtrees of large nodes near the root are built on their own threads,
+// each into a node list of its own that is spliced in after the left
+// subtree: the node order (pre-order) and every field equal the sequential
+// build's.  Emitter ranges of sibling subtrees are disjoint, so they share
+// the emitter array and the identity maps.
+constexpr uint32_t kParallelDepth = 3u;      // up to 8 subtrees in flight
+constexpr uint32_t kParallelMinCount = 4096u;
+
 class Builder {
   public:
-    LightTree tree;
+    LightTree &tree;                 // emitters and identity maps (shared)
+    std::vector<LtNode> &nodes;      // this builder's node list
     uint32_t max_leaf;
 
+    Builder(LightTree &t, std::vector<LtNode> &n, uint32_t leaf) : tree(t), nodes(n), max_leaf(leaf) {}
+
     uint32_t append(uint32_t parent) {
-        const uint32_t index = uint32_t(tree.nodes.size());
+        const uint32_t index = uint32_t(nodes.size());
         LtNode n;
         n.parent = parent;
-        tree.nodes.push_back(n);
+        nodes.push_back(n);
         return index;
     }
 
-    uint32_t build_local(uint32_t begin, uint32_t end, uint32_t parent) {
+    uint32_t build_local(uint32_t begin, uint32_t end, uint32_t parent, uint32_t depth = 0u) {
         const uint32_t node_index = append(parent);
         const uint32_t count = end - begin;
         if (count == 0u) {
-            tree.nodes[node_index].kind = kLtLeaf;
+            nodes[node_index].kind = kLtLeaf;
             return node_index;
         }
         LtMeasure node_measure;
@@ -141,7 +154,7 @@ class Builder {
             for (int k = 0; k < 3; ++k) point.lo[k] = point.hi[k] = e.centroid[k];
             cb = merge_bounds(cb, point);
         }
-        tree.nodes[node_index].measure = node_measure;
+        nodes[node_index].measure = node_measure;
         size_t split_axis = std::numeric_limits<size_t>::max();
         uint32_t split_middle = begin + count / 2u;
         float best_cost = std::numeric_limits<float>::infinity();
@@ -185,7 +198,7 @@ class Builder {
         }
         const bool should_split = count > max_leaf || split_axis != std::numeric_limits<size_t>::max();
         if (!should_split) {
-            LtNode &n = tree.nodes[node_index];
+            LtNode &n = nodes[node_index];
             n.kind = kLtLeaf;
             n.first = begin;
             n.count = count;
@@ -203,11 +216,32 @@ class Builder {
                                  return av < bv || (av == bv && a.emitter_id < b.emitter_id);
                              });
         }
-        tree.nodes[node_index].kind = kLtInner;
-        const uint32_t l = build_local(begin, split_middle, node_index);
-        const uint32_t r = build_local(split_middle, end, node_index);
-        tree.nodes[node_index].left = l;
-        tree.nodes[node_index].right = r;
+        nodes[node_index].kind = kLtInner;
+        uint32_t l = kLtInvalid, r = kLtInvalid;
+        if (depth < kParallelDepth && end - begin >= kParallelMinCount) {
+            std::vector<LtNode> right_nodes;
+            Builder right(tree, right_nodes, max_leaf);
+            std::thread worker([&]() { right.build_local(split_middle, end, kLtInvalid, depth + 1u); });
+            l = build_local(begin, split_middle, node_index, depth + 1u);
+            worker.join();
+            // splice: the right subtree's nodes follow the left subtree's
+            const uint32_t offset = uint32_t(nodes.size());
+            auto shift = [offset](uint32_t v) { return v == kLtInvalid ? v : v + offset; };
+            for (LtNode &n : right_nodes) {
+                n.parent = shift(n.parent);
+                n.left = shift(n.left);
+                n.right = shift(n.right);
+            }
+            right_nodes.front().parent = node_index;
+            nodes.insert(nodes.end(), right_nodes.begin(), right_nodes.end());
+            for (uint32_t i = split_middle; i < end; ++i) tree.emitter_to_leaf[tree.emitters[i].emitter_id] += offset;
+            r = offset;
+        } else {
+            l = build_local(begin, split_middle, node_index, depth + 1u);
+            r = build_local(split_middle, end, node_index, depth + 1u);
+        }
+        nodes[node_index].left = l;
+        nodes[node_index].right = r;
         return node_index;
     }
 };
@@ -244,8 +278,8 @@ float lt_cost(const LtMeasure &m) {
 }
 
 LightTree lt_build(const std::vector<LtEmitter> &source, uint32_t max_leaf) {
-    Builder b;
-    b.max_leaf = std::max(max_leaf, 1u);
+    LightTree result;
+    Builder b(result, result.nodes, std::max(max_leaf, 1u));
     b.tree.emitters.reserve(source.size());
     for (const LtEmitter &s : source) {
         LtEmitter e = s;
@@ -253,7 +287,7 @@ LightTree lt_build(const std::vector<LtEmitter> &source, uint32_t max_leaf) {
         if (!finite3(e.centroid)) e.centroid[0] = e.centroid[1] = e.centroid[2] = 0.0f;
         b.tree.emitters.push_back(e);
     }
-    if (b.tree.emitters.empty()) return std::move(b.tree);
+    if (b.tree.emitters.empty()) return result;
     std::vector<bool> seen(b.tree.emitters.size(), false);
     for (const LtEmitter &e : b.tree.emitters) {
         if (e.emitter_id >= seen.size() || seen[e.emitter_id])
@@ -285,7 +319,7 @@ LightTree lt_build(const std::vector<LtEmitter> &source, uint32_t max_leaf) {
     root.left = local;
     root.right = distant;
     root.measure = lt_merge(b.tree.nodes[local].measure, b.tree.nodes[distant].measure);
-    return std::move(b.tree);
+    return result;
 }
 
 LtEmitter lt_triangle_emitter(uint32_t id, const float *p0, const float *p1, const float *p2, const float *emission,
