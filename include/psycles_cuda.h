@@ -163,8 +163,15 @@ typedef struct psy_light_desc {
     float spread;                /* area light spread; pi = full */
 } psy_light_desc;
 
-/* contract::CameraDesc (include/psycles/contract/scene.h:347),
- * perspective projection. */
+/* contract::CameraProjection (include/psycles/contract/scene.h:335). */
+#define PSY_CAMERA_PERSPECTIVE 0u
+#define PSY_CAMERA_ORTHOGRAPHIC 1u
+#define PSY_CAMERA_PANORAMA 2u   /* equirectangular: 360 x 180 degrees */
+
+/* contract::CameraDesc (include/psycles/contract/scene.h:347).  Depth of
+ * field applies to perspective cameras with aperture_radius > 0 and
+ * focal_distance > 0 (src/luisa/path_tracer_kernel.cpp:275-278); a zero
+ * aperture_ratio is taken as 1e-5, as the reference clamps it. */
 typedef struct psy_camera_desc {
     float camera_to_world[16];   /* column-major */
     float field_of_view;         /* vertical angle, radians */
@@ -174,6 +181,13 @@ typedef struct psy_camera_desc {
     float lens_shift_y;
     float near_clip;
     float far_clip;
+    uint32_t projection;         /* PSY_CAMERA_* */
+    float orthographic_scale;    /* along the fitted sensor dimension */
+    float aperture_radius;
+    float focal_distance;
+    uint32_t aperture_blades;    /* 0: round aperture, else a regular polygon */
+    float aperture_rotation;
+    float aperture_ratio;        /* anamorphic ratio, 1 = round */
     uint32_t reserved;
 } psy_camera_desc;
 

@@ -1287,6 +1287,8 @@ struct Settings {
     float inv_rr_threshold;
     bool use_light_tree;
     float htan, vtan, shift_x, shift_y;
+    float ortho_span;     // orthographic_viewplane_span().vertical
+    bool depth_of_field;  // perspective with aperture and focal distance
     std::array<float, 1024> filter;
     SobolTable sobol;
 };
@@ -1316,6 +1318,10 @@ static void derive_settings(Settings &st, const Scene &s, const psy_render_setti
     st.htan = st.vtan * aspect;
     st.shift_x = s.camera.lens_shift_x * (hfit ? 1.0f : 1.0f / aspect);
     st.shift_y = s.camera.lens_shift_y * (hfit ? aspect : 1.0f);
+    // camera_sampling.h:47-53 and path_tracer_kernel.cpp:275-278
+    st.ortho_span = hfit ? s.camera.orthographic_scale / aspect : s.camera.orthographic_scale;
+    st.depth_of_field = s.camera.projection == PSY_CAMERA_PERSPECTIVE && s.camera.aperture_radius > 0.0f &&
+                        s.camera.focal_distance > 0.0f;
     st.filter = pixel_filter_table(r.pixel_filter, r.filter_width);
     st.sobol.sequence_size = sobol_sequence_size_for_samples(total);
     st.sobol.rows = sobol_generate_table(st.sobol.sequence_size);
@@ -1466,6 +1472,23 @@ static uint32_t tree_emitter(const Scene &s, uint32_t object, uint32_t primitive
     return lt::kLtInvalid;
 }
 
+// sample_regular_polygon / sample_aperture (include/psycles/luisa/camera_sampling.h:118-152).
+static float2 sample_aperture(float2 r, uint32_t blades, float rotation) {
+    if (blades == 0u) return sample_uniform_disk(r);
+    const float corners = static_cast<float>(blades);
+    float u = r.x, v = r.y;
+    const float corner = std::floor(u * corners);
+    u = u * corners - corner;
+    u = std::sqrt(u);
+    v *= u;
+    u = 1.0f - u;
+    const float half_corner = kPi / corners;
+    const float2 point = f2((u + v) * cos_(half_corner), (u - v) * sin_(half_corner));
+    const float angle = rotation + corner * (2.0f * half_corner);
+    const float c = cos_(angle), sn = sin_(angle);
+    return f2(c * point.x - sn * point.y, sn * point.x + c * point.y);
+}
+
 static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, uint32_t y, uint32_t sample,
                               psy_path_trace *trace) {
     const psy_render_settings &r = st.raw;
@@ -1474,16 +1497,41 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
     const uint32_t rng_hash = pixel_hash(x, cycles_y, r.seed);
     const float4 fs = st.sobol.sample_4d(sample, rng_hash, kDimFilter);
     float2 filter = sample == 0u ? f2(0.5f, 0.5f) : f2(fs.x, fs.y);
-    // construct_camera_ray (path_tracer_camera.cpp:47-246), perspective, no DOF
+    // construct_camera_ray (path_tracer_camera.cpp:47-246): perspective,
+    // orthographic or equirectangular panorama, thin-lens depth of field
     const float jx = pixel_filter_sample(st.filter, filter.x);
     const float jy = 1.0f - pixel_filter_sample(st.filter, filter.y);
     const float W = static_cast<float>(r.full_width), H = static_cast<float>(r.full_height);
     const float sx = 2.0f * (static_cast<float>(x) + jx) / W - 1.0f + 2.0f * st.shift_x;
     const float sy = 1.0f - 2.0f * (static_cast<float>(y) + jy) / H + 2.0f * st.shift_y;
-    const float3 local_dir = normalize(f3(sx * st.htan, sy * st.vtan, -1.0f));
-    const float clip_cos = -local_dir.z;
+    float3 local_origin = f3(0.0f);
+    float3 local_dir = f3(0.0f, 0.0f, -1.0f);
+    float clip_cos = 1.0f;
+    if (s.camera.projection == PSY_CAMERA_PERSPECTIVE) {
+        local_dir = normalize(f3(sx * st.htan, sy * st.vtan, -1.0f));
+        clip_cos = -local_dir.z;
+    } else if (s.camera.projection == PSY_CAMERA_ORTHOGRAPHIC) {
+        const float aspect = W / H;
+        local_origin = f3(sx * st.ortho_span * aspect * 0.5f, sy * st.ortho_span * 0.5f, 0.0f);
+    } else {
+        const float longitude = sx * kPi;
+        const float latitude = sy * kPi * 0.5f;
+        const float cos_lat = cos_(latitude);
+        local_dir = f3(cos_lat * sin_(longitude), sin_(latitude), -cos_lat * cos_(longitude));
+    }
+    if (st.depth_of_field) {
+        // sample_3d at camera_lens_time_dimension (path_tracer_camera.cpp:35-45): lens = .yz
+        const float4 lt = st.sobol.sample_4d(sample, rng_hash, 1u);
+        float2 lens = sample_aperture(f2(lt.y, lt.z), s.camera.aperture_blades, s.camera.aperture_rotation) *
+                      s.camera.aperture_radius;
+        lens.x /= maxf(s.camera.aperture_ratio, 1.0e-5f);
+        const float focus_scale = s.camera.focal_distance / maxf(-local_dir.z, 1.0e-6f);
+        const float3 focus = local_dir * focus_scale;
+        local_origin = f3(lens.x, lens.y, 0.0f);
+        local_dir = normalize(focus - local_origin);
+    }
     const mat4 cam = mat4_from_column_major(s.camera.camera_to_world);
-    float3 origin = transform_point(cam, f3(0.0f));
+    float3 origin = transform_point(cam, local_origin);
     const float3 dir = safe_normalize(transform_direction(cam, local_dir), f3(0.0f, 0.0f, -1.0f));
     const float safe_cos = maxf(std::fabs(clip_cos), 1.0e-20f);
     const float near_t = s.camera.near_clip / safe_cos;

@@ -70,7 +70,14 @@ class CameraDesc(ctypes.Structure):
     _fields_ = [("camera_to_world", ctypes.c_float * 16), ("field_of_view", ctypes.c_float),
                 ("horizontal_field_of_view", ctypes.c_float), ("sensor_fit", ctypes.c_uint32),
                 ("lens_shift_x", ctypes.c_float), ("lens_shift_y", ctypes.c_float),
-                ("near_clip", ctypes.c_float), ("far_clip", ctypes.c_float), ("reserved", ctypes.c_uint32)]
+                ("near_clip", ctypes.c_float), ("far_clip", ctypes.c_float), ("projection", ctypes.c_uint32),
+                ("orthographic_scale", ctypes.c_float), ("aperture_radius", ctypes.c_float),
+                ("focal_distance", ctypes.c_float), ("aperture_blades", ctypes.c_uint32),
+                ("aperture_rotation", ctypes.c_float), ("aperture_ratio", ctypes.c_float),
+                ("reserved", ctypes.c_uint32)]
+
+
+CAMERA_PERSPECTIVE, CAMERA_ORTHOGRAPHIC, CAMERA_PANORAMA = 0, 1, 2
 
 
 class SceneDesc(ctypes.Structure):

@@ -620,6 +620,18 @@ psy_status derive_params(psy_session *s, const psy_render_settings &r) {
     p.shift_y = c.lens_shift_y * (hfit ? aspect : 1.0f);
     p.near_clip = c.near_clip;
     p.far_clip = c.far_clip;
+    // orthographic_viewplane_span (include/psycles/luisa/camera_sampling.h:47-53)
+    // and the depth-of-field switch (src/luisa/path_tracer_kernel.cpp:246-278)
+    if (c.projection > PSY_CAMERA_PANORAMA) return fail(PSY_ERROR_INVALID_ARGUMENT, "unknown camera projection");
+    p.projection = c.projection;
+    p.ortho_span = hfit ? c.orthographic_scale / aspect : c.orthographic_scale;
+    p.aperture_radius = c.aperture_radius;
+    p.focal_distance = c.focal_distance;
+    p.aperture_ratio = c.aperture_ratio;
+    p.aperture_blades = c.aperture_blades;
+    p.aperture_rotation = c.aperture_rotation;
+    p.depth_of_field =
+        (c.projection == PSY_CAMERA_PERSPECTIVE && c.aperture_radius > 0.0f && c.focal_distance > 0.0f) ? 1u : 0u;
     store34(p.cam, m34(c.camera_to_world));
     s->pixels = ww * wh;
     return PSY_OK;

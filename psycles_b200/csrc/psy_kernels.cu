@@ -47,6 +47,55 @@ __device__ __forceinline__ void set3(float *d, f3 v) {
 // ------------------------------------------------------------------ raygen
 // begin_path_sample / construct_camera_ray (src/luisa/path_kernel_setup.cpp:485-700,
 // src/luisa/path_tracer_camera.cpp:10-246).
+// sample_regular_polygon / sample_aperture (include/psycles/luisa/camera_sampling.h:
+// 118-152): a corner triangle of the blade polygon, sampled by area.
+__device__ __forceinline__ f2 sample_aperture(f2 r, uint32_t blades, float rotation) {
+    if (blades == 0u) return sample_uniform_disk(r);
+    const float corners = static_cast<float>(blades);
+    float u = r.x, v = r.y;
+    const float corner = floorf(u * corners);
+    u = u * corners - corner;
+    u = sqrtf(u);
+    v *= u;
+    u = 1.0f - u;
+    const float half_corner = kPi / corners;
+    const f2 point = mk2((u + v) * cos_(half_corner), (u - v) * sin_(half_corner));
+    const float angle = rotation + corner * (2.0f * half_corner);
+    const float c = cos_(angle), s = sin_(angle);
+    return mk2(c * point.x - s * point.y, s * point.x + c * point.y);
+}
+
+// construct_camera_ray (src/luisa/path_tracer_camera.cpp:51-246): the camera-space
+// ray of the projection (screen coordinates sx, sy in [-1, 1] plus lens
+// shift), then the thin-lens update for depth of field.  `clip_cos` is the
+// pinhole direction's cosine that scales the clipping range.
+__device__ __forceinline__ void camera_local_ray(const RenderParams &p, float sx, float sy, f2 lens_sample, f3 &origin,
+                                                 f3 &direction, float &clip_cos) {
+    origin = mk3(0.0f);
+    direction = mk3(0.0f, 0.0f, -1.0f);
+    clip_cos = 1.0f;
+    if (p.projection == PSY_CAMERA_PERSPECTIVE) {
+        direction = normalize(mk3(sx * p.htan, sy * p.vtan, -1.0f));
+        clip_cos = -direction.z;
+    } else if (p.projection == PSY_CAMERA_ORTHOGRAPHIC) {
+        const float aspect = static_cast<float>(p.full_w) / static_cast<float>(p.full_h);
+        origin = mk3(sx * p.ortho_span * aspect * 0.5f, sy * p.ortho_span * 0.5f, 0.0f);
+    } else {
+        const float longitude = sx * kPi;
+        const float latitude = sy * kPi * 0.5f;
+        const float cos_lat = cos_(latitude);
+        direction = mk3(cos_lat * sin_(longitude), sin_(latitude), -cos_lat * cos_(longitude));
+    }
+    if (p.depth_of_field) {
+        f2 lens = sample_aperture(lens_sample, p.aperture_blades, p.aperture_rotation) * p.aperture_radius;
+        lens.x /= maxf_(p.aperture_ratio, 1.0e-5f);
+        const float focus_scale = p.focal_distance / maxf_(-direction.z, 1.0e-6f);
+        const f3 focus = direction * focus_scale;
+        origin = mk3(lens.x, lens.y, 0.0f);
+        direction = normalize(focus - origin);
+    }
+}
+
 __device__ __forceinline__ void raygen_path(const RenderParams &p, const PathBuffers &b, uint32_t i, uint32_t local,
                                             uint32_t sample, uint32_t trace_path, psy_path_trace *trace) {
     const uint32_t x = p.win_x + local % p.win_w;
@@ -60,10 +109,17 @@ __device__ __forceinline__ void raygen_path(const RenderParams &p, const PathBuf
     const float W = static_cast<float>(p.full_w), H = static_cast<float>(p.full_h);
     const float sx = 2.0f * (static_cast<float>(x) + jx) / W - 1.0f + 2.0f * p.shift_x;
     const float sy = 1.0f - 2.0f * (static_cast<float>(y) + jy) / H + 2.0f * p.shift_y;
-    const f3 local_dir = normalize(mk3(sx * p.htan, sy * p.vtan, -1.0f));
-    const float clip_cos = -local_dir.z;
+    f3 local_origin, local_dir;
+    float clip_cos;
+    f2 lens_sample = mk2(0.0f, 0.0f);
+    if (p.depth_of_field) {
+        // sample_3d at camera_lens_time_dimension, lens = .yz (path_tracer_camera.cpp:35-45)
+        const float4 lt = sample_4d(p, sample, rng_hash, 1u);
+        lens_sample = mk2(lt.y, lt.z);
+    }
+    camera_local_ray(p, sx, sy, lens_sample, local_origin, local_dir, clip_cos);
     const Xform cam = xform12(p.cam);
-    f3 origin = xform_point(cam, mk3(0.0f));
+    f3 origin = xform_point(cam, local_origin);
     const f3 dir = safe_normalize(xform_direction(cam, local_dir), mk3(0.0f, 0.0f, -1.0f));
     const float safe_cos = maxf_(fabsf(clip_cos), 1.0e-20f);
     const float near_t = p.near_clip / safe_cos;

@@ -158,6 +158,8 @@ struct RenderParams {
     uint32_t direct_mode, nee, use_light_tree;
     float cam[12];  // camera_to_world columns c0..c3
     float htan, vtan, shift_x, shift_y, near_clip, far_clip;
+    uint32_t projection, aperture_blades, depth_of_field, pad_camera;  // PSY_CAMERA_*; DOF on / off
+    float ortho_span, aperture_radius, focal_distance, aperture_ratio, aperture_rotation;
     const float4 *sobol;
     uint32_t sobol_size;
     const float *filter;  // 1024 entries

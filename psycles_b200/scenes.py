@@ -84,6 +84,13 @@ class Camera:
     lens_shift_y: float = 0.0
     near_clip: float = 1.0e-4
     far_clip: float = 1.0e5
+    projection: int = 0  # _abi.CAMERA_*
+    orthographic_scale: float = 1.0
+    aperture_radius: float = 0.0
+    focal_distance: float = 0.0
+    aperture_blades: int = 0
+    aperture_rotation: float = 0.0
+    aperture_ratio: float = 1.0
 
 
 @dataclasses.dataclass
@@ -119,6 +126,9 @@ def camera_desc(cam: "Camera") -> _abi.CameraDesc:
     c.sensor_fit = cam.sensor_fit
     c.lens_shift_x, c.lens_shift_y = cam.lens_shift_x, cam.lens_shift_y
     c.near_clip, c.far_clip = cam.near_clip, cam.far_clip
+    c.projection, c.orthographic_scale = cam.projection, cam.orthographic_scale
+    c.aperture_radius, c.focal_distance = cam.aperture_radius, cam.focal_distance
+    c.aperture_blades, c.aperture_rotation, c.aperture_ratio = cam.aperture_blades, cam.aperture_rotation, cam.aperture_ratio
     return c
 
 
