@@ -520,7 +520,7 @@ def run_viewports(backend, compiled, count: int = 64, capacity: int = 0) -> dict
 # procedural render: DRAM read + write of the launch over its duration).
 # The traffic of a bench launch is this rate times the launch's mean
 # event-timed duration (the procedural workload only).
-NCU_DRAM_GBS = {"intersect": (959.2 + 121.9) / 2.741, "shadow": (102.6 + 20.5) / 2.762,
+NCU_DRAM_GBS = {"intersect": (959.2 + 121.9) / 2.741, "shadow": (100.2 + 13.0) / 2.353,
                 "shade": (2522.6 + 681.5) / 1.276}
 
 
