@@ -846,10 +846,18 @@ psy_status build_light_tree(psy_scene *sc, bool sync = true) {
                 b = make_float4(m.bounds.hi[0], m.bounds.hi[1], m.bounds.hi[2], m.orientation.theta_o);
                 c = make_float4(m.orientation.axis[0], m.orientation.axis[1], m.orientation.axis[2], m.orientation.theta_e);
             };
+            // the cone's trigonometry, double-rounded as the kernels' own
+            auto cone = [](const psy::LtMeasure &m) {
+                const float to = m.orientation.theta_o, te = m.orientation.theta_e;
+                auto rc = [](float v) { return static_cast<float>(std::cos(static_cast<double>(v))); };
+                return make_float4(rc(to), static_cast<float>(std::sin(static_cast<double>(to))), rc(to + te),
+                                   rc(te - to));
+            };
             lt_nodes.reserve(tree.nodes.size());
             for (const psy::LtNode &n : tree.nodes) {
                 psy::LtNodeGpu g{};
                 pack(n.measure, g.min_energy, g.max_theta_o, g.axis_theta_e);
+                g.cone = cone(n.measure);
                 g.topology = make_uint4(n.parent, n.left, n.right, n.kind);
                 g.emitters = make_uint4(n.first, n.count, flags(n.measure, n.kind == psy::kLtDistant), 0u);
                 lt_nodes.push_back(g);
@@ -858,6 +866,7 @@ psy_status build_light_tree(psy_scene *sc, bool sync = true) {
             for (const psy::LtEmitter &e : tree.emitters) {
                 psy::LtEmitterGpu g{};
                 pack(e.measure, g.min_energy, g.max_theta_o, g.axis_theta_e);
+                g.cone = cone(e.measure);
                 g.identity = make_uint4(e.emitter_id, flags(e.measure, e.distant), 0u, 0u);
                 lt_emitters.push_back(g);
             }

@@ -29,8 +29,8 @@ __device__ __forceinline__ float lt_cos_subtended(f3 bmax, f3 centroid, f3 point
 
 // bounded_importance, surface case (path_tracer_light_tree.cpp:86-193).
 __device__ __forceinline__ f2 lt_bounded_importance(f3 n, bool has_transmission, f3 p2c, float cos_u, f3 axis,
-                                                    float theta_o, float theta_e, float max_d, float min_d,
-                                                    float energy) {
+                                                    float theta_o, float theta_e, float4 cone, float max_d,
+                                                    float min_d, float energy) {
     cos_u = clampf_(cos_u, -1.0f, 1.0f);
     const float sin_u = lt_sin_from_cos(cos_u);
     bool visible = energy > 0.0f;
@@ -42,10 +42,10 @@ __device__ __forceinline__ f2 lt_bounded_importance(f3 n, bool has_transmission,
     const float th_cos = clampf_(dot(axis, -p2c), -1.0f, 1.0f);
     const float th_sin = lt_sin_from_cos(th_cos);
     const float tmu_cos = th_cos * cos_u + th_sin * sin_u;
-    const float to_cos = cos_(theta_o);
-    const float to_sin = sin_(theta_o);
+    const float to_cos = cone.x;
+    const float to_sin = cone.y;
     const bool fully = th_cos >= cos_u || tmu_cos >= to_cos;
-    const bool partially = !fully && (theta_o + theta_e > kLtPi || tmu_cos > cos_(theta_o + theta_e));
+    const bool partially = !fully && (theta_o + theta_e > kLtPi || tmu_cos > cone.z);
     const float tmu_sin = lt_sin_from_cos(clampf_(tmu_cos, -1.0f, 1.0f));
     const float min_out = fully ? 1.0f : (partially ? tmu_cos * to_cos + tmu_sin * to_sin : 0.0f);
     visible = visible && (fully || partially);
@@ -55,7 +55,7 @@ __device__ __forceinline__ f2 lt_bounded_importance(f3 n, bool has_transmission,
     const float maximum = visible ? fabsf(min_inc * energy * min_out * geometric) : 0.0f;
     const float tpu_cos = th_cos * cos_u - th_sin * sin_u;
     const bool min_zero = (theta_e - theta_o < 0.0f) || (th_cos < 0.0f) || (cos_u < 0.0f) ||
-                          (tpu_cos < cos_(theta_e - theta_o));
+                          (tpu_cos < cone.w);
     const float tpu_sin = lt_sin_from_cos(clampf_(tpu_cos, -1.0f, 1.0f));
     const float max_out = tpu_cos * to_cos - tpu_sin * to_sin;
     const float minimum = (min_zero || !visible) ? 0.0f : fabsf(max_inc * energy * max_out / (max_d * max_d));
@@ -64,7 +64,8 @@ __device__ __forceinline__ f2 lt_bounded_importance(f3 n, bool has_transmission,
 
 // measure_importance (path_tracer_light_tree.cpp:195-277).
 __device__ __noinline__ f2 lt_measure_importance(float4 min_energy, float4 max_theta_o, float4 axis_theta_e,
-                                                    uint32_t flags, f3 point, f3 n, bool has_transmission) {
+                                                    float4 cone, uint32_t flags, f3 point, f3 n,
+                                                    bool has_transmission) {
     f2 result = {0.0f, 0.0f};
     const bool has_orientation = (flags & kLtFlagOrientation) != 0u;
     const bool has_bounds = (flags & kLtFlagBounds) != 0u;
@@ -72,7 +73,7 @@ __device__ __noinline__ f2 lt_measure_importance(float4 min_energy, float4 max_t
     if (!(has_orientation && min_energy.w > 0.0f)) return result;
     const f3 axis = lt_safe_normalize(ld3(axis_theta_e), mk3(0.0f, 0.0f, 1.0f));
     f3 p2c = -axis;
-    float cos_u = cos_(max_theta_o.w + axis_theta_e.w);
+    float cos_u = cone.z;
     float emitter_distance = 1.0f;
     bool visible = true;
     if (!distant) {
@@ -90,14 +91,14 @@ __device__ __noinline__ f2 lt_measure_importance(float4 min_energy, float4 max_t
         emitter_distance = maxf_(0.5f * length(centroid - bmax), emitter_distance);
     }
     if (visible)
-        result = lt_bounded_importance(n, has_transmission, p2c, cos_u, axis, max_theta_o.w, axis_theta_e.w,
+        result = lt_bounded_importance(n, has_transmission, p2c, cos_u, axis, max_theta_o.w, axis_theta_e.w, cone,
                                        emitter_distance, emitter_distance, min_energy.w);
     return result;
 }
 
 __device__ __forceinline__ f2 lt_emitter_importance(const SceneView &s, uint32_t e, f3 point, f3 n, bool tr) {
     const LtEmitterGpu em = s.lt_emitters[e];
-    return lt_measure_importance(em.min_energy, em.max_theta_o, em.axis_theta_e, em.identity.y, point, n, tr);
+    return lt_measure_importance(em.min_energy, em.max_theta_o, em.axis_theta_e, em.cone, em.identity.y, point, n, tr);
 }
 
 // child_importance (path_tracer_light_tree.cpp:321-356).
@@ -105,7 +106,8 @@ __device__ __forceinline__ f2 lt_child_importance(const SceneView &s, uint32_t n
     const LtNodeGpu node = s.lt_nodes[node_index];
     const bool inner = node.topology.w == kLtInner;
     if (inner || node.emitters.y > 1u)
-        return lt_measure_importance(node.min_energy, node.max_theta_o, node.axis_theta_e, node.emitters.z, point, n, tr);
+        return lt_measure_importance(node.min_energy, node.max_theta_o, node.axis_theta_e, node.cone, node.emitters.z,
+                                     point, n, tr);
     if (node.emitters.y == 1u) return lt_emitter_importance(s, node.emitters.x, point, n, tr);
     return {0.0f, 0.0f};
 }

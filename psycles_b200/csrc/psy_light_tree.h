@@ -73,10 +73,14 @@ LtEmitter lt_analytic_emitter(uint32_t id, const void *light_desc);
 // (src/luisa/path_tracer_light_tree_scene.cpp:102-128).
 constexpr uint32_t kLtFlagOrientation = 1u, kLtFlagBounds = 2u, kLtFlagDistant = 4u;
 
+// `cone` holds the orientation cone's cosines and sine the importance
+// bounds use, computed on the host in double and rounded once:
+// cos(theta_o), sin(theta_o), cos(theta_o + theta_e), cos(theta_e - theta_o).
 struct alignas(16) LtNodeGpu {
     float4 min_energy;      // bounds min, energy
     float4 max_theta_o;     // bounds max, theta_o
     float4 axis_theta_e;    // cone axis, theta_e
+    float4 cone;
     uint4 topology;         // parent, left, right, kind
     uint4 emitters;         // first, count, flags, pad
 };
@@ -85,6 +89,7 @@ struct alignas(16) LtEmitterGpu {
     float4 min_energy;
     float4 max_theta_o;
     float4 axis_theta_e;
+    float4 cone;
     uint4 identity;         // distribution index, flags, emitter id, pad
 };
 
