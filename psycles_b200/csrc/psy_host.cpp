@@ -323,6 +323,7 @@ struct Builder {
     std::vector<Prim> prims;
     uint32_t leaf_size = PSY_LEAF_SIZE;
     bool leaf_is_id = false;  // TLAS: leaf link = ~prim id, count 1
+    bool parallel = true;     // large subtrees on threads of their own
 
     struct Child {
         Box box;
@@ -335,7 +336,14 @@ struct Builder {
         return {box, ~int(begin), int(end - begin)};
     }
 
-    Child build(uint32_t begin, uint32_t end, int depth) {
+    // Binary SAH build of prims [begin, end) into `out` (pre-order node
+    // list).  Large ranges near the root build their right half on a thread
+    // of its own into a separate list that is spliced in after the left
+    // half, so the tree and its node order equal the sequential build's
+    // (the two halves touch disjoint prim ranges).
+    Child build(uint32_t begin, uint32_t end, int depth) { return build_into(nodes, begin, end, depth); }
+
+    Child build_into(std::vector<psy::BvhNodeGpu> &out, uint32_t begin, uint32_t end, int depth) {
         Box box, cbox;
         for (uint32_t i = begin; i < end; ++i) {
             box.grow(prims[i].box);
@@ -407,19 +415,36 @@ struct Builder {
                                  return a.c[axis] < b.c[axis] || (a.c[axis] == b.c[axis] && a.id < b.id);
                              });
         }
-        const int index = int(nodes.size());
-        nodes.push_back({});
-        const Child l = build(begin, mid, depth + 1);
-        const Child r = build(mid, end, depth + 1);
-        write(index, l, r);
+        const int index = int(out.size());
+        out.push_back({});
+        Child l, r;
+        if (parallel && depth < 3 && count >= 16384u) {
+            std::vector<psy::BvhNodeGpu> right_nodes;
+            std::thread worker([&]() { r = build_into(right_nodes, mid, end, depth + 1); });
+            l = build_into(out, begin, mid, depth + 1);
+            worker.join();
+            const int offset = int(out.size());
+            for (psy::BvhNodeGpu &n : right_nodes) {
+                if (n.child.x >= 0) n.child.x += offset;
+                if (n.child.y >= 0) n.child.y += offset;
+            }
+            out.insert(out.end(), right_nodes.begin(), right_nodes.end());
+            if (r.link >= 0) r.link += offset;
+        } else {
+            l = build_into(out, begin, mid, depth + 1);
+            r = build_into(out, mid, end, depth + 1);
+        }
+        write(out, index, l, r);
         return {box, index, 0};
     }
 
-    void write(int index, const Child &l, const Child &r) {
+    void write(int index, const Child &l, const Child &r) { write(nodes, index, l, r); }
+
+    void write(std::vector<psy::BvhNodeGpu> &out, int index, const Child &l, const Child &r) {
         float llo[3], lhi[3], rlo[3], rhi[3];
         padded(l.box, llo, lhi);
         padded(r.box, rlo, rhi);
-        psy::BvhNodeGpu &n = nodes[size_t(index)];
+        psy::BvhNodeGpu &n = out[size_t(index)];
         n.x = make_float4(llo[0], lhi[0], rlo[0], rhi[0]);
         n.y = make_float4(llo[1], lhi[1], rlo[1], rhi[1]);
         n.z = make_float4(llo[2], lhi[2], rlo[2], rhi[2]);
