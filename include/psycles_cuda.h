@@ -268,7 +268,9 @@ void psy_render_settings_default(psy_render_settings *settings);
 const char *psy_last_error(void);
 uint32_t psy_abi_version(void);
 
-/* One context per CUDA device; owns the stream all sessions launch on. */
+/* One context per CUDA device; owns the stream all sessions launch on.
+ * Destroy every server, batch, session and scene of a context before the
+ * context: their device memory is freed in the order of its stream. */
 psy_status psy_context_create(int device, psy_context **out);
 void psy_context_destroy(psy_context *context);
 

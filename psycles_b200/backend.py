@@ -11,14 +11,32 @@ libpsycles_cuda.so.
 
 from __future__ import annotations
 
+import atexit
 import ctypes
 import dataclasses
 import threading
+import weakref
 
 import numpy as np
 
 from . import _abi
 from .scenes import Scene
+
+# Live native objects by kind.  At interpreter exit they are closed in
+# dependency order (servers and batches, then sessions, scenes, contexts),
+# before module teardown could free them in arbitrary order: a scene freed
+# after its context would free device memory on a destroyed stream.
+_LIVE = {kind: weakref.WeakSet() for kind in ("server", "batch", "session", "scene", "context")}
+
+
+@atexit.register
+def _close_all() -> None:
+    for kind in ("server", "batch", "session", "scene", "context"):
+        for obj in list(_LIVE[kind]):
+            try:
+                obj.close()
+            except Exception:
+                pass
 
 PassKind = {
     "combined": _abi.PASS_COMBINED, "normal": _abi.PASS_NORMAL, "albedo": _abi.PASS_ALBEDO,
@@ -96,6 +114,7 @@ class Context:
         h = ctypes.c_void_p()
         _abi.check(self.lib.psy_context_create(device, ctypes.byref(h)))
         self.handle = h
+        _LIVE["context"].add(self)
 
     def close(self) -> None:
         if self.handle:
@@ -113,6 +132,7 @@ class CompiledScene:
     def __init__(self, context: Context, handle: ctypes.c_void_p, scene: Scene):
         self.context = context
         self.handle = handle
+        _LIVE["scene"].add(self)
         self.scene = scene
         self.lib = context.lib
 
@@ -161,6 +181,7 @@ class RenderSession:
                  passes: list[PassRequest]):
         self.compiled = compiled
         self.handle = handle
+        _LIVE["session"].add(self)
         self.settings = settings
         self.passes = passes
         self.lib = compiled.lib
@@ -282,6 +303,7 @@ class BatchRenderer:
         h = ctypes.c_void_p()
         _abi.check(self.lib.psy_batch_create(context.handle, ctypes.byref(cfg), ctypes.byref(h)))
         self.handle = h
+        _LIVE["batch"].add(self)
 
     def render(self, work: list[tuple[RenderSession, SampleRange]]) -> bool:
         n = len(work)
@@ -339,6 +361,7 @@ class RenderServer:
         h = ctypes.c_void_p()
         _abi.check(self.lib.psy_server_create(context.handle, ctypes.byref(cfg), ctypes.byref(h)))
         self.handle = h
+        _LIVE["server"].add(self)
 
     def submit(self, compiled: CompiledScene, settings: _abi.RenderSettings, samples: int, camera=None) -> int:
         from .scenes import camera_desc

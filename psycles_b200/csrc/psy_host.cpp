@@ -1075,7 +1075,10 @@ psy_status psy_context_get_tuning(const psy_context *c, psy_tuning *t) {
 void psy_context_destroy(psy_context *c) {
     if (!c) return;
     cudaSetDevice(c->device);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream) {
+        cudaStreamSynchronize(c->stream);
+        cudaStreamDestroy(c->stream);
+    }
     if (c->readback) cudaStreamDestroy(c->readback);
     if (c->readback_host) cudaFreeHost(c->readback_host);
     delete c;
@@ -1251,28 +1254,41 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         g.mesh = id.mesh;
         g.material = id.material;
         g.visibility = id.visibility;
-        const Box &mb = mesh_boxes[id.mesh];
-        if (mb.empty()) continue;
-        Prim p;
-        for (int corner = 0; corner < 8; ++corner) {
-            const double x = (corner & 1) ? mb.hi[0] : mb.lo[0];
-            const double y = (corner & 2) ? mb.hi[1] : mb.lo[1];
-            const double z = (corner & 4) ? mb.hi[2] : mb.lo[2];
-            const M34 &m = o2w[i];
-            const double wx = x * m.c0.x + y * m.c1.x + z * m.c2.x + m.c3.x;
-            const double wy = x * m.c0.y + y * m.c1.y + z * m.c2.y + m.c3.y;
-            const double wz = x * m.c0.z + y * m.c1.z + z * m.c2.z + m.c3.z;
-            p.box.grow(wx, wy, wz);
+    }
+    // Instance boxes: the world-space bounds of the instance's transformed
+    // vertices (the mesh box's transformed corners would be up to about 1.7
+    // times wider per axis under rotation), computed in double per instance
+    // in parallel, then widened for the float transform of the ray by ten
+    // times the mesh boxes' relative padding.
+    {
+        std::vector<Box> instance_boxes(d->instance_count);
+        uint32_t box_threads = 0u;
+        const psy_status boxed = parallel_for(d->instance_count, &box_threads, [&](uint32_t i) {
+            const psy_mesh_desc &m = d->meshes[d->instances[i].mesh];
+            if (mesh_boxes[d->instances[i].mesh].empty()) return;
+            const M34 &t = o2w[i];
+            Box &b = instance_boxes[i];
+            for (uint64_t v = 0; v < m.vertex_count; ++v) {
+                const double x = m.positions[3 * v], y = m.positions[3 * v + 1], z = m.positions[3 * v + 2];
+                b.grow(x * t.c0.x + y * t.c1.x + z * t.c2.x + t.c3.x, x * t.c0.y + y * t.c1.y + z * t.c2.y + t.c3.y,
+                       x * t.c0.z + y * t.c1.z + z * t.c2.z + t.c3.z);
+            }
+        });
+        if (boxed != PSY_OK) return boxed;
+        for (uint32_t i = 0; i < d->instance_count; ++i) {
+            if (instance_boxes[i].empty()) continue;
+            Prim p;
+            p.box = instance_boxes[i];
+            for (int a = 0; a < 3; ++a) {
+                const double pad = 1e-4 * (p.box.hi[a] - p.box.lo[a]) +
+                                   1e-5 * std::max(std::fabs(p.box.lo[a]), std::fabs(p.box.hi[a]));
+                p.box.lo[a] -= pad;
+                p.box.hi[a] += pad;
+                p.c[a] = 0.5 * (p.box.lo[a] + p.box.hi[a]);
+            }
+            p.id = i;
+            tl.prims.push_back(p);
         }
-        // relative widening for the float transform of the ray
-        for (int a = 0; a < 3; ++a) {
-            const double pad = 1e-5 * (p.box.hi[a] - p.box.lo[a]) + 1e-6 * std::max(std::fabs(p.box.lo[a]), std::fabs(p.box.hi[a]));
-            p.box.lo[a] -= pad;
-            p.box.hi[a] += pad;
-            p.c[a] = 0.5 * (p.box.lo[a] + p.box.hi[a]);
-        }
-        p.id = i;
-        tl.prims.push_back(p);
     }
     tl.build_root();
     Box world;
