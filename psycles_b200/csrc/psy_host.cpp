@@ -1427,7 +1427,15 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     sc->lights_host = lights;
     sc->stats.emitters_ms = lap();
 
-    // ---- upload
+    // ---- upload.  Every scene array is a stream-ordered allocation from the
+    // device pool: a later compile reuses the memory a destroyed scene gave
+    // back, and parameter blocks replaced by edits are retired without
+    // waiting on the device.
+    for (DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tris, &sc->instances, &sc->meshes, &sc->positions, &sc->normals,
+                            &sc->indices, &sc->tri_materials, &sc->material_buf, &sc->code, &sc->scalar_buf,
+                            &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights, &sc->lamp_consts,
+                            &sc->lamp_bounds, &sc->lamp_ids})
+        b->ordered = st;
     PSY_CUDA_TRY(sc->tlas.upload(tl.widen(), st));
     PSY_CUDA_TRY(sc->blas.upload(blas, st));
     PSY_CUDA_TRY(sc->tris.upload(tris, st));
@@ -1439,10 +1447,6 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->tri_materials.upload(tri_materials, st));
     PSY_CUDA_TRY(sc->material_buf.upload(sc->materials, st));
     PSY_CUDA_TRY(sc->code.upload(code, st));
-    // parameter blocks are replaced by edits while work may still read them:
-    // stream-ordered, so retiring them never waits on the device
-    sc->scalar_buf.ordered = st;
-    sc->vector_buf.ordered = st;
     PSY_CUDA_TRY(sc->scalar_buf.upload(sc->scalars, st));
     PSY_CUDA_TRY(sc->vector_buf.upload(sc->vectors, st));
     PSY_CUDA_TRY(sc->emitters.upload(emitters, st));
