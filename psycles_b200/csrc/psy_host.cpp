@@ -1324,11 +1324,22 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     // ---- emissive triangles + flat light distribution
     // (src/sampling/light_distribution.cpp:25-150; emitter geometry as in
     // src/luisa/path_kernel_emissive_triangle.cpp:80-150)
-    // per instance in parallel, concatenated in instance order
-    std::vector<std::vector<psy::EmitterGpu>> instance_emitters(d->instance_count);
+    // in parallel over chunks of an instance's triangles, concatenated in
+    // (instance, triangle) order
+    constexpr uint32_t kEmitterChunk = 4096u;
+    struct EmitterJob {
+        uint32_t instance, first, end;
+    };
+    std::vector<EmitterJob> emitter_jobs;
+    for (uint32_t i = 0; i < d->instance_count; ++i) {
+        const uint32_t n = d->meshes[d->instances[i].mesh].triangle_count;
+        for (uint32_t f = 0; f < n; f += kEmitterChunk) emitter_jobs.push_back({i, f, std::min(n, f + kEmitterChunk)});
+    }
+    std::vector<std::vector<psy::EmitterGpu>> instance_emitters(emitter_jobs.size());
     uint32_t emitter_threads = 0u;
-    const psy_status emit_status = parallel_for(d->instance_count, &emitter_threads, [&](uint32_t i) {
-        std::vector<psy::EmitterGpu> &out_e = instance_emitters[i];
+    const psy_status emit_status = parallel_for(uint32_t(emitter_jobs.size()), &emitter_threads, [&](uint32_t job) {
+        const uint32_t i = emitter_jobs[job].instance;
+        std::vector<psy::EmitterGpu> &out_e = instance_emitters[job];
         const psy_instance_desc &id = d->instances[i];
         const psy_mesh_desc &m = d->meshes[id.mesh];
         const psy::InstanceGpu &g = instances[i];
@@ -1337,7 +1348,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         nrm.c1 = {g.nrm[3], g.nrm[4], g.nrm[5]};
         nrm.c2 = {g.nrm[6], g.nrm[7], g.nrm[8]};
         nrm.c3 = {0, 0, 0};
-        for (uint32_t k = 0; k < m.triangle_count; ++k) {
+        for (uint32_t k = emitter_jobs[job].first; k < emitter_jobs[job].end; ++k) {
             const uint32_t mi = m.materials ? m.materials[k] : id.material;
             const psy::MaterialGpu &mat = sc->materials[mi];
             if (!mat.has_emission || mat.emission_sampling == 0u) continue;
@@ -1374,6 +1385,10 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     if (emit_status != PSY_OK) return emit_status;
     std::vector<psy::EmitterGpu> emitters;
     std::vector<float> areas;
+    size_t emitter_total = 0;
+    for (const std::vector<psy::EmitterGpu> &v : instance_emitters) emitter_total += v.size();
+    emitters.reserve(emitter_total);
+    areas.reserve(emitter_total);
     for (const std::vector<psy::EmitterGpu> &v : instance_emitters)
         for (const psy::EmitterGpu &e : v) {
             emitters.push_back(e);
@@ -1381,6 +1396,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         }
     std::vector<psy::DistEntryGpu> dist;
     const uint32_t tri_n = uint32_t(areas.size()), light_n = d->light_count;
+    dist.reserve(size_t(tri_n) + light_n + 1u);
     auto valid_area = [](float a) { return std::isfinite(a) && a > 0.0f ? a : 0.0f; };
     float total = 0.0f;
     for (uint32_t i = 0; i < tri_n; ++i) {
@@ -2029,8 +2045,15 @@ psy_status psy_session_read_pass(psy_session *s, uint32_t pass_kind, float *out,
     PSY_CUDA_TRY(cudaGetLastError());
     PSY_CUDA_TRY(cudaMemcpyAsync(ctx->readback_host, ctx->readback_pass.ptr, bytes, cudaMemcpyDeviceToHost, st));
     PSY_CUDA_TRY(cudaStreamSynchronize(st));
-    std::memcpy(out, ctx->readback_host, bytes);
-    return PSY_OK;
+    // staging -> caller's buffer, in 8 MiB pieces on several host threads
+    constexpr size_t kPiece = size_t(8) << 20;
+    const size_t pieces = (bytes + kPiece - 1) / kPiece;
+    const unsigned char *from = static_cast<const unsigned char *>(ctx->readback_host);
+    unsigned char *to = reinterpret_cast<unsigned char *>(out);
+    return parallel_for(uint32_t(pieces), nullptr, [&](uint32_t k) {
+        const size_t at = size_t(k) * kPiece;
+        std::memcpy(to + at, from + at, std::min(kPiece, bytes - at));
+    });
 }
 
 psy_status psy_session_set_profiling(psy_session *s, uint32_t enabled) {
