@@ -610,13 +610,20 @@ __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneVi
         const uint32_t lk[4] = {uint32_t(n.link.x), uint32_t(n.link.y), uint32_t(n.link.z), uint32_t(n.link.w)};
         const int ct[4] = {n.count.x, n.count.y, n.count.z, n.count.w};
         // leaves first: their triangles may shrink tmax before the inner
-        // children are ordered
+        // children are ordered.  The hit leaf slots are walked as a bit set
+        // through one copy of the triangle test, so lanes whose leaves sit
+        // in different slots test them together.
         if (blas) {
+            uint32_t leaves = 0u;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (!hit[k] || ct[k] == 0) continue;
-                const uint32_t first = lk[k];
-                for (int q = 0; q < ct[k]; ++q) {
+            for (int k = 0; k < 4; ++k)
+                if (hit[k] && ct[k] != 0) leaves |= 1u << k;
+            while (leaves != 0u) {
+                const uint32_t k = uint32_t(__ffs(int(leaves)) - 1);
+                leaves &= leaves - 1u;
+                const uint32_t first = k == 0u ? lk[0] : k == 1u ? lk[1] : k == 2u ? lk[2] : lk[3];
+                const int cnt = k == 0u ? ct[0] : k == 1u ? ct[1] : k == 2u ? ct[2] : ct[3];
+                for (int q = 0; q < cnt; ++q) {
                     const float4 *tp = s.tris + 3u * (first + uint32_t(q));
                     const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
                     const uint32_t local = __float_as_uint(a.w);
