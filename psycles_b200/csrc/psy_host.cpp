@@ -28,6 +28,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <exception>
 #include <thread>
 #include <vector>
 
@@ -336,19 +337,33 @@ struct Builder {
         return {box, ~int(begin), int(end - begin)};
     }
 
+    static void grow_side(const Prim &p, Box &box, Box &cbox) {
+        box.grow(p.box);
+        cbox.grow(p.c[0], p.c[1], p.c[2]);
+    }
+
     // Binary SAH build of prims [begin, end) into `out` (pre-order node
     // list).  Large ranges near the root build their right half on a thread
     // of its own into a separate list that is spliced in after the left
     // half, so the tree and its node order equal the sequential build's
     // (the two halves touch disjoint prim ranges).
-    Child build(uint32_t begin, uint32_t end, int depth) { return build_into(nodes, begin, end, depth); }
-
-    Child build_into(std::vector<psy::BvhNodeGpu> &out, uint32_t begin, uint32_t end, int depth) {
+    Child build(uint32_t begin, uint32_t end, int depth) {
         Box box, cbox;
+        bounds(begin, end, box, cbox);
+        return build_into(nodes, begin, end, depth, box, cbox);
+    }
+
+    // Box of the prims [begin, end) and of their centroids.
+    void bounds(uint32_t begin, uint32_t end, Box &box, Box &cbox) const {
         for (uint32_t i = begin; i < end; ++i) {
             box.grow(prims[i].box);
             cbox.grow(prims[i].c[0], prims[i].c[1], prims[i].c[2]);
         }
+    }
+
+    // `box` / `cbox` bound the prims [begin, end) and their centroids.
+    Child build_into(std::vector<psy::BvhNodeGpu> &out, uint32_t begin, uint32_t end, int depth, const Box &box,
+                     const Box &cbox) {
         const uint32_t count = end - begin;
         if (count <= leaf_size) return leaf(begin, end, box);
         // binned SAH: PSY_SAH_BINS bins on every axis with a centroid extent
@@ -358,53 +373,116 @@ struct Builder {
             if (cbox.hi[a] - cbox.lo[a] > cbox.hi[axis] - cbox.lo[axis]) axis = a;
         uint32_t mid = begin + count / 2u;
         bool done = false;
+        Box lbox, lcbox, rbox, rcbox;
         if (depth < 60) {
+            // one pass bins the centroids on every axis; the sweep then visits
+            // only the boundaries right after non-empty bins (a boundary after
+            // an empty bin costs the same as the one before it, and the first
+            // of equal costs wins, so the chosen split is the one a sweep over
+            // every boundary finds)
             constexpr int kBins = PSY_SAH_BINS;
+            struct BinBox {
+                double lo[3], hi[3];
+            };
+            BinBox bins[3][kBins];
+            uint32_t counts[3][kBins] = {};
+            double scale[3];
+            bool use[3];
+            for (int a = 0; a < 3; ++a) {
+                const double extent = cbox.hi[a] - cbox.lo[a];
+                use[a] = (PSY_SAH_AXES != 1 || a == axis) && extent > 0.0;
+                scale[a] = use[a] ? kBins / extent : 0.0;
+            }
+            for (uint32_t i = begin; i < end; ++i) {
+                const Prim &p = prims[i];
+                for (int a = 0; a < 3; ++a) {
+                    if (!use[a]) continue;
+                    const int bn = std::min(std::max(int((p.c[a] - cbox.lo[a]) * scale[a]), 0), kBins - 1);
+                    BinBox &bb = bins[a][bn];
+                    if (counts[a][bn]++ == 0u) {
+                        for (int e = 0; e < 3; ++e) {
+                            bb.lo[e] = p.box.lo[e];
+                            bb.hi[e] = p.box.hi[e];
+                        }
+                    } else {
+                        for (int e = 0; e < 3; ++e) {
+                            bb.lo[e] = std::min(bb.lo[e], p.box.lo[e]);
+                            bb.hi[e] = std::max(bb.hi[e], p.box.hi[e]);
+                        }
+                    }
+                }
+            }
             double best = 1e300;
             int best_split = -1, best_axis = -1;
             for (int a = 0; a < 3; ++a) {
-                if (PSY_SAH_AXES == 1 && a != axis) continue;
-                const double extent = cbox.hi[a] - cbox.lo[a];
-                if (!(extent > 0.0)) continue;
-                Box bins[kBins];
-                uint32_t counts[kBins] = {};
-                const double scale = kBins / extent;
-                for (uint32_t i = begin; i < end; ++i) {
-                    const int bn = std::min(std::max(int((prims[i].c[a] - cbox.lo[a]) * scale), 0), kBins - 1);
-                    bins[bn].grow(prims[i].box);
-                    counts[bn]++;
-                }
+                if (!use[a]) continue;
+                int filled[kBins];
+                int m = 0;
+                for (int bn = 0; bn < kBins; ++bn)
+                    if (counts[a][bn] != 0u) filled[m++] = bn;
+                if (m < 2) continue;
                 double right_area[kBins];
                 uint32_t right_count[kBins];
                 Box acc;
                 uint32_t acc_n = 0u;
-                for (int bn = kBins - 1; bn > 0; --bn) {
-                    acc.grow(bins[bn]);
-                    acc_n += counts[bn];
-                    right_area[bn] = acc.area();
-                    right_count[bn] = acc_n;
+                for (int j = m - 1; j > 0; --j) {
+                    const BinBox &bb = bins[a][filled[j]];
+                    for (int e = 0; e < 3; ++e) {
+                        acc.lo[e] = std::min(acc.lo[e], bb.lo[e]);
+                        acc.hi[e] = std::max(acc.hi[e], bb.hi[e]);
+                    }
+                    acc_n += counts[a][filled[j]];
+                    right_area[j] = acc.area();
+                    right_count[j] = acc_n;
                 }
                 Box left;
                 uint32_t left_n = 0u;
-                for (int bn = 1; bn < kBins; ++bn) {
-                    left.grow(bins[bn - 1]);
-                    left_n += counts[bn - 1];
-                    if (left_n == 0u || right_count[bn] == 0u) continue;
-                    const double cost = left.area() * left_n + right_area[bn] * right_count[bn];
+                for (int j = 1; j < m; ++j) {
+                    const BinBox &bb = bins[a][filled[j - 1]];
+                    for (int e = 0; e < 3; ++e) {
+                        left.lo[e] = std::min(left.lo[e], bb.lo[e]);
+                        left.hi[e] = std::max(left.hi[e], bb.hi[e]);
+                    }
+                    left_n += counts[a][filled[j - 1]];
+                    const double cost = left.area() * left_n + right_area[j] * right_count[j];
                     if (cost < best) {
                         best = cost;
-                        best_split = bn;
+                        best_split = filled[j - 1] + 1;
                         best_axis = a;
                     }
                 }
             }
             if (best_split > 0) {
                 const int a = best_axis;
-                const double scale = kBins / (cbox.hi[a] - cbox.lo[a]);
-                auto it = std::partition(prims.begin() + begin, prims.begin() + end, [&](const Prim &p) {
-                    return std::min(std::max(int((p.c[a] - cbox.lo[a]) * scale), 0), kBins - 1) < best_split;
-                });
-                mid = uint32_t(it - prims.begin());
+                const double scale_a = scale[a];
+                const auto left_side = [&](const Prim &p) {
+                    return std::min(std::max(int((p.c[a] - cbox.lo[a]) * scale_a), 0), kBins - 1) < best_split;
+                };
+                // two-ended partition (the classic exchange order, so the
+                // permutation is the one std::partition gives on these
+                // iterators) that also bounds both sides for the children
+                uint32_t first = begin, last = end;
+                for (;;) {
+                    while (first != last && left_side(prims[first])) {
+                        grow_side(prims[first], lbox, lcbox);
+                        ++first;
+                    }
+                    if (first == last) break;
+                    --last;
+                    while (first != last && !left_side(prims[last])) {
+                        grow_side(prims[last], rbox, rcbox);
+                        --last;
+                    }
+                    if (first == last) {
+                        grow_side(prims[last], rbox, rcbox);
+                        break;
+                    }
+                    std::swap(prims[first], prims[last]);
+                    grow_side(prims[first], lbox, lcbox);
+                    grow_side(prims[last], rbox, rcbox);
+                    ++first;
+                }
+                mid = first;
                 done = mid > begin && mid < end;
             }
         }
@@ -414,15 +492,31 @@ struct Builder {
                              [&](const Prim &a, const Prim &b) {
                                  return a.c[axis] < b.c[axis] || (a.c[axis] == b.c[axis] && a.id < b.id);
                              });
+            lbox = lcbox = rbox = rcbox = Box{};
+            bounds(begin, mid, lbox, lcbox);
+            bounds(mid, end, rbox, rcbox);
         }
         const int index = int(out.size());
         out.push_back({});
         Child l, r;
-        if (parallel && depth < 3 && count >= 16384u) {
+        if (parallel && depth < 8 && count >= 2048u) {
             std::vector<psy::BvhNodeGpu> right_nodes;
-            std::thread worker([&]() { r = build_into(right_nodes, mid, end, depth + 1); });
-            l = build_into(out, begin, mid, depth + 1);
+            std::exception_ptr error;
+            std::thread worker([&]() {
+                try {
+                    r = build_into(right_nodes, mid, end, depth + 1, rbox, rcbox);
+                } catch (...) {
+                    error = std::current_exception();
+                }
+            });
+            try {
+                l = build_into(out, begin, mid, depth + 1, lbox, lcbox);
+            } catch (...) {
+                worker.join();
+                throw;
+            }
             worker.join();
+            if (error) std::rethrow_exception(error);
             const int offset = int(out.size());
             for (psy::BvhNodeGpu &n : right_nodes) {
                 if (n.child.x >= 0) n.child.x += offset;
@@ -431,8 +525,8 @@ struct Builder {
             out.insert(out.end(), right_nodes.begin(), right_nodes.end());
             if (r.link >= 0) r.link += offset;
         } else {
-            l = build_into(out, begin, mid, depth + 1);
-            r = build_into(out, mid, end, depth + 1);
+            l = build_into(out, begin, mid, depth + 1, lbox, lcbox);
+            r = build_into(out, mid, end, depth + 1, rbox, rcbox);
         }
         write(out, index, l, r);
         return {box, index, 0};
@@ -1156,7 +1250,11 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     std::vector<float4> tris;
     std::vector<Box> mesh_boxes(d->mesh_count);
     std::vector<std::vector<psy::WideNodeGpu>> mesh_wide(d->mesh_count);
-    std::vector<std::vector<uint32_t>> mesh_order(d->mesh_count);
+    // triangle records in BVH leaf order, written by each mesh's build at
+    // the mesh's offset (meshes in input order)
+    std::vector<uint64_t> mesh_tri_first(d->mesh_count + 1u, 0u);
+    for (uint32_t i = 0; i < d->mesh_count; ++i) mesh_tri_first[i + 1u] = mesh_tri_first[i] + d->meshes[i].triangle_count;
+    tris.resize(3u * mesh_tri_first[d->mesh_count]);
     {
         std::vector<uint32_t> by_size(d->mesh_count);
         for (uint32_t i = 0; i < d->mesh_count; ++i) by_size[i] = i;
@@ -1179,8 +1277,16 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
             }
             mesh_boxes[i] = bld.build_root();
             mesh_wide[i] = bld.widen();
-            mesh_order[i].resize(bld.prims.size());
-            for (size_t k = 0; k < bld.prims.size(); ++k) mesh_order[i][k] = bld.prims[k].id;
+            float4 *out = tris.data() + 3u * mesh_tri_first[i];
+            for (const Prim &p : bld.prims) {
+                const uint32_t id = p.id;
+                for (int c = 0; c < 3; ++c) {
+                    const float *v = m.positions + 3ull * m.indices[3ull * id + c];
+                    float w = 0.0f;
+                    if (c == 0) std::memcpy(&w, &id, 4);
+                    *out++ = make_float4(v[0], v[1], v[2], w);
+                }
+            }
         });
         if (built != PSY_OK) return built;
     }
@@ -1205,7 +1311,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
             g.material_offset = psy::kInvalidId;
         }
         g.node_offset = uint32_t(blas.size());
-        g.tri_offset = uint32_t(tris.size() / 3u);
+        g.tri_offset = uint32_t(mesh_tri_first[i]);
         // global node and triangle indices of the mesh's links
         for (psy::WideNodeGpu &w : mesh_wide[i]) {
             int *lk = &w.link.x;
@@ -1219,14 +1325,6 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         }
         blas.insert(blas.end(), mesh_wide[i].begin(), mesh_wide[i].end());
         std::vector<psy::WideNodeGpu>().swap(mesh_wide[i]);
-        for (const uint32_t id : mesh_order[i]) {
-            for (int c = 0; c < 3; ++c) {
-                const float *v = m.positions + 3ull * m.indices[3ull * id + c];
-                float w = 0.0f;
-                if (c == 0) std::memcpy(&w, &id, 4);
-                tris.push_back(make_float4(v[0], v[1], v[2], w));
-            }
-        }
         sc->triangle_count += m.triangle_count;
     }
     if (blas.empty()) blas.push_back({});
@@ -1383,17 +1481,22 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         }
     });
     if (emit_status != PSY_OK) return emit_status;
-    std::vector<psy::EmitterGpu> emitters;
-    std::vector<float> areas;
-    size_t emitter_total = 0;
-    for (const std::vector<psy::EmitterGpu> &v : instance_emitters) emitter_total += v.size();
-    emitters.reserve(emitter_total);
-    areas.reserve(emitter_total);
-    for (const std::vector<psy::EmitterGpu> &v : instance_emitters)
-        for (const psy::EmitterGpu &e : v) {
-            emitters.push_back(e);
-            areas.push_back(e.area);
+    // the chunks' emitters concatenated in chunk order, each chunk copied on
+    // a thread of its own
+    std::vector<size_t> chunk_first(instance_emitters.size() + 1u, 0u);
+    for (size_t j = 0; j < instance_emitters.size(); ++j)
+        chunk_first[j + 1u] = chunk_first[j] + instance_emitters[j].size();
+    std::vector<psy::EmitterGpu> emitters(chunk_first.back());
+    std::vector<float> areas(chunk_first.back());
+    const psy_status gathered = parallel_for(uint32_t(instance_emitters.size()), nullptr, [&](uint32_t job) {
+        const std::vector<psy::EmitterGpu> &v = instance_emitters[job];
+        for (size_t k = 0; k < v.size(); ++k) {
+            emitters[chunk_first[job] + k] = v[k];
+            areas[chunk_first[job] + k] = v[k].area;
         }
+    });
+    if (gathered != PSY_OK) return gathered;
+    std::vector<std::vector<psy::EmitterGpu>>().swap(instance_emitters);
     std::vector<psy::DistEntryGpu> dist;
     const uint32_t tri_n = uint32_t(areas.size()), light_n = d->light_count;
     dist.reserve(size_t(tri_n) + light_n + 1u);
@@ -1439,7 +1542,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     }
 
     sc->code_host = code;
-    sc->emitters_host = emitters;
+    sc->emitters_host = std::move(emitters);
     sc->lights_host = lights;
     sc->stats.emitters_ms = lap();
 
@@ -1465,7 +1568,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->code.upload(code, st));
     PSY_CUDA_TRY(sc->scalar_buf.upload(sc->scalars, st));
     PSY_CUDA_TRY(sc->vector_buf.upload(sc->vectors, st));
-    PSY_CUDA_TRY(sc->emitters.upload(emitters, st));
+    PSY_CUDA_TRY(sc->emitters.upload(sc->emitters_host, st));
     PSY_CUDA_TRY(sc->distribution.upload(dist, st));
     PSY_CUDA_TRY(sc->lights.upload(lights, st));
     std::vector<psy::LampConstGpu> lamp_consts;
