@@ -275,7 +275,8 @@ def run_cuda(args) -> None:
         else:
             e2e_ms.append((t3 - t0) * 1e3)
         bs = comp2.scene.build_stats()
-        phases = {"compile_ms": (t1 - t0) * 1e3, "session_render_ms": (t2 - t1) * 1e3, "readback_ms": (t3 - t2) * 1e3,
+        phases = {"compile_ms": (t1 - t0) * 1e3, "session_render_ms": (t2 - t1) * 1e3,
+                  "render_device_ms": sess2.stats().ms_total, "readback_ms": (t3 - t2) * 1e3,
                   "build": {n: (round(getattr(bs, n), 3) if isinstance(getattr(bs, n), float) else getattr(bs, n))
                             for n, _ in bs._fields_}}
         sess2.close()

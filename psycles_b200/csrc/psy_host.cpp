@@ -41,22 +41,26 @@ psy_status fail(psy_status status, const std::string &message) {
     return status;
 }
 
+void bind_records(PathBuffers &b, unsigned char *records) {
+    b.ray_o.base = records + psy::kRecRayO;
+    b.ray_d.base = records + psy::kRecRayD;
+    b.st.base = records + psy::kRecSt;
+    b.st2.base = records + psy::kRecSt2;
+    b.tp.base = records + psy::kRecTp;
+    b.rad.base = records + psy::kRecRad;
+    b.hit.base = records + psy::kRecHit;
+    b.hit_prim.base = records + psy::kRecHitPrim;
+}
+
 psy_status PathArena::ensure(uint32_t n, bool with_job) {
     if (capacity >= n && (!with_job || job.ptr)) return PSY_OK;
     const uint32_t c = std::max(n, capacity);
     const size_t f4 = sizeof(float4) * size_t(c), u4 = sizeof(uint4) * size_t(c), u1 = sizeof(uint32_t) * size_t(c);
-    PSY_CUDA_TRY(ray_o.alloc(f4));
-    PSY_CUDA_TRY(ray_d.alloc(f4));
-    PSY_CUDA_TRY(tp.alloc(f4));
-    PSY_CUDA_TRY(rad.alloc(f4));
-    PSY_CUDA_TRY(st.alloc(u4));
-    PSY_CUDA_TRY(st2.alloc(u4));
+    PSY_CUDA_TRY(records.alloc(psy::kPathRecordBytes * size_t(c)));
     PSY_CUDA_TRY(sample.alloc(u1));
     PSY_CUDA_TRY(aov_n.alloc(f4));
     PSY_CUDA_TRY(aov_a.alloc(f4));
     PSY_CUDA_TRY(mis_n.alloc(f4));
-    PSY_CUDA_TRY(hit.alloc(f4));
-    PSY_CUDA_TRY(hit_prim.alloc(u1));
     PSY_CUDA_TRY(sh_o.alloc(f4));
     PSY_CUDA_TRY(sh_d.alloc(f4));
     PSY_CUDA_TRY(sh_c.alloc(f4));
@@ -76,18 +80,11 @@ psy_status PathArena::ensure(uint32_t n, bool with_job) {
     if (!stats.ptr) PSY_CUDA_TRY(stats.alloc(64));
     capacity = c;
     PathBuffers &b = view;
-    b.ray_o = ray_o.as<float4>();
-    b.ray_d = ray_d.as<float4>();
-    b.tp = tp.as<float4>();
-    b.rad = rad.as<float4>();
-    b.st = st.as<uint4>();
-    b.st2 = st2.as<uint4>();
+    bind_records(b, records.as<unsigned char>());
     b.sample = sample.as<uint32_t>();
     b.aov_n = aov_n.as<float4>();
     b.aov_a = aov_a.as<float4>();
     b.mis_n = mis_n.as<float4>();
-    b.hit = hit.as<float4>();
-    b.hit_prim = hit_prim.as<uint32_t>();
     b.sh_o = sh_o.as<float4>();
     b.sh_d = sh_d.as<float4>();
     b.sh_c = sh_c.as<float4>();
@@ -106,7 +103,8 @@ psy_status PathArena::ensure(uint32_t n, bool with_job) {
 }
 
 size_t PathArena::bytes_per_path(bool with_job) {
-    return 10u * sizeof(float4) + 4u * sizeof(uint4) + (9u + (with_job ? 1u : 0u)) * sizeof(uint32_t);
+    return psy::kPathRecordBytes + 6u * sizeof(float4) + 1u * sizeof(uint4) +
+           (8u + (with_job ? 1u : 0u)) * sizeof(uint32_t);
 }
 
 }  // namespace psy::host
@@ -2024,18 +2022,11 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
     };
     const size_t n = psy::kStaticMaxPaths;
     psy::PathBuffers b{};
-    b.ray_o = reinterpret_cast<float4 *>(carve(16 * n));
-    b.ray_d = reinterpret_cast<float4 *>(carve(16 * n));
-    b.tp = reinterpret_cast<float4 *>(carve(16 * n));
-    b.rad = reinterpret_cast<float4 *>(carve(16 * n));
-    b.st = reinterpret_cast<uint4 *>(carve(16 * n));
-    b.st2 = reinterpret_cast<uint4 *>(carve(16 * n));
+    psy::host::bind_records(b, carve(psy::kPathRecordBytes * n));
     b.sample = reinterpret_cast<uint32_t *>(carve(4 * n));
     b.aov_n = reinterpret_cast<float4 *>(carve(16 * n));
     b.aov_a = reinterpret_cast<float4 *>(carve(16 * n));
     b.mis_n = reinterpret_cast<float4 *>(carve(16 * n));
-    b.hit = reinterpret_cast<float4 *>(carve(16 * n));
-    b.hit_prim = reinterpret_cast<uint32_t *>(carve(4 * n));
     b.sh_o = reinterpret_cast<float4 *>(carve(16 * n));
     b.sh_d = reinterpret_cast<float4 *>(carve(16 * n));
     b.sh_c = reinterpret_cast<float4 *>(carve(16 * n));

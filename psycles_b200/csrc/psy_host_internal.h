@@ -101,16 +101,20 @@ struct DeviceBuffer {
     }
 };
 
-// Wavefront path state over `capacity` paths (structure of arrays); the
-// per-path job array only for batched wavefronts.
+// Wavefront path state over `capacity` paths: the 128-byte per-path
+// records and the arrays of the other fields; the per-path job array only
+// for batched wavefronts.
 struct PathArena {
     uint32_t capacity = 0;
-    DeviceBuffer ray_o, ray_d, tp, rad, st, st2, sample, aov_n, aov_a, mis_n, hit, hit_prim, sh_o, sh_d, sh_c, sh_ids,
-        sh_path, qa, qb, sq, job, sort_keys, queue_sorted, sort_hist, counters, stats;
+    DeviceBuffer records, sample, aov_n, aov_a, mis_n, sh_o, sh_d, sh_c, sh_ids, sh_path, qa, qb, sq, job, sort_keys,
+        queue_sorted, sort_hist, counters, stats;
     PathBuffers view{};
     psy_status ensure(uint32_t n, bool with_job);
     static size_t bytes_per_path(bool with_job);
 };
+
+// Points the record fields of `b` into the records starting at `records`.
+void bind_records(PathBuffers &b, unsigned char *records);
 
 }  // namespace psy::host
 

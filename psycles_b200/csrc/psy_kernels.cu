@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(128, PSY_INTERSECT_MIN_BLOCKS)
             });
             if (done) {
                 b.hit[path] = make_float4(best.t, best.u, best.v, __uint_as_float(best.instance));
-                b.hit_prim[path] = has ? best.prim : kInvalid;
+                b.hit_prim[path] = make_uint4(has ? best.prim : kInvalid, 0u, 0u, 0u);
                 active = false;
             }
         }
@@ -437,7 +437,7 @@ __global__ void k_sort_count(const __grid_constant__ SceneView s_arg, const __gr
     __syncthreads();
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
         const uint32_t i = b.queue_in[q];
-        const uint32_t prim = b.hit_prim[i];
+        const uint32_t prim = b.hit_prim[i].x;
         uint32_t key = 0u;
         if (prim != kInvalid) {
             const uint32_t job = kMulti ? b.job[i] : 0u;
@@ -647,7 +647,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
             DistEntryGpu selected = p.use_light_tree ? DistEntryGpu{0.0f, 0.0f, 3u, 0u}
                                                      : distribution_sample(s, light_sample.z);
             const float4 h4 = b.hit[i];
-            const uint32_t prim = b.hit_prim[i];
+            const uint32_t prim = b.hit_prim[i].x;
             if (ev) {
                 ev->rng_offset = ps.rng_offset;
                 ev->random_terminate = terminate_sample;

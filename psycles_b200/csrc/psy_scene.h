@@ -166,19 +166,37 @@ struct RenderParams {
 };
 
 // Wavefront path state, structure of arrays over `capacity` paths.
+// The per-path fields every bounce reads and writes share one 128-byte
+// record per path, in four 32-byte sectors: ray origin and direction; the
+// two state words; throughput and radiance; the hit and its primitive
+// (whose sector's other 12 bytes are written as zeros, so the closest-hit
+// kernel writes whole sectors).  The shading kernel takes its paths in
+// material order, and one cache line per path then replaces a sector in
+// each of eight arrays.
+constexpr size_t kPathRecordBytes = 128u;
+template <class T>
+struct PathField {
+    unsigned char *base;  // the field in path 0's record
+    __host__ __device__ __forceinline__ T &operator[](size_t i) const {
+        return *reinterpret_cast<T *>(base + i * kPathRecordBytes);
+    }
+};
+constexpr size_t kRecRayO = 0u, kRecRayD = 16u, kRecSt = 32u, kRecSt2 = 48u, kRecTp = 64u, kRecRad = 80u,
+                 kRecHit = 96u, kRecHitPrim = 112u;
+
 struct PathBuffers {
-    float4 *ray_o;    // origin, tmin
-    float4 *ray_d;    // direction, tmax
-    float4 *tp;       // throughput, previous bsdf pdf
-    float4 *rad;      // radiance, transparency
-    uint4 *st;        // flag, cycles visibility, rng_offset, packed counters
-    uint4 *st2;       // transparent bounce | bits, source object, source prim, pixel
-    uint32_t *sample; // absolute sample index
-    float4 *aov_n;    // first-surface normal
-    float4 *aov_a;    // albedo
-    float4 *mis_n;    // shading normal of the last non-transparent scatter (light-tree MIS)
-    float4 *hit;      // t, u, v, instance bits
-    uint32_t *hit_prim;
+    PathField<float4> ray_o;    // origin, tmin
+    PathField<float4> ray_d;    // direction, tmax
+    PathField<float4> tp;       // throughput, previous bsdf pdf
+    PathField<float4> rad;      // radiance, transparency
+    PathField<uint4> st;        // flag, cycles visibility, rng_offset, packed counters
+    PathField<uint4> st2;       // transparent bounce | bits, source object, source prim, pixel
+    uint32_t *sample;           // absolute sample index
+    float4 *aov_n;              // first-surface normal
+    float4 *aov_a;              // albedo
+    float4 *mis_n;              // shading normal of the last non-transparent scatter (light-tree MIS)
+    PathField<float4> hit;      // t, u, v, instance bits
+    PathField<uint4> hit_prim;  // x: primitive (kInvalid on a miss); y, z, w: 0
     float4 *sh_o;     // shadow origin, tmax
     float4 *sh_d;     // shadow direction, transparent depth bits
     float4 *sh_c;     // unshadowed contribution
