@@ -528,8 +528,8 @@ def run_viewports(backend, compiled, count: int = 64, capacity: int = 0) -> dict
 # procedural render: DRAM read + write of the launch over its duration).
 # The traffic of a bench launch is this rate times the launch's mean
 # event-timed duration (the procedural workload only).
-NCU_DRAM_GBS = {"intersect": (954.8 + 120.9) / 2.333, "shadow": (99.5 + 12.6) / 1.961,
-                "shade": (2491.0 + 647.9) / 1.294}
+NCU_DRAM_GBS = {"intersect": (319.3 + 65.7) / 2.150, "shadow": (109.0 + 13.2) / 1.775,
+                "shade": (615.8 + 297.4) / 1.066}
 
 
 def kernel_profile(args, backend, compiled, settings) -> dict:
