@@ -300,6 +300,17 @@ typedef struct psy_scene_build_stats {
     double light_tree_ms;
     uint32_t build_threads; /* host threads of the BLAS builds */
     uint32_t light_tree_builds;
+    /* Traversal stack: the largest stack any ray can build in this scene's
+     * trees (TLAS entries + the return to the world ray + BLAS entries),
+     * proved at compile time to fit the device stack of stack_capacity
+     * entries; a mesh whose SAH tree would not fit is rebuilt with median
+     * splits (counted in median_rebuilds), and a scene that still would
+     * not fit fails to compile with PSY_ERROR_UNSUPPORTED. */
+    uint32_t stack_need;
+    uint32_t stack_capacity;
+    uint32_t median_rebuilds;
+    uint32_t reserved;
+    uint64_t upload_bytes;  /* host -> device bytes of the compile */
 } psy_scene_build_stats;
 psy_status psy_scene_get_build_stats(const psy_scene *scene, psy_scene_build_stats *out);
 
@@ -341,17 +352,21 @@ psy_status psy_session_render_samples(psy_session *session, uint32_t first,
                                       uint32_t total);
 
 /* Allocation-free render_samples, for callers that cannot allocate device
- * memory at render time (a plugin inside a host application's fixed memory
- * budget, work issued into a stream the caller does not own, a real-time
- * viewport thread).  No counterpart in the reference.  Renders the same
- * samples with the same kernels as psy_session_render_samples, but the path
- * state lives in static device arrays (about 17 MiB that every GPU loading
- * the library holds until exit) and the session's Sobol table is not used:
- * at most 65536 window pixels and renders of at most 256 total samples
- * (PSY_ERROR_RANGE beyond).  It calls no cudaMalloc or cudaFree.  The first
- * call on a device takes the arrays' device addresses and fills the static
- * Sobol table; make it before any stream capture.  All calls share the
- * arrays: calls that overlap on the GPU race. */
+ * memory at render time (a plugin held to its host application's fixed
+ * device-memory budget, or a real-time viewport thread that must not stall
+ * on an allocation's implicit synchronisation).  No counterpart in the
+ * reference.  Renders the same samples with the same kernels, in the same
+ * order, as psy_session_render_samples, so the film is bit-identical; the
+ * path state lives in static device arrays (about 17 MiB that every GPU
+ * loading the library holds until exit) and the session's Sobol table is not
+ * used: at most 65536 window pixels and renders of at most 256 total samples
+ * (PSY_ERROR_RANGE beyond).  It calls no cudaMalloc, cudaFree or other
+ * allocating routine.  Like psy_session_render_samples it issues its work on
+ * the context's stream and blocks until the film is updated.  The first call
+ * on a device takes the arrays' device addresses and fills the static Sobol
+ * table; make that first call before any stream capture.  Calls on one
+ * context are serialised; calls on different contexts of one device share
+ * the arrays and race when they overlap on the GPU. */
 psy_status psy_session_render_samples_static(psy_session *session,
                                              uint32_t first, uint32_t count,
                                              uint32_t offset, uint32_t total);

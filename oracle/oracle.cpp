@@ -2032,22 +2032,28 @@ extern "C" {
 // Film sums for the window (row-major): combined (rgb, transparency),
 // normal (xyz, count), albedo (xyz, count), sample count.  Accumulates into
 // the caller's buffers, so progressive calls compose.
-int oracle_render(const psy_scene_desc *desc, const psy_render_settings *settings, uint32_t first, uint32_t count,
-                  uint32_t total, float *combined, float *normal, float *albedo, uint32_t *sample_count,
-                  int threads, int brute_force, int trace_x, int trace_y, int trace_sample, psy_path_trace *trace) {
-    if (!desc || !settings || !combined || !normal || !albedo || !sample_count) return 1;
-    auto scene = prepare_scene(desc, brute_force != 0);
+}  // extern "C"
+
+namespace {
+
+// Renders the window rows whose index is a multiple of `row_stride` over a
+// prepared scene, accumulating into window-sized film sums.
+void render_window(const Scene &scene, const psy_render_settings *settings, uint32_t first, uint32_t count,
+                   uint32_t total, uint32_t row_stride, float *combined, float *normal, float *albedo,
+                   uint32_t *sample_count, int threads, int trace_x, int trace_y, int trace_sample,
+                   psy_path_trace *trace) {
     Settings st;
-    derive_settings(st, *scene, *settings, total);
+    derive_settings(st, scene, *settings, total);
     const psy_render_settings &r = *settings;
     const uint32_t wx = r.window_x, wy = r.window_y;
     const uint32_t ww = r.window_width ? r.window_width : r.full_width;
     const uint32_t wh = r.window_height ? r.window_height : r.full_height;
     if (threads <= 0) threads = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    if (row_stride == 0u) row_stride = 1u;
     std::atomic<uint32_t> next_row{0u};
     auto worker = [&]() {
         for (;;) {
-            const uint32_t row = next_row.fetch_add(1u);
+            const uint32_t row = row_stride * next_row.fetch_add(1u);
             if (row >= wh) return;
             for (uint32_t col = 0; col < ww; ++col) {
                 const uint32_t x = wx + col, y = wy + row;
@@ -2056,7 +2062,7 @@ int oracle_render(const psy_scene_desc *desc, const psy_render_settings *setting
                     const uint32_t sample = first + k;
                     psy_path_trace *tr = nullptr;
                     if (trace && int(x) == trace_x && int(y) == trace_y && int(sample) == trace_sample) tr = trace;
-                    const PathOutput o = render_path(*scene, st, x, y, sample, tr);
+                    const PathOutput o = render_path(scene, st, x, y, sample, tr);
                     combined[4 * pix + 0] += o.radiance.x;
                     combined[4 * pix + 1] += o.radiance.y;
                     combined[4 * pix + 2] += o.radiance.z;
@@ -2078,6 +2084,32 @@ int oracle_render(const psy_scene_desc *desc, const psy_render_settings *setting
     for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
     worker();
     for (auto &t : pool) t.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_render(const psy_scene_desc *desc, const psy_render_settings *settings, uint32_t first, uint32_t count,
+                  uint32_t total, float *combined, float *normal, float *albedo, uint32_t *sample_count,
+                  int threads, int brute_force, int trace_x, int trace_y, int trace_sample, psy_path_trace *trace) {
+    if (!desc || !settings || !combined || !normal || !albedo || !sample_count) return 1;
+    auto scene = prepare_scene(desc, brute_force != 0);
+    render_window(*scene, settings, first, count, total, 1u, combined, normal, albedo, sample_count, threads, trace_x,
+                  trace_y, trace_sample, trace);
+    return 0;
+}
+
+// oracle_render over a scene prepared once by oracle_scene_create (so the
+// BVH build and emitter tables stay out of a timed render), rendering only
+// the window rows whose index is a multiple of `row_stride`.
+int oracle_render_prepared(const void *scene, const psy_render_settings *settings, uint32_t first, uint32_t count,
+                           uint32_t total, uint32_t row_stride, float *combined, float *normal, float *albedo,
+                           uint32_t *sample_count, int threads, int trace_x, int trace_y, int trace_sample,
+                           psy_path_trace *trace) {
+    if (!scene || !settings || !combined || !normal || !albedo || !sample_count) return 1;
+    render_window(*static_cast<const Scene *>(scene), settings, first, count, total, row_stride, combined, normal,
+                  albedo, sample_count, threads, trace_x, trace_y, trace_sample, trace);
     return 0;
 }
 

@@ -33,6 +33,10 @@ def load() -> ctypes.CDLL:
         lib.oracle_render.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp, vp, vp, vp,
                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
         lib.oracle_render.restype = ctypes.c_int
+        lib.oracle_render_prepared.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                               ctypes.c_uint32, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int, vp]
+        lib.oracle_render_prepared.restype = ctypes.c_int
         lib.oracle_resolve_pass.argtypes = [ctypes.c_uint32, vp, vp, ctypes.c_uint64, ctypes.c_float, vp]
         lib.oracle_sobol_fingerprint.restype = ctypes.c_uint64
         lib.oracle_scene_create.restype = vp
@@ -86,6 +90,25 @@ class OracleFilm:
                                ctypes.cast(ctypes.byref(t), ctypes.c_void_p) if t is not None else None)
         if st != 0:
             raise RuntimeError("oracle_render failed")
+        return t
+
+    def render_prepared(self, scene: "OracleScene", first: int, count: int, total: int, row_stride: int = 1,
+                        threads: int = 0, trace: tuple[int, int, int] | None = None):
+        """render() over a scene prepared once (OracleScene), rendering only
+        the window rows whose index is a multiple of `row_stride`."""
+        lib = load()
+        t = None
+        tx = ty = ts = -1
+        if trace is not None:
+            from psycles_b200 import _abi
+            t = _abi.PathTrace()
+            tx, ty, ts = trace
+        st = lib.oracle_render_prepared(scene.handle, ctypes.cast(ctypes.byref(self.settings), ctypes.c_void_p),
+                                        first, count, total, row_stride, _p(self.combined), _p(self.normal),
+                                        _p(self.albedo), _p(self.count), threads, tx, ty, ts,
+                                        ctypes.cast(ctypes.byref(t), ctypes.c_void_p) if t is not None else None)
+        if st != 0:
+            raise RuntimeError("oracle_render_prepared failed")
         return t
 
     def resolve(self, kind: int) -> np.ndarray:

@@ -181,7 +181,9 @@ JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
 class SceneBuildStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in ("total_ms", "validate_ms", "blas_ms", "tlas_ms", "emitters_ms",
                                                "upload_ms", "light_tree_ms")] + [
-        ("build_threads", ctypes.c_uint32), ("light_tree_builds", ctypes.c_uint32)]
+        ("build_threads", ctypes.c_uint32), ("light_tree_builds", ctypes.c_uint32),
+        ("stack_need", ctypes.c_uint32), ("stack_capacity", ctypes.c_uint32), ("median_rebuilds", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32), ("upload_bytes", ctypes.c_uint64)]
 
 
 # Entry points declared by include/psycles_cuda.h: (name, restype, argtypes).

@@ -504,7 +504,17 @@ __device__ __forceinline__ void wide_slabs(const WideNodeRay &n, f3 oinv, f3 inv
     }
 }
 
-constexpr int kStackSize = 48;
+constexpr int kStackSize = int(kTraversalStackSize);
+
+// Pushes that found the traversal stack full.  Scene compile bounds every
+// tree's worst-case stack by kTraversalStackSize, so this stays 0; a
+// non-zero count fails the render instead of dropping subtrees silently.
+__device__ unsigned int g_stack_overflows;
+
+__device__ __forceinline__ void stack_push(uint32_t *stack, uint32_t &sp, uint32_t entry) {
+    if (sp < uint32_t(kStackSize)) stack[sp++] = entry;
+    else atomicAdd(&g_stack_overflows, 1u);
+}
 
 
 __device__ __forceinline__ float rcp_approx(float x) {
@@ -583,7 +593,7 @@ __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneVi
                 t.cur = make_slab_ray(xform_point(w2o, t.ray.o), xform_direction(w2o, t.ray.d));
                 t.inst = idx;
                 t.prim_offset = mesh.prim_offset;
-                if (t.sp < uint32_t(kStackSize)) t.stack[t.sp++] = kTagLeave;
+                stack_push(t.stack, t.sp, kTagLeave);
                 t.node = kTagBlas | mesh.node_offset;
                 continue;
             }
@@ -642,7 +652,7 @@ __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneVi
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 if (!(hit[k] && near[k] <= t.tmax && ct[k] == 0)) continue;
-                if (next != kInvalid && t.sp < uint32_t(kStackSize)) t.stack[t.sp++] = next;
+                if (next != kInvalid) stack_push(t.stack, t.sp, next);
                 next = lk[k];
             }
             if (next == kInvalid) {
@@ -684,7 +694,7 @@ __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneVi
             }
 #pragma unroll
             for (int k = 3; k >= 1; --k)
-                if (key[k] != kInf && t.sp < uint32_t(kStackSize)) t.stack[t.sp++] = val[k];
+                if (key[k] != kInf) stack_push(t.stack, t.sp, val[k]);
             t.node = val[0];
         }
     }

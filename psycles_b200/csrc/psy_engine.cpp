@@ -205,6 +205,9 @@ psy_status WavefrontEngine::run(const EnginePlan &plan, uint32_t steps, EngineRu
 psy_status WavefrontEngine::elapsed(float *ms, uint64_t *closest_rays, uint64_t *shadow_rays) {
     PSY_CUDA_TRY(cudaGetLastError());
     PSY_CUDA_TRY(cudaStreamSynchronize(context_->stream));
+    uint32_t overflows = 0u;
+    PSY_CUDA_TRY(take_stack_overflows(context_->stream, &overflows));
+    if (overflows != 0u) return fail(PSY_ERROR_UNSUPPORTED, "traversal stack overflow on the device");
     *ms = 0.0f;
     if (began_) PSY_CUDA_TRY(cudaEventElapsedTime(ms, ev_begin_, ev_end_));
     unsigned long long rays[2] = {0ull, 0ull};

@@ -323,6 +323,10 @@ struct Builder {
     uint32_t leaf_size = PSY_LEAF_SIZE;
     bool leaf_is_id = false;  // TLAS: leaf link = ~prim id, count 1
     bool parallel = true;     // large subtrees on threads of their own
+    // binary depth below which splits are chosen by SAH; deeper ranges split
+    // at the centroid median of the widest axis (0: median splits only, the
+    // balanced tree the traversal-stack check falls back to)
+    int sah_depth_limit = 60;
 
     struct Child {
         Box box;
@@ -372,7 +376,7 @@ struct Builder {
         uint32_t mid = begin + count / 2u;
         bool done = false;
         Box lbox, lcbox, rbox, rcbox;
-        if (depth < 60) {
+        if (depth < sah_depth_limit) {
             // one pass bins the centroids on every axis; the sweep then visits
             // only the boundaries right after non-empty bins (a boundary after
             // an empty bin costs the same as the one before it, and the first
@@ -666,6 +670,59 @@ struct Builder {
         return box;
     }
 };
+
+// Traversal-stack bound.  A visit of a wide node pushes every hit child it
+// does not descend into (inner nodes; instances in the TLAS) and continues
+// with one of them, so while a child's subtree is walked at most (n - 1) of
+// the node's n pushable children wait on the stack, whichever order the ray
+// takes.  Entering an instance pushes one more entry (the return to the
+// world ray) before the BLAS root.  The bounds below are therefore the
+// largest stack any ray can build, and the compile step keeps them within
+// the device stack (psy::kTraversalStackSize).
+
+// Pushable children (count-0 slots with a link) of a wide node.
+int wide_pushable(const psy::WideNodeGpu &w, uint32_t links[4]) {
+    const int *lk = &w.link.x;
+    const int *ct = &w.count.x;
+    int n = 0;
+    for (int k = 0; k < 4; ++k)
+        if (ct[k] == 0 && uint32_t(lk[k]) != psy::kInvalidId) links[n++] = uint32_t(lk[k]);
+    return n;
+}
+
+// Entries a BLAS walk adds above those waiting when its root is entered
+// (mesh-local node indices; a parent precedes its children).
+uint32_t blas_stack_need(const std::vector<psy::WideNodeGpu> &w) {
+    std::vector<uint32_t> need(w.size(), 0u);
+    for (size_t i = w.size(); i-- > 0;) {
+        uint32_t links[4];
+        const int n = wide_pushable(w[i], links);
+        uint32_t deepest = 0u;
+        for (int k = 0; k < n; ++k) deepest = std::max(deepest, need[links[k] & ~psy::kTagMask]);
+        need[i] = n > 0 ? uint32_t(n - 1) + deepest : 0u;
+    }
+    return w.empty() ? 0u : need[0];
+}
+
+// Entries waiting on the stack when each instance of the TLAS is entered
+// (0 for instances the TLAS does not reference).
+std::vector<uint32_t> tlas_instance_depths(const std::vector<psy::WideNodeGpu> &w, uint32_t instance_count) {
+    std::vector<uint32_t> depth(w.size(), 0u), inst(instance_count, 0u);
+    for (size_t i = 0; i < w.size(); ++i) {
+        uint32_t links[4];
+        const int n = wide_pushable(w[i], links);
+        for (int k = 0; k < n; ++k) {
+            const uint32_t below = depth[i] + uint32_t(n - 1);
+            const uint32_t idx = links[k] & ~psy::kTagMask;
+            if ((links[k] & psy::kTagMask) == psy::kTagInstance) {
+                if (idx < instance_count) inst[idx] = below;
+            } else if (idx < w.size()) {
+                depth[idx] = below;
+            }
+        }
+    }
+    return inst;
+}
 
 
 }  // namespace
@@ -1253,79 +1310,46 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     std::vector<uint64_t> mesh_tri_first(d->mesh_count + 1u, 0u);
     for (uint32_t i = 0; i < d->mesh_count; ++i) mesh_tri_first[i + 1u] = mesh_tri_first[i] + d->meshes[i].triangle_count;
     tris.resize(3u * mesh_tri_first[d->mesh_count]);
+    // one mesh's BLAS, its triangle records in leaf order and its stack need
+    std::vector<uint32_t> mesh_need(d->mesh_count, 0u);
+    auto build_mesh = [&](uint32_t i, int sah_depth_limit) {
+        const psy_mesh_desc &m = d->meshes[i];
+        Builder bld;
+        bld.sah_depth_limit = sah_depth_limit;
+        bld.prims.resize(m.triangle_count);
+        for (uint32_t k = 0; k < m.triangle_count; ++k) {
+            Prim &p = bld.prims[k];
+            for (int c = 0; c < 3; ++c) {
+                const float *v = m.positions + 3ull * m.indices[3ull * k + c];
+                p.box.grow(v[0], v[1], v[2]);
+            }
+            for (int a = 0; a < 3; ++a) p.c[a] = 0.5 * (p.box.lo[a] + p.box.hi[a]);
+            p.id = k;
+        }
+        mesh_boxes[i] = bld.build_root();
+        mesh_wide[i] = bld.widen();
+        mesh_need[i] = blas_stack_need(mesh_wide[i]);
+        float4 *out = tris.data() + 3u * mesh_tri_first[i];
+        for (const Prim &p : bld.prims) {
+            const uint32_t id = p.id;
+            for (int c = 0; c < 3; ++c) {
+                const float *v = m.positions + 3ull * m.indices[3ull * id + c];
+                float w = 0.0f;
+                if (c == 0) std::memcpy(&w, &id, 4);
+                *out++ = make_float4(v[0], v[1], v[2], w);
+            }
+        }
+    };
     {
         std::vector<uint32_t> by_size(d->mesh_count);
         for (uint32_t i = 0; i < d->mesh_count; ++i) by_size[i] = i;
         std::stable_sort(by_size.begin(), by_size.end(), [d](uint32_t a, uint32_t b) {
             return d->meshes[a].triangle_count > d->meshes[b].triangle_count;
         });
-        const psy_status built = parallel_for(d->mesh_count, &sc->stats.build_threads, [&](uint32_t job) {
-            const uint32_t i = by_size[job];
-            const psy_mesh_desc &m = d->meshes[i];
-            Builder bld;
-            bld.prims.resize(m.triangle_count);
-            for (uint32_t k = 0; k < m.triangle_count; ++k) {
-                Prim &p = bld.prims[k];
-                for (int c = 0; c < 3; ++c) {
-                    const float *v = m.positions + 3ull * m.indices[3ull * k + c];
-                    p.box.grow(v[0], v[1], v[2]);
-                }
-                for (int a = 0; a < 3; ++a) p.c[a] = 0.5 * (p.box.lo[a] + p.box.hi[a]);
-                p.id = k;
-            }
-            mesh_boxes[i] = bld.build_root();
-            mesh_wide[i] = bld.widen();
-            float4 *out = tris.data() + 3u * mesh_tri_first[i];
-            for (const Prim &p : bld.prims) {
-                const uint32_t id = p.id;
-                for (int c = 0; c < 3; ++c) {
-                    const float *v = m.positions + 3ull * m.indices[3ull * id + c];
-                    float w = 0.0f;
-                    if (c == 0) std::memcpy(&w, &id, 4);
-                    *out++ = make_float4(v[0], v[1], v[2], w);
-                }
-            }
-        });
+        const psy_status built = parallel_for(d->mesh_count, &sc->stats.build_threads,
+                                              [&](uint32_t job) { build_mesh(by_size[job], Builder{}.sah_depth_limit); });
         if (built != PSY_OK) return built;
     }
-    uint32_t prim_offset = 0;
-    for (uint32_t i = 0; i < d->mesh_count; ++i) {
-        const psy_mesh_desc &m = d->meshes[i];
-        psy::MeshGpu &g = meshes[i];
-        g.vertex_offset = uint32_t(positions.size() / 3u);
-        g.index_offset = uint32_t(indices.size());
-        g.triangle_count = m.triangle_count;
-        g.prim_offset = prim_offset;
-        g.smooth = m.smooth ? 1u : 0u;
-        prim_offset += m.triangle_count;
-        positions.insert(positions.end(), m.positions, m.positions + 3ull * m.vertex_count);
-        if (m.smooth) normals.insert(normals.end(), m.normals, m.normals + 3ull * m.vertex_count);
-        else normals.resize(positions.size(), 0.0f);
-        indices.insert(indices.end(), m.indices, m.indices + 3ull * m.triangle_count);
-        if (m.materials) {
-            g.material_offset = uint32_t(tri_materials.size());
-            tri_materials.insert(tri_materials.end(), m.materials, m.materials + m.triangle_count);
-        } else {
-            g.material_offset = psy::kInvalidId;
-        }
-        g.node_offset = uint32_t(blas.size());
-        g.tri_offset = uint32_t(mesh_tri_first[i]);
-        // global node and triangle indices of the mesh's links
-        for (psy::WideNodeGpu &w : mesh_wide[i]) {
-            int *lk = &w.link.x;
-            const int *ct = &w.count.x;
-            for (int k = 0; k < 4; ++k) {
-                const uint32_t v = uint32_t(lk[k]);
-                if (ct[k] > 0) lk[k] = int(v + g.tri_offset);
-                else if (v != psy::kInvalidId && (v & psy::kTagMask) == psy::kTagBlas)
-                    lk[k] = int(psy::kTagBlas | ((v & ~psy::kTagMask) + g.node_offset));
-            }
-        }
-        blas.insert(blas.end(), mesh_wide[i].begin(), mesh_wide[i].end());
-        std::vector<psy::WideNodeGpu>().swap(mesh_wide[i]);
-        sc->triangle_count += m.triangle_count;
-    }
-    if (blas.empty()) blas.push_back({});
     sc->stats.blas_ms = lap();
 
     // ---- instances + TLAS
@@ -1393,6 +1417,92 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     for (uint32_t i = 0; i < d->instance_count; ++i)
         sc->instance_mirrored[i] = dt(o2w[i].c0, crs(o2w[i].c1, o2w[i].c2)) < 0.0f ? 1u : 0u;
     sc->stats.tlas_ms = lap();
+
+    // ---- traversal-stack bound: every ray's stack must fit the device's
+    // kTraversalStackSize entries.  A tree that could exceed it is rebuilt
+    // with median splits only (balanced: about 3 entries per two binary
+    // levels); a scene that still exceeds it is rejected, so no traversal
+    // ever drops a subtree.
+    const uint32_t stack_cap = psy::kTraversalStackSize;
+    std::vector<psy::WideNodeGpu> tl_wide = tl.widen();
+    std::vector<uint32_t> inst_depth = tlas_instance_depths(tl_wide, d->instance_count);
+    auto tlas_depth = [&]() {
+        uint32_t deepest = 0u;
+        for (const Prim &p : tl.prims) deepest = std::max(deepest, inst_depth[p.id]);
+        return deepest;
+    };
+    if (!tl.prims.empty() && tlas_depth() + 1u > stack_cap / 2u) {
+        tl.sah_depth_limit = 0;
+        tl.build_root();
+        tl_wide = tl.widen();
+        inst_depth = tlas_instance_depths(tl_wide, d->instance_count);
+    }
+    auto mesh_budgets = [&]() {
+        std::vector<uint32_t> budget(d->mesh_count, stack_cap);
+        for (const Prim &p : tl.prims) {
+            const uint32_t mesh = d->instances[p.id].mesh;
+            const uint32_t used = inst_depth[p.id] + 1u;
+            budget[mesh] = std::min(budget[mesh], used >= stack_cap ? 0u : stack_cap - used);
+        }
+        return budget;
+    };
+    {
+        const std::vector<uint32_t> budget = mesh_budgets();
+        for (uint32_t i = 0; i < d->mesh_count; ++i) {
+            if (mesh_need[i] <= budget[i]) continue;
+            build_mesh(i, 0);
+            sc->stats.median_rebuilds += 1u;
+            if (mesh_need[i] > budget[i])
+                return fail(PSY_ERROR_UNSUPPORTED, "mesh " + std::to_string(i) + ": its BVH needs " +
+                                                       std::to_string(mesh_need[i]) + " traversal stack entries below " +
+                                                       "its instances, more than the " + std::to_string(budget[i]) +
+                                                       " left of " + std::to_string(stack_cap));
+        }
+        uint32_t need = 0u;
+        for (const Prim &p : tl.prims)
+            need = std::max(need, inst_depth[p.id] + 1u + mesh_need[d->instances[p.id].mesh]);
+        sc->stats.stack_need = need;
+        sc->stats.stack_capacity = stack_cap;
+    }
+
+    uint32_t prim_offset = 0;
+    for (uint32_t i = 0; i < d->mesh_count; ++i) {
+        const psy_mesh_desc &m = d->meshes[i];
+        psy::MeshGpu &g = meshes[i];
+        g.vertex_offset = uint32_t(positions.size() / 3u);
+        g.index_offset = uint32_t(indices.size());
+        g.triangle_count = m.triangle_count;
+        g.prim_offset = prim_offset;
+        g.smooth = m.smooth ? 1u : 0u;
+        prim_offset += m.triangle_count;
+        positions.insert(positions.end(), m.positions, m.positions + 3ull * m.vertex_count);
+        if (m.smooth) normals.insert(normals.end(), m.normals, m.normals + 3ull * m.vertex_count);
+        else normals.resize(positions.size(), 0.0f);
+        indices.insert(indices.end(), m.indices, m.indices + 3ull * m.triangle_count);
+        if (m.materials) {
+            g.material_offset = uint32_t(tri_materials.size());
+            tri_materials.insert(tri_materials.end(), m.materials, m.materials + m.triangle_count);
+        } else {
+            g.material_offset = psy::kInvalidId;
+        }
+        g.node_offset = uint32_t(blas.size());
+        g.tri_offset = uint32_t(mesh_tri_first[i]);
+        // global node and triangle indices of the mesh's links
+        for (psy::WideNodeGpu &w : mesh_wide[i]) {
+            int *lk = &w.link.x;
+            const int *ct = &w.count.x;
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t v = uint32_t(lk[k]);
+                if (ct[k] > 0) lk[k] = int(v + g.tri_offset);
+                else if (v != psy::kInvalidId && (v & psy::kTagMask) == psy::kTagBlas)
+                    lk[k] = int(psy::kTagBlas | ((v & ~psy::kTagMask) + g.node_offset));
+            }
+        }
+        blas.insert(blas.end(), mesh_wide[i].begin(), mesh_wide[i].end());
+        std::vector<psy::WideNodeGpu>().swap(mesh_wide[i]);
+        sc->triangle_count += m.triangle_count;
+    }
+    if (blas.empty()) blas.push_back({});
 
     // ---- materials and parameter blocks
     std::vector<psy_closure_instruction> code;
@@ -1553,7 +1663,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
                             &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights, &sc->lamp_consts,
                             &sc->lamp_bounds, &sc->lamp_ids})
         b->ordered = st;
-    PSY_CUDA_TRY(sc->tlas.upload(tl.widen(), st));
+    PSY_CUDA_TRY(sc->tlas.upload(tl_wide, st));
     PSY_CUDA_TRY(sc->blas.upload(blas, st));
     PSY_CUDA_TRY(sc->tris.upload(tris, st));
     PSY_CUDA_TRY(sc->instances.upload(instances, st));
@@ -1599,6 +1709,12 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->lamp_bounds.upload(lamp_bounds, st));
     PSY_CUDA_TRY(sc->lamp_ids.upload(lamp_ids, st));
     PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    sc->stats.upload_bytes = 0u;
+    for (const DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tris, &sc->instances, &sc->meshes, &sc->positions,
+                                  &sc->normals, &sc->indices, &sc->tri_materials, &sc->material_buf, &sc->code,
+                                  &sc->scalar_buf, &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights,
+                                  &sc->lamp_consts, &sc->lamp_bounds, &sc->lamp_ids})
+        sc->stats.upload_bytes += b->bytes;
     psy::SceneView &v = sc->view;
     v.tlas = sc->tlas.as<psy::WideNodeGpu>();
     v.blas = sc->blas.as<psy::WideNodeGpu>();
@@ -1964,6 +2080,9 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
     PSY_CUDA_TRY(cudaEventRecord(s->ev_end, st));
     PSY_CUDA_TRY(cudaGetLastError());
     PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    uint32_t overflows = 0u;
+    PSY_CUDA_TRY(psy::take_stack_overflows(st, &overflows));
+    if (overflows != 0u) return fail(PSY_ERROR_UNSUPPORTED, "traversal stack overflow on the device");
     float ms = 0.0f;
     PSY_CUDA_TRY(cudaEventElapsedTime(&ms, s->ev_begin, s->ev_end));
     unsigned long long counts[2] = {0, 0};
@@ -1984,8 +2103,11 @@ psy_status psy_session_render_samples(psy_session *s, uint32_t first, uint32_t c
 // render time.  Same kernels and sample order as psy_session_render_samples;
 // the wavefront state and the Sobol table come from static device arrays
 // (psy_static.cu).  The first call on a device takes the arrays' addresses
-// and fills the table; make that first call before any stream capture.
-// Calls share the arrays: overlapping calls on the GPU race.
+// and fills the table (ordered on the context stream and synchronised before
+// the device counts as set up); make that first call before any stream
+// capture.  Calls on one context are serialised by the context's render
+// lock; calls on different contexts of one device share the arrays and race
+// when they overlap on the GPU.
 psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uint32_t count, uint32_t offset,
                                              uint32_t total) {
     if (!s) return fail(PSY_ERROR_INVALID_ARGUMENT, "null session");
@@ -1999,20 +2121,12 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
     if (s->pixels > psy::kStaticMaxPaths)
         return fail(PSY_ERROR_RANGE, "the static render supports windows of at most 65536 pixels");
     psy_context *ctx = s->scene->context;
+    std::lock_guard<std::mutex> render_lock(ctx->render_mutex);
     cudaStream_t st = ctx->stream;
     PSY_CUDA_TRY(cudaSetDevice(ctx->device));
     void *base = nullptr;
     float4 *sobol = nullptr;
-    bool first_use = false;
-    PSY_CUDA_TRY(psy::static_scratch(ctx->device, &base, &sobol, &first_use));
-    if (first_use) {
-        float pattern[psy::kStaticSobolSize * 4u];  // one 4 KiB pattern at a time, no heap
-        for (uint32_t k = 0; k < 256u; ++k) {
-            sobol_pattern(pattern, psy::kStaticSobolSize, k);
-            PSY_CUDA_TRY(cudaMemcpy(sobol + size_t(k) * psy::kStaticSobolSize, pattern, sizeof(pattern),
-                                    cudaMemcpyHostToDevice));
-        }
-    }
+    PSY_CUDA_TRY(psy::static_scratch(ctx->device, st, sobol_pattern, &base, &sobol));
     // carve the static bytes into the wavefront arrays
     unsigned char *cursor = static_cast<unsigned char *>(base);
     auto carve = [&](size_t bytes) {
@@ -2086,6 +2200,9 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
     PSY_CUDA_TRY(cudaEventRecord(s->ev_end, st));
     PSY_CUDA_TRY(cudaGetLastError());
     PSY_CUDA_TRY(cudaStreamSynchronize(st));
+    uint32_t overflows = 0u;
+    PSY_CUDA_TRY(psy::take_stack_overflows(st, &overflows));
+    if (overflows != 0u) return fail(PSY_ERROR_UNSUPPORTED, "traversal stack overflow on the device");
     float ms = 0.0f;
     PSY_CUDA_TRY(cudaEventElapsedTime(&ms, s->ev_begin, s->ev_end));
     unsigned long long counts[2] = {0, 0};

@@ -1495,4 +1495,17 @@ void launch_debug_sobol(cudaStream_t st, const float4 *table, uint32_t size, con
     k_debug_sobol<<<(count + 127u) / 128u, 128, 0, st>>>(table, size, queries, count, out, out_index);
 }
 
+cudaError_t take_stack_overflows(cudaStream_t st, uint32_t *count) {
+    unsigned int v = 0u;
+    cudaError_t e = cudaMemcpyFromSymbolAsync(&v, g_stack_overflows, sizeof(v), 0, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && v != 0u) {
+        const unsigned int zero = 0u;
+        e = cudaMemcpyToSymbolAsync(g_stack_overflows, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    *count = v;
+    return e;
+}
+
 }  // namespace psy

@@ -55,5 +55,8 @@ void launch_debug_light_tree(cudaStream_t st, const SceneView &s, const float4 *
                              uint32_t count, uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf);
 void launch_debug_sobol(cudaStream_t st, const float4 *table, uint32_t size, const uint32_t *queries, uint32_t count,
                         float4 *out, uint32_t *out_index);
+// Reads (after synchronising `st`) and clears the device's count of
+// traversal pushes that found the stack full.
+cudaError_t take_stack_overflows(cudaStream_t st, uint32_t *count);
 
 }  // namespace psy

@@ -21,9 +21,16 @@ constexpr uint32_t kStaticSobolSize = 256u;
 constexpr size_t kStaticSobolRows = size_t(kStaticSobolSize) * 256u;
 constexpr int kStaticMaxDevices = 64;
 
-// Device addresses of the static arrays on `device` (taken with that device
-// current on first use and cached).  `first_use` reports whether this call
-// did the set-up.
-cudaError_t static_scratch(int device, void **paths, float4 **sobol, bool *first_use);
+// Writes the `size` 4-D points of Sobol pattern `pattern` (4 floats each).
+using StaticSobolFill = void (*)(float *points, uint32_t size, uint32_t pattern);
+
+// Device addresses of the static arrays on `device`.  The first call for a
+// device, with the set-up lock held, makes `device` current, takes the
+// arrays' addresses with cudaGetSymbolAddress, writes the 256 Sobol patterns
+// into the static table through `fill` (copies ordered on `stream`, then a
+// synchronisation of `stream`), and only then marks the device ready; a
+// failing step leaves it not ready, so the next call repeats the set-up.
+// Later calls return the cached addresses.
+cudaError_t static_scratch(int device, cudaStream_t stream, StaticSobolFill fill, void **paths, float4 **sobol);
 
 }  // namespace psy

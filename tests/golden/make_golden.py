@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes
 import json
+import os
 import pathlib
 import re
 import sys
@@ -157,7 +158,7 @@ def reference_tables() -> dict:
 
 
 def main() -> None:
-    ref = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PSYCLES_REFERENCE", "/root/reference"))
     data = {
         "source": "Psycles reference tests read as text; tables from its sampling sources",
         "sobol": sobol_fixtures(ref),
