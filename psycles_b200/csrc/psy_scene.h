@@ -49,8 +49,9 @@ constexpr uint32_t kTagTlas = 0u, kTagBlas = 1u << 30, kTagInstance = 2u << 30, 
 constexpr uint32_t kTagMask = 3u << 30;
 // Entries of the per-ray traversal stack.  Scene compile proves, from the
 // built trees, that no ray can push more (see blas_stack_need /
-// tlas_instance_depths in psy_host.cpp); the device still counts a push
-// that would not fit (g_stack_overflows) and the render reports it.
+// tlas_instance_depths in psy_host.cpp), rebuilding a mesh with median
+// splits or rejecting the scene where needed; a debug build
+// (-DPSY_STACK_CHECK=1) also counts pushes that would not fit on the device.
 constexpr uint32_t kTraversalStackSize = 48u;
 
 // Four children of a wide BVH node: boxes as six planes of four lanes, and

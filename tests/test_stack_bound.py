@@ -85,4 +85,5 @@ def test_regular_scene_needs_no_rebuild(backend):
     stats = compiled.scene.build_stats()
     assert stats.median_rebuilds == 0
     assert 0 < stats.stack_need <= stats.stack_capacity
-    assert stats.upload_bytes > 100_000_000  # BVH, triangle records, meshes and instances of ~1M triangles
+    # BVH nodes, triangle records, vertices and indices of the 124,740 triangles of the eight meshes
+    assert stats.upload_bytes > 20_000_000
