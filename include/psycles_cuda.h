@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PSY_ABI_VERSION 1u
+#define PSY_ABI_VERSION 2u
 
 typedef enum psy_status {
     PSY_OK = 0,
@@ -95,16 +95,87 @@ typedef enum psy_closure_op {
     PSY_CLOSURE_MIX = 5
 } psy_closure_op;
 
-/* One closure instruction.  `color` names a vector slot and `scalar` a
- * scalar slot of the material's parameter block (emission strength, mix
- * factor); `a`/`b` are child instruction indices for add and mix. */
+/* Closure inputs.  A closure input (colour, strength / factor, roughness)
+ * is either a slot of the material's parameter block that belongs to the
+ * closure node itself -- an unlinked socket, the literal
+ * estimate_surface_emission reads (src/compiler/surface_program.cpp:180-186)
+ * -- or, with PSY_INPUT_VALUE set, the index of an instruction of the
+ * material's value stream (a ValueExpressionId: a linked socket).
+ * PSY_INPUT_NONE marks an absent optional input (roughness 0). */
+#define PSY_INPUT_VALUE 0x80000000u
+#define PSY_INPUT_NONE 0xffffffffu
+
+/* One closure instruction (compiler::ClosureInstruction,
+ * include/psycles/compiler/surface_program.h:415-470, in-scope fields):
+ * `color` (vector input: diffuse / transparent / emission colour),
+ * `scalar` (emission strength, mix factor), `roughness` (diffuse
+ * roughness: Lambert below 1e-5, else Oren-Nayar), `a`/`b` child
+ * instruction indices of add and mix. */
 typedef struct psy_closure_instruction {
     uint32_t op;
     uint32_t a;
     uint32_t b;
     uint32_t color;
     uint32_t scalar;
+    uint32_t roughness;
 } psy_closure_instruction;
+
+/* Value operations of the in-scope subset, numbered as
+ * compiler::ValueOperation (include/psycles/compiler/surface_program.h:51);
+ * semantics of src/luisa/graph_surface_value_math.cpp,
+ * graph_surface_value_context.cpp and graph_surface_value_procedural.cpp. */
+#define PSY_VALUE_PARAMETER 0u          /* the block's `parameter` slot (scalar or vector block by type) */
+#define PSY_VALUE_PASSTHROUGH 1u        /* a */
+#define PSY_VALUE_SCALAR_TO_COLOR 2u    /* (a, a, a) */
+#define PSY_VALUE_SCALAR_TO_BOOLEAN 3u  /* int(a) != 0 */
+#define PSY_VALUE_COLOR_TO_SCALAR 4u    /* dot(a, Film::rgb_to_y) */
+#define PSY_VALUE_VECTOR_TO_SCALAR 5u   /* (a.x + a.y + a.z) / 3 */
+#define PSY_VALUE_ADD 6u
+#define PSY_VALUE_SUBTRACT 7u
+#define PSY_VALUE_MULTIPLY 8u
+#define PSY_VALUE_DIVIDE 9u             /* 0 where |b| <= 1e-20 */
+#define PSY_VALUE_MINIMUM 10u
+#define PSY_VALUE_MAXIMUM 11u
+#define PSY_VALUE_POWER 12u             /* pow(max(a, 0), b) */
+#define PSY_VALUE_ABSOLUTE 14u
+#define PSY_VALUE_CLAMP01 15u
+#define PSY_VALUE_CLAMP_RANGE 16u       /* clamp(a, b, c); static_u0 1: swap reversed bounds */
+#define PSY_VALUE_MIX_FLOAT 21u         /* lerp(a, b, c); static_u0: clamp c */
+#define PSY_VALUE_MIX_VECTOR 22u        /* lerp(a, b, t); static_u0: vector t, static_u1: clamp t */
+#define PSY_VALUE_MIX 23u               /* colour blend static_u0 (PSY_BLEND_*), static_u1 bit 0: clamp c */
+#define PSY_VALUE_MULTIPLY_COLOR 24u    /* lerp(a, a * b, clamp(c, 0, 1)) */
+#define PSY_VALUE_INVERT 26u            /* lerp(a, 1 - a, b) */
+#define PSY_VALUE_SEPARATE_R 100u       /* static_u0 0 (RGB) only */
+#define PSY_VALUE_SEPARATE_G 101u
+#define PSY_VALUE_SEPARATE_B 102u
+#define PSY_VALUE_COMBINE_COLOR 103u    /* (a, b, c); static_u0 0 (RGB) only */
+
+/* compiler::BlendOperation (surface_program.h:239) of PSY_VALUE_MIX. */
+#define PSY_BLEND_MIX 0u
+#define PSY_BLEND_DARKEN 1u
+#define PSY_BLEND_MULTIPLY 2u
+#define PSY_BLEND_LIGHTEN 4u
+#define PSY_BLEND_SCREEN 5u
+#define PSY_BLEND_ADD 7u
+#define PSY_BLEND_DIFFERENCE 11u
+#define PSY_BLEND_SUBTRACT 13u
+
+#define PSY_VALUE_TYPE_SCALAR 0u
+#define PSY_VALUE_TYPE_VECTOR 1u
+
+/* One value instruction (compiler::ValueInstruction, surface_program.h:359):
+ * operands a, b, c name earlier instructions of the same stream, which is
+ * topologically ordered. */
+typedef struct psy_value_instruction {
+    uint32_t op;                 /* PSY_VALUE_* */
+    uint32_t type;               /* PSY_VALUE_TYPE_* of the result */
+    uint32_t parameter;          /* PSY_VALUE_PARAMETER: block slot */
+    uint32_t a;
+    uint32_t b;
+    uint32_t c;
+    uint32_t static_u0;
+    uint32_t static_u1;
+} psy_value_instruction;
 
 /* contract::EmissionSampling (include/psycles/contract/scene.h:69). */
 #define PSY_EMISSION_SAMPLING_NONE 0u
@@ -113,9 +184,11 @@ typedef struct psy_closure_instruction {
 #define PSY_EMISSION_SAMPLING_BACK 3u
 #define PSY_EMISSION_SAMPLING_FRONT_BACK 4u
 
-/* A compiled SurfaceProgram (closure tree) with its SurfaceParameterBlock
- * (compiler::SurfaceProgram surface_program.h:512, SurfaceParameterBlock
- * surface_program.h:570). */
+/* A compiled SurfaceProgram (value stream + closure tree) with its
+ * SurfaceParameterBlock (compiler::SurfaceProgram surface_program.h:512,
+ * SurfaceParameterBlock surface_program.h:570).  The block is split into
+ * scalar and vector slots; a program compiled by the reference gives each
+ * ParameterDesc the same index in both. */
 typedef struct psy_material_desc {
     const psy_closure_instruction *closures;
     uint32_t closure_count;
@@ -125,7 +198,8 @@ typedef struct psy_material_desc {
     uint32_t vector_count;
     const float *vectors;        /* vector_count * 3 floats */
     uint32_t emission_sampling;  /* PSY_EMISSION_SAMPLING_* */
-    uint32_t reserved;
+    uint32_t value_count;        /* at most 64 */
+    const psy_value_instruction *values;
 } psy_material_desc;
 
 /* contract::LightType order (include/psycles/contract/scene.h:369). */

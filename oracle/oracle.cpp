@@ -46,6 +46,7 @@ struct Instance {
 
 struct Material {
     std::vector<psy_closure_instruction> code;
+    std::vector<psy_value_instruction> values;
     uint32_t root{0};
     std::vector<float> scalars;
     std::vector<float3> vectors;
@@ -158,12 +159,118 @@ static void build_mesh_bvh(Mesh &m) {
 
 // ------------------------------------------------------ closure programs
 
+// The value stream (GraphSurfaceImplementation::trace_value_stage,
+// src/luisa/graph_surface_values.cpp:70-100): instructions 0..id in order,
+// scalars held in x.  Operations as src/luisa/graph_surface_value_math.cpp:
+// 54-880 (parameter, conversions, float math, mixes, colour blends),
+// graph_surface_value_context.cpp:80-108 (multiply_color, invert) and
+// graph_surface_value_procedural.cpp:568-600 (separate / combine RGB).
+// cast<int>(x) of scalar_to_boolean truncates toward zero, NaN giving 0.
+static bool truncates_nonzero(float x) {
+    if (std::isnan(x)) return false;
+    return std::trunc(x) != 0.0f;
+}
+static float3 lerp3(float3 a, float3 b, float3 t) {
+    return f3(lerp(a.x, b.x, t.x), lerp(a.y, b.y, t.y), lerp(a.z, b.z, t.z));
+}
+static float3 eval_value(const Material &mat, uint32_t id) {
+    std::vector<float3> v;
+    const uint32_t n = std::min<uint32_t>(id + 1u, uint32_t(mat.values.size()));
+    v.reserve(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const psy_value_instruction &in = mat.values[i];
+        const float3 a = in.a < i ? v[in.a] : f3(0.0f);
+        const float3 b = in.b < i ? v[in.b] : f3(0.0f);
+        const float3 c = in.c < i ? v[in.c] : f3(0.0f);
+        auto clamp01 = [](float x) { return std::fmin(std::fmax(x, 0.0f), 1.0f); };
+        float3 r = f3(0.0f);
+        switch (in.op) {
+        case PSY_VALUE_PARAMETER:
+            r = in.type == PSY_VALUE_TYPE_SCALAR ? f3(mat.scalars[in.parameter], 0.0f, 0.0f) : mat.vectors[in.parameter];
+            break;
+        case PSY_VALUE_PASSTHROUGH: r = a; break;
+        case PSY_VALUE_SCALAR_TO_COLOR: r = f3(a.x); break;
+        case PSY_VALUE_SCALAR_TO_BOOLEAN: r.x = truncates_nonzero(a.x) ? 1.0f : 0.0f; break;
+        case PSY_VALUE_COLOR_TO_SCALAR: r.x = a.x * 0.21267404f + a.y * 0.7151516f + a.z * 0.07217542f; break;
+        case PSY_VALUE_VECTOR_TO_SCALAR: r.x = (a.x + a.y + a.z) / 3.0f; break;
+        case PSY_VALUE_ADD: r.x = a.x + b.x; break;
+        case PSY_VALUE_SUBTRACT: r.x = a.x - b.x; break;
+        case PSY_VALUE_MULTIPLY: r.x = a.x * b.x; break;
+        case PSY_VALUE_DIVIDE: r.x = std::fabs(b.x) > 1.0e-20f ? a.x / b.x : 0.0f; break;
+        case PSY_VALUE_MINIMUM: r.x = std::fmin(a.x, b.x); break;
+        case PSY_VALUE_MAXIMUM: r.x = std::fmax(a.x, b.x); break;
+        case PSY_VALUE_POWER: r.x = pow_(std::fmax(a.x, 0.0f), b.x); break;
+        case PSY_VALUE_ABSOLUTE: r.x = std::fabs(a.x); break;
+        case PSY_VALUE_CLAMP01: r.x = clamp01(a.x); break;
+        case PSY_VALUE_CLAMP_RANGE: {
+            float lo = b.x, hi = c.x;
+            if (in.static_u0 == 1u && lo > hi) std::swap(lo, hi);
+            r.x = std::fmin(std::fmax(a.x, lo), hi);
+            break;
+        }
+        case PSY_VALUE_MIX_FLOAT: r.x = lerp(a.x, b.x, in.static_u0 != 0u ? clamp01(c.x) : c.x); break;
+        case PSY_VALUE_MIX_VECTOR: {
+            float3 t = in.static_u0 != 0u ? c : f3(c.x);
+            if (in.static_u1 != 0u) t = f3(clamp01(t.x), clamp01(t.y), clamp01(t.z));
+            r = lerp3(a, b, t);
+            break;
+        }
+        case PSY_VALUE_MIX: {
+            const float t = (in.static_u1 & 1u) != 0u ? clamp01(c.x) : c.x;
+            const float3 tt = f3(t);
+            switch (in.static_u0) {
+            case PSY_BLEND_DARKEN: r = lerp3(a, f3(std::fmin(a.x, b.x), std::fmin(a.y, b.y), std::fmin(a.z, b.z)), tt); break;
+            case PSY_BLEND_MULTIPLY: r = lerp3(a, a * b, tt); break;
+            case PSY_BLEND_LIGHTEN: r = lerp3(a, f3(std::fmax(a.x, b.x), std::fmax(a.y, b.y), std::fmax(a.z, b.z)), tt); break;
+            case PSY_BLEND_SCREEN: {
+                const float k = 1.0f - t;
+                r = f3(1.0f - (k + t * (1.0f - b.x)) * (1.0f - a.x), 1.0f - (k + t * (1.0f - b.y)) * (1.0f - a.y),
+                       1.0f - (k + t * (1.0f - b.z)) * (1.0f - a.z));
+                break;
+            }
+            case PSY_BLEND_ADD: r = lerp3(a, a + b, tt); break;
+            case PSY_BLEND_DIFFERENCE:
+                r = lerp3(a, f3(std::fabs(a.x - b.x), std::fabs(a.y - b.y), std::fabs(a.z - b.z)), tt);
+                break;
+            case PSY_BLEND_SUBTRACT: r = lerp3(a, a - b, tt); break;
+            default: r = lerp3(a, b, tt); break;
+            }
+            break;
+        }
+        case PSY_VALUE_MULTIPLY_COLOR: r = lerp3(a, a * b, f3(clamp01(c.x))); break;
+        case PSY_VALUE_INVERT: r = lerp3(a, f3(1.0f) - a, f3(b.x)); break;
+        case PSY_VALUE_SEPARATE_R: r.x = a.x; break;
+        case PSY_VALUE_SEPARATE_G: r.x = a.y; break;
+        case PSY_VALUE_SEPARATE_B: r.x = a.z; break;
+        case PSY_VALUE_COMBINE_COLOR: r = f3(a.x, b.x, c.x); break;
+        default: break;
+        }
+        v.push_back(r);
+    }
+    return n > id ? v[id] : f3(0.0f);
+}
+
+// A closure input: the closure node's own parameter slot (an unlinked
+// socket), or a value of the stream (PSY_INPUT_VALUE: a linked socket).
+static float3 input_vector(const Material &mat, uint32_t ref) {
+    if ((ref & PSY_INPUT_VALUE) == 0u) return mat.vectors[ref];
+    return eval_value(mat, ref & ~PSY_INPUT_VALUE);
+}
+static float input_scalar(const Material &mat, uint32_t ref) {
+    if (ref == PSY_INPUT_NONE) return 0.0f;
+    if ((ref & PSY_INPUT_VALUE) == 0u) return mat.scalars[ref];
+    return eval_value(mat, ref & ~PSY_INPUT_VALUE).x;
+}
+
 // compiler::ClosureOperation walk of GraphSurfaceImplementation::
 // for_each_closure (src/luisa/graph_surface_closures.cpp:5-356): add visits
-// both children with the same weight, mix splits clamp(fac, 0, 1).
+// both children with the same weight, mix splits clamp(fac, 0, 1).  A
+// diffuse leaf keeps its authored colour and roughness.
 struct TracedClosure {
     uint32_t op;
     float3 weight;
+    float3 color;
+    float roughness;
 };
 
 static void walk_closures(const Material &mat, uint32_t id, float mix_weight, std::vector<TracedClosure> &out,
@@ -176,18 +283,23 @@ static void walk_closures(const Material &mat, uint32_t id, float mix_weight, st
         walk_closures(mat, c.b, mix_weight, out, depth + 1);
         return;
     case PSY_CLOSURE_MIX: {
-        const float factor = clampf(mat.scalars[c.scalar], 0.0f, 1.0f);
+        const float factor = clampf(input_scalar(mat, c.scalar), 0.0f, 1.0f);
         walk_closures(mat, c.a, mix_weight * (1.0f - factor), out, depth + 1);
         walk_closures(mat, c.b, mix_weight * factor, out, depth + 1);
         return;
     }
     case PSY_CLOSURE_DIFFUSE:
-    case PSY_CLOSURE_TRANSPARENT:
-        out.push_back({c.op, mat.vectors[c.color] * mix_weight});
+    case PSY_CLOSURE_TRANSPARENT: {
+        const float3 color = input_vector(mat, c.color);
+        const float roughness = c.op == PSY_CLOSURE_DIFFUSE ? input_scalar(mat, c.roughness) : 0.0f;
+        out.push_back({c.op, color * mix_weight, color, roughness});
         return;
-    case PSY_CLOSURE_EMISSION:
-        out.push_back({c.op, mat.vectors[c.color] * mat.scalars[c.scalar] * mix_weight});
+    }
+    case PSY_CLOSURE_EMISSION: {
+        const float3 color = input_vector(mat, c.color) * input_scalar(mat, c.scalar);
+        out.push_back({c.op, color * mix_weight, color, 0.0f});
         return;
+    }
     default:
         return;
     }
@@ -211,6 +323,8 @@ struct PhysicalClosure {
     float3 weight;
     float sample_weight;
     float3 normal;
+    float3 color;     // authored colour (Oren-Nayar albedo)
+    float roughness;  // diffuse roughness (Lambert below 1e-5)
 };
 
 struct SurfaceClosures {
@@ -235,6 +349,8 @@ static SurfaceClosures collect_surface(const Material &mat, float3 shading_norma
         if (s.count >= kMaxClosures) continue;
         PhysicalClosure p;
         p.op = t.op;
+        p.color = t.color;
+        p.roughness = t.roughness;
         if (t.op == PSY_CLOSURE_DIFFUSE) {
             p.weight = bsdf_allocated_weight(t.weight);
             p.sample_weight = closure_sample_weight(p.weight);
@@ -309,8 +425,47 @@ struct Evaluation {
 // and SurfaceClosureEvaluationAccumulator::finish :410-438).  `selected`
 // marks the closure that produced the direction (its pdf survives a zero
 // bump term).
-static Evaluation evaluate_mixture(const SurfaceClosures &s, float3 shading_normal, float3 outgoing_raw,
-                                   uint32_t lobe_mask, int selected) {
+// oren_nayar_g (src/luisa/graph_surface_scattering.cpp:463-473).
+static float oren_nayar_g(float cosine) {
+    const float c = clampf(cosine, 0.0f, 1.0f);
+    const float sine = std::sqrt(maxf(1.0f - c * c, 0.0f));
+    const float theta = acos_(c);
+    const float safe_cosine = maxf(c, 1.0e-6f);
+    const float regular = sine * (theta - 2.0f / 3.0f - sine * c) +
+                          2.0f / 3.0f * (sine / safe_cosine) * (1.0f - sine * sine * sine);
+    const float taylor = (kPi * 0.5f - 2.0f / 3.0f) - c;
+    return c < 1.0e-6f ? taylor : regular;
+}
+
+// diffuse_intensity (src/luisa/graph_surface_scattering.cpp:475-506): Lambert
+// below roughness 1e-5, else Cycles' energy-compensated Oren-Nayar (single
+// scattering a + b t plus the multiple-scattering term of the clamped
+// albedo).  `incoming` points to the viewer, `outgoing` to the light.
+static float3 diffuse_intensity(const PhysicalClosure &c, float3 incoming, float3 outgoing) {
+    const float nl = maxf(dot(c.normal, outgoing), 0.0f);
+    const float sigma = clampf(c.roughness, 0.0f, 1.0f);
+    if (sigma < 1.0e-5f) return f3(nl * kInvPi);
+    const float a = 1.0f / (kPi + sigma * (kPi * 0.5f - 2.0f / 3.0f));
+    const float b = sigma * a;
+    const float nv = maxf(dot(c.normal, incoming), 0.0f);
+    float t = dot(outgoing, incoming) - nl * nv;
+    if (t > 0.0f) t = t / (maxf(nl, nv) + 1.17549435e-38f);
+    const float single_scatter = a + b * t;
+    const float3 albedo = clamp3(c.color, 0.0f, 1.0f);
+    const float e_average = a * kPi + ((2.0f * kPi - 5.6f) / 3.0f) * b;
+    const float ratio = e_average / (1.0f - e_average);
+    const float keep = 1.0f - e_average;
+    const float3 e_ms = f3(kInvPi * (albedo.x * albedo.x) * ratio / (1.0f - albedo.x * keep),
+                           kInvPi * (albedo.y * albedo.y) * ratio / (1.0f - albedo.y * keep),
+                           kInvPi * (albedo.z * albedo.z) * ratio / (1.0f - albedo.z * keep));
+    const float e_incoming = a * kPi + b * oren_nayar_g(nv);
+    const float3 multiscatter = e_ms * (1.0f - e_incoming);
+    const float e_outgoing = a * kPi + b * oren_nayar_g(nl);
+    return (f3(single_scatter) + multiscatter * (1.0f - e_outgoing)) * nl;
+}
+
+static Evaluation evaluate_mixture(const SurfaceClosures &s, float3 shading_normal, float3 incoming,
+                                   float3 outgoing_raw, uint32_t lobe_mask, int selected) {
     const float3 outgoing = safe_normalize(outgoing_raw, shading_normal);
     Evaluation e;
     float total = 0.0f, weighted_pdf = 0.0f;
@@ -327,8 +482,7 @@ static Evaluation evaluate_mixture(const SurfaceClosures &s, float3 shading_norm
         float pdf = maxf(dot(c.normal, outgoing), 0.0f) * kInvPi;
         if (!pdf_valid) pdf = 0.0f;
         if (!diffuse_enabled) continue;  // any_allowed false: no weight, no pdf
-        const float nl = maxf(dot(c.normal, outgoing), 0.0f);
-        const float3 value = c.weight * (nl * kInvPi) * bump;
+        const float3 value = c.weight * diffuse_intensity(c, incoming, outgoing) * bump;
         e.f += value;
         e.diffuse_f += value;
         total += c.sample_weight;
@@ -385,7 +539,7 @@ static SurfaceSample sample_surface(const SurfaceClosures &s, float3 shading_nor
     out.closure_index = uint32_t(chosen);
     out.wi = direction;
     if (!sample_valid) return out;
-    Evaluation mixture = evaluate_mixture(s, shading_normal, direction, lobe_mask, chosen);
+    Evaluation mixture = evaluate_mixture(s, shading_normal, incoming, direction, lobe_mask, chosen);
     Evaluation r;
     r.f = mixture.f;
     r.diffuse_f = mixture.diffuse_f;
@@ -449,15 +603,26 @@ static float3 material_emission(const Material &mat) {
 // bottom-up over the instructions; emission colour x strength, add a + b,
 // mix a (1 - f) + b f with the factor as authored; a forward or missing
 // operand counts as one.
+// Only an unlinked socket of the closure node itself is a literal
+// (direct_parameter_value, surface_program.cpp:170-186): a linked colour or
+// strength counts as one, and a mix with a linked factor sums its branches.
 static float3 emission_estimate(const Material &mat) {
     std::vector<float3> e;
+    auto literal = [](uint32_t ref) { return (ref & PSY_INPUT_VALUE) == 0u; };
     for (const psy_closure_instruction &c : mat.code) {
         auto operand = [&](uint32_t id) { return id < e.size() ? e[id] : f3(1.0f); };
         float3 v = f3(0.0f);
-        if (c.op == PSY_CLOSURE_EMISSION) v = mat.vectors[c.color] * mat.scalars[c.scalar];
-        else if (c.op == PSY_CLOSURE_ADD) v = operand(c.a) + operand(c.b);
-        else if (c.op == PSY_CLOSURE_MIX)
-            v = operand(c.a) * (1.0f - mat.scalars[c.scalar]) + operand(c.b) * mat.scalars[c.scalar];
+        if (c.op == PSY_CLOSURE_EMISSION) {
+            const float strength = literal(c.scalar) ? mat.scalars[c.scalar] : 1.0f;
+            v = (literal(c.color) ? mat.vectors[c.color] : f3(1.0f)) * strength;
+        } else if (c.op == PSY_CLOSURE_ADD) {
+            v = operand(c.a) + operand(c.b);
+        } else if (c.op == PSY_CLOSURE_MIX) {
+            if (literal(c.scalar))
+                v = operand(c.a) * (1.0f - mat.scalars[c.scalar]) + operand(c.b) * mat.scalars[c.scalar];
+            else
+                v = operand(c.a) + operand(c.b);
+        }
         e.push_back(v);
     }
     return mat.root < e.size() ? e[mat.root] : f3(0.0f);
@@ -1752,7 +1917,7 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
                     const bool reject_self = same_primitive && dot(ls.direction, oriented) > 0.0f;
                     if (!reject_self) {
                         const float3 light_radiance = material_emission(s.materials[em.material]);
-                        const Evaluation e = evaluate_mixture(closures, sp.n, ls.direction, lobe_mask, -1);
+                        const Evaluation e = evaluate_mixture(closures, sp.n, -ray.d, ls.direction, lobe_mask, -1);
                         float mis = 1.0f;
                         mis = nee_light_weight(mode, pdf, e.pdf);
                         const float3 weighted = e.f * light_radiance * (mis / pdf);
@@ -1785,7 +1950,7 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
                     const float light_pdf = a.pdf * selected.selection_pdf;
                     if (a.valid && light_pdf > 0.0f) {
                         const float3 light_radiance = f3(l.color[0], l.color[1], l.color[2]) * (l.power * a.eval_factor);
-                        const Evaluation e = evaluate_mixture(closures, sp.n, a.direction, lobe_mask, -1);
+                        const Evaluation e = evaluate_mixture(closures, sp.n, -ray.d, a.direction, lobe_mask, -1);
                         // MIS only for lamps a BSDF ray can also hit (path_kernel_nee_analytic.cpp:286-292)
                         const float mis = (l.flags & kLightForward) != 0u ? nee_light_weight(mode, light_pdf, e.pdf) : 1.0f;
                         const float3 weighted = e.f * light_radiance * (mis / maxf(light_pdf, 1.0e-20f));
@@ -1899,6 +2064,7 @@ static std::unique_ptr<Scene> prepare_scene(const psy_scene_desc *d, bool brute_
         const psy_material_desc &md = d->materials[i];
         Material m;
         m.code.assign(md.closures, md.closures + md.closure_count);
+        if (md.values) m.values.assign(md.values, md.values + md.value_count);
         m.root = md.root;
         m.scalars.assign(md.scalars, md.scalars + md.scalar_count);
         for (uint32_t v = 0; v < md.vector_count; ++v)
@@ -2174,6 +2340,21 @@ void oracle_next_surface(const uint32_t *state, uint32_t label, uint32_t runtime
     std::memcpy(out, v, sizeof(v));
 }
 uint32_t oracle_contract_visibility(uint32_t v) { return contract_visibility(v); }
+// diffuse_intensity of one diffuse closure (normal, authored colour,
+// roughness) for a viewer direction and a light direction.
+void oracle_diffuse_intensity(const float *normal, const float *color, float roughness, const float *incoming,
+                              const float *outgoing, float *out) {
+    PhysicalClosure c{};
+    c.op = PSY_CLOSURE_DIFFUSE;
+    c.normal = f3(normal[0], normal[1], normal[2]);
+    c.color = f3(color[0], color[1], color[2]);
+    c.roughness = roughness;
+    const float3 v = diffuse_intensity(c, f3(incoming[0], incoming[1], incoming[2]),
+                                       f3(outgoing[0], outgoing[1], outgoing[2]));
+    out[0] = v.x;
+    out[1] = v.y;
+    out[2] = v.z;
+}
 
 // Prepared scene handle for traversal parity tests.
 void *oracle_scene_create(const psy_scene_desc *desc, int brute_force) {

@@ -169,6 +169,9 @@ inline float sin_(float x) { return static_cast<float>(std::sin(static_cast<doub
 inline float cos_(float x) { return static_cast<float>(std::cos(static_cast<double>(x))); }
 inline float acos_(float x) { return static_cast<float>(std::acos(static_cast<double>(x))); }
 inline float asin_(float x) { return static_cast<float>(std::asin(static_cast<double>(x))); }
+inline float pow_(float x, float y) {
+    return static_cast<float>(std::pow(static_cast<double>(x), static_cast<double>(y)));
+}
 inline float tan_(float x) { return static_cast<float>(std::tan(static_cast<double>(x))); }
 inline float atan2_(float y, float x) {
     return static_cast<float>(std::atan2(static_cast<double>(y), static_cast<double>(x)));

@@ -32,6 +32,18 @@ PASS_DENOISING_NORMAL, PASS_DENOISING_ALBEDO, PASS_SAMPLE_COUNT = 18, 19, 20
 FILTER_BOX, FILTER_GAUSSIAN, FILTER_BLACKMAN_HARRIS = 0, 1, 2
 DIRECT_MIS, DIRECT_FORWARD, DIRECT_NEE = 0, 1, 2
 TRACE_MAX_EVENTS = 16
+# closure inputs (psy_closure_instruction colour / scalar / roughness)
+INPUT_VALUE, INPUT_NONE = 0x80000000, 0xFFFFFFFF
+# value operations (compiler::ValueOperation numbering) and blend modes
+VALUE_TYPE_SCALAR, VALUE_TYPE_VECTOR = 0, 1
+(VALUE_PARAMETER, VALUE_PASSTHROUGH, VALUE_SCALAR_TO_COLOR, VALUE_SCALAR_TO_BOOLEAN, VALUE_COLOR_TO_SCALAR,
+ VALUE_VECTOR_TO_SCALAR, VALUE_ADD, VALUE_SUBTRACT, VALUE_MULTIPLY, VALUE_DIVIDE, VALUE_MINIMUM, VALUE_MAXIMUM,
+ VALUE_POWER) = range(13)
+VALUE_ABSOLUTE, VALUE_CLAMP01, VALUE_CLAMP_RANGE = 14, 15, 16
+VALUE_MIX_FLOAT, VALUE_MIX_VECTOR, VALUE_MIX, VALUE_MULTIPLY_COLOR, VALUE_INVERT = 21, 22, 23, 24, 26
+VALUE_SEPARATE_R, VALUE_SEPARATE_G, VALUE_SEPARATE_B, VALUE_COMBINE_COLOR = 100, 101, 102, 103
+BLEND_MIX, BLEND_DARKEN, BLEND_MULTIPLY, BLEND_LIGHTEN, BLEND_SCREEN, BLEND_ADD = 0, 1, 2, 4, 5, 7
+BLEND_DIFFERENCE, BLEND_SUBTRACT = 11, 13
 
 
 class MeshDesc(ctypes.Structure):
@@ -47,14 +59,19 @@ class InstanceDesc(ctypes.Structure):
 
 class ClosureInstruction(ctypes.Structure):
     _fields_ = [("op", ctypes.c_uint32), ("a", ctypes.c_uint32), ("b", ctypes.c_uint32),
-                ("color", ctypes.c_uint32), ("scalar", ctypes.c_uint32)]
+                ("color", ctypes.c_uint32), ("scalar", ctypes.c_uint32), ("roughness", ctypes.c_uint32)]
+
+
+class ValueInstruction(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("op", "type", "parameter", "a", "b", "c", "static_u0", "static_u1")]
 
 
 class MaterialDesc(ctypes.Structure):
     _fields_ = [("closures", ctypes.POINTER(ClosureInstruction)), ("closure_count", ctypes.c_uint32),
                 ("root", ctypes.c_uint32), ("scalars", c_float_p), ("scalar_count", ctypes.c_uint32),
                 ("vector_count", ctypes.c_uint32), ("vectors", c_float_p),
-                ("emission_sampling", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("emission_sampling", ctypes.c_uint32), ("value_count", ctypes.c_uint32),
+                ("values", ctypes.POINTER(ValueInstruction))]
 
 
 class LightDesc(ctypes.Structure):

@@ -145,11 +145,15 @@ __device__ __forceinline__ ConeSample sample_uniform_cone(f3 axis, float one_min
 constexpr uint32_t kMaxClosures = 16u;
 constexpr uint32_t kMaxClosureStack = 32u;
 
+// One allocated closure.  Diffuse closures keep their authored colour and
+// roughness for the Oren-Nayar evaluation (roughness below 1e-5: Lambert).
 struct PhysicalClosure {
     f3 weight;
     f3 normal;
     float sample_weight;
     uint32_t op;
+    f3 color;
+    float roughness;
 };
 
 struct SurfaceClosures {
@@ -173,9 +177,124 @@ __device__ __forceinline__ float ld_scalar(const SceneView &s, const MaterialGpu
     return s.scalars[m.scalar_offset + slot];
 }
 
+// Film::rgb_to_y of Blender 4.5's default scene-linear space, the
+// coefficients of color_to_scalar (src/luisa/graph_surface_value_math.cpp:91-103).
+constexpr float kRgbToYR = 0.21267404f, kRgbToYG = 0.7151516f, kRgbToYB = 0.07217542f;
+
+__device__ __forceinline__ f3 lerp3(f3 a, f3 b, f3 t) {
+    return {lerpf_(a.x, b.x, t.x), lerpf_(a.y, b.y, t.y), lerpf_(a.z, b.z, t.z)};
+}
+
+// cast<int>(x) != 0 of scalar_to_boolean: truncation toward zero, with the
+// saturating conversion of the hardware (NaN converts to 0).
+__device__ __forceinline__ bool truncates_nonzero(float x) { return __float2int_rz(x) != 0; }
+
+// The value stream of a SurfaceProgram (GraphSurfaceImplementation::
+// trace_value_stage, src/luisa/graph_surface_values.cpp:70-100): instructions
+// 0..id in order, each reading earlier results; scalars are held in x.
+// Operations: src/luisa/graph_surface_value_math.cpp:54-880,
+// graph_surface_value_context.cpp:80-108, graph_surface_value_procedural.cpp:
+// 568-600.  Scene compile checks the operations, operand order, types and
+// parameter slots.  Out of line: only linked closure inputs reach it.
+__device__ __noinline__ f3 eval_value(const SceneView &s, const MaterialGpu &m, uint32_t id) {
+    f3 v[kMaxValues];
+    const uint32_t n = min(id + 1u, min(m.value_count, kMaxValues));
+    for (uint32_t i = 0; i < n; ++i) {
+        const psy_value_instruction in = s.values[m.value_offset + i];
+        const f3 a = in.a < i ? v[in.a] : mk3(0.0f);
+        const f3 b = in.b < i ? v[in.b] : mk3(0.0f);
+        const f3 c = in.c < i ? v[in.c] : mk3(0.0f);
+        f3 r = mk3(0.0f);
+        switch (in.op) {
+        case PSY_VALUE_PARAMETER:
+            r = in.type == PSY_VALUE_TYPE_SCALAR ? mk3(ld_scalar(s, m, in.parameter), 0.0f, 0.0f)
+                                                 : ld_vector(s, m, in.parameter);
+            break;
+        case PSY_VALUE_PASSTHROUGH: r = a; break;
+        case PSY_VALUE_SCALAR_TO_COLOR: r = mk3(a.x); break;
+        case PSY_VALUE_SCALAR_TO_BOOLEAN: r.x = truncates_nonzero(a.x) ? 1.0f : 0.0f; break;
+        case PSY_VALUE_COLOR_TO_SCALAR: r.x = a.x * kRgbToYR + a.y * kRgbToYG + a.z * kRgbToYB; break;
+        case PSY_VALUE_VECTOR_TO_SCALAR: r.x = (a.x + a.y + a.z) / 3.0f; break;
+        case PSY_VALUE_ADD: r.x = a.x + b.x; break;
+        case PSY_VALUE_SUBTRACT: r.x = a.x - b.x; break;
+        case PSY_VALUE_MULTIPLY: r.x = a.x * b.x; break;
+        case PSY_VALUE_DIVIDE: r.x = fabsf(b.x) > 1.0e-20f ? a.x / b.x : 0.0f; break;
+        case PSY_VALUE_MINIMUM: r.x = fminf(a.x, b.x); break;
+        case PSY_VALUE_MAXIMUM: r.x = fmaxf(a.x, b.x); break;
+        case PSY_VALUE_POWER: r.x = pow_(fmaxf(a.x, 0.0f), b.x); break;
+        case PSY_VALUE_ABSOLUTE: r.x = fabsf(a.x); break;
+        case PSY_VALUE_CLAMP01: r.x = fminf(fmaxf(a.x, 0.0f), 1.0f); break;
+        case PSY_VALUE_CLAMP_RANGE: {
+            float lo = b.x, hi = c.x;
+            if (in.static_u0 == 1u && lo > hi) {
+                lo = c.x;
+                hi = b.x;
+            }
+            r.x = fminf(fmaxf(a.x, lo), hi);
+            break;
+        }
+        case PSY_VALUE_MIX_FLOAT: {
+            const float t = in.static_u0 != 0u ? fminf(fmaxf(c.x, 0.0f), 1.0f) : c.x;
+            r.x = lerpf_(a.x, b.x, t);
+            break;
+        }
+        case PSY_VALUE_MIX_VECTOR: {
+            f3 t = in.static_u0 != 0u ? c : mk3(c.x);
+            if (in.static_u1 != 0u) t = clamp3(t, 0.0f, 1.0f);
+            r = lerp3(a, b, t);
+            break;
+        }
+        case PSY_VALUE_MIX: {
+            const float t = (in.static_u1 & 1u) != 0u ? fminf(fmaxf(c.x, 0.0f), 1.0f) : c.x;
+            const f3 tt = mk3(t);
+            switch (in.static_u0) {
+            case PSY_BLEND_DARKEN: r = lerp3(a, mk3(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)), tt); break;
+            case PSY_BLEND_MULTIPLY: r = lerp3(a, a * b, tt); break;
+            case PSY_BLEND_LIGHTEN: r = lerp3(a, mk3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)), tt); break;
+            case PSY_BLEND_SCREEN: {
+                const float k = 1.0f - t;
+                r = mk3(1.0f - (k + t * (1.0f - b.x)) * (1.0f - a.x), 1.0f - (k + t * (1.0f - b.y)) * (1.0f - a.y),
+                        1.0f - (k + t * (1.0f - b.z)) * (1.0f - a.z));
+                break;
+            }
+            case PSY_BLEND_ADD: r = lerp3(a, a + b, tt); break;
+            case PSY_BLEND_DIFFERENCE:
+                r = lerp3(a, mk3(fabsf(a.x - b.x), fabsf(a.y - b.y), fabsf(a.z - b.z)), tt);
+                break;
+            case PSY_BLEND_SUBTRACT: r = lerp3(a, a - b, tt); break;
+            default: r = lerp3(a, b, tt); break;  // PSY_BLEND_MIX
+            }
+            break;
+        }
+        case PSY_VALUE_MULTIPLY_COLOR: r = lerp3(a, a * b, mk3(fminf(fmaxf(c.x, 0.0f), 1.0f))); break;
+        case PSY_VALUE_INVERT: r = lerp3(a, mk3(1.0f) - a, mk3(b.x)); break;
+        case PSY_VALUE_SEPARATE_R: r.x = a.x; break;
+        case PSY_VALUE_SEPARATE_G: r.x = a.y; break;
+        case PSY_VALUE_SEPARATE_B: r.x = a.z; break;
+        case PSY_VALUE_COMBINE_COLOR: r = mk3(a.x, b.x, c.x); break;
+        default: break;
+        }
+        v[i] = r;
+    }
+    return n > id ? v[id] : mk3(0.0f);
+}
+
+// A closure input: the closure node's own parameter slot, or a value of the
+// stream (PSY_INPUT_VALUE).
+__device__ __forceinline__ f3 input_vector(const SceneView &s, const MaterialGpu &m, uint32_t ref) {
+    if ((ref & PSY_INPUT_VALUE) == 0u) return ld_vector(s, m, ref);
+    return eval_value(s, m, ref & ~PSY_INPUT_VALUE);
+}
+__device__ __forceinline__ float input_scalar(const SceneView &s, const MaterialGpu &m, uint32_t ref) {
+    if (ref == PSY_INPUT_NONE) return 0.0f;
+    if ((ref & PSY_INPUT_VALUE) == 0u) return ld_scalar(s, m, ref);
+    return eval_value(s, m, ref & ~PSY_INPUT_VALUE).x;
+}
+
 // Visits closure leaves depth-first, `a` before `b`, with the add / mix
-// weight rule; `visit(op, weight)` receives diffuse / transparent /
-// emission leaves.
+// weight rule; `visit(op, weight, color, roughness)` receives diffuse /
+// transparent / emission leaves with their authored colour (x strength for
+// emission) and, for diffuse, the roughness input.
 template <typename Visit>
 __device__ __forceinline__ void walk_closures(const SceneView &s, const MaterialGpu &m, Visit visit) {
     uint32_t stack_id[kMaxClosureStack];
@@ -196,13 +315,16 @@ __device__ __forceinline__ void walk_closures(const SceneView &s, const Material
             stack_id[sp] = c.a; stack_w[sp] = w; ++sp;
         } else if (c.op == PSY_CLOSURE_MIX) {
             if (sp + 2 > int(kMaxClosureStack)) continue;
-            const float f = clampf_(ld_scalar(s, m, c.scalar), 0.0f, 1.0f);
+            const float f = clampf_(input_scalar(s, m, c.scalar), 0.0f, 1.0f);
             stack_id[sp] = c.b; stack_w[sp] = w * f; ++sp;
             stack_id[sp] = c.a; stack_w[sp] = w * (1.0f - f); ++sp;
         } else if (c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_TRANSPARENT) {
-            visit(c.op, ld_vector(s, m, c.color) * w);
+            const f3 color = input_vector(s, m, c.color);
+            const float roughness = c.op == PSY_CLOSURE_DIFFUSE ? input_scalar(s, m, c.roughness) : 0.0f;
+            visit(c.op, color * w, color, roughness);
         } else if (c.op == PSY_CLOSURE_EMISSION) {
-            visit(c.op, ld_vector(s, m, c.color) * ld_scalar(s, m, c.scalar) * w);
+            const f3 color = input_vector(s, m, c.color) * input_scalar(s, m, c.scalar);
+            visit(c.op, color * w, color, 0.0f);
         }
     }
 }
@@ -212,7 +334,7 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
     out.count = 0u;
     out.emission = mk3(0.0f);
     const f3 closure_normal = safe_normalize(shading_normal, shading_normal);
-    walk_closures(s, m, [&](uint32_t op, f3 w) {
+    walk_closures(s, m, [&](uint32_t op, f3 w, f3 color, float roughness) {
         if (op == PSY_CLOSURE_EMISSION) {
             out.emission = out.emission + w;
             return;
@@ -220,6 +342,8 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
         if (out.count >= kMaxClosures) return;
         PhysicalClosure p;
         p.op = op;
+        p.color = color;
+        p.roughness = roughness;
         if (op == PSY_CLOSURE_DIFFUSE) {
             p.weight = bsdf_allocated_weight(w);
             p.sample_weight = closure_sample_weight(p.weight);
@@ -238,7 +362,7 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
 
 __device__ __forceinline__ f3 material_emission(const SceneView &s, const MaterialGpu &m) {
     f3 r = mk3(0.0f);
-    walk_closures(s, m, [&](uint32_t op, f3 w) {
+    walk_closures(s, m, [&](uint32_t op, f3 w, f3, float) {
         if (op == PSY_CLOSURE_EMISSION) r = r + w;
     });
     return r;
@@ -247,7 +371,7 @@ __device__ __forceinline__ f3 material_emission(const SceneView &s, const Materi
 // transparent_extinction (src/luisa/graph_surface_implementation.cpp:354-372).
 __device__ __forceinline__ f3 transparent_extinction(const SceneView &s, const MaterialGpu &m) {
     f3 r = mk3(0.0f);
-    walk_closures(s, m, [&](uint32_t op, f3 w) {
+    walk_closures(s, m, [&](uint32_t op, f3 w, f3, float) {
         if (op == PSY_CLOSURE_TRANSPARENT && closure_sample_weight(w) >= 1.0e-5f) r = r + w;
     });
     return r;
@@ -290,12 +414,51 @@ struct Evaluation {
     uint32_t events;
 };
 
+// oren_nayar_g (src/luisa/graph_surface_scattering.cpp:463-473).
+__device__ __noinline__ float oren_nayar_g(float cosine) {
+    const float c = clampf_(cosine, 0.0f, 1.0f);
+    const float sine = sqrtf(maxf_(1.0f - c * c, 0.0f));
+    const float theta = acos_(c);
+    const float safe_cosine = maxf_(c, 1.0e-6f);
+    const float regular = sine * (theta - 2.0f / 3.0f - sine * c) +
+                          2.0f / 3.0f * (sine / safe_cosine) * (1.0f - sine * sine * sine);
+    const float taylor = (kPi * 0.5f - 2.0f / 3.0f) - c;
+    return c < 1.0e-6f ? taylor : regular;
+}
+
+// diffuse_intensity (src/luisa/graph_surface_scattering.cpp:475-506): Lambert
+// below roughness 1e-5, else the energy-compensated Oren-Nayar model of
+// Cycles (single scattering plus a multiple-scattering term from the
+// clamped albedo).  `incoming` points to the viewer, `outgoing` to the light.
+__device__ __noinline__ f3 diffuse_intensity(const PhysicalClosure &c, f3 incoming, f3 outgoing) {
+    const float nl = maxf_(dot(c.normal, outgoing), 0.0f);
+    const float sigma = clampf_(c.roughness, 0.0f, 1.0f);
+    if (sigma < 1.0e-5f) return mk3(nl * kInvPi);
+    const float a = 1.0f / (kPi + sigma * (kPi * 0.5f - 2.0f / 3.0f));
+    const float b = sigma * a;
+    const float nv = maxf_(dot(c.normal, incoming), 0.0f);
+    float t = dot(outgoing, incoming) - nl * nv;
+    if (t > 0.0f) t = t / (maxf_(nl, nv) + 1.17549435e-38f);
+    const float single_scatter = a + b * t;
+    const f3 albedo = clamp3(c.color, 0.0f, 1.0f);
+    const float e_average = a * kPi + ((2.0f * kPi - 5.6f) / 3.0f) * b;
+    const float ratio = e_average / (1.0f - e_average);
+    const float keep = 1.0f - e_average;
+    const f3 e_ms = mk3(kInvPi * (albedo.x * albedo.x) * ratio / (1.0f - albedo.x * keep),
+                        kInvPi * (albedo.y * albedo.y) * ratio / (1.0f - albedo.y * keep),
+                        kInvPi * (albedo.z * albedo.z) * ratio / (1.0f - albedo.z * keep));
+    const float e_incoming = a * kPi + b * oren_nayar_g(nv);
+    const f3 multiscatter = e_ms * (1.0f - e_incoming);
+    const float e_outgoing = a * kPi + b * oren_nayar_g(nl);
+    return (mk3(single_scatter) + multiscatter * (1.0f - e_outgoing)) * nl;
+}
+
 // surface_closure_evaluation_contribution + accumulator
 // (src/luisa/surface_closure_evaluation.cpp:71-438).  Out of line: the
 // shading kernel calls it for the light sample and for the BSDF sample, and
 // a single copy keeps the kernel's code within the instruction cache.
-__device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, f3 shading_normal, f3 outgoing_raw,
-                                                       uint32_t lobe_mask, int selected) {
+__device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, f3 shading_normal, f3 incoming,
+                                                    f3 outgoing_raw, uint32_t lobe_mask, int selected) {
     const f3 outgoing = safe_normalize(outgoing_raw, shading_normal);
     Evaluation e{mk3(0.0f), 0.0f, 0u};
     float total = 0.0f, weighted_pdf = 0.0f;
@@ -312,8 +475,7 @@ __device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, f3
         float pdf = maxf_(dot(c.normal, outgoing), 0.0f) * kInvPi;
         if (!pdf_valid) pdf = 0.0f;
         if (!diffuse_enabled) continue;
-        const float nl = maxf_(dot(c.normal, outgoing), 0.0f);
-        const f3 value = c.weight * (nl * kInvPi) * bump;
+        const f3 value = c.weight * diffuse_intensity(c, incoming, outgoing) * bump;
         e.f = e.f + value;
         total += c.sample_weight;
         weighted_pdf += c.sample_weight * pdf;
@@ -368,7 +530,7 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
     out.closure_index = uint32_t(chosen);
     out.wi = direction;
     if (!(transparent || dot(geometric_normal, direction) > 0.0f)) return out;
-    const Evaluation mixture = evaluate_mixture(s, shading_normal, direction, lobe_mask, chosen);
+    const Evaluation mixture = evaluate_mixture(s, shading_normal, incoming, direction, lobe_mask, chosen);
     Evaluation r;
     r.f = mixture.f;
     float delta = 0.0f;

@@ -833,28 +833,120 @@ psy_status clear_film(psy_session *s, bool sync = true) {
 }
 
 
+// Checks a compiled SurfaceProgram against what the kernels interpret: the
+// in-scope closure and value operations, operands that name earlier value
+// instructions of the right type, parameter slots inside the block, and
+// closure inputs of the type their socket takes.
+psy_status validate_material(const psy_material_desc &m) {
+    if (m.closure_count == 0u || !m.closures || m.root >= m.closure_count)
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "material without a valid closure root");
+    if (m.value_count > psy::kMaxValues)
+        return fail(PSY_ERROR_UNSUPPORTED, "value stream longer than " + std::to_string(psy::kMaxValues) +
+                                               " instructions");
+    if (m.value_count != 0u && !m.values) return fail(PSY_ERROR_INVALID_ARGUMENT, "value stream without instructions");
+    constexpr uint32_t S = PSY_VALUE_TYPE_SCALAR, V = PSY_VALUE_TYPE_VECTOR, X = 0xffffffffu;
+    for (uint32_t k = 0; k < m.value_count; ++k) {
+        const psy_value_instruction &in = m.values[k];
+        // result type and operand types (X: operand unused) per operation
+        uint32_t result = S, ta = X, tb = X, tc = X;
+        switch (in.op) {
+        case PSY_VALUE_PARAMETER: result = in.type; break;
+        case PSY_VALUE_PASSTHROUGH: result = in.type; ta = in.type; break;
+        case PSY_VALUE_SCALAR_TO_COLOR: result = V; ta = S; break;
+        case PSY_VALUE_SCALAR_TO_BOOLEAN: ta = S; break;
+        case PSY_VALUE_COLOR_TO_SCALAR:
+        case PSY_VALUE_VECTOR_TO_SCALAR: ta = V; break;
+        case PSY_VALUE_ADD: case PSY_VALUE_SUBTRACT: case PSY_VALUE_MULTIPLY: case PSY_VALUE_DIVIDE:
+        case PSY_VALUE_MINIMUM: case PSY_VALUE_MAXIMUM: case PSY_VALUE_POWER: ta = tb = S; break;
+        case PSY_VALUE_ABSOLUTE: case PSY_VALUE_CLAMP01: ta = S; break;
+        case PSY_VALUE_CLAMP_RANGE: case PSY_VALUE_MIX_FLOAT: ta = tb = tc = S; break;
+        case PSY_VALUE_MIX_VECTOR: result = V; ta = tb = V; tc = in.static_u0 != 0u ? V : S; break;
+        case PSY_VALUE_MIX:
+            if (in.static_u0 != PSY_BLEND_MIX && in.static_u0 != PSY_BLEND_DARKEN && in.static_u0 != PSY_BLEND_MULTIPLY &&
+                in.static_u0 != PSY_BLEND_LIGHTEN && in.static_u0 != PSY_BLEND_SCREEN && in.static_u0 != PSY_BLEND_ADD &&
+                in.static_u0 != PSY_BLEND_DIFFERENCE && in.static_u0 != PSY_BLEND_SUBTRACT)
+                return fail(PSY_ERROR_UNSUPPORTED, "colour blend mode outside the supported set");
+            result = V; ta = tb = V; tc = S;
+            break;
+        case PSY_VALUE_MULTIPLY_COLOR: result = V; ta = tb = V; tc = S; break;
+        case PSY_VALUE_INVERT: result = V; ta = V; tb = S; break;
+        case PSY_VALUE_SEPARATE_R: case PSY_VALUE_SEPARATE_G: case PSY_VALUE_SEPARATE_B:
+            if (in.static_u0 != 0u) return fail(PSY_ERROR_UNSUPPORTED, "separate colour outside RGB mode");
+            ta = V;
+            break;
+        case PSY_VALUE_COMBINE_COLOR:
+            if (in.static_u0 != 0u) return fail(PSY_ERROR_UNSUPPORTED, "combine colour outside RGB mode");
+            result = V; ta = tb = tc = S;
+            break;
+        default:
+            return fail(PSY_ERROR_UNSUPPORTED, "value operation " + std::to_string(in.op) + " outside the supported set");
+        }
+        if (in.type != result) return fail(PSY_ERROR_INVALID_ARGUMENT, "value instruction of the wrong result type");
+        if (in.op == PSY_VALUE_PARAMETER && in.parameter >= (in.type == S ? m.scalar_count : m.vector_count))
+            return fail(PSY_ERROR_INVALID_ARGUMENT, "value parameter slot out of range");
+        const uint32_t ops[3] = {in.a, in.b, in.c}, types[3] = {ta, tb, tc};
+        for (int o = 0; o < 3; ++o) {
+            if (types[o] == X) continue;
+            if (ops[o] >= k) return fail(PSY_ERROR_INVALID_ARGUMENT, "value operand is not an earlier instruction");
+            if (m.values[ops[o]].type != types[o])
+                return fail(PSY_ERROR_INVALID_ARGUMENT, "value operand of the wrong type");
+        }
+    }
+    // a closure input of type `type`; `optional` admits PSY_INPUT_NONE
+    auto input_ok = [&](uint32_t ref, uint32_t type, bool optional) {
+        if (ref == PSY_INPUT_NONE) return optional;
+        if (ref & PSY_INPUT_VALUE) {
+            const uint32_t id = ref & ~PSY_INPUT_VALUE;
+            return id < m.value_count && m.values[id].type == type;
+        }
+        return ref < (type == S ? m.scalar_count : m.vector_count);
+    };
+    for (uint32_t k = 0; k < m.closure_count; ++k) {
+        const psy_closure_instruction &c = m.closures[k];
+        if (c.op > PSY_CLOSURE_MIX) return fail(PSY_ERROR_UNSUPPORTED, "closure operation outside the supported set");
+        if ((c.op == PSY_CLOSURE_ADD || c.op == PSY_CLOSURE_MIX) && (c.a >= m.closure_count || c.b >= m.closure_count))
+            return fail(PSY_ERROR_INVALID_ARGUMENT, "closure child out of range");
+        if ((c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_TRANSPARENT) &&
+            !input_ok(c.color, V, false))
+            return fail(PSY_ERROR_INVALID_ARGUMENT, "closure colour input out of range");
+        if ((c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_MIX) && !input_ok(c.scalar, S, false))
+            return fail(PSY_ERROR_INVALID_ARGUMENT, "closure scalar input out of range");
+        if (c.op == PSY_CLOSURE_DIFFUSE && !input_ok(c.roughness, S, true))
+            return fail(PSY_ERROR_INVALID_ARGUMENT, "closure roughness input out of range");
+    }
+    return PSY_OK;
+}
+
 // Emission estimate of a closure program for the light tree
 // (estimate_surface_emission, src/compiler/surface_program.cpp:244-330): one
 // estimate per instruction in program order -- emission colour x strength,
 // add a + b, mix a (1 - f) + b f with the unclamped factor -- where an
-// operand that is not an earlier instruction counts as one.
+// operand that is not an earlier instruction counts as one.  Only an
+// unlinked socket of the closure node itself is read as a literal
+// (direct_parameter_value, surface_program.cpp:170-186); a linked colour or
+// strength counts as one, and a mix with a linked factor sums its branches.
 void emission_estimate(const psy_material_desc &m, float out[3]) {
     std::vector<std::array<float, 3>> est;
     est.reserve(m.closure_count);
     auto dep = [&](uint32_t id) { return id < est.size() ? est[id] : std::array<float, 3>{1.0f, 1.0f, 1.0f}; };
+    auto literal = [](uint32_t ref) { return (ref & PSY_INPUT_VALUE) == 0u; };
     for (uint32_t i = 0; i < m.closure_count; ++i) {
         const psy_closure_instruction &c = m.closures[i];
         std::array<float, 3> e{0.0f, 0.0f, 0.0f};
         if (c.op == PSY_CLOSURE_EMISSION) {
-            const float strength = m.scalars[c.scalar];
-            for (int k = 0; k < 3; ++k) e[k] = m.vectors[3u * c.color + k] * strength;
+            const float strength = literal(c.scalar) ? m.scalars[c.scalar] : 1.0f;
+            for (int k = 0; k < 3; ++k) e[k] = (literal(c.color) ? m.vectors[3u * c.color + k] : 1.0f) * strength;
         } else if (c.op == PSY_CLOSURE_ADD) {
             const auto a = dep(c.a), b = dep(c.b);
             for (int k = 0; k < 3; ++k) e[k] = a[k] + b[k];
         } else if (c.op == PSY_CLOSURE_MIX) {
             const auto a = dep(c.a), b = dep(c.b);
-            const float f = m.scalars[c.scalar];
-            for (int k = 0; k < 3; ++k) e[k] = a[k] * (1.0f - f) + b[k] * f;
+            if (literal(c.scalar)) {
+                const float f = m.scalars[c.scalar];
+                for (int k = 0; k < 3; ++k) e[k] = a[k] * (1.0f - f) + b[k] * f;
+            } else {
+                for (int k = 0; k < 3; ++k) e[k] = a[k] + b[k];
+            }
         }
         est.push_back(e);
     }
@@ -995,6 +1087,8 @@ psy_status build_light_tree(psy_scene *sc, bool sync = true) {
         m.root = g.root;
         m.scalars = sc->scalars.data() + g.scalar_offset;
         m.vectors = sc->vectors.data() + 3ull * g.vector_offset;
+        m.values = sc->values_host.data() + g.value_offset;
+        m.value_count = g.value_count;
         if (g.has_emission) emission_estimate(m, estimates[i].data());
         else estimates[i] = {0.0f, 0.0f, 0.0f};
     }
@@ -1257,20 +1351,8 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         if (m.smooth && !m.normals) return fail(PSY_ERROR_INVALID_ARGUMENT, "smooth mesh without normals");
     }
     for (uint32_t i = 0; i < d->material_count; ++i) {
-        const psy_material_desc &m = d->materials[i];
-        if (m.closure_count == 0u || !m.closures || m.root >= m.closure_count)
-            return fail(PSY_ERROR_INVALID_ARGUMENT, "material without a valid closure root");
-        for (uint32_t k = 0; k < m.closure_count; ++k) {
-            const psy_closure_instruction &c = m.closures[k];
-            if (c.op > PSY_CLOSURE_MIX) return fail(PSY_ERROR_UNSUPPORTED, "closure operation outside the supported set");
-            if ((c.op == PSY_CLOSURE_ADD || c.op == PSY_CLOSURE_MIX) && (c.a >= m.closure_count || c.b >= m.closure_count))
-                return fail(PSY_ERROR_INVALID_ARGUMENT, "closure child out of range");
-            if ((c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_TRANSPARENT) &&
-                c.color >= m.vector_count)
-                return fail(PSY_ERROR_INVALID_ARGUMENT, "closure colour slot out of range");
-            if ((c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_MIX) && c.scalar >= m.scalar_count)
-                return fail(PSY_ERROR_INVALID_ARGUMENT, "closure scalar slot out of range");
-        }
+        const psy_status valid = validate_material(d->materials[i]);
+        if (valid != PSY_OK) return valid;
     }
     for (uint32_t i = 0; i < d->light_count; ++i) {
         const psy_light_desc &l = d->lights[i];
@@ -1506,12 +1588,16 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
 
     // ---- materials and parameter blocks
     std::vector<psy_closure_instruction> code;
+    std::vector<psy_value_instruction> values;
     bool any_transparent = false;
     for (uint32_t i = 0; i < d->material_count; ++i) {
         const psy_material_desc &m = d->materials[i];
         psy::MaterialGpu g{};
         g.code_offset = uint32_t(code.size());
         g.code_count = m.closure_count;
+        g.value_offset = uint32_t(values.size());
+        g.value_count = m.value_count;
+        values.insert(values.end(), m.values, m.values + m.value_count);
         g.root = m.root;
         g.scalar_offset = uint32_t(sc->scalars.size());
         g.vector_offset = uint32_t(sc->vectors.size() / 3u);
@@ -1650,6 +1736,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     }
 
     sc->code_host = code;
+    sc->values_host = values;
     sc->emitters_host = std::move(emitters);
     sc->lights_host = lights;
     sc->stats.emitters_ms = lap();
@@ -1659,7 +1746,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     // back, and parameter blocks replaced by edits are retired without
     // waiting on the device.
     for (DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tris, &sc->instances, &sc->meshes, &sc->positions, &sc->normals,
-                            &sc->indices, &sc->tri_materials, &sc->material_buf, &sc->code, &sc->scalar_buf,
+                            &sc->indices, &sc->tri_materials, &sc->material_buf, &sc->code, &sc->value_buf, &sc->scalar_buf,
                             &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights, &sc->lamp_consts,
                             &sc->lamp_bounds, &sc->lamp_ids})
         b->ordered = st;
@@ -1674,6 +1761,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->tri_materials.upload(tri_materials, st));
     PSY_CUDA_TRY(sc->material_buf.upload(sc->materials, st));
     PSY_CUDA_TRY(sc->code.upload(code, st));
+    PSY_CUDA_TRY(sc->value_buf.upload(values, st));
     PSY_CUDA_TRY(sc->scalar_buf.upload(sc->scalars, st));
     PSY_CUDA_TRY(sc->vector_buf.upload(sc->vectors, st));
     PSY_CUDA_TRY(sc->emitters.upload(sc->emitters_host, st));
@@ -1712,7 +1800,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     sc->stats.upload_bytes = 0u;
     for (const DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tris, &sc->instances, &sc->meshes, &sc->positions,
                                   &sc->normals, &sc->indices, &sc->tri_materials, &sc->material_buf, &sc->code,
-                                  &sc->scalar_buf, &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights,
+                                  &sc->value_buf, &sc->scalar_buf, &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights,
                                   &sc->lamp_consts, &sc->lamp_bounds, &sc->lamp_ids})
         sc->stats.upload_bytes += b->bytes;
     psy::SceneView &v = sc->view;
@@ -1727,6 +1815,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     v.tri_materials = sc->tri_materials.as<uint32_t>();
     v.materials = sc->material_buf.as<psy::MaterialGpu>();
     v.code = sc->code.as<psy_closure_instruction>();
+    v.values = sc->value_buf.as<psy_value_instruction>();
     v.scalars = sc->scalar_buf.as<float>();
     v.vectors = sc->vector_buf.as<float>();
     v.emitters = sc->emitters.as<psy::EmitterGpu>();
@@ -1931,7 +2020,7 @@ psy_status psy_session_read_trace(psy_session *s, psy_path_trace *out) {
 uint64_t psy::host::scene_device_bytes(const psy_scene *s) {
     uint64_t n = 0u;
     for (const DeviceBuffer *b : {&s->tlas, &s->blas, &s->tris, &s->instances, &s->meshes, &s->positions, &s->normals,
-                                  &s->indices, &s->tri_materials, &s->material_buf, &s->code, &s->scalar_buf,
+                                  &s->indices, &s->tri_materials, &s->material_buf, &s->code, &s->value_buf, &s->scalar_buf,
                                   &s->vector_buf, &s->emitters, &s->distribution, &s->lights, &s->lamp_consts, &s->lamp_bounds,
                                   &s->lamp_ids, &s->lt_nodes, &s->lt_emitters, &s->lt_mapping, &s->lt_lookup})
         n += b->bytes;

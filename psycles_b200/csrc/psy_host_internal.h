@@ -154,7 +154,7 @@ struct psy_scene {
     std::vector<psy::MaterialGpu> materials;
     std::vector<float> scalars, vectors;
     psy::host::DeviceBuffer tlas, blas, tris, instances, meshes, positions, normals, indices, tri_materials, material_buf, code,
-        scalar_buf, vector_buf, emitters, distribution, lights, lamp_consts, lamp_bounds, lamp_ids, lt_nodes, lt_emitters,
+        value_buf, scalar_buf, vector_buf, emitters, distribution, lights, lamp_consts, lamp_bounds, lamp_ids, lt_nodes, lt_emitters,
         lt_mapping, lt_lookup;
     psy::SceneView view{};
     uint64_t triangle_count = 0;
@@ -165,6 +165,7 @@ struct psy_scene {
     std::vector<psy::EmitterGpu> emitters_host;
     std::vector<psy_light_desc> lights_host;
     std::vector<psy_closure_instruction> code_host;
+    std::vector<psy_value_instruction> values_host;
     std::vector<uint8_t> instance_mirrored;  // object-to-world determinant < 0
     std::mutex light_tree_mutex;
     bool light_tree_built = false;

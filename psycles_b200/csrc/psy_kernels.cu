@@ -866,7 +866,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                             }
                         }
                         if (sampled) {
-                            const Evaluation e = evaluate_mixture(closures, sp.n, ldir, lobe_mask, -1);
+                            const Evaluation e = evaluate_mixture(closures, sp.n, -ray.d, ldir, lobe_mask, -1);
                             const float mis = weigh_mis ? nee_light_weight(p.direct_mode, light_pdf, e.pdf) : 1.0f;
                             const f3 weighted = e.f * light_radiance * (mis / pdf_divisor);
                             if (any_nonzero(weighted)) {

@@ -102,6 +102,9 @@ __device__ __noinline__ float asin_(float x) { return static_cast<float>(asin(st
 __device__ __noinline__ float atan2_(float y, float x) {
     return static_cast<float>(atan2(static_cast<double>(y), static_cast<double>(x)));
 }
+__device__ __noinline__ float pow_(float x, float y) {
+    return static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y)));
+}
 
 constexpr float kPi = 3.1415926535897932f;
 constexpr float kInvPi = 0.31830988618379067154f;

@@ -86,7 +86,12 @@ struct alignas(16) MeshGpu {
 struct alignas(16) MaterialGpu {
     uint32_t code_offset, code_count, root, scalar_offset;
     uint32_t vector_offset, emission_sampling, has_emission, has_transparent;
+    uint32_t value_offset, value_count, pad0, pad1;
 };
+
+// Value instructions a material's program may hold (its stream is
+// evaluated into a per-thread array of this many entries).
+constexpr uint32_t kMaxValues = 64u;
 
 struct alignas(16) EmitterGpu {
     float p0[3], p1[3], p2[3], ng[3];
@@ -125,6 +130,7 @@ struct SceneView {
     const uint32_t *tri_materials;
     const MaterialGpu *materials;
     const psy_closure_instruction *code;
+    const psy_value_instruction *values;
     const float *scalars;
     const float *vectors;
     const EmitterGpu *emitters;

@@ -28,7 +28,7 @@ import numpy as np
 
 from . import _abi
 from .materials import (CompiledMaterial, ShaderGraph, compile_surface_program, diffuse_material,
-                        emission_material, random_material)
+                        emission_material, random_material, value_graph_material)
 
 
 @dataclasses.dataclass
@@ -133,24 +133,28 @@ def camera_desc(cam: "Camera") -> _abi.CameraDesc:
 
 
 def _material_descs(mats) -> tuple:
-    """psy_material_desc array of `mats`: every program, scalar block and
-    vector block concatenated into one array each, and the descriptors
-    filled as one structured numpy array (a scene may hold thousands of
-    materials; per-material ctypes pointers would dominate its flattening)."""
+    """psy_material_desc array of `mats`: every closure program, value
+    stream, scalar block and vector block concatenated into one array each,
+    and the descriptors filled as one structured numpy array (a scene may
+    hold thousands of materials; per-material ctypes pointers would dominate
+    its flattening)."""
     n = max(len(mats), 1)
-    codes = [np.ascontiguousarray(cm.program.closures, dtype=np.uint32).reshape(-1, 5) for cm in mats]
+    codes = [np.ascontiguousarray(cm.program.closures, dtype=np.uint32).reshape(-1, 6) for cm in mats]
+    vals = [np.ascontiguousarray(cm.program.values, dtype=np.uint32).reshape(-1, 8) for cm in mats]
     scal = [np.ascontiguousarray(cm.parameters.scalars, dtype=np.float32).reshape(-1) for cm in mats]
     vecs = [np.ascontiguousarray(cm.parameters.vectors, dtype=np.float32).reshape(-1) for cm in mats]
-    code_all = np.concatenate(codes) if codes else np.zeros((1, 5), np.uint32)
+    code_all = np.concatenate(codes) if codes else np.zeros((1, 6), np.uint32)
+    val_all = np.concatenate(vals + [np.zeros((1, 8), np.uint32)])
     scal_all = np.concatenate(scal + [np.zeros(1, np.float32)])
     vec_all = np.concatenate(vecs + [np.zeros(3, np.float32)])
     c_counts = np.array([c.shape[0] for c in codes], np.uint64)
+    w_counts = np.array([v.shape[0] for v in vals], np.uint64)
     s_counts = np.array([s.size for s in scal], np.uint64)
     v_counts = np.array([v.size for v in vecs], np.uint64)
     start = lambda counts: np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.uint64) if len(counts) else counts
     rec = np.zeros(n, dtype=_MATERIAL_DESC_DTYPE)
     if mats:
-        rec["closures"] = np.uint64(code_all.ctypes.data) + start(c_counts) * np.uint64(20)
+        rec["closures"] = np.uint64(code_all.ctypes.data) + start(c_counts) * np.uint64(24)
         rec["closure_count"] = c_counts
         rec["root"] = [cm.program.root for cm in mats]
         rec["scalars"] = np.uint64(scal_all.ctypes.data) + start(s_counts) * np.uint64(4)
@@ -158,16 +162,19 @@ def _material_descs(mats) -> tuple:
         rec["vector_count"] = v_counts // np.uint64(3)
         rec["vectors"] = np.uint64(vec_all.ctypes.data) + start(v_counts) * np.uint64(4)
         rec["emission_sampling"] = [cm.emission_sampling for cm in mats]
+        rec["value_count"] = w_counts
+        rec["values"] = np.uint64(val_all.ctypes.data) + start(w_counts) * np.uint64(32)
     descs = (_abi.MaterialDesc * n).from_buffer(rec)
-    return descs, [rec, code_all, scal_all, vec_all]
+    return descs, [rec, code_all, val_all, scal_all, vec_all]
 
 
-# psy_material_desc of include/psycles_cuda.h on LP64 hosts (48 bytes)
+# psy_material_desc of include/psycles_cuda.h on LP64 hosts (56 bytes)
 _MATERIAL_DESC_DTYPE = np.dtype({
     "names": ["closures", "closure_count", "root", "scalars", "scalar_count", "vector_count", "vectors",
-              "emission_sampling", "reserved"],
-    "formats": [np.uint64, np.uint32, np.uint32, np.uint64, np.uint32, np.uint32, np.uint64, np.uint32, np.uint32],
-    "offsets": [0, 8, 12, 16, 24, 28, 32, 40, 44], "itemsize": 48})
+              "emission_sampling", "value_count", "values"],
+    "formats": [np.uint64, np.uint32, np.uint32, np.uint64, np.uint32, np.uint32, np.uint64, np.uint32, np.uint32,
+                np.uint64],
+    "offsets": [0, 8, 12, 16, 24, 28, 32, 40, 44, 48], "itemsize": 56})
 
 
 class SceneDescHandle:
@@ -516,6 +523,21 @@ def lamp_scene(seed: int = 0) -> Scene:
     ]
     cam = Camera(look_at((0.0, 2.0, 7.0), (0.0, 1.5, -1.0)), math.radians(45.0), math.radians(45.0), 0)
     return Scene(meshes, instances, mats, ls, cam, background=(0.05, 0.05, 0.08))
+
+
+def value_graph_scene(seed: int = 0) -> Scene:
+    """The small test scene's geometry and lamps with materials whose closure
+    inputs are linked to value nodes (RGB / Value nodes through colour
+    blends, float math, conversions, separate / combine RGB into rough
+    diffuse colours, mix factors and emission strengths), plus rough and
+    smooth diffuse walls."""
+    rng = np.random.default_rng(seed)
+    graphs = [diffuse_material((0.7, 0.7, 0.7), 0.5), emission_material((1.0, 0.9, 0.8), 6.0)]
+    for _ in range(6):
+        graphs.append(value_graph_material(rng))
+    base = small_test_scene(seed=seed)
+    base.materials = _materials(graphs)
+    return base
 
 
 def render_settings(width: int, height: int, max_bounces: int = 4, seed: int = 0, **overrides) -> _abi.RenderSettings:

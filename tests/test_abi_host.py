@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert _abi.load().psy_abi_version() == 1
+    assert _abi.load().psy_abi_version() == 2
 
 
 def test_sobol_table_matches_oracle(oracle_lib, golden):

@@ -141,7 +141,7 @@ def test_rebind_parameters_equals_recompiled_scene(backend):
     scene = scenes.cornell_box()
     st = scenes.render_settings(48, 48, max_bounces=4)
     comp = backend.compile_scene(scene).scene
-    comp.rebind_parameters(1, np.zeros(0, np.float32), np.array([[0.1, 0.6, 0.7]], np.float32))
+    comp.rebind_parameters(1, scene.materials[1].parameters.scalars, np.array([[0.1, 0.6, 0.7]], np.float32))
     s1 = backend.create_session(comp, st)
     assert s1.render_samples(SampleRange(0, 4, 0, 4))
     from psycles_b200.materials import diffuse_material
