@@ -100,6 +100,29 @@ class MemoryOutputSink(OutputSink):
     def pass_pixels(self, kind: int) -> np.ndarray:
         return self.tiles[kind].pixels
 
+    def write_pfm(self, kind: int, path) -> None:
+        """io::write_pfm of the pass (include/psycles/io/image.h:63)."""
+        write_pfm(self.tiles[kind].pixels, path)
+
+
+def write_pfm(pixels: np.ndarray, path) -> None:
+    """A pass image as a Portable Float Map, as io::write_pfm writes it
+    (src/io/image.cpp:156-197): "PF" with the first three channels of a pass
+    of three or more, else "Pf" with the first; scale -1.0 (little-endian
+    floats); rows from the bottom of the image to the top.  `pixels` is
+    [height, width, channels], top row first."""
+    img = np.asarray(pixels, dtype=np.float32)
+    if img.ndim == 2:
+        img = img[..., None]
+    h, w, c = img.shape
+    if w == 0 or h == 0 or c == 0:
+        raise ValueError("empty pass image")
+    color = c >= 3
+    body = img[::-1, :, :3] if color else img[::-1, :, :1]
+    with open(path, "wb") as f:
+        f.write(f"{'PF' if color else 'Pf'}\n{w} {h}\n-1.0\n".encode())
+        f.write(np.ascontiguousarray(body, dtype="<f4").tobytes())
+
 
 @dataclasses.dataclass
 class RenderDiagnostic:

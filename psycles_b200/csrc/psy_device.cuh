@@ -147,9 +147,11 @@ constexpr uint32_t kMaxClosureStack = 32u;
 
 // One allocated closure.  Diffuse closures keep their authored colour and
 // roughness for the Oren-Nayar evaluation (roughness below 1e-5: Lambert).
+// The in-scope closures have no Normal input, so every diffuse closure
+// shares the normalised shading normal (SurfaceClosures::normal) and a
+// transparent closure never reads one.
 struct PhysicalClosure {
     f3 weight;
-    f3 normal;
     float sample_weight;
     uint32_t op;
     f3 color;
@@ -157,6 +159,7 @@ struct PhysicalClosure {
 };
 
 struct SurfaceClosures {
+    f3 normal;  // the diffuse closures' normal
     PhysicalClosure c[kMaxClosures];
     uint32_t count;
     f3 emission;
@@ -333,7 +336,7 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
                                                 SurfaceClosures &out) {
     out.count = 0u;
     out.emission = mk3(0.0f);
-    const f3 closure_normal = safe_normalize(shading_normal, shading_normal);
+    out.normal = safe_normalize(shading_normal, shading_normal);
     walk_closures(s, m, [&](uint32_t op, f3 w, f3 color, float roughness) {
         if (op == PSY_CLOSURE_EMISSION) {
             out.emission = out.emission + w;
@@ -347,14 +350,12 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
         if (op == PSY_CLOSURE_DIFFUSE) {
             p.weight = bsdf_allocated_weight(w);
             p.sample_weight = closure_sample_weight(p.weight);
-            p.normal = closure_normal;
             if (!any_nonzero(p.weight)) return;
         } else {
             const float sw = closure_sample_weight(w);
             if (!(sw >= 1.0e-5f)) return;
             p.weight = w;
             p.sample_weight = sw;
-            p.normal = shading_normal;
         }
         out.c[out.count++] = p;
     });
@@ -426,17 +427,18 @@ __device__ __noinline__ float oren_nayar_g(float cosine) {
     return c < 1.0e-6f ? taylor : regular;
 }
 
-// diffuse_intensity (src/luisa/graph_surface_scattering.cpp:475-506): Lambert
-// below roughness 1e-5, else the energy-compensated Oren-Nayar model of
-// Cycles (single scattering plus a multiple-scattering term from the
-// clamped albedo).  `incoming` points to the viewer, `outgoing` to the light.
-__device__ __noinline__ f3 diffuse_intensity(const PhysicalClosure &c, f3 incoming, f3 outgoing) {
-    const float nl = maxf_(dot(c.normal, outgoing), 0.0f);
-    const float sigma = clampf_(c.roughness, 0.0f, 1.0f);
-    if (sigma < 1.0e-5f) return mk3(nl * kInvPi);
+// diffuse_intensity (src/luisa/graph_surface_scattering.cpp:475-506) of a
+// closure whose clamped roughness `sigma` is at least 1e-5: Cycles'
+// energy-compensated Oren-Nayar model (single scattering plus a multiple-
+// scattering term from the clamped albedo).  `n` is the closure normal,
+// `incoming` points to the viewer, `outgoing` to the light, nl = max(n.outgoing, 0).
+// Below the cutoff the intensity is Lambert's nl / pi, which the callers
+// evaluate inline.
+__device__ __noinline__ f3 oren_nayar_intensity(const PhysicalClosure &c, float sigma, f3 n, f3 incoming,
+                                                f3 outgoing, float nl) {
     const float a = 1.0f / (kPi + sigma * (kPi * 0.5f - 2.0f / 3.0f));
     const float b = sigma * a;
-    const float nv = maxf_(dot(c.normal, incoming), 0.0f);
+    const float nv = maxf_(dot(n, incoming), 0.0f);
     float t = dot(outgoing, incoming) - nl * nv;
     if (t > 0.0f) t = t / (maxf_(nl, nv) + 1.17549435e-38f);
     const float single_scatter = a + b * t;
@@ -454,9 +456,11 @@ __device__ __noinline__ f3 diffuse_intensity(const PhysicalClosure &c, f3 incomi
 }
 
 // surface_closure_evaluation_contribution + accumulator
-// (src/luisa/surface_closure_evaluation.cpp:71-438).  Out of line: the
-// shading kernel calls it for the light sample and for the BSDF sample, and
-// a single copy keeps the kernel's code within the instruction cache.
+// (src/luisa/surface_closure_evaluation.cpp:71-438).  Every diffuse closure
+// shares the closure normal, so the cosine, pdf and bump term are taken
+// once.  Out of line: the shading kernel calls it for the light sample and
+// for the BSDF sample, and a single copy keeps the kernel's code within the
+// instruction cache.
 __device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, f3 shading_normal, f3 incoming,
                                                     f3 outgoing_raw, uint32_t lobe_mask, int selected) {
     const f3 outgoing = safe_normalize(outgoing_raw, shading_normal);
@@ -464,18 +468,22 @@ __device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, f3
     float total = 0.0f, weighted_pdf = 0.0f;
     const bool diffuse_enabled = (lobe_mask & kEventDiffuse) != 0u;
     const bool transparent_enabled = (lobe_mask & kEventTransparent) != 0u;
+    const f3 n = s.normal;
+    const float nl = maxf_(dot(n, outgoing), 0.0f);
+    const float bump = bump_shadowing(shading_normal, n, outgoing);
+    const float lambert = nl * kInvPi;
     for (uint32_t i = 0; i < s.count; ++i) {
         const PhysicalClosure &c = s.c[i];
         if (c.op == PSY_CLOSURE_TRANSPARENT) {
             if (transparent_enabled) total += c.sample_weight;
             continue;
         }
-        const float bump = bump_shadowing(shading_normal, c.normal, outgoing);
         const bool pdf_valid = bump != 0.0f || int(i) == selected;
-        float pdf = maxf_(dot(c.normal, outgoing), 0.0f) * kInvPi;
-        if (!pdf_valid) pdf = 0.0f;
+        const float pdf = pdf_valid ? lambert : 0.0f;
         if (!diffuse_enabled) continue;
-        const f3 value = c.weight * diffuse_intensity(c, incoming, outgoing) * bump;
+        const float sigma = clampf_(c.roughness, 0.0f, 1.0f);
+        const f3 intensity = sigma < 1.0e-5f ? mk3(lambert) : oren_nayar_intensity(c, sigma, n, incoming, outgoing, nl);
+        const f3 value = c.weight * intensity * bump;
         e.f = e.f + value;
         total += c.sample_weight;
         weighted_pdf += c.sample_weight * pdf;
@@ -526,7 +534,7 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
     if (chosen < 0) return out;
     const PhysicalClosure c = s.c[chosen];
     const bool transparent = c.op == PSY_CLOSURE_TRANSPARENT;
-    const f3 direction = transparent ? -incoming : sample_cosine_hemisphere(c.normal, u_dir, nullptr);
+    const f3 direction = transparent ? -incoming : sample_cosine_hemisphere(s.normal, u_dir, nullptr);
     out.closure_index = uint32_t(chosen);
     out.wi = direction;
     if (!(transparent || dot(geometric_normal, direction) > 0.0f)) return out;
@@ -557,7 +565,7 @@ __device__ __forceinline__ void surface_aov(const SurfaceClosures &s, f3 shading
         if (c.op == PSY_CLOSURE_DIFFUSE) {
             albedo = albedo + c.weight;
             const float w = closure_sample_weight(c.weight);
-            n = n + c.normal * w;
+            n = n + s.normal * w;
             total += w;
         } else {
             transparency = transparency + c.weight;

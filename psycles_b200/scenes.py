@@ -540,6 +540,85 @@ def value_graph_scene(seed: int = 0) -> Scene:
     return base
 
 
+def _f32_view(eye, target) -> np.ndarray:
+    """Camera-to-world matrix looking from `eye` at `target` (+y up, camera
+    space -z forward), evaluated in float32 in the order a C++ float
+    implementation takes: unit(v) = v * (1 / sqrt(max(dot(v, v), 1e-20)))."""
+    f = np.float32
+
+    def unit(v):
+        d = f(v[0] * v[0]) + f(v[1] * v[1])
+        d = f(d + f(v[2] * v[2]))
+        s = f(f(1.0) / f(np.sqrt(max(d, f(1e-20)))))
+        return [f(v[0] * s), f(v[1] * s), f(v[2] * s)]
+
+    def cross(a, b):
+        return [f(f(a[1] * b[2]) - f(a[2] * b[1])), f(f(a[2] * b[0]) - f(a[0] * b[2])),
+                f(f(a[0] * b[1]) - f(a[1] * b[0]))]
+
+    e = [f(v) for v in eye]
+    t = [f(v) for v in target]
+    forward = unit([f(t[i] - e[i]) for i in range(3)])
+    right = unit(cross(forward, [f(0), f(1), f(0)]))
+    back = [-forward[0], -forward[1], -forward[2]]
+    up = unit(cross(back, right))
+    m = np.eye(4, dtype=np.float32)
+    m[:3, 0], m[:3, 1], m[:3, 2], m[:3, 3] = right, up, back, e
+    return m
+
+
+def luisa_demo_scene(graph_material: bool = False) -> Scene:
+    """The Cornell-style room of the reference's Luisa demo
+    (examples/render_luisa_demo.cpp:203-305) in this scene model: a floor and
+    three walls in one mesh with per-triangle materials, a cube scaled to a
+    block, rough diffuse plaster / red / green / blue, a 1.8 m square area
+    light under the open ceiling and a background light, 47 degree camera.
+    With `graph_material` the block's colour is an RGB-node mix and its
+    roughness float math, as tests/adapter/adapter_probe.cpp builds them."""
+    f = np.float32
+    graphs = [diffuse_material((0.72, 0.72, 0.72), 0.35), diffuse_material((0.72, 0.06, 0.035), 0.45),
+              diffuse_material((0.04, 0.54, 0.12), 0.45)]
+    if graph_material:
+        g = ShaderGraph()
+        color = g.mix_color(0.3, g.rgb((0.035, 0.18, 0.85)), g.rgb((0.9, 0.5, 0.1)))
+        g.set_output(g.diffuse_bsdf(color, g.math("clamp", g.math("multiply", g.value(0.6), 0.5))))
+        graphs.append(g)
+    else:
+        graphs.append(diffuse_material((0.035, 0.18, 0.85), 0.16))
+    mats = _materials(graphs)
+
+    def quads(qs):
+        pos, idx = [], []
+        for q in qs:
+            b = len(pos)
+            pos += q
+            idx += [(b, b + 1, b + 2), (b, b + 2, b + 3)]
+        return np.array(pos, np.float32), np.array(idx, np.uint32)
+
+    rp, ri = quads([[(-3, 0, 2.5), (3, 0, 2.5), (3, 0, -3), (-3, 0, -3)],
+                    [(-3, 0, -3), (3, 0, -3), (3, 4.5, -3), (-3, 4.5, -3)],
+                    [(-3, 0, 2.5), (-3, 0, -3), (-3, 4.5, -3), (-3, 4.5, 2.5)],
+                    [(3, 0, -3), (3, 0, 2.5), (3, 4.5, 2.5), (3, 4.5, -3)]])
+    cp, ci = quads([[(-1, -1, 1), (1, -1, 1), (1, 1, 1), (-1, 1, 1)],
+                    [(1, -1, -1), (-1, -1, -1), (-1, 1, -1), (1, 1, -1)],
+                    [(-1, -1, -1), (-1, -1, 1), (-1, 1, 1), (-1, 1, -1)],
+                    [(1, -1, 1), (1, -1, -1), (1, 1, -1), (1, 1, 1)],
+                    [(-1, 1, 1), (1, 1, 1), (1, 1, -1), (-1, 1, -1)]])
+    meshes = [Mesh(rp, ri, materials=np.array([0, 0, 0, 0, 1, 1, 2, 2], np.uint32)), Mesh(cp, ci)]
+    block = np.eye(4, dtype=np.float32)
+    block[0, 0], block[1, 1], block[2, 2] = f(0.72), f(1.15), f(0.72)
+    block[:3, 3] = [f(0.35), f(1.15), f(-0.55)]
+    instances = [Instance(0, 0), Instance(1, 3, block)]
+    pi = f(3.14159265358979323846)
+    fov = f(f(f(47.0) * pi) / f(180.0))
+    cam = Camera(_f32_view((0.0, 2.05, 7.0), (0.0, 1.5, -0.8)), float(fov), float(fov), 2, near_clip=1.0e-3,
+                 far_clip=100.0)
+    light = Light(_abi.LIGHT_AREA, (1.0, 0.82, 0.62), 18.0, position=(-0.4, 4.25, -0.6), axis_x=(1, 0, 0),
+                  axis_y=(0, 0, 1), axis_z=(0, 1, 0), radius=1.8, size_u=1.8, size_v=1.8, spread=float(pi),
+                  spot_smooth=0.15, flags=_abi.LIGHT_FLAG_NORMALIZE | _abi.LIGHT_FLAG_SPHERE)
+    return Scene(meshes, instances, mats, [light], cam, background=(0.008, 0.012, 0.025))
+
+
 def render_settings(width: int, height: int, max_bounces: int = 4, seed: int = 0, **overrides) -> _abi.RenderSettings:
     s = _abi.default_settings()
     s.full_width, s.full_height = width, height
