@@ -294,11 +294,16 @@ __device__ __forceinline__ float input_scalar(const SceneView &s, const Material
     return eval_value(s, m, ref & ~PSY_INPUT_VALUE).x;
 }
 
+// Leaf kinds a closure walk reports (kLeaves of walk_closures).
+constexpr uint32_t kLeafDiffuse = 1u, kLeafTransparent = 2u, kLeafEmission = 4u, kLeafAll = 7u;
+
 // Visits closure leaves depth-first, `a` before `b`, with the add / mix
-// weight rule; `visit(op, weight, color, roughness)` receives diffuse /
-// transparent / emission leaves with their authored colour (x strength for
-// emission) and, for diffuse, the roughness input.
-template <typename Visit>
+// weight rule; `visit(op, weight, color, roughness)` receives the diffuse /
+// transparent / emission leaves selected by kLeaves with their authored
+// colour (x strength for emission) and, for diffuse, the roughness input.
+// Unselected leaves read no inputs (a shadow ray's extinction needs only
+// the transparent ones).
+template <uint32_t kLeaves = kLeafAll, typename Visit>
 __device__ __forceinline__ void walk_closures(const SceneView &s, const MaterialGpu &m, Visit visit) {
     uint32_t stack_id[kMaxClosureStack];
     float stack_w[kMaxClosureStack];
@@ -321,11 +326,17 @@ __device__ __forceinline__ void walk_closures(const SceneView &s, const Material
             const float f = clampf_(input_scalar(s, m, c.scalar), 0.0f, 1.0f);
             stack_id[sp] = c.b; stack_w[sp] = w * f; ++sp;
             stack_id[sp] = c.a; stack_w[sp] = w * (1.0f - f); ++sp;
-        } else if (c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_TRANSPARENT) {
-            const f3 color = input_vector(s, m, c.color);
-            const float roughness = c.op == PSY_CLOSURE_DIFFUSE ? input_scalar(s, m, c.roughness) : 0.0f;
-            visit(c.op, color * w, color, roughness);
-        } else if (c.op == PSY_CLOSURE_EMISSION) {
+        } else if (c.op == PSY_CLOSURE_DIFFUSE) {
+            if constexpr ((kLeaves & kLeafDiffuse) != 0u) {
+                const f3 color = input_vector(s, m, c.color);
+                visit(c.op, color * w, color, input_scalar(s, m, c.roughness));
+            }
+        } else if (c.op == PSY_CLOSURE_TRANSPARENT) {
+            if constexpr ((kLeaves & kLeafTransparent) != 0u) {
+                const f3 color = input_vector(s, m, c.color);
+                visit(c.op, color * w, color, 0.0f);
+            }
+        } else if (c.op == PSY_CLOSURE_EMISSION && (kLeaves & kLeafEmission) != 0u) {
             const f3 color = input_vector(s, m, c.color) * input_scalar(s, m, c.scalar);
             visit(c.op, color * w, color, 0.0f);
         }
@@ -363,7 +374,7 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
 
 __device__ __forceinline__ f3 material_emission(const SceneView &s, const MaterialGpu &m) {
     f3 r = mk3(0.0f);
-    walk_closures(s, m, [&](uint32_t op, f3 w, f3, float) {
+    walk_closures<kLeafEmission>(s, m, [&](uint32_t op, f3 w, f3, float) {
         if (op == PSY_CLOSURE_EMISSION) r = r + w;
     });
     return r;
@@ -372,7 +383,7 @@ __device__ __forceinline__ f3 material_emission(const SceneView &s, const Materi
 // transparent_extinction (src/luisa/graph_surface_implementation.cpp:354-372).
 __device__ __forceinline__ f3 transparent_extinction(const SceneView &s, const MaterialGpu &m) {
     f3 r = mk3(0.0f);
-    walk_closures(s, m, [&](uint32_t op, f3 w, f3, float) {
+    walk_closures<kLeafTransparent>(s, m, [&](uint32_t op, f3 w, f3, float) {
         if (op == PSY_CLOSURE_TRANSPARENT && closure_sample_weight(w) >= 1.0e-5f) r = r + w;
     });
     return r;
@@ -730,6 +741,7 @@ __device__ __forceinline__ SlabRay make_slab_ray(f3 o, f3 raw) {
 // visitor requests) that is neither the source nor the light identity is
 // handed to `on_hit(instance, local, cycles_prim, t, u, v)`; a true return
 // ends the traversal.
+#if PSY_BVH_WIDTH != 8
 struct TraversalState {
     Ray ray;      // world ray
     SlabRay cur;  // slab ray of the current level
@@ -880,6 +892,182 @@ __device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneVi
     }
     return false;
 }
+
+#else  // PSY_BVH_WIDTH == 8
+
+// Group-stack traversal of the compressed 8-wide trees (after Ylitie,
+// Karras and Laine 2017).  A visit tests the node's eight quantised boxes
+// one child at a time (one FMA per plane after a per-node change of
+// variables), tests hit leaf triangles at once, and continues into the hit
+// inner child of lowest octant-remapped bit (near first for the ray's
+// direction octant), leaving the node's other hit children as ONE stack
+// entry (base, hit bits, inner mask).  In the TLAS the hit instances are
+// entered one by one from an instance-group entry, each behind a marker
+// that returns to the world ray.  Every triangle whose box the ray reaches
+// within [tmin, tmax] is tested, as in the 4-wide traversal, so the closest
+// hit does not depend on the order.
+constexpr int kStackSize8 = int(kTraversalStackSize8);
+constexpr uint32_t kNoNode = 0xffffffffu;
+
+struct TraversalState {
+    Ray ray;      // world ray
+    SlabRay cur;  // slab ray of the current level
+    float tmax;
+    uint32_t node, sp, inst, prim_offset;  // node: tagged node to visit, or kNoNode (pop)
+    uint32_t visibility, src_obj, src_prim, light_obj, light_prim;
+    uint2 stack[kStackSize8];  // x: tag | base index, y: hit bits (0-7) | child or leaf mask (8-15)
+};
+
+__device__ __forceinline__ void traversal_begin(TraversalState &t, const SceneView &s, const Ray &ray,
+                                                uint32_t visibility, uint32_t src_obj, uint32_t src_prim,
+                                                uint32_t light_obj, uint32_t light_prim) {
+    t.ray = ray;
+    t.cur = make_slab_ray(ray.o, ray.d);
+    t.tmax = ray.tmax;
+    t.node = s.instance_count == 0u ? kNoNode : kTagTlas;
+    t.sp = 0u;
+    t.inst = kInvalid;
+    t.prim_offset = 0u;
+    t.visibility = visibility;
+    t.src_obj = src_obj;
+    t.src_prim = src_prim;
+    t.light_obj = light_obj;
+    t.light_prim = light_prim;
+}
+
+__device__ __forceinline__ void stack_push8(TraversalState &t, uint32_t x, uint32_t y) {
+    if (t.sp < uint32_t(kStackSize8)) t.stack[t.sp++] = make_uint2(x, y);
+}
+
+// Enters instance `i` (object-space slab ray, return marker) when the ray
+// may see it; otherwise the next entry is popped.
+__device__ __forceinline__ void enter_instance8(TraversalState &t, const SceneView &s, uint32_t i) {
+    const InstanceGpu &in = s.instances[i];
+    if ((in.visibility & t.visibility) == 0u) {
+        t.node = kNoNode;
+        return;
+    }
+    const MeshGpu mesh = s.meshes[in.mesh];
+    const Xform w2o = load_xform(in.w2o);
+    t.cur = make_slab_ray(xform_point(w2o, t.ray.o), xform_direction(w2o, t.ray.d));
+    t.inst = i;
+    t.prim_offset = mesh.prim_offset;
+    stack_push8(t, kTagLeave, 0u);
+    t.node = kTagBlas | mesh.node_offset;
+}
+
+__device__ __forceinline__ uint32_t below(uint32_t mask, uint32_t bit) { return __popc(mask & ((1u << bit) - 1u)); }
+
+// Advances at most `budget` loop iterations; true once the traversal ended.
+// The octant order serves closest-hit and any-hit queries alike.
+template <bool kNearFirst = true, typename OnHit>
+__device__ __forceinline__ bool traversal_steps(TraversalState &t, const SceneView &s, int budget, OnHit on_hit) {
+    for (int it = 0; it < budget; ++it) {
+        if (t.node == kNoNode) {
+            if (t.sp == 0u) return true;
+            const uint2 e = t.stack[t.sp - 1u];
+            const uint32_t tag = e.x & kTagMask;
+            if (tag == kTagLeave) {
+                t.cur = make_slab_ray(t.ray.o, t.ray.d);
+                t.inst = kInvalid;
+                --t.sp;
+                continue;
+            }
+            const uint32_t bits = e.y & 0xffu, mask = (e.y >> 8) & 0xffu;
+            const uint32_t b = uint32_t(__ffs(int(bits)) - 1);
+            const uint32_t rest = bits & (bits - 1u);
+            if (rest != 0u) t.stack[t.sp - 1u].y = rest | (mask << 8);
+            else --t.sp;
+            if (tag == kTagInstance) {
+                enter_instance8(t, s, s.tlas_ids[(e.x & ~kTagMask) + below(mask, b)]);
+            } else {
+                t.node = tag | ((e.x & ~kTagMask) + below(mask, b ^ t.cur.neg));
+            }
+            continue;
+        }
+        const uint32_t tag = t.node & kTagMask;
+        const bool blas = tag == kTagBlas;
+        const float4 *np = reinterpret_cast<const float4 *>((blas ? s.blas8 : s.tlas8) + (t.node & ~kTagMask));
+        const float4 w0 = __ldg(np);
+        const uint4 w1 = __ldg(reinterpret_cast<const uint4 *>(np + 1));
+        const uint4 w2 = __ldg(reinterpret_cast<const uint4 *>(np + 2));
+        const uint4 w3 = __ldg(reinterpret_cast<const uint4 *>(np + 3));
+        const uint4 w4 = __ldg(reinterpret_cast<const uint4 *>(np + 4));
+        const uint32_t em = __float_as_uint(w0.w);
+        const uint32_t imask = em >> 24, leafmask = w1.z;
+        // slab distances of child k: t = q * (cell * inv) + (p - o) * inv
+        const SlabRay &r = t.cur;
+        const float ax = __uint_as_float((em & 0xffu) << 23) * r.inv.x;
+        const float ay = __uint_as_float(((em >> 8) & 0xffu) << 23) * r.inv.y;
+        const float az = __uint_as_float(((em >> 16) & 0xffu) << 23) * r.inv.z;
+        const float bx = (w0.x - r.o.x) * r.inv.x;
+        const float by = (w0.y - r.o.y) * r.inv.y;
+        const float bz = (w0.z - r.o.z) * r.inv.z;
+        // near / far byte planes by direction sign: lo x (w2.x, w2.y), lo y
+        // (w2.z, w2.w), lo z (w3.x, w3.y), hi x (w3.z, w3.w), hi y (w4.x,
+        // w4.y), hi z (w4.z, w4.w)
+        const bool nx = (r.neg & 1u) != 0u, ny = (r.neg & 2u) != 0u, nz = (r.neg & 4u) != 0u;
+        const uint32_t nx0 = nx ? w3.z : w2.x, nx1 = nx ? w3.w : w2.y, fx0 = nx ? w2.x : w3.z, fx1 = nx ? w2.y : w3.w;
+        const uint32_t ny0 = ny ? w4.x : w2.z, ny1 = ny ? w4.y : w2.w, fy0 = ny ? w2.z : w4.x, fy1 = ny ? w2.w : w4.y;
+        const uint32_t nz0 = nz ? w4.z : w3.x, nz1 = nz ? w4.w : w3.y, fz0 = nz ? w3.x : w4.z, fz1 = nz ? w3.y : w4.w;
+        const uint32_t occupied = imask | leafmask;
+        uint32_t hit_inner = 0u, hit_leaf = 0u;
+        const float tmin = t.ray.tmin, tmax = t.tmax;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (((occupied >> k) & 1u) == 0u) continue;
+            const int sh = 8 * (k & 3);
+            const bool hi_word = k >= 4;
+            const float qnx = float(((hi_word ? nx1 : nx0) >> sh) & 0xffu);
+            const float qfx = float(((hi_word ? fx1 : fx0) >> sh) & 0xffu);
+            const float qny = float(((hi_word ? ny1 : ny0) >> sh) & 0xffu);
+            const float qfy = float(((hi_word ? fy1 : fy0) >> sh) & 0xffu);
+            const float qnz = float(((hi_word ? nz1 : nz0) >> sh) & 0xffu);
+            const float qfz = float(((hi_word ? fz1 : fz0) >> sh) & 0xffu);
+            const float nr = fmaxf(fmaxf(fmaf(qnx, ax, bx), fmaf(qny, ay, by)), fmaxf(fmaf(qnz, az, bz), tmin));
+            const float fr = fminf(fminf(fmaf(qfx, ax, bx), fmaf(qfy, ay, by)), fminf(fmaf(qfz, az, bz), tmax));
+            if (nr <= fmaxf(fmaf(fr, 1.00000095367431640625f, 1.0e-30f), fr)) {
+                if ((imask >> k) & 1u) hit_inner |= 1u << (uint32_t(k) ^ r.neg);
+                else hit_leaf |= 1u << k;
+            }
+        }
+        if (blas) {
+            // leaves first: their triangles may shrink tmax
+            while (hit_leaf != 0u) {
+                const uint32_t k = uint32_t(__ffs(int(hit_leaf)) - 1);
+                hit_leaf &= hit_leaf - 1u;
+                const float4 *tp = s.tris + 3u * (w1.y + below(leafmask, k));
+                const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                const uint32_t local = __float_as_uint(a.w);
+                const uint32_t cp = t.prim_offset + local;
+                if ((t.src_obj == t.inst && t.src_prim == cp) || (t.light_obj == t.inst && t.light_prim == cp)) continue;
+                float th, u, v;
+                if (!intersect_triangle(t.cur.o, t.cur.d, t.ray.tmin, t.tmax, ld3(a), ld3(b), ld3(c), th, u, v))
+                    continue;
+                if (on_hit(t.inst, local, cp, th, u, v)) return true;
+            }
+        } else if (hit_leaf != 0u) {
+            // TLAS: stack the inner hits, then enter the hit instances one by one
+            if (hit_inner != 0u) stack_push8(t, kTagTlas | w1.x, hit_inner | (imask << 8));
+            const uint32_t k = uint32_t(__ffs(int(hit_leaf)) - 1);
+            const uint32_t rest = hit_leaf & (hit_leaf - 1u);
+            if (rest != 0u) stack_push8(t, kTagInstance | w1.y, rest | (leafmask << 8));
+            enter_instance8(t, s, s.tlas_ids[w1.y + below(leafmask, k)]);
+            continue;
+        }
+        if (hit_inner == 0u) {
+            t.node = kNoNode;
+            continue;
+        }
+        const uint32_t b = uint32_t(__ffs(int(hit_inner)) - 1);
+        const uint32_t rest = hit_inner & (hit_inner - 1u);
+        if (rest != 0u) stack_push8(t, tag | w1.x, rest | (imask << 8));
+        t.node = tag | (w1.x + below(imask, b ^ r.neg));
+    }
+    return false;
+}
+
+#endif  // PSY_BVH_WIDTH
 
 // Whole traversal in one call.
 template <typename OnHit>

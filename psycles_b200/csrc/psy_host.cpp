@@ -645,6 +645,133 @@ struct Builder {
         return index;
     }
 
+    // The compressed 8-wide BVH of the binary nodes: each node takes up to
+    // eight children by opening the inner child of largest area (as
+    // collapse does for four), assigns them to slots by octant, and
+    // quantises their padded boxes outward onto a per-node byte grid.  Nodes
+    // are emitted breadth first, so a node's inner children are contiguous;
+    // `leaves` receives each node's leaf entries (binary leaf: prim index;
+    // TLAS: instance id) in slot order, which is the order their records
+    // must be laid out in.  Indices are relative to the tree.
+    std::vector<psy::CwNodeGpu> widen8(std::vector<uint32_t> &leaves) const {
+        std::vector<psy::CwNodeGpu> out(1);
+        leaves.clear();
+        std::vector<std::pair<int, uint32_t>> queue{{0, 0u}};  // (binary node, output node)
+        for (size_t j = 0; j < queue.size(); ++j) {
+            WideChild kids[8] = {child_of(queue[j].first, 0), child_of(queue[j].first, 1)};
+            int n = 2;
+            while (n < 8) {
+                int best = -1;
+                double best_area = -2.0;
+                for (int k = 0; k < n; ++k)
+                    if (kids[k].link >= 0 && kids[k].area() > best_area) {
+                        best = k;
+                        best_area = kids[k].area();
+                    }
+                if (best < 0) break;
+                const int inner = kids[best].link;
+                kids[best] = child_of(inner, 0);
+                kids[n++] = child_of(inner, 1);
+            }
+            // drop empty children (no link, no triangles)
+            int m = 0;
+            for (int k = 0; k < n; ++k)
+                if (kids[k].link >= 0 || kids[k].count > 0) kids[m++] = kids[k];
+            n = m;
+            // node box and slot assignment: slot s takes the child whose
+            // centre lies furthest against direction octant s, greedily by
+            // the most negative projection first
+            double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+            for (int k = 0; k < n; ++k)
+                for (int a = 0; a < 3; ++a) {
+                    lo[a] = std::min(lo[a], double(kids[k].lo[a]));
+                    hi[a] = std::max(hi[a], double(kids[k].hi[a]));
+                }
+            int slot_of[8];
+            {
+                bool used_child[8] = {}, used_slot[8] = {};
+                double cost[8][8];
+                for (int k = 0; k < n; ++k)
+                    for (int s = 0; s < 8; ++s) {
+                        double c = 0.0;
+                        for (int a = 0; a < 3; ++a) {
+                            const double d = 0.5 * (double(kids[k].lo[a]) + kids[k].hi[a]) - 0.5 * (lo[a] + hi[a]);
+                            c += ((s >> a) & 1) ? -d : d;
+                        }
+                        cost[k][s] = c;
+                    }
+                for (int step = 0; step < n; ++step) {
+                    int bk = -1, bs = -1;
+                    for (int k = 0; k < n; ++k)
+                        for (int s = 0; s < 8; ++s)
+                            if (!used_child[k] && !used_slot[s] && (bk < 0 || cost[k][s] < cost[bk][bs])) {
+                                bk = k;
+                                bs = s;
+                            }
+                    used_child[bk] = used_slot[bs] = true;
+                    slot_of[bk] = bs;
+                }
+            }
+            int child_in_slot[8];
+            for (int s = 0; s < 8; ++s) child_in_slot[s] = -1;
+            for (int k = 0; k < n; ++k) child_in_slot[slot_of[k]] = k;
+            // quantisation grid: origin below the node box by a margin that
+            // covers the slab test's float rounding (relative to the node's
+            // extent and magnitude), power-of-two cells of 255 steps
+            psy::CwNodeGpu node{};
+            double origin[3], cell[3], margin[3];
+            uint32_t exps = 0u;
+            for (int a = 0; a < 3; ++a) {
+                if (n == 0) {
+                    lo[a] = hi[a] = 0.0;
+                }
+                margin[a] = 4e-6 * (hi[a] - lo[a]) + 4e-6 * std::max(std::fabs(lo[a]), std::fabs(hi[a])) + 1e-30;
+                const float p = std::nextafter(float(lo[a] - margin[a]), -INFINITY);
+                origin[a] = double(p);
+                const double span = (hi[a] + margin[a]) - origin[a];
+                int e = int(std::ceil(std::log2(std::max(span, 1e-300) / 255.0)));
+                e = std::max(e, -126);
+                while (std::ldexp(255.0, e) < span) ++e;
+                cell[a] = std::ldexp(1.0, e);
+                exps |= uint32_t(e + 127) << (8 * a);
+            }
+            node.px = float(origin[0]);
+            node.py = float(origin[1]);
+            node.pz = float(origin[2]);
+            uint32_t imask = 0u, leafmask = 0u;
+            for (int s = 0; s < 8; ++s) {
+                const int k = child_in_slot[s];
+                if (k < 0) continue;
+                if (kids[k].link >= 0) imask |= 1u << s;
+                else leafmask |= 1u << s;
+                for (int a = 0; a < 3; ++a) {
+                    const double ql = std::floor(((double(kids[k].lo[a]) - margin[a]) - origin[a]) / cell[a]);
+                    const double qh = std::ceil(((double(kids[k].hi[a]) + margin[a]) - origin[a]) / cell[a]);
+                    const uint32_t bl = uint32_t(std::min(std::max(ql, 0.0), 255.0));
+                    const uint32_t bh = uint32_t(std::min(std::max(qh, 0.0), 255.0));
+                    node.q[2 * a + (s >> 2)] |= bl << (8 * (s & 3));
+                    node.q[6 + 2 * a + (s >> 2)] |= bh << (8 * (s & 3));
+                }
+            }
+            node.exps_imask = exps | (imask << 24);
+            node.leafmask = leafmask;
+            node.child_base = uint32_t(out.size());
+            node.leaf_base = uint32_t(leaves.size());
+            for (int s = 0; s < 8; ++s) {
+                const int k = child_in_slot[s];
+                if (k < 0) continue;
+                if (kids[k].link >= 0) {
+                    queue.push_back({kids[k].link, uint32_t(out.size())});
+                    out.push_back({});
+                } else {
+                    leaves.push_back(uint32_t(~kids[k].link));
+                }
+            }
+            out[queue[j].second] = node;
+        }
+        return out;
+    }
+
     // Root node: a single leaf still gets a two-child root (empty right).
     Box build_root() {
         nodes.clear();
@@ -702,6 +829,40 @@ uint32_t blas_stack_need(const std::vector<psy::WideNodeGpu> &w) {
         need[i] = n > 0 ? uint32_t(n - 1) + deepest : 0u;
     }
     return w.empty() ? 0u : need[0];
+}
+
+// The same bounds for the compressed 8-wide trees, whose traversal keeps
+// one stack entry per node group: a visit that continues into one of n hit
+// inner children leaves the other n - 1 as one entry (so one entry when
+// n >= 2).  In the TLAS a node with hit instances first stacks its inner
+// hits (one entry when it has any), then the other hit instances (one entry
+// when there are two or more) and the return to the world ray.
+uint32_t blas_stack_need8(const std::vector<psy::CwNodeGpu> &w) {
+    std::vector<uint32_t> need(w.size(), 0u);
+    for (size_t i = w.size(); i-- > 0;) {
+        const uint32_t imask = w[i].exps_imask >> 24;
+        const uint32_t n = uint32_t(__builtin_popcount(imask));
+        uint32_t deepest = 0u;
+        for (uint32_t k = 0; k < n; ++k) deepest = std::max(deepest, need[w[i].child_base + k]);
+        need[i] = n > 0 ? (n >= 2 ? 1u : 0u) + deepest : 0u;
+    }
+    return w.empty() ? 0u : need[0];
+}
+
+std::vector<uint32_t> tlas_instance_depths8(const std::vector<psy::CwNodeGpu> &w, const std::vector<uint32_t> &leaves,
+                                            uint32_t instance_count) {
+    std::vector<uint32_t> depth(w.size(), 0u), inst(instance_count, 0u);
+    for (size_t i = 0; i < w.size(); ++i) {
+        const uint32_t imask = w[i].exps_imask >> 24, leafmask = w[i].leafmask;
+        const uint32_t ni = uint32_t(__builtin_popcount(imask)), nl = uint32_t(__builtin_popcount(leafmask));
+        for (uint32_t k = 0; k < ni; ++k) depth[w[i].child_base + k] = depth[i] + (ni >= 2 ? 1u : 0u);
+        const uint32_t entered = depth[i] + (ni > 0 ? 1u : 0u) + (nl >= 2 ? 1u : 0u);
+        for (uint32_t k = 0; k < nl; ++k) {
+            const uint32_t id = leaves[w[i].leaf_base + k];
+            if (id < instance_count) inst[id] = entered;
+        }
+    }
+    return inst;
 }
 
 // Entries waiting on the stack when each instance of the TLAS is entered
@@ -1387,6 +1548,8 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     std::vector<float4> tris;
     std::vector<Box> mesh_boxes(d->mesh_count);
     std::vector<std::vector<psy::WideNodeGpu>> mesh_wide(d->mesh_count);
+    std::vector<std::vector<psy::CwNodeGpu>> mesh_cw(d->mesh_count);
+    std::vector<psy::CwNodeGpu> blas8;
     // triangle records in BVH leaf order, written by each mesh's build at
     // the mesh's offset (meshes in input order)
     std::vector<uint64_t> mesh_tri_first(d->mesh_count + 1u, 0u);
@@ -1409,18 +1572,26 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
             p.id = k;
         }
         mesh_boxes[i] = bld.build_root();
-        mesh_wide[i] = bld.widen();
-        mesh_need[i] = blas_stack_need(mesh_wide[i]);
         float4 *out = tris.data() + 3u * mesh_tri_first[i];
-        for (const Prim &p : bld.prims) {
-            const uint32_t id = p.id;
+        auto put = [&](uint32_t id) {
             for (int c = 0; c < 3; ++c) {
                 const float *v = m.positions + 3ull * m.indices[3ull * id + c];
                 float w = 0.0f;
                 if (c == 0) std::memcpy(&w, &id, 4);
                 *out++ = make_float4(v[0], v[1], v[2], w);
             }
-        }
+        };
+#if PSY_BVH_WIDTH == 8
+        // triangle records in the slot order of the 8-wide leaves
+        std::vector<uint32_t> leaves;
+        mesh_cw[i] = bld.widen8(leaves);
+        mesh_need[i] = blas_stack_need8(mesh_cw[i]);
+        for (const uint32_t leaf : leaves) put(bld.prims[leaf].id);
+#else
+        mesh_wide[i] = bld.widen();
+        mesh_need[i] = blas_stack_need(mesh_wide[i]);
+        for (const Prim &p : bld.prims) put(p.id);
+#endif
     };
     {
         std::vector<uint32_t> by_size(d->mesh_count);
@@ -1505,9 +1676,24 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     // with median splits only (balanced: about 3 entries per two binary
     // levels); a scene that still exceeds it is rejected, so no traversal
     // ever drops a subtree.
+#if PSY_BVH_WIDTH == 8
+    const uint32_t stack_cap = psy::kTraversalStackSize8;
+    std::vector<psy::WideNodeGpu> tl_wide(1);
+    std::vector<uint32_t> tl_leaves;
+    std::vector<psy::CwNodeGpu> tl_cw = tl.widen8(tl_leaves);
+    auto instance_depths = [&]() {
+        tl_cw = tl.widen8(tl_leaves);
+        return tlas_instance_depths8(tl_cw, tl_leaves, d->instance_count);
+    };
+#else
     const uint32_t stack_cap = psy::kTraversalStackSize;
     std::vector<psy::WideNodeGpu> tl_wide = tl.widen();
-    std::vector<uint32_t> inst_depth = tlas_instance_depths(tl_wide, d->instance_count);
+    auto instance_depths = [&]() {
+        tl_wide = tl.widen();
+        return tlas_instance_depths(tl_wide, d->instance_count);
+    };
+#endif
+    std::vector<uint32_t> inst_depth = instance_depths();
     auto tlas_depth = [&]() {
         uint32_t deepest = 0u;
         for (const Prim &p : tl.prims) deepest = std::max(deepest, inst_depth[p.id]);
@@ -1516,8 +1702,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     if (!tl.prims.empty() && tlas_depth() + 1u > stack_cap / 2u) {
         tl.sah_depth_limit = 0;
         tl.build_root();
-        tl_wide = tl.widen();
-        inst_depth = tlas_instance_depths(tl_wide, d->instance_count);
+        inst_depth = instance_depths();
     }
     auto mesh_budgets = [&]() {
         std::vector<uint32_t> budget(d->mesh_count, stack_cap);
@@ -1567,8 +1752,17 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         } else {
             g.material_offset = psy::kInvalidId;
         }
-        g.node_offset = uint32_t(blas.size());
         g.tri_offset = uint32_t(mesh_tri_first[i]);
+#if PSY_BVH_WIDTH == 8
+        g.node_offset = uint32_t(blas8.size());
+        for (psy::CwNodeGpu &w : mesh_cw[i]) {
+            w.child_base += g.node_offset;
+            w.leaf_base += g.tri_offset;
+        }
+        blas8.insert(blas8.end(), mesh_cw[i].begin(), mesh_cw[i].end());
+        std::vector<psy::CwNodeGpu>().swap(mesh_cw[i]);
+#endif
+        g.node_offset = PSY_BVH_WIDTH == 8 ? g.node_offset : uint32_t(blas.size());
         // global node and triangle indices of the mesh's links
         for (psy::WideNodeGpu &w : mesh_wide[i]) {
             int *lk = &w.link.x;
@@ -1585,6 +1779,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         sc->triangle_count += m.triangle_count;
     }
     if (blas.empty()) blas.push_back({});
+    if (blas8.empty()) blas8.push_back({});
 
     // ---- materials and parameter blocks
     std::vector<psy_closure_instruction> code;
@@ -1745,13 +1940,19 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     // device pool: a later compile reuses the memory a destroyed scene gave
     // back, and parameter blocks replaced by edits are retired without
     // waiting on the device.
-    for (DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tris, &sc->instances, &sc->meshes, &sc->positions, &sc->normals,
+    for (DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tlas8, &sc->blas8, &sc->tlas_ids, &sc->tris, &sc->instances, &sc->meshes, &sc->positions, &sc->normals,
                             &sc->indices, &sc->tri_materials, &sc->material_buf, &sc->code, &sc->value_buf, &sc->scalar_buf,
                             &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights, &sc->lamp_consts,
                             &sc->lamp_bounds, &sc->lamp_ids})
         b->ordered = st;
     PSY_CUDA_TRY(sc->tlas.upload(tl_wide, st));
     PSY_CUDA_TRY(sc->blas.upload(blas, st));
+#if PSY_BVH_WIDTH == 8
+    if (tl_leaves.empty()) tl_leaves.push_back(0u);
+    PSY_CUDA_TRY(sc->tlas8.upload(tl_cw, st));
+    PSY_CUDA_TRY(sc->blas8.upload(blas8, st));
+    PSY_CUDA_TRY(sc->tlas_ids.upload(tl_leaves, st));
+#endif
     PSY_CUDA_TRY(sc->tris.upload(tris, st));
     PSY_CUDA_TRY(sc->instances.upload(instances, st));
     PSY_CUDA_TRY(sc->meshes.upload(meshes, st));
@@ -1798,7 +1999,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->lamp_ids.upload(lamp_ids, st));
     PSY_CUDA_TRY(cudaStreamSynchronize(st));
     sc->stats.upload_bytes = 0u;
-    for (const DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tris, &sc->instances, &sc->meshes, &sc->positions,
+    for (const DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tlas8, &sc->blas8, &sc->tlas_ids, &sc->tris, &sc->instances, &sc->meshes, &sc->positions,
                                   &sc->normals, &sc->indices, &sc->tri_materials, &sc->material_buf, &sc->code,
                                   &sc->value_buf, &sc->scalar_buf, &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights,
                                   &sc->lamp_consts, &sc->lamp_bounds, &sc->lamp_ids})
@@ -1806,6 +2007,9 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     psy::SceneView &v = sc->view;
     v.tlas = sc->tlas.as<psy::WideNodeGpu>();
     v.blas = sc->blas.as<psy::WideNodeGpu>();
+    v.tlas8 = sc->tlas8.as<psy::CwNodeGpu>();
+    v.blas8 = sc->blas8.as<psy::CwNodeGpu>();
+    v.tlas_ids = sc->tlas_ids.as<uint32_t>();
     v.tris = sc->tris.as<float4>();
     v.instances = sc->instances.as<psy::InstanceGpu>();
     v.meshes = sc->meshes.as<psy::MeshGpu>();
@@ -2019,7 +2223,7 @@ psy_status psy_session_read_trace(psy_session *s, psy_path_trace *out) {
 
 uint64_t psy::host::scene_device_bytes(const psy_scene *s) {
     uint64_t n = 0u;
-    for (const DeviceBuffer *b : {&s->tlas, &s->blas, &s->tris, &s->instances, &s->meshes, &s->positions, &s->normals,
+    for (const DeviceBuffer *b : {&s->tlas, &s->blas, &s->tlas8, &s->blas8, &s->tlas_ids, &s->tris, &s->instances, &s->meshes, &s->positions, &s->normals,
                                   &s->indices, &s->tri_materials, &s->material_buf, &s->code, &s->value_buf, &s->scalar_buf,
                                   &s->vector_buf, &s->emitters, &s->distribution, &s->lights, &s->lamp_consts, &s->lamp_bounds,
                                   &s->lamp_ids, &s->lt_nodes, &s->lt_emitters, &s->lt_mapping, &s->lt_lookup})

@@ -153,7 +153,7 @@ struct psy_scene {
     psy_camera_desc camera{};
     std::vector<psy::MaterialGpu> materials;
     std::vector<float> scalars, vectors;
-    psy::host::DeviceBuffer tlas, blas, tris, instances, meshes, positions, normals, indices, tri_materials, material_buf, code,
+    psy::host::DeviceBuffer tlas, blas, tlas8, blas8, tlas_ids, tris, instances, meshes, positions, normals, indices, tri_materials, material_buf, code,
         value_buf, scalar_buf, vector_buf, emitters, distribution, lights, lamp_consts, lamp_bounds, lamp_ids, lt_nodes, lt_emitters,
         lt_mapping, lt_lookup;
     psy::SceneView view{};

@@ -53,6 +53,8 @@ constexpr uint32_t kTagMask = 3u << 30;
 // splits or rejecting the scene where needed; a debug build
 // (-DPSY_STACK_CHECK=1) also counts pushes that would not fit on the device.
 constexpr uint32_t kTraversalStackSize = 48u;
+// Entries (node groups) of the 8-wide traversal's stack.
+constexpr uint32_t kTraversalStackSize8 = 32u;
 
 // Four children of a wide BVH node: boxes as six planes of four lanes, and
 // per child either a ready stack entry (count 0: a tagged global node index
@@ -64,6 +66,27 @@ struct alignas(16) WideNodeGpu {
     int4 count;
 };
 static_assert(sizeof(WideNodeGpu) == 128, "wide BVH node is two 64-byte lines");
+
+// Compressed 8-wide BVH node (80 B, after Ylitie, Karras and Laine, "Efficient
+// Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs", HPG 2017):
+// the eight children's boxes as bytes on a per-node grid -- origin p and a
+// power-of-two cell 2^(e - 127) per axis -- rounded outward (plus a margin
+// that covers the float rounding of the slab test), so every dequantised
+// box contains the child's padded box.  Inner children are stored
+// contiguously from child_base in slot order, leaves (one triangle record,
+// or in the TLAS one instance id) contiguously from leaf_base in slot order.
+// Slots are assigned by octant: slot s holds the child nearest to a ray of
+// direction octant s (bit a set where component a is negative).
+struct alignas(16) CwNodeGpu {
+    float px, py, pz;
+    uint32_t exps_imask;  // ex | ey << 8 | ez << 16 | imask << 24 (imask bit k: slot k is an inner child)
+    uint32_t child_base;  // global index of the first inner child
+    uint32_t leaf_base;   // global index of the first leaf entry
+    uint32_t leafmask;    // bit k: slot k is a leaf
+    uint32_t pad;
+    uint32_t q[12];       // lo x, lo y, lo z, hi x, hi y, hi z: two words of eight bytes each, slot k in byte k
+};
+static_assert(sizeof(CwNodeGpu) == 80, "compressed 8-wide node is five 16-byte words");
 
 struct alignas(16) InstanceGpu {
     float o2w[12];  // column-major c0, c1, c2, c3 (xyz each)
@@ -118,9 +141,17 @@ struct alignas(16) LampConstGpu {
     float4 factors;  // x: point eval factor, y: distant cone one minus cosine, z: distant eval factor
 };
 
+// Width of the BVH the kernels traverse: 4 (WideNodeGpu) or 8 (CwNodeGpu).
+#ifndef PSY_BVH_WIDTH
+#define PSY_BVH_WIDTH 4
+#endif
+
 struct SceneView {
-    const WideNodeGpu *tlas;
+    const WideNodeGpu *tlas;  // 4-wide trees
     const WideNodeGpu *blas;
+    const CwNodeGpu *tlas8;   // compressed 8-wide trees
+    const CwNodeGpu *blas8;
+    const uint32_t *tlas_ids;  // instance id of each TLAS leaf entry (8-wide)
     const float4 *tris;
     const InstanceGpu *instances;
     const MeshGpu *meshes;

@@ -42,6 +42,11 @@ def assert_traces_match(gt, ot, where=None) -> None:
         for f in SCALARS + VECTORS:
             assert close(getattr(a, f), getattr(b, f)), (where, k, f, getattr(a, f), getattr(b, f))
     assert close(gt.radiance, ot.radiance), (where, list(gt.radiance), list(ot.radiance))
+    # the same pair as schema-v2 documents under the reference comparator's
+    # slot policies (psycles_b200.trace_schema)
+    from psycles_b200 import trace_schema
+    failures = trace_schema.compare(trace_schema.document(ot, "oracle"), trace_schema.document(gt, "cuda"))
+    assert failures == [], (where, failures)
 
 
 def assert_passes_match(session, film, passes, max_bit_mismatch=0.01) -> dict:
