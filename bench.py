@@ -2,6 +2,8 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
                     [--config procedural|cornell|many_light] [--spp S]
+    python bench.py --workload serving [--serving-jobs J] [--serving-scenes S] [--serving-rate R]
+    python bench.py --workload viewports
 
 Workload (default): the procedural mesh scene -- 64 seeded affine instances
 of 8 geodesic spheres (997,920 instanced fp32 triangles, smooth normals), 32
@@ -20,6 +22,14 @@ work shards by frame with no data-path collective (weak scaling).
 
 --impl reference times the reference path's CPU restatement (the oracle,
 all host threads) on a bounded row band of the same workload.
+
+The headline line also carries two secondary measurements on the same GPU:
+`viewports` (64 concurrent viewport renders, batched against sequential,
+after a one-knob-at-a-time tuning sweep) and `serving` (a Poisson job
+stream through the render server against one session per job; 64 jobs over
+16 resident scenes by default).  `--workload serving` / `--workload
+viewports` run only that measurement, at the --serving-* sizes or over the
+full 27-point tuning grid.
 """
 
 from __future__ import annotations
@@ -363,7 +373,8 @@ def run_cuda(args) -> None:
         line["kernels"] = kernel["kernels"]
     if args.serving and args.config == "procedural":
         line["viewports"] = run_viewports(backend, comp.scene)
-        line["serving"] = run_serving(backend)
+        line["serving"] = run_serving(backend, jobs=args.serving_jobs, rate=args.serving_rate,
+                                      scene_count=args.serving_scenes)
     if args.cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, scene)
     print(json.dumps(line), flush=True)
@@ -395,12 +406,20 @@ def _parameter_edit(rng, material):
     return sc, vc
 
 
-def serving_workload(seed: int, jobs: int, rate: float):
-    """The serving stream: Poisson arrivals at `rate` jobs/s over 4 resident
-    procedural scenes (8-64 instances, 125k-1M triangles), resolution drawn
-    from {256^2, 512^2, 1024x768, 1920x1080}, spp uniform in 1-64, random
-    camera poses; 30 % of jobs preceded by a parameter-only material edit and
-    5 % by a structural graph edit (a recompiled material)."""
+def serving_scenes(count: int):
+    """The serving stream's resident scenes: procedural scenes built like the
+    headline one with 8..64 instances of the 8 base meshes (125k-1M
+    triangles), seeds 0..count-1."""
+    from psycles_b200 import scenes
+    return [scenes.procedural_scene(seed=k, instances_per_mesh=1 + k % 8) for k in range(count)]
+
+
+def serving_workload(seed: int, jobs: int, rate: float, scene_count: int = 16):
+    """The serving stream: Poisson arrivals at `rate` jobs/s over
+    `scene_count` resident procedural scenes, resolution drawn from
+    {256^2, 512^2, 1024x768, 1920x1080}, spp uniform in 1-64, random camera
+    poses; 30 % of jobs preceded by a parameter-only material edit and 5 % by
+    a structural graph edit (a recompiled material)."""
     import numpy as np
     rng = np.random.default_rng(seed)
     t = 0.0
@@ -409,14 +428,27 @@ def serving_workload(seed: int, jobs: int, rate: float):
         t += float(rng.exponential(1.0 / rate))
         w, h = SERVING_SIZES[int(rng.integers(0, len(SERVING_SIZES)))]
         u = float(rng.random())
-        out.append({"arrival": t, "scene": int(rng.integers(0, 4)), "width": w, "height": h,
+        out.append({"arrival": t, "scene": int(rng.integers(0, scene_count)), "width": w, "height": h,
                     "spp": int(rng.integers(1, 65)), "camera": _random_camera(rng),
                     "edit": "structural" if u < 0.05 else ("parameters" if u < 0.35 else None),
                     "edit_seed": int(rng.integers(0, 1 << 30)), "seed": k})
     return out
 
 
-def run_serving(backend, jobs: int = 32, rate: float = 200.0, capacity: int = 0) -> dict:
+def _latency_summary(latencies, stream) -> dict:
+    """p50 / p99 latency over all jobs and per resolution class."""
+    import numpy as np
+    lat = np.array(latencies)
+    out = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)), "per_class": {}}
+    for w, h in SERVING_SIZES:
+        sel = np.array([j["width"] == w and j["height"] == h for j in stream])
+        if sel.any():
+            out["per_class"][f"{w}x{h}"] = {"jobs": int(sel.sum()), "p50_ms": float(np.percentile(lat[sel], 50)),
+                                            "p99_ms": float(np.percentile(lat[sel], 99))}
+    return out
+
+
+def run_serving(backend, jobs: int = 64, rate: float = 200.0, scene_count: int = 16, capacity: int = 0) -> dict:
     """The same job stream through the render server (continuous batching)
     and through plain one-session-per-job renders; both arms read every pass
     back.  Latency is arrival -> passes in host memory."""
@@ -425,8 +457,8 @@ def run_serving(backend, jobs: int = 32, rate: float = 200.0, capacity: int = 0)
     from psycles_b200.backend import RenderServer, SampleRange
     from psycles_b200.materials import random_material
 
-    base = [scenes.procedural_scene(seed=k, instances_per_mesh=ipm) for k, ipm in enumerate((1, 2, 4, 8))]
-    stream = serving_workload(7, jobs, rate)
+    base = serving_scenes(scene_count)
+    stream = serving_workload(7, jobs, rate, scene_count)
     passes = (_abi.PASS_COMBINED, _abi.PASS_NORMAL, _abi.PASS_ALBEDO, _abi.PASS_SAMPLE_COUNT)
     total_samples = sum(j["width"] * j["height"] * j["spp"] for j in stream)
     structural = {}  # job index -> recompiled scene (built before the clock starts: the same for both arms)
@@ -444,7 +476,7 @@ def run_serving(backend, jobs: int = 32, rate: float = 200.0, capacity: int = 0)
         compiled = [backend.compile_scene(sc).scene for sc in base]
         recompiled = {i: backend.compile_scene(sc).scene for i, sc in structural.items()}
         current = list(compiled)
-        latencies, t_done = [], 0.0
+        latencies, t_done = [None] * len(stream), 0.0
         server = RenderServer(backend.context, path_capacity=capacity) if serve else None
         ids = [None] * len(stream)
         edits = [(i, j) for i, j in enumerate(stream)]
@@ -481,13 +513,13 @@ def run_serving(backend, jobs: int = 32, rate: float = 200.0, capacity: int = 0)
                     server.read_pass(ids[i], k, j["width"], j["height"])
                 server.release(ids[i])
                 now = time.perf_counter() - t0
-                latencies.append((now - j["arrival"]) * 1e3)
+                latencies[i] = (now - j["arrival"]) * 1e3
                 t_done = now
             th.join()
             st = server.stats()
             extra = {"wavefronts": int(st.wavefronts), "server_p50_ms": st.latency_p50_ms,
                      "server_p99_ms": st.latency_p99_ms, "bytes_peak": int(st.bytes_peak),
-                     "device_busy_s": st.busy_ms / 1e3}
+                     "loop_busy_s": st.busy_ms / 1e3}
             server.close()
         else:
             device_ms = 0.0
@@ -504,31 +536,49 @@ def run_serving(backend, jobs: int = 32, rate: float = 200.0, capacity: int = 0)
                     sess.read_pass(k)
                 sess.close()
                 now = time.perf_counter() - t0
-                latencies.append((now - j["arrival"]) * 1e3)
+                latencies[i] = (now - j["arrival"]) * 1e3
                 t_done = now
-            extra = {"device_busy_s": device_ms / 1e3}
+            extra = {"device_s": device_ms / 1e3}
         for c in list(compiled) + list(recompiled.values()):
             c.close()
-        lat = np.array(latencies)
-        return dict({"samples_per_s": total_samples / t_done, "wall_s": t_done,
-                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}, **extra)
+        return dict({"samples_per_s": total_samples / t_done, "wall_s": t_done},
+                    **_latency_summary(latencies, stream), **extra)
 
     plain = arm(False)
     served = arm(True)
-    return {"workload": f"{jobs} jobs, Poisson arrivals at {rate:g}/s over 4 resident procedural scenes "
+    arrival_span = stream[-1]["arrival"]
+    offered = total_samples / arrival_span
+    cut = f"; {jobs} of the stated 10,000 jobs" if jobs < 10000 else ""
+    return {"workload": f"{jobs} jobs, Poisson arrivals at {rate:g}/s over {scene_count} resident procedural scenes "
                         "(125k-1M triangles); sizes 256^2..1920x1080, spp U[1,64], 8 bounces; 30% parameter "
-                        "edits, 5% structural edits; every pass read back",
-            "samples": total_samples, "path_capacity": capacity, "server": served, "plain": plain,
+                        f"edits, 5% structural edits; HBM admission budget 120 GB; every pass read back{cut}",
+            "jobs": jobs, "rate_jobs_per_s": rate, "scenes": scene_count, "samples": total_samples,
+            "path_capacity": capacity,
+            "load": {"arrival_span_s": arrival_span, "offered_samples_per_s": offered,
+                     "offered_vs_served": offered / served["samples_per_s"],
+                     "note": ("the stream offers more samples per second than one GPU renders, so jobs queue and "
+                              "latency measures the drain of that queue, not admission under steady load")
+                     if offered > served["samples_per_s"] else "the GPU keeps up with the offered load"},
+            "server": served, "plain": plain,
             "server_vs_plain": served["samples_per_s"] / plain["samples_per_s"]}
 
 
-def run_viewports(backend, compiled, count: int = 64, capacity: int = 0) -> dict:
+VIEWPORT_SWEEP = {"path_capacity": (1 << 20, 1 << 22, 1 << 24), "sort_threshold": (0, 1 << 16, 1 << 20),
+                  "stream_block_size": (128, 256, 512)}
+
+
+def run_viewports(backend, compiled, count: int = 64, sweep: str = "descent") -> dict:
     """64 concurrent viewport renders of the procedural scene from random
-    camera poses (128^2 .. 1920x1080, 1-16 spp): one batched call (shared
-    wavefronts, each replayed as a captured CUDA graph) against the same
-    sessions rendered one after another.  Both arms check out bit-identical."""
+    camera poses (128^2 .. 1920x1080, 1-16 spp) in one batched call (shared
+    wavefronts, each replayed as a captured CUDA graph), after a tuning sweep
+    over queue capacity {1M, 4M, 16M} paths, sort-by-material threshold
+    {never, 64Ki, 1Mi} and block size {128, 256, 512} of the camera-ray and
+    film kernels (`sweep`: "grid" = all 27 points, "descent" = one knob at a
+    time from the defaults), against the same 64 sessions rendered one after
+    another at the chosen tuning.  Both arms check out bit-identical."""
+    import itertools
     import numpy as np
-    from psycles_b200 import _abi, scenes
+    from psycles_b200 import _abi, autotune, scenes
     from psycles_b200.backend import BatchRenderer, SampleRange
     rng = np.random.default_rng(11)
     sizes = [(128, 128), (256, 256), (512, 512), (1024, 768), (1920, 1080)]
@@ -546,6 +596,55 @@ def run_viewports(backend, compiled, count: int = 64, capacity: int = 0) -> dict
             out.append((s, spp))
         return out
 
+    default = autotune.get_tuning(backend)
+
+    def batched(point: dict, keep: bool = False):
+        autotune.set_tuning(backend, dict(default, sort_threshold=point["sort_threshold"],
+                                          stream_block_size=point["stream_block_size"]))
+        batch = BatchRenderer(backend.context, path_capacity=point["path_capacity"], use_graph=True)
+        warm = sessions()  # the first call captures the wavefront graph and sizes the path state
+        assert batch.render([(s, SampleRange(0, spp, 0, spp)) for s, spp in warm])
+        for s, _ in warm:
+            s.close()
+        bs = sessions()
+        t0 = time.perf_counter()
+        assert batch.render([(s, SampleRange(0, spp, 0, spp)) for s, spp in bs])
+        wall = time.perf_counter() - t0
+        st = batch.stats()
+        result = {"samples_per_s": total / wall, "device_samples_per_s": total / (st.ms_total / 1e3), "wall_s": wall,
+                  "wavefronts": int(st.wavefronts), "graph_launches": int(st.graph_launches),
+                  "kernel_launches": int(st.kernel_launches)}
+        batch.close()
+        if keep:
+            return result, bs
+        for s, _ in bs:
+            s.close()
+        return result, None
+
+    start = {"path_capacity": 1 << 24, "sort_threshold": default["sort_threshold"],
+             "stream_block_size": default["stream_block_size"]}
+    trials = []
+    if sweep == "grid":
+        for vals in itertools.product(*VIEWPORT_SWEEP.values()):
+            point = dict(zip(VIEWPORT_SWEEP, vals))
+            trials.append((point, batched(point)[0]))
+        best = max(trials, key=lambda t: t[1]["device_samples_per_s"])[0]
+    else:
+        best = dict(start)
+        trials.append((dict(best), batched(best)[0]))
+        rate = trials[-1][1]["device_samples_per_s"]
+        for knob, values in VIEWPORT_SWEEP.items():
+            for v in values:
+                if v == best[knob]:
+                    continue
+                point = dict(best, **{knob: v})
+                trials.append((point, batched(point)[0]))
+                if trials[-1][1]["device_samples_per_s"] > rate:
+                    rate, best = trials[-1][1]["device_samples_per_s"], point
+    # the two arms at the chosen tuning
+    batch_result, bs = batched(best, keep=True)
+    autotune.set_tuning(backend, dict(default, sort_threshold=best["sort_threshold"],
+                                      stream_block_size=best["stream_block_size"]))
     ss = sessions()
     t0 = time.perf_counter()
     dev = 0.0
@@ -553,31 +652,20 @@ def run_viewports(backend, compiled, count: int = 64, capacity: int = 0) -> dict
         assert s.render_samples(SampleRange(0, spp, 0, spp))
         dev += s.stats().ms_total
     plain_wall = time.perf_counter() - t0
-    ref = [s.read_pass(_abi.PASS_COMBINED) for s, _ in ss]
-    for s, _ in ss:
+    same = all(np.array_equal(a.read_pass(_abi.PASS_COMBINED).view(np.uint32),
+                              b.read_pass(_abi.PASS_COMBINED).view(np.uint32)) for (a, _), (b, _) in zip(bs, ss))
+    for s, _ in list(ss) + list(bs):
         s.close()
-    batch = BatchRenderer(backend.context, path_capacity=capacity, use_graph=True)
-    warm = sessions()
-    assert batch.render([(s, SampleRange(0, spp, 0, spp)) for s, spp in warm])
-    for s, _ in warm:
-        s.close()
-    bs = sessions()
-    t0 = time.perf_counter()
-    assert batch.render([(s, SampleRange(0, spp, 0, spp)) for s, spp in bs])
-    batch_wall = time.perf_counter() - t0
-    st = batch.stats()
-    same = all(np.array_equal(s.read_pass(_abi.PASS_COMBINED).view(np.uint32), r.view(np.uint32))
-               for (s, _), r in zip(bs, ref))
-    for s, _ in bs:
-        s.close()
-    batch.close()
-    return {"workload": f"{count} viewports of the procedural scene, random poses, 128^2..1920x1080, 1-16 spp",
-            "samples": total, "path_capacity": capacity,
-            "batched": {"samples_per_s": total / batch_wall, "device_samples_per_s": total / (st.ms_total / 1e3),
-                        "wall_s": batch_wall, "wavefronts": int(st.wavefronts), "graph_launches": int(st.graph_launches)},
+    autotune.set_tuning(backend, default)
+    return {"workload": f"{count} viewports of the procedural scene, random poses, 128^2..1920x1080, 1-16 spp, "
+                        "8 bounces",
+            "samples": total, "sweep": sweep,
+            "trials": [dict(point, device_samples_per_s=r["device_samples_per_s"], samples_per_s=r["samples_per_s"])
+                       for point, r in trials],
+            "chosen": best, "batched": batch_result,
             "plain": {"samples_per_s": total / plain_wall, "device_samples_per_s": total / (dev / 1e3),
                       "wall_s": plain_wall},
-            "batched_vs_plain": plain_wall / batch_wall, "identical": bool(same)}
+            "batched_vs_plain": plain_wall / batch_result["wall_s"], "identical": bool(same)}
 
 
 # DRAM bytes per second of device time of the traversal and shading kernels,
@@ -631,6 +719,28 @@ def kernel_profile(args, backend, compiled, settings) -> dict:
                          else "fallback 6.65 TB/s"}}
 
 
+def run_workload(args) -> None:
+    """One serving-stream or viewport-batch measurement on one GPU (rank 0
+    of a torchrun launch; the other ranks exit without work)."""
+    from psycles_b200 import dist as pdist
+    rank, _, local = pdist.rank_env()
+    if rank != 0:
+        return
+    from psycles_b200.backend import CudaPathTracerBackend
+    backend = CudaPathTracerBackend(local)
+    line = {"workload": args.workload, "n_gpus": 1, "data": "synthetic"}
+    with ClockSampler(local) as clocks:
+        if args.workload == "serving":
+            line["serving"] = run_serving(backend, jobs=args.serving_jobs, rate=args.serving_rate,
+                                          scene_count=args.serving_scenes)
+        else:
+            comp = backend.compile_scene(make_scene("procedural"))
+            line["viewports"] = run_viewports(backend, comp.scene, sweep="grid")
+            comp.scene.close()
+    line["clocks"] = clocks.summary()
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -643,6 +753,12 @@ def main() -> None:
     ap.add_argument("--no-kernel-timing", dest="kernel_timing", action="store_false")
     ap.add_argument("--no-serving", dest="serving", action="store_false",
                     help="skip the batched-viewport and serving-stream measurements")
+    ap.add_argument("--workload", default="frame", choices=["frame", "serving", "viewports"],
+                    help="frame: the headline line (default); serving / viewports: only that measurement, "
+                         "one JSON line, at the sizes of the --serving-* options or with the full tuning grid")
+    ap.add_argument("--serving-jobs", type=int, default=64)
+    ap.add_argument("--serving-scenes", type=int, default=16)
+    ap.add_argument("--serving-rate", type=float, default=200.0)
     args = ap.parse_args()
     if args.spp is None:
         args.spp = CONFIGS[args.config]["spp"]
@@ -650,6 +766,8 @@ def main() -> None:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload != "frame":
+        run_workload(args)
     else:
         run_cuda(args)
 

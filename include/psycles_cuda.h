@@ -586,6 +586,10 @@ typedef struct psy_tuning {
                                           0 = never (the default), 0xffffffff = the default */
     uint32_t ray_sort_threshold;       /* sort closest-hit queues of at least this many rays by origin
                                           cell and octant; 0 = never (the default), 0xffffffff = the default */
+    uint32_t stream_block_size;        /* threads per block of the camera-ray and film kernels: 128, 256 or
+                                          512; 0 = 256.  The persistent traversal and shading kernels keep
+                                          128-thread blocks (their register budgets are compiled in; their
+                                          occupancy is tuned by blocks per SM) */
 } psy_tuning;
 
 psy_status psy_context_set_tuning(psy_context *context, const psy_tuning *tuning);

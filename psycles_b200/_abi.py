@@ -5,10 +5,12 @@ CPU fallback, and loading fails loudly when the extension is missing."""
 from __future__ import annotations
 
 import ctypes
+import os
 import pathlib
 
 HERE = pathlib.Path(__file__).resolve().parent
-LIB_PATH = HERE / "libpsycles_cuda.so"
+# PSYCLES_CUDA_LIB selects a variant build (python -m psycles_b200.build --out)
+LIB_PATH = pathlib.Path(os.environ.get("PSYCLES_CUDA_LIB") or HERE / "libpsycles_cuda.so")
 
 c_float_p = ctypes.POINTER(ctypes.c_float)
 c_uint32_p = ctypes.POINTER(ctypes.c_uint32)
@@ -160,7 +162,7 @@ class KernelProfile(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("path_capacity", "stream_blocks_per_sm", "traversal_blocks_per_sm",
                                                "shade_blocks_per_sm", "sort_threshold", "shadow_sort_threshold",
-                                               "ray_sort_threshold")]
+                                               "ray_sort_threshold", "stream_block_size")]
 
 
 class BatchConfig(ctypes.Structure):

@@ -4,9 +4,10 @@ Searches the knobs of psy_tuning on a short render of the caller's workload:
 the path capacity of a wavefront (queue capacity), the grid caps of the
 persistent traversal kernels and of the shading kernel (resident blocks of
 128 threads per SM; the kernels' register budgets are fixed at compile time,
-so occupancy is tuned through blocks per SM rather than block size), and
-the queue size from which shading queues are sorted by material.  The search
-is coordinate descent from the defaults: each knob in turn takes the
+so occupancy is tuned through blocks per SM rather than block size), the
+queue size from which shading queues are sorted by material, and the block
+size of the camera-ray and film kernels.  The search is coordinate descent
+from the defaults: each knob in turn takes the
 candidate with the highest samples/s (device time), the others held.  No
 counterpart in the reference.
 
@@ -30,6 +31,7 @@ CANDIDATES = {
     "ray_sort_threshold": (0, 1 << 16, 1 << 20),
     "traversal_blocks_per_sm": (8, 12, 16),
     "shade_blocks_per_sm": (8, 16, 32),
+    "stream_block_size": (128, 256, 512),
 }
 
 

@@ -81,5 +81,20 @@ def _build(force: bool, verbose_ptxas: bool, defs: list[str]) -> pathlib.Path:
     return OUT
 
 
+def main(argv: list[str]) -> None:
+    """`--force`, `--ptxas`, `-D NAME=VALUE` (repeatable: a kernel tuning
+    macro or the build option PSY_BVH_WIDTH=8) and `--out PATH` (a variant
+    library beside the default one; load it with PSYCLES_CUDA_LIB=PATH)."""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m psycles_b200.build")
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--ptxas", action="store_true")
+    ap.add_argument("-D", dest="defines", action="append", default=[])
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    out = pathlib.Path(a.out).resolve() if a.out else None
+    build(force=a.force, verbose_ptxas=a.ptxas, defines=tuple(a.defines), out=out)
+
+
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose_ptxas="--ptxas" in sys.argv)
+    main(sys.argv[1:])

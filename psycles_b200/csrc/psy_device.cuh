@@ -4,10 +4,50 @@
 // Psycles function it implements.
 #pragma once
 
+#include <type_traits>
+
 #include "psy_math.cuh"
 #include "psy_scene.h"
 
 namespace psy {
+
+// ------------------------------------------------------- record sectors
+// A path record's 16-byte fields pair up into its four 32-byte sectors (ray
+// origin + direction, the two state words, throughput + radiance, hit + hit
+// primitive).  One 256-bit access (ld / st.global.v8.b32, sm_100) moves a
+// pair: a lane fills a whole sector per request instead of half of one.
+// The field passed is the pair's first; its record offset is 32-byte aligned.
+__device__ __forceinline__ uint4 bits4(const float4 &v) {
+    return make_uint4(__float_as_uint(v.x), __float_as_uint(v.y), __float_as_uint(v.z), __float_as_uint(v.w));
+}
+__device__ __forceinline__ float4 floats4(const uint4 &v) {
+    return make_float4(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z), __uint_as_float(v.w));
+}
+__device__ __forceinline__ void load_sector(const void *p, uint4 &a, uint4 &b) {
+    asm volatile("ld.global.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+                 : "l"(p));
+}
+__device__ __forceinline__ void store_sector(void *p, const uint4 &a, const uint4 &b) {
+    asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(a.x), "r"(a.y), "r"(a.z),
+                 "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+                 : "memory");
+}
+template <class A, class B>
+__device__ __forceinline__ void load_pair(const PathField<A> &first, size_t i, A &a, B &b) {
+    uint4 ua, ub;
+    load_sector(&first[i], ua, ub);
+    if constexpr (std::is_same<A, float4>::value) a = floats4(ua);
+    else a = ua;
+    if constexpr (std::is_same<B, float4>::value) b = floats4(ub);
+    else b = ub;
+}
+__device__ __forceinline__ uint4 as_bits(const float4 &v) { return bits4(v); }
+__device__ __forceinline__ uint4 as_bits(const uint4 &v) { return v; }
+template <class A, class B>
+__device__ __forceinline__ void store_pair(const PathField<A> &first, size_t i, const A &a, const B &b) {
+    store_sector(&first[i], as_bits(a), as_bits(b));
+}
 
 // ------------------------------------------------------------- sampler
 // include/psycles/luisa/cycles_sampler.h:36-339.

@@ -1450,6 +1450,9 @@ psy_status psy_context_set_tuning(psy_context *c, const psy_tuning *t) {
     if (t->stream_blocks_per_sm > 64u || t->traversal_blocks_per_sm > 64u || t->shade_blocks_per_sm > 64u)
         return fail(PSY_ERROR_INVALID_ARGUMENT, "at most 64 blocks per SM");
     if (t->path_capacity > (1u << 26)) return fail(PSY_ERROR_INVALID_ARGUMENT, "path capacity above 64 Mi");
+    if (t->stream_block_size && t->stream_block_size != 128u && t->stream_block_size != 256u &&
+        t->stream_block_size != 512u)
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "stream block size must be 128, 256 or 512");
     const psy::LaunchConfig defaults;
     c->path_capacity = t->path_capacity ? t->path_capacity : (1u << 24);
     c->launch.stream_blocks_per_sm = t->stream_blocks_per_sm ? t->stream_blocks_per_sm : defaults.stream_blocks_per_sm;
@@ -1461,6 +1464,7 @@ psy_status psy_context_set_tuning(psy_context *c, const psy_tuning *t) {
         t->shadow_sort_threshold == 0xffffffffu ? defaults.shadow_sort_threshold : t->shadow_sort_threshold;
     c->launch.ray_sort_threshold =
         t->ray_sort_threshold == 0xffffffffu ? defaults.ray_sort_threshold : t->ray_sort_threshold;
+    c->launch.stream_block = t->stream_block_size ? t->stream_block_size : defaults.stream_block;
     return PSY_OK;
 }
 
@@ -1473,6 +1477,7 @@ psy_status psy_context_get_tuning(const psy_context *c, psy_tuning *t) {
     t->sort_threshold = c->launch.sort_threshold;
     t->shadow_sort_threshold = c->launch.shadow_sort_threshold;
     t->ray_sort_threshold = c->launch.ray_sort_threshold;
+    t->stream_block_size = c->launch.stream_block;
     return PSY_OK;
 }
 

@@ -125,13 +125,10 @@ __device__ __forceinline__ void raygen_path(const RenderParams &p, const PathBuf
     const float near_t = p.near_clip / safe_cos;
     const float far_t = (p.far_clip - p.near_clip) / safe_cos;
     origin = origin + dir * near_t;
-    b.ray_o[i] = make_float4(origin.x, origin.y, origin.z, 0.0f);
-    b.ray_d[i] = make_float4(dir.x, dir.y, dir.z, far_t);
-    b.tp[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    b.rad[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    store_pair(b.ray_o, i, make_float4(origin.x, origin.y, origin.z, 0.0f), make_float4(dir.x, dir.y, dir.z, far_t));
+    store_pair(b.tp, i, make_float4(1.0f, 1.0f, 1.0f, 0.0f), make_float4(0.0f, 0.0f, 0.0f, 0.0f));
     // initial_state (include/psycles/luisa/cycles_path_state.h:187-199)
-    b.st[i] = make_uint4(128u | 512u, 1u, 16u, 0u);
-    b.st2[i] = make_uint4(kSt2Delta, kInvalid, kInvalid, local);
+    store_pair(b.st, i, make_uint4(128u | 512u, 1u, 16u, 0u), make_uint4(kSt2Delta, kInvalid, kInvalid, local));
     b.sample[i] = sample;
     b.aov_n[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     b.aov_a[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -252,9 +249,11 @@ __global__ void __launch_bounds__(128, PSY_INTERSECT_MIN_BLOCKS)
         }
         const SceneView &s = kMulti ? jobs[job].s : s_arg;
         if (q != kInvalid) {
-            const float4 o = b.ray_o[path], d = b.ray_d[path];
-            const uint32_t vis = b.st[path].y;
-            const uint4 st2 = b.st2[path];
+            float4 o, d;
+            uint4 st, st2;
+            load_pair(b.ray_o, path, o, d);
+            load_pair(b.st, path, st, st2);
+            const uint32_t vis = st.y;
             const Ray ray{mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, d.w};
             traversal_begin(t, s, ray, contract_visibility(vis), st2.y, st2.z, kInvalid, kInvalid);
             has = false;
@@ -281,8 +280,8 @@ __global__ void __launch_bounds__(128, PSY_INTERSECT_MIN_BLOCKS)
                 return false;
             });
             if (done) {
-                b.hit[path] = make_float4(best.t, best.u, best.v, __uint_as_float(best.instance));
-                b.hit_prim[path] = make_uint4(has ? best.prim : kInvalid, 0u, 0u, 0u);
+                store_pair(b.hit, path, make_float4(best.t, best.u, best.v, __uint_as_float(best.instance)),
+                           make_uint4(has ? best.prim : kInvalid, 0u, 0u, 0u));
                 active = false;
             }
         }
@@ -404,8 +403,9 @@ __device__ __forceinline__ uint32_t surface_material(const SceneView &s, uint32_
 __device__ __forceinline__ uint32_t nee_kind_hint(const SceneView &s, const RenderParams &p, const PathBuffers &b,
                                                   uint32_t i) {
     if (p.use_light_tree || !p.nee || s.emitter_count == 0u) return 0u;
-    const uint4 st = b.st[i];
-    const uint32_t local = b.st2[i].w;
+    uint4 st, st2;
+    load_pair(b.st, i, st, st2);
+    const uint32_t local = st2.w;
     const uint32_t x = p.win_x + local % p.win_w, y = p.win_y + local / p.win_w;
     const uint32_t rng_hash = pixel_hash(x, p.full_h - 1u - y, p.seed);
     const float u = sample_4d(p, b.sample[i], rng_hash, st.z + 1u).z;
@@ -437,13 +437,16 @@ __global__ void k_sort_count(const __grid_constant__ SceneView s_arg, const __gr
     __syncthreads();
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
         const uint32_t i = b.queue_in[q];
-        const uint32_t prim = b.hit_prim[i].x;
+        float4 h4;
+        uint4 hp4;
+        load_pair(b.hit, i, h4, hp4);
+        const uint32_t prim = hp4.x;
         uint32_t key = 0u;
         if (prim != kInvalid) {
             const uint32_t job = kMulti ? b.job[i] : 0u;
             const SceneView &s = kMulti ? jobs[job].s : s_arg;
             const RenderParams &p = kMulti ? jobs[job].p : p_arg;
-            const uint32_t mat = surface_material(s, __float_as_uint(b.hit[i].w), prim);
+            const uint32_t mat = surface_material(s, __float_as_uint(h4.w), prim);
             key = 1u + (mat * 8u + nee_kind_hint(s, p, b, i) + job * 977u) % (kSortBuckets - 1u);
         }
         b.sort_keys[q] = key;
@@ -539,7 +542,8 @@ __global__ void k_sort_count_rays(const __grid_constant__ SceneView s_arg, const
         const uint32_t i = b.queue_in[q];
         const uint32_t job = kMulti ? b.job[i] : 0u;
         const SceneView &s = kMulti ? jobs[job].s : s_arg;
-        const float4 o = b.ray_o[i], d = b.ray_d[i];
+        float4 o, d;
+        load_pair(b.ray_o, i, o, d);
         auto cell = [](float v, float lo, float hi, float n) {
             const float f = hi > lo ? (v - lo) / (hi - lo) : 0.0f;
             return uint32_t(fminf(fmaxf(f * n, 0.0f), n - 1.0f));
@@ -618,16 +622,17 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                 ev = &trace->events[step];
                 trace->event_count = step + 1u;
             }
-            const float4 ro = b.ray_o[i], rd = b.ray_d[i];
+            float4 ro, rd, tp4, rad4, h4;
+            uint4 st, st2, hp4;
+            load_pair(b.ray_o, i, ro, rd);
+            load_pair(b.tp, i, tp4, rad4);
+            load_pair(b.st, i, st, st2);
+            load_pair(b.hit, i, h4, hp4);
             Ray ray{mk3(ro.x, ro.y, ro.z), mk3(rd.x, rd.y, rd.z), ro.w, rd.w};
-            float4 tp4 = b.tp[i];
             f3 throughput = mk3(tp4.x, tp4.y, tp4.z);
             float previous_bsdf_pdf = tp4.w;
-            float4 rad4 = b.rad[i];
             f3 radiance = mk3(rad4.x, rad4.y, rad4.z);
             float transparency = rad4.w;
-            uint4 st = b.st[i];
-            uint4 st2 = b.st2[i];
             PathState ps = unpack_state(st, st2);
             bool previous_delta = (st2.x & kSt2Delta) != 0u;
             bool primary_recorded = (st2.x & kSt2Primary) != 0u;
@@ -646,8 +651,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
             const float4 bs4 = sample_4d(p, sample, rng_hash, ps.rng_offset + 3u);
             DistEntryGpu selected = p.use_light_tree ? DistEntryGpu{0.0f, 0.0f, 3u, 0u}
                                                      : distribution_sample(s, light_sample.z);
-            const float4 h4 = b.hit[i];
-            const uint32_t prim = b.hit_prim[i].x;
+            const uint32_t prim = hp4.x;
             if (ev) {
                 ev->rng_offset = ps.rng_offset;
                 ev->random_terminate = terminate_sample;
@@ -945,21 +949,22 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                     if (!keep && ev) ev->terminated = 1u;
                 }
             }
-            b.rad[i] = make_float4(radiance.x, radiance.y, radiance.z, transparency);
+            const float4 rad_out = make_float4(radiance.x, radiance.y, radiance.z, transparency);
+            if (!keep) b.rad[i] = rad_out;
             if (keep) {
-                b.ray_o[i] = make_float4(ray.o.x, ray.o.y, ray.o.z, ray.tmin);
-                b.ray_d[i] = make_float4(ray.d.x, ray.d.y, ray.d.z, ray.tmax);
-                b.tp[i] = make_float4(throughput.x, throughput.y, throughput.z, previous_bsdf_pdf);
-                b.st[i] = make_uint4(ps.flag, ps.visibility, ps.rng_offset,
-                                     ps.bounce | (ps.diffuse_bounce << 8) | (ps.glossy_bounce << 16) |
-                                         (ps.transmission_bounce << 24));
+                store_pair(b.ray_o, i, make_float4(ray.o.x, ray.o.y, ray.o.z, ray.tmin),
+                           make_float4(ray.d.x, ray.d.y, ray.d.z, ray.tmax));
+                store_pair(b.tp, i, make_float4(throughput.x, throughput.y, throughput.z, previous_bsdf_pdf), rad_out);
+                const uint4 st_out = make_uint4(ps.flag, ps.visibility, ps.rng_offset,
+                                                ps.bounce | (ps.diffuse_bounce << 8) | (ps.glossy_bounce << 16) |
+                                                    (ps.transmission_bounce << 24));
                 uint32_t bits = ps.transparent_bounce & 0xffu;
                 if (previous_delta) bits |= kSt2Delta;
                 if (primary_recorded) bits |= kSt2Primary;
                 if ((ps.flag & kFlagTerminateOnNextSurface) != 0u) bits |= kSt2TermNext;
                 if ((ps.flag & kFlagTerminateAfterTransparent) != 0u) bits |= kSt2TermAfter;
                 st2.x = bits;
-                b.st2[i] = st2;
+                store_pair(b.st, i, st_out, st2);
             }
         }
         const uint32_t slot = warp_push(&b.counters[1], active && keep);
@@ -1216,16 +1221,13 @@ __device__ __forceinline__ void film_pixel(const PathBuffers &b, uint32_t px, ui
                                            uint32_t path_begin, float4 *combined, float4 *normal, float4 *albedo,
                                            uint32_t *sample_count, uint32_t trace_path, psy_path_trace *trace) {
     float4 c = combined[px], n = normal[px], a = albedo[px];
-    for (uint32_t k = 0; k < samples; ++k) {
-        const uint32_t i = path_begin + k * pixels + px;
-        const float4 r = b.rad[i];
+    auto add = [&](uint32_t i, const float4 &r, const float4 &nn, const float4 &aa) {
         f3 rad = mk3(r.x, r.y, r.z);
         if (any_nan(rad)) rad = mk3(0.0f);
         c.x += rad.x;
         c.y += rad.y;
         c.z += rad.z;
         c.w += r.w;
-        const float4 nn = b.aov_n[i], aa = b.aov_a[i];
         n.x += nn.x;
         n.y += nn.y;
         n.z += nn.z;
@@ -1235,6 +1237,27 @@ __device__ __forceinline__ void film_pixel(const PathBuffers &b, uint32_t px, ui
         a.z += aa.z;
         a.w += 1.0f;
         if (trace && i == trace_path) set3(trace->radiance, rad);
+    };
+    // Four samples' loads are issued before any of them is added (the
+    // trace store could alias them, so the compiler would not hoist a later
+    // sample's loads above it); the sums still run in sample order.
+    constexpr uint32_t kGroup = 4u;
+    uint32_t k = 0;
+    for (; k + kGroup <= samples; k += kGroup) {
+        float4 r[kGroup], nn[kGroup], aa[kGroup];
+#pragma unroll
+        for (uint32_t u = 0; u < kGroup; ++u) {
+            const uint32_t i = path_begin + (k + u) * pixels + px;
+            r[u] = b.rad[i];
+            nn[u] = b.aov_n[i];
+            aa[u] = b.aov_a[i];
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < kGroup; ++u) add(path_begin + (k + u) * pixels + px, r[u], nn[u], aa[u]);
+    }
+    for (; k < samples; ++k) {
+        const uint32_t i = path_begin + k * pixels + px;
+        add(i, b.rad[i], b.aov_n[i], b.aov_a[i]);
     }
     combined[px] = c;
     normal[px] = n;
@@ -1375,7 +1398,8 @@ int launch_grid(uint32_t work, int block, const LaunchConfig &lc) {
 
 void launch_raygen(cudaStream_t st, const LaunchConfig &lc, const RenderParams &p, const PathBuffers &b, uint32_t pixels,
                    uint32_t paths, uint32_t sample_base, uint32_t trace_path, psy_path_trace *trace) {
-    k_raygen<<<launch_grid(paths, 256, lc), 256, 0, st>>>(p, b, pixels, paths, sample_base, trace_path, trace);
+    k_raygen<<<launch_grid(paths, int(lc.stream_block), lc), lc.stream_block, 0, st>>>(p, b, pixels, paths, sample_base,
+                                                                                    trace_path, trace);
 }
 void launch_set_counters(cudaStream_t st, uint32_t *counters, uint32_t n) { k_set_counters<<<1, 1, 0, st>>>(counters, n); }
 // Persistent kernels: enough resident warps to fill every SM (bounded by the
@@ -1456,13 +1480,14 @@ void launch_resolve_pass(cudaStream_t st, const float4 *film, const uint32_t *co
 }
 void launch_film(cudaStream_t st, const LaunchConfig &lc, const PathBuffers &b, uint32_t pixels, uint32_t samples, float4 *combined,
                  float4 *normal, float4 *albedo, uint32_t *sample_count, uint32_t trace_path, psy_path_trace *trace) {
-    k_film<<<launch_grid(pixels, 256, lc), 256, 0, st>>>(b, pixels, samples, combined, normal, albedo, sample_count,
-                                                        trace_path, trace);
+    k_film<<<launch_grid(pixels, int(lc.stream_block), lc), lc.stream_block, 0, st>>>(b, pixels, samples, combined, normal,
+                                                                                      albedo, sample_count, trace_path,
+                                                                                      trace);
 }
 // Batched wavefront: every kernel reads each path's job record.
 void launch_raygen_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const BatchItem *items, const uint32_t *round,
                          const PathBuffers &b, uint32_t max_paths) {
-    k_raygen_batch<<<launch_grid(max_paths, 256, lc), 256, 0, st>>>(jobs, items, round, b);
+    k_raygen_batch<<<launch_grid(max_paths, int(lc.stream_block), lc), lc.stream_block, 0, st>>>(jobs, items, round, b);
 }
 void launch_intersect_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work) {
     if (lc.ray_sort_threshold) launch_ray_sort<true>(st, lc, SceneView{}, b, jobs, max_work);
@@ -1482,7 +1507,7 @@ void launch_shadow_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *
 }
 void launch_film_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const BatchItem *items, const uint32_t *round,
                        const PathBuffers &b, uint32_t max_pixels) {
-    k_film_batch<<<launch_grid(max_pixels, 256, lc), 256, 0, st>>>(jobs, items, round, b);
+    k_film_batch<<<launch_grid(max_pixels, int(lc.stream_block), lc), lc.stream_block, 0, st>>>(jobs, items, round, b);
 }
 
 void launch_debug_light_tree(cudaStream_t st, const SceneView &s, const float4 *queries, const uint32_t *pdf_emitters,

@@ -17,6 +17,7 @@ struct LaunchConfig {
     uint32_t sort_threshold = 1u << 16;     // 0: never sort
     uint32_t shadow_sort_threshold = 0;     // shadow queue by direction (off: it measured slower); 0: never
     uint32_t ray_sort_threshold = 0;        // closest-hit queue by origin cell and octant (off: it measured slower)
+    uint32_t stream_block = 256;            // threads per block of raygen and film
 };
 
 int launch_grid(uint32_t work, int block, const LaunchConfig &lc);

@@ -26,6 +26,8 @@ def _render(backend, compiled, st, spp):
     {"sort_threshold": 1, "shadow_sort_threshold": 0, "path_capacity": 3000, "traversal_blocks_per_sm": 2,
      "shade_blocks_per_sm": 1},
     {"stream_blocks_per_sm": 1, "traversal_blocks_per_sm": 64, "shade_blocks_per_sm": 64},
+    {"stream_block_size": 128, "stream_blocks_per_sm": 1},
+    {"stream_block_size": 512},
 ])
 def test_tuning_never_changes_results(backend, tuning):
     default = autotune.get_tuning(backend)
@@ -62,3 +64,5 @@ def test_autotune_applies_its_best_trial(backend):
 def test_tuning_rejects_out_of_range(backend):
     with pytest.raises(_abi.PsyError):
         autotune.set_tuning(backend, {"shade_blocks_per_sm": 1000})
+    with pytest.raises(_abi.PsyError):
+        autotune.set_tuning(backend, {"stream_block_size": 96})
