@@ -57,6 +57,9 @@ psy_status PathArena::ensure(uint32_t n, bool with_job) {
     const uint32_t c = std::max(n, capacity);
     const size_t f4 = sizeof(float4) * size_t(c), u4 = sizeof(uint4) * size_t(c), u1 = sizeof(uint32_t) * size_t(c);
     PSY_CUDA_TRY(records.alloc(psy::kPathRecordBytes * size_t(c)));
+    // the kernels move record sectors with 32-byte accesses
+    if (reinterpret_cast<uintptr_t>(records.ptr) % psy::kPathRecordBytes != 0u)
+        return fail(PSY_ERROR_CUDA, "path records are not 128-byte aligned");
     PSY_CUDA_TRY(sample.alloc(u1));
     PSY_CUDA_TRY(aov_n.alloc(f4));
     PSY_CUDA_TRY(aov_a.alloc(f4));
