@@ -519,7 +519,8 @@ def run_serving(backend, jobs: int = 64, rate: float = 200.0, scene_count: int =
             st = server.stats()
             extra = {"wavefronts": int(st.wavefronts), "server_p50_ms": st.latency_p50_ms,
                      "server_p99_ms": st.latency_p99_ms, "bytes_peak": int(st.bytes_peak),
-                     "loop_busy_s": st.busy_ms / 1e3}
+                     "loop_busy_s": st.busy_ms / 1e3, "device_s": st.device_ms / 1e3,
+                     "device_samples_per_s": total_samples / (st.device_ms / 1e3)}
             server.close()
         else:
             device_ms = 0.0
@@ -538,7 +539,7 @@ def run_serving(backend, jobs: int = 64, rate: float = 200.0, scene_count: int =
                 now = time.perf_counter() - t0
                 latencies[i] = (now - j["arrival"]) * 1e3
                 t_done = now
-            extra = {"device_s": device_ms / 1e3}
+            extra = {"device_s": device_ms / 1e3, "device_samples_per_s": total_samples / (device_ms / 1e3)}
         for c in list(compiled) + list(recompiled.values()):
             c.close()
         return dict({"samples_per_s": total_samples / t_done, "wall_s": t_done},

@@ -687,6 +687,7 @@ typedef struct psy_server_stats {
     double latency_p99_ms;
     uint32_t latency_jobs;
     uint32_t reserved;
+    double device_ms;            /* sum of the wavefronts' event-timed device spans */
 } psy_server_stats;
 
 psy_status psy_server_create(psy_context *context, const psy_server_config *config, psy_server **out);

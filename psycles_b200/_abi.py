@@ -191,7 +191,7 @@ class ServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("jobs_submitted", "jobs_done", "jobs_failed", "samples", "wavefronts",
                                                "bytes_in_use", "bytes_peak")] + [
         ("busy_ms", ctypes.c_double), ("latency_p50_ms", ctypes.c_double), ("latency_p99_ms", ctypes.c_double),
-        ("latency_jobs", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+        ("latency_jobs", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("device_ms", ctypes.c_double)]
 
 
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4

@@ -96,7 +96,7 @@ struct psy_server {
     uint64_t next_id = 1;
     uint64_t bytes_in_use = 0, bytes_peak = 0, fixed_bytes = 0;
     uint64_t samples_done = 0, wavefronts = 0, jobs_failed = 0, jobs_done = 0, jobs_submitted = 0;
-    double busy_ms = 0.0;
+    double busy_ms = 0.0, device_ms = 0.0;
     std::vector<double> latencies;  // submit -> done of every finished job
     psy_status loop_status = PSY_OK;
     std::string loop_error;
@@ -209,14 +209,32 @@ struct psy_server {
     void run_loop() {
         std::vector<Job *> running;
         struct InFlight {
-            cudaEvent_t done = nullptr;
+            cudaEvent_t begin = nullptr, done = nullptr;
             uint64_t wave = 0;
             double issued_ms = 0.0;
             bool active = false;
         } flight[2];
         cudaSetDevice(context->device);
-        for (auto &f : flight) cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming);
+        for (auto &f : flight) {
+            cudaEventCreate(&f.begin);
+            cudaEventCreate(&f.done);
+        }
         uint64_t wave_counter = 0, finished_wave = 0;
+        // a finished wavefront's device span: from the stream reaching its
+        // first launch to its last kernel's end (`locked`: the caller holds mu)
+        auto retire = [&](InFlight &f, bool locked) {
+            float ms = 0.0f;
+            if (cudaEventElapsedTime(&ms, f.begin, f.done) == cudaSuccess) {
+                if (locked) {
+                    device_ms += ms;
+                } else {
+                    std::lock_guard<std::mutex> lock(mu);
+                    device_ms += ms;
+                }
+            }
+            f.active = false;
+            finished_wave = std::max(finished_wave, f.wave + 1u);
+        };
         double busy_since = -1.0;
         for (;;) {
             {
@@ -248,8 +266,7 @@ struct psy_server {
             if (slot.active) {
                 // both buffers busy: wait for the older wavefront first
                 cudaEventSynchronize(slot.done);
-                slot.active = false;
-                finished_wave = std::max(finished_wave, slot.wave + 1u);
+                retire(slot, false);
             }
             if (!plan.empty()) {
                 std::vector<psy::BatchItem> items;
@@ -259,7 +276,8 @@ struct psy_server {
                 EnginePlan ep;
                 ep.add(items, paths, film, engine.max_jobs());
                 EngineRun run;
-                psy_status r = engine.run(ep, steps, run);
+                psy_status r = cudaEventRecord(slot.begin, engine.stream()) == cudaSuccess ? PSY_OK : PSY_ERROR_CUDA;
+                if (r == PSY_OK) r = engine.run(ep, steps, run);
                 if (r == PSY_OK && cudaEventRecord(slot.done, engine.stream()) != cudaSuccess) r = PSY_ERROR_CUDA;
                 if (r != PSY_OK) {
                     std::lock_guard<std::mutex> lock(mu);
@@ -290,18 +308,14 @@ struct psy_server {
                 for (auto &f : flight) {
                     if (!f.active) continue;
                     cudaEventSynchronize(f.done);
-                    f.active = false;
-                    finished_wave = std::max(finished_wave, f.wave + 1u);
+                    retire(f, false);
                 }
             }
             // retire jobs whose last wavefront has finished
             {
                 std::lock_guard<std::mutex> lock(mu);
                 for (auto &f : flight) {
-                    if (f.active && cudaEventQuery(f.done) == cudaSuccess) {
-                        f.active = false;
-                        finished_wave = std::max(finished_wave, f.wave + 1u);
-                    }
+                    if (f.active && cudaEventQuery(f.done) == cudaSuccess) retire(f, true);
                 }
                 bool any = false;
                 for (auto it = running.begin(); it != running.end();) {
@@ -340,6 +354,7 @@ struct psy_server {
         }
         for (auto &f : flight) {
             if (f.active) cudaEventSynchronize(f.done);
+            cudaEventDestroy(f.begin);
             cudaEventDestroy(f.done);
         }
         if (busy_since >= 0.0) busy_ms += now_ms() - busy_since;
@@ -518,6 +533,7 @@ psy_status psy_server_get_stats(psy_server *sv, psy_server_stats *out) {
     out->bytes_in_use = sv->bytes_in_use;
     out->bytes_peak = sv->bytes_peak;
     out->busy_ms = sv->busy_ms;
+    out->device_ms = sv->device_ms;
     out->latency_p50_ms = percentile(lat, 0.5);
     out->latency_p99_ms = percentile(lat, 0.99);
     out->latency_jobs = uint32_t(lat.size());

@@ -65,6 +65,7 @@ def test_jobs_equal_sessions_alone_in_a_mix(backend):
     assert stats.jobs_done == len(jobs) and stats.jobs_failed == 0
     assert stats.latency_jobs == len(jobs) and 0.0 < stats.latency_p50_ms <= stats.latency_p99_ms
     assert stats.wavefronts >= 2
+    assert 0.0 < stats.device_ms <= stats.busy_ms + 1.0
     for j in ids:
         server.release(j)
     server.close()
