@@ -476,6 +476,7 @@ def run_serving(backend, jobs: int = 64, rate: float = 200.0, scene_count: int =
         compiled = [backend.compile_scene(sc).scene for sc in base]
         recompiled = {i: backend.compile_scene(sc).scene for i, sc in structural.items()}
         current = list(compiled)
+        current_desc = list(base)  # the host scene each resident scene was compiled from
         latencies, t_done = [None] * len(stream), 0.0
         server = RenderServer(backend.context, path_capacity=capacity) if serve else None
         ids = [None] * len(stream)
@@ -484,9 +485,10 @@ def run_serving(backend, jobs: int = 64, rate: float = 200.0, scene_count: int =
         def apply_edit(i, j):
             if j["edit"] == "structural":
                 current[j["scene"]] = recompiled[i]
+                current_desc[j["scene"]] = structural[i]
             elif j["edit"] == "parameters":
                 rng = np.random.default_rng(j["edit_seed"])
-                sc = base[j["scene"]]
+                sc = current_desc[j["scene"]]
                 m = int(rng.integers(0, len(sc.materials)))
                 scal, vec = _parameter_edit(rng, sc.materials[m])
                 if serve:
