@@ -558,10 +558,12 @@ def run_serving(backend, jobs: int = 64, rate: float = 200.0, scene_count: int =
             "jobs": jobs, "rate_jobs_per_s": rate, "scenes": scene_count, "samples": total_samples,
             "path_capacity": capacity,
             "load": {"arrival_span_s": arrival_span, "offered_samples_per_s": offered,
-                     "offered_vs_served": offered / served["samples_per_s"],
-                     "note": ("the stream offers more samples per second than one GPU renders, so jobs queue and "
-                              "latency measures the drain of that queue, not admission under steady load")
-                     if offered > served["samples_per_s"] else "the GPU keeps up with the offered load"},
+                     "server_device_samples_per_s": served["device_samples_per_s"],
+                     "utilisation": offered / served["device_samples_per_s"],
+                     "note": ("the stream offers more samples per second than the GPU renders (utilisation above 1), "
+                              "so jobs queue and latency measures the drain of that queue, not admission under "
+                              "steady load") if offered > served["device_samples_per_s"]
+                     else "the GPU keeps up with the offered load: latency is admission under steady load"},
             "server": served, "plain": plain,
             "server_vs_plain": served["samples_per_s"] / plain["samples_per_s"]}
 
@@ -577,7 +579,7 @@ def run_viewports(backend, compiled, count: int = 64, sweep: str = "descent") ->
     over queue capacity {1M, 4M, 16M} paths, sort-by-material threshold
     {never, 64Ki, 1Mi} and block size {128, 256, 512} of the camera-ray and
     film kernels (`sweep`: "grid" = all 27 points, "descent" = one knob at a
-    time from the defaults), against the same 64 sessions rendered one after
+    time from the defaults, "none" = the defaults only), against the same 64 sessions rendered one after
     another at the chosen tuning.  Both arms check out bit-identical."""
     import itertools
     import numpy as np
@@ -632,6 +634,8 @@ def run_viewports(backend, compiled, count: int = 64, sweep: str = "descent") ->
             point = dict(zip(VIEWPORT_SWEEP, vals))
             trials.append((point, batched(point)[0]))
         best = max(trials, key=lambda t: t[1]["device_samples_per_s"])[0]
+    elif sweep == "none":
+        best = dict(start)
     else:
         best = dict(start)
         trials.append((dict(best), batched(best)[0]))
@@ -738,7 +742,7 @@ def run_workload(args) -> None:
                                           scene_count=args.serving_scenes)
         else:
             comp = backend.compile_scene(make_scene("procedural"))
-            line["viewports"] = run_viewports(backend, comp.scene, sweep="grid")
+            line["viewports"] = run_viewports(backend, comp.scene, sweep=args.viewport_sweep)
             comp.scene.close()
     line["clocks"] = clocks.summary()
     print(json.dumps(line), flush=True)
@@ -762,6 +766,8 @@ def main() -> None:
     ap.add_argument("--serving-jobs", type=int, default=64)
     ap.add_argument("--serving-scenes", type=int, default=16)
     ap.add_argument("--serving-rate", type=float, default=200.0)
+    ap.add_argument("--viewport-sweep", default="grid", choices=["grid", "descent", "none"],
+                    help="tuning sweep of --workload viewports (none: the defaults only)")
     args = ap.parse_args()
     if args.spp is None:
         args.spp = CONFIGS[args.config]["spp"]
