@@ -92,8 +92,16 @@ typedef enum psy_closure_op {
     PSY_CLOSURE_EMISSION = 2,
     PSY_CLOSURE_TRANSPARENT = 3,
     PSY_CLOSURE_ADD = 4,
-    PSY_CLOSURE_MIX = 5
+    PSY_CLOSURE_MIX = 5,
+    PSY_CLOSURE_GLOSSY = 6
 } psy_closure_op;
+
+/* Microfacet distribution of a glossy closure (`a` of its instruction):
+ * the Glossy BSDF node's Distribution property (GGX, the default, or
+ * BECKMANN; MULTI_GGX's tabulated energy preservation is not in the
+ * subset and a scene that uses it is rejected). */
+#define PSY_GLOSSY_GGX 0u
+#define PSY_GLOSSY_BECKMANN 1u
 
 /* Closure inputs.  A closure input (colour, strength / factor, roughness)
  * is either a slot of the material's parameter block that belongs to the
@@ -107,10 +115,12 @@ typedef enum psy_closure_op {
 
 /* One closure instruction (compiler::ClosureInstruction,
  * include/psycles/compiler/surface_program.h:415-470, in-scope fields):
- * `color` (vector input: diffuse / transparent / emission colour),
- * `scalar` (emission strength, mix factor), `roughness` (diffuse
- * roughness: Lambert below 1e-5, else Oren-Nayar), `a`/`b` child
- * instruction indices of add and mix. */
+ * `color` (vector input: diffuse / glossy / transparent / emission
+ * colour), `scalar` (emission strength, mix factor), `roughness` (diffuse
+ * roughness: Lambert below 1e-5, else Oren-Nayar; glossy roughness, whose
+ * square is the microfacet alpha), `a`/`b` child instruction indices of add
+ * and mix, and for glossy `a` = PSY_GLOSSY_*.  Every closure's Normal input
+ * is the shading normal (the socket unlinked). */
 typedef struct psy_closure_instruction {
     uint32_t op;
     uint32_t a;
@@ -200,7 +210,15 @@ typedef struct psy_material_desc {
     uint32_t emission_sampling;  /* PSY_EMISSION_SAMPLING_* */
     uint32_t value_count;        /* at most 64 */
     const psy_value_instruction *values;
+    uint32_t flags;              /* PSY_MATERIAL_* */
+    uint32_t reserved;
 } psy_material_desc;
+
+/* contract::Material::use_bump_map_correction (include/psycles/contract/
+ * scene.h:111-114) is on by default: glossy closures then correct their
+ * normal so the specular reflection of the viewing direction stays above
+ * the geometric surface.  This flag turns it off. */
+#define PSY_MATERIAL_NO_BUMP_MAP_CORRECTION 1u
 
 /* contract::LightType order (include/psycles/contract/scene.h:369). */
 typedef enum psy_light_type {

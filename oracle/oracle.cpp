@@ -53,6 +53,7 @@ struct Material {
     uint32_t emission_sampling{0};
     bool has_emission{false};
     bool has_transparent{false};
+    bool bump_correction{true};  // contract::Material::use_bump_map_correction
 };
 
 struct Emitter {
@@ -265,7 +266,11 @@ static float input_scalar(const Material &mat, uint32_t ref) {
 // compiler::ClosureOperation walk of GraphSurfaceImplementation::
 // for_each_closure (src/luisa/graph_surface_closures.cpp:5-356): add visits
 // both children with the same weight, mix splits clamp(fac, 0, 1).  A
-// diffuse leaf keeps its authored colour and roughness.
+// diffuse leaf keeps its authored colour and roughness, a glossy leaf its
+// roughness; a glossy op carries kBeckmann for the Beckmann distribution.
+constexpr uint32_t kBeckmann = 0x100u;
+inline bool is_glossy(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_GLOSSY; }
+
 struct TracedClosure {
     uint32_t op;
     float3 weight;
@@ -300,6 +305,12 @@ static void walk_closures(const Material &mat, uint32_t id, float mix_weight, st
         out.push_back({c.op, color * mix_weight, color, 0.0f});
         return;
     }
+    case PSY_CLOSURE_GLOSSY: {
+        const float3 color = input_vector(mat, c.color);
+        const uint32_t op = c.a == PSY_GLOSSY_BECKMANN ? (uint32_t(PSY_CLOSURE_GLOSSY) | kBeckmann) : uint32_t(PSY_CLOSURE_GLOSSY);
+        out.push_back({op, color * mix_weight, color, input_scalar(mat, c.roughness)});
+        return;
+    }
     default:
         return;
     }
@@ -319,12 +330,12 @@ constexpr uint32_t kMaxClosures = 16u;
 
 // One retained physical closure: Cycles' ShaderClosure after allocation.
 struct PhysicalClosure {
-    uint32_t op;  // DIFFUSE or TRANSPARENT
+    uint32_t op;  // DIFFUSE, TRANSPARENT or GLOSSY (| kBeckmann)
     float3 weight;
     float sample_weight;
-    float3 normal;
+    float3 normal;    // diffuse: the shading normal; glossy: after setup's specular-reflection correction
     float3 color;     // authored colour (Oren-Nayar albedo)
-    float roughness;  // diffuse roughness (Lambert below 1e-5)
+    float roughness;  // diffuse roughness (Lambert below 1e-5); glossy roughness (alpha = roughness^2)
 };
 
 struct SurfaceClosures {
@@ -333,20 +344,63 @@ struct SurfaceClosures {
     float3 emission{};
 };
 
-// Closure allocation (graph_surface_state.cpp:26-48): diffuse goes through
-// bsdf_alloc (negative weight clamped, average cutoff 1e-5); transparent
-// keeps its signed weight and uses the same cutoff on |average|.
-static SurfaceClosures collect_surface(const Material &mat, float3 shading_normal) {
+// The surface point's inputs to closure setup, evaluation and sampling.
+struct ClosurePoint {
+    float3 shading_normal;   // SurfacePoint::shading_normal
+    float3 geometric_normal; // SurfacePoint::geometric_normal (facing the incoming ray)
+    float3 incoming;         // SurfacePoint::incoming (-ray direction)
+    bool bump_correction;    // SurfacePoint::use_bump_map_correction
+};
+
+// ensure_valid_specular_reflection (src/luisa/graph_surface_scattering.cpp:119-155):
+// a shading normal whose mirror direction of `incoming` would dip below the
+// geometric surface is tilted toward the geometric normal until the
+// reflection clears it by min(0.9 cos_i, 0.01).
+static float3 ensure_valid_specular_reflection(float3 ng, float3 incoming, float3 n) {
+    const float3 reflected = 2.0f * dot(n, incoming) * n - incoming;
+    const float ig = maxf(dot(incoming, ng), 0.0f);
+    const float threshold = minf(0.9f * ig, 0.01f);
+    const bool valid = dot(ng, reflected) >= threshold;
+    const float3 tangent = safe_normalize(n - dot(n, ng) * ng, n);
+    const float it = dot(incoming, tangent);
+    const float a = it * it + ig * ig;
+    const float b = 2.0f * (a + ig * threshold);
+    const float c = (threshold + ig) * (threshold + ig);
+    const float disc = maxf(b * b - 4.0f * a * c, 0.0f);
+    const float signed_root = it < 0.0f ? b + std::sqrt(disc) : b - std::sqrt(disc);
+    const float nz2 = clampf(0.25f * signed_root / maxf(a, 1.0e-20f), 0.0f, 1.0f);
+    const float3 corrected =
+        safe_normalize(std::sqrt(maxf(1.0f - nz2, 0.0f)) * tangent + std::sqrt(nz2) * ng, ng);
+    return (!valid && a > 1.0e-20f) ? corrected : n;
+}
+
+// maybe_ensure_valid_specular_reflection (graph_surface_scattering.cpp:157-168).
+static float3 specular_normal(bool correction, float3 ng, float3 incoming, float3 n) {
+    const bool equal = ng.x == n.x && ng.y == n.y && ng.z == n.z;
+    return correction && !equal ? ensure_valid_specular_reflection(ng, incoming, n) : n;
+}
+
+// Closure allocation (graph_surface_state.cpp:26-48,
+// graph_surface_physical_closures.cpp:158-520): diffuse goes through
+// bsdf_alloc (negative weight clamped, average cutoff 1e-5); glossy is
+// allocated the same way (reflective caustics on), its normal corrected
+// for a valid specular reflection and its weight kept (GGX / Beckmann
+// without energy preservation: darkening and evaluation scale one);
+// transparent keeps its signed weight, uses the cutoff on |average|, and
+// every allocated transparent contribution merges into the first one
+// (bsdf_transparent_setup, :483-518: summed weights and sample weights).
+static SurfaceClosures collect_surface(const Material &mat, const ClosurePoint &pt) {
     std::vector<TracedClosure> traced;
     walk_closures(mat, mat.root, 1.0f, traced, 0);
     SurfaceClosures s;
-    const float3 closure_normal = safe_normalize(shading_normal, shading_normal);
+    const float3 closure_normal = safe_normalize(pt.shading_normal, pt.shading_normal);
+    const float3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
+    int transparent_slot = -1;
     for (const auto &t : traced) {
         if (t.op == PSY_CLOSURE_EMISSION) {
             s.emission += t.weight;
             continue;
         }
-        if (s.count >= kMaxClosures) continue;
         PhysicalClosure p;
         p.op = t.op;
         p.color = t.color;
@@ -356,20 +410,34 @@ static SurfaceClosures collect_surface(const Material &mat, float3 shading_norma
             p.sample_weight = closure_sample_weight(p.weight);
             p.normal = closure_normal;
             if (!(p.weight.x != 0.0f || p.weight.y != 0.0f || p.weight.z != 0.0f)) continue;
+        } else if (is_glossy(t.op)) {
+            const float3 allocated = max3(t.weight, f3(0.0f));
+            const float allocation = closure_sample_weight(allocated);
+            if (!(allocation >= 1.0e-5f)) continue;
+            p.weight = allocated;
+            p.sample_weight = allocation * closure_sample_weight(f3(1.0f));
+            p.normal = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, closure_normal);
         } else {
             const float sw = closure_sample_weight(t.weight);
             if (!(sw >= 1.0e-5f)) continue;
+            if (transparent_slot >= 0) {
+                s.c[transparent_slot].weight += t.weight;
+                s.c[transparent_slot].sample_weight += sw;
+                continue;
+            }
             p.weight = t.weight;
             p.sample_weight = sw;
-            p.normal = shading_normal;
+            p.normal = pt.shading_normal;
         }
+        if (s.count >= kMaxClosures) continue;
+        if (t.op == PSY_CLOSURE_TRANSPARENT) transparent_slot = int(s.count);
         s.c[s.count++] = p;
     }
     return s;
 }
 
 // Cycles ClosureLabel / runtime-flag constants
-// (include/psycles/luisa/cycles_closure.h:39-63) and contract surface
+// (include/psycles/luisa/cycles_closure.h:39-66) and contract surface
 // events (include/psycles/contract/surface.h).
 constexpr uint32_t kEventReflection = 1u, kEventTransmission = 2u, kEventDiffuse = 4u, kEventGlossy = 8u,
                    kEventSingular = 16u, kEventTransparent = 32u;
@@ -377,6 +445,7 @@ constexpr uint32_t kLabelTransmit = 1u, kLabelReflect = 2u, kLabelDiffuse = 4u, 
                    kLabelSingular = 16u, kLabelTransparent = 32u;
 constexpr uint32_t kRuntimeBackfacing = 1u, kRuntimeEmission = 4u, kRuntimeBsdf = 8u, kRuntimeBsdfHasEval = 16u,
                    kRuntimeTransparent = 1024u, kRuntimeBsdfHasTransmission = 2048u;
+constexpr float kMicrofacetSingularAlphaProduct = 2.0e-10f;
 
 // cycles_closure::label_from_events (cycles_closure.h:67-112).
 static uint32_t label_from_events(uint32_t e) {
@@ -390,27 +459,109 @@ static uint32_t label_from_events(uint32_t e) {
     return l;
 }
 
-// cycles_runtime_flags (src/luisa/graph_surface_scattering.cpp:292-345)
+// microfacet_alpha / microfacet_is_singular (graph_surface_scattering.cpp:549-568)
+// without the glossy filter (its roughness is zero: Filter Glossy off).
+static float microfacet_alpha(float roughness) {
+    const float a = clampf(roughness, 0.0f, 1.0f);
+    return a * a;
+}
+static bool microfacet_singular(float roughness) {
+    const float a = microfacet_alpha(roughness);
+    return a * a <= kMicrofacetSingularAlphaProduct;
+}
+
+// cycles_runtime_flags (src/luisa/graph_surface_scattering.cpp:292-365)
 // for the in-scope closures, plus the back-facing bit.
 static uint32_t runtime_flags(const SurfaceClosures &s, bool back_facing) {
     uint32_t f = back_facing ? kRuntimeBackfacing : 0u;
     for (uint32_t i = 0; i < s.count; ++i) {
-        if (s.c[i].op == PSY_CLOSURE_DIFFUSE) f |= kRuntimeBsdf | kRuntimeBsdfHasEval;
+        const PhysicalClosure &c = s.c[i];
+        if (c.op == PSY_CLOSURE_DIFFUSE) f |= kRuntimeBsdf | kRuntimeBsdfHasEval;
+        else if (is_glossy(c.op)) f |= kRuntimeBsdf | (microfacet_singular(c.roughness) ? 0u : kRuntimeBsdfHasEval);
         else f |= kRuntimeBsdf | kRuntimeTransparent;
     }
     return f;
 }
 
-// bump_shadowing_term (graph_surface_scattering.cpp:219-281) for a diffuse
-// closure without bump correction.
-static float bump_shadowing(float3 smooth_normal, float3 closure_normal, float3 direction) {
+// bump_shadowing_term (graph_surface_scattering.cpp:219-281) of a diffuse
+// or glossy closure: one when the closure normal is the shading normal;
+// otherwise a direction on the wrong side of the smooth surface is rejected
+// during evaluation (and, for diffuse closures, also when sampling), and
+// a diffuse closure under bump correction gets the smoothed shadowing
+// factor.
+static float bump_shadowing(float3 smooth_normal, float3 closure_normal, float3 direction, bool is_evaluation,
+                            bool diffuse, bool bump_correction) {
     if (closure_normal.x == smooth_normal.x && closure_normal.y == smooth_normal.y &&
         closure_normal.z == smooth_normal.z)
         return 1.0f;
     const float csd = dot(smooth_normal, direction);
     const float csc = dot(smooth_normal, closure_normal);
     const float ccd = dot(closure_normal, direction);
-    return (csd * csc * ccd < 0.0f) ? 0.0f : 1.0f;
+    const bool reject = csd * csc * ccd < 0.0f && (is_evaluation || diffuse);
+    const float cos_i = std::fabs(csd);
+    const float cos_d = std::fabs(csc);
+    const float tan_d2 = maxf(1.0f / maxf(cos_d * cos_d, 1.0e-20f) - 1.0f, 0.0f);
+    const float bump_alpha2 = clampf(0.125f * tan_d2, 0.0f, 1.0f);
+    const float tan_i2 = maxf(1.0f / maxf(cos_i * cos_i, 1.0e-20f) - 1.0f, 0.0f);
+    const float lambda = 0.5f * (std::sqrt(1.0f + bump_alpha2 * tan_i2) - 1.0f);
+    const float smoothed = 1.0f / (1.0f + lambda);
+    const bool domain = diffuse && bump_correction && cos_d < 1.0f && cos_i < 1.0f;
+    const bool grazing = domain && cos_i < 1.0e-6f;
+    float result = domain && !grazing ? smoothed : 1.0f;
+    if (reject || grazing) result = 0.0f;
+    return result;
+}
+
+// microfacet_distribution / microfacet_lambda (graph_surface_scattering.cpp:508-547).
+static float microfacet_distribution(bool beckmann, float n_dot_h, float alpha) {
+    const float alpha2 = alpha * alpha;
+    const float cosine2 = minf(n_dot_h * n_dot_h, 1.0f);
+    const float one_minus = 1.0f - cosine2;
+    if (!beckmann) {
+        const float den = one_minus + alpha2 * cosine2;
+        return alpha2 / maxf(kPi * den * den, 1.0e-20f);
+    }
+    const float exponent = one_minus / (cosine2 * alpha2);
+    return 1.0f / (exp_(exponent) * kPi * alpha2 * cosine2 * cosine2);
+}
+static float microfacet_lambda(bool beckmann, float n_dot_v, float alpha) {
+    const float cosine2 = n_dot_v * n_dot_v;
+    const float sat = alpha * alpha * maxf(1.0f / cosine2 - 1.0f, 0.0f);
+    if (!beckmann) return 0.5f * (std::sqrt(1.0f + sat) - 1.0f);
+    const float a = 1.0f / std::sqrt(sat);
+    const float approximation = ((0.396f * a - 1.259f) * a + 1.0f) / ((2.181f * a + 3.535f) * a);
+    return sat < 0.39f ? 0.0f : approximation;
+}
+
+// microfacet_intensity and microfacet_pdf (graph_surface_scattering.cpp:665-728)
+// of a standalone glossy closure (Fresnel constant one: its colour is in
+// the closure weight).
+static float microfacet_intensity(const PhysicalClosure &c, float3 incoming, float3 outgoing, float3 gn) {
+    const bool beckmann = (c.op & kBeckmann) != 0u;
+    const float ndv = maxf(dot(gn, incoming), 0.0f);
+    const float ndl = maxf(dot(gn, outgoing), 0.0f);
+    const float3 h = safe_normalize(incoming + outgoing, gn);
+    const float ndh = maxf(dot(gn, h), 0.0f);
+    const float vdh = maxf(dot(incoming, h), 0.0f);
+    const bool singular = microfacet_singular(c.roughness);
+    const float alpha = maxf(microfacet_alpha(c.roughness), 1.0e-10f);
+    const float d = microfacet_distribution(beckmann, ndh, alpha);
+    const float g = 1.0f / (1.0f + microfacet_lambda(beckmann, ndv, alpha) + microfacet_lambda(beckmann, ndl, alpha));
+    const float intensity = d * g / maxf(4.0f * ndv, 1.0e-20f);
+    return (ndv > 0.0f && ndl > 0.0f && ndh > 0.0f && vdh > 0.0f && !singular) ? intensity : 0.0f;
+}
+static float microfacet_pdf(const PhysicalClosure &c, float3 incoming, float3 outgoing, float3 gn) {
+    const bool beckmann = (c.op & kBeckmann) != 0u;
+    const float3 h = safe_normalize(incoming + outgoing, gn);
+    const float ndh = maxf(dot(gn, h), 0.0f);
+    const float vdh = maxf(dot(incoming, h), 0.0f);
+    const bool singular = microfacet_singular(c.roughness);
+    const float alpha = maxf(microfacet_alpha(c.roughness), 1.0e-10f);
+    const float ndv = maxf(dot(gn, incoming), 0.0f);
+    const float ndl = maxf(dot(gn, outgoing), 0.0f);
+    const float pdf = microfacet_distribution(beckmann, ndh, alpha) / maxf(4.0f * ndv, 1.0e-20f) /
+                      (1.0f + microfacet_lambda(beckmann, ndv, alpha));
+    return (ndv > 0.0f && ndl > 0.0f && ndh > 0.0f && vdh > 0.0f && !singular) ? pdf : 0.0f;
 }
 
 struct Evaluation {
@@ -420,11 +571,6 @@ struct Evaluation {
     uint32_t events{0u};
 };
 
-// Mixture evaluation of every retained closure in a direction
-// (surface_closure_evaluation_contribution, src/luisa/surface_closure_evaluation.cpp:71-394,
-// and SurfaceClosureEvaluationAccumulator::finish :410-438).  `selected`
-// marks the closure that produced the direction (its pdf survives a zero
-// bump term).
 // oren_nayar_g (src/luisa/graph_surface_scattering.cpp:463-473).
 static float oren_nayar_g(float cosine) {
     const float c = clampf(cosine, 0.0f, 1.0f);
@@ -464,12 +610,19 @@ static float3 diffuse_intensity(const PhysicalClosure &c, float3 incoming, float
     return (f3(single_scatter) + multiscatter * (1.0f - e_outgoing)) * nl;
 }
 
-static Evaluation evaluate_mixture(const SurfaceClosures &s, float3 shading_normal, float3 incoming,
-                                   float3 outgoing_raw, uint32_t lobe_mask, int selected) {
-    const float3 outgoing = safe_normalize(outgoing_raw, shading_normal);
+// Mixture evaluation of every retained closure in a direction
+// (surface_closure_evaluation_contribution, src/luisa/surface_closure_evaluation.cpp:61-394,
+// and SurfaceClosureEvaluationAccumulator::finish :410-438).  `selected`
+// marks the closure that produced the direction (its pdf survives a zero
+// bump term, and a glossy closure is not rejected for it).
+static Evaluation evaluate_mixture(const SurfaceClosures &s, const ClosurePoint &pt, float3 outgoing_raw,
+                                   uint32_t lobe_mask, int selected) {
+    const float3 outgoing = safe_normalize(outgoing_raw, pt.shading_normal);
+    const float3 incoming = safe_normalize(pt.incoming, -outgoing);
     Evaluation e;
     float total = 0.0f, weighted_pdf = 0.0f;
     const bool diffuse_enabled = (lobe_mask & kEventDiffuse) != 0u;
+    const bool glossy_enabled = (lobe_mask & kEventGlossy) != 0u;
     const bool transparent_enabled = (lobe_mask & kEventTransparent) != 0u;
     for (uint32_t i = 0; i < s.count; ++i) {
         const PhysicalClosure &c = s.c[i];
@@ -477,11 +630,25 @@ static Evaluation evaluate_mixture(const SurfaceClosures &s, float3 shading_norm
             if (transparent_enabled) total += c.sample_weight;
             continue;
         }
-        const float bump = bump_shadowing(shading_normal, c.normal, outgoing);
-        const bool pdf_valid = bump != 0.0f || int(i) == selected;
+        const bool glossy = is_glossy(c.op);
+        const bool is_selected = int(i) == selected;
+        const float bump = bump_shadowing(pt.shading_normal, c.normal, outgoing, !is_selected, !glossy,
+                                          pt.bump_correction);
+        const bool pdf_valid = bump != 0.0f || is_selected;
+        if (glossy) {
+            if (!glossy_enabled) continue;  // any_allowed false: no weight, no pdf
+            const float3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.normal);
+            const float pdf = pdf_valid ? microfacet_pdf(c, incoming, outgoing, gn) : 0.0f;
+            const float3 value = c.weight * microfacet_intensity(c, incoming, outgoing, gn) * bump;
+            e.f += value;
+            total += c.sample_weight;
+            weighted_pdf += c.sample_weight * pdf;
+            if (closure_sample_weight(value) > 0.0f) e.events |= kEventGlossy | kEventReflection;
+            continue;
+        }
         float pdf = maxf(dot(c.normal, outgoing), 0.0f) * kInvPi;
         if (!pdf_valid) pdf = 0.0f;
-        if (!diffuse_enabled) continue;  // any_allowed false: no weight, no pdf
+        if (!diffuse_enabled) continue;
         const float3 value = c.weight * diffuse_intensity(c, incoming, outgoing) * bump;
         e.f += value;
         e.diffuse_f += value;
@@ -503,16 +670,23 @@ struct SurfaceSample {
 
 // Closure selection + conditional sample + mixture (SurfaceClosureSamplingVisitor::visit,
 // src/luisa/surface_closure_sampling_core.cpp:744-812; selection :97-214;
-// categorical inversion :420-437; conditional sample :216-337; finish :490-700).
-static SurfaceSample sample_surface(const SurfaceClosures &s, float3 shading_normal, float3 geometric_normal,
-                                    float3 incoming, float u_lobe, float2 u_dir, uint32_t lobe_mask) {
+// categorical inversion :420-437; conditional sample :216-337, glossy
+// sample_microfacet_reflection graph_surface_scattering.cpp:730-770;
+// finish :490-660).
+static SurfaceSample sample_surface(const SurfaceClosures &s, const ClosurePoint &pt, float u_lobe, float2 u_dir,
+                                    uint32_t lobe_mask) {
     SurfaceSample out;
     const bool diffuse_enabled = (lobe_mask & kEventDiffuse) != 0u;
+    const bool glossy_enabled = (lobe_mask & kEventGlossy) != 0u;
     const bool transparent_enabled = (lobe_mask & kEventTransparent) != 0u;
+    const float3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
     float weights[kMaxClosures];
     float total = 0.0f;
     for (uint32_t i = 0; i < s.count; ++i) {
-        const bool eligible = s.c[i].op == PSY_CLOSURE_DIFFUSE ? diffuse_enabled : transparent_enabled;
+        const uint32_t op = s.c[i].op;
+        const bool eligible = op == PSY_CLOSURE_DIFFUSE ? diffuse_enabled
+                              : is_glossy(op)           ? glossy_enabled
+                                                        : transparent_enabled;
         weights[i] = eligible ? s.c[i].sample_weight : 0.0f;
         total += weights[i];
     }
@@ -529,17 +703,29 @@ static SurfaceSample sample_surface(const SurfaceClosures &s, float3 shading_nor
     const PhysicalClosure &c = s.c[chosen];
     float3 direction;
     const bool transparent = c.op == PSY_CLOSURE_TRANSPARENT;
+    const bool glossy = is_glossy(c.op);
+    bool candidate_valid = true, singular = false;
     if (transparent) {
-        direction = -incoming;
+        direction = pt.incoming * -1.0f;
+    } else if (glossy) {
+        const float3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.normal);
+        const float alpha = microfacet_alpha(c.roughness);
+        const float sampling_alpha = maxf(alpha, 1.0e-10f);
+        const float3 h = (c.op & kBeckmann) != 0u ? sample_beckmann_visible_normal(gn, incoming, sampling_alpha, u_dir)
+                                                  : sample_ggx_visible_normal(gn, incoming, sampling_alpha, u_dir);
+        singular = alpha * alpha <= kMicrofacetSingularAlphaProduct;
+        direction = singular ? 2.0f * dot(gn, incoming) * gn - incoming : 2.0f * dot(incoming, h) * h - incoming;
+        candidate_valid = dot(gn, incoming) > 0.0f && dot(gn, direction) > 0.0f &&
+                          dot(pt.geometric_normal, direction) > 0.0f;
     } else {
         direction = sample_cosine_hemisphere(c.normal, u_dir).direction;
     }
-    const bool geometric_valid = dot(geometric_normal, direction) > 0.0f;
-    const bool sample_valid = transparent || geometric_valid;
+    const bool geometric_valid = dot(pt.geometric_normal, direction) > 0.0f;
+    const bool sample_valid = candidate_valid && (transparent || geometric_valid);
     out.closure_index = uint32_t(chosen);
     out.wi = direction;
     if (!sample_valid) return out;
-    Evaluation mixture = evaluate_mixture(s, shading_normal, incoming, direction, lobe_mask, chosen);
+    Evaluation mixture = evaluate_mixture(s, pt, direction, lobe_mask, chosen);
     Evaluation r;
     r.f = mixture.f;
     r.diffuse_f = mixture.diffuse_f;
@@ -547,9 +733,16 @@ static SurfaceSample sample_surface(const SurfaceClosures &s, float3 shading_nor
     if (transparent) {
         r.f += c.weight * 1.0e6f;
         delta_pdf_numerator = 1.0e6f * weights[chosen];
+    } else if (glossy && singular) {
+        // singular_evaluation = weight x Fresnel (one) x bump term (one
+        // when sampling a glossy closure) x 1e6, singular pdf 1e6
+        r.f += c.weight * 1.0e6f;
+        delta_pdf_numerator = 1.0e6f * weights[chosen];
     }
     r.pdf = mixture.pdf + delta_pdf_numerator / maxf(total, 1.0e-20f);
-    r.events = transparent ? (kEventTransmission | kEventTransparent) : (kEventDiffuse | kEventReflection);
+    if (transparent) r.events = kEventTransmission | kEventTransparent;
+    else if (glossy) r.events = singular ? (kEventSingular | kEventReflection) : (kEventGlossy | kEventReflection);
+    else r.events = kEventDiffuse | kEventReflection;
     out.eval = r;
     out.valid = true;
     return out;
@@ -559,8 +752,9 @@ static SurfaceSample sample_surface(const SurfaceClosures &s, float3 shading_nor
 struct Aov {
     float3 albedo, normal, transparency;
 };
-static Aov surface_aov(const SurfaceClosures &s, float3 shading_normal) {
-    Aov a{f3(0.0f), shading_normal, f3(0.0f)};
+static Aov surface_aov(const SurfaceClosures &s, const ClosurePoint &pt) {
+    Aov a{f3(0.0f), pt.shading_normal, f3(0.0f)};
+    const float3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
     float total = 0.0f;
     float3 normal = f3(0.0f);
     for (uint32_t i = 0; i < s.count; ++i) {
@@ -570,11 +764,17 @@ static Aov surface_aov(const SurfaceClosures &s, float3 shading_normal) {
             const float w = closure_sample_weight(c.weight);
             normal += c.normal * w;
             total += w;
+        } else if (is_glossy(c.op)) {
+            // glossy colour is not in the Albedo pass; its corrected normal
+            // is in the Normal pass
+            const float w = closure_sample_weight(c.weight);
+            normal += specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.normal) * w;
+            total += w;
         } else {
             a.transparency += c.weight;
         }
     }
-    a.normal = safe_normalize(total > 0.0f ? normal : shading_normal, shading_normal);
+    a.normal = safe_normalize(total > 0.0f ? normal : pt.shading_normal, pt.shading_normal);
     return a;
 }
 
@@ -1832,7 +2032,8 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
         }
         const SurfacePoint sp = surface_point(s, hit, ray);
         const Material &mat = s.materials[sp.material];
-        const SurfaceClosures closures = collect_surface(mat, sp.n);
+        const ClosurePoint cpt{sp.n, sp.ng, -ray.d, mat.bump_correction};
+        const SurfaceClosures closures = collect_surface(mat, cpt);
         // SurfaceShadingStageImpl::emit (src/luisa/path_kernel_surface_shading.cpp:117-250)
         float emission_weight = 1.0f;
         if (nee && !s.emitters.empty() && mat.emission_sampling != 0u && mat.has_emission) {
@@ -1871,7 +2072,7 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
             throughput /= cp;
         }
         if (depth == 0u) {
-            const Aov aov = surface_aov(closures, sp.n);
+            const Aov aov = surface_aov(closures, cpt);
             out.albedo += throughput * aov.albedo;
             const float3 alpha = clamp3(f3(1.0f) - aov.transparency, 0.0f, 1.0f);
             const float average_alpha = (alpha.x + alpha.y + alpha.z) * (1.0f / 3.0f);
@@ -1917,7 +2118,7 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
                     const bool reject_self = same_primitive && dot(ls.direction, oriented) > 0.0f;
                     if (!reject_self) {
                         const float3 light_radiance = material_emission(s.materials[em.material]);
-                        const Evaluation e = evaluate_mixture(closures, sp.n, -ray.d, ls.direction, lobe_mask, -1);
+                        const Evaluation e = evaluate_mixture(closures, cpt, ls.direction, lobe_mask, -1);
                         float mis = 1.0f;
                         mis = nee_light_weight(mode, pdf, e.pdf);
                         const float3 weighted = e.f * light_radiance * (mis / pdf);
@@ -1950,7 +2151,7 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
                     const float light_pdf = a.pdf * selected.selection_pdf;
                     if (a.valid && light_pdf > 0.0f) {
                         const float3 light_radiance = f3(l.color[0], l.color[1], l.color[2]) * (l.power * a.eval_factor);
-                        const Evaluation e = evaluate_mixture(closures, sp.n, -ray.d, a.direction, lobe_mask, -1);
+                        const Evaluation e = evaluate_mixture(closures, cpt, a.direction, lobe_mask, -1);
                         // MIS only for lamps a BSDF ray can also hit (path_kernel_nee_analytic.cpp:286-292)
                         const float mis = (l.flags & kLightForward) != 0u ? nee_light_weight(mode, light_pdf, e.pdf) : 1.0f;
                         const float3 weighted = e.f * light_radiance * (mis / maxf(light_pdf, 1.0e-20f));
@@ -1976,8 +2177,8 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
             if (ev) trace_set3(ev->nee, contribution);
         }
         // SurfaceScatterStageImpl::emit (src/luisa/path_kernel_surface_scatter.cpp:136-291)
-        const SurfaceSample ss = sample_surface(closures, sp.n, sp.ng, -ray.d, bsdf_sample.z,
-                                                f2(bsdf_sample.x, bsdf_sample.y), lobe_mask);
+        const SurfaceSample ss = sample_surface(closures, cpt, bsdf_sample.z, f2(bsdf_sample.x, bsdf_sample.y),
+                                                lobe_mask);
         if (ev) {
             ev->closure_index = ss.closure_index;
             ev->bsdf_pdf = ss.eval.pdf;
@@ -2070,6 +2271,7 @@ static std::unique_ptr<Scene> prepare_scene(const psy_scene_desc *d, bool brute_
         for (uint32_t v = 0; v < md.vector_count; ++v)
             m.vectors.push_back(f3(md.vectors[3 * v], md.vectors[3 * v + 1], md.vectors[3 * v + 2]));
         m.emission_sampling = md.emission_sampling;
+        m.bump_correction = (md.flags & PSY_MATERIAL_NO_BUMP_MAP_CORRECTION) == 0u;
         m.has_emission = program_has(m, PSY_CLOSURE_EMISSION);
         m.has_transparent = program_has(m, PSY_CLOSURE_TRANSPARENT);
         s->materials.push_back(std::move(m));
@@ -2323,6 +2525,16 @@ void oracle_sample_cosine_hemisphere(const float *n, const float *r, float *out_
     out_dir[1] = h.direction.y;
     out_dir[2] = h.direction.z;
     *out_pdf = h.pdf;
+}
+// Visible-normal samples of the glossy closures (`beckmann` 0: GGX).
+void oracle_sample_visible_normal(int beckmann, const float *n, const float *incoming, float alpha, const float *r,
+                                  float *out_half) {
+    const float3 nn = f3(n[0], n[1], n[2]), in = f3(incoming[0], incoming[1], incoming[2]);
+    const float3 h = beckmann ? sample_beckmann_visible_normal(nn, in, alpha, f2(r[0], r[1]))
+                              : sample_ggx_visible_normal(nn, in, alpha, f2(r[0], r[1]));
+    out_half[0] = h.x;
+    out_half[1] = h.y;
+    out_half[2] = h.z;
 }
 void oracle_make_orthonormals(const float *n, float *t, float *b) {
     const Basis bs = make_orthonormals(f3(n[0], n[1], n[2]));

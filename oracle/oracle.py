@@ -51,6 +51,7 @@ def load() -> ctypes.CDLL:
         lib.oracle_scene_emitter_count.restype = ctypes.c_uint32
         lib.oracle_pixel_filter_table.argtypes = [ctypes.c_uint32, ctypes.c_float, vp]
         lib.oracle_sample_cosine_hemisphere.argtypes = [vp, vp, vp, vp]
+        lib.oracle_sample_visible_normal.argtypes = [ctypes.c_int, vp, vp, ctypes.c_float, vp, vp]
         lib.oracle_next_surface.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
         lib.oracle_diffuse_intensity.argtypes = [vp, vp, ctypes.c_float, vp, vp, vp]
         _lib = lib

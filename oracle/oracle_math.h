@@ -173,6 +173,8 @@ inline float pow_(float x, float y) {
     return static_cast<float>(std::pow(static_cast<double>(x), static_cast<double>(y)));
 }
 inline float tan_(float x) { return static_cast<float>(std::tan(static_cast<double>(x))); }
+inline float exp_(float x) { return static_cast<float>(std::exp(static_cast<double>(x))); }
+inline float log_(float x) { return static_cast<float>(std::log(static_cast<double>(x))); }
 inline float atan2_(float y, float x) {
     return static_cast<float>(std::atan2(static_cast<double>(y), static_cast<double>(x)));
 }

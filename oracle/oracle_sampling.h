@@ -316,6 +316,125 @@ inline HemisphereSample sample_cosine_hemisphere(float3 n, float2 r) {
     return {b.tangent * d.x + b.bitangent * d.y + n * c, c * kInvPi};
 }
 
+// sample_ggx_visible_normal (cycles_sample_mapping.h:131-183): Heitz 2018,
+// "Sampling the GGX Distribution of Visible Normals", in the frame of
+// make_orthonormals(normal) with the concentric disk map; the half vector
+// is not renormalised in world space.
+inline float3 sample_ggx_visible_normal(float3 normal, float3 incoming, float alpha, float2 random) {
+    const Basis w = make_orthonormals(normal);
+    const float3 li = f3(dot(w.tangent, incoming), dot(w.bitangent, incoming), dot(normal, incoming));
+    const float3 si = normalize(f3(alpha * li.x, alpha * li.y, li.z));
+    const float pl2 = si.x * si.x + si.y * si.y;
+    const float3 pt = f3(-si.y, si.x, 0.0f) / std::sqrt(maxf(pl2, 1.0e-20f));
+    const float3 bx = pl2 > 1.0e-7f ? pt : f3(1.0f, 0.0f, 0.0f);
+    const float3 by = cross(si, bx);
+    float2 disk = sample_uniform_disk(random);
+    const float projected_area = 0.5f * (1.0f + si.z);
+    disk.y = lerp(std::sqrt(maxf(1.0f - disk.x * disk.x, 0.0f)), disk.y, projected_area);
+    const float hz = std::sqrt(maxf(1.0f - disk.x * disk.x - disk.y * disk.y, 0.0f));
+    const float3 sh = bx * disk.x + by * disk.y + si * hz;
+    const float3 lh = normalize(f3(alpha * sh.x, alpha * sh.y, maxf(sh.z, 0.0f)));
+    return w.tangent * lh.x + w.bitangent * lh.y + normal * lh.z;
+}
+
+// erf of Abramowitz & Stegun 7.1.28 (1 - 1 / (1 + a1 x + ... + a6 x^6)^16,
+// |error| <= 3e-7) as Cycles evaluates it (cycles_sample_mapping.h:188-208):
+// Horner steps as fused multiply-adds, +-1 beyond |x| = 12.3.
+inline float fast_erf(float value) {
+    const float magnitude = std::fabs(value);
+    const float crushed = 1.0f - (1.0f - magnitude);
+    float p = std::fmaf(0.0000430638f, crushed, 0.0002765672f);
+    p = std::fmaf(p, crushed, 0.0001520143f);
+    p = std::fmaf(p, crushed, 0.0092705272f);
+    p = std::fmaf(p, crushed, 0.0422820123f);
+    p = std::fmaf(p, crushed, 0.0705230784f);
+    p = std::fmaf(p, crushed, 1.0f);
+    const float square = p * p;
+    const float fourth = square * square;
+    const float eighth = fourth * fourth;
+    const float sixteenth = eighth * eighth;
+    const float unsigned_result = 1.0f - 1.0f / sixteenth;
+    if (magnitude >= 12.3f) return value >= 0.0f ? 1.0f : -1.0f;
+    return value >= 0.0f ? unsigned_result : -unsigned_result;
+}
+
+// erfinv of Giles, "Approximating the erfinv function" (GPU Computing Gems,
+// 2011), single-precision branch pair on w = -log((1 - x)(1 + x)), as
+// Cycles evaluates it (cycles_sample_mapping.h:210-237).
+inline float fast_inverse_erf(float value) {
+    const float magnitude = minf(std::fabs(value), 0.99999994f);
+    const float base = -log_((1.0f - magnitude) * (1.0f + magnitude));
+    const float cx = base - 2.5f;
+    float central = std::fmaf(2.81022636e-08f, cx, 3.43273939e-07f);
+    central = std::fmaf(central, cx, -3.5233877e-06f);
+    central = std::fmaf(central, cx, -4.39150654e-06f);
+    central = std::fmaf(central, cx, 0.00021858087f);
+    central = std::fmaf(central, cx, -0.00125372503f);
+    central = std::fmaf(central, cx, -0.00417768164f);
+    central = std::fmaf(central, cx, 0.246640727f);
+    central = std::fmaf(central, cx, 1.50140941f);
+    const float tx = std::sqrt(base) - 3.0f;
+    float tail = std::fmaf(-0.000200214257f, tx, 0.000100950558f);
+    tail = std::fmaf(tail, tx, 0.00134934322f);
+    tail = std::fmaf(tail, tx, -0.00367342844f);
+    tail = std::fmaf(tail, tx, 0.00573950773f);
+    tail = std::fmaf(tail, tx, -0.0076224613f);
+    tail = std::fmaf(tail, tx, 0.00943887047f);
+    tail = std::fmaf(tail, tx, 1.00167406f);
+    tail = std::fmaf(tail, tx, 2.83297682f);
+    return (base < 5.0f ? central : tail) * value;
+}
+
+// sample_beckmann_visible_normal (cycles_sample_mapping.h:239-310): the
+// visible-slope sampler of Heitz and d'Eon (2014) with Cycles' root solve
+// -- a quadratic first guess, at most three Newton steps kept inside the
+// bracket (bisection otherwise) -- in the frame of make_orthonormals(normal).
+inline float3 sample_beckmann_visible_normal(float3 normal, float3 incoming, float alpha, float2 random) {
+    const Basis w = make_orthonormals(normal);
+    const float3 li = f3(dot(w.tangent, incoming), dot(w.bitangent, incoming), dot(normal, incoming));
+    const float3 si = normalize(f3(alpha * li.x, alpha * li.y, li.z));
+    const float normal_radius = std::sqrt(-log_(random.x));
+    const float normal_phi = 2.0f * kPi * random.y;
+    const float2 normal_slope = f2(normal_radius * cos_(normal_phi), normal_radius * sin_(normal_phi));
+    const float cosine = si.z;
+    const float sine = std::sqrt(maxf(1.0f - cosine * cosine, 0.0f));
+    const float safe_cosine = cosine != 0.0f ? cosine : 1.0f;
+    const float safe_sine = sine != 0.0f ? sine : 1.0f;
+    const float tangent = sine / safe_cosine;
+    const float safe_tangent = tangent != 0.0f ? tangent : 1.0f;
+    const float cotangent = 1.0f / safe_tangent;
+    const float erf_a = fast_erf(cotangent);
+    const float exponential = exp_(-cotangent * cotangent);
+    const float cosine_phi = sine != 0.0f ? si.x / safe_sine : 1.0f;
+    const float sine_phi = sine != 0.0f ? si.y / safe_sine : 0.0f;
+    const float k = tangent * 0.56418958354f;
+    const float approximate_y = random.x * (1.0f + erf_a + k * (1.0f - erf_a * erf_a));
+    const float exact_y = random.x * (1.0f + erf_a + k * exponential);
+    const float safe_k = k > 0.0f ? k : 1.0f;
+    const float quadratic_b = (0.5f - std::sqrt(maxf(k * (k - approximate_y + 1.0f) + 0.25f, 0.0f))) / safe_k;
+    const float b = k > 0.0f ? quadratic_b : approximate_y - 1.0f;
+    float inverse_erf = fast_inverse_erf(b);
+    float2 begin = f2(-1.0f, -exact_y);
+    float2 end = f2(erf_a, 1.0f + erf_a + k * exponential - exact_y);
+    float2 current = f2(b, 1.0f + b + k * exp_(-inverse_erf * inverse_erf) - exact_y);
+    for (uint32_t iteration = 0; std::fabs(current.y) > 1.0e-6f && iteration < 3u; ++iteration) {
+        const bool same_sign = (begin.y < 0.0f) == (current.y < 0.0f);
+        if (same_sign) begin = current;
+        else end.x = current.x;
+        const float newton = current.x - current.y / (1.0f - inverse_erf * tangent);
+        const bool inside = newton >= begin.x && newton <= end.x;
+        current.x = inside ? newton : 0.5f * (begin.x + end.x);
+        inverse_erf = fast_inverse_erf(current.x);
+        current.y = 1.0f + current.x + k * exp_(-inverse_erf * inverse_erf) - exact_y;
+    }
+    const float2 general_slope = f2(inverse_erf, fast_inverse_erf(2.0f * random.y - 1.0f));
+    const float2 slope = si.z >= 0.99999f ? normal_slope : general_slope;
+    const float2 rotated = f2(cosine_phi * slope.x - sine_phi * slope.y, sine_phi * slope.x + cosine_phi * slope.y) *
+                           alpha;
+    const float3 lh = normalize(f3(-rotated.x, -rotated.y, 1.0f));
+    return w.tangent * lh.x + w.bitangent * lh.y + normal * lh.z;
+}
+
 // sin_squared_to_one_minus_cosine (cycles_sample_mapping.h:302-309).
 inline float sin_squared_to_one_minus_cosine(float s2) {
     return s2 > 0.0004f ? 1.0f - std::sqrt(maxf(1.0f - s2, 0.0f)) : 0.5f * s2;

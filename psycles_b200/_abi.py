@@ -23,7 +23,9 @@ STATUS_NAMES = {
     5: "range", 6: "unsupported", 7: "state", 8: "timeout",
 }
 
-CLOSURE_NULL, CLOSURE_DIFFUSE, CLOSURE_EMISSION, CLOSURE_TRANSPARENT, CLOSURE_ADD, CLOSURE_MIX = range(6)
+CLOSURE_NULL, CLOSURE_DIFFUSE, CLOSURE_EMISSION, CLOSURE_TRANSPARENT, CLOSURE_ADD, CLOSURE_MIX, CLOSURE_GLOSSY = range(7)
+GLOSSY_GGX, GLOSSY_BECKMANN = 0, 1
+MATERIAL_NO_BUMP_MAP_CORRECTION = 1
 LIGHT_POINT, LIGHT_SPOT, LIGHT_AREA, LIGHT_DISTANT = range(4)
 LIGHT_FLAG_SPHERE, LIGHT_FLAG_NORMALIZE, LIGHT_FLAG_ELLIPSE, LIGHT_FLAG_USE_MIS = 1, 2, 4, 8
 VIS_CAMERA, VIS_DIFFUSE, VIS_GLOSSY, VIS_TRANSMISSION, VIS_SHADOW, VIS_VOLUME = 1, 2, 4, 8, 16, 32
@@ -73,7 +75,8 @@ class MaterialDesc(ctypes.Structure):
                 ("root", ctypes.c_uint32), ("scalars", c_float_p), ("scalar_count", ctypes.c_uint32),
                 ("vector_count", ctypes.c_uint32), ("vectors", c_float_p),
                 ("emission_sampling", ctypes.c_uint32), ("value_count", ctypes.c_uint32),
-                ("values", ctypes.POINTER(ValueInstruction))]
+                ("values", ctypes.POINTER(ValueInstruction)), ("flags", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class LightDesc(ctypes.Structure):

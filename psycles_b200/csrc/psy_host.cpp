@@ -1067,16 +1067,19 @@ psy_status validate_material(const psy_material_desc &m) {
     };
     for (uint32_t k = 0; k < m.closure_count; ++k) {
         const psy_closure_instruction &c = m.closures[k];
-        if (c.op > PSY_CLOSURE_MIX) return fail(PSY_ERROR_UNSUPPORTED, "closure operation outside the supported set");
+        if (c.op > PSY_CLOSURE_GLOSSY) return fail(PSY_ERROR_UNSUPPORTED, "closure operation outside the supported set");
         if ((c.op == PSY_CLOSURE_ADD || c.op == PSY_CLOSURE_MIX) && (c.a >= m.closure_count || c.b >= m.closure_count))
             return fail(PSY_ERROR_INVALID_ARGUMENT, "closure child out of range");
-        if ((c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_TRANSPARENT) &&
+        if ((c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_TRANSPARENT ||
+             c.op == PSY_CLOSURE_GLOSSY) &&
             !input_ok(c.color, V, false))
             return fail(PSY_ERROR_INVALID_ARGUMENT, "closure colour input out of range");
         if ((c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_MIX) && !input_ok(c.scalar, S, false))
             return fail(PSY_ERROR_INVALID_ARGUMENT, "closure scalar input out of range");
-        if (c.op == PSY_CLOSURE_DIFFUSE && !input_ok(c.roughness, S, true))
+        if ((c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_GLOSSY) && !input_ok(c.roughness, S, true))
             return fail(PSY_ERROR_INVALID_ARGUMENT, "closure roughness input out of range");
+        if (c.op == PSY_CLOSURE_GLOSSY && c.a != PSY_GLOSSY_GGX && c.a != PSY_GLOSSY_BECKMANN)
+            return fail(PSY_ERROR_UNSUPPORTED, "glossy distribution outside GGX and Beckmann");
     }
     return PSY_OK;
 }
@@ -1805,6 +1808,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         g.scalar_offset = uint32_t(sc->scalars.size());
         g.vector_offset = uint32_t(sc->vectors.size() / 3u);
         g.emission_sampling = m.emission_sampling;
+        g.bump_correction = (m.flags & PSY_MATERIAL_NO_BUMP_MAP_CORRECTION) == 0u ? 1u : 0u;
         for (uint32_t k = 0; k < m.closure_count; ++k) {
             if (m.closures[k].op == PSY_CLOSURE_EMISSION) g.has_emission = 1u;
             if (m.closures[k].op == PSY_CLOSURE_TRANSPARENT) g.has_transparent = 1u;

@@ -105,6 +105,8 @@ __device__ __noinline__ float atan2_(float y, float x) {
 __device__ __noinline__ float pow_(float x, float y) {
     return static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y)));
 }
+__device__ __noinline__ float exp_(float x) { return static_cast<float>(exp(static_cast<double>(x))); }
+__device__ __noinline__ float log_(float x) { return static_cast<float>(log(static_cast<double>(x))); }
 
 constexpr float kPi = 3.1415926535897932f;
 constexpr float kInvPi = 0.31830988618379067154f;

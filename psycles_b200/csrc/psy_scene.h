@@ -109,7 +109,9 @@ struct alignas(16) MeshGpu {
 struct alignas(16) MaterialGpu {
     uint32_t code_offset, code_count, root, scalar_offset;
     uint32_t vector_offset, emission_sampling, has_emission, has_transparent;
-    uint32_t value_offset, value_count, pad0, pad1;
+    uint32_t value_offset, value_count;
+    uint32_t bump_correction;  // contract::Material::use_bump_map_correction
+    uint32_t pad0;
 };
 
 // Value instructions a material's program may hold (its stream is

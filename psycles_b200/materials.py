@@ -483,6 +483,7 @@ class CompiledMaterial:
     program: SurfaceProgram
     parameters: SurfaceParameterBlock
     emission_sampling: int = _abi.EMISSION_AUTOMATIC
+    use_bump_map_correction: bool = True
 
 
 class MaterialLibrary:
@@ -503,7 +504,8 @@ class MaterialLibrary:
                     kinds[name] = MaterialUpdateKind.UNCHANGED
                 else:
                     block = bind_surface_parameters(old.program, graph)  # raises before commit
-                    staged[name] = CompiledMaterial(graph, old.program, block, old.emission_sampling)
+                    staged[name] = CompiledMaterial(graph, old.program, block, old.emission_sampling,
+                                                    old.use_bump_map_correction)
                     kinds[name] = MaterialUpdateKind.PARAMETERS_REBOUND
             else:
                 program, block = compile_surface_program(graph)  # raises before commit

@@ -164,17 +164,19 @@ def _material_descs(mats) -> tuple:
         rec["emission_sampling"] = [cm.emission_sampling for cm in mats]
         rec["value_count"] = w_counts
         rec["values"] = np.uint64(val_all.ctypes.data) + start(w_counts) * np.uint64(32)
+        rec["flags"] = [0 if getattr(cm, "use_bump_map_correction", True) else _abi.MATERIAL_NO_BUMP_MAP_CORRECTION
+                        for cm in mats]
     descs = (_abi.MaterialDesc * n).from_buffer(rec)
     return descs, [rec, code_all, val_all, scal_all, vec_all]
 
 
-# psy_material_desc of include/psycles_cuda.h on LP64 hosts (56 bytes)
+# psy_material_desc of include/psycles_cuda.h on LP64 hosts (64 bytes)
 _MATERIAL_DESC_DTYPE = np.dtype({
     "names": ["closures", "closure_count", "root", "scalars", "scalar_count", "vector_count", "vectors",
-              "emission_sampling", "value_count", "values"],
+              "emission_sampling", "value_count", "values", "flags", "reserved"],
     "formats": [np.uint64, np.uint32, np.uint32, np.uint64, np.uint32, np.uint32, np.uint64, np.uint32, np.uint32,
-                np.uint64],
-    "offsets": [0, 8, 12, 16, 24, 28, 32, 40, 44, 48], "itemsize": 56})
+                np.uint64, np.uint32, np.uint32],
+    "offsets": [0, 8, 12, 16, 24, 28, 32, 40, 44, 48, 56, 60], "itemsize": 64})
 
 
 class SceneDescHandle:

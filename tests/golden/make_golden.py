@@ -85,7 +85,42 @@ def sample_mapping_fixtures(ref: pathlib.Path) -> dict:
     for c in cases:
         if len(c) >= 9:
             out.append({"normal": c[0:3], "random": c[3:5], "direction": c[5:8], "pdf": c[8]})
-    return {"cosine_hemisphere": out, "tolerance": 2.5e-6}
+    return {"cosine_hemisphere": out, "tolerance": 2.5e-6, "visible_normal": visible_normal_fixtures(text)}
+
+
+def _floats(text: str) -> list[float]:
+    return [float(x) for x in re.findall(r"-?\d+\.\d+(?:e-?\d+)?", text)]
+
+
+def visible_normal_fixtures(text: str) -> dict:
+    """The GGX and Beckmann visible-normal cases of
+    test_luisa_cycles_sample_mapping.cpp: the GGX reflection recorded from
+    Cycles (normal, incoming, alpha, random -> reflected direction) and the
+    two Beckmann cases (oblique and normal incidence, alpha 0.64, random
+    (0.37, 0.73) -> reflected direction)."""
+    ggx_call = text[text.index("sample_ggx_visible_normal_reflection("):]
+    ggx_call = ggx_call[: ggx_call.index("ggx.write")]
+    g = _floats(ggx_call)
+    ggx_expected = text[text.index("expected_ggx_direction"):]
+    ggx_expected = _floats(ggx_expected[: ggx_expected.index("};")])
+    beck = text[text.index("const auto normal = make_float3(0.0f, 0.0f, 1.0f);"):]
+    beck = beck[: beck.index("beckmann.write(1u")]
+    oblique = _floats(beck[beck.index("oblique_incoming ="): beck.index("const auto sample_random")])
+    random = _floats(beck[beck.index("sample_random ="): beck.index("const auto oblique_half")])
+    alpha = _floats(beck[beck.index("normal, oblique_incoming,"): beck.index("sample_random);")])
+    expected = text[text.index("expected_beckmann_directions{"):]
+    expected = _floats(expected[: expected.index("}};")])
+    return {
+        "ggx": {"normal": g[0:3], "incoming": g[3:6], "alpha": g[6], "random": g[7:9],
+                "direction": ggx_expected[0:3], "tolerance": 2.5e-6},
+        "beckmann": [
+            {"normal": [0.0, 0.0, 1.0], "incoming_unnormalised": oblique, "alpha": alpha[0], "random": random,
+             "direction": expected[0:3]},
+            {"normal": [0.0, 0.0, 1.0], "incoming_unnormalised": [0.0, 0.0, 1.0], "alpha": alpha[0],
+             "random": random, "direction": expected[3:6]},
+        ],
+        "beckmann_tolerance": 1.0e-5,
+    }
 
 
 def path_state_fixtures(ref: pathlib.Path) -> dict:

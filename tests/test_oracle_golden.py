@@ -1,7 +1,8 @@
 """The CPU oracle pinned to the reference's golden vectors: the tabulated
 Sobol LUT fingerprint and rows (tests/test_tabulated_sobol.cpp), the device
 Sobol probe bits and shuffled indices (tests/test_luisa_sobol_fallback.cpp),
-the cosine-hemisphere cases (tests/test_luisa_cycles_sample_mapping.cpp),
+the cosine-hemisphere and GGX / Beckmann visible-normal cases
+(tests/test_luisa_cycles_sample_mapping.cpp),
 the path-state transitions (tests/test_luisa_cycles_path_state.cpp), and the
 tables the reference's own sampling code produces (oracle/_ref)."""
 
@@ -164,3 +165,32 @@ def test_light_tree_against_reference_library_when_built(oracle_lib):
             a = oracle.build_light_tree(oracle_lib, "oracle_build_light_tree", rec, max_leaf)
             b = oracle.build_light_tree(ref, "ref_build_light_tree", rec, max_leaf)
             assert oracle.light_tree_fingerprint(a) == oracle.light_tree_fingerprint(b), (seed, count, max_leaf)
+
+
+def _reflect(half, incoming):
+    d = np.float32(2.0) * np.float32(np.dot(incoming, half)) * half - incoming
+    return d.astype(np.float32)
+
+
+def test_visible_normal_cases(oracle_lib, golden):
+    """The glossy closures' visible-normal samplers against the GGX sample
+    Cycles recorded and the two Beckmann cases of
+    tests/test_luisa_cycles_sample_mapping.cpp (reflected directions)."""
+    vn = golden["sample_mapping"]["visible_normal"]
+    g = vn["ggx"]
+    n, i = np.array(g["normal"], np.float32), np.array(g["incoming"], np.float32)
+    r = np.array(g["random"], np.float32)
+    h = np.zeros(3, np.float32)
+    oracle_lib.oracle_sample_visible_normal(0, _p(n), _p(i), ctypes.c_float(g["alpha"]), _p(r), _p(h))
+    d, exp = _reflect(h, i), np.array(g["direction"], np.float32)
+    tol = g["tolerance"]
+    assert np.all(np.abs(d - exp) <= tol * np.maximum(1.0, np.maximum(np.abs(d), np.abs(exp)))), (d, exp)
+    for c in vn["beckmann"]:
+        n = np.array(c["normal"], np.float32)
+        i = np.array(c["incoming_unnormalised"], np.float32)
+        i = (i / np.float32(np.sqrt(np.float32(np.dot(i, i))))).astype(np.float32)
+        r = np.array(c["random"], np.float32)
+        oracle_lib.oracle_sample_visible_normal(1, _p(n), _p(i), ctypes.c_float(c["alpha"]), _p(r), _p(h))
+        d, exp = _reflect(h, i), np.array(c["direction"], np.float32)
+        tol = vn["beckmann_tolerance"]
+        assert np.all(np.abs(d - exp) <= tol * np.maximum(1.0, np.maximum(np.abs(d), np.abs(exp)))), (d, exp)
