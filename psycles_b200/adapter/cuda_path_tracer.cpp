@@ -94,6 +94,7 @@ std::uint32_t closure_op(ClosureOperation op) {
     case ClosureOperation::transparent: return PSY_CLOSURE_TRANSPARENT;
     case ClosureOperation::add: return PSY_CLOSURE_ADD;
     case ClosureOperation::mix: return PSY_CLOSURE_MIX;
+    case ClosureOperation::glossy: return PSY_CLOSURE_GLOSSY;
     default: return 0xffffffffu;
     }
 }
@@ -183,6 +184,18 @@ struct Flattener {
                 return v.parameter.value;
             return PSY_INPUT_VALUE | id.value;
         };
+        // the closure normal must be the shading normal: an unlinked Normal
+        // socket holding the zero vector, which safe_normalize replaces by
+        // the shading normal
+        auto shading_normal = [&](const compiler::ClosureInstruction &c) {
+            if (c.normal_uses_bump || !c.normal.valid() || c.normal.value >= values.size()) return false;
+            const auto &n = values[c.normal.value];
+            if (n.operation != ValueOperation::parameter || !n.parameter.valid() ||
+                n.parameter.value >= parameters.size())
+                return false;
+            const float *v = &f.vectors[3u * n.parameter.value];
+            return v[0] == 0.0f && v[1] == 0.0f && v[2] == 0.0f;
+        };
         for (const auto &c : program.closure_instructions()) {
             const std::uint32_t op = closure_op(c.operation);
             if (op == 0xffffffffu)
@@ -190,25 +203,23 @@ struct Flattener {
                              " is not available in the CUDA path");
             psy_closure_instruction k{op, 0u, 0u, PSY_INPUT_NONE, PSY_INPUT_NONE, PSY_INPUT_NONE};
             switch (c.operation) {
-            case ClosureOperation::diffuse: {
+            case ClosureOperation::diffuse:
                 k.color = input(c.color, c, false);
                 k.roughness = input(c.roughness, c, true);
-                // the closure normal must be the shading normal: an unlinked
-                // Normal socket holding the zero vector, which safe_normalize
-                // replaces by the shading normal
-                bool shading_normal = false;
-                if (c.normal.valid() && c.normal.value < values.size()) {
-                    const auto &n = values[c.normal.value];
-                    if (n.operation == ValueOperation::parameter && n.parameter.valid() &&
-                        n.parameter.value < parameters.size()) {
-                        const float *v = &f.vectors[3u * n.parameter.value];
-                        shading_normal = v[0] == 0.0f && v[1] == 0.0f && v[2] == 0.0f;
-                    }
-                }
-                if (!shading_normal || c.normal_uses_bump)
+                if (!shading_normal(c))
                     return error(who + "closure normals other than the shading normal are not available in the CUDA path");
                 break;
-            }
+            case ClosureOperation::glossy:
+                // Distribution GGX (default) or BECKMANN; MULTI_GGX's
+                // tabulated energy preservation is not in the CUDA path
+                if (c.preserve_ggx_energy)
+                    return error(who + "the Multiscatter GGX distribution is not available in the CUDA path");
+                k.a = c.beckmann ? PSY_GLOSSY_BECKMANN : PSY_GLOSSY_GGX;
+                k.color = input(c.color, c, false);
+                k.roughness = input(c.roughness, c, false);
+                if (!shading_normal(c))
+                    return error(who + "closure normals other than the shading normal are not available in the CUDA path");
+                break;
             case ClosureOperation::emission:
                 k.color = input(c.color, c, false);
                 k.scalar = input(c.strength, c, false);
@@ -233,6 +244,7 @@ struct Flattener {
         }
         f.root = program.root().value;
         f.emission_sampling = static_cast<std::uint32_t>(desc.emission_sampling);
+        f.flags = desc.use_bump_map_correction ? 0u : PSY_MATERIAL_NO_BUMP_MAP_CORRECTION;
         out._materials.push_back(std::move(f));
         return true;
     }
@@ -462,6 +474,7 @@ struct Flattener {
             d.vectors = m.vectors.data();
             d.vector_count = std::uint32_t(m.vectors.size() / 3u);
             d.emission_sampling = m.emission_sampling;
+            d.flags = m.flags;
             d.values = m.values.data();
             d.value_count = std::uint32_t(m.values.size());
             out._material_descs.push_back(d);
@@ -530,11 +543,13 @@ namespace {
 // CompiledScene over a psy_scene (the device owns the uploaded scene).
 class CudaCompiledScene final : public contract::CompiledScene {
 public:
-    CudaCompiledScene(psy_scene *scene, std::uint32_t light_count) : scene(scene), light_count(light_count) {}
+    CudaCompiledScene(psy_scene *scene, std::uint32_t light_count, bool glossy)
+        : scene(scene), light_count(light_count), glossy(glossy) {}
     ~CudaCompiledScene() noexcept override { psy_scene_destroy(scene); }
     [[nodiscard]] std::uint64_t source_revision() const noexcept override { return psy_scene_source_revision(scene); }
     psy_scene *scene;
     std::uint32_t light_count;
+    bool glossy;  // a material holds a glossy closure
 };
 
 bool supported_pass(contract::PassKind kind) {
@@ -643,7 +658,12 @@ contract::SceneCompilation CudaPathTracerBackend::compile_scene(const contract::
         result.diagnostics.push_back({psy_last_error()});
         return result;
     }
-    result.scene = std::make_unique<CudaCompiledScene>(scene, flat.desc().light_count);
+    bool glossy = false;
+    for (std::uint32_t i = 0; i < flat.desc().material_count; ++i) {
+        const psy_material_desc &m = flat.desc().materials[i];
+        for (std::uint32_t k = 0; k < m.closure_count; ++k) glossy = glossy || m.closures[k].op == PSY_CLOSURE_GLOSSY;
+    }
+    result.scene = std::make_unique<CudaCompiledScene>(scene, flat.desc().light_count, glossy);
     return result;
 }
 
@@ -660,6 +680,12 @@ std::unique_ptr<contract::RenderSession> CudaPathTracerBackend::create_session(
         return nullptr;
     for (const auto &pass : settings.passes)
         if (!supported_pass(pass.kind)) return nullptr;
+    // glossy closures render with Filter Glossy off and both caustics on
+    // (the contract's defaults): the glossy blur and the caustics lobe masks
+    // are not in the CUDA path
+    if (compiled.glossy && (settings.integrator.filter_glossy > 0.0f || !settings.integrator.reflective_caustics ||
+                            !settings.integrator.refractive_caustics))
+        return nullptr;
     const psy_render_settings s = to_psy_settings(settings, _options.next_event_estimation);
     psy_session *session = nullptr;
     if (psy_session_create(compiled.scene, &s, &session) != PSY_OK) return nullptr;

@@ -62,6 +62,7 @@ private:
         std::vector<float> scalars, vectors;
         std::uint32_t root = 0;
         std::uint32_t emission_sampling = PSY_EMISSION_SAMPLING_AUTOMATIC;
+        std::uint32_t flags = 0u;  // PSY_MATERIAL_*
     };
     std::vector<Mesh> _meshes;
     std::vector<Material> _materials;

@@ -178,6 +178,124 @@ __device__ __forceinline__ ConeSample sample_uniform_cone(f3 axis, float one_min
     return {axis, 1.0f, 1.0f};
 }
 
+// sample_ggx_visible_normal (cycles_sample_mapping.h:131-183): Heitz 2018,
+// "Sampling the GGX Distribution of Visible Normals", in the frame of
+// make_orthonormals(normal) with the concentric disk map; the half vector
+// is not renormalised in world space.
+__device__ __noinline__ f3 sample_ggx_visible_normal(f3 normal, f3 incoming, float alpha, f2 random) {
+    const Basis w = make_orthonormals(normal);
+    const f3 li = mk3(dot(w.tangent, incoming), dot(w.bitangent, incoming), dot(normal, incoming));
+    const f3 si = normalize(mk3(alpha * li.x, alpha * li.y, li.z));
+    const float pl2 = si.x * si.x + si.y * si.y;
+    const f3 pt = mk3(-si.y, si.x, 0.0f) / sqrtf(maxf_(pl2, 1.0e-20f));
+    const f3 bx = pl2 > 1.0e-7f ? pt : mk3(1.0f, 0.0f, 0.0f);
+    const f3 by = cross(si, bx);
+    f2 disk = sample_uniform_disk(random);
+    const float projected_area = 0.5f * (1.0f + si.z);
+    disk.y = lerpf_(sqrtf(maxf_(1.0f - disk.x * disk.x, 0.0f)), disk.y, projected_area);
+    const float hz = sqrtf(maxf_(1.0f - disk.x * disk.x - disk.y * disk.y, 0.0f));
+    const f3 sh = bx * disk.x + by * disk.y + si * hz;
+    const f3 lh = normalize(mk3(alpha * sh.x, alpha * sh.y, maxf_(sh.z, 0.0f)));
+    return w.tangent * lh.x + w.bitangent * lh.y + normal * lh.z;
+}
+
+// erf of Abramowitz & Stegun 7.1.28 (1 - 1 / (1 + a1 x + ... + a6 x^6)^16,
+// |error| <= 3e-7) as Cycles evaluates it (cycles_sample_mapping.h:188-208):
+// Horner steps as fused multiply-adds, +-1 beyond |x| = 12.3.
+__device__ __forceinline__ float fast_erf(float value) {
+    const float magnitude = fabsf(value);
+    const float crushed = 1.0f - (1.0f - magnitude);
+    float p = fmaf(0.0000430638f, crushed, 0.0002765672f);
+    p = fmaf(p, crushed, 0.0001520143f);
+    p = fmaf(p, crushed, 0.0092705272f);
+    p = fmaf(p, crushed, 0.0422820123f);
+    p = fmaf(p, crushed, 0.0705230784f);
+    p = fmaf(p, crushed, 1.0f);
+    const float square = p * p;
+    const float fourth = square * square;
+    const float eighth = fourth * fourth;
+    const float sixteenth = eighth * eighth;
+    const float unsigned_result = 1.0f - 1.0f / sixteenth;
+    if (magnitude >= 12.3f) return value >= 0.0f ? 1.0f : -1.0f;
+    return value >= 0.0f ? unsigned_result : -unsigned_result;
+}
+
+// erfinv of Giles, "Approximating the erfinv function" (GPU Computing Gems,
+// 2011), single-precision branch pair on w = -log((1 - x)(1 + x)), as
+// Cycles evaluates it (cycles_sample_mapping.h:210-237).
+__device__ __forceinline__ float fast_inverse_erf(float value) {
+    const float magnitude = minf_(fabsf(value), 0.99999994f);
+    const float base = -log_((1.0f - magnitude) * (1.0f + magnitude));
+    const float cx = base - 2.5f;
+    float central = fmaf(2.81022636e-08f, cx, 3.43273939e-07f);
+    central = fmaf(central, cx, -3.5233877e-06f);
+    central = fmaf(central, cx, -4.39150654e-06f);
+    central = fmaf(central, cx, 0.00021858087f);
+    central = fmaf(central, cx, -0.00125372503f);
+    central = fmaf(central, cx, -0.00417768164f);
+    central = fmaf(central, cx, 0.246640727f);
+    central = fmaf(central, cx, 1.50140941f);
+    const float tx = sqrtf(base) - 3.0f;
+    float tail = fmaf(-0.000200214257f, tx, 0.000100950558f);
+    tail = fmaf(tail, tx, 0.00134934322f);
+    tail = fmaf(tail, tx, -0.00367342844f);
+    tail = fmaf(tail, tx, 0.00573950773f);
+    tail = fmaf(tail, tx, -0.0076224613f);
+    tail = fmaf(tail, tx, 0.00943887047f);
+    tail = fmaf(tail, tx, 1.00167406f);
+    tail = fmaf(tail, tx, 2.83297682f);
+    return (base < 5.0f ? central : tail) * value;
+}
+
+// sample_beckmann_visible_normal (cycles_sample_mapping.h:239-310): the
+// visible-slope sampler of Heitz and d'Eon (2014) with Cycles' root solve
+// -- a quadratic first guess, at most three Newton steps kept inside the
+// bracket (bisection otherwise) -- in the frame of make_orthonormals(normal).
+__device__ __noinline__ f3 sample_beckmann_visible_normal(f3 normal, f3 incoming, float alpha, f2 random) {
+    const Basis w = make_orthonormals(normal);
+    const f3 li = mk3(dot(w.tangent, incoming), dot(w.bitangent, incoming), dot(normal, incoming));
+    const f3 si = normalize(mk3(alpha * li.x, alpha * li.y, li.z));
+    const float normal_radius = sqrtf(-log_(random.x));
+    const float normal_phi = 2.0f * kPi * random.y;
+    const f2 normal_slope = mk2(normal_radius * cos_(normal_phi), normal_radius * sin_(normal_phi));
+    const float cosine = si.z;
+    const float sine = sqrtf(maxf_(1.0f - cosine * cosine, 0.0f));
+    const float safe_cosine = cosine != 0.0f ? cosine : 1.0f;
+    const float safe_sine = sine != 0.0f ? sine : 1.0f;
+    const float tangent = sine / safe_cosine;
+    const float safe_tangent = tangent != 0.0f ? tangent : 1.0f;
+    const float cotangent = 1.0f / safe_tangent;
+    const float erf_a = fast_erf(cotangent);
+    const float exponential = exp_(-cotangent * cotangent);
+    const float cosine_phi = sine != 0.0f ? si.x / safe_sine : 1.0f;
+    const float sine_phi = sine != 0.0f ? si.y / safe_sine : 0.0f;
+    const float k = tangent * 0.56418958354f;
+    const float approximate_y = random.x * (1.0f + erf_a + k * (1.0f - erf_a * erf_a));
+    const float exact_y = random.x * (1.0f + erf_a + k * exponential);
+    const float safe_k = k > 0.0f ? k : 1.0f;
+    const float quadratic_b = (0.5f - sqrtf(maxf_(k * (k - approximate_y + 1.0f) + 0.25f, 0.0f))) / safe_k;
+    const float b = k > 0.0f ? quadratic_b : approximate_y - 1.0f;
+    float inverse_erf = fast_inverse_erf(b);
+    f2 begin = mk2(-1.0f, -exact_y);
+    f2 end = mk2(erf_a, 1.0f + erf_a + k * exponential - exact_y);
+    f2 current = mk2(b, 1.0f + b + k * exp_(-inverse_erf * inverse_erf) - exact_y);
+    for (uint32_t iteration = 0; fabsf(current.y) > 1.0e-6f && iteration < 3u; ++iteration) {
+        const bool same_sign = (begin.y < 0.0f) == (current.y < 0.0f);
+        if (same_sign) begin = current;
+        else end.x = current.x;
+        const float newton = current.x - current.y / (1.0f - inverse_erf * tangent);
+        const bool inside = newton >= begin.x && newton <= end.x;
+        current.x = inside ? newton : 0.5f * (begin.x + end.x);
+        inverse_erf = fast_inverse_erf(current.x);
+        current.y = 1.0f + current.x + k * exp_(-inverse_erf * inverse_erf) - exact_y;
+    }
+    const f2 general_slope = mk2(inverse_erf, fast_inverse_erf(2.0f * random.y - 1.0f));
+    const f2 slope = si.z >= 0.99999f ? normal_slope : general_slope;
+    const f2 rotated = mk2(cosine_phi * slope.x - sine_phi * slope.y, sine_phi * slope.x + cosine_phi * slope.y) * alpha;
+    const f3 lh = normalize(mk3(-rotated.x, -rotated.y, 1.0f));
+    return w.tangent * lh.x + w.bitangent * lh.y + normal * lh.z;
+}
+
 // ------------------------------------------------------ closure programs
 // GraphSurfaceImplementation::for_each_closure (src/luisa/graph_surface_closures.cpp:5-356)
 // with allocation (src/luisa/graph_surface_state.cpp:19-48).
@@ -189,13 +307,27 @@ constexpr uint32_t kMaxClosureStack = 32u;
 // roughness for the Oren-Nayar evaluation (roughness below 1e-5: Lambert).
 // The in-scope closures have no Normal input, so every diffuse closure
 // shares the normalised shading normal (SurfaceClosures::normal) and a
-// transparent closure never reads one.
+// transparent closure never reads one.  A glossy closure's `color` holds
+// its normal after setup's specular-reflection correction (its colour is
+// in its weight), `roughness` its roughness (microfacet alpha = roughness^2),
+// and its op carries kGlossyBeckmann for the Beckmann distribution.
 struct PhysicalClosure {
     f3 weight;
     float sample_weight;
     uint32_t op;
     f3 color;
     float roughness;
+};
+
+constexpr uint32_t kGlossyBeckmann = 0x100u;
+__device__ __forceinline__ bool is_glossy(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_GLOSSY; }
+
+// The surface point's inputs to closure setup, evaluation and sampling.
+struct ClosurePoint {
+    f3 shading_normal;    // SurfacePoint::shading_normal
+    f3 geometric_normal;  // SurfacePoint::geometric_normal (facing the incoming ray)
+    f3 incoming;          // SurfacePoint::incoming (-ray direction)
+    bool bump_correction; // SurfacePoint::use_bump_map_correction
 };
 
 struct SurfaceClosures {
@@ -335,12 +467,13 @@ __device__ __forceinline__ float input_scalar(const SceneView &s, const Material
 }
 
 // Leaf kinds a closure walk reports (kLeaves of walk_closures).
-constexpr uint32_t kLeafDiffuse = 1u, kLeafTransparent = 2u, kLeafEmission = 4u, kLeafAll = 7u;
+constexpr uint32_t kLeafDiffuse = 1u, kLeafTransparent = 2u, kLeafEmission = 4u, kLeafGlossy = 8u, kLeafAll = 15u;
 
 // Visits closure leaves depth-first, `a` before `b`, with the add / mix
 // weight rule; `visit(op, weight, color, roughness)` receives the diffuse /
-// transparent / emission leaves selected by kLeaves with their authored
-// colour (x strength for emission) and, for diffuse, the roughness input.
+// glossy / transparent / emission leaves selected by kLeaves with their
+// authored colour (x strength for emission) and, for diffuse and glossy,
+// the roughness input (a Beckmann glossy leaf's op carries kGlossyBeckmann).
 // Unselected leaves read no inputs (a shadow ray's extinction needs only
 // the transparent ones).
 template <uint32_t kLeaves = kLeafAll, typename Visit>
@@ -376,6 +509,13 @@ __device__ __forceinline__ void walk_closures(const SceneView &s, const Material
                 const f3 color = input_vector(s, m, c.color);
                 visit(c.op, color * w, color, 0.0f);
             }
+        } else if (c.op == PSY_CLOSURE_GLOSSY) {
+            if constexpr ((kLeaves & kLeafGlossy) != 0u) {
+                const f3 color = input_vector(s, m, c.color);
+                const uint32_t op = c.a == PSY_GLOSSY_BECKMANN ? (uint32_t(PSY_CLOSURE_GLOSSY) | kGlossyBeckmann)
+                                                               : uint32_t(PSY_CLOSURE_GLOSSY);
+                visit(op, color * w, color, input_scalar(s, m, c.roughness));
+            }
         } else if (c.op == PSY_CLOSURE_EMISSION && (kLeaves & kLeafEmission) != 0u) {
             const f3 color = input_vector(s, m, c.color) * input_scalar(s, m, c.scalar);
             visit(c.op, color * w, color, 0.0f);
@@ -383,17 +523,54 @@ __device__ __forceinline__ void walk_closures(const SceneView &s, const Material
     }
 }
 
-__device__ __forceinline__ void collect_surface(const SceneView &s, const MaterialGpu &m, f3 shading_normal,
+// ensure_valid_specular_reflection (src/luisa/graph_surface_scattering.cpp:119-155):
+// a shading normal whose mirror direction of `incoming` would dip below the
+// geometric surface is tilted toward the geometric normal until the
+// reflection clears it by min(0.9 cos_i, 0.01).
+__device__ __noinline__ f3 ensure_valid_specular_reflection(f3 ng, f3 incoming, f3 n) {
+    const f3 reflected = n * (2.0f * dot(n, incoming)) - incoming;
+    const float ig = maxf_(dot(incoming, ng), 0.0f);
+    const float threshold = minf_(0.9f * ig, 0.01f);
+    const bool valid = dot(ng, reflected) >= threshold;
+    const f3 tangent = safe_normalize(n - ng * dot(n, ng), n);
+    const float it = dot(incoming, tangent);
+    const float a = it * it + ig * ig;
+    const float b = 2.0f * (a + ig * threshold);
+    const float c = (threshold + ig) * (threshold + ig);
+    const float disc = maxf_(b * b - 4.0f * a * c, 0.0f);
+    const float signed_root = it < 0.0f ? b + sqrtf(disc) : b - sqrtf(disc);
+    const float nz2 = clampf_(0.25f * signed_root / maxf_(a, 1.0e-20f), 0.0f, 1.0f);
+    const f3 corrected = safe_normalize(tangent * sqrtf(maxf_(1.0f - nz2, 0.0f)) + ng * sqrtf(nz2), ng);
+    return (!valid && a > 1.0e-20f) ? corrected : n;
+}
+
+// maybe_ensure_valid_specular_reflection (graph_surface_scattering.cpp:157-168).
+__device__ __forceinline__ f3 specular_normal(bool correction, f3 ng, f3 incoming, f3 n) {
+    const bool equal = ng.x == n.x && ng.y == n.y && ng.z == n.z;
+    return correction && !equal ? ensure_valid_specular_reflection(ng, incoming, n) : n;
+}
+
+// Closure allocation (graph_surface_state.cpp:26-48,
+// graph_surface_physical_closures.cpp:158-520): diffuse goes through
+// bsdf_alloc (negative weight clamped, average cutoff 1e-5); glossy is
+// allocated the same way (reflective caustics on), its normal corrected for
+// a valid specular reflection and its weight kept (GGX / Beckmann without
+// energy preservation: darkening and evaluation scale one); transparent
+// keeps its signed weight, uses the cutoff on |average|, and every
+// allocated transparent contribution merges into the first one
+// (bsdf_transparent_setup, :483-518: summed weights and sample weights).
+__device__ __forceinline__ void collect_surface(const SceneView &s, const MaterialGpu &m, const ClosurePoint &pt,
                                                 SurfaceClosures &out) {
     out.count = 0u;
     out.emission = mk3(0.0f);
-    out.normal = safe_normalize(shading_normal, shading_normal);
+    out.normal = safe_normalize(pt.shading_normal, pt.shading_normal);
+    const f3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
+    int transparent_slot = -1;
     walk_closures(s, m, [&](uint32_t op, f3 w, f3 color, float roughness) {
         if (op == PSY_CLOSURE_EMISSION) {
             out.emission = out.emission + w;
             return;
         }
-        if (out.count >= kMaxClosures) return;
         PhysicalClosure p;
         p.op = op;
         p.color = color;
@@ -402,12 +579,26 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
             p.weight = bsdf_allocated_weight(w);
             p.sample_weight = closure_sample_weight(p.weight);
             if (!any_nonzero(p.weight)) return;
+        } else if (is_glossy(op)) {
+            const f3 allocated = max3(w, mk3(0.0f));
+            const float allocation = closure_sample_weight(allocated);
+            if (!(allocation >= 1.0e-5f)) return;
+            p.weight = allocated;
+            p.sample_weight = allocation * closure_sample_weight(mk3(1.0f));
+            p.color = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, out.normal);
         } else {
             const float sw = closure_sample_weight(w);
             if (!(sw >= 1.0e-5f)) return;
+            if (transparent_slot >= 0) {
+                out.c[transparent_slot].weight = out.c[transparent_slot].weight + w;
+                out.c[transparent_slot].sample_weight += sw;
+                return;
+            }
             p.weight = w;
             p.sample_weight = sw;
         }
+        if (out.count >= kMaxClosures) return;
+        if (op == PSY_CLOSURE_TRANSPARENT) transparent_slot = int(out.count);
         out.c[out.count++] = p;
     });
 }
@@ -447,17 +638,103 @@ __device__ __forceinline__ uint32_t label_from_events(uint32_t e) {
     return l;
 }
 
+constexpr float kMicrofacetSingularAlphaProduct = 2.0e-10f;
+
+// microfacet_alpha / microfacet_is_singular (graph_surface_scattering.cpp:549-568)
+// without the glossy filter (its roughness is zero: Filter Glossy off).
+__device__ __forceinline__ float microfacet_alpha(float roughness) {
+    const float a = clampf_(roughness, 0.0f, 1.0f);
+    return a * a;
+}
+__device__ __forceinline__ bool microfacet_singular(float roughness) {
+    const float a = microfacet_alpha(roughness);
+    return a * a <= kMicrofacetSingularAlphaProduct;
+}
+
+// cycles_runtime_flags (src/luisa/graph_surface_scattering.cpp:292-365).
 __device__ __forceinline__ uint32_t runtime_flags(const SurfaceClosures &s, bool back_facing) {
     uint32_t f = back_facing ? kRuntimeBackfacing : 0u;
-    for (uint32_t i = 0; i < s.count; ++i)
-        f |= s.c[i].op == PSY_CLOSURE_DIFFUSE ? (kRuntimeBsdf | kRuntimeBsdfHasEval) : (kRuntimeBsdf | kRuntimeTransparent);
+    for (uint32_t i = 0; i < s.count; ++i) {
+        const PhysicalClosure &c = s.c[i];
+        if (c.op == PSY_CLOSURE_DIFFUSE) f |= kRuntimeBsdf | kRuntimeBsdfHasEval;
+        else if (is_glossy(c.op)) f |= kRuntimeBsdf | (microfacet_singular(c.roughness) ? 0u : kRuntimeBsdfHasEval);
+        else f |= kRuntimeBsdf | kRuntimeTransparent;
+    }
     return f;
 }
 
-// bump_shadowing_term (src/luisa/graph_surface_scattering.cpp:219-281).
-__device__ __forceinline__ float bump_shadowing(f3 smooth, f3 cn, f3 dir) {
+// bump_shadowing_term (src/luisa/graph_surface_scattering.cpp:219-281) of a
+// diffuse or glossy closure whose normal is `cn`: one when it is the
+// smooth shading normal; otherwise a direction on the wrong side of the
+// smooth surface is rejected during evaluation (and, for diffuse closures,
+// also when sampling), and a diffuse closure under bump correction gets the
+// smoothed shadowing factor.  The in-scope diffuse closures have the
+// shading normal, so only glossy closures reach the general case.
+__device__ __forceinline__ float bump_shadowing(f3 smooth, f3 cn, f3 dir, bool is_evaluation, bool diffuse,
+                                                bool bump_correction) {
     if (cn.x == smooth.x && cn.y == smooth.y && cn.z == smooth.z) return 1.0f;
-    return (dot(smooth, dir) * dot(smooth, cn) * dot(cn, dir) < 0.0f) ? 0.0f : 1.0f;
+    const float csd = dot(smooth, dir);
+    const float csc = dot(smooth, cn);
+    const float ccd = dot(cn, dir);
+    const bool reject = csd * csc * ccd < 0.0f && (is_evaluation || diffuse);
+    const float cos_i = fabsf(csd);
+    const float cos_d = fabsf(csc);
+    const float tan_d2 = maxf_(1.0f / maxf_(cos_d * cos_d, 1.0e-20f) - 1.0f, 0.0f);
+    const float bump_alpha2 = clampf_(0.125f * tan_d2, 0.0f, 1.0f);
+    const float tan_i2 = maxf_(1.0f / maxf_(cos_i * cos_i, 1.0e-20f) - 1.0f, 0.0f);
+    const float lambda = 0.5f * (sqrtf(1.0f + bump_alpha2 * tan_i2) - 1.0f);
+    const float smoothed = 1.0f / (1.0f + lambda);
+    const bool domain = diffuse && bump_correction && cos_d < 1.0f && cos_i < 1.0f;
+    const bool grazing = domain && cos_i < 1.0e-6f;
+    float result = domain && !grazing ? smoothed : 1.0f;
+    if (reject || grazing) result = 0.0f;
+    return result;
+}
+
+// microfacet_distribution / microfacet_lambda (graph_surface_scattering.cpp:508-547).
+__device__ __forceinline__ float microfacet_distribution(bool beckmann, float n_dot_h, float alpha) {
+    const float alpha2 = alpha * alpha;
+    const float cosine2 = minf_(n_dot_h * n_dot_h, 1.0f);
+    const float one_minus = 1.0f - cosine2;
+    if (!beckmann) {
+        const float den = one_minus + alpha2 * cosine2;
+        return alpha2 / maxf_(kPi * den * den, 1.0e-20f);
+    }
+    const float exponent = one_minus / (cosine2 * alpha2);
+    return 1.0f / (exp_(exponent) * kPi * alpha2 * cosine2 * cosine2);
+}
+__device__ __forceinline__ float microfacet_lambda(bool beckmann, float n_dot_v, float alpha) {
+    const float cosine2 = n_dot_v * n_dot_v;
+    const float sat = alpha * alpha * maxf_(1.0f / cosine2 - 1.0f, 0.0f);
+    if (!beckmann) return 0.5f * (sqrtf(1.0f + sat) - 1.0f);
+    const float a = 1.0f / sqrtf(sat);
+    const float approximation = ((0.396f * a - 1.259f) * a + 1.0f) / ((2.181f * a + 3.535f) * a);
+    return sat < 0.39f ? 0.0f : approximation;
+}
+
+// microfacet_intensity and microfacet_pdf (graph_surface_scattering.cpp:665-728)
+// of a standalone glossy closure (Fresnel constant one: its colour is in
+// the closure weight), in the corrected normal `gn`.
+struct Microfacet {
+    float intensity, pdf;
+};
+__device__ __noinline__ Microfacet microfacet_eval(uint32_t op, float roughness, f3 incoming, f3 outgoing, f3 gn) {
+    const bool beckmann = (op & kGlossyBeckmann) != 0u;
+    const float ndv = maxf_(dot(gn, incoming), 0.0f);
+    const float ndl = maxf_(dot(gn, outgoing), 0.0f);
+    const f3 h = safe_normalize(incoming + outgoing, gn);
+    const float ndh = maxf_(dot(gn, h), 0.0f);
+    const float vdh = maxf_(dot(incoming, h), 0.0f);
+    const bool singular = microfacet_singular(roughness);
+    const float alpha = maxf_(microfacet_alpha(roughness), 1.0e-10f);
+    const float d = microfacet_distribution(beckmann, ndh, alpha);
+    const float lv = microfacet_lambda(beckmann, ndv, alpha);
+    const float g = 1.0f / (1.0f + lv + microfacet_lambda(beckmann, ndl, alpha));
+    const bool valid = ndv > 0.0f && ndl > 0.0f && ndh > 0.0f && vdh > 0.0f && !singular;
+    Microfacet r;
+    r.intensity = valid ? d * g / maxf_(4.0f * ndv, 1.0e-20f) : 0.0f;
+    r.pdf = valid ? d / maxf_(4.0f * ndv, 1.0e-20f) / (1.0f + lv) : 0.0f;
+    return r;
 }
 
 struct Evaluation {
@@ -507,26 +784,45 @@ __device__ __noinline__ f3 oren_nayar_intensity(const PhysicalClosure &c, float 
 }
 
 // surface_closure_evaluation_contribution + accumulator
-// (src/luisa/surface_closure_evaluation.cpp:71-438).  Every diffuse closure
+// (src/luisa/surface_closure_evaluation.cpp:61-438).  Every diffuse closure
 // shares the closure normal, so the cosine, pdf and bump term are taken
-// once.  Out of line: the shading kernel calls it for the light sample and
-// for the BSDF sample, and a single copy keeps the kernel's code within the
-// instruction cache.
-__device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, f3 shading_normal, f3 incoming,
+// once; a glossy closure is evaluated in its corrected normal, and its bump
+// term (which rejects a direction on the wrong side of the smooth surface
+// unless the closure produced it) is its own.  Out of line: the shading
+// kernel calls it for the light sample and for the BSDF sample, and a
+// single copy keeps the kernel's code within the instruction cache.
+__device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, const ClosurePoint &pt,
                                                     f3 outgoing_raw, uint32_t lobe_mask, int selected) {
-    const f3 outgoing = safe_normalize(outgoing_raw, shading_normal);
+    const f3 outgoing = safe_normalize(outgoing_raw, pt.shading_normal);
+    const f3 incoming = safe_normalize(pt.incoming, -outgoing);
     Evaluation e{mk3(0.0f), 0.0f, 0u};
     float total = 0.0f, weighted_pdf = 0.0f;
     const bool diffuse_enabled = (lobe_mask & kEventDiffuse) != 0u;
+    const bool glossy_enabled = (lobe_mask & kEventGlossy) != 0u;
     const bool transparent_enabled = (lobe_mask & kEventTransparent) != 0u;
     const f3 n = s.normal;
     const float nl = maxf_(dot(n, outgoing), 0.0f);
-    const float bump = bump_shadowing(shading_normal, n, outgoing);
+    const float bump = bump_shadowing(pt.shading_normal, n, outgoing, true, true, pt.bump_correction);
     const float lambert = nl * kInvPi;
     for (uint32_t i = 0; i < s.count; ++i) {
         const PhysicalClosure &c = s.c[i];
         if (c.op == PSY_CLOSURE_TRANSPARENT) {
             if (transparent_enabled) total += c.sample_weight;
+            continue;
+        }
+        if (is_glossy(c.op)) {
+            if (!glossy_enabled) continue;
+            const bool is_selected = int(i) == selected;
+            const float gb = bump_shadowing(pt.shading_normal, c.color, outgoing, !is_selected, false,
+                                            pt.bump_correction);
+            const f3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.color);
+            const Microfacet m = microfacet_eval(c.op, c.roughness, incoming, outgoing, gn);
+            const float pdf = (gb != 0.0f || is_selected) ? m.pdf : 0.0f;
+            const f3 value = c.weight * m.intensity * gb;
+            e.f = e.f + value;
+            total += c.sample_weight;
+            weighted_pdf += c.sample_weight * pdf;
+            if (closure_sample_weight(value) > 0.0f) e.events |= kEventGlossy | kEventReflection;
             continue;
         }
         const bool pdf_valid = bump != 0.0f || int(i) == selected;
@@ -552,29 +848,32 @@ struct SurfaceSample {
     uint32_t closure_index;
 };
 
-// SurfaceClosureSamplingVisitor::visit (src/luisa/surface_closure_sampling_core.cpp:744-812).
-__device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s, f3 shading_normal, f3 geometric_normal,
-                                                        f3 incoming, float u_lobe, f2 u_dir, uint32_t lobe_mask) {
+__device__ __forceinline__ bool closure_eligible(uint32_t op, uint32_t lobe_mask) {
+    if (op == PSY_CLOSURE_DIFFUSE) return (lobe_mask & kEventDiffuse) != 0u;
+    if (is_glossy(op)) return (lobe_mask & kEventGlossy) != 0u;
+    return (lobe_mask & kEventTransparent) != 0u;
+}
+
+// SurfaceClosureSamplingVisitor::visit (src/luisa/surface_closure_sampling_core.cpp:744-812;
+// selection :97-214, categorical inversion :420-437, conditional sample
+// :216-337 with the glossy sample_microfacet_reflection of
+// graph_surface_scattering.cpp:730-770, finish :490-660).
+__device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s, const ClosurePoint &pt, float u_lobe,
+                                                        f2 u_dir, uint32_t lobe_mask) {
     SurfaceSample out;
     out.valid = false;
     out.wi = mk3(0.0f);
     out.eval = {mk3(0.0f), 0.0f, 0u};
     out.closure_index = kInvalid;
-    const bool diffuse_enabled = (lobe_mask & kEventDiffuse) != 0u;
-    const bool transparent_enabled = (lobe_mask & kEventTransparent) != 0u;
     float total = 0.0f;
-    for (uint32_t i = 0; i < s.count; ++i) {
-        const bool eligible = s.c[i].op == PSY_CLOSURE_DIFFUSE ? diffuse_enabled : transparent_enabled;
-        total += eligible ? s.c[i].sample_weight : 0.0f;
-    }
+    for (uint32_t i = 0; i < s.count; ++i) total += closure_eligible(s.c[i].op, lobe_mask) ? s.c[i].sample_weight : 0.0f;
     const float random_lobe = clampf_(u_lobe, 0.0f, 0.99999994f);
     const float target = random_lobe * total;
     float accumulated = 0.0f;
     int chosen = -1;
     float chosen_weight = 0.0f;
     for (uint32_t i = 0; i < s.count; ++i) {
-        const bool eligible = s.c[i].op == PSY_CLOSURE_DIFFUSE ? diffuse_enabled : transparent_enabled;
-        const float w = eligible ? s.c[i].sample_weight : 0.0f;
+        const float w = closure_eligible(s.c[i].op, lobe_mask) ? s.c[i].sample_weight : 0.0f;
         const float next = accumulated + w;
         if (chosen < 0 && w > 0.0f && target < next) {
             chosen = int(i);
@@ -585,27 +884,56 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
     if (chosen < 0) return out;
     const PhysicalClosure c = s.c[chosen];
     const bool transparent = c.op == PSY_CLOSURE_TRANSPARENT;
-    const f3 direction = transparent ? -incoming : sample_cosine_hemisphere(s.normal, u_dir, nullptr);
+    const bool glossy = is_glossy(c.op);
+    bool candidate_valid = true, singular = false;
+    f3 direction;
+    if (transparent) {
+        direction = -pt.incoming;
+    } else if (glossy) {
+        const f3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
+        const f3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.color);
+        const float alpha = microfacet_alpha(c.roughness);
+        const float sampling_alpha = maxf_(alpha, 1.0e-10f);
+        singular = alpha * alpha <= kMicrofacetSingularAlphaProduct;
+        if (singular) {
+            direction = gn * (2.0f * dot(gn, incoming)) - incoming;
+        } else {
+            const f3 h = (c.op & kGlossyBeckmann) != 0u
+                             ? sample_beckmann_visible_normal(gn, incoming, sampling_alpha, u_dir)
+                             : sample_ggx_visible_normal(gn, incoming, sampling_alpha, u_dir);
+            direction = h * (2.0f * dot(incoming, h)) - incoming;
+        }
+        candidate_valid = dot(gn, incoming) > 0.0f && dot(gn, direction) > 0.0f &&
+                          dot(pt.geometric_normal, direction) > 0.0f;
+    } else {
+        direction = sample_cosine_hemisphere(s.normal, u_dir, nullptr);
+    }
     out.closure_index = uint32_t(chosen);
     out.wi = direction;
-    if (!(transparent || dot(geometric_normal, direction) > 0.0f)) return out;
-    const Evaluation mixture = evaluate_mixture(s, shading_normal, incoming, direction, lobe_mask, chosen);
+    if (!(candidate_valid && (transparent || dot(pt.geometric_normal, direction) > 0.0f))) return out;
+    const Evaluation mixture = evaluate_mixture(s, pt, direction, lobe_mask, chosen);
     Evaluation r;
     r.f = mixture.f;
     float delta = 0.0f;
-    if (transparent) {
+    if (transparent || (glossy && singular)) {
+        // transparent: weight x 1e6; singular glossy: weight x Fresnel (one)
+        // x bump term (one when sampling a glossy closure) x 1e6
         r.f = r.f + c.weight * 1.0e6f;
         delta = 1.0e6f * chosen_weight;
     }
     r.pdf = mixture.pdf + delta / maxf_(total, 1.0e-20f);
-    r.events = transparent ? (kEventTransmission | kEventTransparent) : (kEventDiffuse | kEventReflection);
+    if (transparent) r.events = kEventTransmission | kEventTransparent;
+    else if (glossy) r.events = singular ? (kEventSingular | kEventReflection) : (kEventGlossy | kEventReflection);
+    else r.events = kEventDiffuse | kEventReflection;
     out.eval = r;
     out.valid = true;
     return out;
 }
 
-// AOV visitor (src/luisa/surface_closure_operations.cpp:402-462).
-__device__ __forceinline__ void surface_aov(const SurfaceClosures &s, f3 shading_normal, f3 &albedo, f3 &normal,
+// AOV visitor (src/luisa/surface_closure_operations.cpp:40-161, 402-462):
+// diffuse colour into Albedo, every diffuse and glossy normal (glossy:
+// corrected) weighted by |average weight| into Normal.
+__device__ __forceinline__ void surface_aov(const SurfaceClosures &s, const ClosurePoint &pt, f3 &albedo, f3 &normal,
                                             f3 &transparency) {
     albedo = mk3(0.0f);
     transparency = mk3(0.0f);
@@ -618,11 +946,16 @@ __device__ __forceinline__ void surface_aov(const SurfaceClosures &s, f3 shading
             const float w = closure_sample_weight(c.weight);
             n = n + s.normal * w;
             total += w;
+        } else if (is_glossy(c.op)) {
+            const f3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
+            const float w = closure_sample_weight(c.weight);
+            n = n + specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.color) * w;
+            total += w;
         } else {
             transparency = transparency + c.weight;
         }
     }
-    normal = safe_normalize(total > 0.0f ? n : shading_normal, shading_normal);
+    normal = safe_normalize(total > 0.0f ? n : pt.shading_normal, pt.shading_normal);
 }
 
 // ---------------------------------------------------------- intersection

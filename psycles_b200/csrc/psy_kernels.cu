@@ -737,7 +737,8 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                 const SurfacePoint sp = surface_point(s, h, ray.d);
                 const MaterialGpu mat = s.materials[sp.material];
                 SurfaceClosures closures;
-                collect_surface(s, mat, sp.n, closures);
+                const ClosurePoint cpt{sp.n, sp.ng, -ray.d, mat.bump_correction != 0u};
+                collect_surface(s, mat, cpt, closures);
                 // SurfaceShadingStageImpl::emit (src/luisa/path_kernel_surface_shading.cpp:117-250)
                 float emission_weight = 1.0f;
                 if (p.nee && s.triangle_emitters > 0u && mat.emission_sampling != 0u && mat.has_emission) {
@@ -782,7 +783,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                 if (alive) {
                     if (depth == 0u) {
                         f3 aov_albedo, aov_normal, aov_transparency;
-                        surface_aov(closures, sp.n, aov_albedo, aov_normal, aov_transparency);
+                        surface_aov(closures, cpt, aov_albedo, aov_normal, aov_transparency);
                         const float4 a4 = b.aov_a[i];
                         const f3 acc = mk3(a4.x, a4.y, a4.z) + throughput * aov_albedo;
                         b.aov_a[i] = make_float4(acc.x, acc.y, acc.z, 0.0f);
@@ -870,7 +871,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                             }
                         }
                         if (sampled) {
-                            const Evaluation e = evaluate_mixture(closures, sp.n, -ray.d, ldir, lobe_mask, -1);
+                            const Evaluation e = evaluate_mixture(closures, cpt, ldir, lobe_mask, -1);
                             const float mis = weigh_mis ? nee_light_weight(p.direct_mode, light_pdf, e.pdf) : 1.0f;
                             const f3 weighted = e.f * light_radiance * (mis / pdf_divisor);
                             if (any_nonzero(weighted)) {
@@ -898,8 +899,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                         }
                     }
                     // SurfaceScatterStageImpl::emit (src/luisa/path_kernel_surface_scatter.cpp:136-291)
-                    const SurfaceSample ss = sample_surface(closures, sp.n, sp.ng, -ray.d, bs4.z, mk2(bs4.x, bs4.y),
-                                                            lobe_mask);
+                    const SurfaceSample ss = sample_surface(closures, cpt, bs4.z, mk2(bs4.x, bs4.y), lobe_mask);
                     if (ev) {
                         ev->closure_index = ss.closure_index;
                         ev->bsdf_pdf = ss.eval.pdf;

@@ -1,8 +1,8 @@
 """Shader graphs, SurfacePrograms and the incremental material library.
 
 Host mirror of the reference's material contract for the in-scope node set:
-closures diffuse (Lambert / Oren-Nayar by roughness), emission, transparent,
-add and mix, fed by constants, float math, conversions, mixes, colour blends
+closures diffuse (Lambert / Oren-Nayar by roughness), glossy (GGX / Beckmann
+microfacet reflection), emission, transparent, add and mix, fed by constants, float math, conversions, mixes, colour blends
 and separate / combine RGB:
 
   * ShaderGraph / node types       include/psycles/contract/shader_graph.h,
@@ -43,6 +43,7 @@ class NodeType(str, enum.Enum):
     DIFFUSE = "psycles.closure.diffuse"
     EMISSION = "psycles.closure.emission"
     TRANSPARENT = "psycles.closure.transparent"
+    GLOSSY = "psycles.closure.glossy"
     ADD = "psycles.closure.add"
     MIX = "psycles.closure.mix"
     # values
@@ -71,7 +72,9 @@ class NodeType(str, enum.Enum):
     COMBINE_COLOR = "psycles.color.combine"
 
 
-CLOSURE_TYPES = (NodeType.DIFFUSE, NodeType.EMISSION, NodeType.TRANSPARENT, NodeType.ADD, NodeType.MIX)
+CLOSURE_TYPES = (NodeType.DIFFUSE, NodeType.EMISSION, NodeType.TRANSPARENT, NodeType.GLOSSY, NodeType.ADD,
+                 NodeType.MIX)
+GLOSSY_DISTRIBUTIONS = {"GGX": _abi.GLOSSY_GGX, "BECKMANN": _abi.GLOSSY_BECKMANN}
 
 F, C = "float", "color"  # socket kinds: scalar and vector values
 
@@ -81,6 +84,7 @@ _SCHEMA: dict[NodeType, tuple[list, list]] = {
     NodeType.DIFFUSE: ([("Color", C, (0.8, 0.8, 0.8)), ("Roughness", F, 0.0)], []),
     NodeType.EMISSION: ([("Color", C, (1.0, 1.0, 1.0)), ("Strength", F, 1.0)], []),
     NodeType.TRANSPARENT: ([("Color", C, (1.0, 1.0, 1.0))], []),
+    NodeType.GLOSSY: ([("Color", C, (0.8, 0.8, 0.8)), ("Roughness", F, 0.2)], []),
     NodeType.ADD: ([], []),
     NodeType.MIX: ([("Factor", F, 0.5)], []),
     NodeType.CONSTANT_FLOAT: ([("Value", F, 0.0)], [("Value", F)]),
@@ -173,6 +177,13 @@ class ShaderGraph:
     # closures
     def diffuse_bsdf(self, color, roughness=0.0) -> int:
         return self._node(NodeType.DIFFUSE, Color=color, Roughness=roughness)
+
+    def glossy_bsdf(self, color, roughness=0.2, distribution: str = "GGX") -> int:
+        """Glossy BSDF (core_nodes.cpp:980-990): GGX or Beckmann microfacet
+        reflection; the Distribution property is structural."""
+        if distribution not in GLOSSY_DISTRIBUTIONS:
+            raise ShaderGraphError(f"glossy distribution {distribution!r} outside GGX and BECKMANN")
+        return self._node(NodeType.GLOSSY, {"Distribution": distribution}, Color=color, Roughness=roughness)
 
     def emission(self, color, strength=1.0) -> int:
         return self._node(NodeType.EMISSION, Color=color, Strength=strength)
@@ -438,6 +449,9 @@ def compile_surface_program(graph: ShaderGraph) -> tuple[SurfaceProgram, Surface
                          low.closure_input(n, "Roughness")))
         elif n.type == NodeType.TRANSPARENT:
             code.append((_abi.CLOSURE_TRANSPARENT, 0, 0, low.closure_input(n, "Color"), none, none))
+        elif n.type == NodeType.GLOSSY:
+            code.append((_abi.CLOSURE_GLOSSY, GLOSSY_DISTRIBUTIONS[n.props.get("Distribution", "GGX")], 0,
+                         low.closure_input(n, "Color"), none, low.closure_input(n, "Roughness")))
         elif n.type == NodeType.EMISSION:
             code.append((_abi.CLOSURE_EMISSION, 0, 0, low.closure_input(n, "Color"), low.closure_input(n, "Strength"),
                          none))
@@ -552,6 +566,36 @@ def random_material(rng: np.random.Generator, max_leaves: int = 6, emission_prob
         else:
             ids.append(g.add_shader(a, b))
     return g.set_output(ids[0])
+
+
+def glossy_material(color, roughness: float = 0.2, distribution: str = "GGX") -> ShaderGraph:
+    g = ShaderGraph()
+    return g.set_output(g.glossy_bsdf(color, roughness, distribution))
+
+
+def glossy_mixture_material(rng: np.random.Generator) -> ShaderGraph:
+    """A random mixture with glossy lobes: diffuse + glossy (mix or add),
+    glossy over a transparent closure, or glossy with a roughness linked to
+    a Value node; GGX or Beckmann, roughness 0 (a mirror: singular) to 0.8."""
+    g = ShaderGraph()
+    dist = "BECKMANN" if rng.random() < 0.35 else "GGX"
+    rough = 0.0 if rng.random() < 0.2 else float(rng.uniform(0.05, 0.8))
+    color = tuple(float(v) for v in rng.uniform(0.3, 0.95, 3))
+    kind = int(rng.integers(0, 4))
+    if kind == 0:
+        gl = g.glossy_bsdf(color, rough, dist)
+        d = g.diffuse_bsdf(tuple(float(v) for v in rng.uniform(0.1, 0.8, 3)), float(rng.uniform(0.0, 0.6)))
+        return g.set_output(g.mix_shader(float(rng.uniform(0.1, 0.9)), d, gl))
+    if kind == 1:
+        gl = g.glossy_bsdf(color, rough, dist)
+        d = g.diffuse_bsdf(tuple(float(v) for v in rng.uniform(0.1, 0.5, 3)))
+        return g.set_output(g.add_shader(d, gl))
+    if kind == 2:
+        gl = g.glossy_bsdf(color, rough, dist)
+        t = g.transparent_bsdf(tuple(float(v) for v in rng.uniform(0.4, 0.9, 3)))
+        return g.set_output(g.mix_shader(float(rng.uniform(0.2, 0.8)), gl, t))
+    r = g.math("multiply", g.value(float(rng.uniform(0.1, 0.9))), float(rng.uniform(0.3, 1.0)))
+    return g.set_output(g.glossy_bsdf(color, r, dist))
 
 
 def value_graph_material(rng: np.random.Generator) -> ShaderGraph:

@@ -28,7 +28,8 @@ import numpy as np
 
 from . import _abi
 from .materials import (CompiledMaterial, ShaderGraph, compile_surface_program, diffuse_material,
-                        emission_material, random_material, value_graph_material)
+                        emission_material, glossy_material, glossy_mixture_material, random_material,
+                        value_graph_material)
 
 
 @dataclasses.dataclass
@@ -527,6 +528,25 @@ def lamp_scene(seed: int = 0) -> Scene:
     return Scene(meshes, instances, mats, ls, cam, background=(0.05, 0.05, 0.08))
 
 
+def glossy_scene(seed: int = 0) -> Scene:
+    """The small test scene's geometry and lamps with glossy materials: GGX
+    and Beckmann at roughness 0 (mirror), 0.1, 0.35 and 0.6 on the spheres
+    and boxes (smooth-normal spheres exercise the specular-reflection normal
+    correction), a glossy floor, and random diffuse + glossy, glossy +
+    transparent and value-linked-roughness mixtures; one material turns the
+    bump-map correction off."""
+    rng = np.random.default_rng(seed)
+    graphs = [glossy_material((0.8, 0.8, 0.8), 0.25), emission_material((1.0, 0.9, 0.8), 6.0),
+              glossy_material((0.9, 0.8, 0.6), 0.0), glossy_material((0.6, 0.8, 0.9), 0.35, "BECKMANN"),
+              glossy_material((0.9, 0.9, 0.9), 0.1), glossy_material((0.7, 0.9, 0.7), 0.6, "BECKMANN")]
+    for _ in range(2):
+        graphs.append(glossy_mixture_material(rng))
+    base = small_test_scene(seed=seed)
+    base.materials = _materials(graphs)
+    base.materials[3].use_bump_map_correction = False
+    return base
+
+
 def value_graph_scene(seed: int = 0) -> Scene:
     """The small test scene's geometry and lamps with materials whose closure
     inputs are linked to value nodes (RGB / Value nodes through colour
@@ -569,22 +589,32 @@ def _f32_view(eye, target) -> np.ndarray:
     return m
 
 
-def luisa_demo_scene(graph_material: bool = False) -> Scene:
+def luisa_demo_scene(variant: int = 0) -> Scene:
     """The Cornell-style room of the reference's Luisa demo
     (examples/render_luisa_demo.cpp:203-305) in this scene model: a floor and
     three walls in one mesh with per-triangle materials, a cube scaled to a
     block, rough diffuse plaster / red / green / blue, a 1.8 m square area
     light under the open ceiling and a background light, 47 degree camera.
-    With `graph_material` the block's colour is an RGB-node mix and its
-    roughness float math, as tests/adapter/adapter_probe.cpp builds them."""
+    Variant 1 (or True): the block's colour is an RGB-node mix and its
+    roughness float math; variant 2: the block is a GGX Glossy BSDF and the
+    plaster a mix of rough diffuse and Beckmann glossy -- as
+    tests/adapter/adapter_probe.cpp builds them."""
     f = np.float32
+    variant = int(variant)
     graphs = [diffuse_material((0.72, 0.72, 0.72), 0.35), diffuse_material((0.72, 0.06, 0.035), 0.45),
               diffuse_material((0.04, 0.54, 0.12), 0.45)]
-    if graph_material:
+    if variant == 2:
+        g = ShaderGraph()
+        g.set_output(g.mix_shader(0.25, g.diffuse_bsdf((0.72, 0.72, 0.72), 0.35),
+                                  g.glossy_bsdf((0.9, 0.9, 0.85), 0.2, "BECKMANN")))
+        graphs[0] = g
+    if variant == 1:
         g = ShaderGraph()
         color = g.mix_color(0.3, g.rgb((0.035, 0.18, 0.85)), g.rgb((0.9, 0.5, 0.1)))
         g.set_output(g.diffuse_bsdf(color, g.math("clamp", g.math("multiply", g.value(0.6), 0.5))))
         graphs.append(g)
+    elif variant == 2:
+        graphs.append(glossy_material((0.035, 0.18, 0.85), 0.3, "GGX"))
     else:
         graphs.append(diffuse_material((0.035, 0.18, 0.85), 0.16))
     mats = _materials(graphs)

@@ -12,7 +12,10 @@
 // background light and rough diffuse materials.  The "graph" variant feeds
 // the block's colour and roughness through value nodes (an RGB node through
 // a colour mix, a Value node through float math) so that the reference's
-// compiler emits a non-trivial value stream.
+// compiler emits a non-trivial value stream.  The "glossy" variant makes the
+// block a GGX Glossy BSDF and the plaster a mix of rough diffuse and
+// Beckmann glossy; the "multiscatter" variant asks for the MULTI_GGX
+// distribution, which the adapter must refuse.
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -91,6 +94,34 @@ ShaderGraph graph_diffuse() {
     return g;
 }
 
+ShaderGraph glossy(Vec3f color, float roughness, const char *distribution) {
+    ShaderGraph g;
+    const NodeId n = g.add_node(compiler::node_type::glossy_bsdf, "Glossy");
+    (void)g.set_input(n, "Color", SocketValue::color(color));
+    (void)g.set_input(n, "Roughness", SocketValue::floating(roughness));
+    (void)g.set_property(n, "Distribution", SocketValue::string(distribution));
+    g.set_root(ShaderDomain::surface, OutputRef{n, "Closure"});
+    return g;
+}
+
+// Plaster as Mix(0.25, rough diffuse, Beckmann glossy).
+ShaderGraph glossy_plaster() {
+    ShaderGraph g;
+    const NodeId d = g.add_node(compiler::node_type::diffuse_bsdf, "Diffuse");
+    (void)g.set_input(d, "Color", SocketValue::color(v3(0.72f, 0.72f, 0.72f)));
+    (void)g.set_input(d, "Roughness", SocketValue::floating(0.35f));
+    const NodeId s = g.add_node(compiler::node_type::glossy_bsdf, "Glossy");
+    (void)g.set_input(s, "Color", SocketValue::color(v3(0.9f, 0.9f, 0.85f)));
+    (void)g.set_input(s, "Roughness", SocketValue::floating(0.2f));
+    (void)g.set_property(s, "Distribution", SocketValue::string("BECKMANN"));
+    const NodeId m = g.add_node(compiler::node_type::mix_closure, "Mix");
+    (void)g.set_input(m, "Factor", SocketValue::floating(0.25f));
+    (void)g.connect(OutputRef{d, "Closure"}, m, "A");
+    (void)g.connect(OutputRef{s, "Closure"}, m, "B");
+    g.set_root(ShaderDomain::surface, OutputRef{m, "Closure"});
+    return g;
+}
+
 void quad(TriangleMeshDesc &m, Vec3f a, Vec3f b, Vec3f c, Vec3f d, Vec3f n, std::uint32_t slot) {
     const auto base = static_cast<std::uint32_t>(m.positions.size());
     for (const Vec3f &p : {a, b, c, d}) {
@@ -103,16 +134,22 @@ void quad(TriangleMeshDesc &m, Vec3f a, Vec3f b, Vec3f c, Vec3f d, Vec3f n, std:
     m.triangle_material_slots.push_back(slot);
 }
 
-SceneSnapshot demo_snapshot(bool graph_material) {
+// variant: 0 plain, 1 value-graph block, 2 glossy block and plaster,
+// 3 a MULTI_GGX block
+SceneSnapshot demo_snapshot(int variant) {
     const MaterialId plaster{1u}, red{2u}, green{3u}, block{4u};
+    const bool graph_material = variant == 1;
     SceneDelta delta;
     delta.base_revision = 0u;
-    delta.emplace<UpsertMaterial>(plaster, MaterialDesc{.name = "Plaster", .shader = rough_diffuse(v3(0.72f, 0.72f, 0.72f), 0.35f)});
+    delta.emplace<UpsertMaterial>(
+        plaster, MaterialDesc{.name = "Plaster",
+                              .shader = variant == 2 ? glossy_plaster() : rough_diffuse(v3(0.72f, 0.72f, 0.72f), 0.35f)});
     delta.emplace<UpsertMaterial>(red, MaterialDesc{.name = "Red wall", .shader = rough_diffuse(v3(0.72f, 0.06f, 0.035f), 0.45f)});
     delta.emplace<UpsertMaterial>(green, MaterialDesc{.name = "Green wall", .shader = rough_diffuse(v3(0.04f, 0.54f, 0.12f), 0.45f)});
-    delta.emplace<UpsertMaterial>(
-        block, MaterialDesc{.name = "Blue block",
-                            .shader = graph_material ? graph_diffuse() : rough_diffuse(v3(0.035f, 0.18f, 0.85f), 0.16f)});
+    ShaderGraph block_shader = graph_material ? graph_diffuse() : rough_diffuse(v3(0.035f, 0.18f, 0.85f), 0.16f);
+    if (variant == 2) block_shader = glossy(v3(0.035f, 0.18f, 0.85f), 0.3f, "GGX");
+    if (variant == 3) block_shader = glossy(v3(0.035f, 0.18f, 0.85f), 0.3f, "MULTI_GGX");
+    delta.emplace<UpsertMaterial>(block, MaterialDesc{.name = "Blue block", .shader = std::move(block_shader)});
     TriangleMeshDesc room;
     room.name = "Room";
     room.material_slots = {plaster, red, green};
@@ -184,8 +221,8 @@ extern "C" {
 
 // The demo snapshot compiled by the reference's MaterialLibrary and
 // flattened by the adapter; null with a message on failure.
-void *probe_demo_flatten(int graph_material, char *error, std::size_t capacity) {
-    const SceneSnapshot snapshot = demo_snapshot(graph_material != 0);
+void *probe_demo_flatten(int variant, char *error, std::size_t capacity) {
+    const SceneSnapshot snapshot = demo_snapshot(variant);
     if (snapshot.revision == 0u) {
         set_error(error, capacity, "SceneDatabase::apply rejected the demo delta");
         return nullptr;
@@ -229,10 +266,10 @@ void probe_flat_destroy(void *flattened) { delete static_cast<Flattened *>(flatt
 // the Combined, Normal, Albedo (4 channels) and Sample Count (1 channel)
 // passes out, and writes the Combined pass with the reference's write_pfm to
 // `pfm_path` when it is not null.  Returns 0, or 1 with a message.
-int probe_demo_render(int device, int graph_material, std::uint32_t width, std::uint32_t height, std::uint32_t spp,
+int probe_demo_render(int device, int variant, std::uint32_t width, std::uint32_t height, std::uint32_t spp,
                       std::uint32_t chunks, float *combined, float *normal, float *albedo, float *sample_count,
                       const char *pfm_path, char *error, std::size_t capacity) {
-    const SceneSnapshot snapshot = demo_snapshot(graph_material != 0);
+    const SceneSnapshot snapshot = demo_snapshot(variant);
     cuda_backend::CudaPathTracerBackend backend{{.device = device, .next_event_estimation = true}};
     if (!backend.valid()) {
         set_error(error, capacity, backend.context_error());

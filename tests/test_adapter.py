@@ -42,12 +42,13 @@ def probe():
 
 
 class Flattened:
-    """The adapter's flattened demo snapshot; `.pointer` as scenes.SceneDescHandle."""
+    """The adapter's flattened demo snapshot (variant 0 plain, 1 value-graph
+    block, 2 glossy); `.pointer` as scenes.SceneDescHandle."""
 
-    def __init__(self, graph_material: bool):
+    def __init__(self, variant):
         self.lib = probe()
         err = ctypes.create_string_buffer(512)
-        self.handle = self.lib.probe_demo_flatten(1 if graph_material else 0, err, 512)
+        self.handle = self.lib.probe_demo_flatten(int(variant), err, 512)
         assert self.handle, err.value.decode()
         self.desc = self.lib.probe_flat_desc(self.handle).contents
         self.pointer = ctypes.pointer(self.desc)
@@ -103,15 +104,23 @@ def test_flattened_snapshot_equals_scene_model():
         assert arr(ma.scalars, ma.scalar_count)[ca.roughness] == arr(mb.scalars, mb.scalar_count)[cb.roughness]
 
 
-@pytest.mark.parametrize("graph_material", [False, True])
+@pytest.mark.parametrize("graph_material", [0, 1, 2])
 def test_flattened_snapshot_renders_as_scene_model(graph_material):
     flat = Flattened(graph_material)
     model = scenes.luisa_demo_scene(graph_material)
-    if graph_material:
+    if graph_material == 1:
         block = flat.desc.materials[3]
         assert block.value_count > 0  # the reference compiler emitted a value stream
         c = block.closures[block.root]
         assert c.color & _abi.INPUT_VALUE and c.roughness & _abi.INPUT_VALUE
+    if graph_material == 2:
+        # the reference compiler's glossy closures: GGX block, Beckmann in the plaster mix
+        block = flat.desc.materials[3]
+        c = block.closures[block.root]
+        assert (c.op, c.a) == (_abi.CLOSURE_GLOSSY, _abi.GLOSSY_GGX)
+        plaster = flat.desc.materials[0]
+        ops = {(plaster.closures[k].op, plaster.closures[k].a) for k in range(plaster.closure_count)}
+        assert (_abi.CLOSURE_GLOSSY, _abi.GLOSSY_BECKMANN) in ops and plaster.flags == 0
     st = scenes.render_settings(64, 48, max_bounces=4)
     fa, fb = OracleFilm(st), OracleFilm(st)
     fa.render(flat, 0, 4, 4)
@@ -134,3 +143,13 @@ def test_pfm_writer_equals_the_reference_writer(tmp_path):
         assert lib.probe_write_pfm(7, 5, channels, img.ctypes.data, str(ref).encode()) == 0
         write_pfm(img, ours)
         assert ref.read_bytes() == ours.read_bytes(), channels
+
+
+def test_multiscatter_glossy_is_refused():
+    """MULTI_GGX needs Cycles' tabulated energy-preservation tables, which
+    are not in the CUDA path: flatten() refuses the material with a
+    diagnostic instead of rendering it as plain GGX."""
+    lib = probe()
+    err = ctypes.create_string_buffer(512)
+    assert not lib.probe_demo_flatten(3, err, 512)
+    assert "Multiscatter GGX" in err.value.decode()

@@ -9,8 +9,9 @@ io::MemoryOutputSink in several sample ranges, then io::write_pfm.  The
 passes must match the oracle's render of the adapter's flattened snapshot
 (relative RMSE 1e-3, at most 1 % of pixels differing in any bit), the PFM
 must hold the Combined pass, and an unsupported pass must be refused with a
-null session.  Both the plain demo materials and the variant whose block the
-reference compiler lowers to a value stream are rendered."""
+null session.  The plain demo materials, the variant whose block the
+reference compiler lowers to a value stream, and the glossy variant (GGX
+block, diffuse + Beckmann plaster) are rendered."""
 
 import ctypes
 import pathlib
@@ -29,7 +30,7 @@ pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not PROBE.exists(), reason="adapter probe not built (make -C oracle adapter)")]
 
 
-@pytest.mark.parametrize("graph_material", [0, 1])
+@pytest.mark.parametrize("graph_material", [0, 1, 2])
 def test_snapshot_renders_through_the_contract(tmp_path, graph_material):
     from test_adapter import Flattened, probe
     lib = probe()
@@ -45,7 +46,7 @@ def test_snapshot_renders_through_the_contract(tmp_path, graph_material):
                                out["normal"].ctypes.data, out["albedo"].ctypes.data, count.ctypes.data,
                                str(pfm).encode(), err, 512)
     assert rc == 0, err.value.decode()
-    flat = Flattened(bool(graph_material))
+    flat = Flattened(graph_material)
     st = scenes.render_settings(w, h, max_bounces=4)
     film = OracleFilm(st)
     film.render(flat, 0, spp, spp)
