@@ -848,6 +848,34 @@ struct SurfaceSample {
     uint32_t closure_index;
 };
 
+// sample_microfacet_reflection (src/luisa/graph_surface_scattering.cpp:730-770)
+// of a glossy closure with normal `cn`: the visible-normal half vector
+// reflects the view, or at alpha^2 <= 2e-10 the mirror direction of the
+// corrected normal; valid when the view and the direction lie above the
+// corrected normal and the direction above the geometric surface.
+struct GlossySample {
+    f3 direction;
+    bool valid, singular;
+};
+__device__ __noinline__ GlossySample sample_glossy(uint32_t op, float roughness, f3 cn, const ClosurePoint &pt,
+                                                   f2 u_dir) {
+    const f3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
+    const f3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, cn);
+    const float alpha = microfacet_alpha(roughness);
+    const float sampling_alpha = maxf_(alpha, 1.0e-10f);
+    GlossySample g;
+    g.singular = alpha * alpha <= kMicrofacetSingularAlphaProduct;
+    if (g.singular) {
+        g.direction = gn * (2.0f * dot(gn, incoming)) - incoming;
+    } else {
+        const f3 h = (op & kGlossyBeckmann) != 0u ? sample_beckmann_visible_normal(gn, incoming, sampling_alpha, u_dir)
+                                                  : sample_ggx_visible_normal(gn, incoming, sampling_alpha, u_dir);
+        g.direction = h * (2.0f * dot(incoming, h)) - incoming;
+    }
+    g.valid = dot(gn, incoming) > 0.0f && dot(gn, g.direction) > 0.0f && dot(pt.geometric_normal, g.direction) > 0.0f;
+    return g;
+}
+
 __device__ __forceinline__ bool closure_eligible(uint32_t op, uint32_t lobe_mask) {
     if (op == PSY_CLOSURE_DIFFUSE) return (lobe_mask & kEventDiffuse) != 0u;
     if (is_glossy(op)) return (lobe_mask & kEventGlossy) != 0u;
@@ -890,21 +918,10 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
     if (transparent) {
         direction = -pt.incoming;
     } else if (glossy) {
-        const f3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
-        const f3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.color);
-        const float alpha = microfacet_alpha(c.roughness);
-        const float sampling_alpha = maxf_(alpha, 1.0e-10f);
-        singular = alpha * alpha <= kMicrofacetSingularAlphaProduct;
-        if (singular) {
-            direction = gn * (2.0f * dot(gn, incoming)) - incoming;
-        } else {
-            const f3 h = (c.op & kGlossyBeckmann) != 0u
-                             ? sample_beckmann_visible_normal(gn, incoming, sampling_alpha, u_dir)
-                             : sample_ggx_visible_normal(gn, incoming, sampling_alpha, u_dir);
-            direction = h * (2.0f * dot(incoming, h)) - incoming;
-        }
-        candidate_valid = dot(gn, incoming) > 0.0f && dot(gn, direction) > 0.0f &&
-                          dot(pt.geometric_normal, direction) > 0.0f;
+        const GlossySample g = sample_glossy(c.op, c.roughness, c.color, pt, u_dir);
+        direction = g.direction;
+        candidate_valid = g.valid;
+        singular = g.singular;
     } else {
         direction = sample_cosine_hemisphere(s.normal, u_dir, nullptr);
     }

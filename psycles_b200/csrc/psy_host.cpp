@@ -840,7 +840,7 @@ uint32_t blas_stack_need(const std::vector<psy::WideNodeGpu> &w) {
 // n >= 2).  In the TLAS a node with hit instances first stacks its inner
 // hits (one entry when it has any), then the other hit instances (one entry
 // when there are two or more) and the return to the world ray.
-uint32_t blas_stack_need8(const std::vector<psy::CwNodeGpu> &w) {
+[[maybe_unused]] uint32_t blas_stack_need8(const std::vector<psy::CwNodeGpu> &w) {
     std::vector<uint32_t> need(w.size(), 0u);
     for (size_t i = w.size(); i-- > 0;) {
         const uint32_t imask = w[i].exps_imask >> 24;
@@ -852,7 +852,7 @@ uint32_t blas_stack_need8(const std::vector<psy::CwNodeGpu> &w) {
     return w.empty() ? 0u : need[0];
 }
 
-std::vector<uint32_t> tlas_instance_depths8(const std::vector<psy::CwNodeGpu> &w, const std::vector<uint32_t> &leaves,
+[[maybe_unused]] std::vector<uint32_t> tlas_instance_depths8(const std::vector<psy::CwNodeGpu> &w, const std::vector<uint32_t> &leaves,
                                             uint32_t instance_count) {
     std::vector<uint32_t> depth(w.size(), 0u), inst(instance_count, 0u);
     for (size_t i = 0; i < w.size(); ++i) {
