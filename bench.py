@@ -663,6 +663,25 @@ def run_viewports(backend, compiled, count: int = 64, sweep: str = "descent") ->
                               b.read_pass(_abi.PASS_COMBINED).view(np.uint32)) for (a, _), (b, _) in zip(bs, ss))
     for s, _ in list(ss) + list(bs):
         s.close()
+    # Upper bound of what graph replay leaves between kernels: a batch of
+    # one 16x16 1-spp view runs the same captured wavefront (same launch
+    # count per step) with almost no work, so its device time per launch
+    # bounds the per-launch gap (launch latency + the kernel's own minimum
+    # duration); times the batched call's launch count, it bounds what a
+    # single fused persistent kernel could save over graph replay.
+    tiny_batch = BatchRenderer(backend.context, path_capacity=best["path_capacity"], use_graph=True)
+    tiny = []
+    for _ in range(2):  # the first call captures the graph
+        t = backend.create_session(compiled, scenes.render_settings(16, 16, max_bounces=8))
+        assert tiny_batch.render([(t, SampleRange(0, 1, 0, 1))])
+        tiny.append(t)
+    tst = tiny_batch.stats()
+    for t in tiny:
+        t.close()
+    tiny_batch.close()
+    per_launch_us = tst.ms_total * 1e3 / max(int(tst.kernel_launches), 1)
+    launch_bound_ms = per_launch_us * batch_result["kernel_launches"] / 1e3
+    batch_device_ms = total / batch_result["device_samples_per_s"] * 1e3
     autotune.set_tuning(backend, default)
     return {"workload": f"{count} viewports of the procedural scene, random poses, 128^2..1920x1080, 1-16 spp, "
                         "8 bounces",
@@ -672,7 +691,12 @@ def run_viewports(backend, compiled, count: int = 64, sweep: str = "descent") ->
             "chosen": best, "batched": batch_result,
             "plain": {"samples_per_s": total / plain_wall, "device_samples_per_s": total / (dev / 1e3),
                       "wall_s": plain_wall},
-            "batched_vs_plain": plain_wall / batch_result["wall_s"], "identical": bool(same)}
+            "batched_vs_plain": plain_wall / batch_result["wall_s"], "identical": bool(same),
+            "graph_gaps": {"tiny_batch_launches": int(tst.kernel_launches), "tiny_batch_device_ms": tst.ms_total,
+                           "device_us_per_launch_bound": per_launch_us,
+                           "batched_launches": batch_result["kernel_launches"],
+                           "launch_bound_ms": launch_bound_ms, "batched_device_ms": batch_device_ms,
+                           "launch_share_bound": launch_bound_ms / batch_device_ms}}
 
 
 # DRAM bytes per second of device time of the traversal and shading kernels,
