@@ -123,7 +123,9 @@ psy_status psy_batch_render(psy_batch *batch, psy_session *const *sessions, cons
         uint32_t film = 0u;
         const uint32_t paths = plan_wavefront(plan, w % n, engine.capacity(), wave, film);
         if (wave.empty()) break;
-        ep.add(wave, paths, film, engine.max_jobs());
+        bool glossy = false;
+        for (const psy::BatchItem &it : wave) glossy = glossy || sessions[it.job]->scene->view.has_glossy != 0u;
+        ep.add(wave, paths, film, engine.max_jobs(), glossy);
     }
     if ((r = engine.reset_counters()) != PSY_OK) return r;
     EngineRun run;

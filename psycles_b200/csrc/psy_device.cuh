@@ -323,15 +323,25 @@ constexpr uint32_t kGlossyBeckmann = 0x100u;
 __device__ __forceinline__ bool is_glossy(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_GLOSSY; }
 
 // The surface point's inputs to closure setup, evaluation and sampling.
+// `view` is the normalised incoming direction every closure routine of
+// the reference takes (safe_normalize(point.incoming, ...): the fallback
+// never applies to a ray direction), normalised once per shading point.
 struct ClosurePoint {
     f3 shading_normal;    // SurfacePoint::shading_normal
     f3 geometric_normal;  // SurfacePoint::geometric_normal (facing the incoming ray)
     f3 incoming;          // SurfacePoint::incoming (-ray direction)
+    f3 view;              // normalize(incoming)
     bool bump_correction; // SurfacePoint::use_bump_map_correction
 };
 
+// Shading routines are instantiated with and without glossy closures
+// (kGlossy): a scene without them runs code with no glossy branch, which
+// keeps the shading kernel's register budget where it was before them.
+constexpr uint32_t kLeavesOf(bool glossy) { return glossy ? 15u : 7u; }
+
 struct SurfaceClosures {
-    f3 normal;  // the diffuse closures' normal
+    f3 normal;          // the diffuse closures' normal
+    bool normal_exact;  // it equals the shading normal bit for bit (bump term one)
     PhysicalClosure c[kMaxClosures];
     uint32_t count;
     f3 emission;
@@ -559,14 +569,16 @@ __device__ __forceinline__ f3 specular_normal(bool correction, f3 ng, f3 incomin
 // keeps its signed weight, uses the cutoff on |average|, and every
 // allocated transparent contribution merges into the first one
 // (bsdf_transparent_setup, :483-518: summed weights and sample weights).
+template <bool kGlossy>
 __device__ __forceinline__ void collect_surface(const SceneView &s, const MaterialGpu &m, const ClosurePoint &pt,
-                                                SurfaceClosures &out) {
+                                    SurfaceClosures &out) {
     out.count = 0u;
     out.emission = mk3(0.0f);
     out.normal = safe_normalize(pt.shading_normal, pt.shading_normal);
-    const f3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
+    out.normal_exact = out.normal.x == pt.shading_normal.x && out.normal.y == pt.shading_normal.y &&
+                       out.normal.z == pt.shading_normal.z;
     int transparent_slot = -1;
-    walk_closures(s, m, [&](uint32_t op, f3 w, f3 color, float roughness) {
+    walk_closures<kLeavesOf(kGlossy)>(s, m, [&](uint32_t op, f3 w, f3 color, float roughness) {
         if (op == PSY_CLOSURE_EMISSION) {
             out.emission = out.emission + w;
             return;
@@ -579,13 +591,13 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
             p.weight = bsdf_allocated_weight(w);
             p.sample_weight = closure_sample_weight(p.weight);
             if (!any_nonzero(p.weight)) return;
-        } else if (is_glossy(op)) {
+        } else if (kGlossy && is_glossy(op)) {
             const f3 allocated = max3(w, mk3(0.0f));
             const float allocation = closure_sample_weight(allocated);
             if (!(allocation >= 1.0e-5f)) return;
             p.weight = allocated;
             p.sample_weight = allocation * closure_sample_weight(mk3(1.0f));
-            p.color = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, out.normal);
+            p.color = specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, out.normal);
         } else {
             const float sw = closure_sample_weight(w);
             if (!(sw >= 1.0e-5f)) return;
@@ -670,9 +682,8 @@ __device__ __forceinline__ uint32_t runtime_flags(const SurfaceClosures &s, bool
 // also when sampling), and a diffuse closure under bump correction gets the
 // smoothed shadowing factor.  The in-scope diffuse closures have the
 // shading normal, so only glossy closures reach the general case.
-__device__ __forceinline__ float bump_shadowing(f3 smooth, f3 cn, f3 dir, bool is_evaluation, bool diffuse,
-                                                bool bump_correction) {
-    if (cn.x == smooth.x && cn.y == smooth.y && cn.z == smooth.z) return 1.0f;
+__device__ __noinline__ float bump_shadowing_general(f3 smooth, f3 cn, f3 dir, bool is_evaluation, bool diffuse,
+                                                     bool bump_correction) {
     const float csd = dot(smooth, dir);
     const float csc = dot(smooth, cn);
     const float ccd = dot(cn, dir);
@@ -689,6 +700,11 @@ __device__ __forceinline__ float bump_shadowing(f3 smooth, f3 cn, f3 dir, bool i
     float result = domain && !grazing ? smoothed : 1.0f;
     if (reject || grazing) result = 0.0f;
     return result;
+}
+__device__ __forceinline__ float bump_shadowing(f3 smooth, f3 cn, f3 dir, bool is_evaluation, bool diffuse,
+                                                bool bump_correction) {
+    if (cn.x == smooth.x && cn.y == smooth.y && cn.z == smooth.z) return 1.0f;
+    return bump_shadowing_general(smooth, cn, dir, is_evaluation, diffuse, bump_correction);
 }
 
 // microfacet_distribution / microfacet_lambda (graph_surface_scattering.cpp:508-547).
@@ -791,10 +807,12 @@ __device__ __noinline__ f3 oren_nayar_intensity(const PhysicalClosure &c, float 
 // unless the closure produced it) is its own.  Out of line: the shading
 // kernel calls it for the light sample and for the BSDF sample, and a
 // single copy keeps the kernel's code within the instruction cache.
+template <bool kGlossy>
 __device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, const ClosurePoint &pt,
                                                     f3 outgoing_raw, uint32_t lobe_mask, int selected) {
     const f3 outgoing = safe_normalize(outgoing_raw, pt.shading_normal);
-    const f3 incoming = safe_normalize(pt.incoming, -outgoing);
+    // make_surface_closure_evaluation_directions (surface_closure_evaluation.cpp:61-70)
+    const f3 incoming = pt.view;
     Evaluation e{mk3(0.0f), 0.0f, 0u};
     float total = 0.0f, weighted_pdf = 0.0f;
     const bool diffuse_enabled = (lobe_mask & kEventDiffuse) != 0u;
@@ -802,7 +820,8 @@ __device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, co
     const bool transparent_enabled = (lobe_mask & kEventTransparent) != 0u;
     const f3 n = s.normal;
     const float nl = maxf_(dot(n, outgoing), 0.0f);
-    const float bump = bump_shadowing(pt.shading_normal, n, outgoing, true, true, pt.bump_correction);
+    const float bump =
+        s.normal_exact ? 1.0f : bump_shadowing_general(pt.shading_normal, n, outgoing, true, true, pt.bump_correction);
     const float lambert = nl * kInvPi;
     for (uint32_t i = 0; i < s.count; ++i) {
         const PhysicalClosure &c = s.c[i];
@@ -810,7 +829,7 @@ __device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, co
             if (transparent_enabled) total += c.sample_weight;
             continue;
         }
-        if (is_glossy(c.op)) {
+        if (kGlossy && is_glossy(c.op)) {
             if (!glossy_enabled) continue;
             const bool is_selected = int(i) == selected;
             const float gb = bump_shadowing(pt.shading_normal, c.color, outgoing, !is_selected, false,
@@ -859,7 +878,7 @@ struct GlossySample {
 };
 __device__ __noinline__ GlossySample sample_glossy(uint32_t op, float roughness, f3 cn, const ClosurePoint &pt,
                                                    f2 u_dir) {
-    const f3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
+    const f3 incoming = pt.view;
     const f3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, cn);
     const float alpha = microfacet_alpha(roughness);
     const float sampling_alpha = maxf_(alpha, 1.0e-10f);
@@ -886,6 +905,7 @@ __device__ __forceinline__ bool closure_eligible(uint32_t op, uint32_t lobe_mask
 // selection :97-214, categorical inversion :420-437, conditional sample
 // :216-337 with the glossy sample_microfacet_reflection of
 // graph_surface_scattering.cpp:730-770, finish :490-660).
+template <bool kGlossy>
 __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s, const ClosurePoint &pt, float u_lobe,
                                                         f2 u_dir, uint32_t lobe_mask) {
     SurfaceSample out;
@@ -912,7 +932,7 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
     if (chosen < 0) return out;
     const PhysicalClosure c = s.c[chosen];
     const bool transparent = c.op == PSY_CLOSURE_TRANSPARENT;
-    const bool glossy = is_glossy(c.op);
+    const bool glossy = kGlossy && is_glossy(c.op);
     bool candidate_valid = true, singular = false;
     f3 direction;
     if (transparent) {
@@ -928,7 +948,7 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
     out.closure_index = uint32_t(chosen);
     out.wi = direction;
     if (!(candidate_valid && (transparent || dot(pt.geometric_normal, direction) > 0.0f))) return out;
-    const Evaluation mixture = evaluate_mixture(s, pt, direction, lobe_mask, chosen);
+    const Evaluation mixture = evaluate_mixture<kGlossy>(s, pt, direction, lobe_mask, chosen);
     Evaluation r;
     r.f = mixture.f;
     float delta = 0.0f;
@@ -950,6 +970,7 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
 // AOV visitor (src/luisa/surface_closure_operations.cpp:40-161, 402-462):
 // diffuse colour into Albedo, every diffuse and glossy normal (glossy:
 // corrected) weighted by |average weight| into Normal.
+template <bool kGlossy>
 __device__ __forceinline__ void surface_aov(const SurfaceClosures &s, const ClosurePoint &pt, f3 &albedo, f3 &normal,
                                             f3 &transparency) {
     albedo = mk3(0.0f);
@@ -963,10 +984,9 @@ __device__ __forceinline__ void surface_aov(const SurfaceClosures &s, const Clos
             const float w = closure_sample_weight(c.weight);
             n = n + s.normal * w;
             total += w;
-        } else if (is_glossy(c.op)) {
-            const f3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
+        } else if (kGlossy && is_glossy(c.op)) {
             const float w = closure_sample_weight(c.weight);
-            n = n + specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.color) * w;
+            n = n + specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, c.color) * w;
             total += w;
         } else {
             transparency = transparency + c.weight;

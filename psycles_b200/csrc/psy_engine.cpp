@@ -34,8 +34,9 @@ uint32_t plan_wavefront(std::vector<PlanJob> &jobs, uint32_t start, uint32_t cap
     return used;
 }
 
-void EnginePlan::add(const std::vector<BatchItem> &wave, uint32_t paths, uint32_t film_pixels, uint32_t max_jobs) {
-    rounds.insert(rounds.end(), {paths, film_pixels, uint32_t(wave.size()), 0u});
+void EnginePlan::add(const std::vector<BatchItem> &wave, uint32_t paths, uint32_t film_pixels, uint32_t max_jobs,
+                     bool glossy) {
+    rounds.insert(rounds.end(), {paths, film_pixels, uint32_t(wave.size()), glossy ? 1u : 0u});
     const size_t base = items.size();
     items.resize(base + max_jobs, BatchItem{});
     std::copy(wave.begin(), wave.end(), items.begin() + base);

@@ -35,12 +35,15 @@ uint32_t plan_wavefront(std::vector<PlanJob> &jobs, uint32_t start, uint32_t cap
                         std::vector<BatchItem> &items, uint32_t &film_pixels);
 
 struct EnginePlan {
-    std::vector<uint32_t> rounds;    // 4 words per wavefront: paths, film pixels, items, 0
+    std::vector<uint32_t> rounds;    // 4 words per wavefront: paths, film pixels, items, glossy
     std::vector<BatchItem> items;    // max_jobs records per wavefront
     uint64_t samples = 0;
     uint32_t waves() const { return uint32_t(rounds.size() / 4u); }
-    // Appends one planned wavefront (padded to `max_jobs` records).
-    void add(const std::vector<BatchItem> &wave, uint32_t paths, uint32_t film_pixels, uint32_t max_jobs);
+    // Appends one planned wavefront (padded to `max_jobs` records);
+    // `glossy`: one of its jobs' scenes holds glossy closures, so the
+    // wavefront shades with the glossy-capable kernel.
+    void add(const std::vector<BatchItem> &wave, uint32_t paths, uint32_t film_pixels, uint32_t max_jobs,
+             bool glossy);
 };
 
 struct EngineRun {

@@ -1795,7 +1795,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     // ---- materials and parameter blocks
     std::vector<psy_closure_instruction> code;
     std::vector<psy_value_instruction> values;
-    bool any_transparent = false;
+    bool any_transparent = false, any_glossy = false;
     for (uint32_t i = 0; i < d->material_count; ++i) {
         const psy_material_desc &m = d->materials[i];
         psy::MaterialGpu g{};
@@ -1814,6 +1814,8 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
             if (m.closures[k].op == PSY_CLOSURE_TRANSPARENT) g.has_transparent = 1u;
         }
         any_transparent = any_transparent || g.has_transparent;
+        for (uint32_t k = 0; k < m.closure_count; ++k)
+            if (m.closures[k].op == PSY_CLOSURE_GLOSSY) any_glossy = true;
         code.insert(code.end(), m.closures, m.closures + m.closure_count);
         sc->scalars.insert(sc->scalars.end(), m.scalars, m.scalars + m.scalar_count);
         sc->vectors.insert(sc->vectors.end(), m.vectors, m.vectors + 3ull * m.vector_count);
@@ -2057,6 +2059,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     v.background[2] = d->background[2];
     v.world_visibility = d->world_visibility;
     v.any_transparent = any_transparent ? 1u : 0u;
+    v.has_glossy = any_glossy ? 1u : 0u;
     // the light tree is built on first use (ensure_light_tree)
     sc->stats.upload_ms = lap();
     sc->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();

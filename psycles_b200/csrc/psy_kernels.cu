@@ -594,11 +594,14 @@ __global__ void k_sort_count_shadow(const __grid_constant__ PathBuffers b, uint3
 // variant carries no trace code.
 // kMulti: paths of a batched wavefront, each shaded with its job's scene and
 // parameters.
-template <bool kTrace, bool kMulti>
+template <bool kTrace, bool kMulti, bool kGlossy>
 __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
     k_shade(const __grid_constant__ SceneView s_arg, const __grid_constant__ RenderParams p_arg,
             const __grid_constant__ PathBuffers b, uint32_t step, uint32_t trace_path, psy_path_trace *trace,
             const JobGpu *jobs, uint32_t sort_threshold) {
+    // a batched wavefront launches both variants; the one that does not
+    // match the wavefront's glossy flag (set by k_begin_round) returns
+    if (kMulti && (b.counters[kCounterWaveGlossy] != 0u) != kGlossy) return;
     const uint32_t count = b.counters[0];
     const uint32_t *queue = (sort_threshold != 0u && count >= sort_threshold) ? b.queue_sorted : b.queue_in;
     const uint32_t rounds = (count + gridDim.x * blockDim.x - 1u) / (gridDim.x * blockDim.x);
@@ -737,8 +740,8 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                 const SurfacePoint sp = surface_point(s, h, ray.d);
                 const MaterialGpu mat = s.materials[sp.material];
                 SurfaceClosures closures;
-                const ClosurePoint cpt{sp.n, sp.ng, -ray.d, mat.bump_correction != 0u};
-                collect_surface(s, mat, cpt, closures);
+                const ClosurePoint cpt{sp.n, sp.ng, -ray.d, safe_normalize(-ray.d, sp.n), mat.bump_correction != 0u};
+                collect_surface<kGlossy>(s, mat, cpt, closures);
                 // SurfaceShadingStageImpl::emit (src/luisa/path_kernel_surface_shading.cpp:117-250)
                 float emission_weight = 1.0f;
                 if (p.nee && s.triangle_emitters > 0u && mat.emission_sampling != 0u && mat.has_emission) {
@@ -783,7 +786,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                 if (alive) {
                     if (depth == 0u) {
                         f3 aov_albedo, aov_normal, aov_transparency;
-                        surface_aov(closures, cpt, aov_albedo, aov_normal, aov_transparency);
+                        surface_aov<kGlossy>(closures, cpt, aov_albedo, aov_normal, aov_transparency);
                         const float4 a4 = b.aov_a[i];
                         const f3 acc = mk3(a4.x, a4.y, a4.z) + throughput * aov_albedo;
                         b.aov_a[i] = make_float4(acc.x, acc.y, acc.z, 0.0f);
@@ -871,7 +874,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                             }
                         }
                         if (sampled) {
-                            const Evaluation e = evaluate_mixture(closures, cpt, ldir, lobe_mask, -1);
+                            const Evaluation e = evaluate_mixture<kGlossy>(closures, cpt, ldir, lobe_mask, -1);
                             const float mis = weigh_mis ? nee_light_weight(p.direct_mode, light_pdf, e.pdf) : 1.0f;
                             const f3 weighted = e.f * light_radiance * (mis / pdf_divisor);
                             if (any_nonzero(weighted)) {
@@ -899,7 +902,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                         }
                     }
                     // SurfaceScatterStageImpl::emit (src/luisa/path_kernel_surface_scatter.cpp:136-291)
-                    const SurfaceSample ss = sample_surface(closures, cpt, bs4.z, mk2(bs4.x, bs4.y), lobe_mask);
+                    const SurfaceSample ss = sample_surface<kGlossy>(closures, cpt, bs4.z, mk2(bs4.x, bs4.y), lobe_mask);
                     if (ev) {
                         ev->closure_index = ss.closure_index;
                         ev->bsdf_pdf = ss.eval.pdf;
@@ -1298,6 +1301,7 @@ __global__ void k_begin_round(uint32_t *counters, uint32_t *round, BatchItem *it
         round[0] = plan_rounds[4u * w];
         round[1] = plan_rounds[4u * w + 1u];
         round[2] = n;
+        counters[kCounterWaveGlossy] = plan_rounds[4u * w + 3u];
         counters[0] = round[0];
         counters[1] = counters[2] = counters[3] = counters[4] = 0u;
         *cursor = w + 1u;
@@ -1447,12 +1451,15 @@ void launch_intersect(cudaStream_t st, const LaunchConfig &lc, const SceneView &
 void launch_shade(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                   uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
     if (lc.sort_threshold) launch_sort<false>(st, lc, s, p, b, nullptr, max_work);
-    if (trace)
-        k_shade<true, false><<<shade_grid(max_work, lc), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr,
-                                                                     lc.sort_threshold);
+    const int grid = shade_grid(max_work, lc);
+    if (trace && s.has_glossy)
+        k_shade<true, false, true><<<grid, 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr, lc.sort_threshold);
+    else if (trace)
+        k_shade<true, false, false><<<grid, 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr, lc.sort_threshold);
+    else if (s.has_glossy)
+        k_shade<false, false, true><<<grid, 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr, lc.sort_threshold);
     else
-        k_shade<false, false><<<shade_grid(max_work, lc), 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr,
-                                                                      lc.sort_threshold);
+        k_shade<false, false, false><<<grid, 128, 0, st>>>(s, p, b, step, trace_path, trace, nullptr, lc.sort_threshold);
 }
 void launch_shadow(cudaStream_t st, const LaunchConfig &lc, const SceneView &s, const RenderParams &p, const PathBuffers &b,
                    uint32_t max_work, uint32_t step, uint32_t trace_path, psy_path_trace *trace) {
@@ -1496,8 +1503,11 @@ void launch_intersect_batch(cudaStream_t st, const LaunchConfig &lc, const JobGp
 void launch_shade_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work,
                         uint32_t step) {
     if (lc.sort_threshold) launch_sort<true>(st, lc, SceneView{}, RenderParams{}, b, jobs, max_work);
-    k_shade<false, true><<<shade_grid(max_work, lc), 128, 0, st>>>(SceneView{}, RenderParams{}, b, step, kInvalid,
-                                                                 nullptr, jobs, lc.sort_threshold);
+    const int grid = shade_grid(max_work, lc);
+    k_shade<false, true, false><<<grid, 128, 0, st>>>(SceneView{}, RenderParams{}, b, step, kInvalid, nullptr, jobs,
+                                                      lc.sort_threshold);
+    k_shade<false, true, true><<<grid, 128, 0, st>>>(SceneView{}, RenderParams{}, b, step, kInvalid, nullptr, jobs,
+                                                     lc.sort_threshold);
 }
 void launch_shadow_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jobs, const PathBuffers &b, uint32_t max_work,
                          uint32_t step) {

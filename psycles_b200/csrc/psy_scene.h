@@ -185,6 +185,7 @@ struct SceneView {
     float background[3];
     uint32_t world_visibility;
     uint32_t any_transparent;
+    uint32_t has_glossy;  // a material holds a glossy closure (selects the shading variant)
     // many-light tree (empty when the scene has no emitter with energy)
     const LtNodeGpu *lt_nodes;
     const LtEmitterGpu *lt_emitters;
@@ -250,7 +251,8 @@ struct PathBuffers {
     uint32_t *queue_in;
     uint32_t *queue_out;
     uint32_t *shadow_queue;
-    uint32_t *counters;  // [0] in count, [1] out count, [2] shadow count, [3..] stats
+    uint32_t *counters;  // [0] in count, [1] out count, [2] shadow count, [3..4] fetch cursors,
+                         // [kCounterWaveGlossy] a batched wavefront's glossy flag
     uint32_t *job;       // batched wavefronts: the job of each path
     // shading-queue sort by material: per-queue-entry bucket, the sorted
     // queue, and kSortBuckets-word histogram / offset arrays
@@ -258,6 +260,7 @@ struct PathBuffers {
 };
 
 constexpr uint32_t kSortBuckets = 2048u;
+constexpr uint32_t kCounterWaveGlossy = 8u;
 
 // One job of a batched wavefront: a session's render parameters, its scene
 // and its film.  Paths of many jobs share the path state; each path reads

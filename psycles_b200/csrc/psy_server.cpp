@@ -274,7 +274,9 @@ struct psy_server {
                 // oldest job first, the others backfill the capacity it leaves
                 const uint32_t paths = plan_wavefront(plan, 0u, engine.capacity(), items, film);
                 EnginePlan ep;
-                ep.add(items, paths, film, engine.max_jobs());
+                bool glossy = false;
+                for (const Job *j : planned) glossy = glossy || j->scene->view.has_glossy != 0u;
+                ep.add(items, paths, film, engine.max_jobs(), glossy);
                 EngineRun run;
                 psy_status r = cudaEventRecord(slot.begin, engine.stream()) == cudaSuccess ? PSY_OK : PSY_ERROR_CUDA;
                 if (r == PSY_OK) r = engine.run(ep, steps, run);
