@@ -74,18 +74,21 @@ def test_glossy_traces_bit_exact(backend, seed):
 
 
 def test_glossy_batched_equals_alone(backend):
-    """Glossy sessions in a shared wavefront end as they do alone."""
+    """Glossy sessions in a shared wavefront end as they do alone, also when
+    the wavefront mixes them with a scene without glossy closures (the
+    wavefront then shades with the glossy-capable kernel variant)."""
     from psycles_b200.backend import BatchRenderer
-    scene = scenes.glossy_scene(seed=3)
-    comp = backend.compile_scene(scene).scene
-    settings = [scenes.render_settings(64, 48, max_bounces=5, seed=k) for k in range(3)]
+    comp = backend.compile_scene(scenes.glossy_scene(seed=3)).scene
+    plain = backend.compile_scene(scenes.small_test_scene(seed=4)).scene
+    work = [(comp, scenes.render_settings(64, 48, max_bounces=5, seed=k)) for k in range(3)]
+    work.append((plain, scenes.render_settings(64, 48, max_bounces=5, seed=9)))
     alone = []
-    for st in settings:
-        s = backend.create_session(comp, st)
+    for sc, st in work:
+        s = backend.create_session(sc, st)
         assert s.render_samples(SampleRange(0, 4, 0, 4))
         alone.append(s.read_pass(_abi.PASS_COMBINED))
     batch = BatchRenderer(backend.context, path_capacity=20000)
-    sessions = [backend.create_session(comp, st) for st in settings]
+    sessions = [backend.create_session(sc, st) for sc, st in work]
     assert batch.render([(s, SampleRange(0, 4, 0, 4)) for s in sessions])
     for s, ref in zip(sessions, alone):
         assert np.array_equal(s.read_pass(_abi.PASS_COMBINED).view(np.uint32), ref.view(np.uint32))
