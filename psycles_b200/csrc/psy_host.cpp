@@ -1081,6 +1081,30 @@ psy_status validate_material(const psy_material_desc &m) {
         if (c.op == PSY_CLOSURE_GLOSSY && c.a != PSY_GLOSSY_GGX && c.a != PSY_GLOSSY_BECKMANN)
             return fail(PSY_ERROR_UNSUPPORTED, "glossy distribution outside GGX and Beckmann");
     }
+    // The device walks the tree with a 32-entry stack and keeps at most 16
+    // BSDF closures per shading point (the reference's capacity is Cycles'
+    // MAX_CLOSURE, 64): a material that would overflow either is refused
+    // rather than rendered with closures dropped.  The walk is replayed here.
+    uint32_t stack[32];
+    uint32_t sp = 0u, leaves = 0u, visits = 0u;
+    bool transparent = false;
+    stack[sp++] = m.root;
+    while (sp > 0u) {
+        const uint32_t id = stack[--sp];
+        if (++visits > 4096u) return fail(PSY_ERROR_UNSUPPORTED, "closure tree too large");
+        const psy_closure_instruction &c = m.closures[id];
+        if (c.op == PSY_CLOSURE_ADD || c.op == PSY_CLOSURE_MIX) {
+            if (sp + 2u > 32u) return fail(PSY_ERROR_UNSUPPORTED, "closure tree deeper than the device walk's stack");
+            stack[sp++] = c.b;
+            stack[sp++] = c.a;
+        } else if (c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_GLOSSY) {
+            ++leaves;
+        } else if (c.op == PSY_CLOSURE_TRANSPARENT) {
+            transparent = true;  // every transparent closure merges into one
+        }
+    }
+    if (leaves + (transparent ? 1u : 0u) > 16u)
+        return fail(PSY_ERROR_UNSUPPORTED, "more than 16 BSDF closures in one material");
     return PSY_OK;
 }
 

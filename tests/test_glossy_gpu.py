@@ -108,3 +108,29 @@ def test_malformed_glossy_is_rejected(backend):
         m.parameters.scalars = np.array([0.3], np.float32)
         m.parameters.vectors = np.array([[0.5, 0.5, 0.5]], np.float32)
         assert not backend.compile_scene(sc).ok(), closure
+
+
+def test_oversized_closure_trees_are_refused(backend):
+    """A material with more BSDF closures than a shading point holds (16)
+    is refused at compile instead of rendering with closures dropped; 16
+    compile."""
+    N = _abi.INPUT_NONE
+
+    def scene_with(leaves):
+        closures = [(_abi.CLOSURE_DIFFUSE, 0, 0, 0, N, N)] * leaves
+        k = leaves
+        prev = 0
+        for i in range(1, leaves):
+            closures.append((_abi.CLOSURE_ADD, prev, i, N, N, N))
+            prev = k
+            k += 1
+        sc = scenes.cornell_box()
+        m = sc.materials[0]
+        m.program.closures = np.array(closures, np.uint32).reshape(-1, 6)
+        m.program.values = np.zeros((0, 8), np.uint32)
+        m.program.root = len(closures) - 1
+        m.parameters.scalars = np.array([0.3], np.float32)
+        m.parameters.vectors = np.array([[0.5, 0.5, 0.5]], np.float32)
+        return sc
+    assert backend.compile_scene(scene_with(16)).ok()
+    assert not backend.compile_scene(scene_with(17)).ok()
