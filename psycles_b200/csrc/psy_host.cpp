@@ -60,6 +60,7 @@ psy_status PathArena::ensure(uint32_t n, bool with_job) {
     // the kernels move record sectors with 32-byte accesses
     if (reinterpret_cast<uintptr_t>(records.ptr) % psy::kPathRecordBytes != 0u)
         return fail(PSY_ERROR_CUDA, "path records are not 128-byte aligned");
+    PSY_CUDA_TRY(rad_final.alloc(f4));
     PSY_CUDA_TRY(sample.alloc(u1));
     PSY_CUDA_TRY(aov_n.alloc(f4));
     PSY_CUDA_TRY(aov_a.alloc(f4));
@@ -84,6 +85,7 @@ psy_status PathArena::ensure(uint32_t n, bool with_job) {
     capacity = c;
     PathBuffers &b = view;
     bind_records(b, records.as<unsigned char>());
+    b.rad_final = rad_final.as<float4>();
     b.sample = sample.as<uint32_t>();
     b.aov_n = aov_n.as<float4>();
     b.aov_a = aov_a.as<float4>();
@@ -2469,6 +2471,7 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
     const size_t n = psy::kStaticMaxPaths;
     psy::PathBuffers b{};
     psy::host::bind_records(b, carve(psy::kPathRecordBytes * n));
+    b.rad_final = reinterpret_cast<float4 *>(carve(16 * n));
     b.sample = reinterpret_cast<uint32_t *>(carve(4 * n));
     b.aov_n = reinterpret_cast<float4 *>(carve(16 * n));
     b.aov_a = reinterpret_cast<float4 *>(carve(16 * n));
@@ -2482,6 +2485,8 @@ psy_status psy_session_render_samples_static(psy_session *s, uint32_t first, uin
     b.queue_out = reinterpret_cast<uint32_t *>(carve(4 * n));
     b.shadow_queue = reinterpret_cast<uint32_t *>(carve(4 * n));
     b.counters = reinterpret_cast<uint32_t *>(carve(64));
+    if (cursor > static_cast<unsigned char *>(base) + psy::kStaticPathBytes)
+        return fail(PSY_ERROR_STATE, "static path state larger than its array");
     unsigned long long *ray_stats = reinterpret_cast<unsigned long long *>(reinterpret_cast<unsigned char *>(b.counters) + 64);
     // the ray counters accumulate: clear them; every other array is written
     // before it is read within the call

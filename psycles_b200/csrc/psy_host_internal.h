@@ -106,7 +106,8 @@ struct DeviceBuffer {
 // for batched wavefronts.
 struct PathArena {
     uint32_t capacity = 0;
-    DeviceBuffer records, sample, aov_n, aov_a, mis_n, sh_o, sh_d, sh_c, sh_ids, sh_path, qa, qb, sq, job, sort_keys,
+    DeviceBuffer records, rad_final, sample, aov_n, aov_a, mis_n, sh_o, sh_d, sh_c, sh_ids, sh_path, qa, qb, sq, job,
+        sort_keys,
         queue_sorted, sort_hist, counters, stats;
     PathBuffers view{};
     psy_status ensure(uint32_t n, bool with_job);

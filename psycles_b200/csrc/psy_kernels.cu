@@ -612,6 +612,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
         const bool active = q < count;
         bool keep = false;
         bool shadow = false;
+        bool final = false;  // the path ends here (its radiance and shadow contribution go to rad_final)
         uint32_t i = 0u;
         float4 sh_o, sh_d, sh_c;
         uint4 sh_ids;
@@ -953,7 +954,11 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                 }
             }
             const float4 rad_out = make_float4(radiance.x, radiance.y, radiance.z, transparency);
-            if (!keep) b.rad[i] = rad_out;
+            // an ended path's radiance goes to the film's array; a path still
+            // alive after the last step (none, by the step bound) is written
+            // there as well
+            final = !keep || step + 1u >= p.steps;
+            if (final) b.rad_final[i] = rad_out;
             if (keep) {
                 store_pair(b.ray_o, i, make_float4(ray.o.x, ray.o.y, ray.o.z, ray.tmin),
                            make_float4(ray.d.x, ray.d.y, ray.d.z, ray.tmax));
@@ -978,7 +983,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
             b.sh_d[sslot] = sh_d;
             b.sh_c[sslot] = sh_c;
             b.sh_ids[sslot] = sh_ids;
-            b.sh_path[sslot] = i;
+            b.sh_path[sslot] = i | (final ? kShadowFinal : 0u);
         }
     }
 }
@@ -1114,7 +1119,7 @@ __global__ void __launch_bounds__(128, PSY_SHADOW_MIN_BLOCKS)
     for (;;) {
         uint32_t q = warp_fetch(&b.counters[4], count, !active, exhausted);
         if (sorted && q != kInvalid) q = b.queue_sorted[q];
-        if (kMulti && q != kInvalid) job = b.job[b.sh_path[q]];
+        if (kMulti && q != kInvalid) job = b.job[b.sh_path[q] & ~kShadowFinal];
         const SceneView &s = kMulti ? jobs[job].s : s_arg;
         const RenderParams &p = kMulti ? jobs[job].p : p_arg;
         if (q != kInvalid) {
@@ -1200,15 +1205,17 @@ __global__ void __launch_bounds__(128, PSY_SHADOW_MIN_BLOCKS)
                 }
             }
         }
-        const uint32_t path = b.sh_path[q_cur];
+        const uint32_t owner = b.sh_path[q_cur];
+        const uint32_t path = owner & ~kShadowFinal;
         f3 contribution = mk3(0.0f);
         if (transmittance.x > 0.0f || transmittance.y > 0.0f || transmittance.z > 0.0f) {
             contribution = clamp_contribution(mk3(c.x, c.y, c.z) * transmittance, depth, p);
-            float4 r = b.rad[path];
+            float4 &dst = (owner & kShadowFinal) != 0u ? b.rad_final[path] : b.rad[path];
+            float4 r = dst;
             r.x += contribution.x;
             r.y += contribution.y;
             r.z += contribution.z;
-            b.rad[path] = r;
+            dst = r;
         }
         if (trace && path == trace_path && step < PSY_TRACE_MAX_EVENTS) set3(trace->events[step].nee, contribution);
     }
@@ -1251,7 +1258,7 @@ __device__ __forceinline__ void film_pixel(const PathBuffers &b, uint32_t px, ui
 #pragma unroll
         for (uint32_t u = 0; u < kGroup; ++u) {
             const uint32_t i = path_begin + (k + u) * pixels + px;
-            r[u] = b.rad[i];
+            r[u] = b.rad_final[i];
             nn[u] = b.aov_n[i];
             aa[u] = b.aov_a[i];
         }
@@ -1260,7 +1267,7 @@ __device__ __forceinline__ void film_pixel(const PathBuffers &b, uint32_t px, ui
     }
     for (; k < samples; ++k) {
         const uint32_t i = path_begin + k * pixels + px;
-        add(i, b.rad[i], b.aov_n[i], b.aov_a[i]);
+        add(i, b.rad_final[i], b.aov_n[i], b.aov_a[i]);
     }
     combined[px] = c;
     normal[px] = n;

@@ -243,6 +243,8 @@ struct PathBuffers {
     float4 *mis_n;              // shading normal of the last non-transparent scatter (light-tree MIS)
     PathField<float4> hit;      // t, u, v, instance bits
     PathField<uint4> hit_prim;  // x: primitive (kInvalid on a miss); y, z, w: 0
+    float4 *rad_final;          // radiance and transparency of an ended path (the film reads these
+                                // coalesced instead of a 16-byte field of each 128-byte record)
     float4 *sh_o;     // shadow origin, tmax
     float4 *sh_d;     // shadow direction, transparent depth bits
     float4 *sh_c;     // unshadowed contribution
@@ -261,6 +263,8 @@ struct PathBuffers {
 
 constexpr uint32_t kSortBuckets = 2048u;
 constexpr uint32_t kCounterWaveGlossy = 8u;
+// sh_path top bit: the shadow ray's path has ended, its contribution goes to rad_final
+constexpr uint32_t kShadowFinal = 0x80000000u;
 
 // One job of a batched wavefront: a session's render parameters, its scene
 // and its film.  Paths of many jobs share the path state; each path reads
