@@ -93,13 +93,17 @@ typedef enum psy_closure_op {
     PSY_CLOSURE_TRANSPARENT = 3,
     PSY_CLOSURE_ADD = 4,
     PSY_CLOSURE_MIX = 5,
-    PSY_CLOSURE_GLOSSY = 6
+    PSY_CLOSURE_GLOSSY = 6,
+    PSY_CLOSURE_GLASS = 7,
+    PSY_CLOSURE_REFRACTION = 8
 } psy_closure_op;
 
-/* Microfacet distribution of a glossy closure (`a` of its instruction):
- * the Glossy BSDF node's Distribution property (GGX, the default, or
- * BECKMANN; MULTI_GGX's tabulated energy preservation is not in the
- * subset and a scene that uses it is rejected). */
+/* Microfacet distribution of a glossy, glass or refraction closure (`a` of
+ * its instruction): the node's Distribution property (GGX, the default, or
+ * BECKMANN; MULTI_GGX's tabulated energy preservation is not in the subset
+ * and a scene that uses it is rejected).  A glass closure must be the only
+ * BSDF closure of its material: its selection weight among other closures
+ * comes from Cycles' tabulated Fresnel albedo, which is not in the subset. */
 #define PSY_GLOSSY_GGX 0u
 #define PSY_GLOSSY_BECKMANN 1u
 
@@ -116,11 +120,12 @@ typedef enum psy_closure_op {
 /* One closure instruction (compiler::ClosureInstruction,
  * include/psycles/compiler/surface_program.h:415-470, in-scope fields):
  * `color` (vector input: diffuse / glossy / transparent / emission
- * colour), `scalar` (emission strength, mix factor), `roughness` (diffuse
- * roughness: Lambert below 1e-5, else Oren-Nayar; glossy roughness, whose
+ * colour, glass tint, refraction colour), `scalar` (emission strength, mix
+ * factor, glass / refraction IOR), `roughness` (diffuse roughness: Lambert
+ * below 1e-5, else Oren-Nayar; glossy, glass and refraction roughness, whose
  * square is the microfacet alpha), `a`/`b` child instruction indices of add
- * and mix, and for glossy `a` = PSY_GLOSSY_*.  Every closure's Normal input
- * is the shading normal (the socket unlinked). */
+ * and mix, and for glossy, glass and refraction `a` = PSY_GLOSSY_*.  Every
+ * closure's Normal input is the shading normal (the socket unlinked). */
 typedef struct psy_closure_instruction {
     uint32_t op;
     uint32_t a;

@@ -270,12 +270,16 @@ static float input_scalar(const Material &mat, uint32_t ref) {
 // roughness; a glossy op carries kBeckmann for the Beckmann distribution.
 constexpr uint32_t kBeckmann = 0x100u;
 inline bool is_glossy(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_GLOSSY; }
+inline bool is_glass(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_GLASS; }
+inline bool is_refraction(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_REFRACTION; }
+inline bool is_dielectric(uint32_t op) { return is_glass(op) || is_refraction(op); }
 
 struct TracedClosure {
     uint32_t op;
     float3 weight;
     float3 color;
     float roughness;
+    float ior{1.0f};
 };
 
 static void walk_closures(const Material &mat, uint32_t id, float mix_weight, std::vector<TracedClosure> &out,
@@ -307,8 +311,21 @@ static void walk_closures(const Material &mat, uint32_t id, float mix_weight, st
     }
     case PSY_CLOSURE_GLOSSY: {
         const float3 color = input_vector(mat, c.color);
-        const uint32_t op = c.a == PSY_GLOSSY_BECKMANN ? (uint32_t(PSY_CLOSURE_GLOSSY) | kBeckmann) : uint32_t(PSY_CLOSURE_GLOSSY);
+        const uint32_t op =
+            c.a == PSY_GLOSSY_BECKMANN ? (uint32_t(PSY_CLOSURE_GLOSSY) | kBeckmann) : uint32_t(PSY_CLOSURE_GLOSSY);
         out.push_back({op, color * mix_weight, color, input_scalar(mat, c.roughness)});
+        return;
+    }
+    case PSY_CLOSURE_GLASS:
+    case PSY_CLOSURE_REFRACTION: {
+        // graph_surface_closures.cpp:290-320: Glass is allocated with the mix
+        // weight and takes Color as its Fresnel tint; Refraction's weight is
+        // Color x mix weight
+        const float3 color = max3(input_vector(mat, c.color), f3(0.0f));
+        const bool glass = c.op == PSY_CLOSURE_GLASS;
+        const uint32_t op = uint32_t(c.op) | (c.a == PSY_GLOSSY_BECKMANN ? kBeckmann : 0u);
+        out.push_back({op, glass ? f3(mix_weight) : color * mix_weight, color, input_scalar(mat, c.roughness),
+                       maxf(input_scalar(mat, c.scalar), 1.0e-5f)});
         return;
     }
     default:
@@ -330,12 +347,15 @@ constexpr uint32_t kMaxClosures = 16u;
 
 // One retained physical closure: Cycles' ShaderClosure after allocation.
 struct PhysicalClosure {
-    uint32_t op;  // DIFFUSE, TRANSPARENT or GLOSSY (| kBeckmann)
+    uint32_t op;  // DIFFUSE, TRANSPARENT, GLOSSY, GLASS or REFRACTION (| kBeckmann)
     float3 weight;
     float sample_weight;
-    float3 normal;    // diffuse: the shading normal; glossy: after setup's specular-reflection correction
-    float3 color;     // authored colour (Oren-Nayar albedo)
-    float roughness;  // diffuse roughness (Lambert below 1e-5); glossy roughness (alpha = roughness^2)
+    float3 normal;    // diffuse: the shading normal; glossy / glass / refraction: after setup's
+                      // specular-reflection correction
+    float3 color;     // authored colour (Oren-Nayar albedo); glass: the Fresnel tint
+    float roughness;  // diffuse roughness (Lambert below 1e-5); microfacet roughness (alpha = roughness^2)
+    float ior{1.0f};  // glass / refraction: the relative IOR (inverted on a back-facing hit)
+    float f0{0.0f};   // glass: F0 of the authored IOR (the Fresnel interpolation's lower end)
 };
 
 struct SurfaceClosures {
@@ -350,6 +370,7 @@ struct ClosurePoint {
     float3 geometric_normal; // SurfacePoint::geometric_normal (facing the incoming ray)
     float3 incoming;         // SurfacePoint::incoming (-ray direction)
     bool bump_correction;    // SurfacePoint::use_bump_map_correction
+    bool back_facing;        // SurfacePoint::back_facing
 };
 
 // ensure_valid_specular_reflection (src/luisa/graph_surface_scattering.cpp:119-155):
@@ -378,6 +399,22 @@ static float3 ensure_valid_specular_reflection(float3 ng, float3 incoming, float
 static float3 specular_normal(bool correction, float3 ng, float3 incoming, float3 n) {
     const bool equal = ng.x == n.x && ng.y == n.y && ng.z == n.z;
     return correction && !equal ? ensure_valid_specular_reflection(ng, incoming, n) : n;
+}
+
+// fresnel_dielectric_cos / f0_from_ior (graph_surface_scattering.cpp:42-58).
+static float fresnel_dielectric_cos(float cosine, float eta) {
+    const float c = std::fabs(cosine);
+    const float g2 = eta * eta - 1.0f + c * c;
+    const float g = std::sqrt(maxf(g2, 0.0f));
+    const float a = (g - c) / maxf(g + c, 1.0e-20f);
+    const float den = c * (g - c) + 1.0f;
+    const float b = (c * (g + c) - 1.0f) / (std::fabs(den) > 1.0e-20f ? den : 1.0e-20f);
+    const float regular = 0.5f * a * a * (1.0f + b * b);
+    return g2 > 0.0f ? regular : 1.0f;
+}
+static float f0_from_ior(float ior) {
+    const float r = (ior - 1.0f) / maxf(ior + 1.0f, 1.0e-20f);
+    return r * r;
 }
 
 // Closure allocation (graph_surface_state.cpp:26-48,
@@ -417,6 +454,23 @@ static SurfaceClosures collect_surface(const Material &mat, const ClosurePoint &
             p.weight = allocated;
             p.sample_weight = allocation * closure_sample_weight(f3(1.0f));
             p.normal = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, closure_normal);
+        } else if (is_dielectric(t.op)) {
+            // MicrofacetGlassComponent::setup (microfacet_glass_component.cpp:180-232): the
+            // corrected normal, roughness sqrt(clamp(r^2)), the IOR inverted on a
+            // back face; weight = max(weight, 0) (no energy preservation: darkening
+            // one).  A glass closure's selection weight would scale this by Cycles'
+            // tabulated Fresnel albedo; a glass closure is the only BSDF closure of
+            // its material (compile refuses other mixes), so that factor only
+            // rescales weighted_pdf / total and is taken as one.
+            const float3 allocated = max3(t.weight, f3(0.0f));
+            const float allocation = closure_sample_weight(allocated);
+            if (!(allocation >= 1.0e-5f)) continue;
+            p.weight = allocated;
+            p.sample_weight = allocation * 1.0f * closure_sample_weight(f3(1.0f));
+            p.normal = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, closure_normal);
+            p.roughness = std::sqrt(clampf(t.roughness * t.roughness, 0.0f, 1.0f));
+            p.ior = pt.back_facing ? 1.0f / t.ior : t.ior;
+            p.f0 = clampf(f0_from_ior(t.ior), 0.0f, 1.0f);
         } else {
             const float sw = closure_sample_weight(t.weight);
             if (!(sw >= 1.0e-5f)) continue;
@@ -478,6 +532,8 @@ static uint32_t runtime_flags(const SurfaceClosures &s, bool back_facing) {
         const PhysicalClosure &c = s.c[i];
         if (c.op == PSY_CLOSURE_DIFFUSE) f |= kRuntimeBsdf | kRuntimeBsdfHasEval;
         else if (is_glossy(c.op)) f |= kRuntimeBsdf | (microfacet_singular(c.roughness) ? 0u : kRuntimeBsdfHasEval);
+        else if (is_dielectric(c.op))
+            f |= kRuntimeBsdf | (microfacet_singular(c.roughness) ? 0u : kRuntimeBsdfHasEval) | kRuntimeBsdfHasTransmission;
         else f |= kRuntimeBsdf | kRuntimeTransparent;
     }
     return f;
@@ -564,6 +620,140 @@ static float microfacet_pdf(const PhysicalClosure &c, float3 incoming, float3 ou
     return (ndv > 0.0f && ndl > 0.0f && ndh > 0.0f && vdh > 0.0f && !singular) ? pdf : 0.0f;
 }
 
+struct GlassFresnel {
+    float3 reflection, transmission;
+};
+
+// glass_fresnel / masked_fresnel (microfacet_glass_component.cpp:32-77) of a
+// standalone Glass closure (F0 of its IOR, F90 one, both tints its colour:
+// caustics on) or Refraction closure (no reflection; transmission one unless
+// totally reflected).
+static GlassFresnel glass_fresnel(const PhysicalClosure &c, float cos_hi, bool reflection_allowed,
+                                  bool transmission_allowed) {
+    const float real = fresnel_dielectric_cos(cos_hi, c.ior);
+    GlassFresnel r;
+    if (is_refraction(c.op)) {
+        r.reflection = f3(0.0f);
+        r.transmission = real == 1.0f ? f3(0.0f) : f3(1.0f);
+    } else {
+        const float real_f0 = f0_from_ior(c.ior);
+        const float t = clampf((real - real_f0) / (1.0f - real_f0), 0.0f, 1.0f);
+        const float3 fresnel = f3(lerp(c.f0, 1.0f, t));
+        r.reflection = fresnel * c.color;
+        r.transmission = (f3(1.0f) - fresnel) * c.color;
+    }
+    if (!reflection_allowed) r.reflection = f3(0.0f);
+    if (!transmission_allowed) r.transmission = f3(0.0f);
+    return r;
+}
+
+static float reflection_probability(const GlassFresnel &f) {
+    const float r = closure_sample_weight(f.reflection);
+    const float t = closure_sample_weight(f.transmission);
+    return r / maxf(r + t, 1.0e-20f);
+}
+
+struct GlassGeometry {
+    float3 half;
+    float inverse_half_length, cos_i, cos_o, cos_hi, cos_nh, cos_ho;
+    bool transmission;
+};
+
+// glass_geometry (microfacet_glass_component.cpp:79-109).
+static GlassGeometry glass_geometry(const PhysicalClosure &c, float3 incoming, float3 outgoing, float3 n) {
+    GlassGeometry g;
+    g.cos_o = dot(n, outgoing);
+    g.transmission = g.cos_o < 0.0f;
+    const float3 uh = g.transmission ? -(c.ior * outgoing + incoming) : incoming + outgoing;
+    const float hl = std::sqrt(dot(uh, uh));
+    const bool unit_ior_transmission = g.transmission && c.ior == 1.0f;
+    const bool finite = hl != 0.0f && !unit_ior_transmission;
+    g.inverse_half_length = finite ? 1.0f / hl : 0.0f;
+    g.half = uh * g.inverse_half_length;
+    g.cos_i = dot(n, incoming);
+    g.cos_hi = dot(g.half, incoming);
+    g.cos_nh = dot(n, g.half);
+    g.cos_ho = dot(g.half, outgoing);
+    return g;
+}
+
+// MicrofacetGlassComponent::intensity and ::pdf (microfacet_glass_component.cpp:234-320).
+static float3 glass_intensity(const PhysicalClosure &c, float3 incoming, float3 outgoing, float3 gn) {
+    const bool beckmann = (c.op & kBeckmann) != 0u;
+    const GlassGeometry g = glass_geometry(c, incoming, outgoing, gn);
+    const float setup_alpha = microfacet_alpha(c.roughness);
+    const float alpha = maxf(setup_alpha, 1.0e-7f);
+    const float d = microfacet_distribution(beckmann, g.cos_nh, alpha);
+    const float li = microfacet_lambda(beckmann, g.cos_i, alpha);
+    const float lo = microfacet_lambda(beckmann, g.cos_o, alpha);
+    const GlassFresnel f = glass_fresnel(c, g.cos_hi, true, true);
+    const float3 lobe = g.transmission ? f.transmission : f.reflection;
+    const float jacobian = c.ior * c.ior * g.inverse_half_length * g.inverse_half_length * std::fabs(g.cos_hi * g.cos_ho);
+    const float common = d / g.cos_i * (g.transmission ? jacobian : 0.25f);
+    const float3 value = lobe * common / (1.0f + li + lo) * 1.0f;
+    const bool valid = g.cos_i > 0.0f && setup_alpha * setup_alpha > kMicrofacetSingularAlphaProduct;
+    return valid ? value : f3(0.0f);
+}
+static float glass_pdf(const PhysicalClosure &c, float3 incoming, float3 outgoing, float3 gn, bool reflection_allowed,
+                       bool transmission_allowed) {
+    const bool beckmann = (c.op & kBeckmann) != 0u;
+    const GlassGeometry g = glass_geometry(c, incoming, outgoing, gn);
+    const float setup_alpha = microfacet_alpha(c.roughness);
+    const float alpha = maxf(setup_alpha, 1.0e-7f);
+    const float d = microfacet_distribution(beckmann, g.cos_nh, alpha);
+    const GlassFresnel f = glass_fresnel(c, g.cos_hi, reflection_allowed, transmission_allowed);
+    const float probability = reflection_probability(f);
+    const float lobe_probability = g.transmission ? 1.0f - probability : probability;
+    const float li = microfacet_lambda(beckmann, g.cos_i, alpha);
+    const float jacobian = c.ior * c.ior * g.inverse_half_length * g.inverse_half_length * std::fabs(g.cos_hi * g.cos_ho);
+    const float common = d / g.cos_i * (g.transmission ? jacobian : 0.25f);
+    const float directional = common / (1.0f + li);
+    const float lobe_energy = g.transmission ? closure_sample_weight(f.transmission) : closure_sample_weight(f.reflection);
+    const bool valid = g.cos_i > 0.0f && lobe_energy > 0.0f && setup_alpha * setup_alpha > kMicrofacetSingularAlphaProduct;
+    return valid ? directional * lobe_probability : 0.0f;
+}
+
+struct GlassSample {
+    float3 direction, singular_evaluation;
+    float singular_pdf;
+    bool transmission, singular, valid;
+};
+
+// MicrofacetGlassComponent::sample (microfacet_glass_component.cpp:322-395).
+static GlassSample glass_sample(const PhysicalClosure &c, float3 incoming, float3 gn, float3 ng, float2 random,
+                                float random_lobe, bool reflection_allowed, bool transmission_allowed) {
+    const float alpha = microfacet_alpha(c.roughness);
+    bool singular = alpha * alpha <= kMicrofacetSingularAlphaProduct;
+    const float sampling_alpha = maxf(alpha, 1.0e-7f);
+    const float3 sampled = (c.op & kBeckmann) != 0u ? sample_beckmann_visible_normal(gn, incoming, sampling_alpha, random)
+                                                    : sample_ggx_visible_normal(gn, incoming, sampling_alpha, random);
+    const float3 h = singular ? gn : sampled;
+    const float cos_hi = dot(h, incoming);
+    const GlassFresnel f = glass_fresnel(c, cos_hi, reflection_allowed, transmission_allowed);
+    const float probability = reflection_probability(f);
+    GlassSample r;
+    r.transmission = random_lobe >= probability;
+    const float3 reflected = 2.0f * cos_hi * h - incoming;
+    const float e2 = c.ior * c.ior - (1.0f - cos_hi * cos_hi);
+    const float cos_ho = -std::sqrt(maxf(e2, 0.0f)) / c.ior;
+    const float inverse_eta = 1.0f / c.ior;
+    const float3 transmitted = (inverse_eta * cos_hi + cos_ho) * h - inverse_eta * incoming;
+    r.direction = r.transmission ? transmitted : reflected;
+    const float3 selected = r.transmission ? f.transmission : f.reflection;
+    const float lobe_probability = r.transmission ? 1.0f - probability : probability;
+    const bool shading_negative = dot(gn, r.direction) < 0.0f;
+    const bool geometric_negative = dot(ng, r.direction) < 0.0f;
+    const bool shading_ok = r.transmission ? shading_negative : !shading_negative;
+    const bool geometric_ok = r.transmission ? geometric_negative : !geometric_negative;
+    const bool has_energy = closure_sample_weight(f.reflection + f.transmission) > 0.0f;
+    r.valid = has_energy && cos_hi > 0.0f && shading_ok && geometric_ok;
+    singular = singular || (r.transmission && std::fabs(c.ior - 1.0f) < 1.0e-4f);
+    r.singular = singular;
+    r.singular_evaluation = c.weight * selected * 1.0f * 1.0e6f;
+    r.singular_pdf = lobe_probability * 1.0e6f;
+    return r;
+}
+
 struct Evaluation {
     float3 f{};
     float3 diffuse_f{};
@@ -624,14 +814,40 @@ static Evaluation evaluate_mixture(const SurfaceClosures &s, const ClosurePoint 
     const bool diffuse_enabled = (lobe_mask & kEventDiffuse) != 0u;
     const bool glossy_enabled = (lobe_mask & kEventGlossy) != 0u;
     const bool transparent_enabled = (lobe_mask & kEventTransparent) != 0u;
+    const bool transmission_enabled = (lobe_mask & kEventTransmission) != 0u;
     for (uint32_t i = 0; i < s.count; ++i) {
         const PhysicalClosure &c = s.c[i];
         if (c.op == PSY_CLOSURE_TRANSPARENT) {
             if (transparent_enabled) total += c.sample_weight;
             continue;
         }
-        const bool glossy = is_glossy(c.op);
         const bool is_selected = int(i) == selected;
+        if (is_dielectric(c.op)) {
+            // glass / refraction (surface_closure_evaluation.cpp:134-394): the side of
+            // `outgoing` picks reflection or transmission; a selected transmission
+            // keeps its bump term, and a selected unit-IOR transmission is a delta
+            const float3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.normal);
+            const bool transmission = dot(gn, outgoing) < 0.0f;
+            const bool unit_ior_delta = is_selected && transmission && std::fabs(c.ior - 1.0f) < 1.0e-4f;
+            float bump = bump_shadowing(pt.shading_normal, c.normal, outgoing, !is_selected, false,
+                                        pt.bump_correction);
+            if (is_selected && transmission) bump = 1.0f;
+            const bool pdf_valid = bump != 0.0f || is_selected;
+            const bool allowed = is_glass(c.op) ? (transmission ? transmission_enabled : glossy_enabled)
+                                                : (glossy_enabled && transmission_enabled);
+            if (!allowed) continue;  // any_allowed false: no weight, no pdf
+            float pdf = glass_pdf(c, incoming, outgoing, gn, glossy_enabled, transmission_enabled);
+            if (!pdf_valid || unit_ior_delta) pdf = 0.0f;
+            float3 value = c.weight * glass_intensity(c, incoming, outgoing, gn) * bump;
+            if (unit_ior_delta) value = f3(0.0f);
+            e.f += value;
+            total += c.sample_weight;
+            weighted_pdf += c.sample_weight * pdf;
+            if (closure_sample_weight(value) > 0.0f)
+                e.events |= kEventGlossy | (transmission ? kEventTransmission : kEventReflection);
+            continue;
+        }
+        const bool glossy = is_glossy(c.op);
         const float bump = bump_shadowing(pt.shading_normal, c.normal, outgoing, !is_selected, !glossy,
                                           pt.bump_correction);
         const bool pdf_valid = bump != 0.0f || is_selected;
@@ -679,6 +895,7 @@ static SurfaceSample sample_surface(const SurfaceClosures &s, const ClosurePoint
     const bool diffuse_enabled = (lobe_mask & kEventDiffuse) != 0u;
     const bool glossy_enabled = (lobe_mask & kEventGlossy) != 0u;
     const bool transparent_enabled = (lobe_mask & kEventTransparent) != 0u;
+    const bool transmission_enabled = (lobe_mask & kEventTransmission) != 0u;
     const float3 incoming = safe_normalize(pt.incoming, pt.shading_normal);
     float weights[kMaxClosures];
     float total = 0.0f;
@@ -686,6 +903,8 @@ static SurfaceSample sample_surface(const SurfaceClosures &s, const ClosurePoint
         const uint32_t op = s.c[i].op;
         const bool eligible = op == PSY_CLOSURE_DIFFUSE ? diffuse_enabled
                               : is_glossy(op)           ? glossy_enabled
+                              : is_glass(op)            ? (glossy_enabled || transmission_enabled)
+                              : is_refraction(op)       ? (glossy_enabled && transmission_enabled)
                                                         : transparent_enabled;
         weights[i] = eligible ? s.c[i].sample_weight : 0.0f;
         total += weights[i];
@@ -694,9 +913,15 @@ static SurfaceSample sample_surface(const SurfaceClosures &s, const ClosurePoint
     const float target = random_lobe * total;
     float accumulated = 0.0f;
     int chosen = -1;
+    float rescaled = random_lobe;
     for (uint32_t i = 0; i < s.count; ++i) {
         const float next = accumulated + weights[i];
-        if (chosen < 0 && weights[i] > 0.0f && target < next) chosen = int(i);
+        if (chosen < 0 && weights[i] > 0.0f && target < next) {
+            chosen = int(i);
+            // SurfaceClosureCategoricalInversion::consider (:420-437): the lobe
+            // number rescaled into the chosen closure's interval
+            if (s.count > 1u) rescaled = (target - accumulated) / maxf(weights[i], 1.0e-20f);
+        }
         accumulated = next;
     }
     if (chosen < 0) return out;
@@ -704,9 +929,18 @@ static SurfaceSample sample_surface(const SurfaceClosures &s, const ClosurePoint
     float3 direction;
     const bool transparent = c.op == PSY_CLOSURE_TRANSPARENT;
     const bool glossy = is_glossy(c.op);
-    bool candidate_valid = true, singular = false;
+    const bool dielectric = is_dielectric(c.op);
+    bool candidate_valid = true, singular = false, transmission = false;
+    GlassSample gs{};
     if (transparent) {
         direction = pt.incoming * -1.0f;
+    } else if (dielectric) {
+        const float3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.normal);
+        gs = glass_sample(c, incoming, gn, pt.geometric_normal, u_dir, rescaled, glossy_enabled, transmission_enabled);
+        direction = gs.direction;
+        candidate_valid = gs.valid;
+        singular = gs.singular;
+        transmission = gs.transmission;
     } else if (glossy) {
         const float3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.normal);
         const float alpha = microfacet_alpha(c.roughness);
@@ -720,7 +954,8 @@ static SurfaceSample sample_surface(const SurfaceClosures &s, const ClosurePoint
     } else {
         direction = sample_cosine_hemisphere(c.normal, u_dir).direction;
     }
-    const bool geometric_valid = dot(pt.geometric_normal, direction) > 0.0f;
+    const bool geometric_valid =
+        transmission ? dot(pt.geometric_normal, direction) < 0.0f : dot(pt.geometric_normal, direction) > 0.0f;
     const bool sample_valid = candidate_valid && (transparent || geometric_valid);
     out.closure_index = uint32_t(chosen);
     out.wi = direction;
@@ -738,9 +973,14 @@ static SurfaceSample sample_surface(const SurfaceClosures &s, const ClosurePoint
         // when sampling a glossy closure) x 1e6, singular pdf 1e6
         r.f += c.weight * 1.0e6f;
         delta_pdf_numerator = 1.0e6f * weights[chosen];
+    } else if (dielectric && singular) {
+        r.f += gs.singular_evaluation;
+        delta_pdf_numerator = gs.singular_pdf * weights[chosen];
     }
     r.pdf = mixture.pdf + delta_pdf_numerator / maxf(total, 1.0e-20f);
     if (transparent) r.events = kEventTransmission | kEventTransparent;
+    else if (dielectric)
+        r.events = (singular ? kEventSingular : kEventGlossy) | (transmission ? kEventTransmission : kEventReflection);
     else if (glossy) r.events = singular ? (kEventSingular | kEventReflection) : (kEventGlossy | kEventReflection);
     else r.events = kEventDiffuse | kEventReflection;
     out.eval = r;
@@ -764,9 +1004,9 @@ static Aov surface_aov(const SurfaceClosures &s, const ClosurePoint &pt) {
             const float w = closure_sample_weight(c.weight);
             normal += c.normal * w;
             total += w;
-        } else if (is_glossy(c.op)) {
-            // glossy colour is not in the Albedo pass; its corrected normal
-            // is in the Normal pass
+        } else if (is_glossy(c.op) || is_dielectric(c.op)) {
+            // glossy and glass colour are not in the Albedo pass; their
+            // corrected normal is in the Normal pass
             const float w = closure_sample_weight(c.weight);
             normal += specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.normal) * w;
             total += w;
@@ -2032,7 +2272,7 @@ static PathOutput render_path(const Scene &s, const Settings &st, uint32_t x, ui
         }
         const SurfacePoint sp = surface_point(s, hit, ray);
         const Material &mat = s.materials[sp.material];
-        const ClosurePoint cpt{sp.n, sp.ng, -ray.d, mat.bump_correction};
+        const ClosurePoint cpt{sp.n, sp.ng, -ray.d, mat.bump_correction, sp.back_facing};
         const SurfaceClosures closures = collect_surface(mat, cpt);
         // SurfaceShadingStageImpl::emit (src/luisa/path_kernel_surface_shading.cpp:117-250)
         float emission_weight = 1.0f;

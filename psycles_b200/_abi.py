@@ -23,7 +23,8 @@ STATUS_NAMES = {
     5: "range", 6: "unsupported", 7: "state", 8: "timeout",
 }
 
-CLOSURE_NULL, CLOSURE_DIFFUSE, CLOSURE_EMISSION, CLOSURE_TRANSPARENT, CLOSURE_ADD, CLOSURE_MIX, CLOSURE_GLOSSY = range(7)
+(CLOSURE_NULL, CLOSURE_DIFFUSE, CLOSURE_EMISSION, CLOSURE_TRANSPARENT, CLOSURE_ADD, CLOSURE_MIX, CLOSURE_GLOSSY,
+ CLOSURE_GLASS, CLOSURE_REFRACTION) = range(9)
 GLOSSY_GGX, GLOSSY_BECKMANN = 0, 1
 MATERIAL_NO_BUMP_MAP_CORRECTION = 1
 LIGHT_POINT, LIGHT_SPOT, LIGHT_AREA, LIGHT_DISTANT = range(4)

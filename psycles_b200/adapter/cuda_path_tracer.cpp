@@ -95,6 +95,8 @@ std::uint32_t closure_op(ClosureOperation op) {
     case ClosureOperation::add: return PSY_CLOSURE_ADD;
     case ClosureOperation::mix: return PSY_CLOSURE_MIX;
     case ClosureOperation::glossy: return PSY_CLOSURE_GLOSSY;
+    case ClosureOperation::glass: return PSY_CLOSURE_GLASS;
+    case ClosureOperation::refraction: return PSY_CLOSURE_REFRACTION;
     default: return 0xffffffffu;
     }
 }
@@ -217,6 +219,17 @@ struct Flattener {
                 k.a = c.beckmann ? PSY_GLOSSY_BECKMANN : PSY_GLOSSY_GGX;
                 k.color = input(c.color, c, false);
                 k.roughness = input(c.roughness, c, false);
+                if (!shading_normal(c))
+                    return error(who + "closure normals other than the shading normal are not available in the CUDA path");
+                break;
+            case ClosureOperation::glass:
+            case ClosureOperation::refraction:
+                if (c.preserve_ggx_energy)
+                    return error(who + "the Multiscatter GGX distribution is not available in the CUDA path");
+                k.a = c.beckmann ? PSY_GLOSSY_BECKMANN : PSY_GLOSSY_GGX;
+                k.color = input(c.color, c, false);
+                k.roughness = input(c.roughness, c, false);
+                k.scalar = input(c.ior, c, false);
                 if (!shading_normal(c))
                     return error(who + "closure normals other than the shading normal are not available in the CUDA path");
                 break;
@@ -549,7 +562,7 @@ public:
     [[nodiscard]] std::uint64_t source_revision() const noexcept override { return psy_scene_source_revision(scene); }
     psy_scene *scene;
     std::uint32_t light_count;
-    bool glossy;  // a material holds a glossy closure
+    bool glossy;  // a material holds a glossy, glass or refraction closure
 };
 
 bool supported_pass(contract::PassKind kind) {
@@ -661,7 +674,9 @@ contract::SceneCompilation CudaPathTracerBackend::compile_scene(const contract::
     bool glossy = false;
     for (std::uint32_t i = 0; i < flat.desc().material_count; ++i) {
         const psy_material_desc &m = flat.desc().materials[i];
-        for (std::uint32_t k = 0; k < m.closure_count; ++k) glossy = glossy || m.closures[k].op == PSY_CLOSURE_GLOSSY;
+        for (std::uint32_t k = 0; k < m.closure_count; ++k)
+            glossy = glossy || m.closures[k].op == PSY_CLOSURE_GLOSSY || m.closures[k].op == PSY_CLOSURE_GLASS ||
+                     m.closures[k].op == PSY_CLOSURE_REFRACTION;
     }
     result.scene = std::make_unique<CudaCompiledScene>(scene, flat.desc().light_count, glossy);
     return result;
@@ -680,9 +695,9 @@ std::unique_ptr<contract::RenderSession> CudaPathTracerBackend::create_session(
         return nullptr;
     for (const auto &pass : settings.passes)
         if (!supported_pass(pass.kind)) return nullptr;
-    // glossy closures render with Filter Glossy off and both caustics on
-    // (the contract's defaults): the glossy blur and the caustics lobe masks
-    // are not in the CUDA path
+    // glossy, glass and refraction closures render with Filter Glossy off and
+    // both caustics on (the contract's defaults): the glossy blur and the
+    // caustics lobe masks are not in the CUDA path
     if (compiled.glossy && (settings.integrator.filter_glossy > 0.0f || !settings.integrator.reflective_caustics ||
                             !settings.integrator.refractive_caustics))
         return nullptr;

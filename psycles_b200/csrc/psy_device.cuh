@@ -310,17 +310,25 @@ constexpr uint32_t kMaxClosureStack = 32u;
 // transparent closure never reads one.  A glossy closure's `color` holds
 // its normal after setup's specular-reflection correction (its colour is
 // in its weight), `roughness` its roughness (microfacet alpha = roughness^2),
-// and its op carries kGlossyBeckmann for the Beckmann distribution.
+// and its op carries kGlossyBeckmann for the Beckmann distribution.  A glass
+// closure's `color` is its Fresnel tint (its normal is recomputed where it
+// is used); a refraction closure's `color` holds its normal like a glossy
+// one (its colour is in its weight).
 struct PhysicalClosure {
     f3 weight;
     float sample_weight;
     uint32_t op;
     f3 color;
     float roughness;
+    float ior;  // glass / refraction: relative IOR (inverted on a back face)
+    float f0;   // glass: F0 of the authored IOR
 };
 
 constexpr uint32_t kGlossyBeckmann = 0x100u;
 __device__ __forceinline__ bool is_glossy(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_GLOSSY; }
+__device__ __forceinline__ bool is_glass(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_GLASS; }
+__device__ __forceinline__ bool is_refraction(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_REFRACTION; }
+__device__ __forceinline__ bool is_dielectric(uint32_t op) { return is_glass(op) || is_refraction(op); }
 
 // The surface point's inputs to closure setup, evaluation and sampling.
 // `view` is the normalised incoming direction every closure routine of
@@ -332,6 +340,7 @@ struct ClosurePoint {
     f3 incoming;          // SurfacePoint::incoming (-ray direction)
     f3 view;              // normalize(incoming)
     bool bump_correction; // SurfacePoint::use_bump_map_correction
+    bool back_facing;     // SurfacePoint::back_facing
 };
 
 // Shading routines are instantiated with and without glossy closures
@@ -480,10 +489,13 @@ __device__ __forceinline__ float input_scalar(const SceneView &s, const Material
 constexpr uint32_t kLeafDiffuse = 1u, kLeafTransparent = 2u, kLeafEmission = 4u, kLeafGlossy = 8u, kLeafAll = 15u;
 
 // Visits closure leaves depth-first, `a` before `b`, with the add / mix
-// weight rule; `visit(op, weight, color, roughness)` receives the diffuse /
-// glossy / transparent / emission leaves selected by kLeaves with their
-// authored colour (x strength for emission) and, for diffuse and glossy,
-// the roughness input (a Beckmann glossy leaf's op carries kGlossyBeckmann).
+// weight rule; `visit(op, weight, color, roughness, ior)` receives the
+// diffuse / microfacet / transparent / emission leaves selected by kLeaves
+// with their authored colour (x strength for emission), the roughness input
+// of diffuse and microfacet leaves, and the IOR of glass and refraction (a
+// Beckmann leaf's op carries kGlossyBeckmann).  Glass is allocated with the
+// mix weight and takes its colour as a tint; refraction's weight is colour x
+// mix weight (graph_surface_closures.cpp:290-320).
 // Unselected leaves read no inputs (a shadow ray's extinction needs only
 // the transparent ones).
 template <uint32_t kLeaves = kLeafAll, typename Visit>
@@ -512,23 +524,30 @@ __device__ __forceinline__ void walk_closures(const SceneView &s, const Material
         } else if (c.op == PSY_CLOSURE_DIFFUSE) {
             if constexpr ((kLeaves & kLeafDiffuse) != 0u) {
                 const f3 color = input_vector(s, m, c.color);
-                visit(c.op, color * w, color, input_scalar(s, m, c.roughness));
+                visit(c.op, color * w, color, input_scalar(s, m, c.roughness), 1.0f);
             }
         } else if (c.op == PSY_CLOSURE_TRANSPARENT) {
             if constexpr ((kLeaves & kLeafTransparent) != 0u) {
                 const f3 color = input_vector(s, m, c.color);
-                visit(c.op, color * w, color, 0.0f);
+                visit(c.op, color * w, color, 0.0f, 1.0f);
             }
         } else if (c.op == PSY_CLOSURE_GLOSSY) {
             if constexpr ((kLeaves & kLeafGlossy) != 0u) {
                 const f3 color = input_vector(s, m, c.color);
                 const uint32_t op = c.a == PSY_GLOSSY_BECKMANN ? (uint32_t(PSY_CLOSURE_GLOSSY) | kGlossyBeckmann)
                                                                : uint32_t(PSY_CLOSURE_GLOSSY);
-                visit(op, color * w, color, input_scalar(s, m, c.roughness));
+                visit(op, color * w, color, input_scalar(s, m, c.roughness), 1.0f);
+            }
+        } else if (c.op == PSY_CLOSURE_GLASS || c.op == PSY_CLOSURE_REFRACTION) {
+            if constexpr ((kLeaves & kLeafGlossy) != 0u) {
+                const f3 color = max3(input_vector(s, m, c.color), mk3(0.0f));
+                const uint32_t op = uint32_t(c.op) | (c.a == PSY_GLOSSY_BECKMANN ? kGlossyBeckmann : 0u);
+                visit(op, c.op == PSY_CLOSURE_GLASS ? mk3(w) : color * w, color, input_scalar(s, m, c.roughness),
+                      maxf_(input_scalar(s, m, c.scalar), 1.0e-5f));
             }
         } else if (c.op == PSY_CLOSURE_EMISSION && (kLeaves & kLeafEmission) != 0u) {
             const f3 color = input_vector(s, m, c.color) * input_scalar(s, m, c.scalar);
-            visit(c.op, color * w, color, 0.0f);
+            visit(c.op, color * w, color, 0.0f, 1.0f);
         }
     }
 }
@@ -560,6 +579,22 @@ __device__ __forceinline__ f3 specular_normal(bool correction, f3 ng, f3 incomin
     return correction && !equal ? ensure_valid_specular_reflection(ng, incoming, n) : n;
 }
 
+// fresnel_dielectric_cos / f0_from_ior (graph_surface_scattering.cpp:42-58).
+__device__ __forceinline__ float fresnel_dielectric_cos(float cosine, float eta) {
+    const float c = fabsf(cosine);
+    const float g2 = eta * eta - 1.0f + c * c;
+    const float g = sqrtf(maxf_(g2, 0.0f));
+    const float a = (g - c) / maxf_(g + c, 1.0e-20f);
+    const float den = c * (g - c) + 1.0f;
+    const float b = (c * (g + c) - 1.0f) / (fabsf(den) > 1.0e-20f ? den : 1.0e-20f);
+    const float regular = 0.5f * a * a * (1.0f + b * b);
+    return g2 > 0.0f ? regular : 1.0f;
+}
+__device__ __forceinline__ float f0_from_ior(float ior) {
+    const float r = (ior - 1.0f) / maxf_(ior + 1.0f, 1.0e-20f);
+    return r * r;
+}
+
 // Closure allocation (graph_surface_state.cpp:26-48,
 // graph_surface_physical_closures.cpp:158-520): diffuse goes through
 // bsdf_alloc (negative weight clamped, average cutoff 1e-5); glossy is
@@ -578,7 +613,7 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
     out.normal_exact = out.normal.x == pt.shading_normal.x && out.normal.y == pt.shading_normal.y &&
                        out.normal.z == pt.shading_normal.z;
     int transparent_slot = -1;
-    walk_closures<kLeavesOf(kGlossy)>(s, m, [&](uint32_t op, f3 w, f3 color, float roughness) {
+    walk_closures<kLeavesOf(kGlossy)>(s, m, [&](uint32_t op, f3 w, f3 color, float roughness, float ior) {
         if (op == PSY_CLOSURE_EMISSION) {
             out.emission = out.emission + w;
             return;
@@ -587,6 +622,8 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
         p.op = op;
         p.color = color;
         p.roughness = roughness;
+        p.ior = 1.0f;
+        p.f0 = 0.0f;
         if (op == PSY_CLOSURE_DIFFUSE) {
             p.weight = bsdf_allocated_weight(w);
             p.sample_weight = closure_sample_weight(p.weight);
@@ -598,6 +635,22 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
             p.weight = allocated;
             p.sample_weight = allocation * closure_sample_weight(mk3(1.0f));
             p.color = specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, out.normal);
+        } else if (kGlossy && is_dielectric(op)) {
+            // MicrofacetGlassComponent::setup (microfacet_glass_component.cpp:180-232): the
+            // corrected normal, roughness sqrt(clamp(r^2)), the IOR inverted on a back
+            // face, weight max(weight, 0) (no energy preservation).  A glass closure's
+            // selection weight would also carry Cycles' tabulated Fresnel albedo; it is
+            // the only BSDF closure of its material (compile refuses other mixes), where
+            // that factor only rescales weighted_pdf / total, and is taken as one.
+            const f3 allocated = max3(w, mk3(0.0f));
+            const float allocation = closure_sample_weight(allocated);
+            if (!(allocation >= 1.0e-5f)) return;
+            p.weight = allocated;
+            p.sample_weight = allocation * 1.0f * closure_sample_weight(mk3(1.0f));
+            p.roughness = sqrtf(clampf_(roughness * roughness, 0.0f, 1.0f));
+            p.ior = pt.back_facing ? 1.0f / ior : ior;
+            p.f0 = clampf_(f0_from_ior(ior), 0.0f, 1.0f);
+            if (is_refraction(op)) p.color = specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, out.normal);
         } else {
             const float sw = closure_sample_weight(w);
             if (!(sw >= 1.0e-5f)) return;
@@ -617,7 +670,7 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
 
 __device__ __forceinline__ f3 material_emission(const SceneView &s, const MaterialGpu &m) {
     f3 r = mk3(0.0f);
-    walk_closures<kLeafEmission>(s, m, [&](uint32_t op, f3 w, f3, float) {
+    walk_closures<kLeafEmission>(s, m, [&](uint32_t op, f3 w, f3, float, float) {
         if (op == PSY_CLOSURE_EMISSION) r = r + w;
     });
     return r;
@@ -626,7 +679,7 @@ __device__ __forceinline__ f3 material_emission(const SceneView &s, const Materi
 // transparent_extinction (src/luisa/graph_surface_implementation.cpp:354-372).
 __device__ __forceinline__ f3 transparent_extinction(const SceneView &s, const MaterialGpu &m) {
     f3 r = mk3(0.0f);
-    walk_closures<kLeafTransparent>(s, m, [&](uint32_t op, f3 w, f3, float) {
+    walk_closures<kLeafTransparent>(s, m, [&](uint32_t op, f3 w, f3, float, float) {
         if (op == PSY_CLOSURE_TRANSPARENT && closure_sample_weight(w) >= 1.0e-5f) r = r + w;
     });
     return r;
@@ -670,6 +723,8 @@ __device__ __forceinline__ uint32_t runtime_flags(const SurfaceClosures &s, bool
         const PhysicalClosure &c = s.c[i];
         if (c.op == PSY_CLOSURE_DIFFUSE) f |= kRuntimeBsdf | kRuntimeBsdfHasEval;
         else if (is_glossy(c.op)) f |= kRuntimeBsdf | (microfacet_singular(c.roughness) ? 0u : kRuntimeBsdfHasEval);
+        else if (is_dielectric(c.op))
+            f |= kRuntimeBsdf | (microfacet_singular(c.roughness) ? 0u : kRuntimeBsdfHasEval) | kRuntimeBsdfHasTransmission;
         else f |= kRuntimeBsdf | kRuntimeTransparent;
     }
     return f;
@@ -753,6 +808,127 @@ __device__ __noinline__ Microfacet microfacet_eval(uint32_t op, float roughness,
     return r;
 }
 
+// ---- glass and refraction (src/luisa/microfacet_glass_component.cpp) ----
+
+// The closure normal of a glossy, glass or refraction closure after setup's
+// specular-reflection correction (glass recomputes it: its `color` holds the tint).
+__device__ __forceinline__ f3 microfacet_setup_normal(const PhysicalClosure &c, const SurfaceClosures &s,
+                                                      const ClosurePoint &pt) {
+    return is_glass(c.op) ? specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, s.normal) : c.color;
+}
+
+struct GlassFresnel {
+    f3 reflection, transmission;
+};
+
+// glass_fresnel / masked_fresnel (microfacet_glass_component.cpp:32-77) of a
+// standalone Glass closure (F0 of its IOR, F90 one, both tints its colour:
+// caustics on) or Refraction closure (no reflection; transmission one unless
+// totally reflected).
+__device__ __forceinline__ GlassFresnel glass_fresnel(const PhysicalClosure &c, float cos_hi, bool reflection_allowed,
+                                                      bool transmission_allowed) {
+    const float real = fresnel_dielectric_cos(cos_hi, c.ior);
+    GlassFresnel r;
+    if (is_refraction(c.op)) {
+        r.reflection = mk3(0.0f);
+        r.transmission = real == 1.0f ? mk3(0.0f) : mk3(1.0f);
+    } else {
+        const float real_f0 = f0_from_ior(c.ior);
+        const float t = clampf_((real - real_f0) / (1.0f - real_f0), 0.0f, 1.0f);
+        const f3 fresnel = mk3(lerpf_(c.f0, 1.0f, t));
+        r.reflection = fresnel * c.color;
+        r.transmission = (mk3(1.0f) - fresnel) * c.color;
+    }
+    if (!reflection_allowed) r.reflection = mk3(0.0f);
+    if (!transmission_allowed) r.transmission = mk3(0.0f);
+    return r;
+}
+
+__device__ __forceinline__ float reflection_probability(const GlassFresnel &f) {
+    const float r = closure_sample_weight(f.reflection);
+    const float t = closure_sample_weight(f.transmission);
+    return r / maxf_(r + t, 1.0e-20f);
+}
+
+// MicrofacetGlassComponent::intensity and ::pdf (microfacet_glass_component.cpp:79-109,
+// 234-320): glass_geometry's half vector (the refractive one oriented by the
+// IOR), D, Lambda, the Fresnel lobe of the side `outgoing` lies on, and the
+// refraction Jacobian.
+__device__ __noinline__ Microfacet glass_eval(const PhysicalClosure &c, f3 incoming, f3 outgoing, f3 n,
+                                              bool reflection_allowed, bool transmission_allowed, f3 &value) {
+    const bool beckmann = (c.op & kGlossyBeckmann) != 0u;
+    const float cos_o = dot(n, outgoing);
+    const bool transmission = cos_o < 0.0f;
+    const f3 uh = transmission ? -(outgoing * c.ior + incoming) : incoming + outgoing;
+    const float hl = sqrtf(dot(uh, uh));
+    const bool finite = hl != 0.0f && !(transmission && c.ior == 1.0f);
+    const float inv_hl = finite ? 1.0f / hl : 0.0f;
+    const f3 h = uh * inv_hl;
+    const float cos_i = dot(n, incoming), cos_hi = dot(h, incoming), cos_nh = dot(n, h), cos_ho = dot(h, outgoing);
+    const float setup_alpha = microfacet_alpha(c.roughness);
+    const float alpha = maxf_(setup_alpha, 1.0e-7f);
+    const float d = microfacet_distribution(beckmann, cos_nh, alpha);
+    const float li = microfacet_lambda(beckmann, cos_i, alpha);
+    const float lo = microfacet_lambda(beckmann, cos_o, alpha);
+    const float jacobian = c.ior * c.ior * inv_hl * inv_hl * fabsf(cos_hi * cos_ho);
+    const float common = d / cos_i * (transmission ? jacobian : 0.25f);
+    const bool regular = setup_alpha * setup_alpha > kMicrofacetSingularAlphaProduct;
+    // intensity (unmasked Fresnel)
+    const GlassFresnel full = glass_fresnel(c, cos_hi, true, true);
+    const f3 lobe = transmission ? full.transmission : full.reflection;
+    value = (cos_i > 0.0f && regular) ? lobe * common / (1.0f + li + lo) * 1.0f : mk3(0.0f);
+    // pdf (Fresnel masked by the enabled lobes)
+    const GlassFresnel f = glass_fresnel(c, cos_hi, reflection_allowed, transmission_allowed);
+    const float probability = reflection_probability(f);
+    const float lobe_probability = transmission ? 1.0f - probability : probability;
+    const float lobe_energy = transmission ? closure_sample_weight(f.transmission) : closure_sample_weight(f.reflection);
+    Microfacet m;
+    m.intensity = 0.0f;
+    m.pdf = (cos_i > 0.0f && lobe_energy > 0.0f && regular) ? common / (1.0f + li) * lobe_probability : 0.0f;
+    return m;
+}
+
+struct GlassSample {
+    f3 direction, singular_evaluation;
+    float singular_pdf;
+    bool transmission, singular, valid;
+};
+
+// MicrofacetGlassComponent::sample (microfacet_glass_component.cpp:322-395).
+__device__ __noinline__ GlassSample glass_sample(const PhysicalClosure &c, f3 incoming, f3 gn, f3 ng, f2 random,
+                                                 float random_lobe, bool reflection_allowed, bool transmission_allowed) {
+    const float alpha = microfacet_alpha(c.roughness);
+    bool singular = alpha * alpha <= kMicrofacetSingularAlphaProduct;
+    const float sampling_alpha = maxf_(alpha, 1.0e-7f);
+    f3 h = gn;
+    if (!singular)
+        h = (c.op & kGlossyBeckmann) != 0u ? sample_beckmann_visible_normal(gn, incoming, sampling_alpha, random)
+                                           : sample_ggx_visible_normal(gn, incoming, sampling_alpha, random);
+    const float cos_hi = dot(h, incoming);
+    const GlassFresnel f = glass_fresnel(c, cos_hi, reflection_allowed, transmission_allowed);
+    const float probability = reflection_probability(f);
+    GlassSample r;
+    r.transmission = random_lobe >= probability;
+    const f3 reflected = h * (2.0f * cos_hi) - incoming;
+    const float e2 = c.ior * c.ior - (1.0f - cos_hi * cos_hi);
+    const float cos_ho = -sqrtf(maxf_(e2, 0.0f)) / c.ior;
+    const float inverse_eta = 1.0f / c.ior;
+    const f3 transmitted = h * (inverse_eta * cos_hi + cos_ho) - incoming * inverse_eta;
+    r.direction = r.transmission ? transmitted : reflected;
+    const f3 selected = r.transmission ? f.transmission : f.reflection;
+    const float lobe_probability = r.transmission ? 1.0f - probability : probability;
+    const bool shading_negative = dot(gn, r.direction) < 0.0f;
+    const bool geometric_negative = dot(ng, r.direction) < 0.0f;
+    const bool shading_ok = r.transmission ? shading_negative : !shading_negative;
+    const bool geometric_ok = r.transmission ? geometric_negative : !geometric_negative;
+    const bool has_energy = closure_sample_weight(f.reflection + f.transmission) > 0.0f;
+    r.valid = has_energy && cos_hi > 0.0f && shading_ok && geometric_ok;
+    r.singular = singular || (r.transmission && fabsf(c.ior - 1.0f) < 1.0e-4f);
+    r.singular_evaluation = c.weight * selected * 1.0f * 1.0e6f;
+    r.singular_pdf = lobe_probability * 1.0e6f;
+    return r;
+}
+
 struct Evaluation {
     f3 f;
     float pdf;
@@ -818,6 +994,7 @@ __device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, co
     const bool diffuse_enabled = (lobe_mask & kEventDiffuse) != 0u;
     const bool glossy_enabled = (lobe_mask & kEventGlossy) != 0u;
     const bool transparent_enabled = (lobe_mask & kEventTransparent) != 0u;
+    const bool transmission_enabled = (lobe_mask & kEventTransmission) != 0u;
     const f3 n = s.normal;
     const float nl = maxf_(dot(n, outgoing), 0.0f);
     const float bump =
@@ -827,6 +1004,31 @@ __device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, co
         const PhysicalClosure &c = s.c[i];
         if (c.op == PSY_CLOSURE_TRANSPARENT) {
             if (transparent_enabled) total += c.sample_weight;
+            continue;
+        }
+        if (kGlossy && is_dielectric(c.op)) {
+            // glass / refraction (surface_closure_evaluation.cpp:134-394): the side of
+            // `outgoing` picks reflection or transmission; a selected transmission
+            // keeps its bump term, and a selected unit-IOR transmission is a delta
+            const bool is_selected = int(i) == selected;
+            const f3 cn = microfacet_setup_normal(c, s, pt);
+            const f3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, cn);
+            const bool transmission = dot(gn, outgoing) < 0.0f;
+            const bool unit_ior_delta = is_selected && transmission && fabsf(c.ior - 1.0f) < 1.0e-4f;
+            float gb = bump_shadowing(pt.shading_normal, cn, outgoing, !is_selected, false, pt.bump_correction);
+            if (is_selected && transmission) gb = 1.0f;
+            const bool allowed = is_glass(c.op) ? (transmission ? transmission_enabled : glossy_enabled)
+                                                : (glossy_enabled && transmission_enabled);
+            if (!allowed) continue;
+            f3 intensity;
+            const Microfacet m = glass_eval(c, incoming, outgoing, gn, glossy_enabled, transmission_enabled, intensity);
+            const float pdf = ((gb != 0.0f || is_selected) && !unit_ior_delta) ? m.pdf : 0.0f;
+            const f3 value = unit_ior_delta ? mk3(0.0f) : c.weight * intensity * gb;
+            e.f = e.f + value;
+            total += c.sample_weight;
+            weighted_pdf += c.sample_weight * pdf;
+            if (closure_sample_weight(value) > 0.0f)
+                e.events |= kEventGlossy | (transmission ? kEventTransmission : kEventReflection);
             continue;
         }
         if (kGlossy && is_glossy(c.op)) {
@@ -898,6 +1100,8 @@ __device__ __noinline__ GlossySample sample_glossy(uint32_t op, float roughness,
 __device__ __forceinline__ bool closure_eligible(uint32_t op, uint32_t lobe_mask) {
     if (op == PSY_CLOSURE_DIFFUSE) return (lobe_mask & kEventDiffuse) != 0u;
     if (is_glossy(op)) return (lobe_mask & kEventGlossy) != 0u;
+    if (is_glass(op)) return (lobe_mask & (kEventGlossy | kEventTransmission)) != 0u;
+    if (is_refraction(op)) return (lobe_mask & kEventGlossy) != 0u && (lobe_mask & kEventTransmission) != 0u;
     return (lobe_mask & kEventTransparent) != 0u;
 }
 
@@ -919,13 +1123,16 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
     const float target = random_lobe * total;
     float accumulated = 0.0f;
     int chosen = -1;
-    float chosen_weight = 0.0f;
+    float chosen_weight = 0.0f, rescaled = random_lobe;
     for (uint32_t i = 0; i < s.count; ++i) {
         const float w = closure_eligible(s.c[i].op, lobe_mask) ? s.c[i].sample_weight : 0.0f;
         const float next = accumulated + w;
         if (chosen < 0 && w > 0.0f && target < next) {
             chosen = int(i);
             chosen_weight = w;
+            // SurfaceClosureCategoricalInversion::consider (:420-437): the lobe
+            // number rescaled into the chosen closure's interval
+            if (s.count > 1u) rescaled = (target - accumulated) / maxf_(w, 1.0e-20f);
         }
         accumulated = next;
     }
@@ -933,10 +1140,22 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
     const PhysicalClosure c = s.c[chosen];
     const bool transparent = c.op == PSY_CLOSURE_TRANSPARENT;
     const bool glossy = kGlossy && is_glossy(c.op);
-    bool candidate_valid = true, singular = false;
-    f3 direction;
+    const bool dielectric = kGlossy && is_dielectric(c.op);
+    bool candidate_valid = true, singular = false, transmission = false;
+    f3 direction, dielectric_delta = mk3(0.0f);
+    float dielectric_pdf = 0.0f;
     if (transparent) {
         direction = -pt.incoming;
+    } else if (dielectric) {
+        const f3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, microfacet_setup_normal(c, s, pt));
+        const GlassSample g = glass_sample(c, pt.view, gn, pt.geometric_normal, u_dir, rescaled,
+                                           (lobe_mask & kEventGlossy) != 0u, (lobe_mask & kEventTransmission) != 0u);
+        direction = g.direction;
+        candidate_valid = g.valid;
+        singular = g.singular;
+        transmission = g.transmission;
+        dielectric_delta = g.singular_evaluation;
+        dielectric_pdf = g.singular_pdf;
     } else if (glossy) {
         const GlossySample g = sample_glossy(c.op, c.roughness, c.color, pt, u_dir);
         direction = g.direction;
@@ -947,7 +1166,9 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
     }
     out.closure_index = uint32_t(chosen);
     out.wi = direction;
-    if (!(candidate_valid && (transparent || dot(pt.geometric_normal, direction) > 0.0f))) return out;
+    const bool geometric_valid =
+        transmission ? dot(pt.geometric_normal, direction) < 0.0f : dot(pt.geometric_normal, direction) > 0.0f;
+    if (!(candidate_valid && (transparent || geometric_valid))) return out;
     const Evaluation mixture = evaluate_mixture<kGlossy>(s, pt, direction, lobe_mask, chosen);
     Evaluation r;
     r.f = mixture.f;
@@ -957,9 +1178,14 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
         // x bump term (one when sampling a glossy closure) x 1e6
         r.f = r.f + c.weight * 1.0e6f;
         delta = 1.0e6f * chosen_weight;
+    } else if (dielectric && singular) {
+        r.f = r.f + dielectric_delta;
+        delta = dielectric_pdf * chosen_weight;
     }
     r.pdf = mixture.pdf + delta / maxf_(total, 1.0e-20f);
     if (transparent) r.events = kEventTransmission | kEventTransparent;
+    else if (dielectric)
+        r.events = (singular ? kEventSingular : kEventGlossy) | (transmission ? kEventTransmission : kEventReflection);
     else if (glossy) r.events = singular ? (kEventSingular | kEventReflection) : (kEventGlossy | kEventReflection);
     else r.events = kEventDiffuse | kEventReflection;
     out.eval = r;
@@ -984,9 +1210,9 @@ __device__ __forceinline__ void surface_aov(const SurfaceClosures &s, const Clos
             const float w = closure_sample_weight(c.weight);
             n = n + s.normal * w;
             total += w;
-        } else if (kGlossy && is_glossy(c.op)) {
+        } else if (kGlossy && (is_glossy(c.op) || is_dielectric(c.op))) {
             const float w = closure_sample_weight(c.weight);
-            n = n + specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, c.color) * w;
+            n = n + specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, microfacet_setup_normal(c, s, pt)) * w;
             total += w;
         } else {
             transparency = transparency + c.weight;

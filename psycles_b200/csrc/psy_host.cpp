@@ -1069,19 +1069,23 @@ psy_status validate_material(const psy_material_desc &m) {
     };
     for (uint32_t k = 0; k < m.closure_count; ++k) {
         const psy_closure_instruction &c = m.closures[k];
-        if (c.op > PSY_CLOSURE_GLOSSY) return fail(PSY_ERROR_UNSUPPORTED, "closure operation outside the supported set");
+        if (c.op > PSY_CLOSURE_REFRACTION)
+            return fail(PSY_ERROR_UNSUPPORTED, "closure operation outside the supported set");
+        const bool microfacet = c.op == PSY_CLOSURE_GLOSSY || c.op == PSY_CLOSURE_GLASS || c.op == PSY_CLOSURE_REFRACTION;
         if ((c.op == PSY_CLOSURE_ADD || c.op == PSY_CLOSURE_MIX) && (c.a >= m.closure_count || c.b >= m.closure_count))
             return fail(PSY_ERROR_INVALID_ARGUMENT, "closure child out of range");
         if ((c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_TRANSPARENT ||
-             c.op == PSY_CLOSURE_GLOSSY) &&
+             microfacet) &&
             !input_ok(c.color, V, false))
             return fail(PSY_ERROR_INVALID_ARGUMENT, "closure colour input out of range");
-        if ((c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_MIX) && !input_ok(c.scalar, S, false))
+        if ((c.op == PSY_CLOSURE_EMISSION || c.op == PSY_CLOSURE_MIX || c.op == PSY_CLOSURE_GLASS ||
+             c.op == PSY_CLOSURE_REFRACTION) &&
+            !input_ok(c.scalar, S, false))
             return fail(PSY_ERROR_INVALID_ARGUMENT, "closure scalar input out of range");
-        if ((c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_GLOSSY) && !input_ok(c.roughness, S, true))
+        if ((c.op == PSY_CLOSURE_DIFFUSE || microfacet) && !input_ok(c.roughness, S, true))
             return fail(PSY_ERROR_INVALID_ARGUMENT, "closure roughness input out of range");
-        if (c.op == PSY_CLOSURE_GLOSSY && c.a != PSY_GLOSSY_GGX && c.a != PSY_GLOSSY_BECKMANN)
-            return fail(PSY_ERROR_UNSUPPORTED, "glossy distribution outside GGX and Beckmann");
+        if (microfacet && c.a != PSY_GLOSSY_GGX && c.a != PSY_GLOSSY_BECKMANN)
+            return fail(PSY_ERROR_UNSUPPORTED, "microfacet distribution outside GGX and Beckmann");
     }
     // The device walks the tree with a 32-entry stack and keeps at most 16
     // BSDF closures per shading point (the reference's capacity is Cycles'
@@ -1089,7 +1093,7 @@ psy_status validate_material(const psy_material_desc &m) {
     // rather than rendered with closures dropped.  The walk is replayed here.
     uint32_t stack[32];
     uint32_t sp = 0u, leaves = 0u, visits = 0u;
-    bool transparent = false;
+    bool transparent = false, glass = false;
     stack[sp++] = m.root;
     while (sp > 0u) {
         const uint32_t id = stack[--sp];
@@ -1099,14 +1103,20 @@ psy_status validate_material(const psy_material_desc &m) {
             if (sp + 2u > 32u) return fail(PSY_ERROR_UNSUPPORTED, "closure tree deeper than the device walk's stack");
             stack[sp++] = c.b;
             stack[sp++] = c.a;
-        } else if (c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_GLOSSY) {
+        } else if (c.op == PSY_CLOSURE_DIFFUSE || c.op == PSY_CLOSURE_GLOSSY || c.op == PSY_CLOSURE_GLASS ||
+                   c.op == PSY_CLOSURE_REFRACTION) {
             ++leaves;
+            glass = glass || c.op == PSY_CLOSURE_GLASS;
         } else if (c.op == PSY_CLOSURE_TRANSPARENT) {
             transparent = true;  // every transparent closure merges into one
         }
     }
     if (leaves + (transparent ? 1u : 0u) > 16u)
         return fail(PSY_ERROR_UNSUPPORTED, "more than 16 BSDF closures in one material");
+    // a glass closure's selection weight among other closures is Cycles'
+    // tabulated Fresnel albedo, which this build does not carry
+    if (glass && leaves + (transparent ? 1u : 0u) > 1u)
+        return fail(PSY_ERROR_UNSUPPORTED, "a glass closure must be the only BSDF closure of its material");
     return PSY_OK;
 }
 
@@ -1841,7 +1851,9 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         }
         any_transparent = any_transparent || g.has_transparent;
         for (uint32_t k = 0; k < m.closure_count; ++k)
-            if (m.closures[k].op == PSY_CLOSURE_GLOSSY) any_glossy = true;
+            if (m.closures[k].op == PSY_CLOSURE_GLOSSY || m.closures[k].op == PSY_CLOSURE_GLASS ||
+                m.closures[k].op == PSY_CLOSURE_REFRACTION)
+                any_glossy = true;
         code.insert(code.end(), m.closures, m.closures + m.closure_count);
         sc->scalars.insert(sc->scalars.end(), m.scalars, m.scalars + m.scalar_count);
         sc->vectors.insert(sc->vectors.end(), m.vectors, m.vectors + 3ull * m.vector_count);

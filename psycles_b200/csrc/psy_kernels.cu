@@ -741,7 +741,8 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                 const SurfacePoint sp = surface_point(s, h, ray.d);
                 const MaterialGpu mat = s.materials[sp.material];
                 SurfaceClosures closures;
-                const ClosurePoint cpt{sp.n, sp.ng, -ray.d, safe_normalize(-ray.d, sp.n), mat.bump_correction != 0u};
+                const ClosurePoint cpt{sp.n, sp.ng, -ray.d, safe_normalize(-ray.d, sp.n), mat.bump_correction != 0u,
+                                       sp.back_facing};
                 collect_surface<kGlossy>(s, mat, cpt, closures);
                 // SurfaceShadingStageImpl::emit (src/luisa/path_kernel_surface_shading.cpp:117-250)
                 float emission_weight = 1.0f;

@@ -185,7 +185,7 @@ struct SceneView {
     float background[3];
     uint32_t world_visibility;
     uint32_t any_transparent;
-    uint32_t has_glossy;  // a material holds a glossy closure (selects the shading variant)
+    uint32_t has_glossy;  // a material holds a glossy, glass or refraction closure (selects the shading variant)
     // many-light tree (empty when the scene has no emitter with energy)
     const LtNodeGpu *lt_nodes;
     const LtEmitterGpu *lt_emitters;

@@ -2,7 +2,8 @@
 
 Host mirror of the reference's material contract for the in-scope node set:
 closures diffuse (Lambert / Oren-Nayar by roughness), glossy (GGX / Beckmann
-microfacet reflection), emission, transparent, add and mix, fed by constants, float math, conversions, mixes, colour blends
+microfacet reflection), glass and refraction (dielectric microfacet
+transmission), emission, transparent, add and mix, fed by constants, float math, conversions, mixes, colour blends
 and separate / combine RGB:
 
   * ShaderGraph / node types       include/psycles/contract/shader_graph.h,
@@ -44,6 +45,8 @@ class NodeType(str, enum.Enum):
     EMISSION = "psycles.closure.emission"
     TRANSPARENT = "psycles.closure.transparent"
     GLOSSY = "psycles.closure.glossy"
+    GLASS = "psycles.closure.glass"
+    REFRACTION = "psycles.closure.refraction"
     ADD = "psycles.closure.add"
     MIX = "psycles.closure.mix"
     # values
@@ -72,8 +75,8 @@ class NodeType(str, enum.Enum):
     COMBINE_COLOR = "psycles.color.combine"
 
 
-CLOSURE_TYPES = (NodeType.DIFFUSE, NodeType.EMISSION, NodeType.TRANSPARENT, NodeType.GLOSSY, NodeType.ADD,
-                 NodeType.MIX)
+CLOSURE_TYPES = (NodeType.DIFFUSE, NodeType.EMISSION, NodeType.TRANSPARENT, NodeType.GLOSSY, NodeType.GLASS,
+                 NodeType.REFRACTION, NodeType.ADD, NodeType.MIX)
 GLOSSY_DISTRIBUTIONS = {"GGX": _abi.GLOSSY_GGX, "BECKMANN": _abi.GLOSSY_BECKMANN}
 
 F, C = "float", "color"  # socket kinds: scalar and vector values
@@ -85,6 +88,8 @@ _SCHEMA: dict[NodeType, tuple[list, list]] = {
     NodeType.EMISSION: ([("Color", C, (1.0, 1.0, 1.0)), ("Strength", F, 1.0)], []),
     NodeType.TRANSPARENT: ([("Color", C, (1.0, 1.0, 1.0))], []),
     NodeType.GLOSSY: ([("Color", C, (0.8, 0.8, 0.8)), ("Roughness", F, 0.2)], []),
+    NodeType.GLASS: ([("Color", C, (1.0, 1.0, 1.0)), ("Roughness", F, 0.0), ("IOR", F, 1.5)], []),
+    NodeType.REFRACTION: ([("Color", C, (1.0, 1.0, 1.0)), ("Roughness", F, 0.0), ("IOR", F, 1.5)], []),
     NodeType.ADD: ([], []),
     NodeType.MIX: ([("Factor", F, 0.5)], []),
     NodeType.CONSTANT_FLOAT: ([("Value", F, 0.0)], [("Value", F)]),
@@ -184,6 +189,22 @@ class ShaderGraph:
         if distribution not in GLOSSY_DISTRIBUTIONS:
             raise ShaderGraphError(f"glossy distribution {distribution!r} outside GGX and BECKMANN")
         return self._node(NodeType.GLOSSY, {"Distribution": distribution}, Color=color, Roughness=roughness)
+
+    def glass_bsdf(self, color=(1.0, 1.0, 1.0), roughness=0.0, ior=1.5, distribution: str = "GGX") -> int:
+        """Glass BSDF (core_nodes.cpp:992-1004): dielectric microfacet
+        reflection and transmission with the Fresnel split; a material may
+        hold no other BSDF closure beside it (its selection weight among
+        others reads Cycles' tabulated Fresnel albedo)."""
+        if distribution not in GLOSSY_DISTRIBUTIONS:
+            raise ShaderGraphError(f"glass distribution {distribution!r} outside GGX and BECKMANN")
+        return self._node(NodeType.GLASS, {"Distribution": distribution}, Color=color, Roughness=roughness, IOR=ior)
+
+    def refraction_bsdf(self, color=(1.0, 1.0, 1.0), roughness=0.0, ior=1.5, distribution: str = "GGX") -> int:
+        """Refraction BSDF (core_nodes.cpp:1006-1019): microfacet
+        transmission only."""
+        if distribution not in GLOSSY_DISTRIBUTIONS:
+            raise ShaderGraphError(f"refraction distribution {distribution!r} outside GGX and BECKMANN")
+        return self._node(NodeType.REFRACTION, {"Distribution": distribution}, Color=color, Roughness=roughness, IOR=ior)
 
     def emission(self, color, strength=1.0) -> int:
         return self._node(NodeType.EMISSION, Color=color, Strength=strength)
@@ -452,6 +473,10 @@ def compile_surface_program(graph: ShaderGraph) -> tuple[SurfaceProgram, Surface
         elif n.type == NodeType.GLOSSY:
             code.append((_abi.CLOSURE_GLOSSY, GLOSSY_DISTRIBUTIONS[n.props.get("Distribution", "GGX")], 0,
                          low.closure_input(n, "Color"), none, low.closure_input(n, "Roughness")))
+        elif n.type in (NodeType.GLASS, NodeType.REFRACTION):
+            op = _abi.CLOSURE_GLASS if n.type == NodeType.GLASS else _abi.CLOSURE_REFRACTION
+            code.append((op, GLOSSY_DISTRIBUTIONS[n.props.get("Distribution", "GGX")], 0,
+                         low.closure_input(n, "Color"), low.closure_input(n, "IOR"), low.closure_input(n, "Roughness")))
         elif n.type == NodeType.EMISSION:
             code.append((_abi.CLOSURE_EMISSION, 0, 0, low.closure_input(n, "Color"), low.closure_input(n, "Strength"),
                          none))
@@ -566,6 +591,12 @@ def random_material(rng: np.random.Generator, max_leaves: int = 6, emission_prob
         else:
             ids.append(g.add_shader(a, b))
     return g.set_output(ids[0])
+
+
+def glass_material(color=(1.0, 1.0, 1.0), roughness: float = 0.0, ior: float = 1.5,
+                   distribution: str = "GGX") -> ShaderGraph:
+    g = ShaderGraph()
+    return g.set_output(g.glass_bsdf(color, roughness, ior, distribution))
 
 
 def glossy_material(color, roughness: float = 0.2, distribution: str = "GGX") -> ShaderGraph:

@@ -28,8 +28,8 @@ import numpy as np
 
 from . import _abi
 from .materials import (CompiledMaterial, ShaderGraph, compile_surface_program, diffuse_material,
-                        emission_material, glossy_material, glossy_mixture_material, random_material,
-                        value_graph_material)
+                        emission_material, glass_material, glossy_material, glossy_mixture_material,
+                        random_material, value_graph_material)
 
 
 @dataclasses.dataclass
@@ -544,6 +544,28 @@ def glossy_scene(seed: int = 0) -> Scene:
     base = small_test_scene(seed=seed)
     base.materials = _materials(graphs)
     base.materials[3].use_bump_map_correction = False
+    return base
+
+
+def glass_scene(seed: int = 0) -> Scene:
+    """The small test scene's geometry and lamps with dielectric materials:
+    smooth (singular) and rough GGX glass, Beckmann glass, a tinted glass,
+    smooth and rough refraction, and refraction mixed with diffuse; the
+    spheres are closed, so paths enter and leave them (back-facing hits with
+    the inverted IOR) and reach total internal reflection."""
+    from .materials import ShaderGraph as _G
+    graphs = [diffuse_material((0.7, 0.7, 0.7)), emission_material((1.0, 0.9, 0.8), 6.0),
+              glass_material((1.0, 1.0, 1.0), 0.0, 1.5), glass_material((0.95, 0.95, 1.0), 0.2, 1.45),
+              glass_material((0.8, 1.0, 0.85), 0.3, 1.33, "BECKMANN"), glass_material((1.0, 0.7, 0.5), 0.0, 1.6)]
+    g = _G()
+    g.set_output(g.refraction_bsdf((0.9, 0.95, 1.0), 0.0, 1.4))
+    graphs.append(g)
+    g = _G()
+    g.set_output(g.mix_shader(0.3, g.refraction_bsdf((1.0, 1.0, 1.0), 0.25, 1.5, "BECKMANN"),
+                              g.diffuse_bsdf((0.6, 0.3, 0.2))))
+    graphs.append(g)
+    base = small_test_scene(seed=seed)
+    base.materials = _materials(graphs)
     return base
 
 
