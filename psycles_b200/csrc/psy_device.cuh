@@ -320,8 +320,20 @@ struct PhysicalClosure {
     uint32_t op;
     f3 color;
     float roughness;
-    float ior;  // glass / refraction: relative IOR (inverted on a back face)
+};
+
+// The closure of the glossy-capable shading variant: glass and refraction
+// closures add their IORs.  The variant without glossy closures keeps the
+// 36-byte closure, so its shading point stores no IOR it never reads.
+struct DielectricClosure : PhysicalClosure {
+    float ior;  // relative IOR (inverted on a back face)
     float f0;   // glass: F0 of the authored IOR
+};
+template <bool kGlossy> struct ClosureSlot {
+    using type = PhysicalClosure;
+};
+template <> struct ClosureSlot<true> {
+    using type = DielectricClosure;
 };
 
 constexpr uint32_t kGlossyBeckmann = 0x100u;
@@ -348,10 +360,11 @@ struct ClosurePoint {
 // keeps the shading kernel's register budget where it was before them.
 constexpr uint32_t kLeavesOf(bool glossy) { return glossy ? 15u : 7u; }
 
+template <bool kGlossy>
 struct SurfaceClosures {
     f3 normal;          // the diffuse closures' normal
     bool normal_exact;  // it equals the shading normal bit for bit (bump term one)
-    PhysicalClosure c[kMaxClosures];
+    typename ClosureSlot<kGlossy>::type c[kMaxClosures];
     uint32_t count;
     f3 emission;
 };
@@ -606,7 +619,7 @@ __device__ __forceinline__ float f0_from_ior(float ior) {
 // (bsdf_transparent_setup, :483-518: summed weights and sample weights).
 template <bool kGlossy>
 __device__ __forceinline__ void collect_surface(const SceneView &s, const MaterialGpu &m, const ClosurePoint &pt,
-                                    SurfaceClosures &out) {
+                                    SurfaceClosures<kGlossy> &out) {
     out.count = 0u;
     out.emission = mk3(0.0f);
     out.normal = safe_normalize(pt.shading_normal, pt.shading_normal);
@@ -618,12 +631,14 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
             out.emission = out.emission + w;
             return;
         }
-        PhysicalClosure p;
+        typename ClosureSlot<kGlossy>::type p;
         p.op = op;
         p.color = color;
         p.roughness = roughness;
-        p.ior = 1.0f;
-        p.f0 = 0.0f;
+        if constexpr (kGlossy) {
+            p.ior = 1.0f;
+            p.f0 = 0.0f;
+        }
         if (op == PSY_CLOSURE_DIFFUSE) {
             p.weight = bsdf_allocated_weight(w);
             p.sample_weight = closure_sample_weight(p.weight);
@@ -648,8 +663,10 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
             p.weight = allocated;
             p.sample_weight = allocation * 1.0f * closure_sample_weight(mk3(1.0f));
             p.roughness = sqrtf(clampf_(roughness * roughness, 0.0f, 1.0f));
-            p.ior = pt.back_facing ? 1.0f / ior : ior;
-            p.f0 = clampf_(f0_from_ior(ior), 0.0f, 1.0f);
+            if constexpr (kGlossy) {
+                p.ior = pt.back_facing ? 1.0f / ior : ior;
+                p.f0 = clampf_(f0_from_ior(ior), 0.0f, 1.0f);
+            }
             if (is_refraction(op)) p.color = specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, out.normal);
         } else {
             const float sw = closure_sample_weight(w);
@@ -717,10 +734,11 @@ __device__ __forceinline__ bool microfacet_singular(float roughness) {
 }
 
 // cycles_runtime_flags (src/luisa/graph_surface_scattering.cpp:292-365).
-__device__ __forceinline__ uint32_t runtime_flags(const SurfaceClosures &s, bool back_facing) {
+template <bool kGlossy>
+__device__ __forceinline__ uint32_t runtime_flags(const SurfaceClosures<kGlossy> &s, bool back_facing) {
     uint32_t f = back_facing ? kRuntimeBackfacing : 0u;
     for (uint32_t i = 0; i < s.count; ++i) {
-        const PhysicalClosure &c = s.c[i];
+        const auto &c = s.c[i];
         if (c.op == PSY_CLOSURE_DIFFUSE) f |= kRuntimeBsdf | kRuntimeBsdfHasEval;
         else if (is_glossy(c.op)) f |= kRuntimeBsdf | (microfacet_singular(c.roughness) ? 0u : kRuntimeBsdfHasEval);
         else if (is_dielectric(c.op))
@@ -812,9 +830,9 @@ __device__ __noinline__ Microfacet microfacet_eval(uint32_t op, float roughness,
 
 // The closure normal of a glossy, glass or refraction closure after setup's
 // specular-reflection correction (glass recomputes it: its `color` holds the tint).
-__device__ __forceinline__ f3 microfacet_setup_normal(const PhysicalClosure &c, const SurfaceClosures &s,
+__device__ __forceinline__ f3 microfacet_setup_normal(const PhysicalClosure &c, f3 diffuse_normal,
                                                       const ClosurePoint &pt) {
-    return is_glass(c.op) ? specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, s.normal) : c.color;
+    return is_glass(c.op) ? specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, diffuse_normal) : c.color;
 }
 
 struct GlassFresnel {
@@ -825,7 +843,7 @@ struct GlassFresnel {
 // standalone Glass closure (F0 of its IOR, F90 one, both tints its colour:
 // caustics on) or Refraction closure (no reflection; transmission one unless
 // totally reflected).
-__device__ __forceinline__ GlassFresnel glass_fresnel(const PhysicalClosure &c, float cos_hi, bool reflection_allowed,
+__device__ __forceinline__ GlassFresnel glass_fresnel(const DielectricClosure &c, float cos_hi, bool reflection_allowed,
                                                       bool transmission_allowed) {
     const float real = fresnel_dielectric_cos(cos_hi, c.ior);
     GlassFresnel r;
@@ -854,7 +872,7 @@ __device__ __forceinline__ float reflection_probability(const GlassFresnel &f) {
 // 234-320): glass_geometry's half vector (the refractive one oriented by the
 // IOR), D, Lambda, the Fresnel lobe of the side `outgoing` lies on, and the
 // refraction Jacobian.
-__device__ __noinline__ Microfacet glass_eval(const PhysicalClosure &c, f3 incoming, f3 outgoing, f3 n,
+__device__ __noinline__ Microfacet glass_eval(const DielectricClosure &c, f3 incoming, f3 outgoing, f3 n,
                                               bool reflection_allowed, bool transmission_allowed, f3 &value) {
     const bool beckmann = (c.op & kGlossyBeckmann) != 0u;
     const float cos_o = dot(n, outgoing);
@@ -895,7 +913,7 @@ struct GlassSample {
 };
 
 // MicrofacetGlassComponent::sample (microfacet_glass_component.cpp:322-395).
-__device__ __noinline__ GlassSample glass_sample(const PhysicalClosure &c, f3 incoming, f3 gn, f3 ng, f2 random,
+__device__ __noinline__ GlassSample glass_sample(const DielectricClosure &c, f3 incoming, f3 gn, f3 ng, f2 random,
                                                  float random_lobe, bool reflection_allowed, bool transmission_allowed) {
     const float alpha = microfacet_alpha(c.roughness);
     bool singular = alpha * alpha <= kMicrofacetSingularAlphaProduct;
@@ -984,7 +1002,7 @@ __device__ __noinline__ f3 oren_nayar_intensity(const PhysicalClosure &c, float 
 // kernel calls it for the light sample and for the BSDF sample, and a
 // single copy keeps the kernel's code within the instruction cache.
 template <bool kGlossy>
-__device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, const ClosurePoint &pt,
+__device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures<kGlossy> &s, const ClosurePoint &pt,
                                                     f3 outgoing_raw, uint32_t lobe_mask, int selected) {
     const f3 outgoing = safe_normalize(outgoing_raw, pt.shading_normal);
     // make_surface_closure_evaluation_directions (surface_closure_evaluation.cpp:61-70)
@@ -1001,17 +1019,17 @@ __device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures &s, co
         s.normal_exact ? 1.0f : bump_shadowing_general(pt.shading_normal, n, outgoing, true, true, pt.bump_correction);
     const float lambert = nl * kInvPi;
     for (uint32_t i = 0; i < s.count; ++i) {
-        const PhysicalClosure &c = s.c[i];
+        const auto &c = s.c[i];
         if (c.op == PSY_CLOSURE_TRANSPARENT) {
             if (transparent_enabled) total += c.sample_weight;
             continue;
         }
-        if (kGlossy && is_dielectric(c.op)) {
+        if constexpr (kGlossy) if (is_dielectric(c.op)) {
             // glass / refraction (surface_closure_evaluation.cpp:134-394): the side of
             // `outgoing` picks reflection or transmission; a selected transmission
             // keeps its bump term, and a selected unit-IOR transmission is a delta
             const bool is_selected = int(i) == selected;
-            const f3 cn = microfacet_setup_normal(c, s, pt);
+            const f3 cn = microfacet_setup_normal(c, s.normal, pt);
             const f3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, cn);
             const bool transmission = dot(gn, outgoing) < 0.0f;
             const bool unit_ior_delta = is_selected && transmission && fabsf(c.ior - 1.0f) < 1.0e-4f;
@@ -1110,7 +1128,7 @@ __device__ __forceinline__ bool closure_eligible(uint32_t op, uint32_t lobe_mask
 // :216-337 with the glossy sample_microfacet_reflection of
 // graph_surface_scattering.cpp:730-770, finish :490-660).
 template <bool kGlossy>
-__device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s, const ClosurePoint &pt, float u_lobe,
+__device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures<kGlossy> &s, const ClosurePoint &pt, float u_lobe,
                                                         f2 u_dir, uint32_t lobe_mask) {
     SurfaceSample out;
     out.valid = false;
@@ -1137,7 +1155,7 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
         accumulated = next;
     }
     if (chosen < 0) return out;
-    const PhysicalClosure c = s.c[chosen];
+    const auto c = s.c[chosen];
     const bool transparent = c.op == PSY_CLOSURE_TRANSPARENT;
     const bool glossy = kGlossy && is_glossy(c.op);
     const bool dielectric = kGlossy && is_dielectric(c.op);
@@ -1146,8 +1164,17 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
     float dielectric_pdf = 0.0f;
     if (transparent) {
         direction = -pt.incoming;
-    } else if (dielectric) {
-        const f3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, microfacet_setup_normal(c, s, pt));
+    } else if (glossy) {
+        const GlossySample g = sample_glossy(c.op, c.roughness, c.color, pt, u_dir);
+        direction = g.direction;
+        candidate_valid = g.valid;
+        singular = g.singular;
+    } else if (!dielectric) {
+        direction = sample_cosine_hemisphere(s.normal, u_dir, nullptr);
+    }
+    if constexpr (kGlossy) if (dielectric) {
+        const f3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, pt.view,
+                                      microfacet_setup_normal(c, s.normal, pt));
         const GlassSample g = glass_sample(c, pt.view, gn, pt.geometric_normal, u_dir, rescaled,
                                            (lobe_mask & kEventGlossy) != 0u, (lobe_mask & kEventTransmission) != 0u);
         direction = g.direction;
@@ -1156,13 +1183,6 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
         transmission = g.transmission;
         dielectric_delta = g.singular_evaluation;
         dielectric_pdf = g.singular_pdf;
-    } else if (glossy) {
-        const GlossySample g = sample_glossy(c.op, c.roughness, c.color, pt, u_dir);
-        direction = g.direction;
-        candidate_valid = g.valid;
-        singular = g.singular;
-    } else {
-        direction = sample_cosine_hemisphere(s.normal, u_dir, nullptr);
     }
     out.closure_index = uint32_t(chosen);
     out.wi = direction;
@@ -1197,14 +1217,14 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures &s
 // diffuse colour into Albedo, every diffuse and glossy normal (glossy:
 // corrected) weighted by |average weight| into Normal.
 template <bool kGlossy>
-__device__ __forceinline__ void surface_aov(const SurfaceClosures &s, const ClosurePoint &pt, f3 &albedo, f3 &normal,
+__device__ __forceinline__ void surface_aov(const SurfaceClosures<kGlossy> &s, const ClosurePoint &pt, f3 &albedo, f3 &normal,
                                             f3 &transparency) {
     albedo = mk3(0.0f);
     transparency = mk3(0.0f);
     f3 n = mk3(0.0f);
     float total = 0.0f;
     for (uint32_t i = 0; i < s.count; ++i) {
-        const PhysicalClosure &c = s.c[i];
+        const auto &c = s.c[i];
         if (c.op == PSY_CLOSURE_DIFFUSE) {
             albedo = albedo + c.weight;
             const float w = closure_sample_weight(c.weight);
@@ -1212,7 +1232,7 @@ __device__ __forceinline__ void surface_aov(const SurfaceClosures &s, const Clos
             total += w;
         } else if (kGlossy && (is_glossy(c.op) || is_dielectric(c.op))) {
             const float w = closure_sample_weight(c.weight);
-            n = n + specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, microfacet_setup_normal(c, s, pt)) * w;
+            n = n + specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, microfacet_setup_normal(c, s.normal, pt)) * w;
             total += w;
         } else {
             transparency = transparency + c.weight;

@@ -740,7 +740,7 @@ __global__ void __launch_bounds__(128, PSY_SHADE_MIN_BLOCKS)
                 }
                 const SurfacePoint sp = surface_point(s, h, ray.d);
                 const MaterialGpu mat = s.materials[sp.material];
-                SurfaceClosures closures;
+                SurfaceClosures<kGlossy> closures;
                 const ClosurePoint cpt{sp.n, sp.ng, -ray.d, safe_normalize(-ray.d, sp.n), mat.bump_correction != 0u,
                                        sp.back_facing};
                 collect_surface<kGlossy>(s, mat, cpt, closures);
