@@ -619,7 +619,9 @@ def luisa_demo_scene(variant: int = 0) -> Scene:
     light under the open ceiling and a background light, 47 degree camera.
     Variant 1 (or True): the block's colour is an RGB-node mix and its
     roughness float math; variant 2: the block is a GGX Glossy BSDF and the
-    plaster a mix of rough diffuse and Beckmann glossy -- as
+    plaster a mix of rough diffuse and Beckmann glossy; variant 4: the block
+    is a rough GGX Glass BSDF (IOR 1.45) and the plaster a mix of rough
+    diffuse and Beckmann Refraction (IOR 1.3) -- as
     tests/adapter/adapter_probe.cpp builds them."""
     f = np.float32
     variant = int(variant)
@@ -630,6 +632,11 @@ def luisa_demo_scene(variant: int = 0) -> Scene:
         g.set_output(g.mix_shader(0.25, g.diffuse_bsdf((0.72, 0.72, 0.72), 0.35),
                                   g.glossy_bsdf((0.9, 0.9, 0.85), 0.2, "BECKMANN")))
         graphs[0] = g
+    if variant == 4:
+        g = ShaderGraph()
+        g.set_output(g.mix_shader(0.3, g.diffuse_bsdf((0.72, 0.72, 0.72), 0.35),
+                                  g.refraction_bsdf((0.9, 0.9, 0.85), 0.2, 1.3, "BECKMANN")))
+        graphs[0] = g
     if variant == 1:
         g = ShaderGraph()
         color = g.mix_color(0.3, g.rgb((0.035, 0.18, 0.85)), g.rgb((0.9, 0.5, 0.1)))
@@ -637,6 +644,8 @@ def luisa_demo_scene(variant: int = 0) -> Scene:
         graphs.append(g)
     elif variant == 2:
         graphs.append(glossy_material((0.035, 0.18, 0.85), 0.3, "GGX"))
+    elif variant == 4:
+        graphs.append(glass_material((0.9, 0.95, 1.0), 0.15, 1.45, "GGX"))
     else:
         graphs.append(diffuse_material((0.035, 0.18, 0.85), 0.16))
     mats = _materials(graphs)

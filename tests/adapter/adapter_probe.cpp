@@ -15,7 +15,9 @@
 // compiler emits a non-trivial value stream.  The "glossy" variant makes the
 // block a GGX Glossy BSDF and the plaster a mix of rough diffuse and
 // Beckmann glossy; the "multiscatter" variant asks for the MULTI_GGX
-// distribution, which the adapter must refuse.
+// distribution, which the adapter must refuse; the "glass" variant makes the
+// (open-bottomed) block a rough GGX Glass BSDF and the plaster a mix of rough
+// diffuse and Beckmann Refraction.
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -122,6 +124,36 @@ ShaderGraph glossy_plaster() {
     return g;
 }
 
+ShaderGraph dielectric(const char *type, Vec3f color, float roughness, float ior, const char *distribution) {
+    ShaderGraph g;
+    const NodeId n = g.add_node(type, "Dielectric");
+    (void)g.set_input(n, "Color", SocketValue::color(color));
+    (void)g.set_input(n, "Roughness", SocketValue::floating(roughness));
+    (void)g.set_input(n, "IOR", SocketValue::floating(ior));
+    (void)g.set_property(n, "Distribution", SocketValue::string(distribution));
+    g.set_root(ShaderDomain::surface, OutputRef{n, "Closure"});
+    return g;
+}
+
+// Plaster as Mix(0.3, rough diffuse, Beckmann refraction).
+ShaderGraph refractive_plaster() {
+    ShaderGraph g;
+    const NodeId d = g.add_node(compiler::node_type::diffuse_bsdf, "Diffuse");
+    (void)g.set_input(d, "Color", SocketValue::color(v3(0.72f, 0.72f, 0.72f)));
+    (void)g.set_input(d, "Roughness", SocketValue::floating(0.35f));
+    const NodeId r = g.add_node(compiler::node_type::refraction_bsdf, "Refraction");
+    (void)g.set_input(r, "Color", SocketValue::color(v3(0.9f, 0.9f, 0.85f)));
+    (void)g.set_input(r, "Roughness", SocketValue::floating(0.2f));
+    (void)g.set_input(r, "IOR", SocketValue::floating(1.3f));
+    (void)g.set_property(r, "Distribution", SocketValue::string("BECKMANN"));
+    const NodeId m = g.add_node(compiler::node_type::mix_closure, "Mix");
+    (void)g.set_input(m, "Factor", SocketValue::floating(0.3f));
+    (void)g.connect(OutputRef{d, "Closure"}, m, "A");
+    (void)g.connect(OutputRef{r, "Closure"}, m, "B");
+    g.set_root(ShaderDomain::surface, OutputRef{m, "Closure"});
+    return g;
+}
+
 void quad(TriangleMeshDesc &m, Vec3f a, Vec3f b, Vec3f c, Vec3f d, Vec3f n, std::uint32_t slot) {
     const auto base = static_cast<std::uint32_t>(m.positions.size());
     for (const Vec3f &p : {a, b, c, d}) {
@@ -135,7 +167,7 @@ void quad(TriangleMeshDesc &m, Vec3f a, Vec3f b, Vec3f c, Vec3f d, Vec3f n, std:
 }
 
 // variant: 0 plain, 1 value-graph block, 2 glossy block and plaster,
-// 3 a MULTI_GGX block
+// 3 a MULTI_GGX block, 4 glass block and refractive plaster
 SceneSnapshot demo_snapshot(int variant) {
     const MaterialId plaster{1u}, red{2u}, green{3u}, block{4u};
     const bool graph_material = variant == 1;
@@ -143,12 +175,16 @@ SceneSnapshot demo_snapshot(int variant) {
     delta.base_revision = 0u;
     delta.emplace<UpsertMaterial>(
         plaster, MaterialDesc{.name = "Plaster",
-                              .shader = variant == 2 ? glossy_plaster() : rough_diffuse(v3(0.72f, 0.72f, 0.72f), 0.35f)});
+                              .shader = variant == 2   ? glossy_plaster()
+                                        : variant == 4 ? refractive_plaster()
+                                                       : rough_diffuse(v3(0.72f, 0.72f, 0.72f), 0.35f)});
     delta.emplace<UpsertMaterial>(red, MaterialDesc{.name = "Red wall", .shader = rough_diffuse(v3(0.72f, 0.06f, 0.035f), 0.45f)});
     delta.emplace<UpsertMaterial>(green, MaterialDesc{.name = "Green wall", .shader = rough_diffuse(v3(0.04f, 0.54f, 0.12f), 0.45f)});
     ShaderGraph block_shader = graph_material ? graph_diffuse() : rough_diffuse(v3(0.035f, 0.18f, 0.85f), 0.16f);
     if (variant == 2) block_shader = glossy(v3(0.035f, 0.18f, 0.85f), 0.3f, "GGX");
     if (variant == 3) block_shader = glossy(v3(0.035f, 0.18f, 0.85f), 0.3f, "MULTI_GGX");
+    if (variant == 4)
+        block_shader = dielectric(compiler::node_type::glass_bsdf, v3(0.9f, 0.95f, 1.0f), 0.15f, 1.45f, "GGX");
     delta.emplace<UpsertMaterial>(block, MaterialDesc{.name = "Blue block", .shader = std::move(block_shader)});
     TriangleMeshDesc room;
     room.name = "Room";

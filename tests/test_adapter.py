@@ -43,7 +43,8 @@ def probe():
 
 class Flattened:
     """The adapter's flattened demo snapshot (variant 0 plain, 1 value-graph
-    block, 2 glossy); `.pointer` as scenes.SceneDescHandle."""
+    block, 2 glossy, 4 glass and refraction); `.pointer` as
+    scenes.SceneDescHandle."""
 
     def __init__(self, variant):
         self.lib = probe()
@@ -104,7 +105,7 @@ def test_flattened_snapshot_equals_scene_model():
         assert arr(ma.scalars, ma.scalar_count)[ca.roughness] == arr(mb.scalars, mb.scalar_count)[cb.roughness]
 
 
-@pytest.mark.parametrize("graph_material", [0, 1, 2])
+@pytest.mark.parametrize("graph_material", [0, 1, 2, 4])
 def test_flattened_snapshot_renders_as_scene_model(graph_material):
     flat = Flattened(graph_material)
     model = scenes.luisa_demo_scene(graph_material)
@@ -121,6 +122,17 @@ def test_flattened_snapshot_renders_as_scene_model(graph_material):
         plaster = flat.desc.materials[0]
         ops = {(plaster.closures[k].op, plaster.closures[k].a) for k in range(plaster.closure_count)}
         assert (_abi.CLOSURE_GLOSSY, _abi.GLOSSY_BECKMANN) in ops and plaster.flags == 0
+    if graph_material == 4:
+        # the reference compiler's dielectric closures: GGX glass block (IOR in a
+        # scalar slot), Beckmann refraction in the plaster mix
+        block = flat.desc.materials[3]
+        c = block.closures[block.root]
+        assert (c.op, c.a) == (_abi.CLOSURE_GLASS, _abi.GLOSSY_GGX)
+        assert not c.scalar & _abi.INPUT_VALUE
+        assert arr(block.scalars, block.scalar_count)[c.scalar] == np.float32(1.45)
+        plaster = flat.desc.materials[0]
+        ops = {(plaster.closures[k].op, plaster.closures[k].a) for k in range(plaster.closure_count)}
+        assert (_abi.CLOSURE_REFRACTION, _abi.GLOSSY_BECKMANN) in ops
     st = scenes.render_settings(64, 48, max_bounces=4)
     fa, fb = OracleFilm(st), OracleFilm(st)
     fa.render(flat, 0, 4, 4)

@@ -10,8 +10,9 @@ passes must match the oracle's render of the adapter's flattened snapshot
 (relative RMSE 1e-3, at most 1 % of pixels differing in any bit), the PFM
 must hold the Combined pass, and an unsupported pass must be refused with a
 null session.  The plain demo materials, the variant whose block the
-reference compiler lowers to a value stream, and the glossy variant (GGX
-block, diffuse + Beckmann plaster) are rendered."""
+reference compiler lowers to a value stream, the glossy variant (GGX
+block, diffuse + Beckmann plaster) and the dielectric variant (rough GGX
+glass block, diffuse + Beckmann refraction plaster) are rendered."""
 
 import ctypes
 import pathlib
@@ -30,7 +31,7 @@ pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not PROBE.exists(), reason="adapter probe not built (make -C oracle adapter)")]
 
 
-@pytest.mark.parametrize("graph_material", [0, 1, 2])
+@pytest.mark.parametrize("graph_material", [0, 1, 2, 4])
 def test_snapshot_renders_through_the_contract(tmp_path, graph_material):
     from test_adapter import Flattened, probe
     lib = probe()
