@@ -705,7 +705,7 @@ def run_viewports(backend, compiled, count: int = 64, sweep: str = "descent") ->
 # The traffic of a bench launch is this rate times the launch's mean
 # event-timed duration (the procedural workload only).
 NCU_DRAM_GBS = {"intersect": (319.3 + 65.7) / 2.150, "shadow": (109.0 + 13.2) / 1.775,
-                "shade": (615.8 + 297.4) / 1.066}
+                "shade": (666.9 + 409.7) / 1.18}
 
 
 def kernel_profile(args, backend, compiled, settings) -> dict:
@@ -740,6 +740,9 @@ def kernel_profile(args, backend, compiled, settings) -> dict:
     for name, rec in kernels.items():
         rec["frac_of_hbm"] = rec["gbs"] / hbm
         rec["algorithmic_bytes_per_launch"] = rec["algorithmic_bytes"] / rec["launches"] if rec["launches"] else 0.0
+        if args.config == "procedural" and name in NCU_DRAM_GBS and rec["launches"]:
+            # DRAM bytes per launch (read + write), from the ncu rate above
+            rec["traffic_per_launch"] = NCU_DRAM_GBS[name] * 1e9 * (rec["ms"] / 1e3) / rec["launches"]
     return {"kernels": kernels,
             "roofline": {"kernel": f"k_{top}", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,

@@ -104,6 +104,12 @@ class MemoryOutputSink(OutputSink):
         """io::write_pfm of the pass (include/psycles/io/image.h:63)."""
         write_pfm(self.tiles[kind].pixels, path)
 
+    def write_multilayer_exr(self, path, view_layer: str = "ViewLayer") -> None:
+        """io::write_multilayer_exr of every pass the sink holds, in the order
+        they were written (include/psycles/io/image.h:77-84)."""
+        from .exr import write_multilayer_exr
+        write_multilayer_exr(list(self.tiles.values()), path, view_layer)
+
 
 def write_pfm(pixels: np.ndarray, path) -> None:
     """A pass image as a Portable Float Map, as io::write_pfm writes it
