@@ -763,6 +763,13 @@ psy_status psy_debug_light_tree(psy_scene *scene,
                                 const float *queries, const uint32_t *pdf_emitters, uint32_t count,
                                 uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf);
 
+/* Evaluates the compiled scene's flat light distribution pick
+ * (src/luisa/path_tracer_light_distribution.cpp:12-55) on the device for
+ * `count` random numbers: the selected entry's kind (0 emissive triangle,
+ * 1 analytic light, 3 none), index and selection pdf. */
+psy_status psy_debug_light_distribution(psy_scene *scene, const float *u, uint32_t count, uint32_t *out_kind,
+                                        uint32_t *out_index, float *out_pdf);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2925,6 +2925,19 @@ int oracle_light_tree_query(const void *scene, const float *queries, const uint3
 
 uint32_t oracle_scene_emitter_count(const void *scene) { return static_cast<const Scene *>(scene)->emitter_count; }
 
+// The flat light distribution's pick for each random number u: the entry's
+// kind, index and selection pdf.
+void oracle_distribution_sample(const void *scene, const float *u, uint32_t count, uint32_t *out_kind,
+                                uint32_t *out_index, float *out_pdf) {
+    const Scene &s = *static_cast<const Scene *>(scene);
+    for (uint32_t i = 0; i < count; ++i) {
+        const DistEntry e = distribution_sample(s, u[i]);
+        out_kind[i] = e.kind;
+        out_index[i] = e.index;
+        out_pdf[i] = e.selection_pdf;
+    }
+}
+
 // Emitter identity of an emissive (object, cycles primitive) pair.
 uint32_t oracle_light_tree_triangle_emitter(const void *scene, uint32_t object, uint32_t primitive) {
     return tree_emitter(*static_cast<const Scene *>(scene), object, primitive);

@@ -48,6 +48,7 @@ def load() -> ctypes.CDLL:
         lib.oracle_light_tree_triangle_emitter.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32]
         lib.oracle_light_tree_triangle_emitter.restype = ctypes.c_uint32
         lib.oracle_scene_emitter_count.argtypes = [vp]
+        lib.oracle_distribution_sample.argtypes = [vp, vp, ctypes.c_uint32, vp, vp, vp]
         lib.oracle_scene_emitter_count.restype = ctypes.c_uint32
         lib.oracle_pixel_filter_table.argtypes = [ctypes.c_uint32, ctypes.c_float, vp]
         lib.oracle_sample_cosine_hemisphere.argtypes = [vp, vp, vp, vp]
@@ -154,6 +155,16 @@ class OracleScene:
         if self.lib.oracle_light_tree_query(self.handle, _p(q), _p(e), q.shape[0], _p(sel), _p(spdf), _p(rpdf)) != 0:
             raise RuntimeError("scene has no usable light tree")
         return sel, spdf, rpdf
+
+    def distribution_sample(self, u: np.ndarray):
+        """(kind, index, selection pdf) of the flat light distribution's
+        pick for each random number u."""
+        u = np.ascontiguousarray(u, np.float32).reshape(-1)
+        kind = np.zeros(u.size, np.uint32)
+        index = np.zeros(u.size, np.uint32)
+        pdf = np.zeros(u.size, np.float32)
+        self.lib.oracle_distribution_sample(self.handle, _p(u), u.size, _p(kind), _p(index), _p(pdf))
+        return kind, index, pdf
 
     def emitter_count(self) -> int:
         """Emissive triangles + analytic lights of the prepared scene."""

@@ -271,6 +271,8 @@ SIGNATURES = [
     ("psy_scene_device_bytes", ctypes.c_uint64, [ctypes.c_void_p]),
     ("psy_debug_light_tree", ctypes.c_int,
      [ctypes.c_void_p, c_float_p, c_uint32_p, ctypes.c_uint32, c_uint32_p, c_float_p, c_float_p]),
+    ("psy_debug_light_distribution", ctypes.c_int,
+     [ctypes.c_void_p, c_float_p, ctypes.c_uint32, c_uint32_p, c_uint32_p, c_float_p]),
 ]
 
 def default_settings() -> RenderSettings:

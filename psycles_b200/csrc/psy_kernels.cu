@@ -1386,6 +1386,16 @@ __global__ void k_debug_sobol(const float4 *table, uint32_t size, const uint32_t
     out_index[i] = idx;
 }
 
+__global__ void k_debug_light_distribution(const __grid_constant__ SceneView s, const float *u, uint32_t count,
+                                           uint32_t *out_kind, uint32_t *out_index, float *out_pdf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const DistEntryGpu e = distribution_sample(s, u[i]);
+    out_kind[i] = e.kind;
+    out_index[i] = e.index;
+    out_pdf[i] = e.selection_pdf;
+}
+
 __global__ void k_debug_light_tree(const __grid_constant__ SceneView s, const float4 *queries, const uint32_t *pdf_emitters, uint32_t count,
                                    uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1532,6 +1542,10 @@ void launch_debug_light_tree(cudaStream_t st, const SceneView &s, const float4 *
                              uint32_t count, uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf) {
     k_debug_light_tree<<<(count + 127u) / 128u, 128, 0, st>>>(s, queries, pdf_emitters, count, out_emitters,
                                                                out_sample_pdf, out_reverse_pdf);
+}
+void launch_debug_light_distribution(cudaStream_t st, const SceneView &s, const float *u, uint32_t count,
+                                     uint32_t *out_kind, uint32_t *out_index, float *out_pdf) {
+    k_debug_light_distribution<<<(count + 127u) / 128u, 128, 0, st>>>(s, u, count, out_kind, out_index, out_pdf);
 }
 void launch_debug_sobol(cudaStream_t st, const float4 *table, uint32_t size, const uint32_t *queries, uint32_t count,
                         float4 *out, uint32_t *out_index) {

@@ -54,6 +54,8 @@ void launch_film_batch(cudaStream_t st, const LaunchConfig &lc, const JobGpu *jo
                        const PathBuffers &b, uint32_t max_pixels);
 void launch_debug_light_tree(cudaStream_t st, const SceneView &s, const float4 *queries, const uint32_t *pdf_emitters,
                              uint32_t count, uint32_t *out_emitters, float *out_sample_pdf, float *out_reverse_pdf);
+void launch_debug_light_distribution(cudaStream_t st, const SceneView &s, const float *u, uint32_t count,
+                                     uint32_t *out_kind, uint32_t *out_index, float *out_pdf);
 void launch_debug_sobol(cudaStream_t st, const float4 *table, uint32_t size, const uint32_t *queries, uint32_t count,
                         float4 *out, uint32_t *out_index);
 // Reads (after synchronising `st`) and clears the device's count of
