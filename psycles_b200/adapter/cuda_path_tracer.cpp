@@ -7,6 +7,7 @@
 #include <cstring>
 #include <map>
 #include <optional>
+#include <set>
 #include <utility>
 
 #include <psycles/compiler/core_nodes.h>
@@ -311,15 +312,83 @@ struct Flattener {
         return true;
     }
 
+    // The world shader's emission where it is constant: the closure tree
+    // walked as GraphSurfaceImplementation::constant_emission does
+    // (src/luisa/graph_surface_emission.cpp:33-96) -- emission colour x
+    // strength x weight, both children of an add, a mix split by its
+    // clamped factor, nothing from any other closure.  A world whose
+    // emission varies with direction (EmissionEvaluationMode::deferred) is
+    // refused: the CUDA path's world is one constant colour.
+    bool world_emission(contract::MaterialId id, Vec3f &world) {
+        const compiler::CompiledMaterial *m = library.find(id);
+        if (m == nullptr) return error("the world shader was not compiled");
+        const compiler::SurfaceProgram &program = *m->surface_program();
+        if (program.volume_root().valid()) return error("world volumes are not available in the CUDA path");
+        if (program.emission_evaluation() == compiler::EmissionEvaluationMode::none) return true;
+        if (program.emission_evaluation() != compiler::EmissionEvaluationMode::constant || !program.root().valid())
+            return error("world shaders whose emission varies with direction are not available in the CUDA path");
+        const auto &values = program.value_instructions();
+        auto slot = [&](compiler::ValueExpressionId e) -> const contract::SocketValue * {
+            if (!e.valid() || e.value >= values.size() || !values[e.value].parameter.valid()) return nullptr;
+            return m->parameters().find(values[e.value].parameter);
+        };
+        auto scalar = [&](compiler::ValueExpressionId e) {
+            const contract::SocketValue *v = slot(e);
+            return v == nullptr ? 0.0f : scalar_literal(*v).value_or(0.0f);
+        };
+        auto vector = [&](compiler::ValueExpressionId e) {
+            const contract::SocketValue *v = slot(e);
+            return v == nullptr ? Vec3f{} : vector_literal(*v).value_or(Vec3f{});
+        };
+        const auto &closures = program.closure_instructions();
+        auto visit = [&](auto &&self, compiler::ClosureExpressionId c, float weight, int depth) -> void {
+            if (!c.valid() || c.value >= closures.size() || depth > 64) return;
+            const auto &k = closures[c.value];
+            switch (k.operation) {
+            case ClosureOperation::emission: {
+                const Vec3f color = vector(k.color);
+                const float strength = scalar(k.strength);
+                world.x += color.x * strength * weight;
+                world.y += color.y * strength * weight;
+                world.z += color.z * strength * weight;
+                return;
+            }
+            case ClosureOperation::add:
+                self(self, k.a, weight, depth + 1);
+                self(self, k.b, weight, depth + 1);
+                return;
+            case ClosureOperation::mix: {
+                const float mix = std::clamp(scalar(k.factor), 0.0f, 1.0f);
+                self(self, k.a, weight * (1.0f - mix), depth + 1);
+                self(self, k.b, weight * mix, depth + 1);
+                return;
+            }
+            default: return;
+            }
+        };
+        visit(visit, program.root(), 1.0f, 0);
+        return true;
+    }
+
     bool run() {
         const std::string stale = "the material library was not updated from this snapshot";
         if (library.source_revision() != snapshot.revision) return error(stale);
         if (!snapshot.curve_geometries.empty()) return error("curves are not available in the CUDA path");
         if (snapshot.environment) return error("environments are not available in the CUDA path");
-        if (snapshot.world_shader)
-            return error("world shaders are not available in the CUDA path; a constant world is a background light");
-        // materials, in MaterialId order
+        Vec3f world{};
+        if (snapshot.world_shader && !world_emission(*snapshot.world_shader, world)) return false;
+        // materials some instance's triangle uses, in MaterialId order; the
+        // others (an importer's default surface, the world and light
+        // shaders) never reach the device, so what they hold is not refused
+        std::set<contract::MaterialId> used;
+        for (const auto &[iid, inst] : snapshot.instances) {
+            const auto git = snapshot.geometries.find(inst.geometry);
+            if (git == snapshot.geometries.end()) continue;
+            for (std::size_t k = 0; k < git->second.triangles.size(); ++k)
+                if (const auto mid = triangle_material(git->second, inst, k)) used.insert(*mid);
+        }
         for (const auto &[id, desc] : snapshot.materials) {
+            if (!used.count(id)) continue;
             const compiler::CompiledMaterial *m = library.find(id);
             if (m == nullptr) return error("Material " + std::to_string(id.value) + " was not compiled");
             material_index[id] = static_cast<std::uint32_t>(out._materials.size());
@@ -503,7 +572,10 @@ struct Flattener {
         s.material_count = std::uint32_t(out._material_descs.size());
         s.light_count = std::uint32_t(out._lights.size());
         s.camera = c;
-        copy3(s.background, background);
+        // the constant environment is the background lights plus the world
+        // shader's constant emission (make_environment_callables,
+        // src/luisa/path_tracer_environment.cpp:39-50)
+        copy3(s.background, Vec3f{background.x + world.x, background.y + world.y, background.z + world.z});
         s.world_visibility = snapshot.world_visibility_mask == ~std::uint32_t{0u}
                                  ? PSY_VISIBILITY_ALL
                                  : (snapshot.world_visibility_mask & PSY_VISIBILITY_ALL);

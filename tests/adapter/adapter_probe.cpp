@@ -24,6 +24,7 @@
 #include <string>
 #include <vector>
 
+#include <psycles/adapter/blender_scene.h>
 #include <psycles/compiler/core_nodes.h>
 #include <psycles/compiler/material_library.h>
 #include <psycles/contract/scene.h>
@@ -360,6 +361,122 @@ int probe_demo_render(int device, int variant, std::uint32_t width, std::uint32_
     if (backend.create_session(*compiled.scene, bad)) {
         set_error(error, capacity, "an unsupported pass was accepted");
         return 1;
+    }
+    return 0;
+}
+
+}  // extern "C"
+
+// ---- Blender scene bundles -------------------------------------------------
+// The reference's importer (load_blender_scene_bundle) feeding the CUDA
+// backend, as examples/render_blender_scene.cpp:232-420 feeds the Luisa one.
+
+namespace {
+
+// The render settings a bundle asks for (render_blender_scene.cpp:400-417),
+// with the passes the CUDA path produces.
+RenderSettings bundle_settings(const adapter::BlenderSceneImport &imported) {
+    RenderSettings settings;
+    settings.full_extent = {imported.width, imported.height};
+    settings.seed = imported.seed;
+    settings.transparent_background = imported.transparent_background;
+    settings.pixel_filter = imported.pixel_filter;
+    settings.filter_width = imported.filter_width;
+    settings.pass_alpha_threshold = imported.pass_alpha_threshold;
+    settings.integrator = imported.integrator;
+    settings.passes = {PassRequest{PassKind::combined, "Combined", "", 4u}, PassRequest{PassKind::normal, "Normal", "", 4u},
+                       PassRequest{PassKind::albedo, "Albedo", "", 4u},
+                       PassRequest{PassKind::sample_count, "Sample Count", "", 1u}};
+    return settings;
+}
+
+std::string import_error(const adapter::BlenderSceneImport &imported) {
+    for (const auto &d : imported.diagnostics)
+        if (d.severity == adapter::BlenderSceneDiagnosticSeverity::error) return d.message;
+    return "the bundle holds no scene";
+}
+
+}  // namespace
+
+extern "C" {
+
+// A bundle imported by load_blender_scene_bundle, compiled by the
+// reference's MaterialLibrary and flattened by the adapter; `settings`
+// receives the psy_render_settings the adapter makes of the bundle's render
+// settings and `samples` the bundle's sample count.  Null with a message on
+// failure (the importer's first error diagnostic, or the adapter's).
+void *probe_bundle_flatten(const char *directory, psy_render_settings *settings, std::uint32_t *samples, char *error,
+                           std::size_t capacity) {
+    const adapter::BlenderSceneImport imported = adapter::load_blender_scene_bundle(directory);
+    if (!imported.ok()) {
+        set_error(error, capacity, import_error(imported));
+        return nullptr;
+    }
+    compiler::ShaderCompiler shader_compiler{compiler::make_core_node_registry()};
+    compiler::MaterialLibrary library;
+    const compiler::MaterialLibraryUpdate update = library.update(*imported.scene, shader_compiler);
+    if (!update.committed) {
+        set_error(error, capacity, update.diagnostics.empty() ? "material update failed" : update.diagnostics[0].message);
+        return nullptr;
+    }
+    auto result = std::make_unique<Flattened>();
+    std::vector<RenderDiagnostic> diagnostics;
+    if (!cuda_backend::flatten(*imported.scene, library, result->flat, diagnostics)) {
+        set_error(error, capacity, diagnostics.empty() ? "flatten failed" : diagnostics[0].message);
+        return nullptr;
+    }
+    if (settings) *settings = cuda_backend::to_psy_settings(bundle_settings(imported), true);
+    if (samples) *samples = imported.samples;
+    return result.release();
+}
+
+// Renders a bundle through CudaPathTracerBackend with the bundle's own
+// render settings: compile_scene(*imported.scene), create_session,
+// render_samples(SampleRange, OutputSink&) into io::MemoryOutputSink in
+// `chunks` sample ranges of a `spp`-sample render; copies out Combined,
+// Normal, Albedo (4 channels) and Sample Count (1 channel).  Returns 0, or
+// 1 with a message.
+int probe_bundle_render(int device, const char *directory, std::uint32_t spp, std::uint32_t chunks, float *combined,
+                        float *normal, float *albedo, float *sample_count, char *error, std::size_t capacity) {
+    const adapter::BlenderSceneImport imported = adapter::load_blender_scene_bundle(directory);
+    if (!imported.ok()) {
+        set_error(error, capacity, import_error(imported));
+        return 1;
+    }
+    cuda_backend::CudaPathTracerBackend backend{{.device = device, .next_event_estimation = true}};
+    if (!backend.valid()) {
+        set_error(error, capacity, backend.context_error());
+        return 1;
+    }
+    SceneCompilation compiled = backend.compile_scene(*imported.scene);
+    if (!compiled.ok()) {
+        set_error(error, capacity, compiled.diagnostics.empty() ? "compile failed" : compiled.diagnostics[0].message);
+        return 1;
+    }
+    const RenderSettings settings = bundle_settings(imported);
+    std::unique_ptr<RenderSession> session = backend.create_session(*compiled.scene, settings);
+    if (!session) {
+        set_error(error, capacity, "create_session returned nullptr");
+        return 1;
+    }
+    io::MemoryOutputSink sink;
+    const std::uint32_t step = std::max(1u, spp / std::max(chunks, 1u));
+    for (std::uint32_t first = 0; first < spp; first += step) {
+        const SampleRange range{first, std::min(step, spp - first), 0u, spp};
+        if (!session->render_samples(range, sink)) {
+            set_error(error, capacity, std::string("render_samples failed: ") + psy_last_error());
+            return 1;
+        }
+    }
+    float *outs[4] = {combined, normal, albedo, sample_count};
+    const PassKind kinds[4] = {PassKind::combined, PassKind::normal, PassKind::albedo, PassKind::sample_count};
+    for (int k = 0; k < 4; ++k) {
+        const io::PassImage *image = sink.find(kinds[k]);
+        if (!image) {
+            set_error(error, capacity, "a pass is missing from the sink");
+            return 1;
+        }
+        std::memcpy(outs[k], image->pixels.data(), image->pixels.size() * sizeof(float));
     }
     return 0;
 }
