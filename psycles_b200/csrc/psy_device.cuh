@@ -1857,14 +1857,6 @@ __device__ __forceinline__ f3 origin_with_self_exclusion(const SurfacePoint &sp,
 __device__ __forceinline__ DistEntryGpu distribution_sample(const SceneView &s, float u) {
     if (s.emitter_count == 0u) return {0.0f, 0.0f, 3u, 0u};
     uint32_t first = 0u, length = s.emitter_count + 1u;
-    if (s.dist_guide_bits != 0u && u >= 0.0f && u < 1.0f) {
-        // u x 2^bits is exact, so k / 2^bits <= u < (k + 1) / 2^bits: every
-        // entry before guide[k] is <= u and every entry from guide[k + 1] on
-        // is > u, and the search over that range ends where the full one does
-        const uint32_t k = uint32_t(u * float(1u << s.dist_guide_bits));
-        first = s.dist_guide[k];
-        length = s.dist_guide[k + 1u] - first;
-    }
     while (length > 0u) {
         const uint32_t half = length >> 1u;
         const uint32_t middle = first + half;

@@ -1970,31 +1970,6 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         for (uint32_t i = 0; i < tri_n + light_n; ++i) dist[i].cumulative *= inv;
         dist.back().cumulative = 1.0f;
     }
-    // the search guide: 2^bits + 1 entries (bits for about one CDF entry per
-    // interval, at most 2^20), entry k = the search's end for u = k / 2^bits,
-    // the last = every entry; only for a CDF without NaN that never
-    // decreases, where the search's end for u is the count of entries <= u
-    std::vector<uint32_t> dist_guide;
-    uint32_t dist_guide_bits = 0u;
-    {
-        const uint32_t n = uint32_t(dist.size());
-        bool monotone = tri_n + light_n > 0u;
-        for (uint32_t j = 0; j < n && monotone; ++j)
-            monotone = !std::isnan(dist[j].cumulative) && (j == 0u || !(dist[j].cumulative < dist[j - 1u].cumulative));
-        if (monotone && n > 2u) {
-            while (dist_guide_bits < 20u && (1u << dist_guide_bits) < n) ++dist_guide_bits;
-            const uint32_t g = 1u << dist_guide_bits;
-            dist_guide.resize(size_t(g) + 1u);
-            uint32_t j = 0u;
-            for (uint32_t k = 0; k < g; ++k) {
-                const float t = float(k) / float(g);
-                while (j < n && !(t < dist[j].cumulative)) ++j;
-                dist_guide[k] = j;
-            }
-            dist_guide[g] = n;
-        }
-    }
-    if (dist_guide.empty()) dist_guide.push_back(0u);
     std::vector<psy_light_desc> lights(d->lights, d->lights + d->light_count);
     // effective use_mis and forward intersectability (path_tracer_scene.cpp:1787-1830)
     for (psy_light_desc &l : lights) {
@@ -2019,7 +1994,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     // waiting on the device.
     for (DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tlas8, &sc->blas8, &sc->tlas_ids, &sc->tris, &sc->instances, &sc->meshes, &sc->positions, &sc->normals,
                             &sc->indices, &sc->tri_materials, &sc->material_buf, &sc->code, &sc->value_buf, &sc->scalar_buf,
-                            &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->dist_guide, &sc->lights, &sc->lamp_consts,
+                            &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights, &sc->lamp_consts,
                             &sc->lamp_bounds, &sc->lamp_ids})
         b->ordered = st;
     PSY_CUDA_TRY(sc->tlas.upload(tl_wide, st));
@@ -2044,7 +2019,6 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->vector_buf.upload(sc->vectors, st));
     PSY_CUDA_TRY(sc->emitters.upload(sc->emitters_host, st));
     PSY_CUDA_TRY(sc->distribution.upload(dist, st));
-    PSY_CUDA_TRY(sc->dist_guide.upload(dist_guide, st));
     PSY_CUDA_TRY(sc->lights.upload(lights, st));
     std::vector<psy::LampConstGpu> lamp_consts;
     lamp_consts.reserve(lights.size());
@@ -2079,7 +2053,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     sc->stats.upload_bytes = 0u;
     for (const DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tlas8, &sc->blas8, &sc->tlas_ids, &sc->tris, &sc->instances, &sc->meshes, &sc->positions,
                                   &sc->normals, &sc->indices, &sc->tri_materials, &sc->material_buf, &sc->code,
-                                  &sc->value_buf, &sc->scalar_buf, &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->dist_guide, &sc->lights,
+                                  &sc->value_buf, &sc->scalar_buf, &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights,
                                   &sc->lamp_consts, &sc->lamp_bounds, &sc->lamp_ids})
         sc->stats.upload_bytes += b->bytes;
     psy::SceneView &v = sc->view;
@@ -2102,8 +2076,6 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     v.vectors = sc->vector_buf.as<float>();
     v.emitters = sc->emitters.as<psy::EmitterGpu>();
     v.distribution = sc->distribution.as<psy::DistEntryGpu>();
-    v.dist_guide = sc->dist_guide.as<uint32_t>();
-    v.dist_guide_bits = dist_guide_bits;
     v.lights = sc->lights.as<psy_light_desc>();
     v.lamp_bounds = sc->lamp_bounds.as<float4>();
     v.lamp_consts = sc->lamp_consts.as<psy::LampConstGpu>();
@@ -2306,7 +2278,7 @@ uint64_t psy::host::scene_device_bytes(const psy_scene *s) {
     uint64_t n = 0u;
     for (const DeviceBuffer *b : {&s->tlas, &s->blas, &s->tlas8, &s->blas8, &s->tlas_ids, &s->tris, &s->instances, &s->meshes, &s->positions, &s->normals,
                                   &s->indices, &s->tri_materials, &s->material_buf, &s->code, &s->value_buf, &s->scalar_buf,
-                                  &s->vector_buf, &s->emitters, &s->distribution, &s->dist_guide, &s->lights, &s->lamp_consts, &s->lamp_bounds,
+                                  &s->vector_buf, &s->emitters, &s->distribution, &s->lights, &s->lamp_consts, &s->lamp_bounds,
                                   &s->lamp_ids, &s->lt_nodes, &s->lt_emitters, &s->lt_mapping, &s->lt_lookup})
         n += b->bytes;
     return n;

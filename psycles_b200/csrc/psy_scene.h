@@ -168,12 +168,6 @@ struct SceneView {
     const float *vectors;
     const EmitterGpu *emitters;
     const DistEntryGpu *distribution;
-    // Guide of the distribution's search: entry k of the 2^dist_guide_bits + 1
-    // is where the search for u = k / 2^bits ends, so the search for any u
-    // runs between the entries of floor(u 2^bits) and the next one and ends
-    // where the search over the whole CDF would (dist_guide_bits 0: no guide)
-    const uint32_t *dist_guide;
-    uint32_t dist_guide_bits;
     const psy_light_desc *lights;
     uint32_t instance_count;
     uint32_t emitter_count;   // distribution entries - 1 (triangles + lights)

@@ -1,13 +1,12 @@
 """The flat light distribution's pick on the device against the oracle.
 
-The device search runs between two entries of a guide table (the search's
-end for u = k / 2^bits, for every k) instead of over the whole CDF; the pick
-must equal the oracle's full search (src/luisa/path_tracer_light_distribution.cpp:12-55)
-for every random number: the bucket edges k / 2^bits of every table size and
-their neighbours one ulp away (the Cornell box's two equal emitters put a
-CDF value on the edge 1/2), 0, the largest float below 1, 1, NaN, and
-uniform numbers.  The not-gpu test checks that the oracle's picks step
-through the distribution in order."""
+The device's binary search over the cumulative distribution must pick what
+the oracle's search picks (src/luisa/path_tracer_light_distribution.cpp:12-55)
+for every random number: the power-of-two fractions k / 2^bits and their
+neighbours one ulp away (the Cornell box's two equal emitters put a CDF
+value on 1/2), 0, the largest float below 1, 1, NaN, and uniform numbers.
+The not-gpu test checks that the oracle's picks step through the
+distribution in order."""
 
 import ctypes
 
