@@ -705,7 +705,7 @@ def run_viewports(backend, compiled, count: int = 64, sweep: str = "descent") ->
 # The traffic of a bench launch is this rate times the launch's mean
 # event-timed duration (the procedural workload only).
 NCU_DRAM_GBS = {"intersect": (319.3 + 65.7) / 2.150, "shadow": (109.0 + 13.2) / 1.775,
-                "shade": (666.9 + 409.7) / 1.18}
+                "shade": (713.4 + 424.1) / 1.202}
 
 
 def kernel_profile(args, backend, compiled, settings) -> dict:
