@@ -106,6 +106,9 @@ typedef enum psy_closure_op {
  * comes from Cycles' tabulated Fresnel albedo, which is not in the subset. */
 #define PSY_GLOSSY_GGX 0u
 #define PSY_GLOSSY_BECKMANN 1u
+/* glossy only: GGX with Cycles' multiple-scattering energy preservation
+ * (MULTI_GGX); the scene must carry the GGX albedo tables (ggx_e, ggx_eavg) */
+#define PSY_GLOSSY_MULTI_GGX 2u
 
 /* Closure inputs.  A closure input (colour, strength / factor, roughness)
  * is either a slot of the material's parameter block that belongs to the
@@ -302,6 +305,14 @@ typedef struct psy_scene_desc {
     float background[3];         /* constant world colour */
     uint32_t world_visibility;   /* PSY_VISIBILITY_* */
     uint64_t revision;           /* SceneSnapshot revision */
+    /* Cycles' GGX directional albedo E (32 rows of incoming cosine x 32
+     * columns of roughness, both over [0, 1]) and its average over the
+     * cosine (32 values of roughness): the tables table_ggx_E and
+     * table_ggx_Eavg that MULTI_GGX glossy closures read
+     * (src/luisa/graph_surface_scattering.cpp:170-198).  The caller passes
+     * the reference's own tables; null when no material asks for them. */
+    const float *ggx_e;
+    const float *ggx_eavg;
 } psy_scene_desc;
 
 /* ------------------------------------------------------------- settings -- */

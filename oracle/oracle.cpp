@@ -54,6 +54,8 @@ struct Material {
     bool has_emission{false};
     bool has_transparent{false};
     bool bump_correction{true};  // contract::Material::use_bump_map_correction
+    const float *ggx_e{nullptr};     // the scene's GGX albedo tables (MULTI_GGX glossy closures)
+    const float *ggx_eavg{nullptr};
 };
 
 struct Emitter {
@@ -269,6 +271,7 @@ static float input_scalar(const Material &mat, uint32_t ref) {
 // diffuse leaf keeps its authored colour and roughness, a glossy leaf its
 // roughness; a glossy op carries kBeckmann for the Beckmann distribution.
 constexpr uint32_t kBeckmann = 0x100u;
+constexpr uint32_t kMultiscatter = 0x200u;  // a MULTI_GGX glossy op; its closure keeps 1 / E in f0
 inline bool is_glossy(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_GLOSSY; }
 inline bool is_glass(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_GLASS; }
 inline bool is_refraction(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_REFRACTION; }
@@ -311,8 +314,9 @@ static void walk_closures(const Material &mat, uint32_t id, float mix_weight, st
     }
     case PSY_CLOSURE_GLOSSY: {
         const float3 color = input_vector(mat, c.color);
-        const uint32_t op =
-            c.a == PSY_GLOSSY_BECKMANN ? (uint32_t(PSY_CLOSURE_GLOSSY) | kBeckmann) : uint32_t(PSY_CLOSURE_GLOSSY);
+        const uint32_t op = c.a == PSY_GLOSSY_BECKMANN    ? (uint32_t(PSY_CLOSURE_GLOSSY) | kBeckmann)
+                            : c.a == PSY_GLOSSY_MULTI_GGX ? (uint32_t(PSY_CLOSURE_GLOSSY) | kMultiscatter)
+                                                          : uint32_t(PSY_CLOSURE_GLOSSY);
         out.push_back({op, color * mix_weight, color, input_scalar(mat, c.roughness)});
         return;
     }
@@ -417,6 +421,47 @@ static float f0_from_ior(float ior) {
     return r * r;
 }
 
+// cycles_table_1d / cycles_table_2d (src/luisa/graph_surface_state.cpp:84-130):
+// coordinates clamped to [0, 1], linear between the two nearest entries; a
+// 2-D table is y_size rows of x_size entries.
+static float cycles_table_1d(const float *table, float x, uint32_t size) {
+    const float coordinate = clampf(x, 0.0f, 1.0f) * float(size - 1u);
+    const uint32_t index = std::min(uint32_t(coordinate), size - 1u);
+    const uint32_t next = std::min(index + 1u, size - 1u);
+    const float t = coordinate - float(index);
+    return lerp(table[index], table[next], t);
+}
+static float cycles_table_2d(const float *table, float x, float y, uint32_t x_size, uint32_t y_size) {
+    const float coordinate = clampf(y, 0.0f, 1.0f) * float(y_size - 1u);
+    const uint32_t index = std::min(uint32_t(coordinate), y_size - 1u);
+    const uint32_t next = std::min(index + 1u, y_size - 1u);
+    const float t = coordinate - float(index);
+    const float d0 = cycles_table_1d(table + x_size * index, x, x_size);
+    const float d1 = cycles_table_1d(table + x_size * next, x, x_size);
+    return lerp(d0, d1, t);
+}
+
+// ggx_energy (src/luisa/graph_surface_scattering.cpp:170-198): MULTI_GGX's
+// darkening of the weight, (1 + Fms (1 - E) / E) E, and evaluation scale 1 / E.
+struct GgxEnergy {
+    float3 darkening;
+    float energy_scale;
+};
+static GgxEnergy ggx_energy(const Material &mat, float roughness, float incoming_cosine, float3 fss) {
+    const float energy = maxf(cycles_table_2d(mat.ggx_e, roughness, incoming_cosine, 32u, 32u), 1.0e-20f);
+    const float average = cycles_table_1d(mat.ggx_eavg, roughness, 32u);
+    const float missing = (1.0f - energy) / energy;
+    const float scale = 1.0f / energy;
+    const float3 fms(fss.x * average / maxf(1.0f - fss.x * (1.0f - average), 1.0e-20f),
+                     fss.y * average / maxf(1.0f - fss.y * (1.0f - average), 1.0e-20f),
+                     fss.z * average / maxf(1.0f - fss.z * (1.0f - average), 1.0e-20f));
+    GgxEnergy r;
+    r.darkening = float3((1.0f + fms.x * missing) / scale, (1.0f + fms.y * missing) / scale,
+                         (1.0f + fms.z * missing) / scale);
+    r.energy_scale = scale;
+    return r;
+}
+
 // Closure allocation (graph_surface_state.cpp:26-48,
 // graph_surface_physical_closures.cpp:158-520): diffuse goes through
 // bsdf_alloc (negative weight clamped, average cutoff 1e-5); glossy is
@@ -454,6 +499,15 @@ static SurfaceClosures collect_surface(const Material &mat, const ClosurePoint &
             p.weight = allocated;
             p.sample_weight = allocation * closure_sample_weight(f3(1.0f));
             p.normal = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, closure_normal);
+            if ((t.op & kMultiscatter) != 0u) {
+                // MULTI_GGX (graph_surface_physical_closures.cpp:379-391): the Fresnel
+                // single-scattering albedo is max(colour, 0)
+                const GgxEnergy e = ggx_energy(mat, clampf(t.roughness, 0.0f, 1.0f),
+                                               clampf(dot(p.normal, incoming), 0.0f, 1.0f), max3(t.color, f3(0.0f)));
+                p.weight = allocated * e.darkening;
+                p.sample_weight = allocation * closure_sample_weight(e.darkening);
+                p.f0 = e.energy_scale;
+            }
         } else if (is_dielectric(t.op)) {
             // MicrofacetGlassComponent::setup (microfacet_glass_component.cpp:180-232): the
             // corrected normal, roughness sqrt(clamp(r^2)), the IOR inverted on a
@@ -603,7 +657,10 @@ static float microfacet_intensity(const PhysicalClosure &c, float3 incoming, flo
     const float alpha = maxf(microfacet_alpha(c.roughness), 1.0e-10f);
     const float d = microfacet_distribution(beckmann, ndh, alpha);
     const float g = 1.0f / (1.0f + microfacet_lambda(beckmann, ndv, alpha) + microfacet_lambda(beckmann, ndl, alpha));
-    const float intensity = d * g / maxf(4.0f * ndv, 1.0e-20f);
+    // the glossy Fresnel factor: one, or MULTI_GGX's scale 1 / E (microfacet_reflection_fresnel,
+    // graph_surface_scattering.cpp:632-662)
+    const float fresnel = (c.op & kMultiscatter) != 0u ? c.f0 : 1.0f;
+    const float intensity = fresnel * d * g / maxf(4.0f * ndv, 1.0e-20f);
     return (ndv > 0.0f && ndl > 0.0f && ndh > 0.0f && vdh > 0.0f && !singular) ? intensity : 0.0f;
 }
 static float microfacet_pdf(const PhysicalClosure &c, float3 incoming, float3 outgoing, float3 gn) {
@@ -969,9 +1026,9 @@ static SurfaceSample sample_surface(const SurfaceClosures &s, const ClosurePoint
         r.f += c.weight * 1.0e6f;
         delta_pdf_numerator = 1.0e6f * weights[chosen];
     } else if (glossy && singular) {
-        // singular_evaluation = weight x Fresnel (one) x bump term (one
-        // when sampling a glossy closure) x 1e6, singular pdf 1e6
-        r.f += c.weight * 1.0e6f;
+        // singular_evaluation = weight x Fresnel (one, or MULTI_GGX's scale)
+        // x bump term (one when sampling a glossy closure) x 1e6, singular pdf 1e6
+        r.f += (c.op & kMultiscatter) != 0u ? c.weight * c.f0 * 1.0e6f : c.weight * 1.0e6f;
         delta_pdf_numerator = 1.0e6f * weights[chosen];
     } else if (dielectric && singular) {
         r.f += gs.singular_evaluation;
@@ -2514,6 +2571,8 @@ static std::unique_ptr<Scene> prepare_scene(const psy_scene_desc *d, bool brute_
         m.bump_correction = (md.flags & PSY_MATERIAL_NO_BUMP_MAP_CORRECTION) == 0u;
         m.has_emission = program_has(m, PSY_CLOSURE_EMISSION);
         m.has_transparent = program_has(m, PSY_CLOSURE_TRANSPARENT);
+        m.ggx_e = d->ggx_e;
+        m.ggx_eavg = d->ggx_eavg;
         s->materials.push_back(std::move(m));
     }
     for (uint32_t i = 0; i < d->instance_count; ++i) {

@@ -12,6 +12,8 @@
 #include <span>
 #include <vector>
 
+#include "cycles_shader_tables_4_5_10.inl"
+
 extern "C" {
 
 int ref_sobol_generate_table(unsigned size, float *out) {
@@ -112,6 +114,14 @@ int ref_build_light_tree(const float *in, unsigned n, unsigned max_leaf, unsigne
     } catch (...) {
         return 1;
     }
+}
+
+// Cycles' GGX albedo tables as the reference ships them
+// (src/luisa/cycles_shader_tables_4_5_10.inl, table_ggx_E: 32 x 32,
+// table_ggx_Eavg: 32), for scenes with MULTI_GGX glossy closures.
+void ref_ggx_tables(float *e, float *eavg) {
+    for (int i = 0; i < 1024; ++i) e[i] = psycles::luisa_backend::cycles45_tables::table_ggx_E[i];
+    for (int i = 0; i < 32; ++i) eavg[i] = psycles::luisa_backend::cycles45_tables::table_ggx_Eavg[i];
 }
 
 }  // extern "C"

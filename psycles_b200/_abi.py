@@ -25,7 +25,7 @@ STATUS_NAMES = {
 
 (CLOSURE_NULL, CLOSURE_DIFFUSE, CLOSURE_EMISSION, CLOSURE_TRANSPARENT, CLOSURE_ADD, CLOSURE_MIX, CLOSURE_GLOSSY,
  CLOSURE_GLASS, CLOSURE_REFRACTION) = range(9)
-GLOSSY_GGX, GLOSSY_BECKMANN = 0, 1
+GLOSSY_GGX, GLOSSY_BECKMANN, GLOSSY_MULTI_GGX = 0, 1, 2
 MATERIAL_NO_BUMP_MAP_CORRECTION = 1
 LIGHT_POINT, LIGHT_SPOT, LIGHT_AREA, LIGHT_DISTANT = range(4)
 LIGHT_FLAG_SPHERE, LIGHT_FLAG_NORMALIZE, LIGHT_FLAG_ELLIPSE, LIGHT_FLAG_USE_MIS = 1, 2, 4, 8
@@ -109,7 +109,8 @@ class SceneDesc(ctypes.Structure):
                 ("mesh_count", ctypes.c_uint32), ("instance_count", ctypes.c_uint32),
                 ("material_count", ctypes.c_uint32), ("light_count", ctypes.c_uint32),
                 ("camera", CameraDesc), ("background", ctypes.c_float * 3),
-                ("world_visibility", ctypes.c_uint32), ("revision", ctypes.c_uint64)]
+                ("world_visibility", ctypes.c_uint32), ("revision", ctypes.c_uint64),
+                ("ggx_e", c_float_p), ("ggx_eavg", c_float_p)]
 
 
 class RenderSettings(ctypes.Structure):

@@ -337,6 +337,10 @@ template <> struct ClosureSlot<true> {
 };
 
 constexpr uint32_t kGlossyBeckmann = 0x100u;
+// A glossy op with kGlossyMultiscatter is MULTI_GGX: GGX with Cycles' tabulated
+// multiple-scattering energy preservation; its closure keeps the evaluation
+// scale 1 / E in `f0`.
+constexpr uint32_t kGlossyMultiscatter = 0x200u;
 __device__ __forceinline__ bool is_glossy(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_GLOSSY; }
 __device__ __forceinline__ bool is_glass(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_GLASS; }
 __device__ __forceinline__ bool is_refraction(uint32_t op) { return (op & 0xffu) == PSY_CLOSURE_REFRACTION; }
@@ -547,8 +551,9 @@ __device__ __forceinline__ void walk_closures(const SceneView &s, const Material
         } else if (c.op == PSY_CLOSURE_GLOSSY) {
             if constexpr ((kLeaves & kLeafGlossy) != 0u) {
                 const f3 color = input_vector(s, m, c.color);
-                const uint32_t op = c.a == PSY_GLOSSY_BECKMANN ? (uint32_t(PSY_CLOSURE_GLOSSY) | kGlossyBeckmann)
-                                                               : uint32_t(PSY_CLOSURE_GLOSSY);
+                const uint32_t op = c.a == PSY_GLOSSY_BECKMANN    ? (uint32_t(PSY_CLOSURE_GLOSSY) | kGlossyBeckmann)
+                                    : c.a == PSY_GLOSSY_MULTI_GGX ? (uint32_t(PSY_CLOSURE_GLOSSY) | kGlossyMultiscatter)
+                                                                  : uint32_t(PSY_CLOSURE_GLOSSY);
                 visit(op, color * w, color, input_scalar(s, m, c.roughness), 1.0f);
             }
         } else if (c.op == PSY_CLOSURE_GLASS || c.op == PSY_CLOSURE_REFRACTION) {
@@ -603,6 +608,52 @@ __device__ __forceinline__ float fresnel_dielectric_cos(float cosine, float eta)
     const float regular = 0.5f * a * a * (1.0f + b * b);
     return g2 > 0.0f ? regular : 1.0f;
 }
+// Cycles' table lookups (cycles_table_1d / cycles_table_2d,
+// src/luisa/graph_surface_state.cpp:84-130): x and y clamped to [0, 1],
+// linear between the two nearest entries; a 2-D table is y_size rows of
+// x_size entries.
+__device__ __forceinline__ float cycles_table_1d(const float *table, float x, uint32_t size) {
+    const float coordinate = clampf_(x, 0.0f, 1.0f) * float(size - 1u);
+    const uint32_t index = min(uint32_t(coordinate), size - 1u);
+    const uint32_t next = min(index + 1u, size - 1u);
+    const float t = coordinate - float(index);
+    return lerpf_(__ldg(table + index), __ldg(table + next), t);
+}
+__device__ __forceinline__ float cycles_table_2d(const float *table, float x, float y, uint32_t x_size,
+                                                 uint32_t y_size) {
+    const float coordinate = clampf_(y, 0.0f, 1.0f) * float(y_size - 1u);
+    const uint32_t index = min(uint32_t(coordinate), y_size - 1u);
+    const uint32_t next = min(index + 1u, y_size - 1u);
+    const float t = coordinate - float(index);
+    const float d0 = cycles_table_1d(table + x_size * index, x, x_size);
+    const float d1 = cycles_table_1d(table + x_size * next, x, x_size);
+    return lerpf_(d0, d1, t);
+}
+
+struct GgxEnergy {
+    f3 darkening;
+    float energy_scale;
+};
+
+// ggx_energy (src/luisa/graph_surface_scattering.cpp:170-198): GGX's
+// directional albedo E(roughness, cos) and its average, the single-scattering
+// Fresnel albedo `fss` turned into the multiple-scattering one, the weight's
+// darkening (1 + Fms (1 - E) / E) E and the evaluation scale 1 / E.
+__device__ __noinline__ GgxEnergy ggx_energy(const SceneView &s, float roughness, float incoming_cosine, f3 fss) {
+    const float energy = maxf_(cycles_table_2d(s.ggx_e, roughness, incoming_cosine, 32u, 32u), 1.0e-20f);
+    const float average = cycles_table_1d(s.ggx_eavg, roughness, 32u);
+    const float missing = (1.0f - energy) / energy;
+    const float scale = 1.0f / energy;
+    const f3 fms = mk3(fss.x * average / maxf_(1.0f - fss.x * (1.0f - average), 1.0e-20f),
+                       fss.y * average / maxf_(1.0f - fss.y * (1.0f - average), 1.0e-20f),
+                       fss.z * average / maxf_(1.0f - fss.z * (1.0f - average), 1.0e-20f));
+    GgxEnergy r;
+    r.darkening = mk3((1.0f + fms.x * missing) / scale, (1.0f + fms.y * missing) / scale,
+                      (1.0f + fms.z * missing) / scale);
+    r.energy_scale = scale;
+    return r;
+}
+
 __device__ __forceinline__ float f0_from_ior(float ior) {
     const float r = (ior - 1.0f) / maxf_(ior + 1.0f, 1.0e-20f);
     return r * r;
@@ -650,6 +701,18 @@ __device__ __forceinline__ void collect_surface(const SceneView &s, const Materi
             p.weight = allocated;
             p.sample_weight = allocation * closure_sample_weight(mk3(1.0f));
             p.color = specular_normal(pt.bump_correction, pt.geometric_normal, pt.view, out.normal);
+            if constexpr (kGlossy) {
+                if ((op & kGlossyMultiscatter) != 0u) {
+                    // ggx_energy (graph_surface_scattering.cpp:170-198) with the Fresnel
+                    // single-scattering albedo max(colour, 0); the weight takes the
+                    // darkening, evaluations the scale 1 / E
+                    const GgxEnergy e = ggx_energy(s, clampf_(roughness, 0.0f, 1.0f),
+                                                   clampf_(dot(p.color, pt.view), 0.0f, 1.0f), max3(color, mk3(0.0f)));
+                    p.weight = allocated * e.darkening;
+                    p.sample_weight = allocation * closure_sample_weight(e.darkening);
+                    p.f0 = e.energy_scale;
+                }
+            }
         } else if (kGlossy && is_dielectric(op)) {
             // MicrofacetGlassComponent::setup (microfacet_glass_component.cpp:180-232): the
             // corrected normal, roughness sqrt(clamp(r^2)), the IOR inverted on a back
@@ -807,7 +870,8 @@ __device__ __forceinline__ float microfacet_lambda(bool beckmann, float n_dot_v,
 struct Microfacet {
     float intensity, pdf;
 };
-__device__ __noinline__ Microfacet microfacet_eval(uint32_t op, float roughness, f3 incoming, f3 outgoing, f3 gn) {
+__device__ __noinline__ Microfacet microfacet_eval(uint32_t op, float roughness, f3 incoming, f3 outgoing, f3 gn,
+                                                   float fresnel) {
     const bool beckmann = (op & kGlossyBeckmann) != 0u;
     const float ndv = maxf_(dot(gn, incoming), 0.0f);
     const float ndl = maxf_(dot(gn, outgoing), 0.0f);
@@ -821,7 +885,7 @@ __device__ __noinline__ Microfacet microfacet_eval(uint32_t op, float roughness,
     const float g = 1.0f / (1.0f + lv + microfacet_lambda(beckmann, ndl, alpha));
     const bool valid = ndv > 0.0f && ndl > 0.0f && ndh > 0.0f && vdh > 0.0f && !singular;
     Microfacet r;
-    r.intensity = valid ? d * g / maxf_(4.0f * ndv, 1.0e-20f) : 0.0f;
+    r.intensity = valid ? fresnel * d * g / maxf_(4.0f * ndv, 1.0e-20f) : 0.0f;
     r.pdf = valid ? d / maxf_(4.0f * ndv, 1.0e-20f) / (1.0f + lv) : 0.0f;
     return r;
 }
@@ -1049,13 +1113,16 @@ __device__ __noinline__ Evaluation evaluate_mixture(const SurfaceClosures<kGloss
                 e.events |= kEventGlossy | (transmission ? kEventTransmission : kEventReflection);
             continue;
         }
-        if (kGlossy && is_glossy(c.op)) {
+        if constexpr (kGlossy) if (is_glossy(c.op)) {
             if (!glossy_enabled) continue;
             const bool is_selected = int(i) == selected;
             const float gb = bump_shadowing(pt.shading_normal, c.color, outgoing, !is_selected, false,
                                             pt.bump_correction);
             const f3 gn = specular_normal(pt.bump_correction, pt.geometric_normal, incoming, c.color);
-            const Microfacet m = microfacet_eval(c.op, c.roughness, incoming, outgoing, gn);
+            // the glossy Fresnel factor: one, or MULTI_GGX's scale 1 / E
+            // (microfacet_reflection_fresnel, graph_surface_scattering.cpp:632-662)
+            const float fresnel = (c.op & kGlossyMultiscatter) != 0u ? c.f0 : 1.0f;
+            const Microfacet m = microfacet_eval(c.op, c.roughness, incoming, outgoing, gn, fresnel);
             const float pdf = (gb != 0.0f || is_selected) ? m.pdf : 0.0f;
             const f3 value = c.weight * m.intensity * gb;
             e.f = e.f + value;
@@ -1194,9 +1261,14 @@ __device__ __forceinline__ SurfaceSample sample_surface(const SurfaceClosures<kG
     r.f = mixture.f;
     float delta = 0.0f;
     if (transparent || (glossy && singular)) {
-        // transparent: weight x 1e6; singular glossy: weight x Fresnel (one)
-        // x bump term (one when sampling a glossy closure) x 1e6
-        r.f = r.f + c.weight * 1.0e6f;
+        // transparent: weight x 1e6; singular glossy: weight x Fresnel (one, or
+        // MULTI_GGX's scale) x bump term (one when sampling a glossy closure) x 1e6
+        if constexpr (kGlossy) {
+            if (glossy && (c.op & kGlossyMultiscatter) != 0u) r.f = r.f + c.weight * c.f0 * 1.0e6f;
+            else r.f = r.f + c.weight * 1.0e6f;
+        } else {
+            r.f = r.f + c.weight * 1.0e6f;
+        }
         delta = 1.0e6f * chosen_weight;
     } else if (dielectric && singular) {
         r.f = r.f + dielectric_delta;

@@ -1084,8 +1084,9 @@ psy_status validate_material(const psy_material_desc &m) {
             return fail(PSY_ERROR_INVALID_ARGUMENT, "closure scalar input out of range");
         if ((c.op == PSY_CLOSURE_DIFFUSE || microfacet) && !input_ok(c.roughness, S, true))
             return fail(PSY_ERROR_INVALID_ARGUMENT, "closure roughness input out of range");
-        if (microfacet && c.a != PSY_GLOSSY_GGX && c.a != PSY_GLOSSY_BECKMANN)
-            return fail(PSY_ERROR_UNSUPPORTED, "microfacet distribution outside GGX and Beckmann");
+        if (microfacet && c.a != PSY_GLOSSY_GGX && c.a != PSY_GLOSSY_BECKMANN &&
+            !(c.op == PSY_CLOSURE_GLOSSY && c.a == PSY_GLOSSY_MULTI_GGX))
+            return fail(PSY_ERROR_UNSUPPORTED, "microfacet distribution outside GGX, Beckmann and (glossy) MULTI_GGX");
     }
     // The device walks the tree with a 32-entry stack and keeps at most 16
     // BSDF closures per shading point (the reference's capacity is Cycles'
@@ -1860,6 +1861,18 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
         sc->materials.push_back(g);
     }
 
+    // ---- Cycles' GGX albedo tables, for MULTI_GGX glossy closures
+    bool any_multi_ggx = false;
+    for (const psy_closure_instruction &c : code)
+        if (c.op == PSY_CLOSURE_GLOSSY && c.a == PSY_GLOSSY_MULTI_GGX) any_multi_ggx = true;
+    if (any_multi_ggx && (d->ggx_e == nullptr || d->ggx_eavg == nullptr))
+        return fail(PSY_ERROR_INVALID_ARGUMENT, "MULTI_GGX glossy closures need the scene's GGX albedo tables");
+    std::vector<float> ggx_tables;
+    if (any_multi_ggx) {
+        ggx_tables.assign(d->ggx_e, d->ggx_e + psy::kGgxETableSize);
+        ggx_tables.insert(ggx_tables.end(), d->ggx_eavg, d->ggx_eavg + psy::kGgxEavgTableSize);
+    }
+
     // ---- emissive triangles + flat light distribution
     // (src/sampling/light_distribution.cpp:25-150; emitter geometry as in
     // src/luisa/path_kernel_emissive_triangle.cpp:80-150)
@@ -1994,7 +2007,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     // waiting on the device.
     for (DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tlas8, &sc->blas8, &sc->tlas_ids, &sc->tris, &sc->instances, &sc->meshes, &sc->positions, &sc->normals,
                             &sc->indices, &sc->tri_materials, &sc->material_buf, &sc->code, &sc->value_buf, &sc->scalar_buf,
-                            &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights, &sc->lamp_consts,
+                            &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->ggx_tables, &sc->lights, &sc->lamp_consts,
                             &sc->lamp_bounds, &sc->lamp_ids})
         b->ordered = st;
     PSY_CUDA_TRY(sc->tlas.upload(tl_wide, st));
@@ -2019,6 +2032,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     PSY_CUDA_TRY(sc->vector_buf.upload(sc->vectors, st));
     PSY_CUDA_TRY(sc->emitters.upload(sc->emitters_host, st));
     PSY_CUDA_TRY(sc->distribution.upload(dist, st));
+    if (!ggx_tables.empty()) PSY_CUDA_TRY(sc->ggx_tables.upload(ggx_tables, st));
     PSY_CUDA_TRY(sc->lights.upload(lights, st));
     std::vector<psy::LampConstGpu> lamp_consts;
     lamp_consts.reserve(lights.size());
@@ -2053,7 +2067,7 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     sc->stats.upload_bytes = 0u;
     for (const DeviceBuffer *b : {&sc->tlas, &sc->blas, &sc->tlas8, &sc->blas8, &sc->tlas_ids, &sc->tris, &sc->instances, &sc->meshes, &sc->positions,
                                   &sc->normals, &sc->indices, &sc->tri_materials, &sc->material_buf, &sc->code,
-                                  &sc->value_buf, &sc->scalar_buf, &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->lights,
+                                  &sc->value_buf, &sc->scalar_buf, &sc->vector_buf, &sc->emitters, &sc->distribution, &sc->ggx_tables, &sc->lights,
                                   &sc->lamp_consts, &sc->lamp_bounds, &sc->lamp_ids})
         sc->stats.upload_bytes += b->bytes;
     psy::SceneView &v = sc->view;
@@ -2076,6 +2090,8 @@ psy_status psy_scene_compile(psy_context *ctx, const psy_scene_desc *d, psy_scen
     v.vectors = sc->vector_buf.as<float>();
     v.emitters = sc->emitters.as<psy::EmitterGpu>();
     v.distribution = sc->distribution.as<psy::DistEntryGpu>();
+    v.ggx_e = ggx_tables.empty() ? nullptr : sc->ggx_tables.as<float>();
+    v.ggx_eavg = ggx_tables.empty() ? nullptr : sc->ggx_tables.as<float>() + psy::kGgxETableSize;
     v.lights = sc->lights.as<psy_light_desc>();
     v.lamp_bounds = sc->lamp_bounds.as<float4>();
     v.lamp_consts = sc->lamp_consts.as<psy::LampConstGpu>();
@@ -2278,7 +2294,7 @@ uint64_t psy::host::scene_device_bytes(const psy_scene *s) {
     uint64_t n = 0u;
     for (const DeviceBuffer *b : {&s->tlas, &s->blas, &s->tlas8, &s->blas8, &s->tlas_ids, &s->tris, &s->instances, &s->meshes, &s->positions, &s->normals,
                                   &s->indices, &s->tri_materials, &s->material_buf, &s->code, &s->value_buf, &s->scalar_buf,
-                                  &s->vector_buf, &s->emitters, &s->distribution, &s->lights, &s->lamp_consts, &s->lamp_bounds,
+                                  &s->vector_buf, &s->emitters, &s->distribution, &s->ggx_tables, &s->lights, &s->lamp_consts, &s->lamp_bounds,
                                   &s->lamp_ids, &s->lt_nodes, &s->lt_emitters, &s->lt_mapping, &s->lt_lookup})
         n += b->bytes;
     return n;

@@ -155,7 +155,7 @@ struct psy_scene {
     std::vector<psy::MaterialGpu> materials;
     std::vector<float> scalars, vectors;
     psy::host::DeviceBuffer tlas, blas, tlas8, blas8, tlas_ids, tris, instances, meshes, positions, normals, indices, tri_materials, material_buf, code,
-        value_buf, scalar_buf, vector_buf, emitters, distribution, lights, lamp_consts, lamp_bounds, lamp_ids, lt_nodes, lt_emitters,
+        value_buf, scalar_buf, vector_buf, emitters, distribution, ggx_tables, lights, lamp_consts, lamp_bounds, lamp_ids, lt_nodes, lt_emitters,
         lt_mapping, lt_lookup;
     psy::SceneView view{};
     uint64_t triangle_count = 0;

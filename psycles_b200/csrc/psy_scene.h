@@ -53,6 +53,7 @@ constexpr uint32_t kTagMask = 3u << 30;
 // splits or rejecting the scene where needed; a debug build
 // (-DPSY_STACK_CHECK=1) also counts pushes that would not fit on the device.
 constexpr uint32_t kTraversalStackSize = 48u;
+constexpr uint32_t kGgxETableSize = 32u * 32u, kGgxEavgTableSize = 32u;
 // Entries (node groups) of the 8-wide traversal's stack.
 constexpr uint32_t kTraversalStackSize8 = 32u;
 
@@ -168,6 +169,11 @@ struct SceneView {
     const float *vectors;
     const EmitterGpu *emitters;
     const DistEntryGpu *distribution;
+    // Cycles' GGX albedo tables (null unless a material has a MULTI_GGX glossy
+    // closure): E, 32 rows of incoming cosine x 32 columns of roughness, and
+    // its average over the cosine, 32 values of roughness
+    const float *ggx_e;
+    const float *ggx_eavg;
     const psy_light_desc *lights;
     uint32_t instance_count;
     uint32_t emitter_count;   // distribution entries - 1 (triangles + lights)

@@ -78,6 +78,9 @@ class NodeType(str, enum.Enum):
 CLOSURE_TYPES = (NodeType.DIFFUSE, NodeType.EMISSION, NodeType.TRANSPARENT, NodeType.GLOSSY, NodeType.GLASS,
                  NodeType.REFRACTION, NodeType.ADD, NodeType.MIX)
 GLOSSY_DISTRIBUTIONS = {"GGX": _abi.GLOSSY_GGX, "BECKMANN": _abi.GLOSSY_BECKMANN}
+# the Glossy BSDF also takes MULTI_GGX (GGX with Cycles' tabulated energy
+# preservation; the scene carries the GGX albedo tables)
+GLOSSY_ONLY_DISTRIBUTIONS = {**GLOSSY_DISTRIBUTIONS, "MULTI_GGX": _abi.GLOSSY_MULTI_GGX}
 
 F, C = "float", "color"  # socket kinds: scalar and vector values
 
@@ -184,10 +187,10 @@ class ShaderGraph:
         return self._node(NodeType.DIFFUSE, Color=color, Roughness=roughness)
 
     def glossy_bsdf(self, color, roughness=0.2, distribution: str = "GGX") -> int:
-        """Glossy BSDF (core_nodes.cpp:980-990): GGX or Beckmann microfacet
-        reflection; the Distribution property is structural."""
-        if distribution not in GLOSSY_DISTRIBUTIONS:
-            raise ShaderGraphError(f"glossy distribution {distribution!r} outside GGX and BECKMANN")
+        """Glossy BSDF (core_nodes.cpp:980-990): GGX, Beckmann or MULTI_GGX
+        microfacet reflection; the Distribution property is structural."""
+        if distribution not in GLOSSY_ONLY_DISTRIBUTIONS:
+            raise ShaderGraphError(f"glossy distribution {distribution!r} outside GGX, BECKMANN and MULTI_GGX")
         return self._node(NodeType.GLOSSY, {"Distribution": distribution}, Color=color, Roughness=roughness)
 
     def glass_bsdf(self, color=(1.0, 1.0, 1.0), roughness=0.0, ior=1.5, distribution: str = "GGX") -> int:
@@ -471,7 +474,7 @@ def compile_surface_program(graph: ShaderGraph) -> tuple[SurfaceProgram, Surface
         elif n.type == NodeType.TRANSPARENT:
             code.append((_abi.CLOSURE_TRANSPARENT, 0, 0, low.closure_input(n, "Color"), none, none))
         elif n.type == NodeType.GLOSSY:
-            code.append((_abi.CLOSURE_GLOSSY, GLOSSY_DISTRIBUTIONS[n.props.get("Distribution", "GGX")], 0,
+            code.append((_abi.CLOSURE_GLOSSY, GLOSSY_ONLY_DISTRIBUTIONS[n.props.get("Distribution", "GGX")], 0,
                          low.closure_input(n, "Color"), none, low.closure_input(n, "Roughness")))
         elif n.type in (NodeType.GLASS, NodeType.REFRACTION):
             op = _abi.CLOSURE_GLASS if n.type == NodeType.GLASS else _abi.CLOSURE_REFRACTION

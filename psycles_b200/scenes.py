@@ -104,6 +104,9 @@ class Scene:
     background: tuple = (0.0, 0.0, 0.0)
     world_visibility: int = _abi.VIS_ALL
     revision: int = 1
+    # Cycles' GGX albedo tables (E: 1024 floats, Eavg: 32) for MULTI_GGX glossy
+    # closures; the caller supplies the reference's own tables
+    ggx_tables: tuple | None = None
 
     @property
     def instanced_triangles(self) -> int:
@@ -231,8 +234,13 @@ class SceneDescHandle:
         desc.background[:] = scene.background
         desc.world_visibility = scene.world_visibility
         desc.revision = scene.revision
+        tables = ()
+        if scene.ggx_tables is not None:
+            tables = tuple(np.ascontiguousarray(t, dtype=np.float32) for t in scene.ggx_tables)
+            desc.ggx_e = tables[0].ctypes.data_as(_abi.c_float_p)
+            desc.ggx_eavg = tables[1].ctypes.data_as(_abi.c_float_p)
         self.desc = desc
-        self._keep = (keep, meshes, instances, materials, lights)
+        self._keep = (keep, meshes, instances, materials, lights, tables)
 
     @property
     def pointer(self):

@@ -29,7 +29,7 @@ def test_glossy_lowering():
     c2 = prog2.closures[prog2.root]
     assert c2[1] == _abi.GLOSSY_GGX and not c2[5] & _abi.INPUT_VALUE
     with pytest.raises(ShaderGraphError):
-        ShaderGraph().glossy_bsdf((1, 1, 1), 0.2, "MULTI_GGX")
+        ShaderGraph().glossy_bsdf((1, 1, 1), 0.2, "ASHIKHMIN_SHIRLEY")
 
 
 def test_distribution_is_structural():
